@@ -1,0 +1,224 @@
+"""ctypes mirror of include/dsp.h.
+
+This is the thin binding a ctypes user of the C ABI writes: the structures of
+dsp.h, the prototypes of the entry points, and a helper that packs per-instance
+arrays into a ``dsp_flux_batch``.  The same structures are passed to the CPU
+oracle library in tests, so both sides see byte-identical inputs.
+
+Arrays may be numpy arrays (host memory) or torch tensors (host or device); an
+array of one instance's shape is shared by all instances (stride 0), an array
+with a leading ``n_inst`` axis is per instance.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+from ctypes import POINTER, c_double, c_int32, c_int64, c_uint32, c_void_p
+
+import numpy as np
+
+DSP_OK = 0
+DSP_ERR_INVALID_INPUT = 1
+DSP_ERR_SINGULAR = 2
+DSP_ERR_NONFINITE = 3
+DSP_ERR_TIMEOUT = 4
+DSP_ERR_CUDA = 5
+DSP_ERR_UNSUPPORTED = 6
+DSP_ERR_NO_MEMORY = 7
+DSP_ERR_EIGEN = 8
+DSP_ERR_NOT_INITIALIZED = 9
+
+STATUS_NAMES = {
+    0: "OK", 1: "INVALID_INPUT", 2: "SINGULAR", 3: "NONFINITE", 4: "TIMEOUT",
+    5: "CUDA_ERROR", 6: "UNSUPPORTED", 7: "NO_MEMORY", 8: "EIGEN", 9: "NOT_INITIALIZED",
+}
+
+FLAG_THERMAL = 1 << 0
+FLAG_DELTA_M_PLUS = 1 << 1
+FLAG_DIFFUSION_LOWER_BC = 1 << 2
+FLAG_INDEX_FROM_BOTTOM = 1 << 3
+FLAG_DEVICE_POINTERS = 1 << 4
+FLAG_SPHERICAL_BEAM = 1 << 5
+FLAG_TEMPERATURE_JAC = 1 << 6
+
+SUPPORTED_NSTR = (4, 6, 8, 10, 12, 14, 16, 32, 64)
+
+
+class DArray(ctypes.Structure):
+    _fields_ = [("ptr", c_void_p), ("stride", c_int64)]
+
+
+FLUX_ARRAY_FIELDS = (
+    "wavenumber_low", "wavenumber_high", "delta_tau", "single_scat_albedo",
+    "phase_function_moments", "temperature", "surface_albedo", "emissivity_top",
+    "direct_beam_flux", "direct_beam_mu", "isotropic_flux_top", "isotropic_flux_bottom",
+    "temperature_top", "temperature_bottom",
+)
+
+FLUX_OUT_FIELDS = (
+    "flux_direct_beam", "flux_down", "flux_up", "flux_tau_divergence",
+    "mean_intensity", "mean_intensity_down", "mean_intensity_up", "mean_intensity_direct_beam",
+)
+
+
+class FluxBatch(ctypes.Structure):
+    _fields_ = [
+        ("n_inst", c_int32), ("num_streams", c_int32), ("num_layers", c_int32),
+        ("num_phase_func_moments", c_int32), ("pmom_count", c_int32), ("flags", c_uint32),
+    ] + [(f, DArray) for f in FLUX_ARRAY_FIELDS]
+
+
+class FluxOut(ctypes.Structure):
+    _fields_ = [(f, POINTER(c_double)) for f in FLUX_OUT_FIELDS] + [("status", POINTER(c_int32))]
+
+
+def _ptr(a) -> int:
+    if a is None:
+        return 0
+    if isinstance(a, np.ndarray):
+        return a.ctypes.data
+    return int(a.data_ptr())  # torch tensor
+
+
+def _darray(a, per_inst_ndim: int, n_inst: int, keep: list) -> DArray:
+    """Stride 0 if `a` has one instance's shape, else the per-instance element count."""
+    if a is None:
+        return DArray(0, 0)
+    if isinstance(a, (int, float)):
+        a = np.array([float(a)], dtype=np.float64)
+    if isinstance(a, np.ndarray):
+        a = np.ascontiguousarray(a, dtype=np.float64)
+    keep.append(a)
+    ndim = a.ndim if isinstance(a, np.ndarray) else a.dim()
+    if ndim == per_inst_ndim + 1 and a.shape[0] == n_inst and per_inst_ndim >= 0:
+        per = 1
+        for s in a.shape[1:]:
+            per *= int(s)
+        return DArray(_ptr(a), per)
+    return DArray(_ptr(a), 0)
+
+
+def make_flux_batch(n_inst: int, num_streams: int, num_layers: int, num_phase_func_moments: int,
+                    pmom_count: int, flags: int, arrays: dict) -> tuple[FluxBatch, list]:
+    """Pack arrays into a dsp_flux_batch.  Returns (batch, keepalive list)."""
+    keep: list = []
+    per_ndim = {  # dimensions of one instance's value
+        "delta_tau": 1, "single_scat_albedo": 1, "phase_function_moments": 2, "temperature": 1,
+    }
+    b = FluxBatch()
+    b.n_inst = n_inst
+    b.num_streams = num_streams
+    b.num_layers = num_layers
+    b.num_phase_func_moments = num_phase_func_moments
+    b.pmom_count = pmom_count
+    b.flags = flags
+    for f in FLUX_ARRAY_FIELDS:
+        a = arrays.get(f)
+        nd = per_ndim.get(f, 0)
+        if nd == 0 and a is not None and not isinstance(a, (int, float)):
+            # scalar field: shape () or (1,) shared, (n_inst,) per instance
+            if isinstance(a, np.ndarray):
+                a = np.ascontiguousarray(a, dtype=np.float64).reshape(-1)
+                if a.shape[0] == n_inst and n_inst > 1:
+                    keep.append(a)
+                    setattr(b, f, DArray(_ptr(a), 1))
+                    continue
+                a = a[:1].copy()
+            else:  # torch
+                a = a.reshape(-1)
+                if a.shape[0] == n_inst and n_inst > 1:
+                    keep.append(a)
+                    setattr(b, f, DArray(_ptr(a), 1))
+                    continue
+        setattr(b, f, _darray(a, nd, n_inst, keep))
+    return b, keep
+
+
+def make_flux_out(arrays: dict, status=None) -> tuple[FluxOut, list]:
+    o = FluxOut()
+    keep = []
+    for f in FLUX_OUT_FIELDS:
+        a = arrays[f]
+        keep.append(a)
+        setattr(o, f, ctypes.cast(c_void_p(_ptr(a)), POINTER(c_double)))
+    o.status = ctypes.cast(c_void_p(_ptr(status)), POINTER(c_int32)) if status is not None else None
+    keep.append(status)
+    return o, keep
+
+
+def alloc_flux_out_numpy(n_inst: int, num_layers: int) -> tuple[dict, np.ndarray]:
+    outs = {f: np.full((n_inst, num_layers + 1), np.nan) for f in FLUX_OUT_FIELDS}
+    status = np.full(n_inst, -1, dtype=np.int32)
+    return outs, status
+
+
+# ---------------------------------------------------------------------------
+# libdsp.so (the product library)
+# ---------------------------------------------------------------------------
+_LIB = None
+
+
+def lib_path() -> str:
+    return os.path.join(os.path.dirname(os.path.abspath(__file__)), "lib", "libdsp.so")
+
+
+def load_library(path: str | None = None):
+    """Load libdsp.so and declare its prototypes.  Raises OSError if it is missing."""
+    global _LIB
+    if _LIB is not None and path is None:
+        return _LIB
+    p = path or lib_path()
+    if not os.path.exists(p):
+        raise OSError(f"libdsp.so not built: {p} (run __graft_entry__.build())")
+    lib = ctypes.CDLL(p)
+    lib.dsp_api_version.restype = c_int32
+    lib.dsp_status_string.restype = ctypes.c_char_p
+    lib.dsp_status_string.argtypes = [c_int32]
+    lib.dsp_context_create.restype = c_int32
+    lib.dsp_context_create.argtypes = [c_int32, c_void_p, POINTER(c_void_p)]
+    lib.dsp_context_destroy.restype = c_int32
+    lib.dsp_context_destroy.argtypes = [c_void_p]
+    lib.dsp_context_set_stream.restype = c_int32
+    lib.dsp_context_set_stream.argtypes = [c_void_p, c_void_p]
+    lib.dsp_context_last_error.restype = ctypes.c_char_p
+    lib.dsp_context_last_error.argtypes = [c_void_p]
+    lib.dsp_flux_workspace_bytes.restype = c_int64
+    lib.dsp_flux_workspace_bytes.argtypes = [POINTER(FluxBatch)]
+    lib.dsp_flux_bands_solve.restype = c_int32
+    lib.dsp_flux_bands_solve.argtypes = [c_void_p, POINTER(FluxBatch), POINTER(FluxOut)]
+    if path is None:
+        _LIB = lib
+    return lib
+
+
+class Context:
+    """RAII wrapper of a dsp_context."""
+
+    def __init__(self, device: int = 0, stream: int = 0, lib=None):
+        self.lib = lib or load_library()
+        h = c_void_p()
+        st = self.lib.dsp_context_create(device, c_void_p(stream), ctypes.byref(h))
+        if st != DSP_OK:
+            raise RuntimeError(f"dsp_context_create failed: {STATUS_NAMES.get(st, st)}")
+        self.h = h
+
+    def set_stream(self, stream: int):
+        self.lib.dsp_context_set_stream(self.h, c_void_p(stream))
+
+    def last_error(self) -> str:
+        s = self.lib.dsp_context_last_error(self.h)
+        return s.decode() if s else ""
+
+    def flux_bands_solve(self, batch: FluxBatch, out: FluxOut) -> int:
+        return self.lib.dsp_flux_bands_solve(self.h, ctypes.byref(batch), ctypes.byref(out))
+
+    def close(self):
+        if getattr(self, "h", None):
+            self.lib.dsp_context_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

@@ -1,0 +1,137 @@
+/*
+ * dsp.h — C ABI of the B200 DISORT spectral engine (libdsp.so).
+ *
+ * One call solves a whole spectral loop: many independent (column, band)
+ * instances of the DISORT boundary-value problem, in FP64, on one GPU.
+ *
+ * The entry points replace these reference interfaces (DisORT++):
+ *   dsp_flux_bands_solve     <- solveFluxSpectralBandsImpl<N> / DisortFluxSolver<N>::solve
+ *                               (src/python_bindings.cpp:170-211, src/FluxSolver.hpp:49)
+ *   dsp_flux_spectral_solve  <- solveFluxSpectralImpl<N> (src/python_bindings.cpp:148-168);
+ *                               same batch with wavenumber_low == wavenumber_high
+ *   dsp_general_bands_solve  <- solveSpectralBands / DisortSolver::solve
+ *                               (src/python_bindings.cpp:108-127, src/DisortSolver.hpp:87)
+ *
+ * Conventions
+ *  - Plain pointers and sizes only; no exceptions cross this boundary.
+ *  - Every array is given as (pointer, instance stride in elements).  A stride of 0
+ *    means "shared by all instances", which is how the reference's base config plus
+ *    optional per-band override lists (SpectralOverrides, python_bindings.cpp:51-82)
+ *    map onto one batch.
+ *  - Buffers are caller owned.  With DSP_FLAG_DEVICE_POINTERS every pointer in the
+ *    batch and the output is device memory and the call is stream ordered (no host
+ *    synchronisation).  Without it every pointer is host memory; the context stages
+ *    the copies through its own device buffers and the call returns after the results
+ *    are back in host memory.
+ *  - Output arrays are instance-major: out[i * (num_layers + 1) + level], level 0 =
+ *    top of atmosphere (or bottom with DSP_FLAG_INDEX_FROM_BOTTOM, as the reference).
+ *  - Per-instance status codes (dsp_status) go to out->status when it is non-NULL.
+ *    The reference throws std::invalid_argument for what is DSP_ERR_INVALID_INPUT
+ *    here; an invalid instance gets NaN outputs and its status, the others are solved.
+ *  - A context is used by one host thread at a time.
+ */
+#ifndef DSP_H
+#define DSP_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define DSP_API_VERSION 1
+
+typedef enum dsp_status {
+  DSP_OK = 0,
+  DSP_ERR_INVALID_INPUT = 1, /* a validate() rule failed (DisortFluxConfig.cpp:43-143) */
+  DSP_ERR_SINGULAR = 2,      /* zero pivot in a linear solve (BandSolver.hpp:76-78 skips it) */
+  DSP_ERR_NONFINITE = 3,     /* a non-finite output value */
+  DSP_ERR_TIMEOUT = 4,       /* a bounded device wait gave up */
+  DSP_ERR_CUDA = 5,          /* a CUDA runtime error; see dsp_context_last_error */
+  DSP_ERR_UNSUPPORTED = 6,   /* option outside the engine (e.g. spherical beam) */
+  DSP_ERR_NO_MEMORY = 7,     /* device or pinned allocation failed */
+  DSP_ERR_EIGEN = 8,         /* neither symmetric factorisation of the layer eigenproblem exists */
+  DSP_ERR_NOT_INITIALIZED = 9
+} dsp_status;
+
+/* batch flags */
+#define DSP_FLAG_THERMAL            (1u << 0) /* use_thermal_emission */
+#define DSP_FLAG_DELTA_M_PLUS       (1u << 1) /* use_delta_m_plus */
+#define DSP_FLAG_DIFFUSION_LOWER_BC (1u << 2) /* use_diffusion_lower_bc */
+#define DSP_FLAG_INDEX_FROM_BOTTOM  (1u << 3) /* index_from_bottom (layer/level arrays reversed) */
+#define DSP_FLAG_DEVICE_POINTERS    (1u << 4) /* every pointer is device memory */
+#define DSP_FLAG_SPHERICAL_BEAM     (1u << 5) /* use_spherical_beam: rejected, DSP_ERR_UNSUPPORTED */
+#define DSP_FLAG_TEMPERATURE_JAC    (1u << 6) /* compute_temperature_jacobian: rejected, DSP_ERR_UNSUPPORTED */
+
+/* A strided double array: element (instance i, index k) = ptr[i * stride + k]. */
+typedef struct dsp_darray {
+  const double* ptr;
+  int64_t stride; /* 0: one copy shared by all instances */
+} dsp_darray;
+
+/*
+ * Flux-only batch (DisortFluxConfig fields, DisortFluxConfig.hpp:15-93).
+ * All instances share num_streams and num_layers, like one reference spectral loop.
+ */
+typedef struct dsp_flux_batch {
+  int32_t n_inst;
+  int32_t num_streams;            /* N: 4, 6, 8, 10, 12, 14, 16, 32 or 64 */
+  int32_t num_layers;             /* L >= 1 */
+  int32_t num_phase_func_moments; /* the config's num_phase_func_moments */
+  int32_t pmom_count;             /* doubles per layer in phase_function_moments (>= nmomNstr()+1) */
+  uint32_t flags;
+
+  dsp_darray wavenumber_low;          /* [1] per instance */
+  dsp_darray wavenumber_high;         /* [1] */
+  dsp_darray delta_tau;               /* [L] */
+  dsp_darray single_scat_albedo;      /* [L] */
+  dsp_darray phase_function_moments;  /* [L][pmom_count] */
+  dsp_darray temperature;             /* [L+1] (thermal only; may be NULL otherwise) */
+  dsp_darray surface_albedo;          /* [1] */
+  dsp_darray emissivity_top;          /* [1] */
+  dsp_darray direct_beam_flux;        /* [1] */
+  dsp_darray direct_beam_mu;          /* [1] */
+  dsp_darray isotropic_flux_top;      /* [1] */
+  dsp_darray isotropic_flux_bottom;   /* [1] */
+  dsp_darray temperature_top;         /* [1] */
+  dsp_darray temperature_bottom;      /* [1] */
+} dsp_flux_batch;
+
+/* FluxResult (FluxResult.hpp:14-22): each array is [n_inst][L+1]. */
+typedef struct dsp_flux_out {
+  double* flux_direct_beam;
+  double* flux_down;
+  double* flux_up;
+  double* flux_tau_divergence;
+  double* mean_intensity;
+  double* mean_intensity_down;
+  double* mean_intensity_up;
+  double* mean_intensity_direct_beam;
+  int32_t* status; /* [n_inst] or NULL */
+} dsp_flux_out;
+
+typedef struct dsp_context_s* dsp_context;
+
+/* Library / context management. `stream` is a cudaStream_t (NULL = legacy default). */
+int32_t dsp_api_version(void);
+const char* dsp_status_string(dsp_status s);
+dsp_status dsp_context_create(int32_t device, void* stream, dsp_context* out);
+dsp_status dsp_context_destroy(dsp_context ctx);
+dsp_status dsp_context_set_stream(dsp_context ctx, void* stream);
+const char* dsp_context_last_error(dsp_context ctx);
+
+/*
+ * Device bytes a DSP_FLAG_DEVICE_POINTERS flux solve of this batch needs as
+ * workspace (the context allocates and caches it on first use).
+ */
+int64_t dsp_flux_workspace_bytes(const dsp_flux_batch* batch);
+
+/* Flux-only spectral-band solve (DisortFluxSolver<N> over every instance). */
+dsp_status dsp_flux_bands_solve(dsp_context ctx, const dsp_flux_batch* batch,
+                                const dsp_flux_out* out);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* DSP_H */

@@ -1,0 +1,359 @@
+// oracle_common.hpp — CPU restatement of DisORT++ numerics used by the oracle.
+//
+// TEST INFRASTRUCTURE ONLY.  This directory is the correctness oracle for the
+// B200 engine: only tests/, __graft_entry__.smoke() and bench.py's CPU-baseline
+// leg may load it.  The product (disort_b200, libdsp.so) never links or calls it.
+//
+// The reference (DisORT++) is C++17 on top of Eigen 3.4, which is not present
+// here, so the reference cannot be compiled; this is a restatement of its
+// algorithms in plain C++, with the dense linear algebra written from textbook
+// algorithms (Golub & Van Loan).  Each routine cites the reference lines it
+// follows.
+#pragma once
+
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <limits>
+#include <stdexcept>
+
+namespace oracle {
+
+// ---------------------------------------------------------------------------
+// Planck band integral (Planck.cpp:35-169, constants Planck.hpp:10-22)
+// ---------------------------------------------------------------------------
+namespace planck_const {
+constexpr double C2 = 1.438786;
+constexpr double SIGMA = 5.67032E-8;
+constexpr double VCUT = 1.5;
+constexpr double A1 = 1.0 / 3.0;
+constexpr double A2 = -1.0 / 8.0;
+constexpr double A3 = 1.0 / 60.0;
+constexpr double A4 = -1.0 / 5040.0;
+constexpr double A5 = 1.0 / 272160.0;
+constexpr double A6 = -1.0 / 13305600.0;
+}  // namespace planck_const
+
+struct PlanckData {
+  double vmax, sigdpi, conc, c1;
+  PlanckData() {
+    vmax = std::log(std::numeric_limits<double>::max());
+    sigdpi = planck_const::SIGMA / M_PI;
+    conc = 15.0 / std::pow(M_PI, 4.0);
+    c1 = 1.1911e-8;
+  }
+};
+inline const PlanckData& planck_data() {
+  static const PlanckData d;
+  return d;
+}
+
+inline double planck_kernel(double v) { return v * v * v / (std::exp(v) - 1.0); }
+
+// planckFunction (Planck.cpp:35-144).  Returns NaN where the reference throws.
+inline double planck_function(double wnumlo, double wnumhi, double temp) {
+  using namespace planck_const;
+  const PlanckData& pd = planck_data();
+  if (temp < 0.0 || wnumhi <= wnumlo || wnumlo < 0.0) return std::nan("");
+  if (temp < 1.e-4) return 0.0;
+  double v[2] = {C2 * wnumlo / temp, C2 * wnumhi / temp};
+  // Simpson's rule for close wavenumbers (Planck.cpp:53-85)
+  if (v[0] > std::numeric_limits<double>::epsilon() && v[1] < pd.vmax &&
+      (wnumhi - wnumlo) / wnumhi < 1.e-2) {
+    const double hh = v[1] - v[0];
+    double oldval = 0.0;
+    const double val0 = planck_kernel(v[0]) + planck_kernel(v[1]);
+    for (int n = 1; n <= 10; ++n) {
+      const double del = hh / (2.0 * n);
+      double val = val0;
+      for (int k = 1; k <= 2 * n - 1; ++k) val += 2.0 * (1 + k % 2) * planck_kernel(v[0] + k * del);
+      val *= del * A1;
+      if (std::abs((val - oldval) / val) <= 1.e-6)
+        return pd.sigdpi * std::pow(temp, 4.0) * pd.conc * val;
+      oldval = val;
+    }
+    return pd.sigdpi * std::pow(temp, 4.0) * pd.conc * oldval;
+  }
+  // Power / exponential series (Planck.cpp:87-143)
+  double p[2] = {0.0, 0.0}, d[2] = {0.0, 0.0};
+  int smallv = 0;
+  constexpr double vcp[7] = {10.25, 5.7, 3.9, 2.9, 2.3, 1.9, 0.0};
+  for (int i = 0; i < 2; ++i) {
+    if (v[i] < VCUT) {
+      smallv++;
+      const double vsq = v[i] * v[i];
+      p[i] = pd.conc * vsq * v[i] * (A1 + v[i] * (A2 + v[i] * (A3 + vsq * (A4 + vsq * (A5 + vsq * A6)))));
+    } else {
+      int mmax = 1;
+      while (v[i] < vcp[mmax - 1]) mmax++;
+      const double ex = std::exp(-v[i]);
+      double exm = 1.0;
+      d[i] = 0.0;
+      for (int m = 1; m <= mmax; ++m) {
+        const double mv = m * v[i];
+        exm *= ex;
+        d[i] += exm * (6.0 + mv * (6.0 + mv * (3.0 + mv))) / (m * m * m * m);
+      }
+      d[i] *= pd.conc;
+    }
+  }
+  double ans;
+  if (smallv == 2) ans = p[1] - p[0];
+  else if (smallv == 1) ans = 1.0 - p[0] - d[1];
+  else ans = d[0] - d[1];
+  ans *= pd.sigdpi * std::pow(temp, 4.0);
+  if (ans == 0.0) return 0.0;
+  return ans;
+}
+
+// planckFunction2 (Planck.cpp:146-169): single-wavenumber form when lo == hi.
+inline double planck_function2(double wnumlo, double wnumhi, double temp) {
+  if (temp < 0.0 || wnumhi < wnumlo || wnumlo < 0.0) return std::nan("");
+  if (temp < 1.e-4) return 0.0;
+  if (wnumhi == wnumlo) {
+    const double wvn = wnumhi;
+    const double arg = std::exp(-planck_const::C2 * wvn / temp);
+    return planck_data().c1 * wvn * wvn * wvn * arg / (1.0 - arg);
+  }
+  return planck_function(wnumlo, wnumhi, temp);
+}
+
+// ---------------------------------------------------------------------------
+// Gauss-Legendre quadrature on (0,1), mirrored (FluxSolver.cpp:257-290)
+// mu[0..n-1] > 0, mu[n..2n-1] = -mu[0..n-1]; w likewise.
+// ---------------------------------------------------------------------------
+inline bool gauss_quadrature(int n, double* mu, double* w) {
+  const double eps = 3.0e-14;
+  const int max_iter = 10;
+  for (int i = 1; i <= n; ++i) {
+    double z = std::cos(M_PI * (i - 0.25) / (n + 0.5));
+    double z1, pp;
+    int iter = 0;
+    do {
+      double p1 = 1.0, p2 = 0.0;
+      for (int j = 1; j <= n; ++j) {
+        const double p3 = p2;
+        p2 = p1;
+        p1 = ((2.0 * j - 1.0) * z * p2 - (j - 1.0) * p3) / j;
+      }
+      pp = n * (z * p1 - p2) / (z * z - 1.0);
+      z1 = z;
+      z = z1 - p1 / pp;
+      if (++iter > max_iter) return false;
+    } while (std::abs(z - z1) > eps);
+    mu[i - 1] = 0.5 * (1.0 + z);
+    w[i - 1] = 1.0 / ((1.0 - z * z) * pp * pp);
+  }
+  for (int i = 0; i < n; ++i) {
+    mu[n + i] = -mu[i];
+    w[n + i] = w[i];
+  }
+  return true;
+}
+
+// ---------------------------------------------------------------------------
+// Normalised associated Legendre polynomials (Legendre.cpp:67-120)
+// ylm[l * ld + i] = P_l^m(mu[i]).  For m > 0 the seed reads row m-1, which must
+// hold the values left by the call for mode m-1 (Legendre.cpp:90-103).
+// ---------------------------------------------------------------------------
+inline void legendre_flat(int nmu, int m, int ld, int twonm1, const double* mu, double* ylm) {
+  if (m == 0) {
+    for (int i = 0; i < nmu; ++i) {
+      ylm[0 * ld + i] = 1.0;
+      if (twonm1 >= 1) ylm[1 * ld + i] = mu[i];
+    }
+    for (int l = 2; l <= twonm1; ++l)
+      for (int i = 0; i < nmu; ++i)
+        ylm[l * ld + i] = ((2.0 * l - 1.0) * mu[i] * ylm[(l - 1) * ld + i] - (l - 1.0) * ylm[(l - 2) * ld + i]) / l;
+  } else {
+    for (int i = 0; i < nmu; ++i) {
+      ylm[m * ld + i] = -std::sqrt((1.0 - 1.0 / (2.0 * m)) * (1.0 - mu[i] * mu[i])) * ylm[(m - 1) * ld + i];
+      if (m + 1 <= twonm1) ylm[(m + 1) * ld + i] = std::sqrt(2.0 * m + 1.0) * mu[i] * ylm[m * ld + i];
+    }
+    for (int l = m + 2; l <= twonm1; ++l) {
+      const double tmp1 = std::sqrt(static_cast<double>((l - m) * (l + m)));
+      const double tmp2 = std::sqrt(static_cast<double>((l - m - 1) * (l + m - 1)));
+      for (int i = 0; i < nmu; ++i)
+        ylm[l * ld + i] = ((2.0 * l - 1.0) * mu[i] * ylm[(l - 1) * ld + i] - tmp2 * ylm[(l - 2) * ld + i]) / tmp1;
+    }
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Dense linear algebra, row-major n x n with leading dimension ld.
+// ---------------------------------------------------------------------------
+
+// LU with partial (row) pivoting, in place: the stand-in for Eigen::PartialPivLU
+// used at FluxSolver.cpp:634 and :758.  Returns false on an exactly zero pivot.
+inline bool lu_factor(double* a, int n, int ld, int* piv) {
+  bool ok = true;
+  for (int k = 0; k < n; ++k) {
+    int p = k;
+    double amax = std::abs(a[k * ld + k]);
+    for (int i = k + 1; i < n; ++i) {
+      const double v = std::abs(a[i * ld + k]);
+      if (v > amax) { amax = v; p = i; }
+    }
+    piv[k] = p;
+    if (p != k)
+      for (int j = 0; j < n; ++j) std::swap(a[k * ld + j], a[p * ld + j]);
+    const double akk = a[k * ld + k];
+    if (akk == 0.0) { ok = false; continue; }
+    for (int i = k + 1; i < n; ++i) {
+      const double lik = a[i * ld + k] / akk;
+      a[i * ld + k] = lik;
+      for (int j = k + 1; j < n; ++j) a[i * ld + j] -= lik * a[k * ld + j];
+    }
+  }
+  return ok;
+}
+
+inline void lu_solve(const double* a, int n, int ld, const int* piv, double* b) {
+  for (int k = 0; k < n; ++k)
+    if (piv[k] != k) std::swap(b[k], b[piv[k]]);
+  for (int i = 1; i < n; ++i) {
+    double s = b[i];
+    for (int j = 0; j < i; ++j) s -= a[i * ld + j] * b[j];
+    b[i] = s;
+  }
+  for (int i = n - 1; i >= 0; --i) {
+    double s = b[i];
+    for (int j = i + 1; j < n; ++j) s -= a[i * ld + j] * b[j];
+    b[i] = s / a[i * ld + i];
+  }
+}
+
+// Cholesky A = L L^T from the lower triangle (Eigen::LLT semantics used at
+// FluxSolver.cpp:523-524): fails on a non-positive pivot.  L is written to l
+// (full n x n, zeros above the diagonal).
+inline bool cholesky_lower(const double* a, int n, int ld, double* l) {
+  for (int i = 0; i < n * ld; ++i) l[i] = 0.0;
+  for (int j = 0; j < n; ++j) {
+    double d = a[j * ld + j];
+    for (int k = 0; k < j; ++k) d -= l[j * ld + k] * l[j * ld + k];
+    if (!(d > 0.0)) return false;
+    const double ljj = std::sqrt(d);
+    l[j * ld + j] = ljj;
+    for (int i = j + 1; i < n; ++i) {
+      double s = a[i * ld + j];
+      for (int k = 0; k < j; ++k) s -= l[i * ld + k] * l[j * ld + k];
+      l[i * ld + j] = s / ljj;
+    }
+  }
+  return true;
+}
+
+// Symmetric eigensolver (stand-in for Eigen::SelfAdjointEigenSolver,
+// FluxSolver.cpp:542): Householder tridiagonalisation followed by implicit
+// symmetric QR steps with Wilkinson shifts (Golub & Van Loan, Alg. 8.3.1 and
+// 8.3.3).  Reads the lower triangle of a.  Eigenvalues ascending in evals,
+// eigenvectors as columns of z (row-major, ld).  Work arrays are local.
+inline void sym_eigen(const double* a_in, int n, int ld, double* evals, double* z) {
+  constexpr int NMAX = 64;
+  double a[NMAX * NMAX];
+  double d[NMAX], e[NMAX];
+  for (int i = 0; i < n; ++i)
+    for (int j = 0; j < n; ++j) {
+      const int ii = std::max(i, j), jj = std::min(i, j);
+      a[i * n + j] = a_in[ii * ld + jj];
+    }
+  for (int i = 0; i < n; ++i)
+    for (int j = 0; j < n; ++j) z[i * ld + j] = (i == j) ? 1.0 : 0.0;
+  // Householder tridiagonalisation: A <- H A H, Z <- Z H
+  double v[NMAX], p[NMAX], w[NMAX];
+  for (int k = 0; k + 2 < n; ++k) {
+    double xnorm2 = 0.0;
+    for (int i = k + 1; i < n; ++i) xnorm2 += a[i * n + k] * a[i * n + k];
+    const double x0 = a[(k + 1) * n + k];
+    double tail2 = xnorm2 - x0 * x0;
+    if (tail2 == 0.0) continue;
+    const double alpha = (x0 >= 0.0) ? -std::sqrt(xnorm2) : std::sqrt(xnorm2);
+    for (int i = k + 1; i < n; ++i) v[i] = a[i * n + k];
+    v[k + 1] -= alpha;
+    double vnorm2 = 0.0;
+    for (int i = k + 1; i < n; ++i) vnorm2 += v[i] * v[i];
+    const double beta = 2.0 / vnorm2;
+    // p = beta * A_sub v
+    for (int i = k + 1; i < n; ++i) {
+      double s = 0.0;
+      for (int j = k + 1; j < n; ++j) s += a[i * n + j] * v[j];
+      p[i] = beta * s;
+    }
+    double vp = 0.0;
+    for (int i = k + 1; i < n; ++i) vp += v[i] * p[i];
+    const double kk = 0.5 * beta * vp;
+    for (int i = k + 1; i < n; ++i) w[i] = p[i] - kk * v[i];
+    for (int i = k + 1; i < n; ++i)
+      for (int j = k + 1; j < n; ++j) a[i * n + j] -= v[i] * w[j] + w[i] * v[j];
+    a[(k + 1) * n + k] = alpha;
+    a[k * n + k + 1] = alpha;
+    for (int i = k + 2; i < n; ++i) { a[i * n + k] = 0.0; a[k * n + i] = 0.0; }
+    // Z <- Z (I - beta v v^T)
+    for (int i = 0; i < n; ++i) {
+      double s = 0.0;
+      for (int j = k + 1; j < n; ++j) s += z[i * ld + j] * v[j];
+      s *= beta;
+      for (int j = k + 1; j < n; ++j) z[i * ld + j] -= s * v[j];
+    }
+  }
+  for (int i = 0; i < n; ++i) d[i] = a[i * n + i];
+  for (int i = 0; i + 1 < n; ++i) e[i] = a[(i + 1) * n + i];
+  e[n - 1] = 0.0;
+  // implicit symmetric QR with Wilkinson shift on (d, e)
+  const double eps = std::numeric_limits<double>::epsilon();
+  int q = n - 1;
+  int iter = 0;
+  while (q > 0 && iter < 60 * n) {
+    // deflate
+    for (int i = 0; i < q; ++i)
+      if (std::abs(e[i]) <= eps * (std::abs(d[i]) + std::abs(d[i + 1]))) e[i] = 0.0;
+    while (q > 0 && e[q - 1] == 0.0) --q;
+    if (q == 0) break;
+    int p0 = q - 1;
+    while (p0 > 0 && e[p0 - 1] != 0.0) --p0;
+    ++iter;
+    // Wilkinson shift from the trailing 2x2 of block [p0..q]
+    const double dd = 0.5 * (d[q - 1] - d[q]);
+    const double ee = e[q - 1];
+    const double sgn = (dd >= 0.0) ? 1.0 : -1.0;
+    const double mu = d[q] - ee * ee / (dd + sgn * std::hypot(dd, ee));
+    double x = d[p0] - mu;
+    double y = e[p0];
+    for (int k = p0; k < q; ++k) {
+      // Givens rotation zeroing y against x
+      double c, s;
+      if (y == 0.0) { c = 1.0; s = 0.0; }
+      else if (std::abs(y) > std::abs(x)) { const double t = -x / y; s = 1.0 / std::sqrt(1.0 + t * t); c = s * t; }
+      else { const double t = -y / x; c = 1.0 / std::sqrt(1.0 + t * t); s = c * t; }
+      if (k > p0) e[k - 1] = c * x - s * y;
+      const double dk = d[k], dk1 = d[k + 1], ek = e[k];
+      // T(k:k+1,k:k+1) <- G^T T G, G = [c s; -s c]
+      d[k] = c * c * dk - 2.0 * c * s * ek + s * s * dk1;
+      d[k + 1] = s * s * dk + 2.0 * c * s * ek + c * c * dk1;
+      e[k] = c * s * (dk - dk1) + (c * c - s * s) * ek;
+      if (k + 1 < q) {
+        x = e[k];
+        y = -s * e[k + 1];
+        e[k + 1] *= c;
+      }
+      for (int i = 0; i < n; ++i) {
+        const double zk = z[i * ld + k], zk1 = z[i * ld + k + 1];
+        z[i * ld + k] = c * zk - s * zk1;
+        z[i * ld + k + 1] = s * zk + c * zk1;
+      }
+    }
+  }
+  // sort ascending (Eigen's order); columns of z follow
+  for (int i = 0; i < n; ++i) evals[i] = d[i];
+  for (int i = 0; i < n - 1; ++i) {
+    int kmin = i;
+    for (int j = i + 1; j < n; ++j)
+      if (evals[j] < evals[kmin]) kmin = j;
+    if (kmin != i) {
+      std::swap(evals[i], evals[kmin]);
+      for (int r = 0; r < n; ++r) std::swap(z[r * ld + i], z[r * ld + kmin]);
+    }
+  }
+}
+
+}  // namespace oracle

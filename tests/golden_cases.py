@@ -1,0 +1,50 @@
+"""Helpers that turn tests/golden/reference_goldens.json cases into flux batches."""
+from __future__ import annotations
+
+import json
+import os
+
+import numpy as np
+
+from disort_b200 import capi
+
+GOLDEN = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden", "reference_goldens.json")
+
+
+def load_cases() -> list:
+    with open(GOLDEN) as f:
+        return json.load(f)["cases"]
+
+
+def flux_workload(c: dict) -> dict:
+    L = c["num_layers"]
+    pm = np.array(c["phase_function_moments"], dtype=np.float64)
+    flags = 0
+    if c["use_thermal_emission"]:
+        flags |= capi.FLAG_THERMAL
+    if c["use_delta_m_plus"]:
+        flags |= capi.FLAG_DELTA_M_PLUS
+    arrays = dict(
+        wavenumber_low=c["wavenumber_low"], wavenumber_high=c["wavenumber_high"],
+        delta_tau=np.array(c["delta_tau"], dtype=np.float64),
+        single_scat_albedo=np.array(c["single_scat_albedo"], dtype=np.float64),
+        phase_function_moments=pm,
+        temperature=np.array(c["temperature"], dtype=np.float64) if c["use_thermal_emission"] else None,
+        surface_albedo=c["surface_albedo"], emissivity_top=c["emissivity_top"],
+        direct_beam_flux=c["direct_beam_flux"], direct_beam_mu=c["direct_beam_mu"],
+        isotropic_flux_top=c["isotropic_flux_top"], isotropic_flux_bottom=0.0,
+        temperature_top=c["temperature_top"], temperature_bottom=c["temperature_bottom"],
+    )
+    return dict(name=c["name"], n_inst=1, num_streams=c["num_streams"], num_layers=L,
+                num_phase_func_moments=c["num_phase_func_moments"], pmom_count=pm.shape[1],
+                flags=flags, arrays=arrays)
+
+
+def level_of(c: dict, index: int):
+    """Output level of expectation `index` (a user-tau index when tau_user is set)."""
+    if c["tau_user"] is None:
+        return index
+    tau = c["tau_user"][index]
+    cum = np.concatenate([[0.0], np.cumsum(c["delta_tau"])])
+    hit = np.nonzero(np.abs(cum - tau) <= 1e-9 * max(1.0, abs(tau)))[0]
+    return int(hit[0]) if hit.size else None

@@ -1,0 +1,53 @@
+"""Loader of the CPU oracle library (oracle/liboracle_disort.so) for tests.
+
+The oracle is the checker: tests call it on the same dsp_flux_batch that the
+GPU library receives and compare outputs.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+import subprocess
+from ctypes import POINTER, c_double, c_int
+
+import numpy as np
+
+from disort_b200 import capi
+
+REPO = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+ORACLE_DIR = os.path.join(REPO, "oracle")
+_LIB = None
+
+
+def load(native: bool = False):
+    """Load (building if needed) the oracle shared library."""
+    global _LIB
+    if _LIB is not None and not native:
+        return _LIB
+    target = "native" if native else "all"
+    path = os.path.join(ORACLE_DIR, "_native" if native else "", "liboracle_disort.so")
+    subprocess.run(["make", "-s", "-C", ORACLE_DIR, target], check=True)
+    lib = ctypes.CDLL(path)
+    lib.oracle_flux_bands_solve.restype = c_int
+    lib.oracle_flux_bands_solve.argtypes = [POINTER(capi.FluxBatch), POINTER(capi.FluxOut), c_int]
+    lib.oracle_quadrature.restype = c_int
+    lib.oracle_quadrature.argtypes = [c_int, POINTER(c_double), POINTER(c_double), POINTER(c_double)]
+    lib.oracle_planck.restype = c_double
+    lib.oracle_planck.argtypes = [c_double, c_double, c_double]
+    if hasattr(lib, "oracle_general_bands_solve"):
+        pass
+    if not native:
+        _LIB = lib
+    return lib
+
+
+def flux_solve(w: dict, nthreads: int = 0, extra_flags: int = 0):
+    """Run the oracle on workload dict `w`; returns (outputs dict, status array)."""
+    lib = load()
+    batch, keep = capi.make_flux_batch(w["n_inst"], w["num_streams"], w["num_layers"],
+                                       w["num_phase_func_moments"], w["pmom_count"],
+                                       w["flags"] | extra_flags, w["arrays"])
+    outs, status = capi.alloc_flux_out_numpy(w["n_inst"], w["num_layers"])
+    o, keep2 = capi.make_flux_out(outs, status)
+    lib.oracle_flux_bands_solve(ctypes.byref(batch), ctypes.byref(o), nthreads)
+    return outs, status

@@ -1,0 +1,53 @@
+"""The CPU oracle against the reference's own known-answer tests.
+
+Every expected value and tolerance comes from DisORT++ tests/test_solver.cpp
+(extracted into tests/golden/reference_goldens.json by
+tests/golden/make_reference_goldens.py).  Fluxes are compared at the output
+levels that coincide with layer boundaries (the flux solver's output grid).
+The Delta-M+ regression cases carry 13 significant digits, so the oracle is
+additionally held to 1e-9 relative there.
+"""
+import numpy as np
+import pytest
+
+import golden_cases
+import oracle_lib
+
+CASES = golden_cases.load_cases()
+
+
+@pytest.mark.parametrize("case", CASES, ids=[c["name"] for c in CASES])
+def test_oracle_flux_goldens(case):
+    w = golden_cases.flux_workload(case)
+    out, status = oracle_lib.flux_solve(w)
+    assert status[0] == 0
+    checked = 0
+    for e in case["expect_flux"]:
+        lev = golden_cases.level_of(case, e["index"])
+        if lev is None:
+            continue
+        got = out[e["field"]][0, lev]
+        assert abs(got - e["value"]) <= e["tol"], (e, got)
+        if case["name"].startswith("DeltaMPlus.") and e["value"] != 0.0:
+            assert abs(got - e["value"]) <= 1e-9 * abs(e["value"]), (e, got)
+        checked += 1
+    assert checked > 0
+
+
+def test_quadrature_and_planck_sanity():
+    import ctypes
+    lib = oracle_lib.load()
+    for n in (4, 16, 64):
+        mu = np.zeros(n); w = np.zeros(n); y = np.zeros((n + 1) * n)
+        assert lib.oracle_quadrature(n, mu.ctypes.data_as(ctypes.POINTER(ctypes.c_double)),
+                                     w.ctypes.data_as(ctypes.POINTER(ctypes.c_double)),
+                                     y.ctypes.data_as(ctypes.POINTER(ctypes.c_double))) == 0
+        assert abs(w[: n // 2].sum() - 1.0) < 1e-13
+        assert np.all(mu[: n // 2] > 0) and np.allclose(mu[n // 2:], -mu[: n // 2])
+    # Stefan-Boltzmann limit of the band integral over (0, 50000) cm^-1 at 300 K
+    sigma = 5.67032e-8
+    b = lib.oracle_planck(0.0, 50000.0, 300.0)
+    assert abs(b - sigma * 300.0 ** 4 / np.pi) / b < 1e-5
+    # single-wavenumber branch and zero-temperature branch
+    assert lib.oracle_planck(1000.0, 1000.0, 300.0) > 0
+    assert lib.oracle_planck(100.0, 200.0, 0.0) == 0.0
