@@ -1,0 +1,372 @@
+"""Benchmark of the B200 DISORT flux path: solves/s on the 60-layer, 16-stream,
+20,000-band thermal sweep (one spectral loop per step).
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+                    [--workload thermal|beam]
+
+Prints one JSON line (rank 0).  A step is one dsp_flux_bands_solve over the whole
+sweep with inputs resident in HBM (`value`); `e2e` repeats the step through the
+same C ABI with pinned host buffers, host<->device copies inside the timed region.
+`--impl reference` times the CPU restatement of the reference solver (oracle/,
+OpenMP over all host threads, the reference loop's structure) on a bounded
+sample of the same sweep.  Multi-GPU runs are replicas: every rank solves its own
+20,000-band sweep (weak scaling), no collective on the data path.
+"""
+from __future__ import annotations
+
+import argparse
+import ctypes
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import threading
+import time
+
+import numpy as np
+
+REPO = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, REPO)
+
+from disort_b200 import capi, flops, workloads  # noqa: E402
+
+METRIC = "solves/s (60 lyr,16 str): plain GPU vs gated surrogate at ≤0.5% flux err"
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--workload", choices=["thermal", "beam"], default="thermal")
+    ap.add_argument("--cpu-seconds", type=float, default=10.0, help="target CPU-baseline sample time")
+    return ap.parse_args()
+
+
+def make_workload(kind: str, rank: int):
+    if kind == "beam":
+        return workloads.beam_sweep()
+    w = workloads.thermal_sweep(seed=2 + rank)
+    if rank:
+        off = 0.14 * 20000 * rank
+        w["arrays"]["wavenumber_low"] = w["arrays"]["wavenumber_low"] + off
+        w["arrays"]["wavenumber_high"] = w["arrays"]["wavenumber_high"] + off
+    return w
+
+
+def config_of(w, args, world):
+    return {
+        "workload": w["name"], "bands_per_gpu": w["n_inst"], "num_layers": w["num_layers"],
+        "num_streams": w["num_streams"], "thermal": bool(w["flags"] & capi.FLAG_THERMAL),
+        "parallelism": f"replicas x{world}" if world > 1 else "single GPU",
+        "l2": "inputs (pmom 163 MB) and workspace (5.7 GB) larger than L2; no flush needed",
+    }
+
+
+# ---------------------------------------------------------------------------
+# CPU baseline (oracle restatement of the reference solver, OpenMP)
+# ---------------------------------------------------------------------------
+def cpu_oracle():
+    sys.path.insert(0, os.path.join(REPO, "tests"))
+    subprocess.run(["make", "-s", "-C", os.path.join(REPO, "oracle"), "native"], check=True)
+    lib = ctypes.CDLL(os.path.join(REPO, "oracle", "_native", "liboracle_disort.so"))
+    lib.oracle_flux_bands_solve.restype = ctypes.c_int
+    lib.oracle_flux_bands_solve.argtypes = [ctypes.POINTER(capi.FluxBatch), ctypes.POINTER(capi.FluxOut),
+                                            ctypes.c_int]
+    return lib
+
+
+def cpu_time(lib, w, threads):
+    batch, keep = workloads.make_batch(w)
+    outs, status = capi.alloc_flux_out_numpy(w["n_inst"], w["num_layers"])
+    o, keep2 = capi.make_flux_out(outs, status)
+    t0 = time.perf_counter()
+    lib.oracle_flux_bands_solve(ctypes.byref(batch), ctypes.byref(o), threads)
+    return time.perf_counter() - t0
+
+
+def cpu_baseline(w, target_s: float):
+    lib = cpu_oracle()
+    threads = os.cpu_count() or 1
+    probe = workloads.subset(w, np.arange(0, w["n_inst"], max(1, w["n_inst"] // (4 * threads)))[: 4 * threads])
+    cpu_time(lib, probe, threads)  # warm-up
+    t = cpu_time(lib, probe, threads)
+    rate = probe["n_inst"] / t
+    m = int(min(w["n_inst"], max(threads, rate * target_s)))
+    idx = np.linspace(0, w["n_inst"] - 1, m).astype(np.int64)
+    sample = workloads.subset(w, idx)
+    t = cpu_time(lib, sample, threads)
+    return dict(value=m / t, unit="solves/s", cores=threads, kind="port",
+                sample=f"{m} of {w['n_inst']} bands evenly spaced across the sweep, "
+                       f"oracle built -march=native, {threads} OpenMP threads, {t:.1f} s"), lib
+
+
+def run_reference(args):
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return
+    w = make_workload(args.workload, 0)
+    lib = cpu_oracle()
+    threads = os.cpu_count() or 1
+    probe = workloads.subset(w, np.arange(0, w["n_inst"], max(1, w["n_inst"] // (4 * threads)))[: 4 * threads])
+    cpu_time(lib, probe, threads)
+    rate = probe["n_inst"] / cpu_time(lib, probe, threads)
+    per_step = max(1.0, min(20.0, 150.0 / max(1, args.steps + args.warmup)))
+    m = int(min(w["n_inst"], max(threads, rate * per_step)))
+    sample = workloads.subset(w, np.linspace(0, w["n_inst"] - 1, m).astype(np.int64))
+    for _ in range(args.warmup):
+        cpu_time(lib, sample, threads)
+    ts = [cpu_time(lib, sample, threads) for _ in range(args.steps)]
+    value = m * len(ts) / sum(ts)
+    desc = (f"{m} of {w['n_inst']} bands per step (evenly spaced), CPU restatement of "
+            f"DisortFluxSolver<16> (oracle/, -march=native), {threads} OpenMP threads")
+    line = {
+        "impl": "reference", "metric": METRIC, "value": value, "unit": "solves/s", "n_gpus": args.gpus,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1000 * statistics.mean(ts),
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+        "data": "synthetic (seeded)", "config": config_of(w, args, 1),
+        "cpu_baseline": {"value": value, "unit": "solves/s", "cores": threads, "kind": "port", "sample": desc},
+        "e2e": {"value": value, "unit": "solves/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+# ---------------------------------------------------------------------------
+# clocks during the timed region
+# ---------------------------------------------------------------------------
+class ClockSampler:
+    FIELDS = ("clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_id: str):
+        self.gpu_id = gpu_id
+        self.proc = None
+        self.fh = None
+
+    def start(self):
+        self.fh = tempfile.NamedTemporaryFile("w+", suffix=".csv", delete=False)
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--id={self.gpu_id}", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+                 "-lms", "100"], stdout=self.fh, stderr=subprocess.DEVNULL)
+        except OSError:
+            self.proc = None
+
+    def stop(self) -> dict:
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        self.proc.wait()
+        self.fh.flush()
+        self.fh.seek(0)
+        rows = [r.strip().split(", ") for r in self.fh.read().splitlines() if r.strip()]
+        os.unlink(self.fh.name)
+        sm, smax, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for r in rows:
+            try:
+                sm.append(float(r[0]))
+                smax.append(float(r[1]))
+                for k, nm in enumerate(names):
+                    if r[4 + k].strip().lower() == "active":
+                        reasons.add(nm)
+            except (ValueError, IndexError):
+                continue
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(smax) if smax else None,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+# ---------------------------------------------------------------------------
+# our arm
+# ---------------------------------------------------------------------------
+def fp64_peak_tflops() -> float | None:
+    try:
+        lib = ctypes.CDLL(os.path.join(REPO, "disort_b200", "lib", "libdsp_bench.so"))
+        lib.dsp_bench_fp64_tflops.restype = ctypes.c_double
+        lib.dsp_bench_fp64_tflops.argtypes = [ctypes.c_int, ctypes.c_int]
+        import torch
+        v = lib.dsp_bench_fp64_tflops(torch.cuda.current_device(), 5)
+        return v if v > 0 else None
+    except OSError:
+        return None
+
+
+def committed_traffic(workload_name: str):
+    p = os.path.join(REPO, "profiles", "traffic.json")
+    if not os.path.exists(p):
+        return None
+    try:
+        return json.load(open(p)).get(workload_name)
+    except (ValueError, OSError):
+        return None
+
+
+def run_ours(args):
+    import torch
+    import torch.distributed as dist
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    if world > 1:
+        import datetime
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+    dev = torch.device("cuda", local)
+    stream = torch.cuda.current_stream()
+
+    w = make_workload(args.workload, rank)
+    n, L, N = w["n_inst"], w["num_layers"], w["num_streams"]
+    ctx = capi.Context(local, stream.cuda_stream)
+
+    # device-resident inputs/outputs
+    dev_arrays = {}
+    for k, a in w["arrays"].items():
+        if a is None:
+            dev_arrays[k] = None
+        elif isinstance(a, np.ndarray):
+            dev_arrays[k] = torch.from_numpy(np.ascontiguousarray(a)).to(dev)
+        else:
+            dev_arrays[k] = torch.tensor([float(a)], dtype=torch.float64, device=dev)
+    batch, keep = capi.make_flux_batch(n, N, L, w["num_phase_func_moments"], w["pmom_count"],
+                                       w["flags"] | capi.FLAG_DEVICE_POINTERS, dev_arrays)
+    douts = {f: torch.empty((n, L + 1), dtype=torch.float64, device=dev) for f in capi.FLUX_OUT_FIELDS}
+    dstatus = torch.empty((n,), dtype=torch.int32, device=dev)
+    out, keep2 = capi.make_flux_out(douts, dstatus)
+
+    def step():
+        rc = ctx.flux_bands_solve(batch, out)
+        if rc != 0:
+            raise RuntimeError(f"dsp_flux_bands_solve: {capi.STATUS_NAMES.get(rc, rc)}: {ctx.last_error()}")
+
+    for _ in range(args.warmup):
+        step()
+    torch.cuda.synchronize()
+    bad = int((dstatus != 0).sum())
+
+    uuid = None
+    try:
+        uuid = str(torch.cuda.get_device_properties(dev).uuid)
+        if not uuid.startswith("GPU-"):
+            uuid = "GPU-" + uuid
+    except Exception:
+        uuid = str(local)
+    clocks = ClockSampler(uuid)
+
+    # ---- timed region: device-resident inputs --------------------------------
+    ctx.set_timing(True)
+    ctx.timing_reset()
+    if world > 1:
+        dist.barrier()
+    torch.cuda.synchronize()
+    clocks.start()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(args.steps):
+        step()
+    e1.record(stream)
+    torch.cuda.synchronize()
+    if world > 1:
+        dist.barrier()
+    ms = e0.elapsed_time(e1)
+    clk = clocks.stop()
+    ktimes = ctx.timings()
+    ctx.set_timing(False)
+    t = torch.tensor([ms], dtype=torch.float64, device=dev)
+    if world > 1:
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    ms_max = float(t.item())
+    value = n * args.steps * world / (ms_max / 1000.0)
+
+    # ---- e2e: through the C ABI with pinned host buffers ----------------------
+    host_arrays = {}
+    h2d = 0
+    for k, a in w["arrays"].items():
+        if isinstance(a, np.ndarray):
+            ta = torch.from_numpy(np.ascontiguousarray(a)).pin_memory()
+            host_arrays[k] = ta
+            h2d += ta.numel() * 8
+        else:
+            host_arrays[k] = a
+            if a is not None:
+                h2d += 8
+    hbatch, hkeep = capi.make_flux_batch(n, N, L, w["num_phase_func_moments"], w["pmom_count"], w["flags"],
+                                         host_arrays)
+    houts = {f: torch.empty((n, L + 1), dtype=torch.float64).pin_memory() for f in capi.FLUX_OUT_FIELDS}
+    hstatus = torch.empty((n,), dtype=torch.int32).pin_memory()
+    hout, hkeep2 = capi.make_flux_out(houts, hstatus)
+    d2h = 8 * n * (L + 1) * 8 + 4 * n
+
+    def hstep():
+        rc = ctx.flux_bands_solve(hbatch, hout)
+        if rc != 0:
+            raise RuntimeError(f"host-pointer solve: {ctx.last_error()}")
+
+    for _ in range(max(1, args.warmup)):
+        hstep()
+    if world > 1:
+        dist.barrier()
+    torch.cuda.synchronize()
+    e2 = torch.cuda.Event(enable_timing=True)
+    e3 = torch.cuda.Event(enable_timing=True)
+    e2.record(stream)
+    for _ in range(args.steps):
+        hstep()
+    e3.record(stream)
+    torch.cuda.synchronize()
+    te = torch.tensor([e2.elapsed_time(e3)], dtype=torch.float64, device=dev)
+    if world > 1:
+        dist.all_reduce(te, op=dist.ReduceOp.MAX)
+    e2e_value = n * args.steps * world / (float(te.item()) / 1000.0)
+    # host results must equal the device-resident results
+    same = all(torch.equal(houts[f], douts[f].cpu()) for f in capi.FLUX_OUT_FIELDS)
+
+    # ---- roofline of the dominant kernel -----------------------------------
+    beam = bool(np.any(np.asarray(w["arrays"]["direct_beam_flux"]) > 0))
+    thermal = bool(w["flags"] & capi.FLAG_THERMAL)
+    fl = flops.flux_solve_flops(N, L, beam, thermal)
+    dom = max((k for k in ktimes if k in fl), key=lambda k: ktimes[k][0])
+    dom_ms, dom_launches = ktimes[dom]
+    achieved = fl[dom] * n * args.steps / (dom_ms / 1000.0) / 1e12
+    peak = fp64_peak_tflops()
+    roofline = {
+        "bound": "fp64", "kernel": dom, "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
+        "frac": (achieved / peak) if peak else None,
+        "peak_source": "measured on this GPU by disort_b200/csrc/fp64_peak.cu (FP64 FMA chains, burst)",
+        "flops_per_solve": fl[dom], "avg_launch_ms": dom_ms / max(1, dom_launches),
+        "traffic": committed_traffic(w["name"]),
+        "kernel_ms_per_step": {k: v[0] / args.steps for k, v in ktimes.items()},
+    }
+
+    if rank == 0:
+        cpu, _ = cpu_baseline(w, args.cpu_seconds)
+        line = {
+            "metric": METRIC, "value": value, "unit": "solves/s", "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": ms_max / args.steps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded PCG64)",
+            "config": config_of(w, args, world),
+            "e2e": {"value": e2e_value, "unit": "solves/s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
+                    "matches_device_result": same},
+            "gpu_launches": int(sum(v[1] for v in ktimes.values())),
+            "roofline": roofline, "cpu_baseline": cpu, "clocks": clk, "bad_status_instances": bad,
+        }
+        print(json.dumps(line), flush=True)
+    ctx.close()
+    if world > 1:
+        dist.destroy_process_group()
+
+
+def main():
+    args = parse()
+    if args.impl == "reference":
+        run_reference(args)
+    else:
+        run_ours(args)
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,68 @@
+"""Build the native libraries of disort_b200 in-tree.
+
+    python -m disort_b200.build          # libdsp.so (sm_100a) + the Python host module
+
+libdsp.so is compiled with nvcc for sm_100a only (-gencode arch=compute_100a,
+code=sm_100a); the host-side Python module (_disortpp) is compiled with g++
+against pybind11 and links libdsp.so by rpath.
+"""
+from __future__ import annotations
+
+import os
+import subprocess
+import sys
+import sysconfig
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+REPO = os.path.dirname(HERE)
+CSRC = os.path.join(HERE, "csrc")
+LIB = os.path.join(HERE, "lib")
+NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
+ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
+
+
+def _run(cmd: list[str]) -> None:
+    print(" ".join(cmd), flush=True)
+    subprocess.run(cmd, check=True)
+
+
+def _stale(target: str, deps: list[str]) -> bool:
+    if not os.path.exists(target):
+        return True
+    t = os.path.getmtime(target)
+    return any(os.path.getmtime(d) > t for d in deps)
+
+
+def _deps(*exts: str) -> list[str]:
+    out = [os.path.join(REPO, "include", "dsp.h")]
+    for root, _, files in os.walk(CSRC):
+        out += [os.path.join(root, f) for f in files if f.endswith(exts)]
+    return out
+
+
+def build_libdsp(force: bool = False) -> str:
+    os.makedirs(LIB, exist_ok=True)
+    target = os.path.join(LIB, "libdsp.so")
+    if force or _stale(target, _deps(".cu", ".cuh", ".h")):
+        _run([NVCC, *ARCH, "-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC", "-shared",
+              "-diag-suppress", "177",
+              "-o", target, os.path.join(CSRC, "dsp_capi.cu")])
+    return target
+
+
+def build_bench(force: bool = False) -> str:
+    os.makedirs(LIB, exist_ok=True)
+    target = os.path.join(LIB, "libdsp_bench.so")
+    src = os.path.join(CSRC, "fp64_peak.cu")
+    if force or _stale(target, [src]):
+        _run([NVCC, *ARCH, "-O3", "-std=c++17", "-Xcompiler", "-fPIC", "-shared", "-o", target, src])
+    return target
+
+
+def build_all(force: bool = False) -> None:
+    build_libdsp(force)
+    build_bench(force)
+
+
+if __name__ == "__main__":
+    build_all(force="--force" in sys.argv)

@@ -184,6 +184,15 @@ def load_library(path: str | None = None):
     lib.dsp_context_last_error.argtypes = [c_void_p]
     lib.dsp_flux_workspace_bytes.restype = c_int64
     lib.dsp_flux_workspace_bytes.argtypes = [POINTER(FluxBatch)]
+    lib.dsp_context_set_timing.restype = c_int32
+    lib.dsp_context_set_timing.argtypes = [c_void_p, c_int32]
+    lib.dsp_context_timing_reset.restype = c_int32
+    lib.dsp_context_timing_reset.argtypes = [c_void_p]
+    lib.dsp_context_timing_count.restype = c_int32
+    lib.dsp_context_timing_count.argtypes = [c_void_p]
+    lib.dsp_context_timing_get.restype = c_int32
+    lib.dsp_context_timing_get.argtypes = [c_void_p, c_int32, POINTER(ctypes.c_char_p),
+                                           POINTER(c_double), POINTER(c_int64)]
     lib.dsp_flux_bands_solve.restype = c_int32
     lib.dsp_flux_bands_solve.argtypes = [c_void_p, POINTER(FluxBatch), POINTER(FluxOut)]
     if path is None:
@@ -211,6 +220,23 @@ class Context:
 
     def flux_bands_solve(self, batch: FluxBatch, out: FluxOut) -> int:
         return self.lib.dsp_flux_bands_solve(self.h, ctypes.byref(batch), ctypes.byref(out))
+
+    def set_timing(self, enable: bool):
+        self.lib.dsp_context_set_timing(self.h, 1 if enable else 0)
+
+    def timing_reset(self):
+        self.lib.dsp_context_timing_reset(self.h)
+
+    def timings(self) -> dict:
+        """{kernel name: (total ms, launches)} accumulated since the last reset."""
+        out = {}
+        for k in range(self.lib.dsp_context_timing_count(self.h)):
+            name = ctypes.c_char_p()
+            ms = c_double()
+            cnt = c_int64()
+            self.lib.dsp_context_timing_get(self.h, k, ctypes.byref(name), ctypes.byref(ms), ctypes.byref(cnt))
+            out[name.value.decode()] = (ms.value, cnt.value)
+        return out
 
     def close(self):
         if getattr(self, "h", None):

@@ -1,0 +1,555 @@
+// dsp_capi.cu — the C ABI of libdsp.so (include/dsp.h): contexts, staging of
+// host buffers, workspace management, per-stream-count tables and the kernel
+// launches of a flux spectral-band solve.
+#include <cuda_runtime.h>
+
+#include <cfloat>
+#include <cmath>
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <map>
+#include <mutex>
+#include <string>
+#include <vector>
+
+#include "../../include/dsp.h"
+#include "dsp_device.cuh"
+#include "flux_bvp.cuh"
+#include "flux_layer.cuh"
+#include "flux_setup.cuh"
+
+using namespace dsp;
+
+struct dsp_context_s {
+  int device = 0;
+  cudaStream_t stream = nullptr;
+  std::string last_error;
+  int sm_count = 148;
+  // device buffers owned by the context
+  void* ws = nullptr;
+  size_t ws_bytes = 0;
+  void* stage_in = nullptr;
+  size_t stage_in_bytes = 0;
+  void* stage_out = nullptr;
+  size_t stage_out_bytes = 0;
+  std::map<int, double*> tables;
+  // optional per-kernel timing
+  bool timing = false;
+  struct Pending {
+    int kernel;
+    cudaEvent_t a, b;
+  };
+  std::vector<Pending> pending;
+  std::vector<cudaEvent_t> free_events;
+  std::vector<std::string> knames;
+  std::vector<double> kms;
+  std::vector<int64_t> kcount;
+};
+
+namespace {
+cudaEvent_t take_event(dsp_context c) {
+  if (!c->free_events.empty()) {
+    cudaEvent_t e = c->free_events.back();
+    c->free_events.pop_back();
+    return e;
+  }
+  cudaEvent_t e;
+  cudaEventCreate(&e);
+  return e;
+}
+
+int kernel_id(dsp_context c, const char* name) {
+  for (size_t k = 0; k < c->knames.size(); ++k)
+    if (c->knames[k] == name) return (int)k;
+  c->knames.push_back(name);
+  c->kms.push_back(0.0);
+  c->kcount.push_back(0);
+  return (int)c->knames.size() - 1;
+}
+
+// Brackets one launch with events when timing is on.
+struct KernelTimer {
+  dsp_context c;
+  int id = -1;
+  cudaEvent_t a = nullptr, b = nullptr;
+  KernelTimer(dsp_context ctx, const char* name) : c(ctx) {
+    if (!c->timing) return;
+    id = kernel_id(c, name);
+    a = take_event(c);
+    b = take_event(c);
+    cudaEventRecord(a, c->stream);
+  }
+  ~KernelTimer() {
+    if (id < 0) return;
+    cudaEventRecord(b, c->stream);
+    c->pending.push_back({id, a, b});
+  }
+};
+
+void drain_timing(dsp_context c) {
+  for (auto& p : c->pending) {
+    float ms = 0.f;
+    cudaEventSynchronize(p.b);
+    cudaEventElapsedTime(&ms, p.a, p.b);
+    c->kms[p.kernel] += ms;
+    c->kcount[p.kernel] += 1;
+    c->free_events.push_back(p.a);
+    c->free_events.push_back(p.b);
+  }
+  c->pending.clear();
+}
+}  // namespace
+
+namespace {
+
+const int kSupported[] = {4, 6, 8, 10, 12, 14, 16, 32, 64};
+
+bool supported_nstr(int n) {
+  for (int s : kSupported)
+    if (s == n) return true;
+  return false;
+}
+
+dsp_status fail(dsp_context ctx, dsp_status st, const std::string& msg) {
+  if (ctx) ctx->last_error = msg;
+  return st;
+}
+
+dsp_status cuda_fail(dsp_context ctx, cudaError_t e, const char* where) {
+  return fail(ctx, DSP_ERR_CUDA, std::string(where) + ": " + cudaGetErrorString(e));
+}
+
+dsp_status ensure(dsp_context ctx, void** buf, size_t* have, size_t need, const char* what) {
+  if (*have >= need) return DSP_OK;
+  if (*buf) {
+    cudaStreamSynchronize(ctx->stream);
+    cudaFree(*buf);
+    *buf = nullptr;
+    *have = 0;
+  }
+  size_t alloc = need + need / 8 + (1 << 20);
+  cudaError_t e = cudaMalloc(buf, alloc);
+  if (e != cudaSuccess) {
+    cudaGetLastError();
+    return fail(ctx, DSP_ERR_NO_MEMORY, std::string("cudaMalloc of ") + what + " failed");
+  }
+  *have = alloc;
+  return DSP_OK;
+}
+
+// Gauss-Legendre nodes/weights on (0,1) by Newton iteration (the reference's
+// gaussianQuadrature, FluxSolver.cpp:257-290) and the m = 0 Legendre table at
+// the nodes (Legendre.cpp:74-88).  Computed on the host so the device and the
+// reference use the same values.
+bool build_tables(int N, std::vector<double>& tab) {
+  const int NN = N / 2;
+  tab.assign(tab_size(N), 0.0);
+  double* mu = tab.data() + tab_mu(N);
+  double* wt = tab.data() + tab_wt(N);
+  for (int i = 1; i <= NN; ++i) {
+    double z = std::cos(M_PI * (i - 0.25) / (NN + 0.5));
+    double z1, pp;
+    int iter = 0;
+    do {
+      double p1 = 1.0, p2 = 0.0;
+      for (int j = 1; j <= NN; ++j) {
+        const double p3 = p2;
+        p2 = p1;
+        p1 = ((2.0 * j - 1.0) * z * p2 - (j - 1.0) * p3) / j;
+      }
+      pp = NN * (z * p1 - p2) / (z * z - 1.0);
+      z1 = z;
+      z = z1 - p1 / pp;
+      if (++iter > 10) return false;
+    } while (std::fabs(z - z1) > 3.0e-14);
+    mu[i - 1] = 0.5 * (1.0 + z);
+    wt[i - 1] = 1.0 / ((1.0 - z * z) * pp * pp);
+  }
+  for (int i = 0; i < NN; ++i) {
+    mu[NN + i] = -mu[i];
+    wt[NN + i] = wt[i];
+  }
+  for (int iq = 0; iq < NN; ++iq) {
+    tab[tab_dsim(N) + iq] = std::sqrt(wt[iq] * mu[iq]);
+    tab[tab_dinv(N) + iq] = 1.0 / tab[tab_dsim(N) + iq];
+  }
+  double* y = tab.data() + tab_ylm(N);
+  for (int i = 0; i < N; ++i) {
+    y[0 * N + i] = 1.0;
+    y[1 * N + i] = mu[i];
+  }
+  for (int l = 2; l < N; ++l)
+    for (int i = 0; i < N; ++i)
+      y[l * N + i] = ((2.0 * l - 1.0) * mu[i] * y[(l - 1) * N + i] - (l - 1.0) * y[(l - 2) * N + i]) / l;
+  return true;
+}
+
+dsp_status get_tables(dsp_context ctx, int N, const double** out) {
+  auto it = ctx->tables.find(N);
+  if (it != ctx->tables.end()) {
+    *out = it->second;
+    return DSP_OK;
+  }
+  std::vector<double> tab;
+  if (!build_tables(N, tab)) return fail(ctx, DSP_ERR_EIGEN, "Gauss quadrature did not converge");
+  double* d = nullptr;
+  cudaError_t e = cudaMalloc(&d, tab.size() * sizeof(double));
+  if (e != cudaSuccess) return cuda_fail(ctx, e, "cudaMalloc(tables)");
+  e = cudaMemcpy(d, tab.data(), tab.size() * sizeof(double), cudaMemcpyHostToDevice);
+  if (e != cudaSuccess) return cuda_fail(ctx, e, "cudaMemcpy(tables)");
+  ctx->tables[N] = d;
+  *out = d;
+  return DSP_OK;
+}
+
+PlanckConsts planck_consts() {
+  PlanckConsts pk;
+  pk.vmax = std::log(DBL_MAX);
+  pk.sigdpi = 5.67032E-8 / M_PI;
+  pk.conc = 15.0 / std::pow(M_PI, 4.0);
+  pk.c1 = 1.1911e-8;
+  return pk;
+}
+
+struct Sizes {
+  size_t inst, layer, bvp;  // doubles per instance
+  size_t per_inst_bytes() const { return (inst + layer + bvp) * sizeof(double) + sizeof(int32_t); }
+};
+
+Sizes sizes_for(int N, int L) {
+  Sizes s;
+  s.inst = InstLayout::make(L, N).stride;
+  s.layer = (size_t)L * lrec_stride(N);
+  s.bvp = (size_t)L * brec_stride(N);
+  return s;
+}
+
+size_t workspace_budget() {
+  const char* e = std::getenv("DSP_WORKSPACE_MB");
+  size_t mb = e ? (size_t)std::strtoull(e, nullptr, 10) : 8192;
+  if (mb < 16) mb = 16;
+  return mb << 20;
+}
+
+template <int N>
+dsp_status launch_flux_chunk(dsp_context ctx, const FluxParams& p) {
+  cudaStream_t s = ctx->stream;
+  {
+    KernelTimer kt(ctx, "flux_setup_kernel");
+    flux_setup_kernel<<<(p.n + 3) / 4, 128, 0, s>>>(p);
+  }
+  {
+    KernelTimer kt(ctx, "flux_layer_kernel");
+    using C = LCfg<N>;
+    const size_t sm = C::smem_bytes();
+    static bool attr = false;
+    if (!attr) {
+      cudaFuncSetAttribute(flux_layer_kernel<N>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+      attr = true;
+    }
+    const long long tasks = (long long)p.n * p.L;
+    const long long grid = (tasks + C::TPC - 1) / C::TPC;
+    flux_layer_kernel<N><<<(unsigned)grid, C::CTA, sm, s>>>(p);
+  }
+  {
+    using C = BCfg<N>;
+    const size_t sm = C::smem_bytes();
+    static bool attr = false;
+    if (!attr) {
+      cudaFuncSetAttribute(flux_bvp_kernel<N>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+      attr = true;
+    }
+    const int grid = (p.n + C::TPC - 1) / C::TPC;
+    KernelTimer kt(ctx, "flux_bvp_kernel");
+    flux_bvp_kernel<N><<<grid, C::CTA, sm, s>>>(p);
+  }
+  cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess) return cuda_fail(ctx, e, "flux kernel launch");
+  return DSP_OK;
+}
+
+dsp_status launch_flux(dsp_context ctx, int N, const FluxParams& p) {
+  switch (N) {
+    case 4: return launch_flux_chunk<4>(ctx, p);
+    case 6: return launch_flux_chunk<6>(ctx, p);
+    case 8: return launch_flux_chunk<8>(ctx, p);
+    case 10: return launch_flux_chunk<10>(ctx, p);
+    case 12: return launch_flux_chunk<12>(ctx, p);
+    case 14: return launch_flux_chunk<14>(ctx, p);
+    case 16: return launch_flux_chunk<16>(ctx, p);
+    case 32: return launch_flux_chunk<32>(ctx, p);
+    case 64: return launch_flux_chunk<64>(ctx, p);
+  }
+  return fail(ctx, DSP_ERR_UNSUPPORTED, "unsupported num_streams");
+}
+
+// elements of one instance's value for each batch array, in FLUX field order
+void per_inst_counts(const dsp_flux_batch* b, int64_t cnt[14]) {
+  const int L = b->num_layers;
+  const int64_t c[14] = {1, 1, L, L, (int64_t)L * b->pmom_count, L + 1, 1, 1, 1, 1, 1, 1, 1, 1};
+  for (int k = 0; k < 14; ++k) cnt[k] = c[k];
+}
+
+dsp_darray* batch_arrays(dsp_flux_batch* b) { return &b->wavenumber_low; }
+
+}  // namespace
+
+extern "C" {
+
+int32_t dsp_api_version(void) { return DSP_API_VERSION; }
+
+const char* dsp_status_string(dsp_status s) {
+  switch (s) {
+    case DSP_OK: return "OK";
+    case DSP_ERR_INVALID_INPUT: return "INVALID_INPUT";
+    case DSP_ERR_SINGULAR: return "SINGULAR";
+    case DSP_ERR_NONFINITE: return "NONFINITE";
+    case DSP_ERR_TIMEOUT: return "TIMEOUT";
+    case DSP_ERR_CUDA: return "CUDA_ERROR";
+    case DSP_ERR_UNSUPPORTED: return "UNSUPPORTED";
+    case DSP_ERR_NO_MEMORY: return "NO_MEMORY";
+    case DSP_ERR_EIGEN: return "EIGEN";
+    case DSP_ERR_NOT_INITIALIZED: return "NOT_INITIALIZED";
+  }
+  return "UNKNOWN";
+}
+
+dsp_status dsp_context_create(int32_t device, void* stream, dsp_context* out) {
+  if (!out) return DSP_ERR_INVALID_INPUT;
+  *out = nullptr;
+  int ndev = 0;
+  cudaError_t e = cudaGetDeviceCount(&ndev);
+  if (e != cudaSuccess || ndev == 0) {
+    cudaGetLastError();
+    return DSP_ERR_CUDA;
+  }
+  if (device < 0 || device >= ndev) return DSP_ERR_INVALID_INPUT;
+  e = cudaSetDevice(device);
+  if (e != cudaSuccess) return DSP_ERR_CUDA;
+  dsp_context c = new dsp_context_s();
+  c->device = device;
+  c->stream = static_cast<cudaStream_t>(stream);
+  cudaDeviceGetAttribute(&c->sm_count, cudaDevAttrMultiProcessorCount, device);
+  *out = c;
+  return DSP_OK;
+}
+
+dsp_status dsp_context_destroy(dsp_context ctx) {
+  if (!ctx) return DSP_ERR_INVALID_INPUT;
+  cudaSetDevice(ctx->device);
+  cudaStreamSynchronize(ctx->stream);
+  drain_timing(ctx);
+  for (cudaEvent_t e : ctx->free_events) cudaEventDestroy(e);
+  if (ctx->ws) cudaFree(ctx->ws);
+  if (ctx->stage_in) cudaFree(ctx->stage_in);
+  if (ctx->stage_out) cudaFree(ctx->stage_out);
+  for (auto& kv : ctx->tables) cudaFree(kv.second);
+  delete ctx;
+  return DSP_OK;
+}
+
+dsp_status dsp_context_set_stream(dsp_context ctx, void* stream) {
+  if (!ctx) return DSP_ERR_INVALID_INPUT;
+  ctx->stream = static_cast<cudaStream_t>(stream);
+  return DSP_OK;
+}
+
+const char* dsp_context_last_error(dsp_context ctx) { return ctx ? ctx->last_error.c_str() : ""; }
+
+dsp_status dsp_context_set_timing(dsp_context ctx, int32_t enable) {
+  if (!ctx) return DSP_ERR_NOT_INITIALIZED;
+  ctx->timing = enable != 0;
+  return DSP_OK;
+}
+
+dsp_status dsp_context_timing_reset(dsp_context ctx) {
+  if (!ctx) return DSP_ERR_NOT_INITIALIZED;
+  drain_timing(ctx);
+  for (auto& v : ctx->kms) v = 0.0;
+  for (auto& v : ctx->kcount) v = 0;
+  return DSP_OK;
+}
+
+int32_t dsp_context_timing_count(dsp_context ctx) {
+  if (!ctx) return 0;
+  drain_timing(ctx);
+  return (int32_t)ctx->knames.size();
+}
+
+dsp_status dsp_context_timing_get(dsp_context ctx, int32_t idx, const char** name, double* total_ms,
+                                  int64_t* launches) {
+  if (!ctx) return DSP_ERR_NOT_INITIALIZED;
+  drain_timing(ctx);
+  if (idx < 0 || idx >= (int32_t)ctx->knames.size()) return DSP_ERR_INVALID_INPUT;
+  if (name) *name = ctx->knames[idx].c_str();
+  if (total_ms) *total_ms = ctx->kms[idx];
+  if (launches) *launches = ctx->kcount[idx];
+  return DSP_OK;
+}
+
+int64_t dsp_flux_workspace_bytes(const dsp_flux_batch* b) {
+  if (!b || b->num_layers <= 0 || !supported_nstr(b->num_streams)) return -1;
+  const Sizes s = sizes_for(b->num_streams, b->num_layers);
+  return (int64_t)s.per_inst_bytes() * (int64_t)b->n_inst;
+}
+
+dsp_status dsp_flux_bands_solve(dsp_context ctx, const dsp_flux_batch* batch_in, const dsp_flux_out* out) {
+  if (!ctx) return DSP_ERR_NOT_INITIALIZED;
+  if (!batch_in || !out) return fail(ctx, DSP_ERR_INVALID_INPUT, "null batch or output");
+  dsp_flux_batch b = *batch_in;
+  const int n = b.n_inst, N = b.num_streams, L = b.num_layers;
+  if (n < 0) return fail(ctx, DSP_ERR_INVALID_INPUT, "n_inst must be >= 0");
+  if (n == 0) return DSP_OK;
+  if (L <= 0) return fail(ctx, DSP_ERR_INVALID_INPUT, "num_layers must be > 0");
+  if (N < 4 || N % 2 != 0) return fail(ctx, DSP_ERR_INVALID_INPUT, "num_streams must be even and >= 4");
+  if (!supported_nstr(N))
+    return fail(ctx, DSP_ERR_UNSUPPORTED, "Unsupported num_streams=" + std::to_string(N) +
+                                              ". Supported values: 4, 6, 8, 10, 12, 14, 16, 32, 64");
+  if (b.num_phase_func_moments < 0) return fail(ctx, DSP_ERR_INVALID_INPUT, "num_phase_func_moments must be >= 0");
+  const int nmomnstr = b.num_phase_func_moments > N ? b.num_phase_func_moments : N;
+  if (b.pmom_count < nmomnstr + 1)
+    return fail(ctx, DSP_ERR_INVALID_INPUT, "phase_function_moments size < nmomNstr()+1");
+  if (b.flags & (DSP_FLAG_SPHERICAL_BEAM | DSP_FLAG_TEMPERATURE_JAC))
+    return fail(ctx, DSP_ERR_UNSUPPORTED, "spherical beam and temperature Jacobians are not in this engine");
+  const bool thermal = (b.flags & DSP_FLAG_THERMAL) != 0;
+  if (!b.delta_tau.ptr || !b.single_scat_albedo.ptr || !b.phase_function_moments.ptr)
+    return fail(ctx, DSP_ERR_INVALID_INPUT, "delta_tau, single_scat_albedo and phase_function_moments are required");
+  if (thermal && (!b.temperature.ptr || !b.wavenumber_low.ptr || !b.wavenumber_high.ptr))
+    return fail(ctx, DSP_ERR_INVALID_INPUT, "thermal emission needs temperature and wavenumber bands");
+  cudaError_t e = cudaSetDevice(ctx->device);
+  if (e != cudaSuccess) return cuda_fail(ctx, e, "cudaSetDevice");
+  cudaStream_t s = ctx->stream;
+  const bool dev = (b.flags & DSP_FLAG_DEVICE_POINTERS) != 0;
+  const int64_t nlev = L + 1;
+  dsp_status st;
+
+  // scalar defaults for absent per-instance scalars (DisortFluxConfig.hpp:30-44)
+  static const double kDefaults[14] = {0, 0, 0, 0, 0, 0, 0.0, 1.0, 0.0, 0.5, 0.0, 0.0, 0.0, 0.0};
+  int64_t cnt[14];
+  per_inst_counts(&b, cnt);
+
+  // ---- stage host inputs (and defaults) into device memory ---------------
+  dsp_darray* arr = batch_arrays(&b);
+  {
+    size_t need = 0;
+    for (int k = 0; k < 14; ++k) {
+      size_t elems;
+      if (!arr[k].ptr) elems = (k <= 1 || k >= 6) ? 1 : 0;
+      else if (dev) elems = 0;
+      else elems = arr[k].stride == 0 ? (size_t)cnt[k] : (size_t)((n - 1) * arr[k].stride + cnt[k]);
+      need += ((elems * sizeof(double) + 255) / 256) * 256;
+    }
+    if ((st = ensure(ctx, &ctx->stage_in, &ctx->stage_in_bytes, need + 256, "input staging")) != DSP_OK) return st;
+    char* cur = static_cast<char*>(ctx->stage_in);
+    for (int k = 0; k < 14; ++k) {
+      if (!arr[k].ptr) {
+        if (k <= 1 || k >= 6) {  // absent scalar: the DisortFluxConfig default
+          e = cudaMemcpyAsync(cur, &kDefaults[k], sizeof(double), cudaMemcpyHostToDevice, s);
+          if (e != cudaSuccess) return cuda_fail(ctx, e, "cudaMemcpyAsync(default)");
+          arr[k].ptr = reinterpret_cast<const double*>(cur);
+          arr[k].stride = 0;
+          cur += 256;
+        }
+        continue;
+      }
+      if (dev) continue;
+      const size_t elems = arr[k].stride == 0 ? (size_t)cnt[k] : (size_t)((n - 1) * arr[k].stride + cnt[k]);
+      e = cudaMemcpyAsync(cur, arr[k].ptr, elems * sizeof(double), cudaMemcpyHostToDevice, s);
+      if (e != cudaSuccess) return cuda_fail(ctx, e, "cudaMemcpyAsync(input)");
+      arr[k].ptr = reinterpret_cast<const double*>(cur);
+      cur += ((elems * sizeof(double) + 255) / 256) * 256;
+    }
+    // kDefaults is static storage; the copies above are ordered before the kernels
+  }
+  // ---- outputs -----------------------------------------------------------
+  double* dout[8];
+  int32_t* dstatus = nullptr;
+  {
+    double* host_out[8] = {out->flux_direct_beam, out->flux_down, out->flux_up, out->flux_tau_divergence,
+                           out->mean_intensity, out->mean_intensity_down, out->mean_intensity_up,
+                           out->mean_intensity_direct_beam};
+    for (int f = 0; f < 8; ++f)
+      if (!host_out[f]) return fail(ctx, DSP_ERR_INVALID_INPUT, "every output array is required");
+    const size_t arr_bytes = ((size_t)n * nlev * sizeof(double) + 255) / 256 * 256;
+    const size_t st_bytes = ((size_t)n * sizeof(int32_t) + 255) / 256 * 256;
+    const size_t need = (dev ? 0 : 8 * arr_bytes) + st_bytes;
+    if ((st = ensure(ctx, &ctx->stage_out, &ctx->stage_out_bytes, need, "output staging")) != DSP_OK) return st;
+    char* cur = static_cast<char*>(ctx->stage_out);
+    for (int f = 0; f < 8; ++f) {
+      if (dev) dout[f] = host_out[f];
+      else {
+        dout[f] = reinterpret_cast<double*>(cur);
+        cur += arr_bytes;
+      }
+    }
+    dstatus = (dev && out->status) ? out->status : reinterpret_cast<int32_t*>(cur);
+  }
+  e = cudaMemsetAsync(dstatus, 0, (size_t)n * sizeof(int32_t), s);
+  if (e != cudaSuccess) return cuda_fail(ctx, e, "cudaMemsetAsync(status)");
+
+  const double* tables = nullptr;
+  if ((st = get_tables(ctx, N, &tables)) != DSP_OK) return st;
+
+  // ---- workspace and chunking -------------------------------------------
+  const Sizes sz = sizes_for(N, L);
+  size_t budget = workspace_budget();
+  size_t freeb = 0, totalb = 0;
+  if (cudaMemGetInfo(&freeb, &totalb) == cudaSuccess && freeb / 2 < budget + ctx->ws_bytes)
+    budget = (freeb + ctx->ws_bytes) / 2;
+  int64_t chunk = (int64_t)(budget / sz.per_inst_bytes());
+  if (chunk < 1) chunk = 1;
+  if (chunk > n) chunk = n;
+  const size_t ws_need = (size_t)chunk * (sz.inst + sz.layer + sz.bvp) * sizeof(double) + 1024;
+  if ((st = ensure(ctx, &ctx->ws, &ctx->ws_bytes, ws_need, "workspace")) != DSP_OK) return st;
+
+  FluxParams p;
+  p.N = N;
+  p.L = L;
+  p.pc = b.pmom_count;
+  p.nmom = b.num_phase_func_moments;
+  p.flags = b.flags;
+  p.tables = tables;
+  p.pk = planck_consts();
+  p.il = InstLayout::make(L, N);
+  DArr* pa[14] = {&p.wlo, &p.whi, &p.dtau, &p.ssa, &p.pmom, &p.temp, &p.alb,
+                  &p.emis, &p.fbeam, &p.umu0, &p.fisot, &p.fisob, &p.ttop, &p.tbot};
+  for (int64_t off = 0; off < n; off += chunk) {
+    const int64_t m = (n - off < chunk) ? (n - off) : chunk;
+    p.n = (int)m;
+    for (int k = 0; k < 14; ++k) {
+      pa[k]->p = arr[k].ptr ? arr[k].ptr + arr[k].stride * off : nullptr;
+      pa[k]->s = arr[k].stride;
+    }
+    double* w = static_cast<double*>(ctx->ws);
+    p.inst_rec = w;
+    p.layer_rec = w + (size_t)m * sz.inst;
+    p.bvp_rec = p.layer_rec + (size_t)m * sz.layer;
+    for (int f = 0; f < 8; ++f) p.out[f] = dout[f] + off * nlev;
+    p.status = dstatus + off;
+    if ((st = launch_flux(ctx, N, p)) != DSP_OK) return st;
+  }
+
+  if (dev) return DSP_OK;
+  // ---- copy back ---------------------------------------------------------
+  double* host_out[8] = {out->flux_direct_beam, out->flux_down, out->flux_up, out->flux_tau_divergence,
+                         out->mean_intensity, out->mean_intensity_down, out->mean_intensity_up,
+                         out->mean_intensity_direct_beam};
+  for (int f = 0; f < 8; ++f) {
+    e = cudaMemcpyAsync(host_out[f], dout[f], (size_t)n * nlev * sizeof(double), cudaMemcpyDeviceToHost, s);
+    if (e != cudaSuccess) return cuda_fail(ctx, e, "cudaMemcpyAsync(output)");
+  }
+  std::vector<int32_t> hst;
+  int32_t* hs = out->status;
+  if (!hs) {
+    hst.resize(n);
+    hs = hst.data();
+  }
+  e = cudaMemcpyAsync(hs, dstatus, (size_t)n * sizeof(int32_t), cudaMemcpyDeviceToHost, s);
+  if (e != cudaSuccess) return cuda_fail(ctx, e, "cudaMemcpyAsync(status)");
+  e = cudaStreamSynchronize(s);
+  if (e != cudaSuccess) return cuda_fail(ctx, e, "flux solve");
+  return DSP_OK;
+}
+
+}  // extern "C"

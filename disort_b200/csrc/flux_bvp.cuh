@@ -1,0 +1,411 @@
+// flux_bvp.cuh — boundary-value problem and fluxes, one team per instance.
+//
+// Replaces setMatrix (FluxSolver.cpp:838-959), solve0 (:966-1131, the LINPACK
+// band LU of BandSolver.hpp:29-172) and computeFluxes (:1138-1287).
+//
+// The reference stores the (N*ncut)^2 system in LINPACK band form (lda = 9NN-2)
+// and factors it with partial pivoting (ml = mu = 3NN-1).  Its rows are a
+// staircase: NN top-boundary rows on x_0, N continuity rows on (x_l, x_{l+1})
+// per interface, NN bottom rows on x_{ncut-1}.  For the N columns of x_l the
+// rows with non-zeros that are not yet pivot rows are exactly NN carried rows
+// plus the N rows of interface (l, l+1) -- the same candidate set the band
+// pivot search sees -- so the elimination is done on a 3NN x (2N+1) panel held
+// in shared memory: pivot = largest |a| among candidates, multipliers
+// a * (-1/pivot) and row updates as in sgbfa, the right-hand side carried along
+// as sgbsl's forward sweep.  After the N pivots of a layer the pivot rows give
+// U_l x_l + V_l x_{l+1} = c_l; the team stores W_l = U_l^{-1} V_l (transposed)
+// and d_l = U_l^{-1} c_l in an L2-resident workspace and keeps the NN remaining
+// rows as the next layer's carried rows.  Back substitution then runs bottom-up,
+// x_l = d_l - W_l x_{l+1}, and each x_l immediately yields the fluxes at the
+// layer's bottom level (and at the top level for layer 0).
+#pragma once
+
+#include "dsp_device.cuh"
+
+namespace dsp {
+
+template <int N>
+struct BCfg {
+  static constexpr int NN = N / 2;
+  static constexpr int TEAM = pow2ceil(2 * N) < 8 ? 8 : pow2ceil(2 * N);
+  static constexpr int CTA = TEAM >= 32 ? TEAM : 32;
+  static constexpr int TPC = CTA / TEAM;
+  static constexpr int PR = 3 * NN;       // panel row slots
+  static constexpr int LDP = 2 * N + 1;   // two column blocks + rhs (odd stride)
+  static constexpr int RHS = 2 * N;
+  static constexpr int O_P = 0;
+  static constexpr int O_M = O_P + PR * LDP;  // multipliers [PR]
+  static constexpr int O_X = O_M + PR;        // x ping-pong [2][N]
+  static constexpr int O_EC = O_X + 2 * N;    // [N]
+  static constexpr int O_I = O_EC + N;        // intensities [N]
+  static constexpr int O_E = O_I + N;         // exp(eig*dtau) of layer l and l+1 [2][NN]
+  static constexpr int O_MISC = O_E + 2 * NN; // 8
+  static constexpr int O_ST = O_MISC + 8;     // int state[PR], pivslot[N], freeslot[PR]
+  static constexpr int TEAM_SMEM = round4(O_ST + (2 * PR + N + 1) / 2 + 1);
+  static constexpr int TAB = tab_size(N);
+  static constexpr size_t smem_bytes() { return sizeof(double) * (size_t)(TAB + TPC * TEAM_SMEM); }
+};
+
+template <int N>
+__global__ void __launch_bounds__(BCfg<N>::CTA) flux_bvp_kernel(FluxParams p) {
+  using C = BCfg<N>;
+  constexpr int NN = C::NN, TEAM = C::TEAM, PR = C::PR, LDP = C::LDP, RHS = C::RHS;
+  constexpr double PI = 3.14159265358979323846;
+  extern __shared__ double smem[];
+  for (int k = threadIdx.x; k < C::TAB; k += blockDim.x) smem[k] = p.tables[k];
+  __syncthreads();
+  const double* mu = smem + tab_mu(N);
+  const double* wt = smem + tab_wt(N);
+
+  const int team = threadIdx.x / TEAM, t = threadIdx.x % TEAM;
+  const int i = blockIdx.x * C::TPC + team;
+  if (i >= p.n) return;
+  const int L = p.L;
+  const long long nlev = L + 1;
+  // index_from_bottom: outputs are reversed (IndexConversion.hpp:60-116)
+  const bool ifb = (p.flags & DSP_FLAG_INDEX_FROM_BOTTOM) != 0;
+  auto oidx = [&](int lev) { return (long long)i * nlev + (ifb ? L - lev : lev); };
+  const int st0 = p.status ? p.status[i] : 0;
+  if (st0 == DSP_ERR_INVALID_INPUT || st0 == DSP_ERR_EIGEN) {
+    const double qnan = __longlong_as_double(0x7ff8000000000000ll);
+    for (int lev = t; lev <= L; lev += TEAM)
+      for (int f = 0; f < 8; ++f) p.out[f][oidx(lev)] = qnan;
+    return;
+  }
+  const InstLayout& il = p.il;
+  const double* rec = p.inst_rec + (long long)i * il.stride;
+  const int ncut = (int)rec[H_NCUT];
+  const bool lyrcut = rec[H_LYRCUT] != 0.0;
+  const bool thermal = (p.flags & DSP_FLAG_THERMAL) != 0;
+  const bool dlbc = (p.flags & DSP_FLAG_DIFFUSION_LOWER_BC) != 0;
+  const double fbeam = rec[H_FBEAM], umu0 = rec[H_UMU0], alb = rec[H_ALB];
+  const bool beam = fbeam > 0.0;
+  const double* taus = rec + il.tau_s;
+  const double* btr = rec + il.btr;
+  const double* dtau_s = rec + il.dtau_s;
+  const double* lrec0 = p.layer_rec + (long long)i * L * lrec_stride(N);
+  double* brec0 = p.bvp_rec + (long long)i * L * brec_stride(N);
+
+  double* sm = smem + C::TAB + team * C::TEAM_SMEM;
+  double* P = sm + C::O_P;
+  double* mlt = sm + C::O_M;
+  double* X = sm + C::O_X;
+  double* ec = sm + C::O_EC;
+  double* Iv = sm + C::O_I;
+  double* E = sm + C::O_E;
+  double* misc = sm + C::O_MISC;
+  int* state = reinterpret_cast<int*>(sm + C::O_ST);
+  int* pivslot = state + PR;
+  int* freeslot = pivslot + N;
+
+  auto LR = [&](int l) { return lrec0 + (long long)l * lrec_stride(N); };
+  bool singular = false;
+
+  // ------------------------------------------------------------------ forward
+  for (int s = t; s < PR; s += TEAM) state[s] = 0;
+  for (int m = t; m < NN; m += TEAM) {
+    const double* l0 = LR(0);
+    E[m] = exp(l0[lrec_eig(N) + m] * dtau_s[0]);
+  }
+  team_sync<TEAM>();
+  // top boundary rows into slots 0..NN-1 (setMatrix :890-907, solve0 :978-990)
+  {
+    const double* l0 = LR(0);
+    const double* G0 = l0 + lrec_G(N);
+    const double ptop = rec[H_PTOP], fisot = rec[H_FISOT];
+    for (int it = t; it < NN * (2 * N + 1); it += TEAM) {
+      const int r = it / (2 * N + 1), col = it % (2 * N + 1);
+      const int jq = NN - 1 - r;
+      double v;
+      if (col < N) v = (col < NN) ? G0[jq * N + col] * E[col] : G0[jq * N + col];
+      else if (col < 2 * N) v = 0.0;
+      else {
+        double s = 0.0;
+        if (beam) s -= l0[lrec_zb(N) + jq];
+        if (thermal) s -= l0[lrec_z0(N) + jq];
+        s += fisot + ptop;
+        v = s;
+      }
+      P[r * LDP + col] = v;
+    }
+    for (int r = t; r < NN; r += TEAM) state[r] = 1;
+  }
+  team_sync<TEAM>();
+
+  for (int l = 0; l < ncut; ++l) {
+    const int cb = (l & 1) * N, nb = ((l & 1) ^ 1) * N;
+    const bool last = (l == ncut - 1);
+    const double* lr = LR(l);
+    const double* Gl = lr + lrec_G(N);
+    const double* Ecur = E + (l & 1) * NN;
+    double* Enext = E + ((l & 1) ^ 1) * NN;
+    // free slots list (slots not carried), carried rows lose their stale block
+    if (t == 0) {
+      int nf = 0;
+      for (int s = 0; s < PR; ++s) {
+        if (state[s] == 2) state[s] = 0;
+        if (state[s] == 0) freeslot[nf++] = s;
+      }
+    }
+    if (!last) {
+      const double* ln = LR(l + 1);
+      for (int m = t; m < NN; m += TEAM) Enext[m] = exp(ln[lrec_eig(N) + m] * dtau_s[l + 1]);
+    }
+    team_sync<TEAM>();
+    if (l > 0)
+      for (int it = t; it < PR * N; it += TEAM) {
+        const int s = it / N, c = it % N;
+        if (state[s] == 1) P[s * LDP + nb + c] = 0.0;
+      }
+    if (!last) {
+      // continuity rows of interface (l, l+1) (setMatrix :852-887, solve0 :1080-1104)
+      const double* ln = LR(l + 1);
+      const double* Gn = ln + lrec_G(N);
+      const double T = btr[l + 1], tau = taus[l + 1];
+      for (int it = t; it < N * (2 * N + 1); it += TEAM) {
+        const int jq = it / (2 * N + 1), col = it % (2 * N + 1);
+        const int s = freeslot[jq];
+        double v;
+        if (col < N) {
+          const int iq = col;
+          v = (iq < NN) ? Gl[jq * N + iq] : Gl[jq * N + iq] * Ecur[N - 1 - iq];
+          P[s * LDP + cb + iq] = v;
+        } else if (col < 2 * N) {
+          const int iq = col - N;
+          v = (iq < NN) ? -Gn[jq * N + iq] * Enext[iq] : -Gn[jq * N + iq];
+          P[s * LDP + nb + iq] = v;
+        } else {
+          double sum = 0.0;
+          if (beam) {
+            sum += ln[lrec_zb(N) + jq] * T;
+            sum -= lr[lrec_zb(N) + jq] * T;
+          }
+          if (thermal) {
+            sum += ln[lrec_z0(N) + jq] - lr[lrec_z0(N) + jq];
+            sum += (ln[lrec_z1(N) + jq] - lr[lrec_z1(N) + jq]) * tau;
+          }
+          P[s * LDP + RHS] = sum;
+        }
+      }
+      for (int jq = t; jq < N; jq += TEAM) state[freeslot[jq]] = 1;
+    } else {
+      // bottom boundary rows (setMatrix :909-958, solve0 :993-1076)
+      const bool plain = lyrcut || dlbc;
+      const double T = btr[ncut], tau = taus[ncut];
+      const double pbot = rec[H_PBOT], pbotd = rec[H_PBOTD], fisob = rec[H_FISOB];
+      for (int it = t; it < NN * (2 * N + 1); it += TEAM) {
+        const int rb = it / (2 * N + 1), col = it % (2 * N + 1);
+        const int jq = NN + rb;
+        const int s = freeslot[rb];
+        if (col < N) {
+          const int iq = col;
+          double base = Gl[jq * N + iq];
+          if (!plain) {
+            double refl = 0.0;
+            for (int k = 0; k < NN; ++k) refl += wt[k] * mu[k] * alb * Gl[(NN - 1 - k) * N + iq];
+            base = Gl[jq * N + iq] - 2.0 * refl;
+          }
+          P[s * LDP + cb + iq] = (iq < NN) ? base : base * Ecur[N - 1 - iq];
+        } else if (col < 2 * N) {
+          P[s * LDP + nb + (col - N)] = 0.0;
+        } else {
+          double sum = 0.0;
+          if (dlbc) {
+            if (beam) sum -= lr[lrec_zb(N) + NN + rb] * T;
+            if (thermal) {
+              sum -= lr[lrec_z0(N) + NN + rb];
+              sum -= lr[lrec_z1(N) + NN + rb] * tau;
+            }
+            sum += pbot + mu[rb] * pbotd;
+          } else {
+            if (!lyrcut) {
+              double refl = 0.0;
+              for (int jj = 0; jj < NN; ++jj) {
+                double ps = 0.0;
+                if (beam) ps += lr[lrec_zb(N) + NN - 1 - jj] * T;
+                if (thermal) ps += lr[lrec_z0(N) + NN - 1 - jj] + lr[lrec_z1(N) + NN - 1 - jj] * tau;
+                refl += wt[jj] * mu[jj] * alb * ps;
+              }
+              sum += 2.0 * refl;
+            }
+            if (beam) {
+              sum -= lr[lrec_zb(N) + NN + rb] * T;
+              if (!lyrcut) sum += alb * umu0 * fbeam * T / PI;
+            }
+            if (thermal) {
+              sum -= lr[lrec_z0(N) + NN + rb];
+              sum -= lr[lrec_z1(N) + NN + rb] * tau;
+            }
+            sum += fisob;
+            if (thermal) sum += (1.0 - alb) * pbot;
+          }
+          P[s * LDP + RHS] = sum;
+        }
+      }
+      for (int rb = t; rb < NN; rb += TEAM) state[freeslot[rb]] = 1;
+    }
+    team_sync<TEAM>();
+
+    // ---- eliminate the N columns of x_l (sgbfa steps) ----------------------
+    for (int c = 0; c < N; ++c) {
+      const int col = cb + c;
+      double v = -1.0;
+      int idx = PR;
+      for (int s = t; s < PR; s += TEAM)
+        if (state[s] == 1) {
+          double a = fabs(P[s * LDP + col]);
+          if (isnan(a)) a = __longlong_as_double(0x7ff0000000000000ll);  // NaN ranks as +inf: one total order
+          if (a > v || (a == v && s < idx)) { v = a; idx = s; }
+        }
+      team_argmax<TEAM>(v, idx, misc);
+      const int ps = idx;
+      const double pv = (ps < PR) ? P[ps * LDP + col] : 0.0;
+      team_sync<TEAM>();
+      if (ps >= PR) {  // no candidate row (cannot happen for a well-formed system)
+        singular = true;
+        if (t == 0) pivslot[c] = freeslot[0];
+        team_sync<TEAM>();
+        continue;
+      }
+      if (t == 0) {
+        state[ps] = 2;
+        pivslot[c] = ps;
+      }
+      if (pv == 0.0) {  // LINPACK skips a zero pivot column (BandSolver.hpp:76-78)
+        singular = true;
+        team_sync<TEAM>();
+        continue;
+      }
+      const double tinv = -1.0 / pv;
+      for (int s = t; s < PR; s += TEAM)
+        mlt[s] = (state[s] == 1 && s != ps) ? P[s * LDP + col] * tinv : 0.0;
+      team_sync<TEAM>();
+      // columns col+1 .. end of block, the next block (unless last) and the rhs
+      const int ncols_cur = N - 1 - c;
+      const int ntot = ncols_cur + (last ? 0 : N) + 1;
+      for (int u = t; u < ntot; u += TEAM) {
+        int j;
+        if (u < ncols_cur) j = col + 1 + u;
+        else if (u < ncols_cur + (last ? 0 : N)) j = nb + (u - ncols_cur);
+        else j = RHS;
+        const double pj = P[ps * LDP + j];
+        if (pj != 0.0)
+          for (int s = 0; s < PR; ++s)
+            if (state[s] == 1) P[s * LDP + j] += mlt[s] * pj;
+      }
+      team_sync<TEAM>();
+    }
+
+    if (!last) {
+      // W_l = U^{-1} V (stored transposed), d_l = U^{-1} c; in place on the pivot rows
+      double* br = brec0 + (long long)l * brec_stride(N);
+      for (int j = t; j <= N; j += TEAM) {
+        const int colj = (j < N) ? nb + j : RHS;
+        for (int c = N - 1; c >= 0; --c) {
+          const int ps = pivslot[c];
+          double s = P[ps * LDP + colj];
+          for (int c2 = c + 1; c2 < N; ++c2) s -= P[ps * LDP + cb + c2] * P[pivslot[c2] * LDP + colj];
+          s = s / P[ps * LDP + cb + c];
+          P[ps * LDP + colj] = s;
+          if (j < N) br[j * N + c] = s;
+          else br[N * N + c] = s;
+        }
+      }
+      team_sync<TEAM>();
+    } else {
+      // x_{ncut-1} = U^{-1} rhs (sgbsl back substitution)
+      double* x = X + (l & 1) * N;
+      if (t == 0) {
+        for (int c = N - 1; c >= 0; --c) {
+          const int ps = pivslot[c];
+          double s = P[ps * LDP + RHS];
+          for (int c2 = c + 1; c2 < N; ++c2) s -= P[ps * LDP + cb + c2] * x[c2];
+          x[c] = s / P[ps * LDP + cb + c];
+        }
+      }
+      team_sync<TEAM>();
+    }
+  }
+  if (singular && t == 0) set_status(p.status, i, DSP_ERR_SINGULAR);
+
+  // ----------------------------------------------------------------- backward
+  // levels below the cut carry zeros (computeFluxes :1151-1163)
+  for (int lev = ncut + 1 + t; lev <= L; lev += TEAM)
+    for (int f = 0; f < 8; ++f) p.out[f][oidx(lev)] = 0.0;
+  bool nonfinite = false;
+  for (int l = ncut - 1; l >= 0; --l) {
+    double* x = X + (l & 1) * N;
+    if (l < ncut - 1) {
+      const double* xn = X + ((l & 1) ^ 1) * N;
+      const double* br = brec0 + (long long)l * brec_stride(N);
+      for (int c = t; c < N; c += TEAM) {
+        double s = br[N * N + c];
+        for (int n = 0; n < N; ++n) s -= br[n * N + c] * xn[n];
+        x[c] = s;
+      }
+      team_sync<TEAM>();
+    }
+    const double* lr = LR(l);
+    const double* eig = lr + lrec_eig(N);
+    const double* Gl = lr + lrec_G(N);
+    // outputs at the bottom level of layer l, and at the top for l == 0
+    for (int pass = 0; pass < (l == 0 ? 2 : 1); ++pass) {
+      const int lu = (pass == 0) ? l + 1 : 0;
+      const double utaupr = taus[lu];
+      for (int j = t; j < N; j += TEAM) {
+        const double d = (j < NN) ? (utaupr - taus[l + 1]) : (utaupr - taus[l]);
+        ec[j] = x[j] * exp(-eig[j] * d);
+      }
+      team_sync<TEAM>();
+      const double fact = beam ? exp(-utaupr / umu0) : 0.0;
+      for (int r = t; r < N; r += TEAM) {
+        double s = 0.0;
+        for (int j = 0; j < N; ++j) s += Gl[r * N + j] * ec[j];
+        if (beam) s += lr[lrec_zb(N) + r] * fact;
+        if (thermal) s += lr[lrec_z0(N) + r] + lr[lrec_z1(N) + r] * utaupr;
+        Iv[r] = s;
+      }
+      team_sync<TEAM>();
+      if (t == 0) {
+        double dirint = 0.0, fldir = 0.0, fdir = 0.0;
+        if (beam) {
+          dirint = fbeam * fact;
+          fldir = umu0 * fbeam * fact;
+          fdir = umu0 * fbeam * exp(-rec[il.tauc + lu] / umu0);
+        }
+        double ua = 0.0, uad = 0.0, uau = 0.0, fldn = 0.0, fup = 0.0;
+        for (int iq = 0; iq < NN; ++iq) {
+          const int cw = NN - iq - 1;
+          ua += wt[cw] * Iv[iq];
+          uad += wt[cw] * Iv[iq];
+          fldn += wt[cw] * Iv[iq] * mu[cw];
+        }
+        for (int iq = NN; iq < N; ++iq) {
+          const int cw = iq - NN;
+          ua += wt[cw] * Iv[iq];
+          uau += wt[cw] * Iv[iq];
+          fup += wt[cw] * Iv[iq] * mu[cw];
+        }
+        fup *= 2.0 * PI;
+        fldn *= 2.0 * PI;
+        const double fdn = (fldn + fldir) - fdir;
+        ua = (2.0 * PI * ua + dirint) / (4.0 * PI);
+        const double uaso = dirint / (4.0 * PI);
+        uad = (2.0 * PI * uad) / (4.0 * PI);
+        uau = (2.0 * PI * uau) / (4.0 * PI);
+        double plsorc = 0.0;
+        if (thermal) plsorc = lr[lrec_xr(N)] + lr[lrec_xr(N) + 1] * utaupr;
+        const double dfdt = (1.0 - p.ssa(i, ifb ? L - 1 - l : l)) * 4.0 * PI * (ua - plsorc);
+        const double o[8] = {fdir, fdn, fup, dfdt, ua, uad, uau, uaso};
+        for (int f = 0; f < 8; ++f) {
+          p.out[f][oidx(lu)] = o[f];
+          if (!isfinite(o[f])) nonfinite = true;
+        }
+      }
+      team_sync<TEAM>();
+    }
+  }
+  if (nonfinite && t == 0) set_status(p.status, i, DSP_ERR_NONFINITE);
+}
+
+}  // namespace dsp

@@ -126,6 +126,17 @@ const char* dsp_context_last_error(dsp_context ctx);
  */
 int64_t dsp_flux_workspace_bytes(const dsp_flux_batch* batch);
 
+/*
+ * Per-kernel device timing (instrumentation; no reference counterpart).  When
+ * enabled, every kernel launch of the context is bracketed by CUDA events on the
+ * context's stream; totals accumulate until reset.  Names are static strings.
+ */
+dsp_status dsp_context_set_timing(dsp_context ctx, int32_t enable);
+dsp_status dsp_context_timing_reset(dsp_context ctx);
+int32_t dsp_context_timing_count(dsp_context ctx);
+dsp_status dsp_context_timing_get(dsp_context ctx, int32_t idx, const char** name, double* total_ms,
+                                  int64_t* launches);
+
 /* Flux-only spectral-band solve (DisortFluxSolver<N> over every instance). */
 dsp_status dsp_flux_bands_solve(dsp_context ctx, const dsp_flux_batch* batch,
                                 const dsp_flux_out* out);

@@ -1,0 +1,32 @@
+"""The parity criterion between the GPU engine and the oracle.
+
+Fluxes and mean intensities must agree within 1e-9 relative with a 1e-12
+absolute floor: |gpu - oracle| <= 1e-9 * |oracle| + 1e-12, element by element.
+"""
+import numpy as np
+
+from disort_b200 import capi
+
+RTOL = 1e-9
+ATOL = 1e-12
+
+
+def worst(gpu: dict, ref: dict) -> tuple[float, str]:
+    """Largest |diff| / (RTOL*|ref| + ATOL) over all outputs (<= 1 passes)."""
+    w, where = 0.0, ""
+    for f in capi.FLUX_OUT_FIELDS:
+        a, b = np.asarray(gpu[f]), np.asarray(ref[f])
+        both_nan = np.isnan(a) & np.isnan(b)
+        r = np.where(both_nan, 0.0, np.abs(a - b) / (RTOL * np.abs(b) + ATOL))
+        r = np.where(np.isnan(r), np.inf, r)
+        k = float(r.max()) if r.size else 0.0
+        if k > w:
+            idx = np.unravel_index(int(np.argmax(r)), r.shape)
+            w, where = k, f"{f}{tuple(int(x) for x in idx)} gpu={a[idx]!r} ref={b[idx]!r}"
+    return w, where
+
+
+def assert_parity(gpu: dict, ref: dict, label: str = ""):
+    w, where = worst(gpu, ref)
+    assert w <= 1.0, f"{label}: parity ratio {w:.3g} at {where}"
+    return w
