@@ -22,7 +22,6 @@ import statistics
 import subprocess
 import sys
 import tempfile
-import threading
 import time
 
 import numpy as np
@@ -43,6 +42,9 @@ def parse():
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--workload", choices=["thermal", "beam"], default="thermal")
     ap.add_argument("--cpu-seconds", type=float, default=10.0, help="target CPU-baseline sample time")
+    ap.add_argument("--bands", type=int, default=0, help="profiling: solve only the first N bands")
+    ap.add_argument("--no-cpu", action="store_true", help="profiling: skip the CPU baseline")
+    ap.add_argument("--no-e2e", action="store_true", help="profiling: skip the host-buffer pass")
     return ap.parse_args()
 
 
@@ -205,6 +207,55 @@ def committed_traffic(workload_name: str):
         return None
 
 
+def run_e2e(args, ctx, w, douts, stream, dev, world):
+    import torch
+    import torch.distributed as dist
+    n, L, N = w["n_inst"], w["num_layers"], w["num_streams"]
+    host_arrays = {}
+    h2d = 0
+    for k, a in w["arrays"].items():
+        if isinstance(a, np.ndarray):
+            ta = torch.from_numpy(np.ascontiguousarray(a)).pin_memory()
+            host_arrays[k] = ta
+            h2d += ta.numel() * 8
+        else:
+            host_arrays[k] = a
+            if a is not None:
+                h2d += 8
+    hbatch, hkeep = capi.make_flux_batch(n, N, L, w["num_phase_func_moments"], w["pmom_count"], w["flags"],
+                                         host_arrays)
+    houts = {f: torch.empty((n, L + 1), dtype=torch.float64).pin_memory() for f in capi.FLUX_OUT_FIELDS}
+    hstatus = torch.empty((n,), dtype=torch.int32).pin_memory()
+    hout, hkeep2 = capi.make_flux_out(houts, hstatus)
+    d2h = 8 * n * (L + 1) * 8 + 4 * n
+
+    def hstep():
+        rc = ctx.flux_bands_solve(hbatch, hout)
+        if rc != 0:
+            raise RuntimeError(f"host-pointer solve: {ctx.last_error()}")
+
+    for _ in range(max(1, args.warmup)):
+        hstep()
+    if world > 1:
+        dist.barrier()
+    torch.cuda.synchronize()
+    e2 = torch.cuda.Event(enable_timing=True)
+    e3 = torch.cuda.Event(enable_timing=True)
+    e2.record(stream)
+    for _ in range(args.steps):
+        hstep()
+    e3.record(stream)
+    torch.cuda.synchronize()
+    te = torch.tensor([e2.elapsed_time(e3)], dtype=torch.float64, device=dev)
+    if world > 1:
+        dist.all_reduce(te, op=dist.ReduceOp.MAX)
+    e2e_value = n * args.steps * world / (float(te.item()) / 1000.0)
+    # host results must equal the device-resident results
+    same = all(torch.equal(houts[f], douts[f].cpu()) for f in capi.FLUX_OUT_FIELDS)
+
+    return e2e_value, h2d, d2h, same
+
+
 def run_ours(args):
     import torch
     import torch.distributed as dist
@@ -219,6 +270,9 @@ def run_ours(args):
     stream = torch.cuda.current_stream()
 
     w = make_workload(args.workload, rank)
+    if args.bands:
+        w = workloads.subset(w, np.arange(min(args.bands, w["n_inst"])))
+        w["name"] += f"_first{w['n_inst']}"
     n, L, N = w["n_inst"], w["num_layers"], w["num_streams"]
     ctx = capi.Context(local, stream.cuda_stream)
 
@@ -283,47 +337,10 @@ def run_ours(args):
     value = n * args.steps * world / (ms_max / 1000.0)
 
     # ---- e2e: through the C ABI with pinned host buffers ----------------------
-    host_arrays = {}
-    h2d = 0
-    for k, a in w["arrays"].items():
-        if isinstance(a, np.ndarray):
-            ta = torch.from_numpy(np.ascontiguousarray(a)).pin_memory()
-            host_arrays[k] = ta
-            h2d += ta.numel() * 8
-        else:
-            host_arrays[k] = a
-            if a is not None:
-                h2d += 8
-    hbatch, hkeep = capi.make_flux_batch(n, N, L, w["num_phase_func_moments"], w["pmom_count"], w["flags"],
-                                         host_arrays)
-    houts = {f: torch.empty((n, L + 1), dtype=torch.float64).pin_memory() for f in capi.FLUX_OUT_FIELDS}
-    hstatus = torch.empty((n,), dtype=torch.int32).pin_memory()
-    hout, hkeep2 = capi.make_flux_out(houts, hstatus)
-    d2h = 8 * n * (L + 1) * 8 + 4 * n
-
-    def hstep():
-        rc = ctx.flux_bands_solve(hbatch, hout)
-        if rc != 0:
-            raise RuntimeError(f"host-pointer solve: {ctx.last_error()}")
-
-    for _ in range(max(1, args.warmup)):
-        hstep()
-    if world > 1:
-        dist.barrier()
-    torch.cuda.synchronize()
-    e2 = torch.cuda.Event(enable_timing=True)
-    e3 = torch.cuda.Event(enable_timing=True)
-    e2.record(stream)
-    for _ in range(args.steps):
-        hstep()
-    e3.record(stream)
-    torch.cuda.synchronize()
-    te = torch.tensor([e2.elapsed_time(e3)], dtype=torch.float64, device=dev)
-    if world > 1:
-        dist.all_reduce(te, op=dist.ReduceOp.MAX)
-    e2e_value = n * args.steps * world / (float(te.item()) / 1000.0)
-    # host results must equal the device-resident results
-    same = all(torch.equal(houts[f], douts[f].cpu()) for f in capi.FLUX_OUT_FIELDS)
+    if args.no_e2e:
+        e2e_value, h2d, d2h, same = None, 0, 0, None
+    else:
+        e2e_value, h2d, d2h, same = run_e2e(args, ctx, w, douts, stream, dev, world)
 
     # ---- roofline of the dominant kernel -----------------------------------
     beam = bool(np.any(np.asarray(w["arrays"]["direct_beam_flux"]) > 0))
@@ -343,7 +360,7 @@ def run_ours(args):
     }
 
     if rank == 0:
-        cpu, _ = cpu_baseline(w, args.cpu_seconds)
+        cpu = None if args.no_cpu else cpu_baseline(w, args.cpu_seconds)[0]
         line = {
             "metric": METRIC, "value": value, "unit": "solves/s", "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": ms_max / args.steps, "higher_is_better": True,
