@@ -6,6 +6,14 @@
 
 #include "../../include/dsp.h"
 
+// Phase markers for cycle-count instrumentation builds; no-ops otherwise.
+#ifndef DSP_PHASE_BEGIN
+#define DSP_PHASE_BEGIN
+#endif
+#ifndef DSP_PHASE
+#define DSP_PHASE(k)
+#endif
+
 namespace dsp {
 
 __host__ __device__ constexpr int pow2ceil(int x) { return x <= 1 ? 1 : 2 * pow2ceil((x + 1) / 2); }

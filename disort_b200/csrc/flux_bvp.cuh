@@ -24,6 +24,20 @@
 
 namespace dsp {
 
+// Bitmask over the panel's row slots, kept identical in every thread of a team.
+template <int PR>
+struct SlotMask {
+  static constexpr int W = (PR + 31) / 32;
+  uint32_t w[W];
+  __device__ __forceinline__ void clear() {
+#pragma unroll
+    for (int k = 0; k < W; ++k) w[k] = 0u;
+  }
+  __device__ __forceinline__ void set(int s) { w[s >> 5] |= 1u << (s & 31); }
+  __device__ __forceinline__ void reset(int s) { w[s >> 5] &= ~(1u << (s & 31)); }
+  __device__ __forceinline__ bool test(int s) const { return (w[s >> 5] >> (s & 31)) & 1u; }
+};
+
 template <int N>
 struct BCfg {
   static constexpr int NN = N / 2;
@@ -44,10 +58,12 @@ struct BCfg {
   static constexpr int TEAM_SMEM = round4(O_ST + (2 * PR + N + 1) / 2 + 1);
   static constexpr int TAB = tab_size(N);
   static constexpr size_t smem_bytes() { return sizeof(double) * (size_t)(TAB + TPC * TEAM_SMEM); }
+  // resident CTAs per SM the register allocation must allow (<= 168 registers for 32-thread CTAs)
+  static constexpr int MINB = TEAM >= 128 ? 1 : (TEAM >= 64 ? 4 : 12);
 };
 
 template <int N>
-__global__ void __launch_bounds__(BCfg<N>::CTA) flux_bvp_kernel(FluxParams p) {
+__global__ void __launch_bounds__(BCfg<N>::CTA, BCfg<N>::MINB) flux_bvp_kernel(FluxParams p) {
   using C = BCfg<N>;
   constexpr int NN = C::NN, TEAM = C::TEAM, PR = C::PR, LDP = C::LDP, RHS = C::RHS;
   constexpr double PI = 3.14159265358979323846;
@@ -101,6 +117,7 @@ __global__ void __launch_bounds__(BCfg<N>::CTA) flux_bvp_kernel(FluxParams p) {
   auto LR = [&](int l) { return lrec0 + (long long)l * lrec_stride(N); };
   bool singular = false;
 
+  DSP_PHASE_BEGIN
   // ------------------------------------------------------------------ forward
   for (int s = t; s < PR; s += TEAM) state[s] = 0;
   for (int m = t; m < NN; m += TEAM) {
@@ -158,33 +175,49 @@ __global__ void __launch_bounds__(BCfg<N>::CTA) flux_bvp_kernel(FluxParams p) {
         if (state[s] == 1) P[s * LDP + nb + c] = 0.0;
       }
     if (!last) {
-      // continuity rows of interface (l, l+1) (setMatrix :852-887, solve0 :1080-1104)
+      // continuity rows of interface (l, l+1) (setMatrix :852-887, solve0 :1080-1104).
+      // All global reads of an item batch are issued before any shared-memory store.
       const double* ln = LR(l + 1);
       const double* Gn = ln + lrec_G(N);
       const double T = btr[l + 1], tau = taus[l + 1];
-      for (int it = t; it < N * (2 * N + 1); it += TEAM) {
-        const int jq = it / (2 * N + 1), col = it % (2 * N + 1);
-        const int s = freeslot[jq];
-        double v;
-        if (col < N) {
-          const int iq = col;
-          v = (iq < NN) ? Gl[jq * N + iq] : Gl[jq * N + iq] * Ecur[N - 1 - iq];
-          P[s * LDP + cb + iq] = v;
-        } else if (col < 2 * N) {
-          const int iq = col - N;
-          v = (iq < NN) ? -Gn[jq * N + iq] * Enext[iq] : -Gn[jq * N + iq];
-          P[s * LDP + nb + iq] = v;
-        } else {
-          double sum = 0.0;
-          if (beam) {
-            sum += ln[lrec_zb(N) + jq] * T;
-            sum -= lr[lrec_zb(N) + jq] * T;
+      constexpr int ITEMS = N * (2 * N + 1);
+      constexpr int PER = (ITEMS + TEAM - 1) / TEAM;
+      double val[PER];
+#pragma unroll
+      for (int k = 0; k < PER; ++k) {
+        const int it = t + k * TEAM;
+        if (it < ITEMS) {
+          const int jq = it / (2 * N + 1), col = it % (2 * N + 1);
+          if (col < N) {
+            const int iq = col;
+            const double g = __ldg(Gl + jq * N + iq);
+            val[k] = (iq < NN) ? g : g * Ecur[N - 1 - iq];
+          } else if (col < 2 * N) {
+            const int iq = col - N;
+            const double g = __ldg(Gn + jq * N + iq);
+            val[k] = (iq < NN) ? -g * Enext[iq] : -g;
+          } else {
+            double sum = 0.0;
+            if (beam) {
+              sum += __ldg(ln + lrec_zb(N) + jq) * T;
+              sum -= __ldg(lr + lrec_zb(N) + jq) * T;
+            }
+            if (thermal) {
+              sum += __ldg(ln + lrec_z0(N) + jq) - __ldg(lr + lrec_z0(N) + jq);
+              sum += (__ldg(ln + lrec_z1(N) + jq) - __ldg(lr + lrec_z1(N) + jq)) * tau;
+            }
+            val[k] = sum;
           }
-          if (thermal) {
-            sum += ln[lrec_z0(N) + jq] - lr[lrec_z0(N) + jq];
-            sum += (ln[lrec_z1(N) + jq] - lr[lrec_z1(N) + jq]) * tau;
-          }
-          P[s * LDP + RHS] = sum;
+        }
+      }
+#pragma unroll
+      for (int k = 0; k < PER; ++k) {
+        const int it = t + k * TEAM;
+        if (it < ITEMS) {
+          const int jq = it / (2 * N + 1), col = it % (2 * N + 1);
+          const int sl = freeslot[jq];
+          const int pc = (col < N) ? cb + col : (col < 2 * N) ? nb + (col - N) : RHS;
+          P[sl * LDP + pc] = val[k];
         }
       }
       for (int jq = t; jq < N; jq += TEAM) state[freeslot[jq]] = 1;
@@ -245,86 +278,120 @@ __global__ void __launch_bounds__(BCfg<N>::CTA) flux_bvp_kernel(FluxParams p) {
       for (int rb = t; rb < NN; rb += TEAM) state[freeslot[rb]] = 1;
     }
     team_sync<TEAM>();
+    DSP_PHASE(10)
 
     // ---- eliminate the N columns of x_l (sgbfa steps) ----------------------
+    // Candidate rows form a bitmask that every thread tracks identically.
+    SlotMask<PR> cand;
+    cand.clear();
+    for (int sl = 0; sl < PR; ++sl)
+      if (state[sl] == 1) cand.set(sl);
+    const int ncols_next = last ? 0 : N;
     for (int c = 0; c < N; ++c) {
       const int col = cb + c;
       double v = -1.0;
       int idx = PR;
-      for (int s = t; s < PR; s += TEAM)
-        if (state[s] == 1) {
-          double a = fabs(P[s * LDP + col]);
+      for (int sl = t; sl < PR; sl += TEAM)
+        if (cand.test(sl)) {
+          double a = fabs(P[sl * LDP + col]);
           if (isnan(a)) a = __longlong_as_double(0x7ff0000000000000ll);  // NaN ranks as +inf: one total order
-          if (a > v || (a == v && s < idx)) { v = a; idx = s; }
+          if (a > v || (a == v && sl < idx)) { v = a; idx = sl; }
         }
       team_argmax<TEAM>(v, idx, misc);
       const int ps = idx;
-      const double pv = (ps < PR) ? P[ps * LDP + col] : 0.0;
-      team_sync<TEAM>();
       if (ps >= PR) {  // no candidate row (cannot happen for a well-formed system)
         singular = true;
-        if (t == 0) pivslot[c] = freeslot[0];
-        team_sync<TEAM>();
+        if (t == 0) pivslot[c] = 0;
         continue;
       }
+      cand.reset(ps);
       if (t == 0) {
         state[ps] = 2;
         pivslot[c] = ps;
       }
+      const double pv = P[ps * LDP + col];
       if (pv == 0.0) {  // LINPACK skips a zero pivot column (BandSolver.hpp:76-78)
         singular = true;
         team_sync<TEAM>();
         continue;
       }
       const double tinv = -1.0 / pv;
-      for (int s = t; s < PR; s += TEAM)
-        mlt[s] = (state[s] == 1 && s != ps) ? P[s * LDP + col] * tinv : 0.0;
-      team_sync<TEAM>();
-      // columns col+1 .. end of block, the next block (unless last) and the rhs
-      const int ncols_cur = N - 1 - c;
-      const int ntot = ncols_cur + (last ? 0 : N) + 1;
-      for (int u = t; u < ntot; u += TEAM) {
-        int j;
-        if (u < ncols_cur) j = col + 1 + u;
-        else if (u < ncols_cur + (last ? 0 : N)) j = nb + (u - ncols_cur);
-        else j = RHS;
+      // one column per thread: col+1 .. end of block, the next block (unless last), rhs
+      const int ncur = N - 1 - c;
+      const int ntot = ncur + ncols_next + 1;
+      if (t < ntot) {
+        const int j = (t < ncur) ? col + 1 + t : (t < ncur + ncols_next) ? nb + (t - ncur) : RHS;
         const double pj = P[ps * LDP + j];
-        if (pj != 0.0)
-          for (int s = 0; s < PR; ++s)
-            if (state[s] == 1) P[s * LDP + j] += mlt[s] * pj;
+        if (pj != 0.0) {
+          // slots in chunks of 16: all loads of a chunk are issued before its FMAs
+          constexpr int CH = PR < 16 ? PR : 16;
+#pragma unroll
+          for (int base = 0; base < PR; base += CH) {
+            double m[CH], a[CH];
+#pragma unroll
+            for (int k = 0; k < CH; ++k) {
+              const int sl = base + k;
+              if (sl < PR && cand.test(sl)) {
+                m[k] = P[sl * LDP + col];
+                a[k] = P[sl * LDP + j];
+              }
+            }
+#pragma unroll
+            for (int k = 0; k < CH; ++k) {
+              const int sl = base + k;
+              if (sl < PR && cand.test(sl)) P[sl * LDP + j] = a[k] + (m[k] * tinv) * pj;
+            }
+          }
+        }
       }
       team_sync<TEAM>();
     }
 
+    DSP_PHASE(11)
     if (!last) {
-      // W_l = U^{-1} V (stored transposed), d_l = U^{-1} c; in place on the pivot rows
+      // W_l = U^{-1} V (stored transposed), d_l = U^{-1} c: one column per thread,
+      // column-oriented back substitution held in registers
       double* br = brec0 + (long long)l * brec_stride(N);
-      for (int j = t; j <= N; j += TEAM) {
-        const int colj = (j < N) ? nb + j : RHS;
+      if (t <= N) {
+        const int colj = (t < N) ? nb + t : RHS;
+        double r[N];
+#pragma unroll
+        for (int c = 0; c < N; ++c) r[c] = P[pivslot[c] * LDP + colj];
+#pragma unroll
         for (int c = N - 1; c >= 0; --c) {
-          const int ps = pivslot[c];
-          double s = P[ps * LDP + colj];
-          for (int c2 = c + 1; c2 < N; ++c2) s -= P[ps * LDP + cb + c2] * P[pivslot[c2] * LDP + colj];
-          s = s / P[ps * LDP + cb + c];
-          P[ps * LDP + colj] = s;
-          if (j < N) br[j * N + c] = s;
-          else br[N * N + c] = s;
+          const double x = r[c] / P[pivslot[c] * LDP + cb + c];
+          r[c] = x;
+#pragma unroll
+          for (int c2 = 0; c2 < c; ++c2) r[c2] -= P[pivslot[c2] * LDP + cb + c] * x;
         }
+        double* dst = (t < N) ? br + t * N : br + N * N;
+#pragma unroll
+        for (int c = 0; c < N; ++c) dst[c] = r[c];
       }
       team_sync<TEAM>();
     } else {
       // x_{ncut-1} = U^{-1} rhs (sgbsl back substitution)
       double* x = X + (l & 1) * N;
       if (t == 0) {
+        int ps[N];
+        double r[N];
+#pragma unroll
+        for (int c = 0; c < N; ++c) ps[c] = pivslot[c];
+#pragma unroll
+        for (int c = 0; c < N; ++c) r[c] = P[ps[c] * LDP + RHS];
+#pragma unroll
         for (int c = N - 1; c >= 0; --c) {
-          const int ps = pivslot[c];
-          double s = P[ps * LDP + RHS];
-          for (int c2 = c + 1; c2 < N; ++c2) s -= P[ps * LDP + cb + c2] * x[c2];
-          x[c] = s / P[ps * LDP + cb + c];
+          const double xv = r[c] / P[ps[c] * LDP + cb + c];
+          r[c] = xv;
+#pragma unroll
+          for (int c2 = 0; c2 < c; ++c2) r[c2] -= P[ps[c2] * LDP + cb + c] * xv;
         }
+#pragma unroll
+        for (int c = 0; c < N; ++c) x[c] = r[c];
       }
       team_sync<TEAM>();
     }
+    DSP_PHASE(12)
   }
   if (singular && t == 0) set_status(p.status, i, DSP_ERR_SINGULAR);
 
@@ -345,6 +412,7 @@ __global__ void __launch_bounds__(BCfg<N>::CTA) flux_bvp_kernel(FluxParams p) {
       }
       team_sync<TEAM>();
     }
+    DSP_PHASE(13)
     const double* lr = LR(l);
     const double* eig = lr + lrec_eig(N);
     const double* Gl = lr + lrec_G(N);
@@ -404,6 +472,7 @@ __global__ void __launch_bounds__(BCfg<N>::CTA) flux_bvp_kernel(FluxParams p) {
       }
       team_sync<TEAM>();
     }
+    DSP_PHASE(14)
   }
   if (nonfinite && t == 0) set_status(p.status, i, DSP_ERR_NONFINITE);
 }

@@ -12,6 +12,12 @@
 // the reference's.  When -B_s is not SPD (the reference's general-eigensolver
 // branch, omega' >= 1-1e-12), -A_s = L'L'^T and S' = L'^T(-B_s)L' give the same
 // eigenpairs of (a+b)(a-b) with u = D^{-1} L' w.
+//
+// Shared-memory layout per team: the phase matrix is kept as its unique half
+// cc_top (NN x N; C = [[P, Q], [Q, P]] with P = cc_top[:, :NN], Q = cc_top[:, NN:]),
+// NN x NN matrices use a padded row stride NS = NN + 1 (conflict-free columns),
+// and the N x N LU matrix of the particular solutions overlays the eigen work
+// area once the eigenvectors have been written out.
 #pragma once
 
 #include "dsp_device.cuh"
@@ -26,26 +32,21 @@ struct LCfg {
   static constexpr int TPC = CTA / TEAM;
   static constexpr int NNP = NN + (NN & 1);
   static constexpr int NPAIR = NNP / 2;
-  static constexpr int LDA = N + 1;  // padded row stride of N x N matrices
+  static constexpr int NS = NN + 1;  // padded row stride of NN x NN matrices
+  static constexpr int MAT = NN * NS;
   // team shared-memory layout (doubles)
-  static constexpr int O_C = 0;                    // C[N][LDA]
-  static constexpr int O_A = O_C + N * LDA;        // A[N][LDA] (LU work)
-  static constexpr int O_GL = O_A + N * LDA;       // gl[N]
-  static constexpr int O_AMB = O_GL + N;           // NN x NN blocks
-  static constexpr int O_APB = O_AMB + NN * NN;
-  static constexpr int O_S0 = O_APB + NN * NN;
-  static constexpr int O_S1 = O_S0 + NN * NN;
-  static constexpr int O_V = O_S1 + NN * NN;
-  static constexpr int O_LC = O_V + NN * NN;
-  static constexpr int O_EV = O_LC + NN * NN;      // eigenvectors of (a+b)(a-b)
-  static constexpr int O_LAM = O_EV + NN * NN;     // NN
-  static constexpr int O_ROT = O_LAM + NN;         // c, s, t per pair: 3*NPAIR
-  static constexpr int O_B = O_ROT + 3 * NPAIR;    // b[N]
-  static constexpr int O_Z = O_B + N;              // z[N]
-  static constexpr int O_MISC = O_Z + N;           // 8 slots: flags, reduction scratch
-  static constexpr int O_PIV = O_MISC + 8;         // N ints (as N doubles)
-  static constexpr int TEAM_SMEM = round4(O_PIV + N);
-  // CTA-level tables: mu[N] wt[N] dsim[NN] dinv[NN] ylm[N*N]
+  static constexpr int O_CC = 0;                     // cc_top[NN][N]
+  static constexpr int O_GL = O_CC + NN * N;         // gl[N]
+  static constexpr int O_W = O_GL + N;               // work area
+  static constexpr int W_SIZE = 7 * MAT;
+  static constexpr int O_LAM = O_W + W_SIZE;         // NN: k = sqrt|lambda|
+  static constexpr int O_LAMR = O_LAM + NN;          // NN: lambda
+  static constexpr int O_ROT = O_LAMR + NN;          // c, s, t per pair
+  static constexpr int O_B = O_ROT + 3 * NPAIR;      // b[N]
+  static constexpr int O_Z = O_B + N;                // z[N]
+  static constexpr int O_MISC = O_Z + N;             // flags, reduction scratch
+  static constexpr int O_PIV = O_MISC + 8;           // N ints
+  static constexpr int TEAM_SMEM = round4(O_PIV + N / 2 + 1);
   static constexpr int TAB = tab_size(N);
   static constexpr size_t smem_bytes() { return sizeof(double) * (size_t)(TAB + TPC * TEAM_SMEM); }
 };
@@ -57,107 +58,166 @@ __device__ __forceinline__ int rr_player(int r, int j) {
   return j == 0 ? 0 : 1 + (j - 1 + r) % (NNP - 1);
 }
 
-// Partial-pivot LU of A (n x n, row stride LDA) in shared memory, the stand-in
-// for Eigen::PartialPivLU (FluxSolver.cpp:634, :758).  Returns false on a zero pivot.
-template <int N, int TEAM>
-__device__ bool team_lu(double* A, int* piv, double* red, int t) {
-  constexpr int LDA = N + 1;
-  bool ok = true;
-  for (int k = 0; k < N; ++k) {
-    double v = -1.0;
-    int idx = N;
-    for (int r = t; r < N; r += TEAM)
-      if (r >= k) {
-        double a = fabs(A[r * LDA + k]);
-        if (isnan(a)) a = __longlong_as_double(0x7ff0000000000000ll);  // NaN ranks as +inf: one total order
-        if (a > v || (a == v && r < idx)) { v = a; idx = r; }
-      }
-    team_argmax<TEAM>(v, idx, red);
-    if (idx >= N) idx = k;
-    if (t == 0) piv[k] = idx;
-    if (idx != k)
-      for (int j = t; j < N; j += TEAM) {
-        const double tmp = A[k * LDA + j];
-        A[k * LDA + j] = A[idx * LDA + j];
-        A[idx * LDA + j] = tmp;
-      }
-    team_sync<TEAM>();
-    const double akk = A[k * LDA + k];
-    if (akk == 0.0) { ok = false; continue; }
-    for (int r = t; r < N; r += TEAM)
-      if (r > k) {
-        const double l = A[r * LDA + k] / akk;
-        A[r * LDA + k] = l;
-        for (int j = k + 1; j < N; ++j) A[r * LDA + j] -= l * A[k * LDA + j];
-      }
-    team_sync<TEAM>();
-  }
-  return ok;
-}
-
-// Solve with the factors of team_lu; b in shared memory, overwritten by x.
-template <int N, int TEAM>
-__device__ void team_lu_solve(const double* A, const int* piv, double* b, int t) {
-  constexpr int LDA = N + 1;
-  if (t == 0)
-    for (int k = 0; k < N; ++k)
-      if (piv[k] != k) {
-        const double tmp = b[k];
-        b[k] = b[piv[k]];
-        b[piv[k]] = tmp;
-      }
-  team_sync<TEAM>();
-  for (int k = 0; k < N - 1; ++k) {
-    const double bk = b[k];
-    for (int r = t; r < N; r += TEAM)
-      if (r > k) b[r] -= A[r * LDA + k] * bk;
-    team_sync<TEAM>();
-  }
-  for (int k = N - 1; k >= 0; --k) {
-    if (t == 0) b[k] = b[k] / A[k * LDA + k];
-    team_sync<TEAM>();
-    const double bk = b[k];
-    for (int r = t; r < N; r += TEAM)
-      if (r < k) b[r] -= A[r * LDA + k] * bk;
-    team_sync<TEAM>();
-  }
-}
-
-// Cholesky of the lower triangle of M (NN x NN) into Lc; false if not SPD.
-// `flag` is team scratch; every thread leaves through a team barrier, so the
-// caller may reuse it immediately.
-template <int NN, int TEAM>
+// Cholesky of the lower triangle of M (NN x NN, stride NS) into Lc; false if
+// not SPD.  `flag` is team scratch; every thread leaves through a team
+// barrier, so the caller may reuse it immediately.
+template <int NN, int NS, int TEAM>
 __device__ bool team_cholesky(const double* M, double* Lc, double* flag, int t) {
-  for (int i = t; i < NN * NN; i += TEAM) Lc[i] = 0.0;
+  for (int i = t; i < NN * NS; i += TEAM) Lc[i] = 0.0;
   if (t == 0) flag[0] = 0.0;
   team_sync<TEAM>();
   for (int j = 0; j < NN; ++j) {
     if (t == 0) {
-      double d = M[j * NN + j];
-      for (int k = 0; k < j; ++k) d -= Lc[j * NN + k] * Lc[j * NN + k];
+      double d = M[j * NS + j];
+      for (int k = 0; k < j; ++k) d -= Lc[j * NS + k] * Lc[j * NS + k];
       if (!(d > 0.0)) flag[0] = 1.0;
-      else Lc[j * NN + j] = sqrt(d);
+      else Lc[j * NS + j] = sqrt(d);
     }
     team_sync<TEAM>();
     const bool failed = flag[0] != 0.0;
     team_sync<TEAM>();
     if (failed) return false;
-    const double ljj = Lc[j * NN + j];
+    const double ljj = Lc[j * NS + j];
     for (int i = t; i < NN; i += TEAM)
       if (i > j) {
-        double s = M[i * NN + j];
-        for (int k = 0; k < j; ++k) s -= Lc[i * NN + k] * Lc[j * NN + k];
-        Lc[i * NN + j] = s / ljj;
+        double s = M[i * NS + j];
+        for (int k = 0; k < j; ++k) s -= Lc[i * NS + k] * Lc[j * NS + k];
+        Lc[i * NS + j] = s / ljj;
       }
     team_sync<TEAM>();
   }
   return true;
 }
 
+
+
+// Right-looking Cholesky with row i held by thread i (sub-warp teams): column
+// j's entries are broadcast by shuffles, no barriers.  Same contract as
+// team_cholesky.
+template <int NN, int NS, int TEAM>
+__device__ bool team_cholesky_reg(const double* M, double* Lc, int t) {
+  static_assert(TEAM <= 32, "shuffle Cholesky needs a sub-warp team");
+  const unsigned msk = team_mask<TEAM>();
+  double row[NN];
+#pragma unroll
+  for (int k = 0; k < NN; ++k) row[k] = (t < NN && k <= t) ? M[t * NS + k] : 0.0;
+  bool ok = true;
+#pragma unroll
+  for (int j = 0; j < NN; ++j) {
+    const double djj = __shfl_sync(msk, row[j], j, TEAM);
+    if (!(djj > 0.0)) ok = false;
+    const double ljj = ok ? sqrt(djj) : 1.0;
+    const double lij = (t == j) ? ljj : ((t > j && t < NN) ? row[j] / ljj : 0.0);
+    if (t < NN) Lc[t * NS + j] = (t >= j) ? lij : 0.0;
+#pragma unroll
+    for (int k = j + 1; k < NN; ++k) {
+      const double lkj = __shfl_sync(msk, lij, k, TEAM);
+      if (t >= k && t < NN) row[k] -= lij * lkj;
+    }
+  }
+  if (t < NN)
+    for (int k = t + 1; k < NN; ++k) Lc[t * NS + k] = 0.0;
+  team_sync<TEAM>();
+  return ok;
+}
+
+template <int NN, int NS, int TEAM>
+__device__ __forceinline__ bool team_chol(const double* M, double* Lc, double* flag, int t) {
+  if constexpr (TEAM <= 32) return team_cholesky_reg<NN, NS, TEAM>(M, Lc, t);
+  else return team_cholesky<NN, NS, TEAM>(M, Lc, flag, t);
+}
+
+// Jacobi rotation (Golub & Van Loan, Alg. 8.4.1) annihilating S[p][q]; tt = 0
+// when |apq| is negligible.  Small angles skip the square roots.
+__device__ __forceinline__ void jacobi_rot(double apq, double app, double aqq, double& c, double& s,
+                                           double& tt) {
+  c = 1.0;
+  s = 0.0;
+  tt = 0.0;
+  if (fabs(apq) > 1e-300 && apq * apq > 1.0e-34 * fabs(app * aqq)) {
+    const double th = (aqq - app) / (2.0 * apq);
+    if (fabs(th) > 1e8) {
+      tt = 0.5 / th;
+      c = 1.0 - 0.5 * tt * tt;
+    } else {
+      tt = (th >= 0.0 ? 1.0 : -1.0) / (fabs(th) + sqrt(th * th + 1.0));
+      c = rsqrt(tt * tt + 1.0);
+    }
+    s = tt * c;
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Length-NN vectors distributed one element per team thread (thread t < NN
+// holds element t).  Sub-warp teams broadcast with shuffles; larger teams go
+// through a shared scratch word.  Matrices are NN x NN, row stride NS.
+// ---------------------------------------------------------------------------
+template <int TEAM>
+__device__ __forceinline__ double team_bcast(double v, int k, int t, double* scratch) {
+  if constexpr (TEAM <= 32) {
+    return __shfl_sync(team_mask<TEAM>(), v, k, TEAM);
+  } else {
+    if (t == k) scratch[0] = v;
+    __syncthreads();
+    const double r = scratch[0];
+    __syncthreads();
+    return r;
+  }
+}
+
+// y = A x (trans = false) or A^T x (trans = true); part: 0 full, 1 lower, 2 upper
+template <int NN, int NS, int TEAM>
+__device__ __forceinline__ double team_matvec(const double* A, double x, bool trans, int part, int t,
+                                              double* scratch) {
+  double acc = 0.0;
+  if constexpr (TEAM <= 32) {
+#pragma unroll
+    for (int k = 0; k < NN; ++k) {
+      const double xk = __shfl_sync(team_mask<TEAM>(), x, k, TEAM);
+      if (t < NN) {
+        const int r = trans ? k : t, c = trans ? t : k;  // element A[r][c]
+        const bool in = part == 0 || (part == 1 ? c <= r : c >= r);
+        if (in) acc += A[r * NS + c] * xk;
+      }
+    }
+  } else {
+    if (t < NN) scratch[t] = x;
+    __syncthreads();
+    if (t < NN)
+      for (int k = 0; k < NN; ++k) {
+        const int r = trans ? k : t, c = trans ? t : k;
+        const bool in = part == 0 || (part == 1 ? c <= r : c >= r);
+        if (in) acc += A[r * NS + c] * scratch[k];
+      }
+    __syncthreads();
+  }
+  return acc;
+}
+
+// x <- L^{-1} x (forward) or L^{-T} x (backward), L lower triangular
+template <int NN, int NS, int TEAM>
+__device__ __forceinline__ double team_trsv(const double* Lm, double x, bool transposed, int t,
+                                            double* scratch) {
+  if (!transposed) {
+    for (int k = 0; k < NN; ++k) {
+      if (t == k) x = x / Lm[k * NS + k];
+      const double xk = team_bcast<TEAM>(x, k, t, scratch);
+      if (t > k && t < NN) x -= Lm[t * NS + k] * xk;
+    }
+  } else {
+    for (int k = NN - 1; k >= 0; --k) {
+      if (t == k) x = x / Lm[k * NS + k];
+      const double xk = team_bcast<TEAM>(x, k, t, scratch);
+      if (t < k) x -= Lm[k * NS + t] * xk;
+    }
+  }
+  return x;
+}
+
 template <int N>
 __global__ void __launch_bounds__(LCfg<N>::CTA) flux_layer_kernel(FluxParams p) {
   using C = LCfg<N>;
-  constexpr int NN = C::NN, TEAM = C::TEAM, LDA = C::LDA, NNP = C::NNP, NPAIR = C::NPAIR;
+  constexpr int NN = C::NN, TEAM = C::TEAM, NNP = C::NNP, NPAIR = C::NPAIR, NS = C::NS;
   extern __shared__ double smem[];
   // CTA-level constant tables
   for (int k = threadIdx.x; k < C::TAB; k += blockDim.x) smem[k] = p.tables[k];
@@ -179,23 +239,31 @@ __global__ void __launch_bounds__(LCfg<N>::CTA) flux_layer_kernel(FluxParams p) 
   if (lc >= ncut) return;  // layers below the absorption cut are never used
 
   double* sm = smem + C::TAB + team * C::TEAM_SMEM;
-  double* Cm = sm + C::O_C;
-  double* A = sm + C::O_A;
+  double* CC = sm + C::O_CC;
   double* gl = sm + C::O_GL;
-  double* AMB = sm + C::O_AMB;
-  double* APB = sm + C::O_APB;
-  double* S0 = sm + C::O_S0;
-  double* S1 = sm + C::O_S1;
-  double* V = sm + C::O_V;
-  double* LC = sm + C::O_LC;
-  double* EV = sm + C::O_EV;
+  double* W = sm + C::O_W;
+  double* AMB = W + 0 * C::MAT;
+  double* APB = W + 1 * C::MAT;
+  double* S0 = W + 2 * C::MAT;
+  double* S1 = W + 3 * C::MAT;
+  double* V = W + 4 * C::MAT;
+  double* LC = W + 5 * C::MAT;
+  double* EV = W + 6 * C::MAT;
   double* lam = sm + C::O_LAM;
+  double* lamraw = sm + C::O_LAMR;
   double* rot = sm + C::O_ROT;
   double* bv = sm + C::O_B;
   double* zv = sm + C::O_Z;
   double* misc = sm + C::O_MISC;
   int* piv = reinterpret_cast<int*>(sm + C::O_PIV);
+  // full phase matrix element C(r, j) from its unique half
+  auto Cfull = [&](int r, int j) -> double {
+    const int rr = r < NN ? r : r - NN;
+    const int jj = (r < NN) ? j : (j < NN ? j + NN : j - NN);
+    return CC[rr * N + jj];
+  };
 
+  DSP_PHASE_BEGIN
   const double ws = rec[il.ssa_s + lc];
   const double dts = rec[il.dtau_s + lc];
   // ---- scaled phase coefficients (disortSet, FluxSolver.cpp:336-386) ----
@@ -217,118 +285,144 @@ __global__ void __launch_bounds__(LCfg<N>::CTA) flux_layer_kernel(FluxParams p) 
     }
   }
   team_sync<TEAM>();
-  // ---- phase matrix C (FluxSolver.cpp:466-482) ---------------------------
-  for (int it = t; it < NN * N; it += TEAM) {
-    const int iq = it / N, jq = it % N;
-    double s = 0.0;
-#pragma unroll 8
-    for (int l = 0; l < N; ++l) s += (gl[l] * Y[l * N + iq]) * Y[l * N + jq];
-    const double cc = (s * 0.5) * wt[jq];
-    Cm[iq * LDA + jq] = cc;
-    if (jq < NN) Cm[(NN + iq) * LDA + NN + jq] = cc;
-    else Cm[(NN + iq) * LDA + jq - NN] = cc;
+  DSP_PHASE(0)
+  // ---- phase matrix, unique half (FluxSolver.cpp:466-482) ---------------
+  // thread t owns column jq = t; its Legendre column is held in registers
+  if (t < N) {
+    const int jq = t;
+    double yj[N];
+#pragma unroll
+    for (int l = 0; l < N; ++l) yj[l] = Y[l * N + jq];
+    const double wj = wt[jq];
+    for (int iq = 0; iq < NN; ++iq) {
+      double s = 0.0;
+#pragma unroll
+      for (int l = 0; l < N; ++l) s += (gl[l] * Y[l * N + iq]) * yj[l];
+      CC[iq * N + jq] = (s * 0.5) * wj;
+    }
   }
   team_sync<TEAM>();
+  DSP_PHASE(1)
   // ---- alpha -/+ beta and the similarity transform (:485-514) ------------
   for (int it = t; it < NN * NN; it += TEAM) {
     const int iq = it / NN, jq = it % NN;
     const double inv_cmu = 1.0 / mu[iq];
-    const double a = Cm[iq * LDA + jq], b = Cm[iq * LDA + NN + jq];
+    const double a = CC[iq * N + jq], b = CC[iq * N + NN + jq];
     double amb = inv_cmu * (a - b), apb = inv_cmu * (a + b);
     if (iq == jq) { amb -= inv_cmu; apb -= inv_cmu; }
-    AMB[it] = amb;
-    APB[it] = apb;
-    S0[it] = dsim[iq] * apb * dinv[jq];     // A_s
-    S1[it] = -dsim[iq] * amb * dinv[jq];    // -B_s
+    AMB[iq * NS + jq] = amb;
+    APB[iq * NS + jq] = apb;
+    S0[iq * NS + jq] = dsim[iq] * apb * dinv[jq];     // A_s
+    S1[iq * NS + jq] = -dsim[iq] * amb * dinv[jq];    // -B_s
   }
   team_sync<TEAM>();
   // ---- Cholesky of -B_s, else of -A_s (:521-558) -------------------------
   bool primary = ws < 1.0 - 1e-12;
-  if (primary) {
-    primary = team_cholesky<NN, TEAM>(S1, LC, misc, t);
-  }
+  if (primary) primary = team_chol<NN, NS, TEAM>(S1, LC, misc, t);
   if (!primary) {
-    // V <- -A_s (temporary), factor it
-    for (int it = t; it < NN * NN; it += TEAM) V[it] = -S0[it];
+    for (int it = t; it < NN * NN; it += TEAM) {
+      const int r = it / NN, c = it % NN;
+      V[r * NS + c] = -S0[r * NS + c];
+    }
     team_sync<TEAM>();
-    if (!team_cholesky<NN, TEAM>(V, LC, misc, t)) {
+    if (!team_chol<NN, NS, TEAM>(V, LC, misc, t)) {
       // -A_s not SPD either: try the primary factorisation regardless of omega'
-      primary = team_cholesky<NN, TEAM>(S1, LC, misc, t);
+      primary = team_chol<NN, NS, TEAM>(S1, LC, misc, t);
       if (!primary) {
         if (t == 0) set_status(p.status, i, DSP_ERR_EIGEN);
         return;
       }
     }
   }
+  DSP_PHASE(2)
   // S = L^T M L with M = -A_s (primary) or -B_s (fallback); EV used as scratch
   for (int it = t; it < NN * NN; it += TEAM) {
     const int r = it / NN, c = it % NN;
     double s = 0.0;
     if (primary)
-      for (int k = 0; k < NN; ++k) s += -S0[r * NN + k] * LC[k * NN + c];
+      for (int k = 0; k < NN; ++k) s += -S0[r * NS + k] * LC[k * NS + c];
     else
-      for (int k = 0; k < NN; ++k) s += S1[r * NN + k] * LC[k * NN + c];
-    EV[it] = s;
+      for (int k = 0; k < NN; ++k) s += S1[r * NS + k] * LC[k * NS + c];
+    EV[r * NS + c] = s;
   }
   team_sync<TEAM>();
   for (int it = t; it < NN * NN; it += TEAM) {
     const int r = it / NN, c = it % NN;
     double s = 0.0;
-    for (int k = 0; k < NN; ++k) s += LC[k * NN + r] * EV[k * NN + c];
-    S0[it] = s;
-    V[it] = (r == c) ? 1.0 : 0.0;
+    for (int k = 0; k < NN; ++k) s += LC[k * NS + r] * EV[k * NS + c];
+    S0[r * NS + c] = s;
+    V[r * NS + c] = (r == c) ? 1.0 : 0.0;
   }
   team_sync<TEAM>();
-  // ---- cyclic Jacobi on S (symmetrise from the lower triangle first) ------
+  // ---- cyclic Jacobi on S (symmetrised from its lower triangle) -----------
   for (int it = t; it < NN * NN; it += TEAM) {
     const int r = it / NN, c = it % NN;
-    if (c > r) S1[it] = S0[c * NN + r];
-    else S1[it] = S0[it];
+    S1[r * NS + c] = (c > r) ? S0[c * NS + r] : S0[r * NS + c];
   }
   team_sync<TEAM>();
+  DSP_PHASE(3)
   double* Sc = S1;
   double* Sn = S0;
   for (int sweep = 0; sweep < 20; ++sweep) {
     if (t == 0) misc[1] = 0.0;
     team_sync<TEAM>();
     for (int r = 0; r < NNP - 1; ++r) {
-      for (int a = t; a < NPAIR; a += TEAM) {
-        const int pp = rr_player<NNP>(r, a), qq = rr_player<NNP>(r, NNP - 1 - a);
-        double c = 1.0, s = 0.0, tt = 0.0;
-        if (pp < NN && qq < NN) {
-          const double apq = Sc[pp * NN + qq], app = Sc[pp * NN + pp], aqq = Sc[qq * NN + qq];
-          if (fabs(apq) > 1e-300 && fabs(apq) > 1.0e-17 * sqrt(fabs(app * aqq))) {
-            const double th = (aqq - app) / (2.0 * apq);
-            tt = (th >= 0.0 ? 1.0 : -1.0) / (fabs(th) + sqrt(th * th + 1.0));
-            c = 1.0 / sqrt(tt * tt + 1.0);
-            s = tt * c;
-            misc[1] = 1.0;
+      // rotation of pair a computed by thread a, then shared with the team
+      double rc[TEAM <= 32 ? NPAIR : 1], rs[TEAM <= 32 ? NPAIR : 1], rt[TEAM <= 32 ? NPAIR : 1];
+      {
+        double c = 1.0, sn = 0.0, tt = 0.0;
+        if (t < NPAIR) {
+          const int pp = rr_player<NNP>(r, t), qq = rr_player<NNP>(r, NNP - 1 - t);
+          if (pp < NN && qq < NN) {
+            jacobi_rot(Sc[pp * NS + qq], Sc[pp * NS + pp], Sc[qq * NS + qq], c, sn, tt);
+            if (tt != 0.0) misc[1] = 1.0;
           }
         }
-        rot[3 * a] = c;
-        rot[3 * a + 1] = s;
-        rot[3 * a + 2] = tt;
+        if constexpr (TEAM <= 32) {
+#pragma unroll
+          for (int q = 0; q < NPAIR; ++q) {
+            rc[q] = __shfl_sync(team_mask<TEAM>(), c, q, TEAM);
+            rs[q] = __shfl_sync(team_mask<TEAM>(), sn, q, TEAM);
+            rt[q] = __shfl_sync(team_mask<TEAM>(), tt, q, TEAM);
+          }
+        } else {
+          if (t < NPAIR) {
+            rot[3 * t] = c;
+            rot[3 * t + 1] = sn;
+            rot[3 * t + 2] = tt;
+          }
+          team_sync<TEAM>();
+        }
       }
-      team_sync<TEAM>();
+      auto getrot = [&](int q, double& c, double& sn, double& tt) {
+        if constexpr (TEAM <= 32) {
+          c = rc[0]; sn = rs[0]; tt = rt[0];
+#pragma unroll
+          for (int k = 1; k < NPAIR; ++k)
+            if (k == q) { c = rc[k]; sn = rs[k]; tt = rt[k]; }
+        } else {
+          c = rot[3 * q]; sn = rot[3 * q + 1]; tt = rot[3 * q + 2];
+        }
+      };
       for (int blk = t; blk < NPAIR * NPAIR; blk += TEAM) {
         const int a = blk / NPAIR, b = blk % NPAIR;
         const int pa = rr_player<NNP>(r, a), qa = rr_player<NNP>(r, NNP - 1 - a);
         const int pb = rr_player<NNP>(r, b), qb = rr_player<NNP>(r, NNP - 1 - b);
-        const double ca = rot[3 * a], sa = rot[3 * a + 1];
-        const double cb = rot[3 * b], sb = rot[3 * b + 1];
+        double ca, sa, ta, cb, sb, tb;
+        getrot(a, ca, sa, ta);
+        getrot(b, cb, sb, tb);
         const bool va = qa < NN && pa < NN, vb = qb < NN && pb < NN;
         if (a == b) {
           if (va) {
-            const double apq = Sc[pa * NN + qa];
-            const double ta = rot[3 * a + 2];
-            Sn[pa * NN + pa] = Sc[pa * NN + pa] - ta * apq;
-            Sn[qa * NN + qa] = Sc[qa * NN + qa] + ta * apq;
+            const double apq = Sc[pa * NS + qa];
+            Sn[pa * NS + pa] = Sc[pa * NS + pa] - ta * apq;
+            Sn[qa * NS + qa] = Sc[qa * NS + qa] + ta * apq;
             const double off = (ta != 0.0) ? 0.0 : apq;
-            Sn[pa * NN + qa] = off;
-            Sn[qa * NN + pa] = off;
+            Sn[pa * NS + qa] = off;
+            Sn[qa * NS + pa] = off;
           } else {
             const int x = pa < NN ? pa : qa;
-            if (x < NN) Sn[x * NN + x] = Sc[x * NN + x];
+            if (x < NN) Sn[x * NS + x] = Sc[x * NS + x];
           }
         } else {
           // rows of pair a (rotated), columns of pair b (rotated); absent
@@ -340,7 +434,7 @@ __global__ void __launch_bounds__(LCfg<N>::CTA) flux_layer_kernel(FluxParams p) 
 #pragma unroll
             for (int v = 0; v < 2; ++v) {
               const int rr = ri[u], cc = cj[v];
-              X[u][v] = (rr < NN && cc < NN) ? Sc[rr * NN + cc] : 0.0;
+              X[u][v] = (rr < NN && cc < NN) ? Sc[rr * NS + cc] : 0.0;
             }
           double Y2[2][2];
           if (va) {
@@ -369,7 +463,7 @@ __global__ void __launch_bounds__(LCfg<N>::CTA) flux_layer_kernel(FluxParams p) 
 #pragma unroll
             for (int v = 0; v < 2; ++v) {
               const int rr = ri[u], cc = cj[v];
-              if (rr < NN && cc < NN) Sn[rr * NN + cc] = Z2[u][v];
+              if (rr < NN && cc < NN) Sn[rr * NS + cc] = Z2[u][v];
             }
         }
       }
@@ -378,10 +472,11 @@ __global__ void __launch_bounds__(LCfg<N>::CTA) flux_layer_kernel(FluxParams p) 
         const int row = u / NPAIR, b = u % NPAIR;
         const int pb = rr_player<NNP>(r, b), qb = rr_player<NNP>(r, NNP - 1 - b);
         if (pb < NN && qb < NN) {
-          const double cb = rot[3 * b], sb = rot[3 * b + 1];
-          const double vp = V[row * NN + pb], vq = V[row * NN + qb];
-          V[row * NN + pb] = cb * vp - sb * vq;
-          V[row * NN + qb] = sb * vp + cb * vq;
+          double cb, sb, tb;
+          getrot(b, cb, sb, tb);
+          const double vp = V[row * NS + pb], vq = V[row * NS + qb];
+          V[row * NS + pb] = cb * vp - sb * vq;
+          V[row * NS + qb] = sb * vp + cb * vq;
         }
       }
       team_sync<TEAM>();
@@ -393,32 +488,33 @@ __global__ void __launch_bounds__(LCfg<N>::CTA) flux_layer_kernel(FluxParams p) 
     team_sync<TEAM>();
     if (!rotated) break;
   }
+  DSP_PHASE(4)
   // ---- sort ascending; eigenvectors of (a+b)(a-b) ------------------------
   for (int k = t; k < NN; k += TEAM) {
-    const double lk = Sc[k * NN + k];
+    const double lk = Sc[k * NS + k];
     int rank = 0;
     for (int j = 0; j < NN; ++j) {
-      const double lj = Sc[j * NN + j];
+      const double lj = Sc[j * NS + j];
       if (lj < lk || (lj == lk && j < k)) ++rank;
     }
     lam[rank] = lk;
-    for (int row = 0; row < NN; ++row) Sn[row * NN + rank] = V[row * NN + k];
+    for (int row = 0; row < NN; ++row) Sn[row * NS + rank] = V[row * NS + k];
   }
   team_sync<TEAM>();
   // primary: evec = D^{-1} L^{-T} w ; fallback: evec = D^{-1} L' w
   for (int c = t; c < NN; c += TEAM) {
     if (primary) {
       for (int r = NN - 1; r >= 0; --r) {
-        double s = Sn[r * NN + c];
-        for (int k = r + 1; k < NN; ++k) s -= LC[k * NN + r] * EV[k * NN + c];
-        EV[r * NN + c] = s / LC[r * NN + r];
+        double s = Sn[r * NS + c];
+        for (int k = r + 1; k < NN; ++k) s -= LC[k * NS + r] * EV[k * NS + c];
+        EV[r * NS + c] = s / LC[r * NS + r];
       }
-      for (int r = 0; r < NN; ++r) EV[r * NN + c] *= dinv[r];
+      for (int r = 0; r < NN; ++r) EV[r * NS + c] *= dinv[r];
     } else {
       for (int r = NN - 1; r >= 0; --r) {
         double s = 0.0;
-        for (int k = 0; k <= r; ++k) s += LC[r * NN + k] * Sn[k * NN + c];
-        EV[r * NN + c] = dinv[r] * s;
+        for (int k = 0; k <= r; ++k) s += LC[r * NS + k] * Sn[k * NS + c];
+        EV[r * NS + c] = dinv[r] * s;
       }
     }
   }
@@ -427,6 +523,7 @@ __global__ void __launch_bounds__(LCfg<N>::CTA) flux_layer_kernel(FluxParams p) 
   double* lrec = p.layer_rec + ((long long)i * p.L + lc) * lrec_stride(N);
   for (int k = t; k < NN; k += TEAM) {
     const double kr = sqrt(fabs(lam[k]));
+    lamraw[k] = lam[k];
     lam[k] = kr;
     lrec[lrec_eig(N) + k + NN] = kr;
     lrec[lrec_eig(N) + NN - 1 - k] = -kr;
@@ -435,19 +532,65 @@ __global__ void __launch_bounds__(LCfg<N>::CTA) flux_layer_kernel(FluxParams p) 
   for (int it = t; it < NN * NN; it += TEAM) {
     const int iq = it / NN, jq = it % NN;
     double s = 0.0;
-    for (int k = 0; k < NN; ++k) s += AMB[iq * NN + k] * EV[k * NN + jq];
+    for (int k = 0; k < NN; ++k) s += AMB[iq * NS + k] * EV[k * NS + jq];
     const double gpplgm = s / lam[jq];
-    const double gpmigm = EV[iq * NN + jq];
+    const double gpmigm = EV[iq * NS + jq];
     double* G = lrec + lrec_G(N);
     G[(NN + iq) * N + NN + jq] = 0.5 * (gpplgm + gpmigm);
     G[(NN - iq - 1) * N + NN + jq] = 0.5 * (gpplgm - gpmigm);
     G[(NN + iq) * N + NN - jq - 1] = 0.5 * (-gpplgm + gpmigm);
     G[(NN - iq - 1) * N + NN - jq - 1] = 0.5 * (-gpplgm - gpmigm);
   }
+  team_sync<TEAM>();
+  DSP_PHASE(5)
 
-  // ---- beam particular solution (FluxSolver.cpp:595-643) -----------------
+  // ---- particular solutions in the eigen basis ------------------------------
+  // The reference factors the N x N matrices I - C and I + diag(mu)/mu0 - C with
+  // a partial-pivot LU (FluxSolver.cpp:634, :758).  With s = z+ + z-, d = z+ - z-
+  // and M = diag(mu_1..mu_NN) these split into the NN x NN blocks
+  //   I - P - Q = -M (a+b),   I - P + Q = -M (a-b),
+  // whose inverses the eigensystem already provides:
+  //   (a+b)^{-1} = D^{-1} A_s^{-1} D,  (a-b)^{-1} = D^{-1} B_s^{-1} D,
+  //   primary  (-B_s = L L^T, L^T(-A_s)L = W Lam W^T):
+  //     B_s^{-1} = -L^{-T} L^{-1},   A_s^{-1} = -L W Lam^{-1} W^T L^T;
+  //   fallback (-A_s = L L^T, L^T(-B_s)L = W Lam W^T): the two roles swap.
+  // The beam matrix reduces to (a-b)(a+b) - mu0^{-2} = D^{-1}(B_s A_s - mu0^{-2})D,
+  // diagonal in the same basis: B_s A_s = L W Lam W^T L^{-1} (primary) or
+  // L^{-T} W Lam W^T L^T (fallback); its singular points are the reference's
+  // dithering condition |1 - mu0^2 k^2| ~ 0 (FluxSolver.cpp:610-618).
+  double* Wm = Sn;  // sorted eigenvectors of S (columns)
+  double* scratch = zv;
+  const double dt_ = (t < NN) ? dsim[t] : 1.0;
+  const double di_ = (t < NN) ? dinv[t] : 1.0;
+  const double mui = (t < NN) ? mu[t] : 1.0;
+  const double lami = (t < NN) ? lamraw[t] : 1.0;
+  // X1 x = -L^{-T} L^{-1} x ;  X2 x = -L W Lam^{-1} W^T L^T x   (shift: Lam -> Lam - shift)
+  auto applyX1 = [&](double x) {
+    x = team_trsv<NN, NS, TEAM>(LC, x, false, t, scratch);
+    x = team_trsv<NN, NS, TEAM>(LC, x, true, t, scratch);
+    return -x;
+  };
+  auto applyX2 = [&](double x) {
+    x = team_matvec<NN, NS, TEAM>(LC, x, true, 1, t, scratch);   // L^T x
+    x = team_matvec<NN, NS, TEAM>(Wm, x, true, 0, t, scratch);   // W^T
+    x = x / lami;
+    x = team_matvec<NN, NS, TEAM>(Wm, x, false, 0, t, scratch);  // W
+    x = team_matvec<NN, NS, TEAM>(LC, x, false, 1, t, scratch);  // L
+    return -x;
+  };
+  // (a+b)^{-1} y and (a-b)^{-1} y
+  auto inv_apb = [&](double y) {
+    const double x = dt_ * y;
+    return di_ * (primary ? applyX2(x) : applyX1(x));
+  };
+  auto inv_amb = [&](double y) {
+    const double x = dt_ * y;
+    return di_ * (primary ? applyX1(x) : applyX2(x));
+  };
+
   const double fbeam = rec[H_FBEAM];
   if (fbeam > 0.0) {
+    // ---- beam (computeBeamSource, FluxSolver.cpp:595-643) -----------------
     const double umu0 = rec[H_UMU0];
     double beam_mu = umu0;
     const double mu0sq = umu0 * umu0;
@@ -460,50 +603,68 @@ __global__ void __launch_bounds__(LCfg<N>::CTA) flux_layer_kernel(FluxParams p) 
     if (dith) beam_mu = 0.999 * umu0;
     const double* yb = rec + il.yb;
     for (int r = t; r < N; r += TEAM) {
-      for (int j = 0; j < N; ++j) A[r * LDA + j] = -Cm[r * LDA + j];
-      A[r * LDA + r] += 1.0 + mu[r] / beam_mu;
-      double s = 0.0;
-      for (int k = 0; k < N; ++k) s += gl[k] * Y[k * N + r] * yb[k];
-      bv[r] = fbeam * s / (4.0 * 3.14159265358979323846);
+      double sacc = 0.0;
+      for (int k = 0; k < N; ++k) sacc += gl[k] * Y[k * N + r] * yb[k];
+      bv[r] = fbeam * sacc / (4.0 * 3.14159265358979323846);
     }
     team_sync<TEAM>();
-    if (!team_lu<N, TEAM>(A, piv, misc + 2, t) && t == 0) set_status(p.status, i, DSP_ERR_SINGULAR);
-    team_lu_solve<N, TEAM>(A, piv, bv, t);
-    for (int iq = t; iq < NN; iq += TEAM) {
-      lrec[lrec_zb(N) + NN + iq] = bv[iq];
-      lrec[lrec_zb(N) + NN - iq - 1] = bv[iq + NN];
+    const double bp = (t < NN) ? bv[t] : 0.0, bm = (t < NN) ? bv[NN + t] : 0.0;
+    const double m1 = (bp + bm) / mui;  // M^{-1} r1
+    const double m2 = (bp - bm) / mui;  // M^{-1} r2
+    // rhs = mu0^{-1} M^{-1} r2 + (a-b) M^{-1} r1
+    double y = m2 / beam_mu + team_matvec<NN, NS, TEAM>(AMB, m1, false, 0, t, scratch);
+    // s = -(D^{-1} (B_s A_s - mu0^{-2})^{-1} D) y
+    const double shift = 1.0 / (beam_mu * beam_mu);
+    double x = dt_ * y;
+    if (primary) {
+      x = team_trsv<NN, NS, TEAM>(LC, x, false, t, scratch);          // L^{-1}
+      x = team_matvec<NN, NS, TEAM>(Wm, x, true, 0, t, scratch);       // W^T
+      x = x / (lami - shift);
+      x = team_matvec<NN, NS, TEAM>(Wm, x, false, 0, t, scratch);      // W
+      x = team_matvec<NN, NS, TEAM>(LC, x, false, 1, t, scratch);      // L
+    } else {
+      x = team_matvec<NN, NS, TEAM>(LC, x, true, 1, t, scratch);       // L^T
+      x = team_matvec<NN, NS, TEAM>(Wm, x, true, 0, t, scratch);       // W^T
+      x = x / (lami - shift);
+      x = team_matvec<NN, NS, TEAM>(Wm, x, false, 0, t, scratch);      // W
+      x = team_trsv<NN, NS, TEAM>(LC, x, true, t, scratch);            // L^{-T}
+    }
+    const double sv = -di_ * x;
+    // d = mu0 ((a+b) s + M^{-1} r1)
+    const double dv = beam_mu * (team_matvec<NN, NS, TEAM>(APB, sv, false, 0, t, scratch) + m1);
+    if (t < NN) {
+      lrec[lrec_zb(N) + NN + t] = 0.5 * (sv + dv);      // z+ (quadrature index t)
+      lrec[lrec_zb(N) + NN - t - 1] = 0.5 * (sv - dv);  // z- (quadrature index NN+t)
     }
     team_sync<TEAM>();
   }
-  // ---- thermal particular solution (FluxSolver.cpp:745-787) --------------
   if (p.flags & DSP_FLAG_THERMAL) {
+    // ---- thermal (computeIsotropicSource, FluxSolver.cpp:745-787) ---------
+    // Z1 solves (I-C) z = (1-w') xr1 (isotropic: d1 = 0); Z0 solves
+    // (I-C) z = (1-w') xr0 + mu Z1, i.e. r1 = 2(1-w') xr0, r2 = M s1.
     const double taus_top = rec[il.tau_s + lc];
     const double pk0 = rec[il.pkag + lc], pk1 = rec[il.pkag + lc + 1];
     double xr1 = 0.0;
     if (dts > 1e-4) xr1 = (pk1 - pk0) / dts;
     const double xr0 = pk0 - xr1 * taus_top;
-    for (int r = t; r < N; r += TEAM) {
-      for (int j = 0; j < N; ++j) A[r * LDA + j] = -Cm[r * LDA + j];
-      A[r * LDA + r] += 1.0;
-      zv[r] = (1.0 - ws) * xr1;
-    }
-    team_sync<TEAM>();
-    if (!team_lu<N, TEAM>(A, piv, misc + 2, t) && t == 0) set_status(p.status, i, DSP_ERR_SINGULAR);
-    team_lu_solve<N, TEAM>(A, piv, zv, t);
-    for (int r = t; r < N; r += TEAM) bv[r] = (1.0 - ws) * xr0 + mu[r] * zv[r];
-    team_sync<TEAM>();
-    team_lu_solve<N, TEAM>(A, piv, bv, t);
-    for (int iq = t; iq < NN; iq += TEAM) {
-      lrec[lrec_z0(N) + NN + iq] = bv[iq];
-      lrec[lrec_z0(N) + NN - iq - 1] = bv[iq + NN];
-      lrec[lrec_z1(N) + NN + iq] = zv[iq];
-      lrec[lrec_z1(N) + NN - iq - 1] = zv[iq + NN];
+    // omega' = 1: no thermal source; (a+b) is singular there, so skip it (uniform per team)
+    const bool src = (1.0 - ws) != 0.0;
+    const double u = src ? -inv_apb(1.0 / mui) : 0.0;  // -(a+b)^{-1} M^{-1} 1
+    const double s1 = 2.0 * (1.0 - ws) * xr1 * u;
+    const double s0 = 2.0 * (1.0 - ws) * xr0 * u;
+    const double d0 = src ? -inv_amb(s1) : 0.0;        // -(a-b)^{-1} M^{-1} (M s1)
+    if (t < NN) {
+      lrec[lrec_z1(N) + NN + t] = 0.5 * s1;
+      lrec[lrec_z1(N) + NN - t - 1] = 0.5 * s1;
+      lrec[lrec_z0(N) + NN + t] = 0.5 * (s0 + d0);
+      lrec[lrec_z0(N) + NN - t - 1] = 0.5 * (s0 - d0);
     }
     if (t == 0) {
       lrec[lrec_xr(N)] = xr0;
       lrec[lrec_xr(N) + 1] = xr1;
     }
   }
+  DSP_PHASE(7)
 }
 
 }  // namespace dsp
