@@ -16,6 +16,7 @@
 #include "../../include/dsp.h"
 #include "dsp_device.cuh"
 #include "flux_bvp.cuh"
+#include "flux_bvp_reg.cuh"
 #include "flux_layer.cuh"
 #include "flux_setup.cuh"
 
@@ -252,7 +253,13 @@ dsp_status launch_flux_chunk(dsp_context ctx, const FluxParams& p) {
     const long long grid = (tasks + C::TPC - 1) / C::TPC;
     flux_layer_kernel<N><<<(unsigned)grid, C::CTA, sm, s>>>(p);
   }
-  {
+  if constexpr (N <= 16) {
+    using C = RCfg<N>;
+    const size_t sm = C::smem_bytes();
+    const int grid = (p.n + C::TPC - 1) / C::TPC;
+    KernelTimer kt(ctx, "flux_bvp_kernel");
+    flux_bvp_reg_kernel<N><<<grid, C::CTA, sm, s>>>(p);
+  } else {
     using C = BCfg<N>;
     const size_t sm = C::smem_bytes();
     static bool attr = false;

@@ -1,0 +1,408 @@
+// flux_bvp_reg.cuh — boundary-value problem and fluxes for N <= 16 with the
+// elimination panel held in registers (one panel row per thread).
+//
+// Same algorithm as flux_bvp.cuh (the staircase form of the LINPACK band LU,
+// setMatrix/solve0/computeFluxes of FluxSolver.cpp:838-1287), mapped so that
+// the sgbfa row operations are register FMAs:
+//  - slot thread s holds its row as cur[N] (columns of x_l), nxt[N] (columns of
+//    x_{l+1}) and rhs; carried rows move nxt -> cur between layers;
+//  - the pivot of column c is an arg-max of |cur[c]| over candidate slots
+//    (shuffles), only the pivot row is broadcast through shared memory;
+//  - free slots (last layer's pivot rows) receive the new continuity rows in
+//    slot order, each thread finding its row index by a popcount;
+//  - W_l = U^{-1}[V | c] is a column-oriented back substitution across the
+//    pivot-row owners, one row of X broadcast per step.
+#pragma once
+
+#include "dsp_device.cuh"
+
+namespace dsp {
+
+template <int N>
+struct RCfg {
+  static constexpr int NN = N / 2;
+  static constexpr int PR = 3 * NN;
+  static constexpr int TEAM = pow2ceil(PR) < 8 ? 8 : pow2ceil(PR);
+  static constexpr int CTA = TEAM >= 32 ? TEAM : 32;
+  static constexpr int TPC = CTA / TEAM;
+  static constexpr int XS = N + 1;  // row stride of the X matrix (next block + rhs)
+  // team shared memory (doubles)
+  static constexpr int O_BUF = 0;              // pivot row: cur[N] nxt[N] rhs
+  static constexpr int O_X = O_BUF + 2 * N + 1;  // X[N][N+1]
+  static constexpr int O_XV = O_X + N * XS;    // x ping-pong [2][N]
+  static constexpr int O_EC = O_XV + 2 * N;    // [N]
+  static constexpr int O_I = O_EC + N;         // intensities [N]
+  static constexpr int O_E = O_I + N;          // exp(eig*dtau) of layers l, l+1 [2][NN]
+  static constexpr int O_MISC = O_E + 2 * NN;  // 8
+  static constexpr int O_PIV = O_MISC + 8;     // int pivot slot per column [N]
+  static constexpr int TEAM_SMEM = round4(O_PIV + N / 2 + 1);
+  static constexpr int TAB = tab_size(N);
+  static constexpr size_t smem_bytes() { return sizeof(double) * (size_t)(TAB + TPC * TEAM_SMEM); }
+};
+
+template <int N>
+__global__ void __launch_bounds__(RCfg<N>::CTA) flux_bvp_reg_kernel(FluxParams p) {
+  using C = RCfg<N>;
+  constexpr int NN = C::NN, TEAM = C::TEAM, PR = C::PR, XS = C::XS;
+  constexpr double PI = 3.14159265358979323846;
+  static_assert(PR <= 32 && TEAM <= 32, "register panel needs one warp");
+  extern __shared__ double smem[];
+  for (int k = threadIdx.x; k < C::TAB; k += blockDim.x) smem[k] = p.tables[k];
+  __syncthreads();
+  const double* mu = smem + tab_mu(N);
+  const double* wt = smem + tab_wt(N);
+
+  const int team = threadIdx.x / TEAM, t = threadIdx.x % TEAM;
+  const int i = blockIdx.x * C::TPC + team;
+  if (i >= p.n) return;
+  const unsigned msk = team_mask<TEAM>();
+  const int L = p.L;
+  const long long nlev = L + 1;
+  const bool ifb = (p.flags & DSP_FLAG_INDEX_FROM_BOTTOM) != 0;
+  auto oidx = [&](int lev) { return (long long)i * nlev + (ifb ? L - lev : lev); };
+  const int st0 = p.status ? p.status[i] : 0;
+  if (st0 == DSP_ERR_INVALID_INPUT || st0 == DSP_ERR_EIGEN) {
+    const double qnan = __longlong_as_double(0x7ff8000000000000ll);
+    for (int lev = t; lev <= L; lev += TEAM)
+      for (int f = 0; f < 8; ++f) p.out[f][oidx(lev)] = qnan;
+    return;
+  }
+  DSP_PHASE_BEGIN
+  const InstLayout& il = p.il;
+  const double* rec = p.inst_rec + (long long)i * il.stride;
+  const int ncut = (int)rec[H_NCUT];
+  const bool lyrcut = rec[H_LYRCUT] != 0.0;
+  const bool thermal = (p.flags & DSP_FLAG_THERMAL) != 0;
+  const bool dlbc = (p.flags & DSP_FLAG_DIFFUSION_LOWER_BC) != 0;
+  const double fbeam = rec[H_FBEAM], umu0 = rec[H_UMU0], alb = rec[H_ALB];
+  const bool beam = fbeam > 0.0;
+  const double* taus = rec + il.tau_s;
+  const double* btr = rec + il.btr;
+  const double* dtau_s = rec + il.dtau_s;
+  const double* lrec0 = p.layer_rec + (long long)i * L * lrec_stride(N);
+  double* brec0 = p.bvp_rec + (long long)i * L * brec_stride(N);
+  auto LR = [&](int l) { return lrec0 + (long long)l * lrec_stride(N); };
+
+  double* sm = smem + C::TAB + team * C::TEAM_SMEM;
+  double* buf = sm + C::O_BUF;
+  double* X = sm + C::O_X;
+  double* XV = sm + C::O_XV;
+  double* ec = sm + C::O_EC;
+  double* Iv = sm + C::O_I;
+  double* E = sm + C::O_E;
+  int* pivslot = reinterpret_cast<int*>(sm + C::O_PIV);
+
+  double cur[N], nxt[N], rhs = 0.0;
+#pragma unroll
+  for (int k = 0; k < N; ++k) { cur[k] = 0.0; nxt[k] = 0.0; }
+  bool singular = false;
+
+  // ------------------------------------------------------------------ forward
+  if (t < NN) E[t] = exp(LR(0)[lrec_eig(N) + t] * dtau_s[0]);
+  __syncwarp(msk);
+  // top boundary rows in slots 0..NN-1 (setMatrix :890-907, solve0 :978-990)
+  if (t < NN) {
+    const double* l0 = LR(0);
+    const int jq = NN - 1 - t;
+#pragma unroll
+    for (int iq = 0; iq < N; ++iq) {
+      const double g = __ldg(l0 + lrec_G(N) + jq * N + iq);
+      cur[iq] = (iq < NN) ? g * E[iq] : g;
+    }
+    double s = 0.0;
+    if (beam) s -= __ldg(l0 + lrec_zb(N) + jq);
+    if (thermal) s -= __ldg(l0 + lrec_z0(N) + jq);
+    s += rec[H_FISOT] + rec[H_PTOP];
+    rhs = s;
+  }
+  unsigned carried = (1u << NN) - 1u;  // slots holding carried (un-pivoted) rows
+
+  for (int l = 0; l < ncut; ++l) {
+    const bool last = (l == ncut - 1);
+    const double* lr = LR(l);
+    const double* Ecur = E + (l & 1) * NN;
+    double* Enext = E + ((l & 1) ^ 1) * NN;
+    if (!last && t < NN) Enext[t] = exp(LR(l + 1)[lrec_eig(N) + t] * dtau_s[l + 1]);
+    __syncwarp(msk);
+    // new rows into the free slots, in slot order
+    const unsigned freem = ((PR == 32) ? 0xffffffffu : ((1u << PR) - 1u)) & ~carried;
+    const bool isfree = t < PR && ((freem >> t) & 1u);
+    const int rank = __popc(freem & ((1u << t) - 1u));
+    const int nnew = last ? NN : N;
+    const bool fresh = isfree && rank < nnew;
+    if (fresh) {
+      if (!last) {
+        // continuity row jq of interface (l, l+1) (setMatrix :852-887, solve0 :1080-1104)
+        const int jq = rank;
+        const double* ln = LR(l + 1);
+        const double* Gl = lr + lrec_G(N) + jq * N;
+        const double* Gn = ln + lrec_G(N) + jq * N;
+#pragma unroll
+        for (int iq = 0; iq < N; ++iq) {
+          const double g = __ldg(Gl + iq);
+          cur[iq] = (iq < NN) ? g : g * Ecur[N - 1 - iq];
+          const double h = __ldg(Gn + iq);
+          nxt[iq] = (iq < NN) ? -h * Enext[iq] : -h;
+        }
+        const double T = btr[l + 1], tau = taus[l + 1];
+        double sum = 0.0;
+        if (beam) {
+          sum += __ldg(ln + lrec_zb(N) + jq) * T;
+          sum -= __ldg(lr + lrec_zb(N) + jq) * T;
+        }
+        if (thermal) {
+          sum += __ldg(ln + lrec_z0(N) + jq) - __ldg(lr + lrec_z0(N) + jq);
+          sum += (__ldg(ln + lrec_z1(N) + jq) - __ldg(lr + lrec_z1(N) + jq)) * tau;
+        }
+        rhs = sum;
+      } else {
+        // bottom boundary row (setMatrix :909-958, solve0 :993-1076)
+        const int rb = rank, jq = NN + rb;
+        const bool plain = lyrcut || dlbc;
+        const double* Gl = lr + lrec_G(N);
+#pragma unroll
+        for (int iq = 0; iq < N; ++iq) {
+          double base = __ldg(Gl + jq * N + iq);
+          if (!plain) {
+            double refl = 0.0;
+            for (int k = 0; k < NN; ++k) refl += wt[k] * mu[k] * alb * __ldg(Gl + (NN - 1 - k) * N + iq);
+            base = base - 2.0 * refl;
+          }
+          cur[iq] = (iq < NN) ? base : base * Ecur[N - 1 - iq];
+          nxt[iq] = 0.0;
+        }
+        const double T = btr[ncut], tau = taus[ncut];
+        double sum = 0.0;
+        if (dlbc) {
+          if (beam) sum -= __ldg(lr + lrec_zb(N) + NN + rb) * T;
+          if (thermal) {
+            sum -= __ldg(lr + lrec_z0(N) + NN + rb);
+            sum -= __ldg(lr + lrec_z1(N) + NN + rb) * tau;
+          }
+          sum += rec[H_PBOT] + mu[rb] * rec[H_PBOTD];
+        } else {
+          if (!lyrcut) {
+            double refl = 0.0;
+            for (int jj = 0; jj < NN; ++jj) {
+              double ps = 0.0;
+              if (beam) ps += __ldg(lr + lrec_zb(N) + NN - 1 - jj) * T;
+              if (thermal) ps += __ldg(lr + lrec_z0(N) + NN - 1 - jj) + __ldg(lr + lrec_z1(N) + NN - 1 - jj) * tau;
+              refl += wt[jj] * mu[jj] * alb * ps;
+            }
+            sum += 2.0 * refl;
+          }
+          if (beam) {
+            sum -= __ldg(lr + lrec_zb(N) + NN + rb) * T;
+            if (!lyrcut) sum += alb * umu0 * fbeam * T / PI;
+          }
+          if (thermal) {
+            sum -= __ldg(lr + lrec_z0(N) + NN + rb);
+            sum -= __ldg(lr + lrec_z1(N) + NN + rb) * tau;
+          }
+          sum += rec[H_FISOB];
+          if (thermal) sum += (1.0 - alb) * rec[H_PBOT];
+        }
+        rhs = sum;
+      }
+    }
+    unsigned newm = 0u;
+#pragma unroll
+    for (int s = 0; s < PR; ++s) {
+      const int rk = __popc(freem & ((1u << s) - 1u));
+      if (((freem >> s) & 1u) && rk < nnew) newm |= 1u << s;
+    }
+    unsigned cand = carried | newm;
+    DSP_PHASE(20)
+
+    // ---- eliminate the N columns of x_l (sgbfa steps) ----------------------
+    int myc = -1;  // pivot column of this thread's row, if it becomes a pivot row
+#pragma unroll
+    for (int c = 0; c < N; ++c) {
+      double v = -1.0;
+      int idx = PR;
+      if (t < PR && ((cand >> t) & 1u)) {
+        double a = fabs(cur[c]);
+        if (isnan(a)) a = __longlong_as_double(0x7ff0000000000000ll);  // NaN ranks as +inf: one total order
+        v = a;
+        idx = t;
+      }
+      team_argmax<TEAM>(v, idx, nullptr);
+      const int ps = idx < PR ? idx : 0;
+      const double pv = __shfl_sync(msk, cur[c], ps, TEAM);
+      cand &= ~(1u << ps);
+      if (t == ps) myc = c;
+      if (t == 0) pivslot[c] = ps;
+      if (idx >= PR || pv == 0.0) {  // LINPACK skips a zero pivot column (BandSolver.hpp:76-78)
+        singular = true;
+        continue;
+      }
+      const double tinv = -1.0 / pv;
+      if (t == ps) {
+#pragma unroll
+        for (int j = c + 1; j < N; ++j) buf[j] = cur[j];
+        if (!last)
+#pragma unroll
+          for (int j = 0; j < N; ++j) buf[N + j] = nxt[j];
+        buf[2 * N] = rhs;
+      }
+      __syncwarp(msk);
+      if ((cand >> t) & 1u) {
+        const double m = cur[c] * tinv;
+#pragma unroll
+        for (int j = c + 1; j < N; ++j) cur[j] += m * buf[j];
+        if (!last)
+#pragma unroll
+          for (int j = 0; j < N; ++j) nxt[j] += m * buf[N + j];
+        rhs += m * buf[2 * N];
+      }
+      __syncwarp(msk);
+    }
+    DSP_PHASE(21)
+
+    if (!last) {
+      // X = U^{-1} [nxt | rhs]: column-oriented back substitution over the pivot rows
+#pragma unroll
+      for (int c = N - 1; c >= 0; --c) {
+        if (myc == c) {
+          const double rinv = 1.0 / cur[c];
+#pragma unroll
+          for (int j = 0; j < N; ++j) {
+            const double x = nxt[j] * rinv;
+            nxt[j] = x;
+            X[c * XS + j] = x;
+          }
+          const double x = rhs * rinv;
+          rhs = x;
+          X[c * XS + N] = x;
+        }
+        __syncwarp(msk);
+        if (myc >= 0 && myc < c) {
+          const double u = cur[c];
+#pragma unroll
+          for (int j = 0; j < N; ++j) nxt[j] -= u * X[c * XS + j];
+          rhs -= u * X[c * XS + N];
+        }
+      }
+      __syncwarp(msk);
+      // W_l transposed (Wt[n][c]) and d_l, coalesced
+      double* br = brec0 + (long long)l * brec_stride(N);
+      for (int it = t; it < N * N; it += TEAM) {
+        const int n = it / N, c = it % N;
+        br[it] = X[c * XS + n];
+      }
+      for (int c = t; c < N; c += TEAM) br[N * N + c] = X[c * XS + N];
+      // carried rows become the next layer's current block
+#pragma unroll
+      for (int k = 0; k < N; ++k) {
+        cur[k] = nxt[k];
+        nxt[k] = 0.0;
+      }
+      carried = cand;
+      __syncwarp(msk);
+    } else {
+      // x_{ncut-1} = U^{-1} rhs (sgbsl back substitution)
+      double* x = XV + (l & 1) * N;
+#pragma unroll
+      for (int c = N - 1; c >= 0; --c) {
+        if (myc == c) {
+          const double xv = rhs / cur[c];
+          rhs = xv;
+          x[c] = xv;
+        }
+        __syncwarp(msk);
+        if (myc >= 0 && myc < c) rhs -= cur[c] * x[c];
+      }
+      __syncwarp(msk);
+    }
+    DSP_PHASE(22)
+  }
+  if (singular && t == 0) set_status(p.status, i, DSP_ERR_SINGULAR);
+
+  // ----------------------------------------------------------------- backward
+  for (int lev = ncut + 1 + t; lev <= L; lev += TEAM)
+    for (int f = 0; f < 8; ++f) p.out[f][oidx(lev)] = 0.0;
+  bool nonfinite = false;
+  for (int l = ncut - 1; l >= 0; --l) {
+    double* x = XV + (l & 1) * N;
+    if (l < ncut - 1) {
+      const double* xn = XV + ((l & 1) ^ 1) * N;
+      const double* br = brec0 + (long long)l * brec_stride(N);
+      if (t < N) {
+        double s = br[N * N + t];
+#pragma unroll
+        for (int n = 0; n < N; ++n) s -= br[n * N + t] * xn[n];
+        x[t] = s;
+      }
+      __syncwarp(msk);
+    }
+    const double* lr = LR(l);
+    const double* eig = lr + lrec_eig(N);
+    const double* Gl = lr + lrec_G(N);
+    for (int pass = 0; pass < (l == 0 ? 2 : 1); ++pass) {
+      const int lu = (pass == 0) ? l + 1 : 0;
+      const double utaupr = taus[lu];
+      if (t < N) {
+        const double d = (t < NN) ? (utaupr - taus[l + 1]) : (utaupr - taus[l]);
+        ec[t] = x[t] * exp(-eig[t] * d);
+      }
+      __syncwarp(msk);
+      const double fact = beam ? exp(-utaupr / umu0) : 0.0;
+      if (t < N) {
+        double s = 0.0;
+#pragma unroll
+        for (int j = 0; j < N; ++j) s += __ldg(Gl + t * N + j) * ec[j];
+        if (beam) s += __ldg(lr + lrec_zb(N) + t) * fact;
+        if (thermal) s += __ldg(lr + lrec_z0(N) + t) + __ldg(lr + lrec_z1(N) + t) * utaupr;
+        Iv[t] = s;
+      }
+      __syncwarp(msk);
+      if (t == 0) {
+        double dirint = 0.0, fldir = 0.0, fdir = 0.0;
+        if (beam) {
+          dirint = fbeam * fact;
+          fldir = umu0 * fbeam * fact;
+          fdir = umu0 * fbeam * exp(-rec[il.tauc + lu] / umu0);
+        }
+        double iv[N];
+#pragma unroll
+        for (int k = 0; k < N; ++k) iv[k] = Iv[k];
+        double ua = 0.0, uad = 0.0, uau = 0.0, fldn = 0.0, fup = 0.0;
+#pragma unroll
+        for (int iq = 0; iq < NN; ++iq) {
+          const int cw = NN - iq - 1;
+          ua += wt[cw] * iv[iq];
+          uad += wt[cw] * iv[iq];
+          fldn += wt[cw] * iv[iq] * mu[cw];
+        }
+#pragma unroll
+        for (int iq = NN; iq < N; ++iq) {
+          const int cw = iq - NN;
+          ua += wt[cw] * iv[iq];
+          uau += wt[cw] * iv[iq];
+          fup += wt[cw] * iv[iq] * mu[cw];
+        }
+        fup *= 2.0 * PI;
+        fldn *= 2.0 * PI;
+        const double fdn = (fldn + fldir) - fdir;
+        ua = (2.0 * PI * ua + dirint) / (4.0 * PI);
+        const double uaso = dirint / (4.0 * PI);
+        uad = (2.0 * PI * uad) / (4.0 * PI);
+        uau = (2.0 * PI * uau) / (4.0 * PI);
+        double plsorc = 0.0;
+        if (thermal) plsorc = lr[lrec_xr(N)] + lr[lrec_xr(N) + 1] * utaupr;
+        const double dfdt = (1.0 - p.ssa(i, ifb ? L - 1 - l : l)) * 4.0 * PI * (ua - plsorc);
+        const double o[8] = {fdir, fdn, fup, dfdt, ua, uad, uau, uaso};
+#pragma unroll
+        for (int f = 0; f < 8; ++f) {
+          p.out[f][oidx(lu)] = o[f];
+          if (!isfinite(o[f])) nonfinite = true;
+        }
+      }
+      __syncwarp(msk);
+    }
+    DSP_PHASE(23)
+  }
+  if (nonfinite && t == 0) set_status(p.status, i, DSP_ERR_NONFINITE);
+}
+
+}  // namespace dsp

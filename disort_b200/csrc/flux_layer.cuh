@@ -32,6 +32,7 @@ struct LCfg {
   static constexpr int TPC = CTA / TEAM;
   static constexpr int NNP = NN + (NN & 1);
   static constexpr int NPAIR = NNP / 2;
+  static constexpr int BPT = (NPAIR * NPAIR + TEAM - 1) / TEAM;  // Jacobi 2x2 blocks per thread
   static constexpr int NS = NN + 1;  // padded row stride of NN x NN matrices
   static constexpr int MAT = NN * NS;
   // team shared-memory layout (doubles)
@@ -55,7 +56,9 @@ struct LCfg {
 // arr[0] = 0, arr[j] = 1 + (j - 1 + r) mod (NNP - 1).
 template <int NNP>
 __device__ __forceinline__ int rr_player(int r, int j) {
-  return j == 0 ? 0 : 1 + (j - 1 + r) % (NNP - 1);
+  int x = j - 1 + r;  // < 2 (NNP - 1) for r < NNP - 1: one conditional subtract replaces the modulo
+  if (x >= NNP - 1) x -= NNP - 1;
+  return j == 0 ? 0 : 1 + x;
 }
 
 // Cholesky of the lower triangle of M (NN x NN, stride NS) into Lc; false if
@@ -217,7 +220,8 @@ __device__ __forceinline__ double team_trsv(const double* Lm, double x, bool tra
 template <int N>
 __global__ void __launch_bounds__(LCfg<N>::CTA) flux_layer_kernel(FluxParams p) {
   using C = LCfg<N>;
-  constexpr int NN = C::NN, TEAM = C::TEAM, NNP = C::NNP, NPAIR = C::NPAIR, NS = C::NS;
+  constexpr int NN = C::NN, TEAM = C::TEAM, NNP = C::NNP, NPAIR = C::NPAIR, NS = C::NS, BPT = C::BPT;
+  constexpr int BPA = NPAIR;  // blocks (a, b) per column pair b
   extern __shared__ double smem[];
   // CTA-level constant tables
   for (int k = threadIdx.x; k < C::TAB; k += blockDim.x) smem[k] = p.tables[k];
@@ -367,50 +371,44 @@ __global__ void __launch_bounds__(LCfg<N>::CTA) flux_layer_kernel(FluxParams p) 
     if (t == 0) misc[1] = 0.0;
     team_sync<TEAM>();
     for (int r = 0; r < NNP - 1; ++r) {
-      // rotation of pair a computed by thread a, then shared with the team
-      double rc[TEAM <= 32 ? NPAIR : 1], rs[TEAM <= 32 ? NPAIR : 1], rt[TEAM <= 32 ? NPAIR : 1];
-      {
-        double c = 1.0, sn = 0.0, tt = 0.0;
-        if (t < NPAIR) {
-          const int pp = rr_player<NNP>(r, t), qq = rr_player<NNP>(r, NNP - 1 - t);
-          if (pp < NN && qq < NN) {
-            jacobi_rot(Sc[pp * NS + qq], Sc[pp * NS + pp], Sc[qq * NS + qq], c, sn, tt);
-            if (tt != 0.0) misc[1] = 1.0;
-          }
-        }
-        if constexpr (TEAM <= 32) {
-#pragma unroll
-          for (int q = 0; q < NPAIR; ++q) {
-            rc[q] = __shfl_sync(team_mask<TEAM>(), c, q, TEAM);
-            rs[q] = __shfl_sync(team_mask<TEAM>(), sn, q, TEAM);
-            rt[q] = __shfl_sync(team_mask<TEAM>(), tt, q, TEAM);
-          }
-        } else {
-          if (t < NPAIR) {
-            rot[3 * t] = c;
-            rot[3 * t + 1] = sn;
-            rot[3 * t + 2] = tt;
-          }
-          team_sync<TEAM>();
+      // rotation of pair a is computed by thread a; each thread then needs the
+      // rotations of its block's two pairs only (blocks are assigned statically)
+      double c = 1.0, sn = 0.0, tt = 0.0;
+      if (t < NPAIR) {
+        const int pp = rr_player<NNP>(r, t), qq = rr_player<NNP>(r, NNP - 1 - t);
+        if (pp < NN && qq < NN) {
+          jacobi_rot(Sc[pp * NS + qq], Sc[pp * NS + pp], Sc[qq * NS + qq], c, sn, tt);
+          if (tt != 0.0) misc[1] = 1.0;
         }
       }
-      auto getrot = [&](int q, double& c, double& sn, double& tt) {
-        if constexpr (TEAM <= 32) {
-          c = rc[0]; sn = rs[0]; tt = rt[0];
-#pragma unroll
-          for (int k = 1; k < NPAIR; ++k)
-            if (k == q) { c = rc[k]; sn = rs[k]; tt = rt[k]; }
-        } else {
-          c = rot[3 * q]; sn = rot[3 * q + 1]; tt = rot[3 * q + 2];
+      if constexpr (TEAM > 32) {
+        if (t < NPAIR) {
+          rot[3 * t] = c;
+          rot[3 * t + 1] = sn;
+          rot[3 * t + 2] = tt;
         }
-      };
-      for (int blk = t; blk < NPAIR * NPAIR; blk += TEAM) {
-        const int a = blk / NPAIR, b = blk % NPAIR;
+        team_sync<TEAM>();
+      }
+#pragma unroll
+      for (int k = 0; k < BPT; ++k) {
+        const int blk = t + k * TEAM;
+        const bool act = blk < NPAIR * NPAIR;
+        const int a = act ? blk / NPAIR : 0, b = act ? blk % NPAIR : 0;  // NPAIR is a power of two or small
+        double ca, sa, ta, cb, sb;
+        if constexpr (TEAM <= 32) {
+          const unsigned m = team_mask<TEAM>();
+          ca = __shfl_sync(m, c, a, TEAM);
+          sa = __shfl_sync(m, sn, a, TEAM);
+          ta = __shfl_sync(m, tt, a, TEAM);
+          cb = __shfl_sync(m, c, b, TEAM);
+          sb = __shfl_sync(m, sn, b, TEAM);
+        } else {
+          ca = rot[3 * a]; sa = rot[3 * a + 1]; ta = rot[3 * a + 2];
+          cb = rot[3 * b]; sb = rot[3 * b + 1];
+        }
+        if (!act) continue;
         const int pa = rr_player<NNP>(r, a), qa = rr_player<NNP>(r, NNP - 1 - a);
         const int pb = rr_player<NNP>(r, b), qb = rr_player<NNP>(r, NNP - 1 - b);
-        double ca, sa, ta, cb, sb, tb;
-        getrot(a, ca, sa, ta);
-        getrot(b, cb, sb, tb);
         const bool va = qa < NN && pa < NN, vb = qb < NN && pb < NN;
         if (a == b) {
           if (va) {
@@ -466,17 +464,16 @@ __global__ void __launch_bounds__(LCfg<N>::CTA) flux_layer_kernel(FluxParams p) 
               if (rr < NN && cc < NN) Sn[rr * NS + cc] = Z2[u][v];
             }
         }
-      }
-      // eigenvectors V <- V J
-      for (int u = t; u < NN * NPAIR; u += TEAM) {
-        const int row = u / NPAIR, b = u % NPAIR;
-        const int pb = rr_player<NNP>(r, b), qb = rr_player<NNP>(r, NNP - 1 - b);
-        if (pb < NN && qb < NN) {
-          double cb, sb, tb;
-          getrot(b, cb, sb, tb);
-          const double vp = V[row * NS + pb], vq = V[row * NS + qb];
-          V[row * NS + pb] = cb * vp - sb * vq;
-          V[row * NS + qb] = sb * vp + cb * vq;
+        // eigenvectors V <- V J for pair b: this thread's share of the rows
+        if (vb) {
+          const int rows_per = (NN + BPA - 1) / BPA;  // blocks sharing pair b split its rows
+          const int r0 = a * rows_per;
+#pragma unroll 4
+          for (int row = r0; row < r0 + rows_per && row < NN; ++row) {
+            const double vp = V[row * NS + pb], vq = V[row * NS + qb];
+            V[row * NS + pb] = cb * vp - sb * vq;
+            V[row * NS + qb] = sb * vp + cb * vq;
+          }
         }
       }
       team_sync<TEAM>();
