@@ -46,7 +46,7 @@ def build_libdsp(force: bool = False) -> str:
     if force or _stale(target, _deps(".cu", ".cuh", ".h")):
         _run([NVCC, *ARCH, "-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC", "-shared",
               "-diag-suppress", "177",
-              "-o", target, os.path.join(CSRC, "dsp_capi.cu")])
+              "-o", target, os.path.join(CSRC, "dsp_capi.cu"), os.path.join(CSRC, "dsp_noalloc.cu")])
     return target
 
 

@@ -195,6 +195,10 @@ def load_library(path: str | None = None):
                                            POINTER(c_double), POINTER(c_int64)]
     lib.dsp_flux_bands_solve.restype = c_int32
     lib.dsp_flux_bands_solve.argtypes = [c_void_p, POINTER(FluxBatch), POINTER(FluxOut)]
+    lib.dsp_noalloc_scratch_bytes.restype = c_int64
+    lib.dsp_noalloc_scratch_bytes.argtypes = []
+    lib.dsp_flux_bands_solve_noalloc.restype = c_int32
+    lib.dsp_flux_bands_solve_noalloc.argtypes = [POINTER(FluxBatch), POINTER(FluxOut), c_void_p]
     if path is None:
         _LIB = lib
     return lib

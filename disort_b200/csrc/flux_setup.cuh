@@ -12,7 +12,7 @@ namespace dsp {
 // planckFunction / planckFunction2 (Planck.cpp:35-169).  NaN where the reference throws.
 __device__ __forceinline__ double planck_kernel(double v) { return v * v * v / (exp(v) - 1.0); }
 
-__device__ double planck2(double lo, double hi, double T, const PlanckConsts& pk) {
+static __device__ double planck2(double lo, double hi, double T, const PlanckConsts& pk) {
   constexpr double C2 = 1.438786, A1 = 1.0 / 3.0, A2 = -1.0 / 8.0, A3 = 1.0 / 60.0,
                    A4 = -1.0 / 5040.0, A5 = 1.0 / 272160.0, A6 = -1.0 / 13305600.0, VCUT = 1.5;
   if (T < 0.0 || hi < lo || lo < 0.0) return __longlong_as_double(0x7ff8000000000000ll);
@@ -69,7 +69,7 @@ __device__ double planck2(double lo, double hi, double T, const PlanckConsts& pk
 }
 
 // Four instances per 128-thread CTA, one warp each.
-__global__ void __launch_bounds__(128) flux_setup_kernel(FluxParams p) {
+static __global__ void __launch_bounds__(128) flux_setup_kernel(FluxParams p) {
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int i = blockIdx.x * 4 + warp;
   if (i >= p.n) return;

@@ -141,6 +141,26 @@ dsp_status dsp_context_timing_get(dsp_context ctx, int32_t idx, const char** nam
 dsp_status dsp_flux_bands_solve(dsp_context ctx, const dsp_flux_batch* batch,
                                 const dsp_flux_out* out);
 
+/*
+ * Flux solve without any allocation (no counterpart in the reference: DisORT++
+ * solves on the CPU and allocates freely).  For callers that must not let a
+ * library allocate device memory -- applications that hand the GPU to their own
+ * pooled allocator, or that forbid allocation after start-up.  It runs the same
+ * kernels as dsp_flux_bands_solve with a workspace compiled into libdsp.so: a
+ * 32 MiB device array (dsp_noalloc_scratch_bytes()) that each GPU loading the
+ * library keeps until exit.  Needs no context; all batch and output pointers
+ * must be device memory (DSP_FLAG_DEVICE_POINTERS).  Work is queued on `stream`
+ * (a cudaStream_t, NULL = legacy default) and not waited for.  An instance whose
+ * workspace exceeds the array is rejected with DSP_ERR_NO_MEMORY before anything
+ * runs; larger batches reuse the array in several launches.  All calls share the
+ * array and it keeps the last call's contents: calls that may overlap on the GPU
+ * race and must be serialised by the caller.  The first call on a device looks
+ * up the array's address and sets kernel attributes; make it before any stream
+ * capture.
+ */
+int64_t dsp_noalloc_scratch_bytes(void);
+dsp_status dsp_flux_bands_solve_noalloc(const dsp_flux_batch* batch, const dsp_flux_out* out, void* stream);
+
 #ifdef __cplusplus
 }
 #endif
