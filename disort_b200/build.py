@@ -59,9 +59,34 @@ def build_bench(force: bool = False) -> str:
     return target
 
 
+CXX = "/usr/bin/g++" if os.path.exists("/usr/bin/g++") else "g++"
+
+
+def build_host(force: bool = False) -> str:
+    """libdisortpp.so (the DisORT++ C++ API over the C ABI) and the _disortpp module."""
+    host = os.path.join(CSRC, "host")
+    inc = os.path.join(REPO, "include")
+    lib = os.path.join(LIB, "libdisortpp.so")
+    deps = [os.path.join(host, "disortpp_flux.cpp"), os.path.join(host, "phase_tables.inc"),
+            os.path.join(inc, "disortpp", "disortpp.hpp"), os.path.join(inc, "dsp.h"), os.path.join(LIB, "libdsp.so")]
+    if force or _stale(lib, deps):
+        _run([CXX, "-std=c++17", "-O2", "-fPIC", "-shared", "-Wall", "-o", lib, deps[0],
+              "-L" + LIB, "-ldsp", "-Wl,-rpath,$ORIGIN"])
+    import pybind11
+    ext = sysconfig.get_config_var("EXT_SUFFIX")
+    mod = os.path.join(HERE, "_disortpp" + ext)
+    src = os.path.join(host, "pybind_module.cpp")
+    if force or _stale(mod, [src, lib, os.path.join(inc, "disortpp", "disortpp.hpp")]):
+        _run([CXX, "-std=c++17", "-O2", "-fPIC", "-shared", "-fvisibility=hidden",
+              "-I" + pybind11.get_include(), "-I" + sysconfig.get_paths()["include"],
+              "-o", mod, src, "-L" + LIB, "-ldisortpp", "-ldsp", "-Wl,-rpath,$ORIGIN/lib"])
+    return mod
+
+
 def build_all(force: bool = False) -> None:
     build_libdsp(force)
     build_bench(force)
+    build_host(force)
 
 
 if __name__ == "__main__":

@@ -1,0 +1,279 @@
+// pybind_module.cpp — the `disortpp` Python API served by the B200 engine.
+//
+// Mirrors the reference module (src/python_bindings.cpp:213-763): the same
+// class, property, function and keyword names, the same immutable-tuple
+// getters for vector fields (RO_VEC1D/RO_VEC2D, :21-44), the GIL released around
+// solves.  Added: solve_flux_spectral_bands_arrays, which takes numpy arrays and
+// returns numpy arrays [n_bands, num_layers+1] without per-band objects.
+#include <pybind11/numpy.h>
+#include <pybind11/pybind11.h>
+#include <pybind11/stl.h>
+
+#include "../../../include/disortpp/disortpp.hpp"
+
+namespace py = pybind11;
+using namespace disortpp;
+
+#define RO_VEC1D(cls, field)                                                   \
+  def_property(                                                                \
+      #field, [](const cls& c) { return py::tuple(py::cast(c.field)); },       \
+      [](cls& c, const std::vector<double>& v) { c.field = v; })
+
+#define RO_VEC2D(cls, field)                                                    \
+  def_property(                                                                 \
+      #field,                                                                   \
+      [](const cls& c) {                                                        \
+        py::list outer;                                                         \
+        for (const auto& row : c.field) outer.append(py::tuple(py::cast(row))); \
+        return py::tuple(outer);                                                \
+      },                                                                        \
+      [](cls& c, const std::vector<std::vector<double>>& v) { c.field = v; })
+
+namespace {
+
+template <int N>
+void bind_flux_solver(py::module_& m, const char* name, const char* doc) {
+  py::class_<DisortFluxSolver<N>>(m, name, doc)
+      .def(py::init<>())
+      .def(
+          "solve",
+          [](DisortFluxSolver<N>& self, const DisortFluxConfig& config) {
+            py::gil_scoped_release release;
+            return self.solve(config);
+          },
+          py::arg("config"));
+}
+
+SpectralOverrides make_overrides(std::vector<std::vector<double>> delta_tau,
+                                 std::vector<std::vector<double>> single_scat_albedo,
+                                 std::vector<std::vector<std::vector<double>>> phase_function_moments,
+                                 std::vector<double> surface_albedo, std::vector<double> emissivity_top,
+                                 std::vector<double> direct_beam_flux, std::vector<double> isotropic_flux_top,
+                                 std::vector<double> isotropic_flux_bottom) {
+  return SpectralOverrides{std::move(delta_tau),        std::move(single_scat_albedo),
+                           std::move(phase_function_moments), std::move(surface_albedo),
+                           std::move(emissivity_top),   std::move(direct_beam_flux),
+                           std::move(isotropic_flux_top), std::move(isotropic_flux_bottom)};
+}
+
+// numpy array (or None) -> nested vectors, shape-checked
+std::vector<std::vector<double>> rows2(const py::object& o, size_t n) {
+  std::vector<std::vector<double>> out;
+  if (o.is_none()) return out;
+  auto a = py::array_t<double, py::array::c_style | py::array::forcecast>::ensure(o);
+  if (!a || a.ndim() != 2 || (size_t)a.shape(0) != n) throw std::invalid_argument("expected an array [n_bands, num_layers]");
+  out.resize(n);
+  const double* p = a.data();
+  for (size_t i = 0; i < n; ++i) out[i].assign(p + i * a.shape(1), p + (i + 1) * a.shape(1));
+  return out;
+}
+
+std::vector<std::vector<std::vector<double>>> rows3(const py::object& o, size_t n) {
+  std::vector<std::vector<std::vector<double>>> out;
+  if (o.is_none()) return out;
+  auto a = py::array_t<double, py::array::c_style | py::array::forcecast>::ensure(o);
+  if (!a || a.ndim() != 3 || (size_t)a.shape(0) != n)
+    throw std::invalid_argument("expected an array [n_bands, num_layers, nmom+1]");
+  out.resize(n);
+  const double* p = a.data();
+  const size_t L = a.shape(1), K = a.shape(2);
+  for (size_t i = 0; i < n; ++i) {
+    out[i].resize(L);
+    for (size_t l = 0; l < L; ++l) out[i][l].assign(p + (i * L + l) * K, p + (i * L + l + 1) * K);
+  }
+  return out;
+}
+
+std::vector<double> vec1(const py::object& o) {
+  if (o.is_none()) return {};
+  auto a = py::array_t<double, py::array::c_style | py::array::forcecast>::ensure(o);
+  if (!a) throw std::invalid_argument("expected a 1-D array");
+  return std::vector<double>(a.data(), a.data() + a.size());
+}
+
+}  // namespace
+
+PYBIND11_MODULE(_disortpp, m) {
+  m.doc() = "DisORT++ API on the B200-native DISORT engine (FP64, sm_100a)";
+  m.attr("__version__") = "1.0";
+
+  py::enum_<PhaseFunction>(m, "PhaseFunction")
+      .value("Isotropic", PhaseFunction::Isotropic)
+      .value("Rayleigh", PhaseFunction::Rayleigh)
+      .value("HenyeyGreenstein", PhaseFunction::HenyeyGreenstein)
+      .value("HazeGarciaSiewert", PhaseFunction::HazeGarciaSiewert)
+      .value("CloudGarciaSiewert", PhaseFunction::CloudGarciaSiewert);
+
+  py::class_<DisortFluxConfig>(m, "DisortFluxConfig")
+      .def(py::init<>())
+      .def(py::init<int, int, int>(), py::arg("num_layers"), py::arg("num_streams"),
+           py::arg("num_phase_func_moments") = 0)
+      .def_readwrite("num_layers", &DisortFluxConfig::num_layers)
+      .def_readwrite("num_streams", &DisortFluxConfig::num_streams)
+      .def_readwrite("num_phase_func_moments", &DisortFluxConfig::num_phase_func_moments)
+      .def_readwrite("use_thermal_emission", &DisortFluxConfig::use_thermal_emission)
+      .def_readwrite("use_spherical_beam", &DisortFluxConfig::use_spherical_beam)
+      .def_readwrite("use_delta_m_plus", &DisortFluxConfig::use_delta_m_plus)
+      .def_readwrite("use_diffusion_lower_bc", &DisortFluxConfig::use_diffusion_lower_bc)
+      .def_readwrite("index_from_bottom", &DisortFluxConfig::index_from_bottom)
+      .def_readwrite("compute_temperature_jacobian", &DisortFluxConfig::compute_temperature_jacobian)
+      .def_readwrite("direct_beam_flux", &DisortFluxConfig::direct_beam_flux)
+      .def_readwrite("direct_beam_mu", &DisortFluxConfig::direct_beam_mu)
+      .def_readwrite("isotropic_flux_top", &DisortFluxConfig::isotropic_flux_top)
+      .def_readwrite("isotropic_flux_bottom", &DisortFluxConfig::isotropic_flux_bottom)
+      .def_readwrite("temperature_top", &DisortFluxConfig::temperature_top)
+      .def_readwrite("temperature_bottom", &DisortFluxConfig::temperature_bottom)
+      .def_readwrite("emissivity_top", &DisortFluxConfig::emissivity_top)
+      .def_readwrite("surface_albedo", &DisortFluxConfig::surface_albedo)
+      .def_readwrite("wavenumber_low", &DisortFluxConfig::wavenumber_low)
+      .def_readwrite("wavenumber_high", &DisortFluxConfig::wavenumber_high)
+      .def_readwrite("bottom_radius", &DisortFluxConfig::bottom_radius)
+      .RO_VEC1D(DisortFluxConfig, delta_tau)
+      .RO_VEC1D(DisortFluxConfig, single_scat_albedo)
+      .RO_VEC2D(DisortFluxConfig, phase_function_moments)
+      .RO_VEC1D(DisortFluxConfig, temperature)
+      .RO_VEC1D(DisortFluxConfig, level_altitudes)
+      .def("nmom_nstr", &DisortFluxConfig::nmomNstr)
+      .def("allocate", &DisortFluxConfig::allocate)
+      .def("validate", &DisortFluxConfig::validate)
+      .def("set_henyey_greenstein", &DisortFluxConfig::setHenyeyGreenstein, py::arg("g"), py::arg("lc") = -1)
+      .def("set_isotropic", &DisortFluxConfig::setIsotropic, py::arg("lc") = -1)
+      .def("set_rayleigh", &DisortFluxConfig::setRayleigh, py::arg("lc") = -1)
+      .def("set_haze_garcia_siewert", &DisortFluxConfig::setHazeGarciaSiewert, py::arg("lc") = -1)
+      .def("set_cloud_garcia_siewert", &DisortFluxConfig::setCloudGarciaSiewert, py::arg("lc") = -1)
+      .def("set_phase_function", &DisortFluxConfig::setPhaseFunction, py::arg("type"), py::arg("g") = 0.0,
+           py::arg("lc") = -1);
+
+  py::class_<FluxResult>(m, "FluxResult")
+      .def(py::init<>())
+      .def_readwrite("flux_direct_beam", &FluxResult::flux_direct_beam)
+      .def_readwrite("flux_down", &FluxResult::flux_down)
+      .def_readwrite("flux_up", &FluxResult::flux_up)
+      .def_readwrite("flux_tau_divergence", &FluxResult::flux_tau_divergence)
+      .def_readwrite("mean_intensity", &FluxResult::mean_intensity)
+      .def_readwrite("mean_intensity_down", &FluxResult::mean_intensity_down)
+      .def_readwrite("mean_intensity_up", &FluxResult::mean_intensity_up)
+      .def_readwrite("mean_intensity_direct_beam", &FluxResult::mean_intensity_direct_beam)
+      .def_readwrite("flux_up_temperature_jac", &FluxResult::flux_up_temperature_jac)
+      .def_readwrite("flux_down_temperature_jac", &FluxResult::flux_down_temperature_jac)
+      .def_readwrite("mean_intensity_temperature_jac", &FluxResult::mean_intensity_temperature_jac)
+      .def_readwrite("mean_intensity_down_temperature_jac", &FluxResult::mean_intensity_down_temperature_jac)
+      .def_readwrite("mean_intensity_up_temperature_jac", &FluxResult::mean_intensity_up_temperature_jac)
+      .def_readwrite("flux_divergence_temperature_jac", &FluxResult::flux_divergence_temperature_jac)
+      .def("num_levels", &FluxResult::num_levels)
+      .def("total_flux_down", &FluxResult::totalFluxDown, py::arg("lev"))
+      .def("net_flux", &FluxResult::netFlux, py::arg("lev"));
+
+  bind_flux_solver<4>(m, "DisortFluxSolver4", "Flux-only solver with 4 streams");
+  bind_flux_solver<6>(m, "DisortFluxSolver6", "Flux-only solver with 6 streams");
+  bind_flux_solver<8>(m, "DisortFluxSolver8", "Flux-only solver with 8 streams");
+  bind_flux_solver<10>(m, "DisortFluxSolver10", "Flux-only solver with 10 streams");
+  bind_flux_solver<12>(m, "DisortFluxSolver12", "Flux-only solver with 12 streams");
+  bind_flux_solver<14>(m, "DisortFluxSolver14", "Flux-only solver with 14 streams");
+  bind_flux_solver<16>(m, "DisortFluxSolver16", "Flux-only solver with 16 streams");
+  bind_flux_solver<32>(m, "DisortFluxSolver32", "Flux-only solver with 32 streams");
+  bind_flux_solver<64>(m, "DisortFluxSolver64", "Flux-only solver with 64 streams");
+
+  m.def(
+      "create_flux_solver",
+      [](int nstr) -> py::object {
+        switch (nstr) {
+          case 4: return py::cast(DisortFluxSolver<4>());
+          case 6: return py::cast(DisortFluxSolver<6>());
+          case 8: return py::cast(DisortFluxSolver<8>());
+          case 10: return py::cast(DisortFluxSolver<10>());
+          case 12: return py::cast(DisortFluxSolver<12>());
+          case 14: return py::cast(DisortFluxSolver<14>());
+          case 16: return py::cast(DisortFluxSolver<16>());
+          case 32: return py::cast(DisortFluxSolver<32>());
+          case 64: return py::cast(DisortFluxSolver<64>());
+          default:
+            throw std::invalid_argument("Unsupported nstr=" + std::to_string(nstr) +
+                                        ". Supported values: 4, 6, 8, 10, 12, 14, 16, 32, 64");
+        }
+      },
+      py::arg("nstr"), "Create a flux-only solver for the given number of streams (4, 6, 8, 10, 12, 14, 16, 32, or 64)");
+
+  m.def(
+      "solve_flux_spectral",
+      [](DisortFluxConfig& config, const std::vector<double>& wavenumbers, std::vector<std::vector<double>> delta_tau,
+         std::vector<std::vector<double>> single_scat_albedo,
+         std::vector<std::vector<std::vector<double>>> phase_function_moments, std::vector<double> surface_albedo,
+         std::vector<double> emissivity_top, std::vector<double> direct_beam_flux,
+         std::vector<double> isotropic_flux_top, std::vector<double> isotropic_flux_bottom) {
+        SpectralOverrides ov = make_overrides(std::move(delta_tau), std::move(single_scat_albedo),
+                                              std::move(phase_function_moments), std::move(surface_albedo),
+                                              std::move(emissivity_top), std::move(direct_beam_flux),
+                                              std::move(isotropic_flux_top), std::move(isotropic_flux_bottom));
+        py::gil_scoped_release release;
+        return solveFluxSpectral(config, wavenumbers, ov);
+      },
+      py::arg("config"), py::arg("wavenumbers"), py::arg("delta_tau") = std::vector<std::vector<double>>{},
+      py::arg("single_scat_albedo") = std::vector<std::vector<double>>{},
+      py::arg("phase_function_moments") = std::vector<std::vector<std::vector<double>>>{},
+      py::arg("surface_albedo") = std::vector<double>{}, py::arg("emissivity_top") = std::vector<double>{},
+      py::arg("direct_beam_flux") = std::vector<double>{}, py::arg("isotropic_flux_top") = std::vector<double>{},
+      py::arg("isotropic_flux_bottom") = std::vector<double>{},
+      "Solve for fluxes at a list of single wavenumbers (all bands in one GPU batch). Returns a list of FluxResult.");
+
+  m.def(
+      "solve_flux_spectral_bands",
+      [](DisortFluxConfig& config, const std::vector<std::pair<double, double>>& wavenumber_bands,
+         std::vector<std::vector<double>> delta_tau, std::vector<std::vector<double>> single_scat_albedo,
+         std::vector<std::vector<std::vector<double>>> phase_function_moments, std::vector<double> surface_albedo,
+         std::vector<double> emissivity_top, std::vector<double> direct_beam_flux,
+         std::vector<double> isotropic_flux_top, std::vector<double> isotropic_flux_bottom) {
+        SpectralOverrides ov = make_overrides(std::move(delta_tau), std::move(single_scat_albedo),
+                                              std::move(phase_function_moments), std::move(surface_albedo),
+                                              std::move(emissivity_top), std::move(direct_beam_flux),
+                                              std::move(isotropic_flux_top), std::move(isotropic_flux_bottom));
+        py::gil_scoped_release release;
+        return solveFluxSpectralBands(config, wavenumber_bands, ov);
+      },
+      py::arg("config"), py::arg("wavenumber_bands"), py::arg("delta_tau") = std::vector<std::vector<double>>{},
+      py::arg("single_scat_albedo") = std::vector<std::vector<double>>{},
+      py::arg("phase_function_moments") = std::vector<std::vector<std::vector<double>>>{},
+      py::arg("surface_albedo") = std::vector<double>{}, py::arg("emissivity_top") = std::vector<double>{},
+      py::arg("direct_beam_flux") = std::vector<double>{}, py::arg("isotropic_flux_top") = std::vector<double>{},
+      py::arg("isotropic_flux_bottom") = std::vector<double>{},
+      "Solve for fluxes at a list of wavenumber bands (pairs of (low, high)), all bands in one GPU batch. "
+      "Returns a list of FluxResult.");
+
+  m.def(
+      "solve_flux_spectral_bands_arrays",
+      [](DisortFluxConfig& config, py::object wavenumber_bands, py::object delta_tau, py::object single_scat_albedo,
+         py::object phase_function_moments, py::object surface_albedo, py::object emissivity_top,
+         py::object direct_beam_flux, py::object isotropic_flux_top, py::object isotropic_flux_bottom) {
+        auto wb = py::array_t<double, py::array::c_style | py::array::forcecast>::ensure(wavenumber_bands);
+        if (!wb || wb.ndim() != 2 || wb.shape(1) != 2)
+          throw std::invalid_argument("wavenumber_bands must be an array [n_bands, 2]");
+        const size_t n = wb.shape(0);
+        std::vector<std::pair<double, double>> bands(n);
+        for (size_t i = 0; i < n; ++i) bands[i] = {wb.at(i, 0), wb.at(i, 1)};
+        SpectralOverrides ov{rows2(delta_tau, n),    rows2(single_scat_albedo, n), rows3(phase_function_moments, n),
+                             vec1(surface_albedo),   vec1(emissivity_top),         vec1(direct_beam_flux),
+                             vec1(isotropic_flux_top), vec1(isotropic_flux_bottom)};
+        const size_t nlev = static_cast<size_t>(config.num_layers) + 1;
+        const char* names[8] = {"flux_direct_beam", "flux_down",         "flux_up",           "flux_tau_divergence",
+                                "mean_intensity",   "mean_intensity_down", "mean_intensity_up", "mean_intensity_direct_beam"};
+        std::vector<py::array_t<double>> arrs;
+        double* out8[8];
+        for (int f = 0; f < 8; ++f) {
+          arrs.emplace_back(std::vector<py::ssize_t>{(py::ssize_t)n, (py::ssize_t)nlev});
+          out8[f] = arrs.back().mutable_data();
+        }
+        {
+          py::gil_scoped_release release;
+          solveFluxSpectralBandsInto(config, bands, ov, out8);
+        }
+        py::dict d;
+        for (int f = 0; f < 8; ++f) d[names[f]] = arrs[f];
+        return d;
+      },
+      py::arg("config"), py::arg("wavenumber_bands"), py::arg("delta_tau") = py::none(),
+      py::arg("single_scat_albedo") = py::none(), py::arg("phase_function_moments") = py::none(),
+      py::arg("surface_albedo") = py::none(), py::arg("emissivity_top") = py::none(),
+      py::arg("direct_beam_flux") = py::none(), py::arg("isotropic_flux_top") = py::none(),
+      py::arg("isotropic_flux_bottom") = py::none(),
+      "solve_flux_spectral_bands with numpy arrays in and a dict of numpy arrays [n_bands, num_layers+1] out.");
+}
