@@ -40,13 +40,32 @@ def _deps(*exts: str) -> list[str]:
     return out
 
 
+LIBDSP_SOURCES = ("dsp_capi.cu", "dsp_general.cu", "dsp_noalloc.cu")
+
+
 def build_libdsp(force: bool = False) -> str:
+    """libdsp.so: each translation unit compiled to an object in parallel, then linked."""
     os.makedirs(LIB, exist_ok=True)
     target = os.path.join(LIB, "libdsp.so")
-    if force or _stale(target, _deps(".cu", ".cuh", ".h")):
-        _run([NVCC, *ARCH, "-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC", "-shared",
-              "-diag-suppress", "177",
-              "-o", target, os.path.join(CSRC, "dsp_capi.cu"), os.path.join(CSRC, "dsp_noalloc.cu")])
+    if not (force or _stale(target, _deps(".cu", ".cuh", ".h", ".hpp"))):
+        return target
+    objdir = os.path.join(LIB, "obj")
+    os.makedirs(objdir, exist_ok=True)
+    procs, objs = [], []
+    for src in LIBDSP_SOURCES:
+        obj = os.path.join(objdir, src.replace(".cu", ".o"))
+        objs.append(obj)
+        cmd = [NVCC, *ARCH, "-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC", "-diag-suppress", "177",
+               "-c", "-o", obj, os.path.join(CSRC, src)]
+        procs.append((cmd, subprocess.Popen(cmd, stdout=subprocess.PIPE, stderr=subprocess.STDOUT, text=True)))
+    failed = []
+    for cmd, pr in procs:
+        outp, _ = pr.communicate()
+        if pr.returncode != 0:
+            failed.append(" ".join(cmd) + "\n" + outp)
+    if failed:
+        raise RuntimeError("nvcc failed:\n" + "\n".join(failed))
+    _run([NVCC, *ARCH, "-shared", "-o", target, *objs])
     return target
 
 

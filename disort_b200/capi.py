@@ -41,6 +41,10 @@ FLAG_DEVICE_POINTERS = 1 << 4
 FLAG_SPHERICAL_BEAM = 1 << 5
 FLAG_TEMPERATURE_JAC = 1 << 6
 
+GFLAG_USER_TAU = 1 << 8
+GFLAG_USER_MU = 1 << 9
+GFLAG_ONLY_FLUXES = 1 << 10
+
 SUPPORTED_NSTR = (4, 6, 8, 10, 12, 14, 16, 32, 64)
 
 
@@ -146,6 +150,138 @@ def make_flux_out(arrays: dict, status=None) -> tuple[FluxOut, list]:
     return o, keep
 
 
+GENERAL_SCALAR_FIELDS = (
+    "wavenumber_low", "wavenumber_high", "surface_albedo", "emissivity_top", "direct_beam_flux",
+    "direct_beam_mu", "direct_beam_phi", "isotropic_flux_top", "isotropic_flux_bottom",
+    "temperature_top", "temperature_bottom",
+)
+GENERAL_SCALAR_DEFAULTS = dict(wavenumber_low=0.0, wavenumber_high=0.0, surface_albedo=0.0,
+                               emissivity_top=1.0, direct_beam_flux=0.0, direct_beam_mu=0.5,
+                               direct_beam_phi=0.0, isotropic_flux_top=0.0, isotropic_flux_bottom=0.0,
+                               temperature_top=0.0, temperature_bottom=0.0)
+
+
+class GeneralBatch(ctypes.Structure):
+    _fields_ = [
+        ("n_inst", c_int32), ("flags", c_uint32),
+        ("num_streams", c_void_p), ("num_layers", c_void_p), ("layer_offset", c_void_p),
+        ("num_phase_func_moments", c_void_p), ("pmom_count", c_int32),
+        ("num_user_tau", c_int32), ("num_user_mu", c_int32), ("num_phi", c_int32),
+        ("accuracy_fourier_series", c_double),
+        ("delta_tau", c_void_p), ("single_scat_albedo", c_void_p), ("phase_function_moments", c_void_p),
+        ("temperature", c_void_p),
+        ("tau_user", DArray), ("mu_user", DArray), ("phi_user", DArray),
+    ] + [(f, DArray) for f in GENERAL_SCALAR_FIELDS]
+
+
+class GeneralOut(ctypes.Structure):
+    _fields_ = [("flux", POINTER(c_double) * 8), ("intensity", POINTER(c_double)),
+                ("intensity_azimuth_avg", POINTER(c_double)), ("status", POINTER(c_int32)),
+                ("ntau_out", c_int32), ("numu_out", c_int32)]
+
+
+def _user_list(insts, key, n):
+    """(array, stride): stride 0 when every instance carries the same list."""
+    vals = [np.asarray(c.get(key), dtype=np.float64).reshape(-1) for c in insts]
+    if any(v.size != n for v in vals):
+        raise ValueError(f"{key}: every instance needs {n} values")
+    if all(np.array_equal(v, vals[0]) for v in vals):
+        return np.ascontiguousarray(vals[0]), 0
+    return np.ascontiguousarray(np.stack(vals)), n
+
+
+def pack_general(insts: list, flags: int, accuracy_fourier_series: float = 0.0,
+                 pmom_count: int | None = None) -> dict:
+    """Pack per-instance dicts into host arrays for a dsp_general_batch.
+
+    Each instance dict carries num_streams, num_layers, num_phase_func_moments,
+    delta_tau [L], single_scat_albedo [L], phase_function_moments [L][>= nmomNstr+1],
+    temperature [L+1] (thermal), the scalar fields of GENERAL_SCALAR_FIELDS
+    (defaults as DisortConfig) and, as the flags ask, tau_user, mu_user, phi_user.
+    Returns a dict of numpy arrays and dimensions (see make_general_batch)."""
+    n = len(insts)
+    N = np.array([c["num_streams"] for c in insts], dtype=np.int32)
+    L = np.array([c["num_layers"] for c in insts], dtype=np.int32)
+    nmom = np.array([c.get("num_phase_func_moments", 0) for c in insts], dtype=np.int32)
+    off = np.zeros(n + 1, dtype=np.int64)
+    off[1:] = np.cumsum(L)
+    if pmom_count is None:
+        pmom_count = int(max(len(np.asarray(c["phase_function_moments"])[0]) for c in insts))
+    tot = int(off[-1])
+    dtau = np.zeros(tot)
+    ssa = np.zeros(tot)
+    pm = np.zeros((tot, pmom_count))
+    temp = np.zeros(tot + n)
+    for i, c in enumerate(insts):
+        a, b = off[i], off[i + 1]
+        dtau[a:b] = c["delta_tau"]
+        ssa[a:b] = c["single_scat_albedo"]
+        m = np.asarray(c["phase_function_moments"], dtype=np.float64)
+        pm[a:b, :m.shape[1]] = m[:, :pmom_count]
+        t = c.get("temperature")
+        if t is not None and len(t):
+            temp[a + i:b + i + 1] = t
+    d = dict(n_inst=n, flags=flags, num_streams=N, num_layers=L, layer_offset=off,
+             num_phase_func_moments=nmom, pmom_count=pmom_count, accuracy=float(accuracy_fourier_series),
+             delta_tau=dtau, single_scat_albedo=ssa, phase_function_moments=pm, temperature=temp)
+    for f in GENERAL_SCALAR_FIELDS:
+        d[f] = np.array([float(c.get(f, GENERAL_SCALAR_DEFAULTS[f])) for c in insts])
+    ntau = numu = nphi = 0
+    if flags & GFLAG_USER_TAU:
+        ntau = len(insts[0]["tau_user"])
+        d["tau_user"] = _user_list(insts, "tau_user", ntau)
+    if flags & GFLAG_USER_MU:
+        numu = len(insts[0]["mu_user"])
+        d["mu_user"] = _user_list(insts, "mu_user", numu)
+    if not (flags & GFLAG_ONLY_FLUXES) or insts[0].get("phi_user") is not None:
+        if insts[0].get("phi_user") is not None:
+            nphi = len(insts[0]["phi_user"])
+            d["phi_user"] = _user_list(insts, "phi_user", nphi)
+    d["num_user_tau"], d["num_user_mu"], d["num_phi"] = ntau, numu, nphi
+    d["ntau_out"] = ntau if flags & GFLAG_USER_TAU else int(L.max()) + 1
+    d["numu_out"] = numu if (flags & GFLAG_USER_MU and not flags & GFLAG_ONLY_FLUXES) else int(N.max())
+    return d
+
+
+def make_general_batch(d: dict) -> tuple[GeneralBatch, list]:
+    """dsp_general_batch over the arrays of pack_general (host pointers)."""
+    keep = [d]
+    b = GeneralBatch()
+    b.n_inst = d["n_inst"]
+    b.flags = d["flags"]
+    for f in ("num_streams", "num_layers", "layer_offset", "num_phase_func_moments",
+              "delta_tau", "single_scat_albedo", "phase_function_moments", "temperature"):
+        setattr(b, f, _ptr(d[f]))
+    b.pmom_count = d["pmom_count"]
+    b.num_user_tau, b.num_user_mu, b.num_phi = d["num_user_tau"], d["num_user_mu"], d["num_phi"]
+    b.accuracy_fourier_series = d["accuracy"]
+    for f in ("tau_user", "mu_user", "phi_user"):
+        if f in d:
+            a, stride = d[f]
+            setattr(b, f, DArray(_ptr(a), stride))
+    for f in GENERAL_SCALAR_FIELDS:
+        a = d[f]
+        setattr(b, f, DArray(_ptr(a), 1 if a.shape[0] > 1 else 0))
+    return b, keep
+
+
+def alloc_general_out_numpy(d: dict) -> tuple[dict, GeneralOut, list]:
+    """NaN-filled host outputs for the batch of pack_general and the dsp_general_out over them."""
+    n, nt, nu, nphi = d["n_inst"], d["ntau_out"], d["numu_out"], max(d["num_phi"], 0)
+    outs = {f: np.full((n, nt), np.nan) for f in FLUX_OUT_FIELDS}
+    outs["intensity"] = np.full((n, nt, nu, nphi), np.nan)
+    outs["intensity_azimuth_avg"] = np.full((n, nt, nu), np.nan)
+    outs["status"] = np.full(n, -1, dtype=np.int32)
+    o = GeneralOut()
+    for k, f in enumerate(FLUX_OUT_FIELDS):
+        o.flux[k] = ctypes.cast(c_void_p(_ptr(outs[f])), POINTER(c_double))
+    o.intensity = ctypes.cast(c_void_p(_ptr(outs["intensity"])), POINTER(c_double))
+    o.intensity_azimuth_avg = ctypes.cast(c_void_p(_ptr(outs["intensity_azimuth_avg"])), POINTER(c_double))
+    o.status = ctypes.cast(c_void_p(_ptr(outs["status"])), POINTER(c_int32))
+    o.ntau_out, o.numu_out = nt, nu
+    return outs, o, [outs]
+
+
 def alloc_flux_out_numpy(n_inst: int, num_layers: int) -> tuple[dict, np.ndarray]:
     outs = {f: np.full((n_inst, num_layers + 1), np.nan) for f in FLUX_OUT_FIELDS}
     status = np.full(n_inst, -1, dtype=np.int32)
@@ -195,6 +331,8 @@ def load_library(path: str | None = None):
                                            POINTER(c_double), POINTER(c_int64)]
     lib.dsp_flux_bands_solve.restype = c_int32
     lib.dsp_flux_bands_solve.argtypes = [c_void_p, POINTER(FluxBatch), POINTER(FluxOut)]
+    lib.dsp_general_bands_solve.restype = c_int32
+    lib.dsp_general_bands_solve.argtypes = [c_void_p, POINTER(GeneralBatch), POINTER(GeneralOut)]
     lib.dsp_noalloc_scratch_bytes.restype = c_int64
     lib.dsp_noalloc_scratch_bytes.argtypes = []
     lib.dsp_flux_bands_solve_noalloc.restype = c_int32
@@ -224,6 +362,9 @@ class Context:
 
     def flux_bands_solve(self, batch: FluxBatch, out: FluxOut) -> int:
         return self.lib.dsp_flux_bands_solve(self.h, ctypes.byref(batch), ctypes.byref(out))
+
+    def general_bands_solve(self, batch: GeneralBatch, out: GeneralOut) -> int:
+        return self.lib.dsp_general_bands_solve(self.h, ctypes.byref(batch), ctypes.byref(out))
 
     def set_timing(self, enable: bool):
         self.lib.dsp_context_set_timing(self.h, 1 if enable else 0)

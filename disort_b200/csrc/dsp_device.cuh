@@ -66,9 +66,27 @@ struct InstLayout {
     return o;
   }
 };
-// header slots
+// header slots (the general solver also uses H_NAZ .. H_NT)
 enum { H_NCUT = 0, H_LYRCUT, H_PTOP, H_PBOT, H_PBOTD, H_DELTAM, H_DMPLUS, H_FBEAM, H_UMU0, H_ALB,
-       H_FISOT, H_FISOB, H_NSLOTS };
+       H_FISOT, H_FISOB, H_NAZ, H_KCONV, H_DONE, H_NT, H_NSLOTS };
+static_assert(H_NSLOTS <= 16, "instance header is 16 doubles");
+
+// General-solver instance record: the InstLayout fields for (L, N), then the
+// output optical depths utau[NT], their scaled values utaus[NT] and the layer
+// of each, lyr[NT] (NT = user taus, or L + 1 levels).
+struct GenLayout {
+  InstLayout il;
+  int utau, utaus, lyr, stride;
+  __host__ __device__ static GenLayout make(int L, int N, int NT) {
+    GenLayout g;
+    g.il = InstLayout::make(L, N);
+    g.utau = g.il.stride;
+    g.utaus = g.utau + NT;
+    g.lyr = g.utaus + NT;
+    g.stride = round4(g.lyr + NT);
+    return g;
+  }
+};
 
 // Layer record (doubles) written by the layer kernel:
 // G[N][N] | eig[N] | zb[N] | z0[N] | z1[N] | xr0 | xr1
@@ -81,6 +99,37 @@ __host__ __device__ constexpr int lrec_xr(int N) { return N * N + 4 * N; }
 __host__ __device__ constexpr int lrec_stride(int N) { return round4(N * N + 4 * N + 2); }
 // Elimination record (doubles) written by the BVP kernel: Wt[N][N] (transposed) | d[N]
 __host__ __device__ constexpr int brec_stride(int N) { return round4(N * N + N); }
+
+// General-solver layer record: the flux layer record, then the eigenvectors
+// and sources at the user polar angles of the current mode:
+// GU[numu][N] | zbu[numu] | z0u[numu] | z1u[numu]
+__host__ __device__ constexpr int glrec_gu(int N) { return lrec_stride(N); }
+__host__ __device__ constexpr int glrec_stride(int N, int numu) { return round4(lrec_stride(N) + numu * (N + 3)); }
+
+// Per-launch view of a general (DisortSolver) chunk.  Instances are addressed by
+// chunk slot ci; ids[ci] is the batch index (inputs, outputs, status).
+struct GenView {
+  int m;                       // azimuth mode of this launch
+  int numu;                    // user polar angles (0: no intensities)
+  int numu_in;                 // num_user_mu of the batch (validated when use_user_mu)
+  int nphi, ntau_out, numu_out;
+  int user_tau;                // number of user optical depths (0: the L + 1 levels)
+  double accur;
+  const int* ids;              // [n] batch instance of each slot
+  const long long* inst_off;   // [n] instance record offsets (doubles)
+  const long long* lay_off;    // [n+1] chunk-local first layer of each slot
+  const int* layer_inst;       // [layers] slot of each chunk-local layer
+  const int* Ls;               // batch num_layers
+  const long long* in_off;     // batch layer_offset (CSR)
+  const int* nmoms;            // batch num_phase_func_moments
+  const double *dtau, *ssa, *pmom, *temp;  // CSR inputs
+  DArr utau, umu, phi, phi0;
+  long long lstride;           // layer record stride (glrec_stride)
+  double* cc;                  // [layers][N] boundary-value solution of the mode
+  double* out_flux[8];         // [batch][ntau_out]
+  double* out_int;             // [batch][ntau_out][numu_out][nphi]
+  double* out_iavg;            // [batch][ntau_out][numu_out]
+};
 
 struct FluxParams {
   int n;          // instances in this launch
@@ -95,7 +144,42 @@ struct FluxParams {
   InstLayout il;
   double* out[8];
   int32_t* status;
+  GenView g;  // general-solver launches only
 };
+
+// P_l^m(x) for l = m..lmax into y[l * stride] (rows l < m set to 0), the
+// recurrence of Legendre.cpp:67-120.  For m > 0 the reference seeds P_m^m with
+// the value its previous-mode call left in row m-1; that chain is the product
+// below, evaluated in the same order.
+__device__ __forceinline__ void legendre_column(int m, double x, int lmax, double* y, int stride) {
+  for (int l = 0; l < m && l <= lmax; ++l) y[l * stride] = 0.0;
+  if (m == 0) {
+    y[0] = 1.0;
+    if (lmax >= 1) y[stride] = x;
+    double y2 = 1.0, y1 = x;
+    for (int l = 2; l <= lmax; ++l) {
+      const double v = ((2.0 * l - 1.0) * x * y1 - (l - 1.0) * y2) / l;
+      y[l * stride] = v;
+      y2 = y1;
+      y1 = v;
+    }
+    return;
+  }
+  double pmm = 1.0;
+  for (int k = 1; k <= m; ++k) pmm = -sqrt((1.0 - 1.0 / (2.0 * k)) * (1.0 - x * x)) * pmm;
+  if (m <= lmax) y[m * stride] = pmm;
+  const double pm1 = sqrt(2.0 * m + 1.0) * x * pmm;
+  if (m + 1 <= lmax) y[(m + 1) * stride] = pm1;
+  double y2 = pmm, y1 = pm1;
+  for (int l = m + 2; l <= lmax; ++l) {
+    const double tmp1 = sqrt(static_cast<double>((l - m) * (l + m)));
+    const double tmp2 = sqrt(static_cast<double>((l - m - 1) * (l + m - 1)));
+    const double v = ((2.0 * l - 1.0) * x * y1 - tmp2 * y2) / tmp1;
+    y[l * stride] = v;
+    y2 = y1;
+    y1 = v;
+  }
+}
 
 // Team helpers.  A team is TEAM consecutive threads; TEAM < 32 lives inside a
 // warp (synchronised by __syncwarp on its own lanes), TEAM >= 32 is the whole CTA.

@@ -1,0 +1,562 @@
+// dsp_general.cu — dsp_general_bands_solve: the general solver (DisortSolver::
+// solve, DisortSolver.cpp:21-399) over a ragged batch of instances.
+//
+// Instances are grouped by stream count (one kernel instantiation per N), the
+// groups cut into chunks that fit the workspace, and each chunk runs
+//   gen_setup_kernel, then for every azimuth mode m the layer kernel (eigen-
+//   systems, particular solutions, user-angle interpolation), the boundary-
+//   value kernel (solution coefficients; fluxes at m = 0) and the intensity
+//   kernel (Fourier accumulation and the convergence test).
+// Instances whose series has ended (last mode, or converged) skip the later
+// mode launches on the device.
+#include "dsp_host.hpp"
+#include "flux_bvp.cuh"
+#include "flux_bvp_reg.cuh"
+#include "flux_layer.cuh"
+#include "gen_kernels.cuh"
+
+using namespace dsp;
+using namespace dsp_host;
+
+namespace {
+
+// Per-mode constant tables for N streams: N copies of the tab_* layout whose
+// Legendre block holds P_l^m(mu_i) of mode m (rows l < m zero).  The rows are
+// produced by running the reference's per-mode recurrence in sequence, each
+// mode seeding P_m^m from row m-1 of the previous mode (Legendre.cpp:89-119).
+bool build_mode_tables(int N, std::vector<double>& out) {
+  std::vector<double> base;
+  if (!build_tables(N, base)) return false;
+  const int T = tab_size(N);
+  out.assign((size_t)T * N, 0.0);
+  const double* mu = base.data() + tab_mu(N);
+  std::vector<double> y((size_t)N * N, 0.0);
+  for (int m = 0; m < N; ++m) {
+    for (int i = 0; i < N; ++i) {
+      if (m == 0) {
+        y[0 * N + i] = 1.0;
+        y[1 * N + i] = mu[i];
+        for (int l = 2; l < N; ++l)
+          y[l * N + i] = ((2.0 * l - 1.0) * mu[i] * y[(l - 1) * N + i] - (l - 1.0) * y[(l - 2) * N + i]) / l;
+      } else {
+        y[m * N + i] = -std::sqrt((1.0 - 1.0 / (2.0 * m)) * (1.0 - mu[i] * mu[i])) * y[(m - 1) * N + i];
+        if (m + 1 < N) y[(m + 1) * N + i] = std::sqrt(2.0 * m + 1.0) * mu[i] * y[m * N + i];
+        for (int l = m + 2; l < N; ++l) {
+          const double tmp1 = std::sqrt(static_cast<double>((l - m) * (l + m)));
+          const double tmp2 = std::sqrt(static_cast<double>((l - m - 1) * (l + m - 1)));
+          y[l * N + i] = ((2.0 * l - 1.0) * mu[i] * y[(l - 1) * N + i] - tmp2 * y[(l - 2) * N + i]) / tmp1;
+        }
+      }
+    }
+    double* t = out.data() + (size_t)m * T;
+    std::memcpy(t, base.data(), sizeof(double) * tab_ylm(N));
+    for (int l = m; l < N; ++l)
+      for (int i = 0; i < N; ++i) t[tab_ylm(N) + l * N + i] = y[l * N + i];
+  }
+  return true;
+}
+
+dsp_status get_mode_tables(dsp_context ctx, int N, const double** out) {
+  auto it = ctx->mode_tables.find(N);
+  if (it != ctx->mode_tables.end()) {
+    *out = it->second;
+    return DSP_OK;
+  }
+  std::vector<double> tab;
+  if (!build_mode_tables(N, tab)) return fail(ctx, DSP_ERR_EIGEN, "Gauss quadrature did not converge");
+  double* d = nullptr;
+  cudaError_t e = cudaMalloc(&d, tab.size() * sizeof(double));
+  if (e != cudaSuccess) return cuda_fail(ctx, e, "cudaMalloc(mode tables)");
+  e = cudaMemcpy(d, tab.data(), tab.size() * sizeof(double), cudaMemcpyHostToDevice);
+  if (e != cudaSuccess) return cuda_fail(ctx, e, "cudaMemcpy(mode tables)");
+  ctx->mode_tables[N] = d;
+  *out = d;
+  return DSP_OK;
+}
+
+template <int N>
+dsp_status launch_general_chunk(dsp_context ctx, FluxParams p, long long layers, int maxm, const double* tabs) {
+  cudaStream_t s = ctx->stream;
+  using LC = LCfg<N, true>;
+  static bool attr = false;
+  if (!attr) {
+    cudaFuncSetAttribute(flux_layer_kernel<N, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                         (int)LC::smem_bytes());
+    if constexpr (N > 16)
+      cudaFuncSetAttribute(flux_bvp_kernel<N, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                           (int)BCfg<N>::smem_bytes());
+    attr = true;
+  }
+  p.tables = tabs;
+  {
+    KernelTimer kt(ctx, "gen_setup_kernel");
+    gen_setup_kernel<<<(p.n + 3) / 4, 128, 0, s>>>(p);
+  }
+  const long long lgrid = (layers + LC::TPC - 1) / LC::TPC;
+  for (int m = 0; m <= maxm; ++m) {
+    p.g.m = m;
+    p.tables = tabs + (size_t)m * tab_size(N);
+    if (lgrid > 0) {
+      KernelTimer kt(ctx, "gen_layer_kernel");
+      flux_layer_kernel<N, true><<<(unsigned)lgrid, LC::CTA, LC::smem_bytes(), s>>>(p);
+    }
+    if constexpr (N <= 16) {
+      using C = RCfg<N>;
+      KernelTimer kt(ctx, "gen_bvp_kernel");
+      flux_bvp_reg_kernel<N, true><<<(p.n + C::TPC - 1) / C::TPC, C::CTA, C::smem_bytes(), s>>>(p);
+    } else {
+      using C = BCfg<N>;
+      KernelTimer kt(ctx, "gen_bvp_kernel");
+      flux_bvp_kernel<N, true><<<(p.n + C::TPC - 1) / C::TPC, C::CTA, C::smem_bytes(), s>>>(p);
+    }
+    if (p.g.numu > 0) {
+      KernelTimer kt(ctx, "gen_intensity_kernel");
+      gen_intensity_kernel<N><<<(p.n + 3) / 4, 128, 0, s>>>(p);
+    }
+  }
+  cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess) return cuda_fail(ctx, e, "general kernel launch");
+  return DSP_OK;
+}
+
+dsp_status launch_general(dsp_context ctx, int N, const FluxParams& p, long long layers, int maxm,
+                          const double* tabs) {
+  switch (N) {
+    case 4: return launch_general_chunk<4>(ctx, p, layers, maxm, tabs);
+    case 6: return launch_general_chunk<6>(ctx, p, layers, maxm, tabs);
+    case 8: return launch_general_chunk<8>(ctx, p, layers, maxm, tabs);
+    case 10: return launch_general_chunk<10>(ctx, p, layers, maxm, tabs);
+    case 12: return launch_general_chunk<12>(ctx, p, layers, maxm, tabs);
+    case 14: return launch_general_chunk<14>(ctx, p, layers, maxm, tabs);
+    case 16: return launch_general_chunk<16>(ctx, p, layers, maxm, tabs);
+    case 32: return launch_general_chunk<32>(ctx, p, layers, maxm, tabs);
+    case 64: return launch_general_chunk<64>(ctx, p, layers, maxm, tabs);
+  }
+  return fail(ctx, DSP_ERR_UNSUPPORTED, "unsupported num_streams");
+}
+
+// Highest azimuth mode of an instance, as gen_setup_kernel decides it (host
+// copy, used only to skip mode launches no instance of a chunk needs).
+int host_naz(int N, uint32_t fl, bool do_int, double fbeam, double umu0, int numu_in, const double* um) {
+  if (!do_int) return 0;
+  const bool user_mu = (fl & DSP_GFLAG_USER_MU) != 0, only = (fl & DSP_GFLAG_ONLY_FLUXES) != 0;
+  const int numu = (user_mu && !only) ? numu_in : N;
+  auto at = [&](int k) { return (user_mu && !only && um && k < numu) ? um[k] : 0.0; };
+  const bool indep = (fbeam == 0.0) || (std::fabs(1.0 - umu0) < 1.e-5) || only ||
+                     (numu == 1 && std::fabs(1.0 - at(1)) < 1.e-5) || (numu == 1 && std::fabs(1.0 + at(1)) < 1.e-5) ||
+                     (numu == 2 && std::fabs(1.0 + at(1)) < 1.e-5 && std::fabs(1.0 - at(2)) < 1.e-5);
+  return indep ? 0 : N - 1;
+}
+
+// Instances the kernels do not take (num_streams outside the supported set)
+// get NaN outputs, like every instance that fails validation.
+__global__ void gen_fill_nan_kernel(const int* ids, int count, int ntau, int numu, int nphi, int ntau_out,
+                                    int numu_out, double* const* flux, double* inten, double* iavg) {
+  const int k = blockIdx.x;
+  if (k >= count) return;
+  const long long i = ids[k];
+  const double qnan = __longlong_as_double(0x7ff8000000000000ll);
+  for (int lu = threadIdx.x; lu < ntau; lu += blockDim.x) {
+    for (int f = 0; f < 8; ++f) flux[f][i * ntau_out + lu] = qnan;
+    for (int iu = 0; iu < numu; ++iu) {
+      const long long o2 = (i * ntau_out + lu) * numu_out + iu;
+      if (iavg) iavg[o2] = qnan;
+      if (inten)
+        for (int j = 0; j < nphi; ++j) inten[o2 * nphi + j] = qnan;
+    }
+  }
+}
+
+struct DevFlux {
+  double* f[8];
+};
+
+inline size_t align256(size_t b) { return (b + 255) / 256 * 256; }
+
+}  // namespace
+
+extern "C" dsp_status dsp_general_bands_solve(dsp_context ctx, const dsp_general_batch* bin,
+                                              const dsp_general_out* out) {
+  if (!ctx) return DSP_ERR_NOT_INITIALIZED;
+  if (!bin || !out) return fail(ctx, DSP_ERR_INVALID_INPUT, "null batch or output");
+  const dsp_general_batch& b = *bin;
+  const int n = b.n_inst;
+  if (n < 0) return fail(ctx, DSP_ERR_INVALID_INPUT, "n_inst must be >= 0");
+  if (n == 0) return DSP_OK;
+  const uint32_t fl = b.flags;
+  if (fl & (DSP_FLAG_SPHERICAL_BEAM | DSP_FLAG_TEMPERATURE_JAC))
+    return fail(ctx, DSP_ERR_UNSUPPORTED, "spherical beam and temperature Jacobians are not in this engine");
+  const bool thermal = (fl & DSP_FLAG_THERMAL) != 0;
+  const bool user_tau = (fl & DSP_GFLAG_USER_TAU) != 0, user_mu = (fl & DSP_GFLAG_USER_MU) != 0;
+  const bool only_fluxes = (fl & DSP_GFLAG_ONLY_FLUXES) != 0;
+  const bool do_int = user_mu && !only_fluxes;
+  const bool dev = (fl & DSP_FLAG_DEVICE_POINTERS) != 0;
+  if (!b.num_streams || !b.num_layers || !b.layer_offset || !b.num_phase_func_moments || !b.delta_tau ||
+      !b.single_scat_albedo || !b.phase_function_moments)
+    return fail(ctx, DSP_ERR_INVALID_INPUT, "num_streams, num_layers, layer_offset, num_phase_func_moments, "
+                                            "delta_tau, single_scat_albedo and phase_function_moments are required");
+  if (thermal && !b.temperature) return fail(ctx, DSP_ERR_INVALID_INPUT, "thermal emission needs temperature");
+  if (b.pmom_count < 1) return fail(ctx, DSP_ERR_INVALID_INPUT, "pmom_count must be >= 1");
+  if (user_tau && (b.num_user_tau <= 0 || !b.tau_user.ptr))
+    return fail(ctx, DSP_ERR_INVALID_INPUT, "use_user_tau needs num_user_tau > 0 and tau_user");
+  if (user_mu && (b.num_user_mu <= 0 || !b.mu_user.ptr))
+    return fail(ctx, DSP_ERR_INVALID_INPUT, "num_user_mu must be positive when use_user_mu=true");
+  if (!only_fluxes && (b.num_phi <= 0 || !b.phi_user.ptr))
+    return fail(ctx, DSP_ERR_INVALID_INPUT, "num_phi must be positive when comp_only_fluxes=false");
+  if (b.accuracy_fourier_series < 0.0)
+    return fail(ctx, DSP_ERR_INVALID_INPUT, "accuracy_fourier_series must be non-negative (0 = disabled)");
+  for (int f = 0; f < 8; ++f)
+    if (!out->flux[f]) return fail(ctx, DSP_ERR_INVALID_INPUT, "every flux output array is required");
+  if (do_int && (!out->intensity || !out->intensity_azimuth_avg))
+    return fail(ctx, DSP_ERR_INVALID_INPUT, "intensity outputs are required when use_user_mu=true");
+  cudaError_t e = cudaSetDevice(ctx->device);
+  if (e != cudaSuccess) return cuda_fail(ctx, e, "cudaSetDevice");
+  cudaStream_t s = ctx->stream;
+  dsp_status st;
+
+  // ---- host view of the per-instance metadata -------------------------------
+  std::vector<int32_t> hN(n), hL(n);
+  std::vector<int64_t> hoff(n + 1);
+  if (dev) {
+    e = cudaMemcpyAsync(hN.data(), b.num_streams, n * sizeof(int32_t), cudaMemcpyDeviceToHost, s);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(hL.data(), b.num_layers, n * sizeof(int32_t), cudaMemcpyDeviceToHost, s);
+    if (e == cudaSuccess)
+      e = cudaMemcpyAsync(hoff.data(), b.layer_offset, (n + 1) * sizeof(int64_t), cudaMemcpyDeviceToHost, s);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+    if (e != cudaSuccess) return cuda_fail(ctx, e, "metadata copy");
+  } else {
+    std::memcpy(hN.data(), b.num_streams, n * sizeof(int32_t));
+    std::memcpy(hL.data(), b.num_layers, n * sizeof(int32_t));
+    std::memcpy(hoff.data(), b.layer_offset, (n + 1) * sizeof(int64_t));
+  }
+  int maxN = 4, maxL = 0;
+  for (int i = 0; i < n; ++i) {
+    if (hL[i] > 0 && hoff[i + 1] - hoff[i] != hL[i])
+      return fail(ctx, DSP_ERR_INVALID_INPUT, "layer_offset does not match num_layers");
+    if (hN[i] > maxN && supported_nstr(hN[i])) maxN = hN[i];
+    if (hL[i] > maxL) maxL = hL[i];
+  }
+  const int ntau_need = user_tau ? b.num_user_tau : maxL + 1;
+  const int numu_eff = do_int ? b.num_user_mu : 0;
+  if (out->ntau_out < ntau_need)
+    return fail(ctx, DSP_ERR_INVALID_INPUT, "ntau_out is smaller than the number of output levels");
+  if (do_int && out->numu_out < b.num_user_mu)
+    return fail(ctx, DSP_ERR_INVALID_INPUT, "numu_out is smaller than num_user_mu");
+  const int64_t total_layers = hoff[n];
+  const int nphi = only_fluxes ? (b.num_phi > 0 ? b.num_phi : 0) : b.num_phi;
+  const int64_t ntau_o = out->ntau_out, numu_o = out->numu_out;
+
+  // ---- stage inputs --------------------------------------------------------
+  static const double kDefaults[11] = {0.0, 0.0, 0.0, 1.0, 0.0, 0.5, 0.0, 0.0, 0.0, 0.0, 0.0};
+  const dsp_darray* sc[11] = {&b.wavenumber_low, &b.wavenumber_high, &b.surface_albedo, &b.emissivity_top,
+                              &b.direct_beam_flux, &b.direct_beam_mu, &b.direct_beam_phi, &b.isotropic_flux_top,
+                              &b.isotropic_flux_bottom, &b.temperature_top, &b.temperature_bottom};
+  const dsp_darray* lists[3] = {&b.tau_user, &b.mu_user, &b.phi_user};
+  const int list_n[3] = {user_tau ? b.num_user_tau : 0, user_mu ? b.num_user_mu : 0, nphi};
+  auto darray_elems = [&](const dsp_darray& a, int64_t per) -> size_t {
+    return a.stride == 0 ? (size_t)per : (size_t)((n - 1) * a.stride + per);
+  };
+  const double* d_dtau;
+  const double* d_ssa;
+  const double* d_pmom;
+  const double* d_temp = nullptr;
+  const int32_t* d_L;
+  const int64_t* d_off;
+  const int32_t* d_nmom;
+  dsp_darray dsc[11], dlists[3];
+  {
+    size_t need = 0;
+    if (!dev) {
+      need += align256(n * sizeof(int32_t)) * 2 + align256((n + 1) * sizeof(int64_t));
+      need += align256(total_layers * sizeof(double)) * 2 + align256(total_layers * b.pmom_count * sizeof(double));
+      if (thermal) need += align256((total_layers + n) * sizeof(double));
+      for (int k = 0; k < 3; ++k)
+        if (lists[k]->ptr && list_n[k] > 0) need += align256(darray_elems(*lists[k], list_n[k]) * sizeof(double));
+    }
+    for (int k = 0; k < 11; ++k)
+      need += (!sc[k]->ptr) ? 256 : (dev ? 0 : align256(darray_elems(*sc[k], 1) * sizeof(double)));
+    if ((st = ensure(ctx, &ctx->stage_in, &ctx->stage_in_bytes, need + 256, "input staging")) != DSP_OK) return st;
+    char* cur = static_cast<char*>(ctx->stage_in);
+    auto put = [&](const void* src, size_t bytes) -> const void* {
+      void* dst = cur;
+      if (bytes) e = cudaMemcpyAsync(dst, src, bytes, cudaMemcpyHostToDevice, s);
+      cur += align256(bytes);
+      return dst;
+    };
+    e = cudaSuccess;
+    if (dev) {
+      d_L = b.num_layers;
+      d_off = b.layer_offset;
+      d_nmom = b.num_phase_func_moments;
+      d_dtau = b.delta_tau;
+      d_ssa = b.single_scat_albedo;
+      d_pmom = b.phase_function_moments;
+      d_temp = thermal ? b.temperature : nullptr;
+      for (int k = 0; k < 3; ++k) dlists[k] = *lists[k];
+    } else {
+      d_L = static_cast<const int32_t*>(put(b.num_layers, n * sizeof(int32_t)));
+      d_off = static_cast<const int64_t*>(put(b.layer_offset, (n + 1) * sizeof(int64_t)));
+      d_nmom = static_cast<const int32_t*>(put(b.num_phase_func_moments, n * sizeof(int32_t)));
+      d_dtau = static_cast<const double*>(put(b.delta_tau, total_layers * sizeof(double)));
+      d_ssa = static_cast<const double*>(put(b.single_scat_albedo, total_layers * sizeof(double)));
+      d_pmom = static_cast<const double*>(put(b.phase_function_moments, total_layers * b.pmom_count * sizeof(double)));
+      if (thermal) d_temp = static_cast<const double*>(put(b.temperature, (total_layers + n) * sizeof(double)));
+      for (int k = 0; k < 3; ++k) {
+        dlists[k] = *lists[k];
+        if (lists[k]->ptr && list_n[k] > 0)
+          dlists[k].ptr = static_cast<const double*>(
+              put(lists[k]->ptr, darray_elems(*lists[k], list_n[k]) * sizeof(double)));
+      }
+    }
+    for (int k = 0; k < 11; ++k) {
+      dsc[k] = *sc[k];
+      if (!sc[k]->ptr) {  // absent scalar: the DisortConfig default
+        dsc[k].ptr = static_cast<const double*>(put(&kDefaults[k], sizeof(double)));
+        dsc[k].stride = 0;
+      } else if (!dev) {
+        dsc[k].ptr = static_cast<const double*>(put(sc[k]->ptr, darray_elems(*sc[k], 1) * sizeof(double)));
+      }
+    }
+    if (e != cudaSuccess) return cuda_fail(ctx, e, "cudaMemcpyAsync(input)");
+  }
+
+  // ---- outputs: zeroed, then written by the kernels -----------------------------
+  const size_t flux_elems = (size_t)n * ntau_o;
+  const size_t int_elems = (out->intensity && nphi > 0) ? (size_t)n * ntau_o * numu_o * nphi : 0;
+  const size_t iavg_elems = out->intensity_azimuth_avg ? (size_t)n * ntau_o * numu_o : 0;
+  double* dflux[8];
+  double* dint = nullptr;
+  double* diavg = nullptr;
+  int32_t* dstatus = nullptr;
+  {
+    const size_t need = (dev ? 0 : 8 * align256(flux_elems * 8) + align256(int_elems * 8) + align256(iavg_elems * 8)) +
+                        2 * align256(n * sizeof(int32_t)) + align256(8 * sizeof(double*));
+    if ((st = ensure(ctx, &ctx->stage_out, &ctx->stage_out_bytes, need, "output staging")) != DSP_OK) return st;
+    char* cur = static_cast<char*>(ctx->stage_out);
+    for (int f = 0; f < 8; ++f) {
+      if (dev) dflux[f] = out->flux[f];
+      else {
+        dflux[f] = reinterpret_cast<double*>(cur);
+        cur += align256(flux_elems * 8);
+      }
+    }
+    if (dev) {
+      dint = int_elems ? out->intensity : nullptr;
+      diavg = iavg_elems ? out->intensity_azimuth_avg : nullptr;
+    } else {
+      if (int_elems) dint = reinterpret_cast<double*>(cur);
+      cur += align256(int_elems * 8);
+      if (iavg_elems) diavg = reinterpret_cast<double*>(cur);
+      cur += align256(iavg_elems * 8);
+    }
+    dstatus = (dev && out->status) ? out->status : reinterpret_cast<int32_t*>(cur);
+    cur += align256(n * sizeof(int32_t));
+    double** dfp = reinterpret_cast<double**>(cur);
+    cur += align256(8 * sizeof(double*));
+    int32_t* dskip = reinterpret_cast<int32_t*>(cur);
+    e = cudaMemcpyAsync(dfp, dflux, sizeof(dflux), cudaMemcpyHostToDevice, s);
+    for (int f = 0; f < 8 && e == cudaSuccess; ++f) e = cudaMemsetAsync(dflux[f], 0, flux_elems * 8, s);
+    if (e == cudaSuccess && dint) e = cudaMemsetAsync(dint, 0, int_elems * 8, s);
+    if (e == cudaSuccess && diavg) e = cudaMemsetAsync(diavg, 0, iavg_elems * 8, s);
+    if (e != cudaSuccess) return cuda_fail(ctx, e, "output initialisation");
+
+    // status: 0, or the verdict on instances no kernel takes
+    std::vector<int32_t> hst(n, 0);
+    std::vector<int32_t> skip;
+    for (int i = 0; i < n; ++i) {
+      if (hN[i] < 4 || hN[i] % 2 != 0) hst[i] = DSP_ERR_INVALID_INPUT;
+      else if (!supported_nstr(hN[i])) hst[i] = DSP_ERR_UNSUPPORTED;
+      if (hst[i]) skip.push_back(i);
+    }
+    e = cudaMemcpyAsync(dstatus, hst.data(), n * sizeof(int32_t), cudaMemcpyHostToDevice, s);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(s);  // hst leaves scope
+    if (e != cudaSuccess) return cuda_fail(ctx, e, "status initialisation");
+    if (!skip.empty()) {
+      e = cudaMemcpyAsync(dskip, skip.data(), skip.size() * sizeof(int32_t), cudaMemcpyHostToDevice, s);
+      if (e == cudaSuccess) {
+        gen_fill_nan_kernel<<<(unsigned)skip.size(), 64, 0, s>>>(dskip, (int)skip.size(), (int)ntau_need,
+                                                                  numu_eff, nphi, (int)ntau_o, (int)numu_o, dfp,
+                                                                  dint, diavg);
+        e = cudaGetLastError();
+      }
+      if (e == cudaSuccess) e = cudaStreamSynchronize(s);  // skip leaves scope
+      if (e != cudaSuccess) return cuda_fail(ctx, e, "unsupported-instance fill");
+    }
+  }
+
+  // ---- groups by stream count, chunks by workspace --------------------------------
+  struct Chunk {
+    int N;
+    std::vector<int32_t> ids;
+    std::vector<int64_t> inst_off, lay_off;
+    int64_t inst_doubles = 0, layers = 0;
+    int maxm = 0;
+  };
+  std::vector<Chunk> chunks;
+  size_t budget = workspace_budget();
+  {
+    size_t freeb = 0, totalb = 0;
+    if (cudaMemGetInfo(&freeb, &totalb) == cudaSuccess && freeb / 2 < budget + ctx->ws_bytes)
+      budget = (freeb + ctx->ws_bytes) / 2;
+  }
+  const double* h_fbeam = (!dev && b.direct_beam_flux.ptr) ? b.direct_beam_flux.ptr : nullptr;
+  const double* h_umu0 = (!dev && b.direct_beam_mu.ptr) ? b.direct_beam_mu.ptr : nullptr;
+  const double* h_mu = (!dev && user_mu) ? b.mu_user.ptr : nullptr;
+  for (int N : kSupported) {
+    const int64_t lstride = glrec_stride(N, numu_eff);
+    const int64_t per_layer = lstride + brec_stride(N) + N;
+    Chunk c;
+    c.N = N;
+    size_t bytes = 0;
+    auto flush = [&]() {
+      if (!c.ids.empty()) {
+        c.lay_off.push_back(c.layers);
+        chunks.push_back(std::move(c));
+      }
+      c = Chunk();
+      c.N = N;
+      bytes = 0;
+    };
+    for (int i = 0; i < n; ++i) {
+      if (hN[i] != N) continue;
+      const int L = hL[i] > 0 ? hL[i] : 0;
+      const int NT = user_tau ? b.num_user_tau : L + 1;
+      const int64_t rec = GenLayout::make(L, N, NT).stride;
+      const size_t ib = (size_t)(rec + (int64_t)L * per_layer) * sizeof(double);
+      if (!c.ids.empty() && bytes + ib > budget) flush();
+      c.ids.push_back(i);
+      c.inst_off.push_back(c.inst_doubles);
+      c.lay_off.push_back(c.layers);
+      c.inst_doubles += rec;
+      c.layers += L;
+      bytes += ib;
+      int naz = N - 1;
+      if (!dev)
+        naz = host_naz(N, fl, do_int, h_fbeam ? h_fbeam[b.direct_beam_flux.stride * i] : 0.0,
+                       h_umu0 ? h_umu0[b.direct_beam_mu.stride * i] : 0.5, b.num_user_mu,
+                       h_mu ? h_mu + b.mu_user.stride * i : nullptr);
+      else if (!do_int) naz = 0;
+      if (naz > c.maxm) c.maxm = naz;
+    }
+    flush();
+  }
+  if (chunks.empty()) goto copy_back;
+  {
+    // chunk index arrays, one upload
+    size_t meta_need = 0, ws_need = 0;
+    for (const Chunk& c : chunks) {
+      meta_need += align256(c.ids.size() * 4) + align256(c.ids.size() * 8) + align256((c.ids.size() + 1) * 8) +
+                   align256(c.layers * 4);
+      const int64_t lstride = glrec_stride(c.N, numu_eff);
+      const size_t w = (size_t)(c.inst_doubles + c.layers * (lstride + brec_stride(c.N) + c.N)) * sizeof(double);
+      if (w > ws_need) ws_need = w;
+    }
+    if ((st = ensure(ctx, &ctx->meta, &ctx->meta_bytes, meta_need, "chunk index")) != DSP_OK) return st;
+    if ((st = ensure(ctx, &ctx->ws, &ctx->ws_bytes, ws_need + 1024, "workspace")) != DSP_OK) return st;
+    std::vector<char> hmeta(meta_need);
+    std::vector<size_t> moff(chunks.size());
+    {
+      size_t o = 0;
+      for (size_t k = 0; k < chunks.size(); ++k) {
+        const Chunk& c = chunks[k];
+        moff[k] = o;
+        const size_t nc = c.ids.size();
+        std::memcpy(hmeta.data() + o, c.ids.data(), nc * 4);
+        o += align256(nc * 4);
+        std::memcpy(hmeta.data() + o, c.inst_off.data(), nc * 8);
+        o += align256(nc * 8);
+        std::memcpy(hmeta.data() + o, c.lay_off.data(), (nc + 1) * 8);
+        o += align256((nc + 1) * 8);
+        int32_t* li = reinterpret_cast<int32_t*>(hmeta.data() + o);
+        for (size_t ci = 0; ci < nc; ++ci)
+          for (int64_t l = c.lay_off[ci]; l < c.lay_off[ci + 1]; ++l) li[l] = (int32_t)ci;
+        o += align256(c.layers * 4);
+      }
+    }
+    e = cudaMemcpyAsync(ctx->meta, hmeta.data(), meta_need, cudaMemcpyHostToDevice, s);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(s);  // hmeta leaves scope
+    if (e != cudaSuccess) return cuda_fail(ctx, e, "chunk index upload");
+
+    FluxParams p;
+    std::memset(&p, 0, sizeof(p));
+    p.pc = b.pmom_count;
+    p.flags = fl;
+    p.pk = planck_consts();
+    p.status = dstatus;
+    DArr* pa[11] = {&p.wlo, &p.whi, &p.alb, &p.emis, &p.fbeam, &p.umu0, &p.g.phi0, &p.fisot, &p.fisob, &p.ttop, &p.tbot};
+    for (int k = 0; k < 11; ++k) {
+      pa[k]->p = dsc[k].ptr;
+      pa[k]->s = dsc[k].stride;
+    }
+    GenView& g = p.g;
+    g.numu = numu_eff;
+    g.numu_in = user_mu ? b.num_user_mu : 0;
+    g.nphi = nphi;
+    g.ntau_out = (int)ntau_o;
+    g.numu_out = (int)numu_o;
+    g.user_tau = user_tau ? b.num_user_tau : 0;
+    g.accur = b.accuracy_fourier_series;
+    g.Ls = d_L;
+    g.in_off = reinterpret_cast<const long long*>(d_off);
+    g.nmoms = d_nmom;
+    g.dtau = d_dtau;
+    g.ssa = d_ssa;
+    g.pmom = d_pmom;
+    g.temp = d_temp;
+    g.utau = {dlists[0].ptr, dlists[0].stride};
+    g.umu = {dlists[1].ptr, dlists[1].stride};
+    g.phi = {dlists[2].ptr, dlists[2].stride};
+    for (int f = 0; f < 8; ++f) g.out_flux[f] = dflux[f];
+    g.out_int = dint;
+    g.out_iavg = diavg;
+    for (size_t k = 0; k < chunks.size(); ++k) {
+      const Chunk& c = chunks[k];
+      const size_t nc = c.ids.size();
+      char* mb = static_cast<char*>(ctx->meta) + moff[k];
+      g.ids = reinterpret_cast<const int*>(mb);
+      mb += align256(nc * 4);
+      g.inst_off = reinterpret_cast<const long long*>(mb);
+      mb += align256(nc * 8);
+      g.lay_off = reinterpret_cast<const long long*>(mb);
+      mb += align256((nc + 1) * 8);
+      g.layer_inst = reinterpret_cast<const int*>(mb);
+      g.lstride = glrec_stride(c.N, numu_eff);
+      p.n = (int)nc;
+      p.N = c.N;
+      double* w = static_cast<double*>(ctx->ws);
+      p.inst_rec = w;
+      p.layer_rec = w + c.inst_doubles;
+      p.bvp_rec = p.layer_rec + c.layers * g.lstride;
+      g.cc = p.bvp_rec + c.layers * brec_stride(c.N);
+      const double* tabs = nullptr;
+      if ((st = get_mode_tables(ctx, c.N, &tabs)) != DSP_OK) return st;
+      if ((st = launch_general(ctx, c.N, p, c.layers, c.maxm, tabs)) != DSP_OK) return st;
+    }
+  }
+
+copy_back:
+  if (dev) return DSP_OK;
+  for (int f = 0; f < 8; ++f) {
+    e = cudaMemcpyAsync(out->flux[f], dflux[f], flux_elems * 8, cudaMemcpyDeviceToHost, s);
+    if (e != cudaSuccess) return cuda_fail(ctx, e, "cudaMemcpyAsync(output)");
+  }
+  if (dint) {
+    e = cudaMemcpyAsync(out->intensity, dint, int_elems * 8, cudaMemcpyDeviceToHost, s);
+    if (e != cudaSuccess) return cuda_fail(ctx, e, "cudaMemcpyAsync(intensity)");
+  }
+  if (diavg) {
+    e = cudaMemcpyAsync(out->intensity_azimuth_avg, diavg, iavg_elems * 8, cudaMemcpyDeviceToHost, s);
+    if (e != cudaSuccess) return cuda_fail(ctx, e, "cudaMemcpyAsync(intensity_azimuth_avg)");
+  }
+  std::vector<int32_t> hs_tmp;
+  int32_t* hs = out->status;
+  if (!hs) {
+    hs_tmp.resize(n);
+    hs = hs_tmp.data();
+  }
+  e = cudaMemcpyAsync(hs, dstatus, n * sizeof(int32_t), cudaMemcpyDeviceToHost, s);
+  if (e != cudaSuccess) return cuda_fail(ctx, e, "cudaMemcpyAsync(status)");
+  e = cudaStreamSynchronize(s);
+  if (e != cudaSuccess) return cuda_fail(ctx, e, "general solve");
+  return DSP_OK;
+}

@@ -40,7 +40,7 @@ struct RCfg {
   static constexpr size_t smem_bytes() { return sizeof(double) * (size_t)(TAB + TPC * TEAM_SMEM); }
 };
 
-template <int N>
+template <int N, bool GEN = false>
 __global__ void __launch_bounds__(RCfg<N>::CTA) flux_bvp_reg_kernel(FluxParams p) {
   using C = RCfg<N>;
   constexpr int NN = C::NN, TEAM = C::TEAM, PR = C::PR, XS = C::XS;
@@ -53,35 +53,72 @@ __global__ void __launch_bounds__(RCfg<N>::CTA) flux_bvp_reg_kernel(FluxParams p
   const double* wt = smem + tab_wt(N);
 
   const int team = threadIdx.x / TEAM, t = threadIdx.x % TEAM;
-  const int i = blockIdx.x * C::TPC + team;
-  if (i >= p.n) return;
+  const int slot = blockIdx.x * C::TPC + team;
+  if (slot >= p.n) return;
   const unsigned msk = team_mask<TEAM>();
-  const int L = p.L;
-  const long long nlev = L + 1;
   const bool ifb = (p.flags & DSP_FLAG_INDEX_FROM_BOTTOM) != 0;
-  auto oidx = [&](int lev) { return (long long)i * nlev + (ifb ? L - lev : lev); };
+  // i: status / input / output index, L: layers, NT: output levels
+  int i, L, NT;
+  const double* rec;
+  InstLayout il_gen;  // general solver: the layout of this instance
+  const double* lrec0;
+  double* brec0;
+  double* cc0 = nullptr;
+  long long lstride;
+  if constexpr (GEN) {
+    i = p.g.ids[slot];
+    L = p.g.Ls[i];
+    NT = p.g.user_tau ? p.g.user_tau : L + 1;
+    il_gen = InstLayout::make(L, N);
+    rec = p.inst_rec + p.g.inst_off[slot];
+    lstride = p.g.lstride;
+    lrec0 = p.layer_rec + p.g.lay_off[slot] * lstride;
+    brec0 = p.bvp_rec + p.g.lay_off[slot] * brec_stride(N);
+    cc0 = p.g.cc + p.g.lay_off[slot] * N;
+  } else {
+    i = slot;
+    L = p.L;
+    NT = L + 1;
+    rec = p.inst_rec + (long long)i * p.il.stride;
+    lstride = lrec_stride(N);
+    lrec0 = p.layer_rec + (long long)i * L * lstride;
+    brec0 = p.bvp_rec + (long long)i * L * brec_stride(N);
+  }
+  const InstLayout& il = GEN ? il_gen : p.il;
+  const int m = GEN ? p.g.m : 0;
+  auto oidx = [&](int lev) {
+    if constexpr (GEN) return (long long)i * p.g.ntau_out + (ifb ? NT - 1 - lev : lev);
+    else return (long long)i * NT + (ifb ? L - lev : lev);
+  };
+  double* const* outp = GEN ? p.g.out_flux : p.out;
   const int st0 = p.status ? p.status[i] : 0;
   if (st0 == DSP_ERR_INVALID_INPUT || st0 == DSP_ERR_EIGEN) {
     const double qnan = __longlong_as_double(0x7ff8000000000000ll);
-    for (int lev = t; lev <= L; lev += TEAM)
-      for (int f = 0; f < 8; ++f) p.out[f][oidx(lev)] = qnan;
+    if (m == 0)
+      for (int lev = t; lev < NT; lev += TEAM)
+        for (int f = 0; f < 8; ++f) outp[f][oidx(lev)] = qnan;
     return;
   }
+  if constexpr (GEN) {
+    if (m > (int)rec[H_NAZ] || rec[H_DONE] != 0.0) return;
+  }
   DSP_PHASE_BEGIN
-  const InstLayout& il = p.il;
-  const double* rec = p.inst_rec + (long long)i * il.stride;
   const int ncut = (int)rec[H_NCUT];
   const bool lyrcut = rec[H_LYRCUT] != 0.0;
-  const bool thermal = (p.flags & DSP_FLAG_THERMAL) != 0;
+  // modes m > 0 carry the beam only: no thermal or isotropic sources and no
+  // Lambertian coupling (DisortSolver.cpp:1246-1250, 1693-1748)
+  const bool thermal = (p.flags & DSP_FLAG_THERMAL) != 0 && m == 0;
   const bool dlbc = (p.flags & DSP_FLAG_DIFFUSION_LOWER_BC) != 0;
-  const double fbeam = rec[H_FBEAM], umu0 = rec[H_UMU0], alb = rec[H_ALB];
+  const double fbeam = rec[H_FBEAM], umu0 = rec[H_UMU0];
+  const double alb = m == 0 ? rec[H_ALB] : 0.0;
+  const double fisot = m == 0 ? rec[H_FISOT] : 0.0, ptop = m == 0 ? rec[H_PTOP] : 0.0;
+  const double fisob = m == 0 ? rec[H_FISOB] : 0.0, pbot = m == 0 ? rec[H_PBOT] : 0.0;
+  const double pbotd = m == 0 ? rec[H_PBOTD] : 0.0;
   const bool beam = fbeam > 0.0;
   const double* taus = rec + il.tau_s;
   const double* btr = rec + il.btr;
   const double* dtau_s = rec + il.dtau_s;
-  const double* lrec0 = p.layer_rec + (long long)i * L * lrec_stride(N);
-  double* brec0 = p.bvp_rec + (long long)i * L * brec_stride(N);
-  auto LR = [&](int l) { return lrec0 + (long long)l * lrec_stride(N); };
+  auto LR = [&](int l) { return lrec0 + (long long)l * lstride; };
 
   double* sm = smem + C::TAB + team * C::TEAM_SMEM;
   double* buf = sm + C::O_BUF;
@@ -112,7 +149,7 @@ __global__ void __launch_bounds__(RCfg<N>::CTA) flux_bvp_reg_kernel(FluxParams p
     double s = 0.0;
     if (beam) s -= __ldg(l0 + lrec_zb(N) + jq);
     if (thermal) s -= __ldg(l0 + lrec_z0(N) + jq);
-    s += rec[H_FISOT] + rec[H_PTOP];
+    s += fisot + ptop;
     rhs = s;
   }
   unsigned carried = (1u << NN) - 1u;  // slots holding carried (un-pivoted) rows
@@ -179,7 +216,7 @@ __global__ void __launch_bounds__(RCfg<N>::CTA) flux_bvp_reg_kernel(FluxParams p
             sum -= __ldg(lr + lrec_z0(N) + NN + rb);
             sum -= __ldg(lr + lrec_z1(N) + NN + rb) * tau;
           }
-          sum += rec[H_PBOT] + mu[rb] * rec[H_PBOTD];
+          sum += pbot + mu[rb] * pbotd;
         } else {
           if (!lyrcut) {
             double refl = 0.0;
@@ -199,8 +236,8 @@ __global__ void __launch_bounds__(RCfg<N>::CTA) flux_bvp_reg_kernel(FluxParams p
             sum -= __ldg(lr + lrec_z0(N) + NN + rb);
             sum -= __ldg(lr + lrec_z1(N) + NN + rb) * tau;
           }
-          sum += rec[H_FISOB];
-          if (thermal) sum += (1.0 - alb) * rec[H_PBOT];
+          sum += fisob;
+          if (thermal) sum += (1.0 - alb) * pbot;
         }
         rhs = sum;
       }
@@ -319,9 +356,87 @@ __global__ void __launch_bounds__(RCfg<N>::CTA) flux_bvp_reg_kernel(FluxParams p
   if (singular && t == 0) set_status(p.status, i, DSP_ERR_SINGULAR);
 
   // ----------------------------------------------------------------- backward
-  for (int lev = ncut + 1 + t; lev <= L; lev += TEAM)
-    for (int f = 0; f < 8; ++f) p.out[f][oidx(lev)] = 0.0;
   bool nonfinite = false;
+  // fluxes at output level lu of layer l (computeFluxes, FluxSolver.cpp:1138-1287;
+  // DisortSolver.cpp:1980-2124): utaupr scaled depth, utau unscaled depth
+  auto eval_level = [&](int l, const double* x, int lu, double utaupr, double utau) {
+    const double* lr = LR(l);
+    const double* eig = lr + lrec_eig(N);
+    const double* Gl = lr + lrec_G(N);
+    if (t < N) {
+      const double d = (t < NN) ? (utaupr - taus[l + 1]) : (utaupr - taus[l]);
+      ec[t] = x[t] * exp(-eig[t] * d);
+    }
+    __syncwarp(msk);
+    const double fact = beam ? exp(-utaupr / umu0) : 0.0;
+    if (t < N) {
+      double s = 0.0;
+#pragma unroll
+      for (int j = 0; j < N; ++j) s += __ldg(Gl + t * N + j) * ec[j];
+      if (beam) s += __ldg(lr + lrec_zb(N) + t) * fact;
+      if (thermal) s += __ldg(lr + lrec_z0(N) + t) + __ldg(lr + lrec_z1(N) + t) * utaupr;
+      Iv[t] = s;
+    }
+    __syncwarp(msk);
+    if (t == 0) {
+      double dirint = 0.0, fldir = 0.0, fdir = 0.0;
+      if (beam) {
+        dirint = fbeam * fact;
+        fldir = umu0 * fbeam * fact;
+        fdir = umu0 * fbeam * exp(-utau / umu0);
+      }
+      double iv[N];
+#pragma unroll
+      for (int k = 0; k < N; ++k) iv[k] = Iv[k];
+      double ua = 0.0, uad = 0.0, uau = 0.0, fldn = 0.0, fup = 0.0;
+#pragma unroll
+      for (int iq = 0; iq < NN; ++iq) {
+        const int cw = NN - iq - 1;
+        ua += wt[cw] * iv[iq];
+        uad += wt[cw] * iv[iq];
+        fldn += wt[cw] * iv[iq] * mu[cw];
+      }
+#pragma unroll
+      for (int iq = NN; iq < N; ++iq) {
+        const int cw = iq - NN;
+        ua += wt[cw] * iv[iq];
+        uau += wt[cw] * iv[iq];
+        fup += wt[cw] * iv[iq] * mu[cw];
+      }
+      fup *= 2.0 * PI;
+      fldn *= 2.0 * PI;
+      const double fdn = (fldn + fldir) - fdir;
+      ua = (2.0 * PI * ua + dirint) / (4.0 * PI);
+      const double uaso = dirint / (4.0 * PI);
+      uad = (2.0 * PI * uad) / (4.0 * PI);
+      uau = (2.0 * PI * uau) / (4.0 * PI);
+      double plsorc = 0.0;
+      if (thermal) plsorc = lr[lrec_xr(N)] + lr[lrec_xr(N) + 1] * utaupr;
+      const int lin = ifb ? L - 1 - l : l;
+      const double w0 = GEN ? p.g.ssa[p.g.in_off[i] + lin] : p.ssa(i, lin);
+      const double dfdt = (1.0 - w0) * 4.0 * PI * (ua - plsorc);
+      const double o[8] = {fdir, fdn, fup, dfdt, ua, uad, uau, uaso};
+#pragma unroll
+      for (int f = 0; f < 8; ++f) {
+        outp[f][oidx(lu)] = o[f];
+        if (!isfinite(o[f])) nonfinite = true;
+      }
+    }
+    __syncwarp(msk);
+  };
+  const double* utau_l = GEN ? rec + GenLayout::make(L, N, NT).utau : nullptr;
+  const double* utaus_l = GEN ? rec + GenLayout::make(L, N, NT).utaus : nullptr;
+  const double* lyr_l = GEN ? rec + GenLayout::make(L, N, NT).lyr : nullptr;
+  if constexpr (!GEN) {
+    for (int lev = ncut + 1 + t; lev <= L; lev += TEAM)
+      for (int f = 0; f < 8; ++f) p.out[f][oidx(lev)] = 0.0;
+  } else {
+    // levels below the absorption cut stay zero (DisortSolver.cpp:1998-2009)
+    if (m == 0)
+      for (int lu = t; lu < NT; lu += TEAM)
+        if ((int)lyr_l[lu] > ncut - 1)
+          for (int f = 0; f < 8; ++f) outp[f][oidx(lu)] = 0.0;
+  }
   for (int l = ncut - 1; l >= 0; --l) {
     double* x = XV + (l & 1) * N;
     if (l < ncut - 1) {
@@ -335,70 +450,14 @@ __global__ void __launch_bounds__(RCfg<N>::CTA) flux_bvp_reg_kernel(FluxParams p
       }
       __syncwarp(msk);
     }
-    const double* lr = LR(l);
-    const double* eig = lr + lrec_eig(N);
-    const double* Gl = lr + lrec_G(N);
-    for (int pass = 0; pass < (l == 0 ? 2 : 1); ++pass) {
-      const int lu = (pass == 0) ? l + 1 : 0;
-      const double utaupr = taus[lu];
-      if (t < N) {
-        const double d = (t < NN) ? (utaupr - taus[l + 1]) : (utaupr - taus[l]);
-        ec[t] = x[t] * exp(-eig[t] * d);
-      }
-      __syncwarp(msk);
-      const double fact = beam ? exp(-utaupr / umu0) : 0.0;
-      if (t < N) {
-        double s = 0.0;
-#pragma unroll
-        for (int j = 0; j < N; ++j) s += __ldg(Gl + t * N + j) * ec[j];
-        if (beam) s += __ldg(lr + lrec_zb(N) + t) * fact;
-        if (thermal) s += __ldg(lr + lrec_z0(N) + t) + __ldg(lr + lrec_z1(N) + t) * utaupr;
-        Iv[t] = s;
-      }
-      __syncwarp(msk);
-      if (t == 0) {
-        double dirint = 0.0, fldir = 0.0, fdir = 0.0;
-        if (beam) {
-          dirint = fbeam * fact;
-          fldir = umu0 * fbeam * fact;
-          fdir = umu0 * fbeam * exp(-rec[il.tauc + lu] / umu0);
-        }
-        double iv[N];
-#pragma unroll
-        for (int k = 0; k < N; ++k) iv[k] = Iv[k];
-        double ua = 0.0, uad = 0.0, uau = 0.0, fldn = 0.0, fup = 0.0;
-#pragma unroll
-        for (int iq = 0; iq < NN; ++iq) {
-          const int cw = NN - iq - 1;
-          ua += wt[cw] * iv[iq];
-          uad += wt[cw] * iv[iq];
-          fldn += wt[cw] * iv[iq] * mu[cw];
-        }
-#pragma unroll
-        for (int iq = NN; iq < N; ++iq) {
-          const int cw = iq - NN;
-          ua += wt[cw] * iv[iq];
-          uau += wt[cw] * iv[iq];
-          fup += wt[cw] * iv[iq] * mu[cw];
-        }
-        fup *= 2.0 * PI;
-        fldn *= 2.0 * PI;
-        const double fdn = (fldn + fldir) - fdir;
-        ua = (2.0 * PI * ua + dirint) / (4.0 * PI);
-        const double uaso = dirint / (4.0 * PI);
-        uad = (2.0 * PI * uad) / (4.0 * PI);
-        uau = (2.0 * PI * uau) / (4.0 * PI);
-        double plsorc = 0.0;
-        if (thermal) plsorc = lr[lrec_xr(N)] + lr[lrec_xr(N) + 1] * utaupr;
-        const double dfdt = (1.0 - p.ssa(i, ifb ? L - 1 - l : l)) * 4.0 * PI * (ua - plsorc);
-        const double o[8] = {fdir, fdn, fup, dfdt, ua, uad, uau, uaso};
-#pragma unroll
-        for (int f = 0; f < 8; ++f) {
-          p.out[f][oidx(lu)] = o[f];
-          if (!isfinite(o[f])) nonfinite = true;
-        }
-      }
-      __syncwarp(msk);
+    if constexpr (GEN) {
+      if (t < N) cc0[(long long)l * N + t] = x[t];
+      if (m == 0)
+        for (int lu = 0; lu < NT; ++lu)
+          if ((int)lyr_l[lu] == l) eval_level(l, x, lu, utaus_l[lu], utau_l[lu]);
+    } else {
+      eval_level(l, x, l + 1, taus[l + 1], rec[il.tauc + l + 1]);
+      if (l == 0) eval_level(0, x, 0, taus[0], rec[il.tauc]);
     }
     DSP_PHASE(23)
   }

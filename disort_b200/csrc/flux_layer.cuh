@@ -24,7 +24,7 @@
 
 namespace dsp {
 
-template <int N>
+template <int N, bool GEN = false>
 struct LCfg {
   static constexpr int NN = N / 2;
   static constexpr int TEAM = pow2ceil(N) < 4 ? 4 : pow2ceil(N);
@@ -47,7 +47,12 @@ struct LCfg {
   static constexpr int O_Z = O_B + N;                // z[N]
   static constexpr int O_MISC = O_Z + N;             // flags, reduction scratch
   static constexpr int O_PIV = O_MISC + 8;           // N ints
-  static constexpr int TEAM_SMEM = round4(O_PIV + N / 2 + 1);
+  // general solver: P_l^m(-mu0), then psi0 / p0 / p1 source moments [N] each
+  static constexpr int O_GX = O_PIV + N / 2 + 1;
+  static constexpr int TEAM_SMEM = round4(O_GX + (GEN ? 4 * N : 0));
+  // user angles whose P_l^m columns fit next to W[N][N] in the work area
+  static constexpr int UCH = (W_SIZE - N * N) / N;
+  static_assert(!GEN || UCH >= 1, "work area too small for the user-angle tables");
   static constexpr int TAB = tab_size(N);
   static constexpr size_t smem_bytes() { return sizeof(double) * (size_t)(TAB + TPC * TEAM_SMEM); }
 };
@@ -217,9 +222,104 @@ __device__ __forceinline__ double team_trsv(const double* Lm, double x, bool tra
   return x;
 }
 
+// Eigenvectors and sources of one layer at the user polar angles for mode m
+// (interpEigenvec, DisortSolver.cpp:2468-2504; interpSource, :2506-2580):
+//   W(l, c)   = 0.5 g'_l sum_jq P_l^m(mu_jq) w_jq G(row(jq), c)
+//   GU(iu, c) = sum_l P_l^m(mu_u) W(l, c)
+// with row(jq) = NN + jq for jq < NN, N - 1 - jq otherwise (the reference's
+// reduced-eigenvector ordering); the beam and thermal sources likewise.
+// Team thread c owns column c; the P_l^m columns of up to UCH user angles at a
+// time sit beside W in the (now free) eigen work area.
 template <int N>
-__global__ void __launch_bounds__(LCfg<N>::CTA) flux_layer_kernel(FluxParams p) {
-  using C = LCfg<N>;
+__device__ void gen_user_angles(const FluxParams& p, int i, double* sm, const double* Y, const double* wt,
+                                const double* gl, double* lrec, double fbeam, double ws, bool thermal,
+                                int t) {
+  using C = LCfg<N, true>;
+  constexpr int NN = N / 2, TEAM = C::TEAM, UCH = C::UCH;
+  const int m = p.g.m, numu = p.g.numu;
+  double* W = sm + C::O_W;           // [N][N]
+  double* U = W + N * N;             // [N][UCH]
+  const double* ybm = sm + C::O_GX;  // P_l^m(-mu0) (written by the beam source)
+  double* psi0 = sm + C::O_GX + N;
+  double* p0 = psi0 + N;
+  double* p1 = p0 + N;
+  const double* G = lrec + lrec_G(N);
+  const bool beam = fbeam > 0.0;
+  team_sync<TEAM>();  // G and the particular solutions of this team are written
+  if (t < N) {
+    const int c = t;
+    double gcol[N];
+#pragma unroll
+    for (int jq = 0; jq < N; ++jq) gcol[jq] = G[(jq < NN ? NN + jq : N - 1 - jq) * N + c];
+    for (int l = 0; l < N; ++l) {
+      double s = 0.0;
+      if (l >= m) {
+#pragma unroll
+        for (int jq = 0; jq < N; ++jq) s += (Y[l * N + jq] * wt[jq]) * gcol[jq];
+        s *= 0.5 * gl[l];
+      }
+      W[l * N + c] = s;
+    }
+    // source moments: psi0(l) = 0.5 g'_l sum_jq w_jq P_l^m(mu_jq) z(jq) with the
+    // unordered beam solution z(jq) = zb[row(jq)], and the thermal z0 / z1 alike
+    const int l = t;
+    double sb = 0.0, s0 = 0.0, s1 = 0.0;
+    if (l >= m) {
+      for (int jq = 0; jq < N; ++jq) {
+        const int r = jq < NN ? NN + jq : N - 1 - jq;
+        const double yw = wt[jq] * Y[l * N + jq];
+        if (beam) sb += yw * lrec[lrec_zb(N) + r];
+        if (thermal) {
+          s0 += yw * lrec[lrec_z0(N) + r];
+          s1 += yw * lrec[lrec_z1(N) + r];
+        }
+      }
+    }
+    psi0[l] = 0.5 * gl[l] * sb;
+    p0[l] = 0.5 * gl[l] * s0;
+    p1[l] = 0.5 * gl[l] * s1;
+  }
+  team_sync<TEAM>();
+  const double xr0 = lrec[lrec_xr(N)], xr1 = lrec[lrec_xr(N) + 1];
+  const double fact = (m == 0 ? 1.0 : 2.0) * fbeam / (4.0 * 3.14159265358979323846);
+  double* GU = lrec + glrec_gu(N);
+  double* zbu = GU + numu * N;
+  double* z0u = zbu + numu;
+  double* z1u = z0u + numu;
+  const double* umu = p.g.umu.row(i);
+  for (int u0 = 0; u0 < numu; u0 += UCH) {
+    const int nu = numu - u0 < UCH ? numu - u0 : UCH;
+    if (t < nu) legendre_column(m, umu[u0 + t], N - 1, U + t, UCH);
+    team_sync<TEAM>();
+    if (t < N)
+      for (int k = 0; k < nu; ++k) {
+        double s = 0.0;
+        for (int l = m; l < N; ++l) s += U[l * UCH + k] * W[l * N + t];
+        GU[(u0 + k) * N + t] = s;
+      }
+    if (t < nu) {
+      if (beam) {
+        double s = 0.0;
+        for (int l = m; l < N; ++l) s += U[l * UCH + t] * (psi0[l] + fact * gl[l] * ybm[l]);
+        zbu[u0 + t] = s;
+      }
+      if (thermal) {
+        double s0 = 0.0, s1 = 0.0;
+        for (int l = m; l < N; ++l) {
+          s0 += U[l * UCH + t] * p0[l];
+          s1 += U[l * UCH + t] * p1[l];
+        }
+        z0u[u0 + t] = s0 + (1.0 - ws) * xr0;
+        z1u[u0 + t] = s1 + (1.0 - ws) * xr1;
+      }
+    }
+    team_sync<TEAM>();
+  }
+}
+
+template <int N, bool GEN = false>
+__global__ void __launch_bounds__(LCfg<N, GEN>::CTA) flux_layer_kernel(FluxParams p) {
+  using C = LCfg<N, GEN>;
   constexpr int NN = C::NN, TEAM = C::TEAM, NNP = C::NNP, NPAIR = C::NPAIR, NS = C::NS, BPT = C::BPT;
   constexpr int BPA = NPAIR;  // blocks (a, b) per column pair b
   extern __shared__ double smem[];
@@ -234,13 +334,39 @@ __global__ void __launch_bounds__(LCfg<N>::CTA) flux_layer_kernel(FluxParams p) 
 
   const int team = threadIdx.x / TEAM, t = threadIdx.x % TEAM;
   const long long task = (long long)blockIdx.x * C::TPC + team;
-  if (task >= (long long)p.n * p.L) return;
-  const int i = (int)(task / p.L), lc = (int)(task % p.L);
+  // i: status / input index; lc: layer; Lin: layers of the instance
+  int i, lc, Lin;
+  const double* rec;
+  InstLayout il_gen;  // general solver: the layout of this instance
+  const double* pml;
+  if constexpr (GEN) {
+    // general solver: ragged layers; task = chunk-local layer
+    if (task >= p.g.lay_off[p.n]) return;
+    const int ci = p.g.layer_inst[task];
+    i = p.g.ids[ci];
+    lc = (int)(task - p.g.lay_off[ci]);
+    Lin = p.g.Ls[i];
+    il_gen = InstLayout::make(Lin, N);
+    rec = p.inst_rec + p.g.inst_off[ci];
+    const int lin = (p.flags & DSP_FLAG_INDEX_FROM_BOTTOM) ? Lin - 1 - lc : lc;
+    pml = p.g.pmom + (p.g.in_off[i] + lin) * (long long)p.pc;
+  } else {
+    if (task >= (long long)p.n * p.L) return;
+    i = (int)(task / p.L);
+    lc = (int)(task % p.L);
+    Lin = p.L;
+    rec = p.inst_rec + (long long)i * p.il.stride;
+    const int lin = (p.flags & DSP_FLAG_INDEX_FROM_BOTTOM) ? p.L - 1 - lc : lc;
+    pml = p.pmom.row(i) + (long long)lin * p.pc;
+  }
+  const InstLayout& il = GEN ? il_gen : p.il;
   if (p.status && p.status[i] == DSP_ERR_INVALID_INPUT) return;
-  const InstLayout& il = p.il;
-  const double* rec = p.inst_rec + (long long)i * il.stride;
   const int ncut = (int)rec[H_NCUT];
   if (lc >= ncut) return;  // layers below the absorption cut are never used
+  if constexpr (GEN) {
+    // modes past the instance's last one, or after its azimuthal series converged
+    if (p.g.m > (int)rec[H_NAZ] || rec[H_DONE] != 0.0) return;
+  }
 
   double* sm = smem + C::TAB + team * C::TEAM_SMEM;
   double* CC = sm + C::O_CC;
@@ -274,10 +400,9 @@ __global__ void __launch_bounds__(LCfg<N>::CTA) flux_layer_kernel(FluxParams p) 
   {
     const int mode = (int)rec[il.mode + lc];
     const double f = rec[il.fsc + lc], sig = rec[il.sig + lc];
-    const int lin = (p.flags & DSP_FLAG_INDEX_FROM_BOTTOM) ? p.L - 1 - lc : lc;
-    const double* pml = p.pmom.row(i) + (long long)lin * p.pc;
     for (int k = t; k < N; k += TEAM) {
-      const double pk = pml[k];
+      // the general solver normalises P_0 to 1 (DisortSolver.cpp:669)
+      const double pk = (GEN && k == 0) ? 1.0 : pml[k];
       double g;
       if (mode == 0) g = (2.0 * k + 1.0) * ws * pk;
       else if (mode == 1) g = (2.0 * k + 1.0) * ws * (pk - f) / (1.0 - f);
@@ -517,7 +642,9 @@ __global__ void __launch_bounds__(LCfg<N>::CTA) flux_layer_kernel(FluxParams p) 
   }
   team_sync<TEAM>();
   // ---- k, G+/-  (FluxSolver.cpp:561-587) ---------------------------------
-  double* lrec = p.layer_rec + ((long long)i * p.L + lc) * lrec_stride(N);
+  double* lrec;
+  if constexpr (GEN) lrec = p.layer_rec + task * p.g.lstride;
+  else lrec = p.layer_rec + ((long long)i * p.L + lc) * lrec_stride(N);
   for (int k = t; k < NN; k += TEAM) {
     const double kr = sqrt(fabs(lam[k]));
     lamraw[k] = lam[k];
@@ -598,11 +725,22 @@ __global__ void __launch_bounds__(LCfg<N>::CTA) flux_layer_kernel(FluxParams p) 
       if (fabs(1.0 - mu0sq * kk * kk) < dither) dith = true;
     }
     if (dith) beam_mu = 0.999 * umu0;
-    const double* yb = rec + il.yb;
+    const double* yb;
+    if constexpr (GEN) {
+      // P_l^m(-mu0) of this mode (DisortSolver.cpp:1334-1335); Y rows l < m are zero
+      double* ybm = sm + C::O_GX;
+      if (t == 0) legendre_column(p.g.m, -umu0, N - 1, ybm, 1);
+      team_sync<TEAM>();
+      yb = ybm;
+    } else {
+      yb = rec + il.yb;
+    }
+    // (2 - delta_m0) F0 sum_k g'_k P_k^m(mu_r) P_k^m(-mu0) / 4pi (DisortSolver.cpp:1361-1368)
+    const double bfac = (GEN && p.g.m > 0) ? 2.0 * fbeam : fbeam;
     for (int r = t; r < N; r += TEAM) {
       double sacc = 0.0;
       for (int k = 0; k < N; ++k) sacc += gl[k] * Y[k * N + r] * yb[k];
-      bv[r] = fbeam * sacc / (4.0 * 3.14159265358979323846);
+      bv[r] = bfac * sacc / (4.0 * 3.14159265358979323846);
     }
     team_sync<TEAM>();
     const double bp = (t < NN) ? bv[t] : 0.0, bm = (t < NN) ? bv[NN + t] : 0.0;
@@ -635,7 +773,8 @@ __global__ void __launch_bounds__(LCfg<N>::CTA) flux_layer_kernel(FluxParams p) 
     }
     team_sync<TEAM>();
   }
-  if (p.flags & DSP_FLAG_THERMAL) {
+  const bool thermal_src = (p.flags & DSP_FLAG_THERMAL) && (!GEN || p.g.m == 0);
+  if (thermal_src) {
     // ---- thermal (computeIsotropicSource, FluxSolver.cpp:745-787) ---------
     // Z1 solves (I-C) z = (1-w') xr1 (isotropic: d1 = 0); Z0 solves
     // (I-C) z = (1-w') xr0 + mu Z1, i.e. r1 = 2(1-w') xr0, r2 = M s1.
@@ -662,6 +801,9 @@ __global__ void __launch_bounds__(LCfg<N>::CTA) flux_layer_kernel(FluxParams p) 
     }
   }
   DSP_PHASE(7)
+  if constexpr (GEN) {
+    if (p.g.numu > 0) gen_user_angles<N>(p, i, sm, Y, wt, gl, lrec, rec[H_FBEAM], ws, thermal_src, t);
+  }
 }
 
 }  // namespace dsp

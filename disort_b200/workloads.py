@@ -10,6 +10,12 @@ baseline all consume the same arrays.
                    lognormal(-3,2) optical depths clipped to [1e-6, 50], ssa U[0,0.99],
                    HG g U[0,0.9], one 61-level temperature profile 180..320 K with
                    +-10 K noise, albedo 0.05, thermal emission on, no beam (seed 2).
+``general_mix``    the general solver's mixed batch: 65,536 instances, N in
+                   {4, 8, 16, 32, 64} (weights .1 .2 .4 .2 .1), L uniform in 10..120,
+                   optical depths and ssa as the thermal sweep, HG g U[0.5, 0.95] with
+                   N+1 moments and delta-M+, beam F0 = 1 at mu0 U[0.1, 1], albedo
+                   U[0, 0.6], no thermal; user taus {0, tau/2, tau}, user mu
+                   {-0.5, -0.1, 0.1, 0.5, 1}, phi {0, 60, 120, 180}, all modes (seed 3).
 """
 from __future__ import annotations
 
@@ -103,3 +109,37 @@ def make_batch(w: dict, extra_flags: int = 0):
     return capi.make_flux_batch(w["n_inst"], w["num_streams"], w["num_layers"],
                                 w["num_phase_func_moments"], w["pmom_count"],
                                 w["flags"] | extra_flags, w["arrays"])
+
+
+GENERAL_NSTR = (4, 8, 16, 32, 64)
+GENERAL_NSTR_WEIGHTS = (0.1, 0.2, 0.4, 0.2, 0.1)
+GENERAL_MU = (-0.5, -0.1, 0.1, 0.5, 1.0)
+GENERAL_PHI = (0.0, 60.0, 120.0, 180.0)
+
+
+def general_mix(n_inst: int = 65536, seed: int = 3, nstr=None, layers=(10, 120)) -> tuple[list, int]:
+    """Instances of the general solver's mixed batch and its flags.
+
+    `nstr` restricts the stream counts (same weights, renormalised); `layers` is
+    the inclusive range of the uniform layer count."""
+    rng = np.random.default_rng(seed)
+    Ns = np.array(GENERAL_NSTR if nstr is None else nstr)
+    w = np.array([GENERAL_NSTR_WEIGHTS[GENERAL_NSTR.index(x)] for x in Ns])
+    w = w / w.sum()
+    Nv = rng.choice(Ns, size=n_inst, p=w)
+    Lv = rng.integers(layers[0], layers[1] + 1, size=n_inst)
+    insts = []
+    for k in range(n_inst):
+        N, L = int(Nv[k]), int(Lv[k])
+        dtau = np.clip(rng.lognormal(-3.0, 2.0, L), 1e-6, 50.0)
+        g = rng.uniform(0.5, 0.95, L)
+        tot = float(np.sum(dtau))
+        insts.append(dict(
+            num_streams=N, num_layers=L, num_phase_func_moments=N + 1,
+            delta_tau=dtau, single_scat_albedo=rng.uniform(0.0, 0.99, L),
+            phase_function_moments=hg_moments(g, N + 2),
+            direct_beam_flux=1.0, direct_beam_mu=float(rng.uniform(0.1, 1.0)), direct_beam_phi=0.0,
+            surface_albedo=float(rng.uniform(0.0, 0.6)),
+            tau_user=[0.0, tot / 2.0, tot], mu_user=list(GENERAL_MU), phi_user=list(GENERAL_PHI)))
+    flags = capi.FLAG_DELTA_M_PLUS | capi.GFLAG_USER_TAU | capi.GFLAG_USER_MU
+    return insts, flags

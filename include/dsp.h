@@ -110,6 +110,53 @@ typedef struct dsp_flux_out {
   int32_t* status; /* [n_inst] or NULL */
 } dsp_flux_out;
 
+/*
+ * General batch (DisortConfig, DisortConfig.hpp:119-243): the full DisortSolver
+ * with Fourier azimuth modes and intensities at user optical depths, polar
+ * angles and azimuths.  Plane-parallel geometry, Lambertian surface.
+ * Instances may differ in num_streams and num_layers: instance i owns layers
+ * layer_offset[i] .. layer_offset[i+1]-1 of the layer arrays (CSR) and levels
+ * layer_offset[i] + i .. layer_offset[i+1] + i of the level arrays.
+ */
+#define DSP_GFLAG_USER_TAU         (1u << 8)  /* use_user_tau (else outputs at the layer boundaries) */
+#define DSP_GFLAG_USER_MU          (1u << 9)  /* use_user_mu */
+#define DSP_GFLAG_ONLY_FLUXES      (1u << 10) /* comp_only_fluxes */
+
+typedef struct dsp_general_batch {
+  int32_t n_inst;
+  uint32_t flags;                 /* DSP_FLAG_* and DSP_GFLAG_* */
+  const int32_t* num_streams;     /* [n_inst] */
+  const int32_t* num_layers;      /* [n_inst] */
+  const int64_t* layer_offset;    /* [n_inst+1] */
+  const int32_t* num_phase_func_moments; /* [n_inst] */
+  int32_t pmom_count;             /* doubles per layer in phase_function_moments */
+  int32_t num_user_tau;           /* ntau (with DSP_GFLAG_USER_TAU), else ignored */
+  int32_t num_user_mu;            /* numu (with DSP_GFLAG_USER_MU) */
+  int32_t num_phi;                /* nphi */
+  double accuracy_fourier_series; /* azimuthal convergence criterion (0: all modes) */
+
+  const double* delta_tau;              /* [total layers] */
+  const double* single_scat_albedo;     /* [total layers] */
+  const double* phase_function_moments; /* [total layers][pmom_count] */
+  const double* temperature;            /* [total layers + n_inst] (thermal only) */
+  dsp_darray tau_user;                  /* [ntau] per instance or shared */
+  dsp_darray mu_user;                   /* [numu], ascending */
+  dsp_darray phi_user;                  /* [nphi], degrees */
+  dsp_darray wavenumber_low, wavenumber_high, surface_albedo, emissivity_top, direct_beam_flux,
+      direct_beam_mu, direct_beam_phi, isotropic_flux_top, isotropic_flux_bottom, temperature_top,
+      temperature_bottom; /* [1] each */
+} dsp_general_batch;
+
+/* DisortResult (DisortResult.hpp:16-125) for the general batch. */
+typedef struct dsp_general_out {
+  double* flux[8];                /* FluxResult order, each [n_inst][ntau_out] */
+  double* intensity;              /* [n_inst][ntau_out][numu_out][nphi] */
+  double* intensity_azimuth_avg;  /* [n_inst][ntau_out][numu_out] */
+  int32_t* status;                /* [n_inst] or NULL */
+  int32_t ntau_out;               /* output row stride: >= ntau (or >= max L+1 without user taus) */
+  int32_t numu_out;               /* output stride: >= numu (or >= max N without user angles) */
+} dsp_general_out;
+
 typedef struct dsp_context_s* dsp_context;
 
 /* Library / context management. `stream` is a cudaStream_t (NULL = legacy default). */
@@ -140,6 +187,10 @@ dsp_status dsp_context_timing_get(dsp_context ctx, int32_t idx, const char** nam
 /* Flux-only spectral-band solve (DisortFluxSolver<N> over every instance). */
 dsp_status dsp_flux_bands_solve(dsp_context ctx, const dsp_flux_batch* batch,
                                 const dsp_flux_out* out);
+
+/* General spectral-band solve (DisortSolver::solve over every instance). */
+dsp_status dsp_general_bands_solve(dsp_context ctx, const dsp_general_batch* batch,
+                                   const dsp_general_out* out);
 
 /*
  * Flux solve without any allocation (no counterpart in the reference: DisORT++

@@ -1,0 +1,791 @@
+// general_oracle.hpp — CPU restatement of DisortSolver::solve
+// (src/DisortSolver.cpp:21-399 of DisORT++) for plane-parallel geometry and a
+// Lambertian surface without intensity corrections: delta-M / delta-M+,
+// Fourier azimuth modes, fluxes at user optical depths and intensities at user
+// polar angles and azimuths.
+//
+// TEST INFRASTRUCTURE ONLY (the oracle).  Never linked into the product.
+#pragma once
+
+#include <vector>
+
+#include "flux_oracle.hpp"
+
+namespace oracle {
+
+struct GeneralInstance {
+  int L = 0, N = 0, nmom = 0, pc = 0;
+  bool thermal = false, dmplus = false, dlbc = false, ifb = false;
+  bool user_tau = false, user_mu = false, only_fluxes = false;
+  double accur = 0.0;
+  double wlo = 0, whi = 0, alb = 0, emis = 1, fbeam = 0, umu0 = 0.5, phi0 = 0, fisot = 0, fisob = 0, ttop = 0, tbot = 0;
+  const double *dtau = nullptr, *ssa = nullptr, *pmom = nullptr, *temp = nullptr;
+  int ntau = 0, numu = 0, nphi = 0;
+  const double *utau = nullptr, *umu = nullptr, *phi = nullptr;
+};
+
+struct GeneralOutput {
+  double* flux[8];   // [ntau_out]
+  double* intensity; // [ntau_out][numu_out][nphi]
+  double* iavg;      // [ntau_out][numu_out]
+  int ntau_out = 0, numu_out = 0;
+};
+
+// DisortConfig::validate (DisortConfig.cpp:72-249) for the fields carried here,
+// in the reference's order and with its comparisons (a NaN passes where the
+// reference's test lets it pass).
+inline int validate_general(const GeneralInstance& c) {
+  if (c.L <= 0 || c.N < 4 || c.N % 2 != 0 || c.nmom < 0) return DSP_ERR_INVALID_INPUT;
+  if (c.pc < std::max(c.nmom, c.N) + 1) return DSP_ERR_INVALID_INPUT;
+  for (int lc = 0; lc < c.L; ++lc) {
+    if (c.dtau[lc] < 0.0) return DSP_ERR_INVALID_INPUT;
+    if (c.ssa[lc] < 0.0 || c.ssa[lc] > 1.0) return DSP_ERR_INVALID_INPUT;
+  }
+  if (c.thermal) {
+    if (!c.temp) return DSP_ERR_INVALID_INPUT;
+    for (int lev = 0; lev <= c.L; ++lev)
+      if (c.temp[lev] < 0.0) return DSP_ERR_INVALID_INPUT;
+    if (c.wlo < 0.0 || c.whi < c.wlo) return DSP_ERR_INVALID_INPUT;
+  }
+  if (c.dlbc && !c.thermal) return DSP_ERR_INVALID_INPUT;
+  if (c.fbeam < 0.0) return DSP_ERR_INVALID_INPUT;
+  if ((c.umu0 <= 0.0 || c.umu0 > 1.0) && c.fbeam > 0.0) return DSP_ERR_INVALID_INPUT;
+  if (c.alb < 0.0 || c.alb > 1.0) return DSP_ERR_INVALID_INPUT;
+  if (c.user_mu) {
+    if (c.numu <= 0 || !c.umu) return DSP_ERR_INVALID_INPUT;
+    for (int iu = 0; iu < c.numu; ++iu) {
+      if (std::abs(c.umu[iu]) > 1.0) return DSP_ERR_INVALID_INPUT;
+      if (iu > 0 && c.umu[iu] <= c.umu[iu - 1]) return DSP_ERR_INVALID_INPUT;
+    }
+  }
+  if (!c.only_fluxes) {
+    if (c.nphi <= 0 || !c.phi) return DSP_ERR_INVALID_INPUT;
+    for (int j = 0; j < c.nphi; ++j)
+      if (c.phi[j] < 0.0 || c.phi[j] > 360.0) return DSP_ERR_INVALID_INPUT;
+  }
+  if (c.dmplus && c.nmom < c.N + 1) return DSP_ERR_INVALID_INPUT;
+  if (c.accur < 0.0) return DSP_ERR_INVALID_INPUT;
+  if (c.thermal) {
+    if (c.wlo < 0.0 || c.whi <= c.wlo) return DSP_ERR_INVALID_INPUT;
+    if (c.ttop < 0.0 || c.tbot < 0.0) return DSP_ERR_INVALID_INPUT;
+    if (c.emis < 0.0 || c.emis > 1.0) return DSP_ERR_INVALID_INPUT;
+  }
+  // boundary of the C ABI: user optical depths must be given when requested
+  if (c.user_tau && (c.ntau <= 0 || !c.utau)) return DSP_ERR_INVALID_INPUT;
+  return DSP_OK;
+}
+
+class GeneralOracle {
+ public:
+  int solve(const GeneralInstance& in, const GeneralOutput& out);
+};
+
+inline int GeneralOracle::solve(const GeneralInstance& cin, const GeneralOutput& out) {
+  GeneralInstance c = cin;
+  const int L = c.L, N = c.N, NN = N / 2;
+  std::vector<double> rdt, rss, rpm, rtp, rut;
+  if (c.ifb) {  // reverseInputArrays (IndexConversion.hpp:16-40)
+    rdt.assign(c.dtau, c.dtau + L);
+    rss.assign(c.ssa, c.ssa + L);
+    std::reverse(rdt.begin(), rdt.end());
+    std::reverse(rss.begin(), rss.end());
+    rpm.resize((size_t)L * c.pc);
+    for (int lc = 0; lc < L; ++lc)
+      std::memcpy(&rpm[(size_t)lc * c.pc], c.pmom + (size_t)(L - 1 - lc) * c.pc, sizeof(double) * c.pc);
+    c.dtau = rdt.data();
+    c.ssa = rss.data();
+    c.pmom = rpm.data();
+    if (c.temp) {
+      rtp.assign(c.temp, c.temp + L + 1);
+      std::reverse(rtp.begin(), rtp.end());
+      c.temp = rtp.data();
+    }
+    if (c.user_tau && c.utau && c.ntau > 0) {
+      double total = 0.0;
+      for (int lc = 0; lc < L; ++lc) total += c.dtau[lc];
+      rut.assign(c.utau, c.utau + c.ntau);
+      for (auto& t : rut) t = total - t;
+      std::reverse(rut.begin(), rut.end());
+      c.utau = rut.data();
+    }
+  }
+  if (int st = validate_general(c)) return st;
+  const int ntau = c.user_tau ? c.ntau : L + 1;
+  const bool do_int = !c.only_fluxes && c.user_mu;
+  const int numu = (c.user_mu && !c.only_fluxes) ? c.numu : N;
+  const int nphi = c.nphi;
+  const int pc = c.pc;
+  // pmom with P_0 = 1 (the reference sets it, DisortSolver.cpp:669)
+  std::vector<double> pm(c.pmom, c.pmom + (size_t)L * pc);
+  for (int lc = 0; lc < L; ++lc) pm[(size_t)lc * pc] = 1.0;
+  auto PM = [&](int k, int lc) { return pm[(size_t)lc * pc + k]; };
+
+  // delta-M decisions (DisortSolver.cpp:72-112)
+  bool deltam = false;
+  for (int lc = 0; lc < L; ++lc)
+    if (PM(N, lc) != 0.0) { deltam = true; break; }
+  const bool needdm = deltam;
+  bool dmplus = c.dmplus;
+  if (dmplus) {
+    for (int lc = 0; lc < L; ++lc) {
+      const double a = PM(N, lc), b = PM(N + 1, lc);
+      if (a < 1e-4 || b < 0.7 * a) { dmplus = false; break; }
+    }
+    deltam = dmplus ? false : needdm;
+  }
+
+  // disortSet (DisortSolver.cpp:641-866)
+  std::vector<double> tauc(L + 1), taus(L + 1), dts(L), ws(L), fsc(L), gl((size_t)L * N), btr(L + 1, 0.0);
+  tauc[0] = 0.0;
+  for (int lc = 0; lc < L; ++lc) tauc[lc + 1] = tauc[lc] + c.dtau[lc];
+  std::vector<double> utau(ntau);
+  if (c.user_tau) for (int k = 0; k < ntau; ++k) utau[k] = c.utau[k];
+  else for (int k = 0; k < ntau; ++k) utau[k] = tauc[k];
+  taus[0] = 0.0;
+  double abstau = 0.0;
+  int ncut = L;
+  for (int lc = 0; lc < L; ++lc) {
+    if (abstau < 10.0) ncut = lc + 1;
+    abstau += (1.0 - c.ssa[lc]) * c.dtau[lc];
+    const double w0 = c.ssa[lc], dt = c.dtau[lc];
+    double f;
+    double* g = &gl[(size_t)lc * N];
+    if (!deltam && !dmplus) {
+      ws[lc] = w0; dts[lc] = dt; taus[lc + 1] = tauc[lc + 1];
+      for (int k = 0; k < N; ++k) g[k] = (2.0 * k + 1.0) * ws[lc] * PM(k, lc);
+      f = 0.0;
+    } else if (!dmplus || PM(N - 1, lc) == PM(N, lc) || PM(N, lc) == PM(N + 1, lc)) {
+      f = PM(N, lc);
+      ws[lc] = w0 * (1.0 - f) / (1.0 - f * w0);
+      dts[lc] = (1.0 - f * w0) * dt;
+      taus[lc + 1] = taus[lc] + dts[lc];
+      for (int k = 0; k < N; ++k) g[k] = (2.0 * k + 1.0) * ws[lc] * (PM(k, lc) - f) / (1.0 - f);
+    } else {
+      const double a = PM(N, lc), b = PM(N + 1, lc);
+      const double M = N;
+      const double sig = ((M + 1.0) * (M + 1.0) - M * M) / (std::log(a * a) - std::log(b * b));
+      const double cc = std::exp(M * M / (2.0 * sig));
+      f = cc * a;
+      ws[lc] = w0 * (1.0 - f) / (1.0 - f * w0);
+      dts[lc] = (1.0 - f * w0) * dt;
+      taus[lc + 1] = taus[lc] + dts[lc];
+      for (int k = 0; k < N; ++k) {
+        const double kd = k;
+        g[k] = (2.0 * k + 1.0) * ws[lc] * (PM(k, lc) - f * std::exp(-kd * kd / (2.0 * sig))) / (1.0 - f);
+      }
+    }
+    fsc[lc] = f;
+  }
+  if (c.fbeam > 0.0) {
+    btr[0] = 1.0;
+    for (int lc = 0; lc < ncut; ++lc) btr[lc + 1] = std::exp(-taus[lc + 1] / c.umu0);
+  }
+  const bool lyrcut = (abstau >= 10.0 && !c.thermal && L > 1);
+  if (!lyrcut) ncut = L;
+  std::vector<double> utaus(ntau);
+  std::vector<int> lyr(ntau);
+  for (int lu = 0; lu < ntau; ++lu) {
+    int lc;
+    for (lc = 0; lc < L - 1; ++lc)
+      if (utau[lu] >= tauc[lc] && utau[lu] <= tauc[lc + 1]) break;
+    utaus[lu] = utau[lu];
+    if (deltam || dmplus) utaus[lu] = taus[lc] + (1.0 - c.ssa[lc] * fsc[lc]) * (utau[lu] - tauc[lc]);
+    lyr[lu] = lc;
+  }
+  std::vector<double> mu(N), wt(N), dsim(NN), dinv(NN);
+  if (!gauss_quadrature(NN, mu.data(), wt.data())) return DSP_ERR_EIGEN;
+  for (int iq = 0; iq < NN; ++iq) {
+    dsim[iq] = std::sqrt(wt[iq] * mu[iq]);
+    dinv[iq] = 1.0 / dsim[iq];
+  }
+  std::vector<double> umu(numu);
+  if (c.user_mu && !c.only_fluxes) for (int iu = 0; iu < numu; ++iu) umu[iu] = c.umu[iu];
+  else {
+    for (int iu = 0; iu < NN; ++iu) umu[iu] = -mu[NN - 1 - iu];
+    for (int iu = NN; iu < N; ++iu) umu[iu] = mu[iu - NN];
+  }
+
+  double ptop = 0, pbot = 0, pbotd = 0;
+  if (c.thermal) {
+    ptop = planck_function2(c.wlo, c.whi, c.ttop) * c.emis;
+    pbot = planck_function2(c.wlo, c.whi, c.tbot);
+    if (c.dlbc) {
+      const double bl = planck_function2(c.wlo, c.whi, c.temp[L - 1]);
+      if (dts[L - 1] > 0.0) pbotd = (pbot - bl) / dts[L - 1];
+    }
+  }
+
+  // naz (DisortSolver.cpp:218-234); the reference's 1-based mu_user lookups
+  // are read here only where the index exists
+  int naz = N - 1;
+  {
+    auto um = [&](int k) { return (k < numu) ? umu[k] : 0.0; };
+    const bool indep = (c.fbeam == 0.0) || (std::abs(1.0 - c.umu0) < 1.e-5) || c.only_fluxes ||
+                       (numu == 1 && std::abs(1.0 - um(1)) < 1.e-5) || (numu == 1 && std::abs(1.0 + um(1)) < 1.e-5) ||
+                       (numu == 2 && std::abs(1.0 + um(1)) < 1.e-5 && std::abs(1.0 - um(2)) < 1.e-5);
+    if (indep) naz = 0;
+  }
+
+  // outputs start at zero
+  for (int f = 0; f < 8; ++f) for (int lu = 0; lu < out.ntau_out; ++lu) out.flux[f][lu] = 0.0;
+  if (out.intensity)
+    for (size_t k = 0; k < (size_t)out.ntau_out * out.numu_out * nphi; ++k) out.intensity[k] = 0.0;
+  if (out.iavg)
+    for (size_t k = 0; k < (size_t)out.ntau_out * out.numu_out; ++k) out.iavg[k] = 0.0;
+  auto I3 = [&](int lu, int iu, int j) -> double& {
+    return out.intensity[((size_t)lu * out.numu_out + iu) * nphi + j];
+  };
+
+  // persistent Legendre tables (the m > 0 recurrence reads row m-1 of the previous mode)
+  std::vector<double> ylq((size_t)(N + 1) * N, 0.0), ylu((size_t)(N + 1) * std::max(numu, 1), 0.0), ylb(N + 1, 0.0);
+  std::vector<double> kk((size_t)L * N), G((size_t)L * N * N), C((size_t)L * N * N), zb((size_t)L * N),
+      zbraw((size_t)L * N), z0((size_t)L * N, 0.0), z1((size_t)L * N, 0.0), xr0(L, 0.0), xr1(L, 0.0),
+      GU((size_t)L * numu * N), zbu((size_t)L * numu, 0.0), z0u((size_t)L * numu, 0.0), z1u((size_t)L * numu, 0.0),
+      cc((size_t)N * L), Im((size_t)ntau * numu);
+  std::vector<double> cc_top((size_t)NN * N), amb(NN * NN), apb(NN * NN), evec(NN * NN), kred(NN), gpg(NN * NN);
+  std::vector<double> A((size_t)N * N), xv(N), bvec(N);
+  std::vector<int> piv(N);
+  int kconv = 0;
+  int status = DSP_OK;
+
+  for (int m = 0; m <= naz; ++m) {
+    const double d0 = (m == 0) ? 1.0 : 0.0;
+    legendre_flat(N, m, N, N - 1, mu.data(), ylq.data());
+    auto Yq = [&](int l, int i) { return ylq[(size_t)l * N + i]; };
+    if (do_int) legendre_flat(numu, m, numu, N - 1, umu.data(), ylu.data());
+    auto Yu = [&](int l, int iu) { return ylu[(size_t)l * numu + iu]; };
+
+    // solveEigen + interpEigenvec per layer (DisortSolver.cpp:872-1140, 2468-2504)
+    for (int lc = 0; lc < L; ++lc) {
+      const double* g = &gl[(size_t)lc * N];
+      for (int iq = 0; iq < NN; ++iq)
+        for (int jq = 0; jq < N; ++jq) {
+          double s = 0.0;
+          for (int l = m; l < N; ++l) s += (Yq(l, iq) * g[l]) * Yq(l, jq);
+          cc_top[iq * N + jq] = (s * 0.5) * wt[jq];
+        }
+      double* Cl = &C[(size_t)lc * N * N];
+      for (int iq = 0; iq < NN; ++iq)
+        for (int jq = 0; jq < N; ++jq) Cl[iq * N + jq] = cc_top[iq * N + jq];
+      for (int iq = 0; iq < NN; ++iq)
+        for (int jq = 0; jq < NN; ++jq) {
+          Cl[(NN + iq) * N + jq] = cc_top[iq * N + NN + jq];
+          Cl[(NN + iq) * N + NN + jq] = cc_top[iq * N + jq];
+        }
+      for (int iq = 0; iq < NN; ++iq) {
+        const double inv = 1.0 / mu[iq];
+        for (int jq = 0; jq < NN; ++jq) {
+          amb[iq * NN + jq] = inv * (cc_top[iq * N + jq] - cc_top[iq * N + NN + jq]);
+          apb[iq * NN + jq] = inv * (cc_top[iq * N + jq] + cc_top[iq * N + NN + jq]);
+        }
+        amb[iq * NN + iq] -= inv;
+        apb[iq * NN + iq] -= inv;
+      }
+      if (int st = layer_eigen(NN, amb.data(), apb.data(), dsim.data(), dinv.data(), ws[lc] < 1.0 - 1e-12,
+                               evec.data(), kred.data()))
+        return st;
+      double* kl = &kk[(size_t)lc * N];
+      for (int iq = 0; iq < NN; ++iq) {
+        kl[iq + NN] = kred[iq];
+        kl[NN - 1 - iq] = -kred[iq];
+      }
+      for (int i = 0; i < NN; ++i)
+        for (int j = 0; j < NN; ++j) {
+          double s = 0.0;
+          for (int k = 0; k < NN; ++k) s += amb[i * NN + k] * evec[k * NN + j];
+          gpg[i * NN + j] = s / kred[j];
+        }
+      double* Gl = &G[(size_t)lc * N * N];
+      for (int jq = 0; jq < NN; ++jq)
+        for (int iq = 0; iq < NN; ++iq) {
+          double gpplgm = gpg[iq * NN + jq];
+          const double gpmigm = evec[iq * NN + jq];
+          Gl[(NN + iq) * N + NN + jq] = 0.5 * (gpplgm + gpmigm);
+          Gl[(NN - iq - 1) * N + NN + jq] = 0.5 * (gpplgm - gpmigm);
+          gpplgm *= -1.0;
+          Gl[(NN + iq) * N + NN - jq - 1] = 0.5 * (gpplgm + gpmigm);
+          Gl[(NN - iq - 1) * N + NN - jq - 1] = 0.5 * (gpplgm - gpmigm);
+        }
+      if (do_int) {
+        // GU(iu, c) = sum_l Yu(l,iu) 0.5 gl(l) sum_jq Yq(l,jq) w(jq) G(row(jq), c)
+        auto row = [&](int jq) { return jq < NN ? NN + jq : N - 1 - jq; };
+        std::vector<double> Wl((size_t)N * N, 0.0);
+        for (int l = m; l < N; ++l)
+          for (int col = 0; col < N; ++col) {
+            double s = 0.0;
+            for (int jq = 0; jq < N; ++jq) s += (Yq(l, jq) * wt[jq]) * Gl[row(jq) * N + col];
+            Wl[(size_t)l * N + col] = s * (0.5 * g[l]);
+          }
+        for (int iu = 0; iu < numu; ++iu)
+          for (int col = 0; col < N; ++col) {
+            double s = 0.0;
+            for (int l = m; l < N; ++l) s += Yu(l, iu) * Wl[(size_t)l * N + col];
+            GU[((size_t)lc * numu + iu) * N + col] = s;
+          }
+      }
+    }
+    // beam particular solution (DisortSolver.cpp:1319-1395)
+    if (c.fbeam > 0.0) {
+      const double umu0n = -c.umu0;
+      legendre_flat(1, m, 1, N - 1, &umu0n, ylb.data());
+      const double dither = 1000.0 * std::numeric_limits<double>::epsilon();
+      for (int lc = 0; lc < L; ++lc) {
+        double beam_mu = c.umu0;
+        const double mu0sq = c.umu0 * c.umu0;
+        for (int iq = 0; iq < NN; ++iq) {
+          const double k = kk[(size_t)lc * N + iq + NN];
+          if (std::abs(1.0 - mu0sq * k * k) < dither) { beam_mu = 0.999 * c.umu0; break; }
+        }
+        const double* Cl = &C[(size_t)lc * N * N];
+        for (int i = 0; i < N; ++i)
+          for (int j = 0; j < N; ++j) A[i * N + j] = -Cl[i * N + j];
+        for (int i = 0; i < N; ++i) A[i * N + i] += 1.0 + mu[i] / beam_mu;
+        for (int iq = 0; iq < N; ++iq) {
+          double s = 0.0;
+          for (int k = m; k < N; ++k) s += gl[(size_t)lc * N + k] * Yq(k, iq) * ylb[k];
+          xv[iq] = (2.0 - d0) * c.fbeam * s / (4.0 * M_PI);
+        }
+        lu_factor(A.data(), N, N, piv.data());
+        lu_solve(A.data(), N, N, piv.data(), xv.data());
+        for (int iq = 0; iq < N; ++iq) zbraw[(size_t)lc * N + iq] = xv[iq];
+        for (int iq = 0; iq < NN; ++iq) {
+          zb[(size_t)lc * N + NN + iq] = xv[iq];
+          zb[(size_t)lc * N + NN - iq - 1] = xv[iq + NN];
+        }
+      }
+    }
+    // thermal particular solution, mode 0 (DisortSolver.cpp:1533-1648)
+    if (c.thermal && m == 0) {
+      std::vector<double> pkag(L + 1), zz1(N);
+      for (int lev = 0; lev <= L; ++lev) pkag[lev] = planck_function2(c.wlo, c.whi, c.temp[lev]);
+      for (int lc = 0; lc < L; ++lc) {
+        const double* Cl = &C[(size_t)lc * N * N];
+        for (int i = 0; i < N; ++i)
+          for (int j = 0; j < N; ++j) A[i * N + j] = -Cl[i * N + j];
+        for (int i = 0; i < N; ++i) A[i * N + i] += 1.0;
+        lu_factor(A.data(), N, N, piv.data());
+        double r1 = 0.0;
+        if (dts[lc] > 1e-4) r1 = (pkag[lc + 1] - pkag[lc]) / dts[lc];
+        const double r0 = pkag[lc] - r1 * taus[lc];
+        xr0[lc] = r0;
+        xr1[lc] = r1;
+        for (int i = 0; i < N; ++i) zz1[i] = (1.0 - ws[lc]) * r1;
+        lu_solve(A.data(), N, N, piv.data(), zz1.data());
+        for (int i = 0; i < N; ++i) bvec[i] = (1.0 - ws[lc]) * r0 + mu[i] * zz1[i];
+        lu_solve(A.data(), N, N, piv.data(), bvec.data());
+        for (int iq = 0; iq < NN; ++iq) {
+          z0[(size_t)lc * N + NN + iq] = bvec[iq];
+          z0[(size_t)lc * N + NN - iq - 1] = bvec[iq + NN];
+          z1[(size_t)lc * N + NN + iq] = zz1[iq];
+          z1[(size_t)lc * N + NN - iq - 1] = zz1[iq + NN];
+        }
+      }
+    }
+    // interpSource (DisortSolver.cpp:2506-2580)
+    if (do_int) {
+      for (int lc = 0; lc < L; ++lc) {
+        const double* g = &gl[(size_t)lc * N];
+        if (c.fbeam > 0.0) {
+          std::vector<double> psi0(N, 0.0);
+          for (int l = m; l < N; ++l) {
+            double ps = 0.0;
+            for (int jq = 0; jq < N; ++jq) ps += wt[jq] * Yq(l, jq) * zbraw[(size_t)lc * N + jq];
+            psi0[l] = 0.5 * g[l] * ps;
+          }
+          const double fact = (2.0 - d0) * c.fbeam / (4.0 * M_PI);
+          for (int iu = 0; iu < numu; ++iu) {
+            double s = 0.0;
+            for (int l = m; l < N; ++l) s += Yu(l, iu) * (psi0[l] + fact * g[l] * ylb[l]);
+            zbu[(size_t)lc * numu + iu] = s;
+          }
+        }
+        if (c.thermal && m == 0) {
+          std::vector<double> p0(N, 0.0), p1(N, 0.0);
+          for (int l = m; l < N; ++l) {
+            double s0 = 0.0, s1 = 0.0;
+            for (int jq = 0; jq < N; ++jq) {
+              const int r = jq < NN ? NN + jq : N - 1 - jq;
+              s0 += wt[jq] * Yq(l, jq) * z0[(size_t)lc * N + r];
+              s1 += wt[jq] * Yq(l, jq) * z1[(size_t)lc * N + r];
+            }
+            p0[l] = 0.5 * g[l] * s0;
+            p1[l] = 0.5 * g[l] * s1;
+          }
+          for (int iu = 0; iu < numu; ++iu) {
+            double s0 = 0.0, s1 = 0.0;
+            for (int l = m; l < N; ++l) {
+              s0 += Yu(l, iu) * p0[l];
+              s1 += Yu(l, iu) * p1[l];
+            }
+            z0u[(size_t)lc * numu + iu] = s0 + (1.0 - ws[lc]) * xr0[lc];
+            z1u[(size_t)lc * numu + iu] = s1 + (1.0 - ws[lc]) * xr1[lc];
+          }
+        }
+      }
+    }
+    // setMatrix (DisortSolver.cpp:1153-1317): Lambertian coupling only for m = 0
+    const int ncd = 3 * NN - 1, lda = 3 * ncd + 1, nshift = lda - 2 * N + 1;
+    std::vector<double> band((size_t)lda * N * L, 0.0);
+    auto BM = [&](int r, int col) -> double& { return band[(size_t)col * lda + r]; };
+    auto Gv = [&](int lc, int r, int col) { return G[(size_t)lc * N * N + r * N + col]; };
+    int ncol = 0;
+    std::vector<double> e(N, 0.0);
+    for (int lc = 0; lc < ncut; ++lc) {
+      for (int iq = 0; iq < NN; ++iq) e[iq] = std::exp(kk[(size_t)lc * N + iq] * dts[lc]);
+      int jcol = 0;
+      for (int iq = 0; iq < NN; ++iq) {
+        int irow = nshift - jcol - 1;
+        for (int jq = 0; jq < N; ++jq) {
+          if (irow + N >= 0 && irow + N < lda) BM(irow + N, ncol) = Gv(lc, jq, iq);
+          if (irow >= 0 && irow < lda) BM(irow, ncol) = -Gv(lc, jq, iq) * e[iq];
+          irow++;
+        }
+        ncol++; jcol++;
+      }
+      for (int iq = NN; iq < N; ++iq) {
+        int irow = nshift - jcol - 1;
+        for (int jq = 0; jq < N; ++jq) {
+          if (irow + N < lda) BM(irow + N, ncol) = Gv(lc, jq, iq) * e[N - iq - 1];
+          BM(irow, ncol) = -Gv(lc, jq, iq);
+          irow++;
+        }
+        ncol++; jcol++;
+      }
+    }
+    {
+      int jcol = 0;
+      for (int iq = 0; iq < NN; ++iq) {
+        const double expa = std::exp(kk[iq] * taus[1]);
+        int irow = nshift - jcol + NN - 1;
+        for (int jq = NN - 1; jq >= 0; --jq) { BM(irow, jcol) = Gv(0, jq, iq) * expa; irow++; }
+        jcol++;
+      }
+      for (int iq = NN; iq < N; ++iq) {
+        int irow = nshift - jcol + NN - 1;
+        for (int jq = NN - 1; jq >= 0; --jq) { BM(irow, jcol) = Gv(0, jq, iq); irow++; }
+        jcol++;
+      }
+      int nncol = ncol - N - 1;
+      jcol = 0;
+      const int lb = ncut - 1;
+      const bool plain = lyrcut || c.dlbc || d0 == 0.0;
+      for (int iq = 0; iq < NN; ++iq) {
+        nncol++;
+        int irow = nshift - jcol + N - 1;
+        for (int jq = NN; jq < N; ++jq) {
+          if (plain) BM(irow, nncol) = Gv(lb, jq, iq);
+          else {
+            double refl = 0.0;
+            for (int k = 0; k < NN; ++k) refl += wt[k] * mu[k] * c.alb * Gv(lb, NN - 1 - k, iq);
+            BM(irow, nncol) = Gv(lb, jq, iq) - (1.0 + d0) * refl;
+          }
+          irow++;
+        }
+        jcol++;
+      }
+      for (int iq = NN; iq < N; ++iq) {
+        nncol++;
+        int irow = nshift - jcol + N - 1;
+        const double expa = e[N - iq - 1];
+        for (int jq = NN; jq < N; ++jq) {
+          if (plain) BM(irow, nncol) = Gv(lb, jq, iq) * expa;
+          else {
+            double refl = 0.0;
+            for (int k = 0; k < NN; ++k) refl += wt[k] * mu[k] * c.alb * Gv(lb, NN - 1 - k, iq);
+            BM(irow, nncol) = (Gv(lb, jq, iq) - (1.0 + d0) * refl) * expa;
+          }
+          irow++;
+        }
+        jcol++;
+      }
+    }
+    // solve0 (DisortSolver.cpp:1669-1974)
+    const int nc = N * ncut;
+    std::vector<double> b(nc, 0.0);
+    const int lb = ncut - 1;
+    auto ZB = [&](int lc, int i) { return zb[(size_t)lc * N + i]; };
+    auto Z0 = [&](int lc, int i) { return z0[(size_t)lc * N + i]; };
+    auto Z1 = [&](int lc, int i) { return z1[(size_t)lc * N + i]; };
+    const bool beam = c.fbeam > 0.0;
+    if (m > 0) {
+      if (beam) {
+        for (int iq = 0; iq < NN; ++iq) b[iq] = -ZB(0, NN - 1 - iq);
+        for (int iq = 0; iq < NN; ++iq) b[nc - NN + iq] = -ZB(lb, NN + iq) * btr[ncut];
+        for (int lc = 1; lc < ncut; ++lc)
+          for (int iq = 0; iq < N; ++iq) b[lc * N - NN + iq] = (ZB(lc, iq) - ZB(lc - 1, iq)) * btr[lc];
+      }
+    } else {
+      for (int iq = 0; iq < NN; ++iq) {
+        double s = 0.0;
+        if (beam) s -= ZB(0, NN - iq - 1);
+        if (c.thermal) s -= Z0(0, NN - iq - 1);
+        s += c.fisot + ptop;
+        b[iq] = s;
+      }
+      if (c.dlbc) {
+        for (int iq = 0; iq < NN; ++iq) {
+          double s = 0.0;
+          if (beam) s -= ZB(lb, NN + iq) * btr[ncut];
+          if (c.thermal) { s -= Z0(lb, NN + iq); s -= Z1(lb, NN + iq) * taus[ncut]; }
+          s += pbot + mu[iq] * pbotd;
+          b[nc - NN + iq] = s;
+        }
+      } else {
+        for (int iq = 0; iq < NN; ++iq) {
+          double s = 0.0;
+          if (!lyrcut) {
+            double refl = 0.0;
+            for (int jq = 0; jq < NN; ++jq) {
+              double ps = 0.0;
+              if (beam) ps += ZB(lb, NN - 1 - jq) * btr[ncut];
+              if (c.thermal) ps += Z0(lb, NN - 1 - jq) + Z1(lb, NN - 1 - jq) * taus[ncut];
+              refl += wt[jq] * mu[jq] * c.alb * ps;
+            }
+            s += 2.0 * refl;
+          }
+          if (beam) {
+            s -= ZB(lb, NN + iq) * btr[ncut];
+            if (!lyrcut) s += c.alb * c.umu0 * c.fbeam * btr[ncut] / M_PI;
+          }
+          if (c.thermal) { s -= Z0(lb, NN + iq); s -= Z1(lb, NN + iq) * taus[ncut]; }
+          s += c.fisob;
+          if (c.thermal) s += (1.0 - c.alb) * pbot;
+          b[nc - NN + iq] = s;
+        }
+      }
+      for (int lc = 1; lc < ncut; ++lc)
+        for (int iq = 0; iq < N; ++iq) {
+          double s = 0.0;
+          if (beam) { s += ZB(lc, iq) * btr[lc]; s -= ZB(lc - 1, iq) * btr[lc]; }
+          if (c.thermal) {
+            s += Z0(lc, iq) - Z0(lc - 1, iq);
+            s += (Z1(lc, iq) - Z1(lc - 1, iq)) * taus[lc];
+          }
+          b[lc * N - NN + iq] = s;
+        }
+    }
+    std::vector<int> ipvt(nc);
+    if (!band_factor(band.data(), lda, nc, ncd, ncd, ipvt.data())) status = DSP_ERR_SINGULAR;
+    band_solve(band.data(), lda, nc, ncd, ncd, ipvt.data(), b.data());
+    std::fill(cc.begin(), cc.end(), 0.0);
+    for (int k = 0; k < nc; ++k) cc[k] = b[k];  // the reference's reorder is the identity
+    auto CCv = [&](int lc, int i) { return cc[(size_t)lc * N + i]; };
+
+    // computeFluxes (DisortSolver.cpp:1980-2124), mode 0
+    if (m == 0) {
+      for (int lu = 0; lu < ntau; ++lu) {
+        const int y = lyr[lu];
+        if (lyrcut && y > ncut - 1) continue;  // zeros
+        const double u = utaus[lu];
+        double fact = 0, dirint = 0, fldir = 0, fdir = 0;
+        if (beam) {
+          fact = std::exp(-u / c.umu0);
+          fdir = c.umu0 * c.fbeam * std::exp(-utau[lu] / c.umu0);
+          dirint = c.fbeam * fact;
+          fldir = c.umu0 * c.fbeam * fact;
+        }
+        std::vector<double> ec(N), in(N);
+        for (int jq = 0; jq < NN; ++jq) ec[jq] = CCv(y, jq) * std::exp(-kk[(size_t)y * N + jq] * (u - taus[y + 1]));
+        for (int jq = NN; jq < N; ++jq) ec[jq] = CCv(y, jq) * std::exp(-kk[(size_t)y * N + jq] * (u - taus[y]));
+        for (int i = 0; i < N; ++i) {
+          double s = 0.0;
+          for (int j = 0; j < N; ++j) s += Gv(y, i, j) * ec[j];
+          in[i] = s;
+        }
+        if (beam) for (int i = 0; i < N; ++i) in[i] += ZB(y, i) * fact;
+        if (c.thermal) for (int i = 0; i < N; ++i) in[i] += Z0(y, i) + Z1(y, i) * u;
+        double ua = 0, uad = 0, uau = 0, fldn = 0, fup = 0;
+        for (int iq = 0; iq < NN; ++iq) {
+          const int cw = NN - iq - 1;
+          ua += wt[cw] * in[iq]; uad += wt[cw] * in[iq]; fldn += wt[cw] * in[iq] * mu[cw];
+        }
+        for (int iq = NN; iq < N; ++iq) {
+          const int cw = iq - NN;
+          ua += wt[cw] * in[iq]; uau += wt[cw] * in[iq]; fup += wt[cw] * in[iq] * mu[cw];
+        }
+        fup *= 2.0 * M_PI;
+        fldn *= 2.0 * M_PI;
+        const double fdn = (fldn + fldir) - fdir;
+        ua = (2.0 * M_PI * ua + dirint) / (4.0 * M_PI);
+        const double uaso = dirint / (4.0 * M_PI);
+        uad = (2.0 * M_PI * uad) / (4.0 * M_PI);
+        uau = (2.0 * M_PI * uau) / (4.0 * M_PI);
+        double pls = 0.0;
+        if (c.thermal) pls = xr0[y] + xr1[y] * u;
+        const double dfdt = (1.0 - c.ssa[y]) * 4.0 * M_PI * (ua - pls);
+        const double o[8] = {fdir, fdn, fup, dfdt, ua, uad, uau, uaso};
+        for (int f = 0; f < 8; ++f) out.flux[f][lu] = o[f];
+      }
+    }
+
+    // computeUserIntensities (DisortSolver.cpp:2938-3268)
+    if (do_int) {
+      for (int lc = 0; lc < ncut; ++lc)
+        for (int iq = 0; iq < N; ++iq)
+          for (int iu = 0; iu < numu; ++iu) GU[((size_t)lc * numu + iu) * N + iq] *= CCv(lc, iq);
+      auto gu = [&](int lc, int iu, int iq) { return GU[((size_t)lc * numu + iu) * N + iq]; };
+      std::vector<double> wk(NN), wkc(NN), wkb(NN);
+      for (int lu = 0; lu < ntau; ++lu) {
+        double exp0 = 0.0;
+        if (beam) exp0 = std::exp(-utaus[lu] / c.umu0);
+        const int y = lyr[lu];
+        for (int iu = 0; iu < numu; ++iu) {
+          const double um = umu[iu];
+          double& Iout = Im[(size_t)lu * numu + iu];
+          if (lyrcut && y >= ncut) { Iout = 0.0; continue; }
+          const bool neg = um < 0.0;
+          int ls, le;
+          double sgn;
+          if (neg) { ls = 0; le = y - 1; sgn = -1.0; }
+          else { ls = y + 1; le = ncut - 1; sgn = 1.0; }
+          double palint = 0.0, plkint = 0.0;
+          for (int lc = ls; lc <= le; ++lc) {
+            const double dt = dts[lc];
+            const double e1 = std::exp((utaus[lu] - taus[lc]) / um);
+            const double e2 = std::exp((utaus[lu] - taus[lc + 1]) / um);
+            if (c.thermal && m == 0) {
+              const double f0n = sgn * (e1 - e2);
+              const double f1n = sgn * ((taus[lc] + um) * e1 - (taus[lc + 1] + um) * e2);
+              plkint += z0u[(size_t)lc * numu + iu] * f0n + z1u[(size_t)lc * numu + iu] * f1n;
+            }
+            if (beam) {
+              const double den = 1.0 + um / c.umu0;
+              double expn;
+              if (std::abs(den) < 0.0001) expn = (dt / c.umu0) * exp0;
+              else expn = (e1 * btr[lc] - e2 * btr[lc + 1]) * sgn / den;
+              palint += zbu[(size_t)lc * numu + iu] * expn;
+            }
+            for (int iq = 0; iq < NN; ++iq) {
+              const double kq = kk[(size_t)lc * N + iq];
+              wk[iq] = std::exp(kq * dt);
+              const double den = 1.0 + um * kq;
+              double expn;
+              if (std::abs(den) < 0.0001) expn = (dt / um) * e2;
+              else expn = sgn * (e1 * wk[iq] - e2) / den;
+              palint += gu(lc, iu, iq) * expn;
+            }
+            for (int iq = NN; iq < N; ++iq) {
+              const double den = 1.0 + um * kk[(size_t)lc * N + iq];
+              double expn;
+              if (std::abs(den) < 0.0001) expn = -(dt / um) * e1;
+              else expn = sgn * (e1 - e2 * wk[N - 1 - iq]) / den;
+              palint += gu(lc, iu, iq) * expn;
+            }
+          }
+          const double dt1 = utaus[lu] - taus[y], dt2 = utaus[lu] - taus[y + 1];
+          if ((std::abs(dt1) >= 1e-6 || !neg) && (std::abs(dt2) >= 1e-6 || neg)) {
+            double e1c = 0.0, e2c = 0.0;
+            if (neg) e1c = std::exp(dt1 / um);
+            else e2c = std::exp(dt2 / um);
+            if (beam) {
+              const double den = 1.0 + um / c.umu0;
+              double expn;
+              if (std::abs(den) < 0.0001) expn = (dt1 / c.umu0) * exp0;
+              else if (neg) expn = (exp0 - btr[y] * e1c) / den;
+              else expn = (exp0 - btr[y + 1] * e2c) / den;
+              palint += zbu[(size_t)y * numu + iu] * expn;
+            }
+            const double dty = dts[y];
+            for (int iq = 0; iq < NN; ++iq) {
+              const double kq = kk[(size_t)y * N + iq];
+              const double den = 1.0 + um * kq;
+              double expn;
+              if (std::abs(den) < 0.0001) expn = -dt2 / um * e2c;
+              else if (neg) expn = (std::exp(-kq * dt2) - std::exp(kq * dty) * e1c) / den;
+              else expn = (std::exp(-kq * dt2) - e2c) / den;
+              wkc[iq] = std::exp(kq * dty);
+              palint += gu(y, iu, iq) * expn;
+            }
+            for (int iq = NN; iq < N; ++iq) {
+              const double kq = kk[(size_t)y * N + iq];
+              const double den = 1.0 + um * kq;
+              double expn;
+              if (std::abs(den) < 0.0001) expn = -(dt1 / um) * e1c;
+              else if (neg) expn = (std::exp(-kq * dt1) - e1c) / den;
+              else expn = (std::exp(-kq * dt1) - std::exp(-kq * dty) * e2c) / den;
+              palint += gu(y, iu, iq) * expn;
+            }
+            if (c.thermal && m == 0) {
+              double expn, fact;
+              if (neg) { expn = e1c; fact = taus[y] + um; }
+              else { expn = e2c; fact = taus[y + 1] + um; }
+              const double f0n = 1.0 - expn;
+              const double f1n = utaus[lu] + um - fact * expn;
+              plkint += z0u[(size_t)y * numu + iu] * f0n + z1u[(size_t)y * numu + iu] * f1n;
+            }
+          }
+          double bndint = 0.0;
+          if (neg && m == 0) {
+            bndint = (c.fisot + ptop) * std::exp(utaus[lu] / um);
+          } else if (!neg) {
+            if (c.dlbc) {
+              if (lyrcut || m > 0) { Iout = palint + plkint; continue; }
+              bndint = (pbot + um * pbotd) * std::exp((utaus[lu] - taus[L]) / um);
+            } else if (lyrcut || m > 0) {
+              Iout = palint + plkint;
+              continue;
+            } else {
+              // Lambertian surface at user angles (DisortSolver.cpp:2655-2662): set only for mu > 0
+              const double rho_u = um > 0.0 ? c.alb : 0.0, emis_u = um > 0.0 ? 1.0 - c.alb : 0.0;
+              for (int jq = NN; jq < N; ++jq) wkb[jq - NN] = std::exp(-kk[(size_t)(L - 1) * N + jq] * dts[L - 1]);
+              double bnddfu = 0.0;
+              for (int iq = NN - 1; iq >= 0; --iq) {
+                double dfu = 0.0;
+                for (int jq = 0; jq < NN; ++jq) dfu += Gv(L - 1, iq, jq) * CCv(L - 1, jq);
+                for (int jq = NN; jq < N; ++jq) dfu += Gv(L - 1, iq, jq) * CCv(L - 1, jq) * wkb[jq - NN];
+                if (beam) dfu += ZB(L - 1, iq) * btr[L];
+                dfu += d0 * (Z0(L - 1, iq) + Z1(L - 1, iq) * taus[L]);
+                bnddfu += (1.0 + d0) * rho_u * mu[NN - iq - 1] * wt[NN - iq - 1] * dfu;
+              }
+              const double bnddir = c.umu0 * c.fbeam / M_PI * rho_u * btr[L];
+              bndint = (bnddfu + bnddir + d0 * emis_u * pbot + c.fisob) * std::exp((utaus[lu] - taus[L]) / um);
+            }
+          }
+          Iout = palint + plkint + bndint;
+        }
+      }
+      if (m == 0) {
+        for (int lu = 0; lu < ntau; ++lu)
+          for (int iu = 0; iu < numu; ++iu) {
+            const double v = Im[(size_t)lu * numu + iu];
+            out.iavg[(size_t)lu * out.numu_out + iu] = v;
+            for (int j = 0; j < nphi; ++j) I3(lu, iu, j) = v;
+          }
+      } else {
+        double maxc = 0.0;
+        for (int j = 0; j < nphi; ++j) {
+          const double phirad = (c.phi[j] - c.phi0) * M_PI / 180.0;
+          const double cosphi = std::cos(static_cast<double>(m) * phirad);
+          for (int lu = 0; lu < ntau; ++lu)
+            for (int iu = 0; iu < numu; ++iu) {
+              const double az = Im[(size_t)lu * numu + iu] * cosphi;
+              I3(lu, iu, j) += az;
+              const double uu = std::abs(I3(lu, iu, j));
+              double ratio;
+              if (uu == 0.0) ratio = 1.0 + std::abs(az);
+              else if (std::abs(az) == 0.0) ratio = 0.0;
+              else ratio = std::abs(az) / uu;
+              maxc = std::max(maxc, ratio);
+            }
+        }
+        if (c.accur > 0.0) {
+          if (maxc <= c.accur) ++kconv;
+          if (kconv >= 2) break;
+        }
+      }
+    }
+  }
+  if (c.ifb) {  // reverseOutputArrays (IndexConversion.hpp:60-80): the level axis
+    for (int f = 0; f < 8; ++f) std::reverse(out.flux[f], out.flux[f] + ntau);
+    if (do_int) {
+      const size_t row3 = (size_t)out.numu_out * nphi, row2 = out.numu_out;
+      for (int a = 0, z = ntau - 1; a < z; ++a, --z) {
+        for (size_t k = 0; k < row3; ++k) std::swap(out.intensity[a * row3 + k], out.intensity[z * row3 + k]);
+        for (size_t k = 0; k < row2; ++k) std::swap(out.iavg[a * row2 + k], out.iavg[z * row2 + k]);
+      }
+    }
+  }
+  return status;
+}
+
+}  // namespace oracle

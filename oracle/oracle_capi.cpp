@@ -10,7 +10,7 @@
 // host pointers.
 #include <omp.h>
 
-#include "flux_oracle.hpp"
+#include "general_oracle.hpp"
 
 namespace {
 inline const double* at(const dsp_darray& a, int64_t i) {
@@ -70,6 +70,88 @@ int oracle_flux_bands_solve(const dsp_flux_batch* b, const dsp_flux_out* o, int 
         st = DSP_ERR_INVALID_INPUT;
       } else {
         st = solver.solve(c, fo);
+      }
+      if (o->status) o->status[i] = st;
+      if (st > local_worst) local_worst = st;
+    }
+#pragma omp critical
+    if (local_worst > worst) worst = local_worst;
+  }
+  return worst;
+}
+
+// The general batch (DisortSolver::solve per instance), same static-schedule
+// OpenMP loop as the flux batch.  Instances are ragged: instance i owns layers
+// layer_offset[i] .. layer_offset[i+1]-1 and levels layer_offset[i] + i ..
+// layer_offset[i+1] + i.
+int oracle_general_bands_solve(const dsp_general_batch* b, const dsp_general_out* o, int nthreads) {
+  if (!b || !o || b->n_inst < 0) return DSP_ERR_INVALID_INPUT;
+  const int n = b->n_inst;
+  const uint32_t fl = b->flags;
+  const int64_t ntau_o = o->ntau_out, numu_o = o->numu_out, nphi = b->num_phi > 0 ? b->num_phi : 0;
+  int worst = DSP_OK;
+  if (nthreads <= 0) nthreads = omp_get_max_threads();
+#pragma omp parallel num_threads(nthreads)
+  {
+    oracle::GeneralOracle solver;
+    int local_worst = DSP_OK;
+#pragma omp for schedule(static)
+    for (int i = 0; i < n; ++i) {
+      oracle::GeneralInstance c;
+      int st = DSP_OK;
+      if (!b->num_streams || !b->num_layers || !b->layer_offset || !b->num_phase_func_moments ||
+          !b->delta_tau || !b->single_scat_albedo || !b->phase_function_moments) {
+        st = DSP_ERR_INVALID_INPUT;
+      } else {
+        const int64_t l0 = b->layer_offset[i];
+        c.L = b->num_layers[i];
+        c.N = b->num_streams[i];
+        c.nmom = b->num_phase_func_moments[i];
+        c.pc = b->pmom_count;
+        c.thermal = (fl & DSP_FLAG_THERMAL) != 0;
+        c.dmplus = (fl & DSP_FLAG_DELTA_M_PLUS) != 0;
+        c.dlbc = (fl & DSP_FLAG_DIFFUSION_LOWER_BC) != 0;
+        c.ifb = (fl & DSP_FLAG_INDEX_FROM_BOTTOM) != 0;
+        c.user_tau = (fl & DSP_GFLAG_USER_TAU) != 0;
+        c.user_mu = (fl & DSP_GFLAG_USER_MU) != 0;
+        c.only_fluxes = (fl & DSP_GFLAG_ONLY_FLUXES) != 0;
+        c.accur = b->accuracy_fourier_series;
+        c.wlo = scalar(b->wavenumber_low, i, 0.0);
+        c.whi = scalar(b->wavenumber_high, i, 0.0);
+        c.alb = scalar(b->surface_albedo, i, 0.0);
+        c.emis = scalar(b->emissivity_top, i, 1.0);
+        c.fbeam = scalar(b->direct_beam_flux, i, 0.0);
+        c.umu0 = scalar(b->direct_beam_mu, i, 0.5);
+        c.phi0 = scalar(b->direct_beam_phi, i, 0.0);
+        c.fisot = scalar(b->isotropic_flux_top, i, 0.0);
+        c.fisob = scalar(b->isotropic_flux_bottom, i, 0.0);
+        c.ttop = scalar(b->temperature_top, i, 0.0);
+        c.tbot = scalar(b->temperature_bottom, i, 0.0);
+        c.dtau = b->delta_tau + l0;
+        c.ssa = b->single_scat_albedo + l0;
+        c.pmom = b->phase_function_moments + l0 * b->pmom_count;
+        c.temp = b->temperature ? b->temperature + l0 + i : nullptr;
+        c.ntau = b->num_user_tau;
+        c.numu = b->num_user_mu;
+        c.nphi = b->num_phi;
+        c.utau = at(b->tau_user, i);
+        c.umu = at(b->mu_user, i);
+        c.phi = at(b->phi_user, i);
+        const int ntau = c.user_tau ? c.ntau : c.L + 1;
+        const int numu = (c.user_mu && !c.only_fluxes) ? c.numu : c.N;
+        if ((fl & (DSP_FLAG_SPHERICAL_BEAM | DSP_FLAG_TEMPERATURE_JAC)) != 0) st = DSP_ERR_UNSUPPORTED;
+        else if (c.L > 0 && b->layer_offset[i + 1] - l0 != c.L) st = DSP_ERR_INVALID_INPUT;
+        else if (ntau > ntau_o || numu > numu_o || c.N > 64) st = DSP_ERR_INVALID_INPUT;
+        else {
+          oracle::GeneralOutput go;
+          for (int f = 0; f < 8; ++f) go.flux[f] = o->flux[f] + ntau_o * i;
+          go.intensity = o->intensity ? o->intensity + (ntau_o * numu_o * nphi) * i : nullptr;
+          go.iavg = o->intensity_azimuth_avg ? o->intensity_azimuth_avg + (ntau_o * numu_o) * i : nullptr;
+          go.ntau_out = (int)ntau_o;
+          go.numu_out = (int)numu_o;
+          if (!c.only_fluxes && c.user_mu && (!go.intensity || !go.iavg)) st = DSP_ERR_INVALID_INPUT;
+          else st = solver.solve(c, go);
+        }
       }
       if (o->status) o->status[i] = st;
       if (st > local_worst) local_worst = st;

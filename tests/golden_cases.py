@@ -48,3 +48,37 @@ def level_of(c: dict, index: int):
     cum = np.concatenate([[0.0], np.cumsum(c["delta_tau"])])
     hit = np.nonzero(np.abs(cum - tau) <= 1e-9 * max(1.0, abs(tau)))[0]
     return int(hit[0]) if hit.size else None
+
+
+def general_instance(c: dict) -> tuple[dict, int]:
+    """A golden case as one instance of the general batch, with its flags.
+
+    Cases without user polar angles are fluxes-only runs (use_user_mu = false
+    computes no intensities, so only the mode-0 fluxes are compared)."""
+    flags = 0
+    if c["use_thermal_emission"]:
+        flags |= capi.FLAG_THERMAL
+    if c["use_delta_m_plus"]:
+        flags |= capi.FLAG_DELTA_M_PLUS
+    inst = dict(
+        num_streams=c["num_streams"], num_layers=c["num_layers"],
+        num_phase_func_moments=c["num_phase_func_moments"],
+        delta_tau=c["delta_tau"], single_scat_albedo=c["single_scat_albedo"],
+        phase_function_moments=c["phase_function_moments"],
+        temperature=c["temperature"] if c["use_thermal_emission"] else None,
+        wavenumber_low=c["wavenumber_low"], wavenumber_high=c["wavenumber_high"],
+        surface_albedo=c["surface_albedo"], emissivity_top=c["emissivity_top"],
+        direct_beam_flux=c["direct_beam_flux"], direct_beam_mu=c["direct_beam_mu"],
+        isotropic_flux_top=c["isotropic_flux_top"],
+        temperature_top=c["temperature_top"], temperature_bottom=c["temperature_bottom"],
+    )
+    if c["tau_user"] is not None:
+        flags |= capi.GFLAG_USER_TAU
+        inst["tau_user"] = c["tau_user"]
+    if c["mu_user"] is not None:
+        flags |= capi.GFLAG_USER_MU
+        inst["mu_user"] = c["mu_user"]
+        inst["phi_user"] = c["phi_user"]
+    else:
+        flags |= capi.GFLAG_ONLY_FLUXES
+    return inst, flags

@@ -51,3 +51,47 @@ def flux_solve_device(w: dict, extra_flags: int = 0):
     rc = ctx.flux_bands_solve(batch, o)
     torch.cuda.synchronize()
     return {k: v.cpu().numpy() for k, v in outs.items()}, status.cpu().numpy(), rc
+
+
+def general_solve(d: dict):
+    """Host-pointer general solve of a pack_general dict: (outputs dict, return code)."""
+    ctx = context()
+    batch, keep = capi.make_general_batch(d)
+    outs, o, keep2 = capi.alloc_general_out_numpy(d)
+    rc = ctx.general_bands_solve(batch, o)
+    return outs, rc
+
+
+def general_solve_device(d: dict):
+    """Device-pointer general solve: every batch array and output is a CUDA tensor."""
+    import torch
+    ctx = context()
+    dd = dict(d)
+    keep = []
+    for k in ("num_streams", "num_layers", "layer_offset", "num_phase_func_moments", "delta_tau",
+              "single_scat_albedo", "phase_function_moments", "temperature") + capi.GENERAL_SCALAR_FIELDS:
+        dd[k] = torch.from_numpy(np.ascontiguousarray(d[k])).cuda()
+    for k in ("tau_user", "mu_user", "phi_user"):
+        if k in d:
+            a, stride = d[k]
+            dd[k] = (torch.from_numpy(np.ascontiguousarray(a)).cuda(), stride)
+    dd["flags"] = d["flags"] | capi.FLAG_DEVICE_POINTERS
+    batch, keep = capi.make_general_batch(dd)
+    n, nt, nu, nphi = d["n_inst"], d["ntau_out"], d["numu_out"], max(d["num_phi"], 0)
+    outs = {f: torch.full((n, nt), float("nan"), dtype=torch.float64, device="cuda") for f in capi.FLUX_OUT_FIELDS}
+    outs["intensity"] = torch.full((n, nt, nu, nphi), float("nan"), dtype=torch.float64, device="cuda")
+    outs["intensity_azimuth_avg"] = torch.full((n, nt, nu), float("nan"), dtype=torch.float64, device="cuda")
+    outs["status"] = torch.full((n,), -1, dtype=torch.int32, device="cuda")
+    o = capi.GeneralOut()
+    import ctypes
+    for k, f in enumerate(capi.FLUX_OUT_FIELDS):
+        o.flux[k] = ctypes.cast(ctypes.c_void_p(outs[f].data_ptr()), ctypes.POINTER(ctypes.c_double))
+    o.intensity = ctypes.cast(ctypes.c_void_p(outs["intensity"].data_ptr()), ctypes.POINTER(ctypes.c_double))
+    o.intensity_azimuth_avg = ctypes.cast(ctypes.c_void_p(outs["intensity_azimuth_avg"].data_ptr()),
+                                          ctypes.POINTER(ctypes.c_double))
+    o.status = ctypes.cast(ctypes.c_void_p(outs["status"].data_ptr()), ctypes.POINTER(ctypes.c_int32))
+    o.ntau_out, o.numu_out = nt, nu
+    ctx.set_stream(torch.cuda.current_stream().cuda_stream)
+    rc = ctx.general_bands_solve(batch, o)
+    torch.cuda.synchronize()
+    return {k: v.cpu().numpy() for k, v in outs.items()}, rc

@@ -34,8 +34,8 @@ def load(native: bool = False):
     lib.oracle_quadrature.argtypes = [c_int, POINTER(c_double), POINTER(c_double), POINTER(c_double)]
     lib.oracle_planck.restype = c_double
     lib.oracle_planck.argtypes = [c_double, c_double, c_double]
-    if hasattr(lib, "oracle_general_bands_solve"):
-        pass
+    lib.oracle_general_bands_solve.restype = c_int
+    lib.oracle_general_bands_solve.argtypes = [POINTER(capi.GeneralBatch), POINTER(capi.GeneralOut), c_int]
     if not native:
         _LIB = lib
     return lib
@@ -51,3 +51,12 @@ def flux_solve(w: dict, nthreads: int = 0, extra_flags: int = 0):
     o, keep2 = capi.make_flux_out(outs, status)
     lib.oracle_flux_bands_solve(ctypes.byref(batch), ctypes.byref(o), nthreads)
     return outs, status
+
+
+def general_solve(d: dict, nthreads: int = 0):
+    """Run the general oracle on a pack_general dict; returns the outputs dict."""
+    lib = load()
+    batch, keep = capi.make_general_batch(d)
+    outs, o, keep2 = capi.alloc_general_out_numpy(d)
+    lib.oracle_general_bands_solve(ctypes.byref(batch), ctypes.byref(o), nthreads)
+    return outs

@@ -30,3 +30,35 @@ def assert_parity(gpu: dict, ref: dict, label: str = ""):
     w, where = worst(gpu, ref)
     assert w <= 1.0, f"{label}: parity ratio {w:.3g} at {where}"
     return w
+
+
+GENERAL_FIELDS = capi.FLUX_OUT_FIELDS + ("intensity", "intensity_azimuth_avg")
+
+
+def worst_general(gpu: dict, ref: dict, rtol: float = RTOL) -> tuple[float, str]:
+    """parity ratio of a general solve: fluxes element-wise as worst(); each
+    instance's intensities against the largest |intensity| of that instance
+    (the Fourier sum cancels, so single elements can be near zero)."""
+    w, where = 0.0, ""
+    for f in GENERAL_FIELDS:
+        a, b = np.asarray(gpu[f]), np.asarray(ref[f])
+        if f.startswith("intensity"):
+            flat = np.abs(np.where(np.isnan(b), 0.0, b)).reshape(b.shape[0], -1)
+            scale = flat.max(axis=1).reshape((-1,) + (1,) * (b.ndim - 1))
+            denom = rtol * np.maximum(np.abs(b), scale) + ATOL
+        else:
+            denom = rtol * np.abs(b) + ATOL
+        both_nan = np.isnan(a) & np.isnan(b)
+        r = np.where(both_nan, 0.0, np.abs(a - b) / denom)
+        r = np.where(np.isnan(r), np.inf, r)
+        k = float(r.max()) if r.size else 0.0
+        if k > w:
+            idx = np.unravel_index(int(np.argmax(r)), r.shape)
+            w, where = k, f"{f}{tuple(int(x) for x in idx)} gpu={a[idx]!r} ref={b[idx]!r}"
+    return w, where
+
+
+def assert_parity_general(gpu: dict, ref: dict, label: str = "", rtol: float = RTOL):
+    w, where = worst_general(gpu, ref, rtol)
+    assert w <= 1.0, f"{label}: parity ratio {w:.3g} at {where}"
+    return w

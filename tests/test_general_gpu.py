@@ -1,0 +1,158 @@
+"""GPU parity of the general path (dsp_general_bands_solve) against the CPU oracle.
+
+Every test calls libdsp.so through its C ABI with the same dsp_general_batch
+the oracle receives.  Fluxes must agree element-wise within 1e-9 relative plus
+1e-12 absolute; intensities within 1e-9 of max(|value|, the instance's largest
+|intensity|) plus 1e-12 (an intensity is a Fourier sum over azimuth modes whose
+terms cancel, so a single element can sit far below the field it comes from).
+"""
+import numpy as np
+import pytest
+
+import golden_cases
+import gpu_lib
+import oracle_lib
+from disort_b200 import capi, workloads
+from parity import assert_parity_general
+
+pytestmark = pytest.mark.gpu
+CASES = golden_cases.load_cases()
+
+
+def both(insts, flags, accuracy=0.0):
+    d = capi.pack_general(insts, flags, accuracy_fourier_series=accuracy)
+    ref = oracle_lib.general_solve(d)
+    got, rc = gpu_lib.general_solve(d)
+    assert rc == 0, gpu_lib.context().last_error()
+    return got, ref, d
+
+
+@pytest.mark.parametrize("case", CASES, ids=[c["name"] for c in CASES])
+def test_general_reference_goldens(case):
+    inst, flags = golden_cases.general_instance(case)
+    got, ref, _ = both([inst], flags)
+    assert got["status"][0] == ref["status"][0] == 0
+    rtol = 1e-8 if max(case["single_scat_albedo"]) >= 1.0 else 1e-9
+    assert_parity_general(got, ref, case["name"], rtol=rtol)
+    for e in case["expect_flux"]:
+        assert abs(got[e["field"]][0, e["index"]] - e["value"]) <= e["tol"]
+    for e in case["expect_intensity"]:
+        assert abs(got["intensity"][0, e["lu"], e["iu"], e["j"]] - e["value"]) <= e["tol"]
+
+
+@pytest.mark.parametrize("nstr", [(4, 8), (16,), (6, 10, 12, 14), (32,)])
+def test_general_mix_small(nstr):
+    insts, flags = workloads.general_mix(24, seed=30 + len(nstr), nstr=nstr, layers=(2, 12))
+    got, ref, _ = both(insts, flags)
+    assert np.all(got["status"] == 0) and np.all(ref["status"] == 0)
+    assert_parity_general(got, ref, f"general mix N={nstr}")
+
+
+def test_general_mix_n64():
+    insts, flags = workloads.general_mix(2, seed=41, nstr=(64,), layers=(3, 5))
+    got, ref, _ = both(insts, flags)
+    assert np.all(got["status"] == 0)
+    assert_parity_general(got, ref, "general mix N=64")
+
+
+def test_general_ragged_mixed_streams_one_batch():
+    """One batch holding every supported stream count and ragged layer counts."""
+    insts = []
+    for k, N in enumerate(capi.SUPPORTED_NSTR[:-1]):
+        part, flags = workloads.general_mix(2, seed=50 + k, nstr=(N,) if N in workloads.GENERAL_NSTR else (4,),
+                                            layers=(1, 9))
+        for p in part:
+            if p["num_streams"] != N:  # stream counts outside the mix's set
+                p["num_streams"] = N
+                p["num_phase_func_moments"] = N + 1
+                p["phase_function_moments"] = workloads.hg_moments(p["phase_function_moments"][:, 1], N + 2)
+        insts += part
+    got, ref, _ = both(insts, flags)
+    assert np.all(got["status"] == 0)
+    assert_parity_general(got, ref, "ragged mixed-N batch")
+
+
+@pytest.mark.parametrize("kind", ["thermal", "thermal_beam", "dlbc", "ifb", "levels", "only_fluxes"])
+def test_general_sources_and_options(kind):
+    rng = np.random.default_rng(7)
+    insts = []
+    for k in range(6):
+        N = (4, 8, 16)[k % 3]
+        L = int(rng.integers(2, 9))
+        g = rng.uniform(0.1, 0.9, L)
+        inst = dict(num_streams=N, num_layers=L, num_phase_func_moments=0,
+                    delta_tau=np.clip(rng.lognormal(-1.0, 1.5, L), 1e-6, 20.0),
+                    single_scat_albedo=rng.uniform(0.0, 0.95, L), phase_function_moments=workloads.hg_moments(g, N + 1),
+                    surface_albedo=float(rng.uniform(0, 0.5)), tau_user=[0.0, 0.3, 1.0],
+                    mu_user=[-0.9, -0.3, 0.2, 0.7], phi_user=[0.0, 30.0, 200.0])
+        if kind.startswith("thermal") or kind in ("dlbc", "ifb"):
+            inst.update(temperature=200.0 + 100.0 * np.arange(L + 1) / L, wavenumber_low=600.0,
+                        wavenumber_high=640.0, temperature_bottom=310.0, temperature_top=40.0, emissivity_top=0.8)
+        if kind in ("thermal_beam", "ifb", "levels", "only_fluxes"):
+            inst.update(direct_beam_flux=2.0, direct_beam_mu=float(rng.uniform(0.2, 0.95)), direct_beam_phi=25.0,
+                        isotropic_flux_top=0.2, isotropic_flux_bottom=0.1)
+        insts.append(inst)
+    flags = capi.GFLAG_USER_TAU | capi.GFLAG_USER_MU
+    if kind in ("thermal", "thermal_beam", "dlbc", "ifb"):
+        flags |= capi.FLAG_THERMAL
+    if kind == "dlbc":
+        flags |= capi.FLAG_DIFFUSION_LOWER_BC
+    if kind == "ifb":
+        flags |= capi.FLAG_INDEX_FROM_BOTTOM
+    if kind == "levels":
+        flags &= ~capi.GFLAG_USER_TAU
+    if kind == "only_fluxes":
+        flags |= capi.GFLAG_ONLY_FLUXES
+    got, ref, _ = both(insts, flags)
+    assert np.all(got["status"] == 0) and np.all(ref["status"] == 0)
+    assert_parity_general(got, ref, kind)
+
+
+def test_general_absorption_cut():
+    """Deep absorbing beam-only columns: levels below the cut are zero."""
+    rng = np.random.default_rng(9)
+    insts = []
+    for k in range(4):
+        L = 6
+        insts.append(dict(num_streams=8, num_layers=L, num_phase_func_moments=0,
+                          delta_tau=np.array([2.0, 5.0, 8.0, 10.0, 3.0, 1.0]) * (1 + 0.1 * k),
+                          single_scat_albedo=np.full(L, 0.2), phase_function_moments=workloads.hg_moments(np.full(L, 0.6), 9),
+                          direct_beam_flux=1.0, direct_beam_mu=0.4 + 0.1 * k, surface_albedo=0.3,
+                          tau_user=[0.0, 3.0, 40.0], mu_user=[-0.5, 0.5], phi_user=[0.0, 90.0]))
+    got, ref, _ = both(insts, capi.GFLAG_USER_TAU | capi.GFLAG_USER_MU)
+    assert_parity_general(got, ref, "lyrcut")
+    assert np.all(got["flux_up"][:, 2] == 0.0) and np.all(got["intensity"][:, 2] == 0.0)
+
+
+def test_general_convergence_early_exit():
+    insts, flags = workloads.general_mix(8, seed=61, nstr=(16,), layers=(2, 6))
+    got, ref, _ = both(insts, flags, accuracy=1e-3)
+    assert_parity_general(got, ref, "accuracy 1e-3")
+
+
+def test_general_invalid_and_unsupported_instances():
+    insts, flags = workloads.general_mix(5, seed=71, nstr=(8,), layers=(2, 4))
+    insts[1]["single_scat_albedo"] = np.r_[1.5, insts[1]["single_scat_albedo"][1:]]
+    insts[3]["num_streams"] = 18  # even, >= 4, but no kernel instantiation
+    insts[3]["num_phase_func_moments"] = 19
+    insts[3]["phase_function_moments"] = workloads.hg_moments(np.full(insts[3]["num_layers"], 0.7), 20)
+    got, ref, _ = both(insts, flags)
+    assert got["status"][1] == capi.DSP_ERR_INVALID_INPUT
+    assert got["status"][3] == capi.DSP_ERR_UNSUPPORTED
+    for k in (1, 3):
+        assert np.all(np.isnan(got["flux_up"][k])) and np.all(np.isnan(got["intensity"][k]))
+    keep = [0, 2, 4]
+    assert np.all(got["status"][keep] == 0)
+    sub = lambda o: {f: o[f][keep] for f in o if f != "status"}
+    assert_parity_general(sub(got), sub(ref), "valid instances beside invalid ones")
+
+
+def test_general_device_pointers_match_host():
+    insts, flags = workloads.general_mix(10, seed=81, nstr=(4, 16), layers=(2, 8))
+    d = capi.pack_general(insts, flags)
+    host, rc = gpu_lib.general_solve(d)
+    assert rc == 0
+    dev, rc2 = gpu_lib.general_solve_device(d)
+    assert rc2 == 0, gpu_lib.context().last_error()
+    for f in host:
+        np.testing.assert_array_equal(dev[f], host[f], err_msg=f)

@@ -1,0 +1,152 @@
+"""The general-solver oracle (oracle/general_oracle.hpp) pinned on the CPU.
+
+1. Every flux and intensity expectation of the reference's known-answer tests
+   (tests/golden/reference_goldens.json, from tests/test_solver.cpp).
+2. The reference's own cross-solver check (test_flux_solver.cpp:104-539): the
+   general solver's mode-0 fluxes equal the flux solver's to 1e-12 relative.
+3. index_from_bottom, and the validation rules of DisortConfig::validate.
+"""
+from __future__ import annotations
+
+import numpy as np
+import pytest
+
+import golden_cases as gc
+import oracle_lib
+from disort_b200 import capi
+
+CASES = gc.load_cases()
+
+
+@pytest.mark.parametrize("case", CASES, ids=[c["name"] for c in CASES])
+def test_general_oracle_goldens(case):
+    inst, flags = gc.general_instance(case)
+    o = oracle_lib.general_solve(capi.pack_general([inst], flags))
+    assert o["status"][0] == 0
+    for e in case["expect_flux"]:
+        v = o[e["field"]][0, e["index"]]
+        assert abs(v - e["value"]) <= e["tol"], (e, v)
+    for e in case["expect_intensity"]:
+        v = o["intensity"][0, e["lu"], e["iu"], e["j"]]
+        assert abs(v - e["value"]) <= e["tol"], (e, v)
+
+
+def random_instance(rng, N, L, thermal, beam, dmplus=False, ssa_max=0.99):
+    g = rng.uniform(0.0, 0.9, L)
+    nmom = N + 1 if dmplus else 0
+    nm = max(nmom, N)
+    pm = g[:, None] ** np.arange(nm + 1)[None, :]
+    inst = dict(num_streams=N, num_layers=L, num_phase_func_moments=nmom,
+                delta_tau=np.clip(rng.lognormal(-1.0, 1.5, L), 1e-6, 50.0),
+                single_scat_albedo=rng.uniform(0.0, ssa_max, L), phase_function_moments=pm,
+                surface_albedo=float(rng.uniform(0, 0.6)))
+    if thermal:
+        inst.update(temperature=180.0 + 140.0 * np.arange(L + 1) / L + rng.uniform(-10, 10, L + 1),
+                    wavenumber_low=500.0, wavenumber_high=520.0, temperature_bottom=300.0,
+                    temperature_top=50.0, emissivity_top=0.9)
+    if beam:
+        inst.update(direct_beam_flux=1.7, direct_beam_mu=float(rng.uniform(0.1, 1.0)),
+                    isotropic_flux_top=0.3)
+    return inst
+
+
+def flux_oracle_of(inst, flags):
+    pm = np.asarray(inst["phase_function_moments"])
+    arrays = dict(delta_tau=np.asarray(inst["delta_tau"]), single_scat_albedo=np.asarray(inst["single_scat_albedo"]),
+                  phase_function_moments=pm, temperature=inst.get("temperature"))
+    for f in ("wavenumber_low", "wavenumber_high", "surface_albedo", "emissivity_top", "direct_beam_flux",
+              "direct_beam_mu", "isotropic_flux_top", "isotropic_flux_bottom", "temperature_top",
+              "temperature_bottom"):
+        arrays[f] = float(inst.get(f, capi.GENERAL_SCALAR_DEFAULTS[f]))
+    w = dict(n_inst=1, num_streams=inst["num_streams"], num_layers=inst["num_layers"],
+             num_phase_func_moments=inst["num_phase_func_moments"], pmom_count=pm.shape[1],
+             flags=flags & 0xFF, arrays=arrays)
+    return oracle_lib.flux_solve(w)
+
+
+@pytest.mark.parametrize("N", [4, 8, 16, 32])
+@pytest.mark.parametrize("kind", ["thermal", "beam", "both", "dmplus", "dlbc", "ifb"])
+def test_general_matches_flux_oracle(N, kind):
+    rng = np.random.default_rng(100 + N)
+    thermal = kind in ("thermal", "both", "dlbc", "ifb")
+    beam = kind in ("beam", "both", "dmplus", "ifb")
+    flags = (capi.FLAG_THERMAL if thermal else 0) | capi.GFLAG_ONLY_FLUXES
+    if kind == "dmplus":
+        flags |= capi.FLAG_DELTA_M_PLUS
+    if kind == "dlbc":
+        flags |= capi.FLAG_DIFFUSION_LOWER_BC
+    if kind == "ifb":
+        flags |= capi.FLAG_INDEX_FROM_BOTTOM
+    L = 7
+    for _ in range(3):
+        inst = random_instance(rng, N, L, thermal, beam, dmplus=kind == "dmplus")
+        og = oracle_lib.general_solve(capi.pack_general([inst], flags))
+        of, st = flux_oracle_of(inst, flags)
+        assert og["status"][0] == 0 and st[0] == 0
+        for f in capi.FLUX_OUT_FIELDS:
+            a, b = og[f][0, :L + 1], of[f][0]
+            np.testing.assert_allclose(a, b, rtol=1e-12, atol=1e-12 * max(1.0, np.abs(b).max()), err_msg=f)
+
+
+def test_general_lyrcut_matches_flux_oracle():
+    """Deep absorbing beam-only column: the absorption cut drops the lower layers."""
+    rng = np.random.default_rng(7)
+    inst = random_instance(rng, 8, 6, thermal=False, beam=True, ssa_max=0.2)
+    inst["delta_tau"] = np.array([2.0, 5.0, 8.0, 10.0, 3.0, 1.0])
+    og = oracle_lib.general_solve(capi.pack_general([inst], capi.GFLAG_ONLY_FLUXES))
+    of, st = flux_oracle_of(inst, 0)
+    for f in capi.FLUX_OUT_FIELDS:
+        np.testing.assert_allclose(og[f][0], of[f][0], rtol=1e-12, atol=1e-14, err_msg=f)
+    assert og["flux_up"][0, -1] == 0.0  # below the cut
+
+
+def test_general_index_from_bottom_reverses():
+    rng = np.random.default_rng(11)
+    inst = random_instance(rng, 8, 5, thermal=True, beam=True)
+    inst.update(tau_user=[0.0, 0.05, 1.0], mu_user=[-0.7, -0.2, 0.3, 1.0], phi_user=[0.0, 45.0, 170.0])
+    flags = capi.FLAG_THERMAL | capi.GFLAG_USER_TAU | capi.GFLAG_USER_MU
+    top = oracle_lib.general_solve(capi.pack_general([inst], flags))
+    tot = float(np.sum(inst["delta_tau"]))
+    rev = dict(inst)
+    rev.update(delta_tau=inst["delta_tau"][::-1].copy(), single_scat_albedo=inst["single_scat_albedo"][::-1].copy(),
+               phase_function_moments=inst["phase_function_moments"][::-1].copy(),
+               temperature=inst["temperature"][::-1].copy(), tau_user=[tot - t for t in inst["tau_user"][::-1]])
+    bot = oracle_lib.general_solve(capi.pack_general([rev], flags | capi.FLAG_INDEX_FROM_BOTTOM))
+    for f in capi.FLUX_OUT_FIELDS + ("intensity", "intensity_azimuth_avg"):
+        np.testing.assert_allclose(bot[f][0][::-1], top[f][0], rtol=1e-12, atol=1e-15, err_msg=f)
+
+
+def test_general_azimuth_modes_matter():
+    """With an oblique beam and azimuth-dependent output the m > 0 modes contribute."""
+    rng = np.random.default_rng(5)
+    inst = random_instance(rng, 16, 3, thermal=False, beam=True)
+    inst.update(direct_beam_mu=0.6, tau_user=[0.0, 0.5], mu_user=[-0.5, 0.5], phi_user=[0.0, 90.0, 180.0])
+    o = oracle_lib.general_solve(capi.pack_general([inst], capi.GFLAG_USER_TAU | capi.GFLAG_USER_MU))
+    I = o["intensity"][0]
+    assert np.all(np.isfinite(I))
+    assert np.abs(I[:, :, 0] - I[:, :, 2]).max() > 1e-3 * np.abs(I).max()
+    np.testing.assert_array_equal(o["intensity_azimuth_avg"][0].shape, (2, 2))
+
+
+@pytest.mark.parametrize("mutate", [
+    lambda i, f: (i.update(num_layers=0, delta_tau=[], single_scat_albedo=[], phase_function_moments=np.zeros((0, 17))) or i, f),
+    lambda i, f: (i.update(single_scat_albedo=np.r_[1.5, i["single_scat_albedo"][1:]]) or i, f),
+    lambda i, f: (i.update(delta_tau=np.r_[-1.0, i["delta_tau"][1:]]) or i, f),
+    lambda i, f: (i.update(mu_user=[0.5, 0.2]) or i, f),
+    lambda i, f: (i.update(mu_user=[-0.5, 1.5]) or i, f),
+    lambda i, f: (i.update(phi_user=[-10.0]) or i, f),
+    lambda i, f: (i.update(direct_beam_mu=0.0) or i, f),
+    lambda i, f: (i, f | capi.FLAG_DIFFUSION_LOWER_BC),
+    lambda i, f: (i, f | capi.FLAG_DELTA_M_PLUS),
+])
+def test_general_validation(mutate):
+    rng = np.random.default_rng(3)
+    inst = random_instance(rng, 16, 3, thermal=False, beam=True)
+    inst.update(tau_user=[0.0], mu_user=[-0.5, 0.5], phi_user=[0.0])
+    inst, flags = mutate(inst, capi.GFLAG_USER_TAU | capi.GFLAG_USER_MU)
+    if inst["num_layers"] == 0:
+        d = capi.pack_general([inst], flags, pmom_count=17)
+    else:
+        d = capi.pack_general([inst], flags)
+    o = oracle_lib.general_solve(d)
+    assert o["status"][0] == capi.DSP_ERR_INVALID_INPUT
