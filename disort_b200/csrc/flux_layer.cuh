@@ -289,7 +289,7 @@ __device__ void gen_user_angles(const FluxParams& p, int i, double* sm, const do
   const double* umu = p.g.umu.row(i);
   for (int u0 = 0; u0 < numu; u0 += UCH) {
     const int nu = numu - u0 < UCH ? numu - u0 : UCH;
-    if (t < nu) legendre_column(m, umu[u0 + t], N - 1, U + t, UCH);
+    for (int k = t; k < nu; k += TEAM) legendre_column(m, umu[u0 + k], N - 1, U + k, UCH);
     team_sync<TEAM>();
     if (t < N)
       for (int k = 0; k < nu; ++k) {
@@ -297,20 +297,20 @@ __device__ void gen_user_angles(const FluxParams& p, int i, double* sm, const do
         for (int l = m; l < N; ++l) s += U[l * UCH + k] * W[l * N + t];
         GU[(u0 + k) * N + t] = s;
       }
-    if (t < nu) {
+    for (int k = t; k < nu; k += TEAM) {
       if (beam) {
         double s = 0.0;
-        for (int l = m; l < N; ++l) s += U[l * UCH + t] * (psi0[l] + fact * gl[l] * ybm[l]);
-        zbu[u0 + t] = s;
+        for (int l = m; l < N; ++l) s += U[l * UCH + k] * (psi0[l] + fact * gl[l] * ybm[l]);
+        zbu[u0 + k] = s;
       }
       if (thermal) {
         double s0 = 0.0, s1 = 0.0;
         for (int l = m; l < N; ++l) {
-          s0 += U[l * UCH + t] * p0[l];
-          s1 += U[l * UCH + t] * p1[l];
+          s0 += U[l * UCH + k] * p0[l];
+          s1 += U[l * UCH + k] * p1[l];
         }
-        z0u[u0 + t] = s0 + (1.0 - ws) * xr0;
-        z1u[u0 + t] = s1 + (1.0 - ws) * xr1;
+        z0u[u0 + k] = s0 + (1.0 - ws) * xr0;
+        z1u[u0 + k] = s1 + (1.0 - ws) * xr1;
       }
     }
     team_sync<TEAM>();

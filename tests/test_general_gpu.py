@@ -32,17 +32,32 @@ def test_general_reference_goldens(case):
     inst, flags = golden_cases.general_instance(case)
     got, ref, _ = both([inst], flags)
     assert got["status"][0] == ref["status"][0] == 0
-    rtol = 1e-8 if max(case["single_scat_albedo"]) >= 1.0 else 1e-9
-    assert_parity_general(got, ref, case["name"], rtol=rtol)
+    # conservative scattering takes the other factorisation; the reference's own
+    # cross-solver tolerance there is 1e-8 relative, 2e-9 absolute (test_flux_solver.cpp:135-136)
+    if max(case["single_scat_albedo"]) >= 1.0:
+        assert_parity_general(got, ref, case["name"], rtol=1e-8, atol=2e-9)
+    else:
+        assert_parity_general(got, ref, case["name"])
     for e in case["expect_flux"]:
         assert abs(got[e["field"]][0, e["index"]] - e["value"]) <= e["tol"]
     for e in case["expect_intensity"]:
         assert abs(got["intensity"][0, e["lu"], e["iu"], e["j"]] - e["value"]) <= e["tol"]
 
 
+def with_streams(insts, Ns):
+    """Re-target mixed-batch instances to the stream counts Ns (cycled): N+1 HG moments."""
+    for k, p in enumerate(insts):
+        N = Ns[k % len(Ns)]
+        g = p["phase_function_moments"][:, 1]
+        p.update(num_streams=N, num_phase_func_moments=N + 1,
+                 phase_function_moments=workloads.hg_moments(g, N + 2))
+    return insts
+
+
 @pytest.mark.parametrize("nstr", [(4, 8), (16,), (6, 10, 12, 14), (32,)])
 def test_general_mix_small(nstr):
-    insts, flags = workloads.general_mix(24, seed=30 + len(nstr), nstr=nstr, layers=(2, 12))
+    insts, flags = workloads.general_mix(24, seed=30 + len(nstr), nstr=(4,), layers=(2, 12))
+    insts = with_streams(insts, nstr)
     got, ref, _ = both(insts, flags)
     assert np.all(got["status"] == 0) and np.all(ref["status"] == 0)
     assert_parity_general(got, ref, f"general mix N={nstr}")
@@ -57,16 +72,9 @@ def test_general_mix_n64():
 
 def test_general_ragged_mixed_streams_one_batch():
     """One batch holding every supported stream count and ragged layer counts."""
-    insts = []
-    for k, N in enumerate(capi.SUPPORTED_NSTR[:-1]):
-        part, flags = workloads.general_mix(2, seed=50 + k, nstr=(N,) if N in workloads.GENERAL_NSTR else (4,),
-                                            layers=(1, 9))
-        for p in part:
-            if p["num_streams"] != N:  # stream counts outside the mix's set
-                p["num_streams"] = N
-                p["num_phase_func_moments"] = N + 1
-                p["phase_function_moments"] = workloads.hg_moments(p["phase_function_moments"][:, 1], N + 2)
-        insts += part
+    Ns = capi.SUPPORTED_NSTR[:-1]
+    insts, flags = workloads.general_mix(2 * len(Ns), seed=50, nstr=(4,), layers=(1, 9))
+    insts = with_streams(insts, Ns)
     got, ref, _ = both(insts, flags)
     assert np.all(got["status"] == 0)
     assert_parity_general(got, ref, "ragged mixed-N batch")
