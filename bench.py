@@ -2,7 +2,7 @@
 20,000-band thermal sweep (one spectral loop per step).
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
-                    [--workload thermal|beam]
+                    [--workload thermal|beam|general]
 
 Prints one JSON line (rank 0).  A step is one dsp_flux_bands_solve over the whole
 sweep with inputs resident in HBM (`value`); `e2e` repeats the step through the
@@ -11,6 +11,11 @@ same C ABI with pinned host buffers, host<->device copies inside the timed regio
 OpenMP over all host threads, the reference loop's structure) on a bounded
 sample of the same sweep.  Multi-GPU runs are replicas: every rank solves its own
 20,000-band sweep (weak scaling), no collective on the data path.
+
+`--workload general` measures the general solver (dsp_general_bands_solve,
+DisortSolver::solve) on the mixed batch of workloads.general_mix: 4,096 instances
+by default (`--bands` sets the count), N 4..64, 10..120 layers, delta-M+, beam,
+3 optical depths x 5 polar angles x 4 azimuths, every azimuth mode.
 """
 from __future__ import annotations
 
@@ -40,7 +45,7 @@ def parse():
     ap.add_argument("--steps", type=int, default=10)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
-    ap.add_argument("--workload", choices=["thermal", "beam"], default="thermal")
+    ap.add_argument("--workload", choices=["thermal", "beam", "general"], default="thermal")
     ap.add_argument("--cpu-seconds", type=float, default=10.0, help="target CPU-baseline sample time")
     ap.add_argument("--bands", type=int, default=0, help="profiling: solve only the first N bands")
     ap.add_argument("--no-cpu", action="store_true", help="profiling: skip the CPU baseline")
@@ -377,9 +382,214 @@ def run_ours(args):
         dist.destroy_process_group()
 
 
+# ---------------------------------------------------------------------------
+# general solver (DisortSolver) on the mixed batch
+# ---------------------------------------------------------------------------
+GENERAL_METRIC = "solves/s (general mix: N 4-64, L 10-120, DM+, beam, 3 tau x 5 mu x 4 phi, all modes)"
+
+
+def general_batch(n: int, seed: int):
+    insts, flags = workloads.general_mix(n, seed=seed)
+    d = capi.pack_general(insts, flags)
+    fl = {"gen_layer_kernel": 0.0, "gen_bvp_kernel": 0.0, "gen_intensity_kernel": 0.0, "total": 0.0}
+    for c in insts:
+        ncut = flops.absorption_cut(c["delta_tau"], c["single_scat_albedo"], False)
+        modes = 1 if abs(1.0 - c["direct_beam_mu"]) < 1e-5 else c["num_streams"]
+        f = flops.general_solve_flops(c["num_streams"], c["num_layers"], ncut, modes, 5, 3, True, False)
+        for k in fl:
+            fl[k] += f[k]
+    return insts, d, fl
+
+
+def general_oracle_lib():
+    subprocess.run(["make", "-s", "-C", os.path.join(REPO, "oracle"), "native"], check=True)
+    lib = ctypes.CDLL(os.path.join(REPO, "oracle", "_native", "liboracle_disort.so"))
+    lib.oracle_general_bands_solve.restype = ctypes.c_int
+    lib.oracle_general_bands_solve.argtypes = [ctypes.POINTER(capi.GeneralBatch), ctypes.POINTER(capi.GeneralOut),
+                                               ctypes.c_int]
+    return lib
+
+
+def general_cpu_time(lib, insts, flags, threads):
+    d = capi.pack_general(insts, flags, pmom_count=66)
+    b, keep = capi.make_general_batch(d)
+    outs, o, keep2 = capi.alloc_general_out_numpy(d)
+    t0 = time.perf_counter()
+    lib.oracle_general_bands_solve(ctypes.byref(b), ctypes.byref(o), threads)
+    return time.perf_counter() - t0
+
+
+def general_cpu_sample(insts, target_s: float):
+    """An evenly spaced sample of the batch sized to about target_s of CPU time."""
+    lib = general_oracle_lib()
+    threads = os.cpu_count() or 1
+    flags = capi.FLAG_DELTA_M_PLUS | capi.GFLAG_USER_TAU | capi.GFLAG_USER_MU
+    n = len(insts)
+    probe = [insts[k] for k in np.linspace(0, n - 1, min(n, 2 * threads)).astype(int)]
+    t = general_cpu_time(lib, probe, flags, threads)
+    m = int(min(n, max(threads, len(probe) * target_s / max(t, 1e-6))))
+    idx = np.linspace(0, n - 1, m).astype(int)
+    return lib, [insts[k] for k in idx], flags, threads
+
+
+def run_general(args):
+    import torch
+    import torch.distributed as dist
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    n = args.bands or 4096
+    if args.impl == "reference":
+        if rank != 0:
+            return
+        insts, flags = workloads.general_mix(n, seed=3)
+        lib, sample, flags, threads = general_cpu_sample(insts, min(20.0, 150.0 / max(1, args.steps + args.warmup)))
+        for _ in range(args.warmup):
+            general_cpu_time(lib, sample, flags, threads)
+        ts = [general_cpu_time(lib, sample, flags, threads) for _ in range(args.steps)]
+        value = len(sample) * len(ts) / sum(ts)
+        desc = (f"{len(sample)} of {n} instances per step (evenly spaced), CPU restatement of DisortSolver "
+                f"(oracle/, -march=native), {threads} OpenMP threads")
+        print(json.dumps({
+            "impl": "reference", "metric": GENERAL_METRIC, "value": value, "unit": "solves/s",
+            "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1000 * statistics.mean(ts),
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic (seeded)", "config": {"workload": f"general_mix_{n}", "instances_per_gpu": n},
+            "cpu_baseline": {"value": value, "unit": "solves/s", "cores": threads, "kind": "port", "sample": desc},
+            "e2e": {"value": value, "unit": "solves/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}), flush=True)
+        return
+    torch.cuda.set_device(local)
+    if world > 1:
+        import datetime
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+    dev = torch.device("cuda", local)
+    stream = torch.cuda.current_stream()
+    insts, d, fl = general_batch(n, 3 + rank)
+    ctx = capi.Context(local, stream.cuda_stream)
+    dd = dict(d)
+    for k in ("num_streams", "num_layers", "layer_offset", "num_phase_func_moments", "delta_tau",
+              "single_scat_albedo", "phase_function_moments", "temperature") + capi.GENERAL_SCALAR_FIELDS:
+        dd[k] = torch.from_numpy(np.ascontiguousarray(d[k])).to(dev)
+    for k in ("tau_user", "mu_user", "phi_user"):
+        a, stride = d[k]
+        dd[k] = (torch.from_numpy(np.ascontiguousarray(a)).to(dev), stride)
+    dd["flags"] = d["flags"] | capi.FLAG_DEVICE_POINTERS
+    batch, keep = capi.make_general_batch(dd)
+    nt, nu, nphi = d["ntau_out"], d["numu_out"], d["num_phi"]
+
+    def make_out(device, pin):
+        mk = (lambda *shape, dt=torch.float64: torch.empty(shape, dtype=dt, device=device)) if device != "cpu" else \
+            (lambda *shape, dt=torch.float64: torch.empty(shape, dtype=dt).pin_memory())
+        outs = {f: mk(n, nt) for f in capi.FLUX_OUT_FIELDS}
+        outs["intensity"] = mk(n, nt, nu, nphi)
+        outs["intensity_azimuth_avg"] = mk(n, nt, nu)
+        outs["status"] = mk(n, dt=torch.int32)
+        o = capi.GeneralOut()
+        for k, f in enumerate(capi.FLUX_OUT_FIELDS):
+            o.flux[k] = ctypes.cast(ctypes.c_void_p(outs[f].data_ptr()), ctypes.POINTER(ctypes.c_double))
+        o.intensity = ctypes.cast(ctypes.c_void_p(outs["intensity"].data_ptr()), ctypes.POINTER(ctypes.c_double))
+        o.intensity_azimuth_avg = ctypes.cast(ctypes.c_void_p(outs["intensity_azimuth_avg"].data_ptr()),
+                                              ctypes.POINTER(ctypes.c_double))
+        o.status = ctypes.cast(ctypes.c_void_p(outs["status"].data_ptr()), ctypes.POINTER(ctypes.c_int32))
+        o.ntau_out, o.numu_out = nt, nu
+        return outs, o
+
+    douts, dout = make_out(dev, False)
+
+    def step(b, o):
+        rc = ctx.general_bands_solve(b, o)
+        if rc != 0:
+            raise RuntimeError(f"dsp_general_bands_solve: {capi.STATUS_NAMES.get(rc, rc)}: {ctx.last_error()}")
+
+    for _ in range(args.warmup):
+        step(batch, dout)
+    torch.cuda.synchronize()
+    bad = int((douts["status"] != 0).sum())
+    clocks = ClockSampler(str(local))
+    ctx.set_timing(True)
+    ctx.timing_reset()
+    if world > 1:
+        dist.barrier()
+    torch.cuda.synchronize()
+    clocks.start()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(args.steps):
+        step(batch, dout)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1)
+    clk = clocks.stop()
+    ktimes = ctx.timings()
+    ctx.set_timing(False)
+    t = torch.tensor([ms], dtype=torch.float64, device=dev)
+    if world > 1:
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    ms_max = float(t.item())
+    value = n * args.steps * world / (ms_max / 1000.0)
+    e2e = None
+    if not args.no_e2e:
+        hb, hkeep = capi.make_general_batch(d)
+        houts, hout = make_out("cpu", True)
+        h2d = sum(int(np.asarray(d[k]).nbytes) for k in ("num_streams", "num_layers", "layer_offset",
+                                                          "num_phase_func_moments", "delta_tau", "single_scat_albedo",
+                                                          "phase_function_moments") + capi.GENERAL_SCALAR_FIELDS)
+        h2d += sum(int(np.asarray(d[k][0]).nbytes) for k in ("tau_user", "mu_user", "phi_user"))
+        d2h = sum(int(v.numel() * v.element_size()) for v in houts.values())
+        step(hb, hout)
+        torch.cuda.synchronize()
+        e2 = torch.cuda.Event(enable_timing=True)
+        e3 = torch.cuda.Event(enable_timing=True)
+        e2.record(stream)
+        for _ in range(args.steps):
+            step(hb, hout)
+        e3.record(stream)
+        torch.cuda.synchronize()
+        te = torch.tensor([e2.elapsed_time(e3)], dtype=torch.float64, device=dev)
+        if world > 1:
+            dist.all_reduce(te, op=dist.ReduceOp.MAX)
+        same = all(torch.equal(houts[f], douts[f].cpu()) for f in houts)
+        e2e = {"value": n * args.steps * world / (float(te.item()) / 1000.0), "unit": "solves/s",
+               "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h, "matches_device_result": same}
+    dom = max((k for k in ktimes if k in fl), key=lambda k: ktimes[k][0])
+    dom_ms, dom_launches = ktimes[dom]
+    achieved = fl[dom] * args.steps / (dom_ms / 1000.0) / 1e12
+    peak = fp64_peak_tflops()
+    roofline = {"bound": "fp64", "kernel": dom, "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
+                "frac": (achieved / peak) if peak else None,
+                "peak_source": "measured on this GPU by disort_b200/csrc/fp64_peak.cu (FP64 FMA chains, burst)",
+                "flops_per_step": fl[dom], "flops_total_per_step": fl["total"],
+                "avg_launch_ms": dom_ms / max(1, dom_launches), "traffic": None,
+                "kernel_ms_per_step": {k: v[0] / args.steps for k, v in ktimes.items()},
+                "all_kernels_tflops": fl["total"] * args.steps / (ms_max / 1000.0) / 1e12}
+    if rank == 0:
+        cpu = None
+        if not args.no_cpu:
+            lib, sample, flags, threads = general_cpu_sample(insts, args.cpu_seconds)
+            tcpu = general_cpu_time(lib, sample, flags, threads)
+            cpu = {"value": len(sample) / tcpu, "unit": "solves/s", "cores": threads, "kind": "port",
+                   "sample": f"{len(sample)} of {n} instances evenly spaced, oracle -march=native, "
+                             f"{threads} OpenMP threads, {tcpu:.1f} s"}
+        print(json.dumps({
+            "metric": GENERAL_METRIC, "value": value, "unit": "solves/s", "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": ms_max / args.steps, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded PCG64)",
+            "config": {"workload": f"general_mix_{n}", "instances_per_gpu": n,
+                       "parallelism": f"replicas x{world}" if world > 1 else "single GPU",
+                       "l2": "workspace larger than L2; no flush needed"},
+            "e2e": e2e, "gpu_launches": int(sum(v[1] for v in ktimes.values())), "roofline": roofline,
+            "cpu_baseline": cpu, "clocks": clk, "bad_status_instances": bad}), flush=True)
+    ctx.close()
+    if world > 1:
+        dist.destroy_process_group()
+
+
 def main():
     args = parse()
-    if args.impl == "reference":
+    if args.workload == "general":
+        run_general(args)
+    elif args.impl == "reference":
         run_reference(args)
     else:
         run_ours(args)
