@@ -202,12 +202,14 @@ def fp64_peak_tflops() -> float | None:
         return None
 
 
-def committed_traffic(workload_name: str):
+def committed_traffic(workload_name: str, kernel: str):
+    """DRAM bytes per launch of `kernel` on this workload, from the committed ncu summary."""
     p = os.path.join(REPO, "profiles", "traffic.json")
     if not os.path.exists(p):
         return None
     try:
-        return json.load(open(p)).get(workload_name)
+        entry = json.load(open(p)).get(workload_name) or {}
+        return entry.get(kernel)
     except (ValueError, OSError):
         return None
 
@@ -360,7 +362,8 @@ def run_ours(args):
         "frac": (achieved / peak) if peak else None,
         "peak_source": "measured on this GPU by disort_b200/csrc/fp64_peak.cu (FP64 FMA chains, burst)",
         "flops_per_solve": fl[dom], "avg_launch_ms": dom_ms / max(1, dom_launches),
-        "traffic": committed_traffic(w["name"]),
+        "traffic": committed_traffic(w["name"], dom),
+        "traffic_source": "profiles/traffic.json (ncu dram bytes of one 4,000-band launch, scaled to the sweep)",
         "kernel_ms_per_step": {k: v[0] / args.steps for k, v in ktimes.items()},
     }
 
