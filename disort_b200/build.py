@@ -69,6 +69,18 @@ def build_libdsp(force: bool = False) -> str:
     return target
 
 
+def build_emu(force: bool = False) -> str:
+    """libdsp_emu.so: the emulator's tcgen05 GEMMs, training loop and gate."""
+    os.makedirs(LIB, exist_ok=True)
+    target = os.path.join(LIB, "libdsp_emu.so")
+    deps = [os.path.join(REPO, "include", "dsp_emu.h"), os.path.join(REPO, "include", "dsp.h")]
+    deps += [os.path.join(CSRC, "emu", f) for f in os.listdir(os.path.join(CSRC, "emu"))]
+    if force or _stale(target, deps):
+        _run([NVCC, *ARCH, "-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC", "-shared",
+              "-o", target, os.path.join(CSRC, "emu", "emu.cu")])
+    return target
+
+
 def build_bench(force: bool = False) -> str:
     os.makedirs(LIB, exist_ok=True)
     target = os.path.join(LIB, "libdsp_bench.so")
@@ -104,6 +116,7 @@ def build_host(force: bool = False) -> str:
 
 def build_all(force: bool = False) -> None:
     build_libdsp(force)
+    build_emu(force)
     build_bench(force)
     build_host(force)
 
