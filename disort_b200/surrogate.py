@@ -13,7 +13,11 @@ the same inputs: log cumulative optical depth at levels 1..40, the level Planck
 fluxes pi B(T) / S and the thermal share of S, where S = pi B(T_surface) + mu0 F0
 is the instance's flux scale (B: band Planck radiance, midpoint rule).
 Targets (82): flux_up and the diffuse downward flux at the 41 levels divided by
-S, as log(x + 1e-6) standardised per output.  The direct beam
+S, as log(x + 1e-3) standardised per output (the offset sits at the error
+metric's floor, so fluxes far below it do not dominate the loss).  The
+standardised features enter the network as hi/lo BF16 pairs (x_hi = bf16(x),
+x_lo = bf16(x - x_hi)), 494 inputs carrying about 16 mantissa bits: a single
+BF16 feature (8 bits) alone perturbs optical depths by ~1 %.  The direct beam
 mu0 F0 exp(-tau/mu0) is exact and added back, so the emulated total downward
 flux is direct + S * diffuse.
 
@@ -43,7 +47,7 @@ NBANDS = 256
 BAND_W = 2800.0 / NBANDS
 FLOOR_FRAC = 1e-3
 GATE_TOL = 2e-3
-EPS = 1e-6
+EPS = 1e-3
 C1, C2 = 1.191042e-8, 1.4387769  # W m^-2 sr^-1 (cm^-1)^-4, cm K
 
 
@@ -180,11 +184,15 @@ class Surrogate:
         self.emu, self.fmean, self.fstd, self.lo, self.hi, self.mu, self.sd = emu, fmean, fstd, lo, hi, mu, sd
 
     def encode(self, raw):
-        """Standardised BF16 features [n][in_stride] for the emulator."""
+        """Standardised features as hi/lo BF16 pairs [n][in_stride] for the emulator."""
         import torch
-        x = torch.zeros((raw.shape[0], self.emu.in_stride), dtype=torch.float32, device=raw.device)
-        x[:, :N_IN] = (raw - self.fmean) / self.fstd
-        return x.to(torch.bfloat16)
+        z = (raw - self.fmean) / self.fstd
+        hi = z.to(torch.bfloat16)
+        lo = (z - hi.float()).to(torch.bfloat16)
+        x = torch.zeros((raw.shape[0], self.emu.in_stride), dtype=torch.bfloat16, device=raw.device)
+        x[:, :N_IN] = hi
+        x[:, N_IN:2 * N_IN] = lo
+        return x
 
 
 def train(ctx: capi.Context, n_columns: int = 1 << 20, epochs: int = 50, batch: int = 4096, seed: int = 4,
@@ -215,7 +223,7 @@ def train(ctx: capi.Context, n_columns: int = 1 << 20, epochs: int = 50, batch: 
     hi = raw[:ntr].amax(dim=0)
     span = hi - lo
     lo, hi = lo - 0.01 * span, hi + 0.01 * span
-    emu = Emulator(n_in=N_IN, hidden=512, n_hidden_layers=4, n_out=N_OUT, n_heads=2, batch=batch, seed=seed)
+    emu = Emulator(n_in=2 * N_IN, hidden=512, n_hidden_layers=4, n_out=N_OUT, n_heads=2, batch=batch, seed=seed)
     sur = Surrogate(emu, fmean, fstd, lo, hi, mu.float(), sd.float())
     X = sur.encode(raw)
     # bagging: each head sees every training instance with a Poisson(1) weight
@@ -243,8 +251,9 @@ def train(ctx: capi.Context, n_columns: int = 1 << 20, epochs: int = 50, batch: 
     return sur, report
 
 
-def gated_run(ctx: capi.Context, sur: Surrogate, arrays: dict, raw, n: int):
-    """Emulate every instance, re-solve the gated ones in FP64, merge: fluxes [n][82] and the fallback count."""
+def gated_run(ctx: capi.Context, sur: Surrogate, arrays: dict, raw, n: int, tol: float = GATE_TOL):
+    """Emulate every instance, re-solve the gated ones in FP64, merge.  Returns the
+    fluxes [n][82], the fallback count and the fallback flags [n] (int32)."""
     import torch
     X = sur.encode(raw)
     preds = torch.empty((n, 2 * N_OUT), dtype=torch.float32, device="cuda")
@@ -256,7 +265,10 @@ def gated_run(ctx: capi.Context, sur: Surrogate, arrays: dict, raw, n: int):
     fb = torch.empty((n,), dtype=torch.int32, device="cuda")
     idx = torch.empty((n,), dtype=torch.int32, device="cuda")
     cnt = torch.zeros((1,), dtype=torch.int32, device="cuda")
-    sur.emu.gate(raw, sur.lo, sur.hi, preds, sur.mu, sur.sd, S.float().contiguous(), add, EPS, GATE_TOL, FLOOR_FRAC,
+    # the envelope test reads the first n_in raw values of each row: raw features twice (hi and lo share it)
+    raw2 = torch.cat([raw, raw], dim=1).contiguous()
+    lo2, hi2 = torch.cat([sur.lo, sur.lo]), torch.cat([sur.hi, sur.hi])
+    sur.emu.gate(raw2, lo2, hi2, preds, sur.mu, sur.sd, S.float().contiguous(), add, EPS, tol, FLOOR_FRAC,
                  flux, fb, idx, cnt)
     k = int(cnt.item())
     out = flux.double()
@@ -266,11 +278,11 @@ def gated_run(ctx: capi.Context, sur: Surrogate, arrays: dict, raw, n: int):
                for key, v in arrays.items()}
         Fk, _ = solve_fp64(ctx, sub, k)
         out.index_copy_(0, rows, Fk)
-    return out, k
+    return out, k, fb
 
 
 def evaluate(ctx: capi.Context, sur: Surrogate, columns: int = 4096, seed: int = 5, ooe: float = 0.05,
-             repeats: int = 3) -> dict:
+             repeats: int = 3, tols=(5e-3, 1e-2, 2e-2, 5e-2)) -> dict:
     """Gated inference against the plain FP64 solve on columns x 256 bands (timed on the device)."""
     import torch
     n = columns * NBANDS
@@ -287,19 +299,42 @@ def evaluate(ctx: capi.Context, sur: Surrogate, columns: int = 4096, seed: int =
     torch.cuda.synchronize()
     t_plain = a.elapsed_time(b) / 1000.0 / repeats
     # gated: features -> emulator -> gate -> FP64 solve of the fallback instances
-    F_g, k = gated_run(ctx, sur, arrays, features_device(arrays), n)
+    F_g, k, _ = gated_run(ctx, sur, arrays, features_device(arrays), n)
     torch.cuda.synchronize()
     a, b = ev()
     a.record()
     for _ in range(repeats):
-        F_g, k = gated_run(ctx, sur, arrays, features_device(arrays), n)
+        F_g, k, _ = gated_run(ctx, sur, arrays, features_device(arrays), n)
     b.record()
     torch.cuda.synchronize()
     t_gated = a.elapsed_time(b) / 1000.0 / repeats
     e = rel_err(F_g, F_ref).amax(dim=1)
     ooe_mask = torch.from_numpy(d["ooe"]).cuda()
-    return dict(instances=n, columns=columns, bands=NBANDS, out_of_envelope_instances=int(ooe_mask.sum()),
-                plain_solves_per_s=n / t_plain, gated_solves_per_s=n / t_gated, speedup=t_plain / t_gated,
-                fallback_instances=k, fallback_fraction=k / n, max_rel_err=float(e.max()),
-                p99_rel_err=float(torch.quantile(e.float(), 0.99)), median_rel_err=float(e.median()),
-                plain_seconds=t_plain, gated_seconds=t_gated, bad_status=int((st != 0).sum()))
+    res = dict(instances=n, columns=columns, bands=NBANDS, out_of_envelope_instances=int(ooe_mask.sum()),
+               plain_solves_per_s=n / t_plain, gated_solves_per_s=n / t_gated, speedup=t_plain / t_gated,
+               gate_tol=GATE_TOL, fallback_instances=k, fallback_fraction=k / n, max_rel_err=float(e.max()),
+               p99_rel_err=float(torch.quantile(e.float(), 0.99)), median_rel_err=float(e.median()),
+               plain_seconds=t_plain, gated_seconds=t_gated, bad_status=int((st != 0).sum()))
+    # the trade-off of looser gates (one timed run each)
+    sweep = []
+    for tol in tols:
+        a, b = ev()
+        a.record()
+        F_t, k_t, _ = gated_run(ctx, sur, arrays, features_device(arrays), n, tol)
+        b.record()
+        torch.cuda.synchronize()
+        tt = a.elapsed_time(b) / 1000.0
+        et = rel_err(F_t, F_ref).amax(dim=1)
+        sweep.append(dict(gate_tol=tol, fallback_fraction=k_t / n, speedup=t_plain / tt,
+                          max_rel_err=float(et.max()), p99_rel_err=float(torch.quantile(et.float(), 0.99))))
+    res["gate_sweep"] = sweep
+    # the raw emulator alone (no gate) on the in-envelope instances
+    X = sur.encode(features_device(arrays))
+    preds = torch.empty((n, 2 * N_OUT), dtype=torch.float32, device="cuda")
+    sur.emu.forward(X, preds)
+    S, fdir, _ = physics(arrays)
+    Fe = 0.5 * (reconstruct(preds[:, :N_OUT], sur.mu, sur.sd, S, fdir) + reconstruct(preds[:, N_OUT:], sur.mu, sur.sd, S, fdir))
+    ee = rel_err(Fe, F_ref).amax(dim=1)[~ooe_mask]
+    res["emulator_only_in_envelope"] = dict(max_rel_err=float(ee.max()), p99_rel_err=float(torch.quantile(ee.float(), 0.99)),
+                                            median_rel_err=float(ee.median()))
+    return res

@@ -1,0 +1,59 @@
+"""GPU test of the gated emulator pipeline (disort_b200/surrogate.py), small scale.
+
+The emulator is trained on columns labelled by the FP64 GPU solver, then used
+on column x band instances with some columns pushed out of the training
+envelope.  What the network gains over the plain solver: at a loose gate most
+instances skip the FP64 solve.  What the gate guarantees: a gated instance
+carries the FP64 result itself, and every out-of-envelope instance is gated at
+any disagreement tolerance.
+"""
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.fixture(scope="module")
+def trained():
+    import torch
+    from disort_b200 import capi, surrogate
+    ctx = capi.Context(0, torch.cuda.current_stream().cuda_stream)
+    sur, rep = surrogate.train(ctx, n_columns=1 << 17, epochs=20, log=lambda *a: None)
+    yield ctx, sur, rep
+    sur.emu.close()
+    ctx.close()
+
+
+def test_training_on_solver_labels(trained):
+    ctx, sur, rep = trained
+    assert rep["bad_label_status"] == 0
+    assert rep["last_loss"] < 0.2 * rep["first_loss"], rep
+
+
+def test_gate_bounds_error_and_catches_out_of_envelope(trained):
+    import torch
+    from disort_b200 import surrogate as s
+    ctx, sur, rep = trained
+    columns = 32
+    n = columns * s.NBANDS
+    d = s.sample(n, 21, columns=columns, ooe_columns=0.125)
+    arrays = s.device_inputs(d)
+    F_ref, st = s.solve_fp64(ctx, arrays, n)
+    assert int((st != 0).sum()) == 0
+    raw = s.features_device(arrays)
+    # strict gate: every gated instance carries the FP64 result itself
+    F, k, fb = s.gated_run(ctx, sur, arrays, raw, n, s.GATE_TOL)
+    fbm = fb.bool()
+    assert int(fbm.sum()) == k
+    assert torch.equal(F[fbm], F_ref[fbm])
+    e = s.rel_err(F, F_ref).amax(dim=1)
+    print(f"strict gate: fallback {k / n:.3f}, max rel err {float(e.max()):.3g}")
+    # loose gate: the emulator carries most instances; out-of-envelope ones are still solved
+    F5, k5, fb5 = s.gated_run(ctx, sur, arrays, raw, n, 0.1)
+    e5 = s.rel_err(F5, F_ref).amax(dim=1)
+    print(f"10 % gate: fallback {k5 / n:.3f}, p50/p99 rel err {float(e5.median()):.3g}/"
+          f"{float(torch.quantile(e5.float(), 0.99)):.3g}")
+    assert k5 < 0.6 * n, k5
+    ooe = torch.from_numpy(d["ooe"]).cuda()
+    assert bool(fb5.bool()[ooe].all())
+    assert torch.equal(F5[ooe], F_ref[ooe])
