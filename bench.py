@@ -45,7 +45,7 @@ def parse():
     ap.add_argument("--steps", type=int, default=10)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
-    ap.add_argument("--workload", choices=["thermal", "beam", "general"], default="thermal")
+    ap.add_argument("--workload", choices=["thermal", "beam", "general", "emulator"], default="thermal")
     ap.add_argument("--cpu-seconds", type=float, default=10.0, help="target CPU-baseline sample time")
     ap.add_argument("--bands", type=int, default=0, help="profiling: solve only the first N bands")
     ap.add_argument("--no-cpu", action="store_true", help="profiling: skip the CPU baseline")
@@ -609,9 +609,76 @@ def run_general(args):
         dist.destroy_process_group()
 
 
+# ---------------------------------------------------------------------------
+# emulator training step on the tensor cores
+# ---------------------------------------------------------------------------
+def measured_bf16_peak():
+    p = os.path.join(REPO, "MEASURED_PEAKS.json")
+    try:
+        j = json.load(open(p))
+        return float(j["bf16_tflops"]), float(j["bf16_tflops_sustained"]), "MEASURED_PEAKS.json (measured)"
+    except (OSError, ValueError, KeyError):
+        return 1590.0, 1400.0, "fallback figure of this GPU pool"
+
+
+def run_emulator(args):
+    """Training throughput of the emulator MLP (494 -> 4 x 512 GELU -> 2 x 82, batch 4,096):
+    one step = forward, loss gradient, backward and Adam over one batch; each epoch
+    is 16 steps over a 65,536-row synthetic set."""
+    import torch
+    from disort_b200.emu import Emulator
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    stream = torch.cuda.current_stream()
+    B, rows = 4096, 65536
+    e = Emulator(n_in=494, hidden=512, n_hidden_layers=4, n_out=82, n_heads=2, batch=B, seed=1, device=local,
+                 stream=stream.cuda_stream)
+    g = torch.Generator(device="cuda").manual_seed(1)
+    x = torch.zeros((rows, e.in_stride), dtype=torch.float32, device="cuda")
+    x[:, :494] = torch.randn((rows, 494), generator=g, device="cuda")
+    y = torch.randn((rows, 82), generator=g, device="cuda")
+    e.set_data(x.to(torch.bfloat16), y)
+    dims = e.layer_dims()
+    fwd = sum(2.0 * B * a * b for a, b in dims)
+    bwd_w = fwd
+    bwd_x = sum(2.0 * B * a * b for a, b in dims[1:])
+    step_flops = fwd + bwd_w + bwd_x
+    steps_per_epoch = rows // B
+    e.train(max(1, args.warmup), lr=1e-3, lr_min=1e-3)
+    torch.cuda.synchronize()
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    clocks = ClockSampler(str(local))
+    clocks.start()
+    ev0.record(stream)
+    e.train(args.steps, lr=1e-3, lr_min=1e-3)
+    ev1.record(stream)
+    torch.cuda.synchronize()
+    clk = clocks.stop()
+    ms = ev0.elapsed_time(ev1)
+    nsteps = args.steps * steps_per_epoch
+    tflops = step_flops * nsteps / (ms / 1000.0) / 1e12
+    peak, peak_sus, src = measured_bf16_peak()
+    if rank == 0:
+        print(json.dumps({
+            "metric": "emulator training steps/s (BF16 tcgen05 GEMMs, batch 4096, 494-4x512-164)",
+            "value": nsteps / (ms / 1000.0), "unit": "steps/s", "n_gpus": 1, "steps": nsteps,
+            "warmup": args.warmup * steps_per_epoch, "ms_per_step": ms / nsteps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "bf16 (fp32 accumulate)", "data": "synthetic",
+            "config": {"workload": "emulator_train_step_b4096", "layers": dims},
+            "roofline": {"bound": "tensor", "kernel": "all GEMMs of a training step (with epilogues, Adam, "
+                         "transposes)", "achieved": tflops, "peak": peak_sus, "unit": "TFLOP/s",
+                         "frac": tflops / peak_sus, "peak_source": src + ", sustained bf16 (kernel timed inside a "
+                         "long loop)", "flops_per_step": step_flops},
+            "clocks": clk}), flush=True)
+    e.close()
+
+
 def main():
     args = parse()
-    if args.workload == "general":
+    if args.workload == "emulator":
+        run_emulator(args)
+    elif args.workload == "general":
         run_general(args)
     elif args.impl == "reference":
         run_reference(args)
