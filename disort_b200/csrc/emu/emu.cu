@@ -126,7 +126,17 @@ struct EpiOut {  // P = acc + b; training: dZ = dLoss/dP (BF16, and transposed),
         dZt[(long long)n * M + row] = gb;
       }
     }
-    if (dZ && loss) atomicAdd(loss, lsum);
+    if (dZ && loss) {
+      // one atomic per warp when the whole warp holds rows (training batches are
+      // multiples of 128 rows); otherwise one per thread
+      if (__activemask() == 0xffffffffu) {
+#pragma unroll
+        for (int off = 16; off > 0; off >>= 1) lsum += __shfl_xor_sync(0xffffffffu, lsum, off);
+        if ((threadIdx.x & 31) == 0) atomicAdd(loss, lsum);
+      } else {
+        atomicAdd(loss, lsum);
+      }
+    }
   }
 };
 
