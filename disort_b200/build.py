@@ -98,10 +98,11 @@ def build_host(force: bool = False) -> str:
     host = os.path.join(CSRC, "host")
     inc = os.path.join(REPO, "include")
     lib = os.path.join(LIB, "libdisortpp.so")
-    deps = [os.path.join(host, "disortpp_flux.cpp"), os.path.join(host, "phase_tables.inc"),
-            os.path.join(inc, "disortpp", "disortpp.hpp"), os.path.join(inc, "dsp.h"), os.path.join(LIB, "libdsp.so")]
+    srcs = [os.path.join(host, "disortpp_flux.cpp"), os.path.join(host, "disortpp_general.cpp")]
+    deps = srcs + [os.path.join(host, "phase_tables.inc"), os.path.join(inc, "disortpp", "disortpp.hpp"),
+                   os.path.join(inc, "dsp.h"), os.path.join(LIB, "libdsp.so")]
     if force or _stale(lib, deps):
-        _run([CXX, "-std=c++17", "-O2", "-fPIC", "-shared", "-Wall", "-o", lib, deps[0],
+        _run([CXX, "-std=c++17", "-O2", "-fPIC", "-shared", "-Wall", "-o", lib, *srcs,
               "-L" + LIB, "-ldsp", "-Wl,-rpath,$ORIGIN"])
     import pybind11
     ext = sysconfig.get_config_var("EXT_SUFFIX")

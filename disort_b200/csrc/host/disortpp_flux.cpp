@@ -177,20 +177,32 @@ void FluxResult::allocate(int num_layers) {
 // ---------------------------------------------------------------------------
 // engine access
 // ---------------------------------------------------------------------------
-namespace {
+namespace detail {
 
-std::mutex g_mu;
-dsp_context g_ctx = nullptr;
+std::mutex& engine_mutex() {
+  static std::mutex mu;
+  return mu;
+}
 
-dsp_context context_locked() {
-  if (!g_ctx) {
+// The library's one engine context (device DSP_DEVICE, default 0); call with
+// engine_mutex() held.
+dsp_context engine_context_locked() {
+  static dsp_context ctx = nullptr;
+  if (!ctx) {
     const char* d = std::getenv("DSP_DEVICE");
     const int dev = d ? std::atoi(d) : 0;
-    if (dsp_context_create(dev, nullptr, &g_ctx) != DSP_OK)
+    if (dsp_context_create(dev, nullptr, &ctx) != DSP_OK)
       throw std::runtime_error("disortpp: no CUDA device available for the B200 engine");
   }
-  return g_ctx;
+  return ctx;
 }
+
+}  // namespace detail
+
+namespace {
+
+std::mutex& g_mu = detail::engine_mutex();
+dsp_context context_locked() { return detail::engine_context_locked(); }
 
 bool supported(int n) {
   for (int s : {4, 6, 8, 10, 12, 14, 16, 32, 64})

@@ -104,6 +104,169 @@ PYBIND11_MODULE(_disortpp, m) {
       .value("HazeGarciaSiewert", PhaseFunction::HazeGarciaSiewert)
       .value("CloudGarciaSiewert", PhaseFunction::CloudGarciaSiewert);
 
+  py::enum_<BoundaryConditionType>(m, "BoundaryConditionType")
+      .value("General", BoundaryConditionType::General)
+      .value("Special", BoundaryConditionType::Special);
+
+  py::enum_<BrdfType>(m, "BrdfType")
+      .value("NONE", BrdfType::None)
+      .value("RPV", BrdfType::RPV)
+      .value("CoxMunk", BrdfType::CoxMunk)
+      .value("Ambrals", BrdfType::Ambrals)
+      .value("Hapke", BrdfType::Hapke);
+
+  py::class_<DisortFlags>(m, "DisortFlags")
+      .def(py::init<>())
+      .def_readwrite("use_user_tau", &DisortFlags::use_user_tau)
+      .def_readwrite("use_user_mu", &DisortFlags::use_user_mu)
+      .def_readwrite("ibcnd", &DisortFlags::ibcnd)
+      .def_readwrite("use_lambertian_surface", &DisortFlags::use_lambertian_surface)
+      .def_readwrite("use_thermal_emission", &DisortFlags::use_thermal_emission)
+      .def_readwrite("use_spherical_beam", &DisortFlags::use_spherical_beam)
+      .def_readwrite("comp_only_fluxes", &DisortFlags::comp_only_fluxes)
+      .def_readwrite("brdf_type", &DisortFlags::brdf_type)
+      .def_readwrite("intensity_corr_buras", &DisortFlags::intensity_corr_buras)
+      .def_readwrite("intensity_corr_nakajima", &DisortFlags::intensity_corr_nakajima)
+      .def_readwrite("use_delta_m_plus", &DisortFlags::use_delta_m_plus)
+      .def_readwrite("use_diffusion_lower_bc", &DisortFlags::use_diffusion_lower_bc)
+      .def_readwrite("output_fourier_expansion", &DisortFlags::output_fourier_expansion)
+      .def_readwrite("index_from_bottom", &DisortFlags::index_from_bottom)
+      .def_readwrite("compute_temperature_jacobian", &DisortFlags::compute_temperature_jacobian);
+
+  py::class_<BoundaryConditions>(m, "BoundaryConditions")
+      .def(py::init<>())
+      .def_readwrite("direct_beam_flux", &BoundaryConditions::direct_beam_flux)
+      .def_readwrite("direct_beam_mu", &BoundaryConditions::direct_beam_mu)
+      .def_readwrite("direct_beam_phi", &BoundaryConditions::direct_beam_phi)
+      .def_readwrite("isotropic_flux_top", &BoundaryConditions::isotropic_flux_top)
+      .def_readwrite("isotropic_flux_bottom", &BoundaryConditions::isotropic_flux_bottom)
+      .def_readwrite("temperature_top", &BoundaryConditions::temperature_top)
+      .def_readwrite("temperature_bottom", &BoundaryConditions::temperature_bottom)
+      .def_readwrite("emissivity_top", &BoundaryConditions::emissivity_top)
+      .def_readwrite("surface_albedo", &BoundaryConditions::surface_albedo);
+
+  py::class_<RpvBrdfSpec>(m, "RpvBrdfSpec")
+      .def(py::init<>())
+      .def_readwrite("rho0", &RpvBrdfSpec::rho0)
+      .def_readwrite("k", &RpvBrdfSpec::k)
+      .def_readwrite("theta", &RpvBrdfSpec::theta)
+      .def_readwrite("sigma", &RpvBrdfSpec::sigma)
+      .def_readwrite("t1", &RpvBrdfSpec::t1)
+      .def_readwrite("t2", &RpvBrdfSpec::t2)
+      .def_readwrite("scale", &RpvBrdfSpec::scale);
+  py::class_<AmbralsBrdfSpec>(m, "AmbralsBrdfSpec")
+      .def(py::init<>())
+      .def_readwrite("iso", &AmbralsBrdfSpec::iso)
+      .def_readwrite("vol", &AmbralsBrdfSpec::vol)
+      .def_readwrite("geo", &AmbralsBrdfSpec::geo);
+  py::class_<CoxMunkBrdfSpec>(m, "CoxMunkBrdfSpec")
+      .def(py::init<>())
+      .def_readwrite("u10", &CoxMunkBrdfSpec::u10)
+      .def_readwrite("pcl", &CoxMunkBrdfSpec::pcl)
+      .def_readwrite("xsal", &CoxMunkBrdfSpec::xsal)
+      .def_readwrite("refractive_index", &CoxMunkBrdfSpec::refractive_index)
+      .def_readwrite("do_shadow", &CoxMunkBrdfSpec::do_shadow);
+  py::class_<HapkeBrdfSpec>(m, "HapkeBrdfSpec")
+      .def(py::init<>())
+      .def_readwrite("b0", &HapkeBrdfSpec::b0)
+      .def_readwrite("hh", &HapkeBrdfSpec::hh)
+      .def_readwrite("w", &HapkeBrdfSpec::w);
+  py::class_<BrdfSpecification>(m, "BrdfSpecification")
+      .def(py::init<>())
+      .def_readwrite("rpv", &BrdfSpecification::rpv)
+      .def_readwrite("ambrals", &BrdfSpecification::ambrals)
+      .def_readwrite("cox_munk", &BrdfSpecification::cox_munk)
+      .def_readwrite("hapke", &BrdfSpecification::hapke)
+      .def("set_rpv", &BrdfSpecification::setRpv, py::arg("spec"))
+      .def("set_ambrals", &BrdfSpecification::setAmbrals, py::arg("spec"))
+      .def("set_cox_munk", &BrdfSpecification::setCoxMunk, py::arg("spec"))
+      .def("set_hapke", &BrdfSpecification::setHapke, py::arg("spec"));
+
+  py::class_<DisortConfig>(m, "DisortConfig")
+      .def(py::init<>())
+      .def(py::init<int, int, int>(), py::arg("num_layers"), py::arg("num_streams"),
+           py::arg("num_phase_func_moments") = 0)
+      .def_readwrite("flags", &DisortConfig::flags)
+      .def_readwrite("bc", &DisortConfig::bc)
+      .def_readwrite("brdf", &DisortConfig::brdf)
+      .def_readwrite("num_layers", &DisortConfig::num_layers)
+      .def_readwrite("num_phase_func_moments", &DisortConfig::num_phase_func_moments)
+      .def_readwrite("num_streams", &DisortConfig::num_streams)
+      .def_readwrite("num_user_tau", &DisortConfig::num_user_tau)
+      .def_readwrite("num_user_mu", &DisortConfig::num_user_mu)
+      .def_readwrite("num_phi", &DisortConfig::num_phi)
+      .def_readwrite("num_phase_func_angles", &DisortConfig::num_phase_func_angles)
+      .def_readwrite("wavenumber_low", &DisortConfig::wavenumber_low)
+      .def_readwrite("wavenumber_high", &DisortConfig::wavenumber_high)
+      .def_readwrite("accuracy_fourier_series", &DisortConfig::accuracy_fourier_series)
+      .def_readwrite("bottom_radius", &DisortConfig::bottom_radius)
+      .RO_VEC1D(DisortConfig, delta_tau)
+      .RO_VEC1D(DisortConfig, single_scat_albedo)
+      .RO_VEC2D(DisortConfig, phase_function_moments)
+      .RO_VEC1D(DisortConfig, temperature)
+      .RO_VEC1D(DisortConfig, level_altitudes)
+      .RO_VEC1D(DisortConfig, tau_user)
+      .RO_VEC1D(DisortConfig, mu_user)
+      .RO_VEC1D(DisortConfig, phi_user)
+      .RO_VEC1D(DisortConfig, mu_phase_function)
+      .RO_VEC2D(DisortConfig, phase_function)
+      .def("nmom_nstr", &DisortConfig::nmomNstr)
+      .def("allocate", &DisortConfig::allocate)
+      .def("validate", &DisortConfig::validate)
+      .def("set_henyey_greenstein", &DisortConfig::setHenyeyGreenstein, py::arg("g"), py::arg("lc") = -1)
+      .def("set_isotropic", &DisortConfig::setIsotropic, py::arg("lc") = -1)
+      .def("set_rayleigh", &DisortConfig::setRayleigh, py::arg("lc") = -1)
+      .def("set_haze_garcia_siewert", &DisortConfig::setHazeGarciaSiewert, py::arg("lc") = -1)
+      .def("set_cloud_garcia_siewert", &DisortConfig::setCloudGarciaSiewert, py::arg("lc") = -1)
+      .def("set_phase_function", &DisortConfig::setPhaseFunction, py::arg("type"), py::arg("g") = 0.0,
+           py::arg("lc") = -1);
+
+  py::class_<DisortResult>(m, "DisortResult")
+      .def(py::init<>())
+      .def_readwrite("flux_direct_beam", &DisortResult::flux_direct_beam)
+      .def_readwrite("flux_down", &DisortResult::flux_down)
+      .def_readwrite("flux_up", &DisortResult::flux_up)
+      .def_readwrite("flux_tau_divergence", &DisortResult::flux_tau_divergence)
+      .def_readwrite("mean_intensity", &DisortResult::mean_intensity)
+      .def_readwrite("mean_intensity_down", &DisortResult::mean_intensity_down)
+      .def_readwrite("mean_intensity_up", &DisortResult::mean_intensity_up)
+      .def_readwrite("mean_intensity_direct_beam", &DisortResult::mean_intensity_direct_beam)
+      .def_readwrite("albedo_medium", &DisortResult::albedo_medium)
+      .def_readwrite("transmissivity_medium", &DisortResult::transmissivity_medium)
+      .def_readwrite("spherical_albedo", &DisortResult::spherical_albedo)
+      .def_readwrite("spherical_transmissivity", &DisortResult::spherical_transmissivity)
+      .def_readwrite("flux_up_temperature_jac", &DisortResult::flux_up_temperature_jac)
+      .def_readwrite("flux_down_temperature_jac", &DisortResult::flux_down_temperature_jac)
+      .def_readwrite("mean_intensity_temperature_jac", &DisortResult::mean_intensity_temperature_jac)
+      .def_readwrite("mean_intensity_down_temperature_jac", &DisortResult::mean_intensity_down_temperature_jac)
+      .def_readwrite("mean_intensity_up_temperature_jac", &DisortResult::mean_intensity_up_temperature_jac)
+      .def_readwrite("flux_divergence_temperature_jac", &DisortResult::flux_divergence_temperature_jac)
+      .def_readwrite("mu_angles", &DisortResult::mu_angles)
+      .def_readwrite("intensity", &DisortResult::intensity)
+      .def_readwrite("intensity_azimuth_avg", &DisortResult::intensity_azimuth_avg)
+      .def_readwrite("intensity_fourier_expansion", &DisortResult::intensity_fourier_expansion)
+      .def("num_user_tau", &DisortResult::num_user_tau)
+      .def("num_user_mu", &DisortResult::num_user_mu)
+      .def("num_phi", &DisortResult::num_phi)
+      .def("total_flux_down", &DisortResult::totalFluxDown, py::arg("lu"))
+      .def("net_flux", &DisortResult::netFlux, py::arg("lu"))
+      .def("intensities", py::overload_cast<int, int, int>(&DisortResult::intensities, py::const_), py::arg("iu"),
+           py::arg("lu"), py::arg("j"))
+      .def("intensities_azimuth_avg", py::overload_cast<int, int>(&DisortResult::intensitiesAzimuthAvg, py::const_),
+           py::arg("iu"), py::arg("lu"));
+
+  py::class_<DisortSolver>(m, "DisortSolver", "General discrete ordinates radiative transfer solver")
+      .def(py::init<>())
+      .def(
+          "solve",
+          [](DisortSolver& self, DisortConfig& config) {
+            py::gil_scoped_release release;
+            return self.solve(config);
+          },
+          py::arg("config"),
+          "Solve the radiative transfer problem. Note: config may be modified by the solver to set automatic "
+          "dimensions.");
+
   py::class_<DisortFluxConfig>(m, "DisortFluxConfig")
       .def(py::init<>())
       .def(py::init<int, int, int>(), py::arg("num_layers"), py::arg("num_streams"),
@@ -193,6 +356,52 @@ PYBIND11_MODULE(_disortpp, m) {
         }
       },
       py::arg("nstr"), "Create a flux-only solver for the given number of streams (4, 6, 8, 10, 12, 14, 16, 32, or 64)");
+
+  m.def(
+      "solve_spectral",
+      [](DisortConfig config, const std::vector<double>& wavenumbers, std::vector<std::vector<double>> delta_tau,
+         std::vector<std::vector<double>> single_scat_albedo,
+         std::vector<std::vector<std::vector<double>>> phase_function_moments, std::vector<double> surface_albedo,
+         std::vector<double> emissivity_top, std::vector<double> direct_beam_flux,
+         std::vector<double> isotropic_flux_top, std::vector<double> isotropic_flux_bottom) {
+        SpectralOverrides ov = make_overrides(std::move(delta_tau), std::move(single_scat_albedo),
+                                              std::move(phase_function_moments), std::move(surface_albedo),
+                                              std::move(emissivity_top), std::move(direct_beam_flux),
+                                              std::move(isotropic_flux_top), std::move(isotropic_flux_bottom));
+        py::gil_scoped_release release;
+        return solveSpectral(config, wavenumbers, ov);
+      },
+      py::arg("config"), py::arg("wavenumbers"), py::arg("delta_tau") = std::vector<std::vector<double>>{},
+      py::arg("single_scat_albedo") = std::vector<std::vector<double>>{},
+      py::arg("phase_function_moments") = std::vector<std::vector<std::vector<double>>>{},
+      py::arg("surface_albedo") = std::vector<double>{}, py::arg("emissivity_top") = std::vector<double>{},
+      py::arg("direct_beam_flux") = std::vector<double>{}, py::arg("isotropic_flux_top") = std::vector<double>{},
+      py::arg("isotropic_flux_bottom") = std::vector<double>{},
+      "Solve for a list of single wavenumbers (wavenumber_low = wavenumber_high = wn), all in one GPU batch. "
+      "Optional per-wavelength arrays override the corresponding config values. Returns a list of DisortResult.");
+
+  m.def(
+      "solve_spectral_bands",
+      [](DisortConfig config, const std::vector<std::pair<double, double>>& wavenumber_bands,
+         std::vector<std::vector<double>> delta_tau, std::vector<std::vector<double>> single_scat_albedo,
+         std::vector<std::vector<std::vector<double>>> phase_function_moments, std::vector<double> surface_albedo,
+         std::vector<double> emissivity_top, std::vector<double> direct_beam_flux,
+         std::vector<double> isotropic_flux_top, std::vector<double> isotropic_flux_bottom) {
+        SpectralOverrides ov = make_overrides(std::move(delta_tau), std::move(single_scat_albedo),
+                                              std::move(phase_function_moments), std::move(surface_albedo),
+                                              std::move(emissivity_top), std::move(direct_beam_flux),
+                                              std::move(isotropic_flux_top), std::move(isotropic_flux_bottom));
+        py::gil_scoped_release release;
+        return solveSpectralBands(config, wavenumber_bands, ov);
+      },
+      py::arg("config"), py::arg("wavenumber_bands"), py::arg("delta_tau") = std::vector<std::vector<double>>{},
+      py::arg("single_scat_albedo") = std::vector<std::vector<double>>{},
+      py::arg("phase_function_moments") = std::vector<std::vector<std::vector<double>>>{},
+      py::arg("surface_albedo") = std::vector<double>{}, py::arg("emissivity_top") = std::vector<double>{},
+      py::arg("direct_beam_flux") = std::vector<double>{}, py::arg("isotropic_flux_top") = std::vector<double>{},
+      py::arg("isotropic_flux_bottom") = std::vector<double>{},
+      "Solve for a list of wavenumber bands (pairs of (low, high)), all in one GPU batch. Optional "
+      "per-wavelength arrays override the corresponding config values. Returns a list of DisortResult.");
 
   m.def(
       "solve_flux_spectral",

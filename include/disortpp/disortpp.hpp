@@ -8,6 +8,7 @@
 // there is no CPU solve path.
 #pragma once
 
+#include <optional>
 #include <stdexcept>
 #include <string>
 #include <utility>
@@ -149,5 +150,166 @@ std::vector<FluxResult> solveFluxSpectral(const DisortFluxConfig& config, const 
 void solveFluxSpectralBandsInto(const DisortFluxConfig& config,
                                 const std::vector<std::pair<double, double>>& wavenumber_bands,
                                 const SpectralOverrides& ov, double* out8[8]);
+
+// ---------------------------------------------------------------------------
+// General solver (DisortConfig.hpp:11-243, DisortResult.hpp:16-125,
+// DisortSolver.hpp:87): plane-parallel geometry, Lambertian surface, Fourier
+// azimuth modes, fluxes and intensities at user optical depths and angles.
+// Configurations asking for what the engine does not implement (special
+// boundary conditions, BRDF surfaces, intensity corrections, pseudo-spherical
+// beam, temperature Jacobians, the Fourier-expansion output, stream counts
+// outside 4-16/32/64) pass validate() like in the reference and are rejected
+// with std::invalid_argument when solved.
+// ---------------------------------------------------------------------------
+enum class BoundaryConditionType { General = 0, Special = 1 };
+enum class BrdfType { None = 0, RPV = 1, CoxMunk = 2, Ambrals = 3, Hapke = 4 };
+
+struct DisortFlags {
+  bool use_user_tau = false;
+  bool use_user_mu = false;
+  BoundaryConditionType ibcnd = BoundaryConditionType::General;
+  bool use_lambertian_surface = true;
+  bool use_thermal_emission = false;
+  bool use_spherical_beam = false;
+  bool comp_only_fluxes = false;
+  BrdfType brdf_type = BrdfType::None;
+  bool intensity_corr_buras = false;
+  bool intensity_corr_nakajima = false;
+  bool use_delta_m_plus = false;
+  bool use_diffusion_lower_bc = false;
+  bool output_fourier_expansion = false;
+  bool index_from_bottom = false;
+  bool compute_temperature_jacobian = false;
+};
+
+struct BoundaryConditions {
+  double direct_beam_flux = 0.0;
+  double direct_beam_mu = 0.5;
+  double direct_beam_phi = 0.0;
+  double isotropic_flux_top = 0.0;
+  double isotropic_flux_bottom = 0.0;
+  double temperature_top = 0.0;
+  double temperature_bottom = 0.0;
+  double emissivity_top = 1.0;
+  double surface_albedo = 0.0;
+};
+
+// BRDF parameter sets (DisortConfig.hpp:48-111).  Carried so that configurations
+// written for the reference compile; a non-Lambertian surface is rejected at solve.
+struct RpvBrdfSpec {
+  double rho0 = 0.0, k = 0.0, theta = 0.0, sigma = 0.0, t1 = 0.0, t2 = 0.0, scale = 1.0;
+};
+struct AmbralsBrdfSpec {
+  double iso = 0.0, vol = 0.0, geo = 0.0;
+};
+struct CoxMunkBrdfSpec {
+  double u10 = 0.0, pcl = 0.0, xsal = 0.0, refractive_index = 1.34;
+  bool do_shadow = true;
+};
+struct HapkeBrdfSpec {
+  double b0 = 1.0, hh = 0.06, w = 0.6;
+};
+struct BrdfSpecification {
+  std::optional<RpvBrdfSpec> rpv;
+  std::optional<AmbralsBrdfSpec> ambrals;
+  std::optional<CoxMunkBrdfSpec> cox_munk;
+  std::optional<HapkeBrdfSpec> hapke;
+  void setRpv(const RpvBrdfSpec& spec) { rpv = spec; }
+  void setAmbrals(const AmbralsBrdfSpec& spec) { ambrals = spec; }
+  void setCoxMunk(const CoxMunkBrdfSpec& spec) { cox_munk = spec; }
+  void setHapke(const HapkeBrdfSpec& spec) { hapke = spec; }
+};
+
+class DisortConfig {
+ public:
+  DisortFlags flags;
+  BoundaryConditions bc;
+  BrdfSpecification brdf;
+  int num_layers = 0;
+  int num_phase_func_moments = 0;
+  int num_streams = 0;
+  int num_user_tau = 0;
+  int num_user_mu = 0;
+  int num_phi = 0;
+  int num_phase_func_angles = 0;
+  int nmomNstr() const { return num_phase_func_moments > num_streams ? num_phase_func_moments : num_streams; }
+  double wavenumber_low = 0.0;
+  double wavenumber_high = 0.0;
+  double accuracy_fourier_series = 0.0;
+  double bottom_radius = 0.0;
+  std::vector<double> delta_tau;
+  std::vector<double> single_scat_albedo;
+  std::vector<std::vector<double>> phase_function_moments;
+  std::vector<double> temperature;
+  std::vector<double> level_altitudes;
+  std::vector<double> tau_user;
+  std::vector<double> mu_user;
+  std::vector<double> phi_user;
+  std::vector<double> mu_phase_function;
+  std::vector<std::vector<double>> phase_function;
+
+  DisortConfig() = default;
+  DisortConfig(int nlyr, int nstr, int nmom = 0);
+  void allocate();
+  void validate() const;  // std::invalid_argument with the reference's messages
+  double& phaseFunctionMoments(int k, int lc) { return phase_function_moments[lc][k]; }
+  const double& phaseFunctionMoments(int k, int lc) const { return phase_function_moments[lc][k]; }
+  void setHenyeyGreenstein(double g, int lc = -1);
+  void setIsotropic(int lc = -1);
+  void setRayleigh(int lc = -1);
+  void setHazeGarciaSiewert(int lc = -1);
+  void setCloudGarciaSiewert(int lc = -1);
+  void setPhaseFunction(PhaseFunction type, double g = 0.0, int lc = -1);
+};
+
+// DisortResult (DisortResult.hpp:16-125).  The special-boundary-condition
+// outputs, the Fourier expansion and the temperature Jacobians stay empty.
+class DisortResult {
+ public:
+  std::vector<double> flux_direct_beam, flux_down, flux_up, flux_tau_divergence, mean_intensity,
+      mean_intensity_down, mean_intensity_up, mean_intensity_direct_beam;
+  std::vector<double> albedo_medium, transmissivity_medium;
+  double spherical_albedo = 0.0;
+  double spherical_transmissivity = 0.0;
+  std::vector<double> mu_angles;
+  std::vector<std::vector<std::vector<double>>> intensity;  // [lu][iu][j]
+  std::vector<std::vector<double>> intensity_azimuth_avg;   // [lu][iu]
+  std::vector<std::vector<std::vector<double>>> intensity_fourier_expansion;
+  std::vector<std::vector<double>> flux_up_temperature_jac, flux_down_temperature_jac, mean_intensity_temperature_jac,
+      mean_intensity_down_temperature_jac, mean_intensity_up_temperature_jac, flux_divergence_temperature_jac;
+
+  int num_user_tau() const { return ntau_; }
+  int num_user_mu() const { return numu_; }
+  int num_phi() const { return nphi_; }
+  void allocate(int num_user_tau, int num_user_mu, int num_phi, int num_streams, bool special_bc,
+                bool compute_intensity, bool output_fourier_expansion);
+  double& intensities(int iu, int lu, int j) { return intensity[lu][iu][j]; }
+  const double& intensities(int iu, int lu, int j) const { return intensity[lu][iu][j]; }
+  double& intensitiesAzimuthAvg(int iu, int lu) { return intensity_azimuth_avg[lu][iu]; }
+  const double& intensitiesAzimuthAvg(int iu, int lu) const { return intensity_azimuth_avg[lu][iu]; }
+  double totalFluxDown(int lu) const { return flux_direct_beam[lu] + flux_down[lu]; }
+  double netFlux(int lu) const { return flux_direct_beam[lu] + flux_down[lu] - flux_up[lu]; }
+
+ private:
+  int ntau_ = 0, numu_ = 0, nphi_ = 0;
+};
+
+// DisortSolver::solve (DisortSolver.cpp:20-399): one instance on the GPU.  Like
+// the reference it allocates a config whose delta_tau is empty and fills in the
+// automatic dimensions of `config`: tau_user at the layer boundaries without
+// user optical depths, mu_user at the computational angles without user angles
+// (or with comp_only_fluxes), and phase-function moment 0 set to 1.
+class DisortSolver {
+ public:
+  DisortResult solve(DisortConfig& config);
+};
+
+// Spectral loops of the general solver (python_bindings.cpp:89-127): every band
+// in one dsp_general_bands_solve call.
+std::vector<DisortResult> solveSpectralBands(const DisortConfig& config,
+                                             const std::vector<std::pair<double, double>>& wavenumber_bands,
+                                             const SpectralOverrides& ov = {});
+std::vector<DisortResult> solveSpectral(const DisortConfig& config, const std::vector<double>& wavenumbers,
+                                        const SpectralOverrides& ov = {});
 
 }  // namespace disortpp

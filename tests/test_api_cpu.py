@@ -64,3 +64,123 @@ def test_phase_function_fillers():
     assert math.isclose(c.phase_function_moments[1][1], 2.41260 / 3)
     c.set_phase_function(disortpp.PhaseFunction.CloudGarciaSiewert, 0.0, 0)
     assert math.isclose(c.phase_function_moments[0][2], 3.883 / 5)
+
+
+# ---------------------------------------------------------------------------
+# general path (DisortConfig.cpp:10-248, python_bindings.cpp:221-380)
+# ---------------------------------------------------------------------------
+def test_general_names_and_defaults():
+    for name in ("DisortConfig", "DisortFlags", "BoundaryConditions", "DisortResult", "DisortSolver",
+                 "solve_spectral", "solve_spectral_bands", "BoundaryConditionType", "BrdfType",
+                 "RpvBrdfSpec", "AmbralsBrdfSpec", "CoxMunkBrdfSpec", "HapkeBrdfSpec", "BrdfSpecification"):
+        assert hasattr(disortpp, name), name
+    f = disortpp.DisortFlags()
+    assert f.use_lambertian_surface and not f.use_user_tau and not f.comp_only_fluxes
+    assert f.ibcnd == disortpp.BoundaryConditionType.General and f.brdf_type == disortpp.BrdfType.NONE
+    bc = disortpp.BoundaryConditions()
+    assert (bc.direct_beam_mu, bc.emissivity_top, bc.direct_beam_phi) == (0.5, 1.0, 0.0)
+    c = disortpp.DisortConfig(3, 8, 4)
+    assert c.nmom_nstr() == 8 and c.accuracy_fourier_series == 0.0
+    c.num_user_tau, c.num_user_mu, c.num_phi = 2, 3, 4
+    c.allocate()
+    assert len(c.delta_tau) == 3 and len(c.phase_function_moments[2]) == 9
+    assert (len(c.tau_user), len(c.mu_user), len(c.phi_user)) == (2, 3, 4)
+    assert disortpp.HapkeBrdfSpec().hh == 0.06 and disortpp.CoxMunkBrdfSpec().refractive_index == 1.34
+    r = disortpp.DisortResult()
+    assert (r.num_user_tau(), r.num_user_mu(), r.num_phi()) == (0, 0, 0)
+
+
+def _general_cfg(nlyr=3, nstr=8):
+    c = disortpp.DisortConfig(nlyr, nstr)
+    c.flags.comp_only_fluxes = True
+    c.allocate()
+    c.delta_tau = [0.5] * nlyr
+    c.single_scat_albedo = [0.5] * nlyr
+    c.set_isotropic()
+    return c
+
+
+def test_general_constructor_and_validate_messages():
+    with pytest.raises(ValueError, match="num_layers must be positive"):
+        disortpp.DisortConfig(0, 8)
+    with pytest.raises(ValueError, match="num_streams must be even and >= 4"):
+        disortpp.DisortConfig(2, 6 + 1)
+    with pytest.raises(ValueError, match="num_phase_func_moments must be non-negative"):
+        disortpp.DisortConfig(2, 8, -1)
+    c = _general_cfg()
+    c.validate()
+    c.delta_tau = [0.5, -1.0, 0.5]
+    with pytest.raises(ValueError, match=r"delta_tau\[1\] is negative"):
+        c.validate()
+    c.delta_tau = [0.5] * 3
+    c.flags.comp_only_fluxes = False
+    with pytest.raises(ValueError, match="num_phi must be positive when comp_only_fluxes=false"):
+        c.validate()
+    c.num_phi = 2
+    c.phi_user = [0.0, 400.0]
+    with pytest.raises(ValueError, match=r"phi_user\[1\] must be in \[0, 360\]"):
+        c.validate()
+    c.phi_user = [0.0, 90.0]
+    c.flags.use_user_mu = True
+    c.num_user_mu = 2
+    c.mu_user = [0.5, 0.1]
+    with pytest.raises(ValueError, match="mu_user must be in increasing order"):
+        c.validate()
+    c.mu_user = [0.1, 0.5]
+    c.accuracy_fourier_series = -1.0
+    with pytest.raises(ValueError, match="accuracy_fourier_series must be non-negative"):
+        c.validate()
+    c.accuracy_fourier_series = 0.0
+    c.flags.use_thermal_emission = True
+    c.temperature = [250.0] * 4
+    c.wavenumber_low = c.wavenumber_high = 500.0
+    with pytest.raises(ValueError, match="requires 0 <= wavenumber_low < wavenumber_high"):
+        c.validate()
+
+
+def test_general_index_from_bottom_reports_reference_index():
+    """The reference validates after reversing the layer arrays (DisortSolver.cpp:31-37)."""
+    c = _general_cfg()
+    c.flags.index_from_bottom = True
+    c.delta_tau = [-1.0, 0.5, 0.5]
+    with pytest.raises(ValueError, match=r"delta_tau\[2\] is negative"):
+        disortpp.DisortSolver().solve(c)
+
+
+def test_general_engine_rejections_before_any_gpu_work():
+    solver = disortpp.DisortSolver()
+    cases = [
+        (lambda c: setattr(c.flags, "ibcnd", disortpp.BoundaryConditionType.Special), "ibcnd=Special"),
+        (lambda c: setattr(c.flags, "use_lambertian_surface", False), "BRDF surfaces"),
+        (lambda c: setattr(c.flags, "intensity_corr_nakajima", True), "intensity corrections"),
+        (lambda c: setattr(c.flags, "output_fourier_expansion", True), "output_fourier_expansion"),
+        (lambda c: setattr(c.flags, "compute_temperature_jacobian", True), "compute_temperature_jacobian"),
+    ]
+    for mutate, msg in cases:
+        c = _general_cfg()
+        mutate(c)
+        with pytest.raises(ValueError, match=msg):
+            solver.solve(c)
+    c = disortpp.DisortConfig(2, 18)
+    c.flags.comp_only_fluxes = True
+    c.allocate()
+    with pytest.raises(ValueError, match="num_streams=18 is not supported by the B200 engine"):
+        solver.solve(c)
+    c = _general_cfg()
+    c.flags.use_user_tau = True
+    with pytest.raises(ValueError, match="use_user_tau=true requires num_user_tau > 0"):
+        solver.solve(c)
+
+
+def test_general_spectral_loop_validation():
+    c = _general_cfg()
+    c.flags.use_thermal_emission = True
+    c.temperature = [250.0] * 4
+    # solve_spectral sets wavenumber_low = wavenumber_high, which thermal emission rejects
+    with pytest.raises(ValueError, match="requires 0 <= wavenumber_low < wavenumber_high"):
+        disortpp.solve_spectral(c, [500.0, 510.0])
+    bands = [(500.0, 510.0), (510.0, 520.0)]
+    with pytest.raises(ValueError, match=r"single_scat_albedo\[0\] must be in \[0, 1\]"):
+        disortpp.solve_spectral_bands(c, bands, single_scat_albedo=[[0.5] * 3, [1.5, 0.5, 0.5]])
+    with pytest.raises(ValueError, match="surface_albedo override has 1 entries for 2 bands"):
+        disortpp.solve_spectral_bands(c, bands, surface_albedo=[0.1])

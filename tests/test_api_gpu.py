@@ -83,3 +83,137 @@ def test_single_wavenumber_spectral_loop():
     w = _as_workload(c, 900.0, 900.0)
     ref, st = oracle_lib.flux_solve(w)
     assert_parity({f: np.array(getattr(res[1], f))[None, :] for f in capi.FLUX_OUT_FIELDS}, ref, "lo == hi")
+
+
+# ---------------------------------------------------------------------------
+# general path: DisortSolver / solve_spectral_bands against the general oracle
+# ---------------------------------------------------------------------------
+from parity import assert_parity_general  # noqa: E402
+
+
+def _general_cfg(nlyr=4, nstr=16, user_tau=True, user_mu=True, only_fluxes=False):
+    c = disortpp.DisortConfig(nlyr, nstr, nstr + 4)
+    f = c.flags
+    f.use_user_tau, f.use_user_mu, f.comp_only_fluxes = user_tau, user_mu, only_fluxes
+    f.use_thermal_emission = True
+    c.wavenumber_low, c.wavenumber_high = 500.0, 520.0
+    c.bc.direct_beam_flux, c.bc.direct_beam_mu, c.bc.direct_beam_phi = 1.0, 0.6, 30.0
+    c.bc.surface_albedo, c.bc.isotropic_flux_top = 0.2, 0.05
+    c.bc.temperature_top, c.bc.temperature_bottom = 200.0, 290.0
+    c.num_user_tau, c.num_user_mu, c.num_phi = 3, 4, 3
+    c.allocate()
+    c.delta_tau = [0.1, 0.5, 1.0, 2.0][:nlyr]
+    c.single_scat_albedo = [0.9, 0.5, 0.2, 0.95][:nlyr]
+    c.temperature = [200.0 + 20 * k for k in range(nlyr + 1)]
+    c.set_henyey_greenstein(0.75)
+    if user_tau:
+        c.tau_user = [0.0, 0.35, 3.6]
+    if user_mu:
+        c.mu_user = [-0.8, -0.2, 0.3, 1.0]
+    c.phi_user = [0.0, 45.0, 170.0]
+    return c
+
+
+def _oracle_inst(c, lo, hi, **over):
+    inst = dict(num_streams=c.num_streams, num_layers=c.num_layers,
+                num_phase_func_moments=c.num_phase_func_moments,
+                delta_tau=list(c.delta_tau), single_scat_albedo=list(c.single_scat_albedo),
+                phase_function_moments=[list(r) for r in c.phase_function_moments],
+                temperature=list(c.temperature), wavenumber_low=lo, wavenumber_high=hi,
+                surface_albedo=c.bc.surface_albedo, emissivity_top=c.bc.emissivity_top,
+                direct_beam_flux=c.bc.direct_beam_flux, direct_beam_mu=c.bc.direct_beam_mu,
+                direct_beam_phi=c.bc.direct_beam_phi, isotropic_flux_top=c.bc.isotropic_flux_top,
+                isotropic_flux_bottom=c.bc.isotropic_flux_bottom, temperature_top=c.bc.temperature_top,
+                temperature_bottom=c.bc.temperature_bottom)
+    f = c.flags
+    if f.use_user_tau:
+        inst["tau_user"] = list(c.tau_user)[:c.num_user_tau]
+    if f.use_user_mu:
+        inst["mu_user"] = list(c.mu_user)[:c.num_user_mu]
+    if not f.comp_only_fluxes:
+        inst["phi_user"] = list(c.phi_user)[:c.num_phi]
+    inst.update(over)
+    return inst
+
+
+def _general_flags(c):
+    f = c.flags
+    return ((capi.FLAG_THERMAL if f.use_thermal_emission else 0)
+            | (capi.FLAG_INDEX_FROM_BOTTOM if f.index_from_bottom else 0)
+            | (capi.GFLAG_USER_TAU if f.use_user_tau else 0)
+            | (capi.GFLAG_USER_MU if f.use_user_mu else 0)
+            | (capi.GFLAG_ONLY_FLUXES if f.comp_only_fluxes else 0))
+
+
+def _as_outputs(results, with_intensity):
+    got = {f: np.array([getattr(r, f) for r in results]) for f in capi.FLUX_OUT_FIELDS}
+    if with_intensity:
+        got["intensity"] = np.array([r.intensity for r in results])
+        got["intensity_azimuth_avg"] = np.array([r.intensity_azimuth_avg for r in results])
+    return got
+
+
+def _oracle(c, insts, with_intensity):
+    ref = oracle_lib.general_solve(capi.pack_general(insts, _general_flags(c), c.accuracy_fourier_series))
+    assert (ref["status"] == 0).all()
+    if not with_intensity:
+        ref = {f: ref[f] for f in capi.FLUX_OUT_FIELDS}
+    return ref
+
+
+@pytest.mark.parametrize("ifb", [False, True])
+def test_disort_solver_matches_oracle(ifb):
+    c = _general_cfg()
+    c.flags.index_from_bottom = ifb
+    r = disortpp.DisortSolver().solve(c)
+    assert (r.num_user_tau(), r.num_user_mu(), r.num_phi()) == (3, 4, 3)
+    assert r.mu_angles == [-0.8, -0.2, 0.3, 1.0]
+    ref = _oracle(c, [_oracle_inst(c, 500.0, 520.0)], True)
+    assert_parity_general(_as_outputs([r], True), ref, f"DisortSolver ifb={ifb}")
+    assert r.intensities(3, 2, 1) == r.intensity[2][3][1]
+    assert r.intensities_azimuth_avg(1, 0) == r.intensity_azimuth_avg[0][1]
+
+
+def test_disort_solver_automatic_dimensions():
+    """Without user depths and angles the config is completed like the reference's
+    (outputs at the layer boundaries, computational angles, intensity arrays
+    allocated at those angles and left zero)."""
+    c = _general_cfg(user_tau=False, user_mu=False)
+    r = disortpp.DisortSolver().solve(c)
+    L, N = c.num_layers, c.num_streams
+    assert c.num_user_tau == L + 1 and r.num_user_tau() == L + 1
+    np.testing.assert_allclose(c.tau_user, np.concatenate([[0.0], np.cumsum(c.delta_tau)]), rtol=0, atol=0)
+    assert c.num_user_mu == N and r.mu_angles == list(c.mu_user)
+    mu = np.array(c.mu_user)
+    assert np.all(np.diff(mu[:N // 2]) != 0) and np.allclose(mu[:N // 2], -mu[N // 2:][::-1])
+    assert all(row[0] == 1.0 for row in c.phase_function_moments)
+    assert np.array(r.intensity).shape == (L + 1, N, 3) and not np.array(r.intensity).any()
+    ref = _oracle(c, [_oracle_inst(c, 500.0, 520.0)], False)
+    assert_parity_general(_as_outputs([r], False), ref, "automatic dimensions")
+
+
+def test_disort_solver_only_fluxes():
+    c = _general_cfg(only_fluxes=True)
+    r = disortpp.DisortSolver().solve(c)
+    assert r.intensity == [] and r.num_user_mu() == c.num_streams
+    ref = _oracle(c, [_oracle_inst(c, 500.0, 520.0)], False)
+    assert_parity_general(_as_outputs([r], False), ref, "comp_only_fluxes")
+
+
+def test_general_spectral_bands_with_overrides_match_oracle():
+    c = _general_cfg()
+    c.accuracy_fourier_series = 1e-4
+    rng = np.random.default_rng(5)
+    n = 24
+    bands = [(300.0 + 5 * i, 305.0 + 5 * i) for i in range(n)]
+    dtau = rng.uniform(0.01, 3.0, (n, 4))
+    alb = rng.uniform(0, 0.5, n)
+    fbeam = rng.uniform(0.5, 2.0, n)
+    res = disortpp.solve_spectral_bands(c, bands, delta_tau=dtau.tolist(), surface_albedo=alb.tolist(),
+                                        direct_beam_flux=fbeam.tolist())
+    insts = [_oracle_inst(c, *bands[i], delta_tau=list(dtau[i]), surface_albedo=float(alb[i]),
+                          direct_beam_flux=float(fbeam[i])) for i in range(n)]
+    ref = _oracle(c, insts, True)
+    assert_parity_general(_as_outputs(res, True), ref, "solve_spectral_bands")
+    # the caller's config is not modified by the spectral loop
+    assert c.num_user_tau == 3 and list(c.delta_tau) == [0.1, 0.5, 1.0, 2.0]
