@@ -34,7 +34,7 @@ import numpy as np
 REPO = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, REPO)
 
-from disort_b200 import capi, flops, workloads  # noqa: E402
+from disort_b200 import capi, flops, replicas, workloads  # noqa: E402
 
 METRIC = "solves/s (60 lyr,16 str): plain GPU vs gated surrogate at ≤0.5% flux err"
 
@@ -218,7 +218,6 @@ def committed_traffic(workload_name: str, kernel: str):
 
 def run_e2e(args, ctx, w, douts, stream, dev, world):
     import torch
-    import torch.distributed as dist
     n, L, N = w["n_inst"], w["num_layers"], w["num_streams"]
     host_arrays = {}
     h2d = 0
@@ -245,8 +244,7 @@ def run_e2e(args, ctx, w, douts, stream, dev, world):
 
     for _ in range(max(1, args.warmup)):
         hstep()
-    if world > 1:
-        dist.barrier()
+    replicas.barrier()
     torch.cuda.synchronize()
     e2 = torch.cuda.Event(enable_timing=True)
     e3 = torch.cuda.Event(enable_timing=True)
@@ -255,10 +253,8 @@ def run_e2e(args, ctx, w, douts, stream, dev, world):
         hstep()
     e3.record(stream)
     torch.cuda.synchronize()
-    te = torch.tensor([e2.elapsed_time(e3)], dtype=torch.float64, device=dev)
-    if world > 1:
-        dist.all_reduce(te, op=dist.ReduceOp.MAX)
-    e2e_value = n * args.steps * world / (float(te.item()) / 1000.0)
+    replicas.barrier()
+    e2e_value = replicas.job_rate(n, args.steps, world, replicas.max_over_ranks(e2.elapsed_time(e3), dev))
     # host results must equal the device-resident results
     same = all(torch.equal(houts[f], douts[f].cpu()) for f in capi.FLUX_OUT_FIELDS)
 
@@ -267,14 +263,9 @@ def run_e2e(args, ctx, w, douts, stream, dev, world):
 
 def run_ours(args):
     import torch
-    import torch.distributed as dist
-    world = int(os.environ.get("WORLD_SIZE", "1"))
-    rank = int(os.environ.get("RANK", "0"))
-    local = int(os.environ.get("LOCAL_RANK", "0"))
+    rank, local, world = replicas.rank_env()
     torch.cuda.set_device(local)
-    if world > 1:
-        import datetime
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+    replicas.init("nccl", 120.0)
     dev = torch.device("cuda", local)
     stream = torch.cuda.current_stream()
 
@@ -322,8 +313,7 @@ def run_ours(args):
     # ---- timed region: device-resident inputs --------------------------------
     ctx.set_timing(True)
     ctx.timing_reset()
-    if world > 1:
-        dist.barrier()
+    replicas.barrier()
     torch.cuda.synchronize()
     clocks.start()
     e0 = torch.cuda.Event(enable_timing=True)
@@ -333,17 +323,13 @@ def run_ours(args):
         step()
     e1.record(stream)
     torch.cuda.synchronize()
-    if world > 1:
-        dist.barrier()
+    replicas.barrier()
     ms = e0.elapsed_time(e1)
     clk = clocks.stop()
     ktimes = ctx.timings()
     ctx.set_timing(False)
-    t = torch.tensor([ms], dtype=torch.float64, device=dev)
-    if world > 1:
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-    ms_max = float(t.item())
-    value = n * args.steps * world / (ms_max / 1000.0)
+    ms_max = replicas.max_over_ranks(ms, dev)
+    value = replicas.job_rate(n, args.steps, world, ms_max)
 
     # ---- e2e: through the C ABI with pinned host buffers ----------------------
     if args.no_e2e:
@@ -385,8 +371,7 @@ def run_ours(args):
             line["surrogate"] = surrogate_leg(ctx)
         print(json.dumps(line), flush=True)
     ctx.close()
-    if world > 1:
-        dist.destroy_process_group()
+    replicas.finish()
 
 
 def surrogate_leg(ctx) -> dict:
@@ -458,10 +443,7 @@ def general_cpu_sample(insts, target_s: float):
 
 def run_general(args):
     import torch
-    import torch.distributed as dist
-    world = int(os.environ.get("WORLD_SIZE", "1"))
-    rank = int(os.environ.get("RANK", "0"))
-    local = int(os.environ.get("LOCAL_RANK", "0"))
+    rank, local, world = replicas.rank_env()
     n = args.bands or 4096
     if args.impl == "reference":
         if rank != 0:
@@ -483,12 +465,10 @@ def run_general(args):
             "e2e": {"value": value, "unit": "solves/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}), flush=True)
         return
     torch.cuda.set_device(local)
-    if world > 1:
-        import datetime
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+    replicas.init("nccl", 300.0)
     dev = torch.device("cuda", local)
     stream = torch.cuda.current_stream()
-    insts, d, fl = general_batch(n, 3 + rank)
+    insts, d, fl = general_batch(n, replicas.replica_seed(3, rank))
     ctx = capi.Context(local, stream.cuda_stream)
     dd = dict(d)
     for k in ("num_streams", "num_layers", "layer_offset", "num_phase_func_moments", "delta_tau",
@@ -532,8 +512,7 @@ def run_general(args):
     clocks = ClockSampler(str(local))
     ctx.set_timing(True)
     ctx.timing_reset()
-    if world > 1:
-        dist.barrier()
+    replicas.barrier()
     torch.cuda.synchronize()
     clocks.start()
     e0 = torch.cuda.Event(enable_timing=True)
@@ -543,15 +522,13 @@ def run_general(args):
         step(batch, dout)
     e1.record(stream)
     torch.cuda.synchronize()
+    replicas.barrier()
     ms = e0.elapsed_time(e1)
     clk = clocks.stop()
     ktimes = ctx.timings()
     ctx.set_timing(False)
-    t = torch.tensor([ms], dtype=torch.float64, device=dev)
-    if world > 1:
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-    ms_max = float(t.item())
-    value = n * args.steps * world / (ms_max / 1000.0)
+    ms_max = replicas.max_over_ranks(ms, dev)
+    value = replicas.job_rate(n, args.steps, world, ms_max)
     e2e = None
     if not args.no_e2e:
         hb, hkeep = capi.make_general_batch(d)
@@ -563,6 +540,7 @@ def run_general(args):
         d2h = sum(int(v.numel() * v.element_size()) for v in houts.values())
         step(hb, hout)
         torch.cuda.synchronize()
+        replicas.barrier()
         e2 = torch.cuda.Event(enable_timing=True)
         e3 = torch.cuda.Event(enable_timing=True)
         e2.record(stream)
@@ -570,11 +548,10 @@ def run_general(args):
             step(hb, hout)
         e3.record(stream)
         torch.cuda.synchronize()
-        te = torch.tensor([e2.elapsed_time(e3)], dtype=torch.float64, device=dev)
-        if world > 1:
-            dist.all_reduce(te, op=dist.ReduceOp.MAX)
+        replicas.barrier()
+        te_max = replicas.max_over_ranks(e2.elapsed_time(e3), dev)
         same = all(torch.equal(houts[f], douts[f].cpu()) for f in houts)
-        e2e = {"value": n * args.steps * world / (float(te.item()) / 1000.0), "unit": "solves/s",
+        e2e = {"value": replicas.job_rate(n, args.steps, world, te_max), "unit": "solves/s",
                "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h, "matches_device_result": same}
     dom = max((k for k in ktimes if k in fl), key=lambda k: ktimes[k][0])
     dom_ms, dom_launches = ktimes[dom]
@@ -605,8 +582,7 @@ def run_general(args):
             "e2e": e2e, "gpu_launches": int(sum(v[1] for v in ktimes.values())), "roofline": roofline,
             "cpu_baseline": cpu, "clocks": clk, "bad_status_instances": bad}), flush=True)
     ctx.close()
-    if world > 1:
-        dist.destroy_process_group()
+    replicas.finish()
 
 
 # ---------------------------------------------------------------------------

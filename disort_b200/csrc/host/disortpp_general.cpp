@@ -293,7 +293,8 @@ dsp_general_batch pack_general(const DisortConfig& c, const std::vector<std::pai
   b.flags = (f.use_thermal_emission ? DSP_FLAG_THERMAL : 0u) | (f.use_delta_m_plus ? DSP_FLAG_DELTA_M_PLUS : 0u) |
             (f.use_diffusion_lower_bc ? DSP_FLAG_DIFFUSION_LOWER_BC : 0u) |
             (f.index_from_bottom ? DSP_FLAG_INDEX_FROM_BOTTOM : 0u) | (f.use_user_tau ? DSP_GFLAG_USER_TAU : 0u) |
-            (f.use_user_mu ? DSP_GFLAG_USER_MU : 0u) | (f.comp_only_fluxes ? DSP_GFLAG_ONLY_FLUXES : 0u);
+            (f.use_user_mu && !f.comp_only_fluxes ? DSP_GFLAG_USER_MU : 0u) |
+            (f.comp_only_fluxes ? DSP_GFLAG_ONLY_FLUXES : 0u);
   pk.nstr.assign(n, c.num_streams);
   pk.nlyr.assign(n, L);
   pk.nmom.assign(n, c.num_phase_func_moments);
@@ -335,7 +336,9 @@ dsp_general_batch pack_general(const DisortConfig& c, const std::vector<std::pai
     b.num_user_tau = c.num_user_tau;
     b.tau_user = {pk.utau.data(), 0};
   }
-  if (f.use_user_mu) {
+  // with comp_only_fluxes the reference replaces mu_user by the computational
+  // angles (DisortSolver.cpp:62-66) and computes no intensities
+  if (f.use_user_mu && !f.comp_only_fluxes) {
     pk.umu.assign(c.mu_user.begin(), c.mu_user.begin() + c.num_user_mu);
     b.num_user_mu = c.num_user_mu;
     b.mu_user = {pk.umu.data(), 0};

@@ -128,7 +128,7 @@ def _oracle_inst(c, lo, hi, **over):
     f = c.flags
     if f.use_user_tau:
         inst["tau_user"] = list(c.tau_user)[:c.num_user_tau]
-    if f.use_user_mu:
+    if f.use_user_mu and not f.comp_only_fluxes:
         inst["mu_user"] = list(c.mu_user)[:c.num_user_mu]
     if not f.comp_only_fluxes:
         inst["phi_user"] = list(c.phi_user)[:c.num_phi]
@@ -141,7 +141,7 @@ def _general_flags(c):
     return ((capi.FLAG_THERMAL if f.use_thermal_emission else 0)
             | (capi.FLAG_INDEX_FROM_BOTTOM if f.index_from_bottom else 0)
             | (capi.GFLAG_USER_TAU if f.use_user_tau else 0)
-            | (capi.GFLAG_USER_MU if f.use_user_mu else 0)
+            | (capi.GFLAG_USER_MU if f.use_user_mu and not f.comp_only_fluxes else 0)
             | (capi.GFLAG_ONLY_FLUXES if f.comp_only_fluxes else 0))
 
 
