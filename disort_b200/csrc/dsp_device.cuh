@@ -235,6 +235,46 @@ __device__ __forceinline__ void team_argmax(double& v, int& idx, double* red) {
   }
 }
 
+// Arg-max of a >= 0 over the candidate lanes of a full warp, ties to the lowest
+// lane; 32 when no lane is a candidate.  Non-negative doubles order like their
+// bit patterns, so the maximum is two 32-bit warp reductions (high words, then
+// the low words of the lanes that tie on the high word) and the winner is the
+// lowest lane of the ballot of exact matches.  `zero` reports a maximum of 0.
+__device__ __forceinline__ int warp_argmax_nonneg(double a, bool cand, bool& zero) {
+  const unsigned long long b = static_cast<unsigned long long>(__double_as_longlong(a));
+  const unsigned hi = cand ? static_cast<unsigned>(b >> 32) : 0u;
+  const unsigned mhi = __reduce_max_sync(0xffffffffu, hi);
+  const bool tie = cand && hi == mhi;
+  const unsigned lo = tie ? static_cast<unsigned>(b) : 0u;
+  const unsigned mlo = __reduce_max_sync(0xffffffffu, lo);
+  const unsigned win = __ballot_sync(0xffffffffu, tie && static_cast<unsigned>(b) == mlo);
+  zero = (mhi | mlo) == 0u;
+  return win ? __ffs(win) - 1 : 32;
+}
+
+// Team copy of nd doubles from global to shared memory: 16-byte cp.async
+// (LDGSTS) chunks when both ends are 16-byte aligned and nd is even, plain
+// loads and stores otherwise.  The copies are waited for with cp_async_wait
+// and made visible to the team by the next team barrier.  Plain (coherent)
+// loads: the source may have been written by this kernel.
+template <int TEAM>
+__device__ __forceinline__ void team_copy_async(double* dst, const double* src, int nd, int t) {
+  const bool al = ((reinterpret_cast<uintptr_t>(dst) | reinterpret_cast<uintptr_t>(src)) & 15u) == 0 && (nd & 1) == 0;
+  if (al) {
+    const unsigned s0 = static_cast<unsigned>(__cvta_generic_to_shared(dst));
+    for (int k = t; k < nd / 2; k += TEAM)
+      asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(s0 + 16u * k), "l"(src + 2 * k) : "memory");
+  } else {
+    for (int k = t; k < nd; k += TEAM) dst[k] = src[k];
+  }
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+// wait until at most N of this thread's most recent groups are pending
+template <int N>
+__device__ __forceinline__ void cp_async_wait() {
+  asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory");
+}
+
 __device__ __forceinline__ void set_status(int32_t* status, int i, int code) {
   if (status) atomicMax(status + i, code);
 }

@@ -7,16 +7,28 @@
 //  - slot thread s holds its row as cur[N] (columns of x_l), nxt[N] (columns of
 //    x_{l+1}) and rhs; carried rows move nxt -> cur between layers;
 //  - the pivot of column c is an arg-max of |cur[c]| over candidate slots
-//    (shuffles), only the pivot row is broadcast through shared memory;
+//    (warp reductions of the bit patterns for a full-warp team, shuffles
+//    otherwise); only the pivot row and its negated reciprocal are broadcast
+//    through shared memory;
 //  - free slots (last layer's pivot rows) receive the new continuity rows in
 //    slot order, each thread finding its row index by a popcount;
 //  - W_l = U^{-1}[V | c] is a column-oriented back substitution across the
-//    pivot-row owners, one row of X broadcast per step.
+//    pivot-row owners, one row of X broadcast per step;
+//  - the layer records (and, going back up, the W_l records) are brought into
+//    a shared-memory ring with cp.async one layer ahead of their use, so the
+//    elimination of a layer hides the memory latency of the next one.
 #pragma once
 
 #include "dsp_device.cuh"
 
 namespace dsp {
+
+#ifndef DSP_BVP_REGS
+#define DSP_BVP_REGS 128
+#endif
+
+// record element read (records are staged in shared memory)
+__device__ __forceinline__ double ld_rec(const double* q) { return *q; }
 
 template <int N>
 struct RCfg {
@@ -27,21 +39,28 @@ struct RCfg {
   static constexpr int TPC = CTA / TEAM;
   static constexpr int XS = N + 1;  // row stride of the X matrix (next block + rhs)
   // team shared memory (doubles)
-  static constexpr int O_BUF = 0;              // pivot row: cur[N] nxt[N] rhs
-  static constexpr int O_X = O_BUF + 2 * N + 1;  // X[N][N+1]
+  static constexpr int O_BUF = 0;                  // 2 x pivot row: cur[N] nxt[N] rhs, -1/pivot
+  static constexpr int O_X = O_BUF + 2 * (2 * N + 2);  // X[N][N+1]
   static constexpr int O_XV = O_X + N * XS;    // x ping-pong [2][N]
   static constexpr int O_EC = O_XV + 2 * N;    // [N]
   static constexpr int O_I = O_EC + N;         // intensities [N]
   static constexpr int O_E = O_I + N;          // exp(eig*dtau) of layers l, l+1 [2][NN]
   static constexpr int O_MISC = O_E + 2 * NN;  // 8
   static constexpr int O_PIV = O_MISC + 8;     // int pivot slot per column [N]
-  static constexpr int TEAM_SMEM = round4(O_PIV + N / 2 + 1);
-  static constexpr int TAB = tab_size(N);
+  // record ring: 3 layer records going down; 2 x (layer record + W record) going up
+  static constexpr int RS = lrec_stride(N);
+  static constexpr int BS = brec_stride(N);
+  static constexpr int O_RING = round4(O_PIV + N / 2 + 1);
+  static constexpr int RING = imax(3 * RS, 2 * (RS + BS));
+  static constexpr int TEAM_SMEM = round4(O_RING + RING);
+  static constexpr int TAB = 2 * N;  // mu and wt of the constant tables
+  // register budget per thread: 128 keeps 16 single-warp CTAs resident per SM
+  static constexpr int MINB = 65536 / (CTA * DSP_BVP_REGS);
   static constexpr size_t smem_bytes() { return sizeof(double) * (size_t)(TAB + TPC * TEAM_SMEM); }
 };
 
 template <int N, bool GEN = false>
-__global__ void __launch_bounds__(RCfg<N>::CTA) flux_bvp_reg_kernel(FluxParams p) {
+__global__ void __launch_bounds__(RCfg<N>::CTA, RCfg<N>::MINB) flux_bvp_reg_kernel(FluxParams p) {
   using C = RCfg<N>;
   constexpr int NN = C::NN, TEAM = C::TEAM, PR = C::PR, XS = C::XS;
   constexpr double PI = 3.14159265358979323846;
@@ -121,13 +140,17 @@ __global__ void __launch_bounds__(RCfg<N>::CTA) flux_bvp_reg_kernel(FluxParams p
   auto LR = [&](int l) { return lrec0 + (long long)l * lstride; };
 
   double* sm = smem + C::TAB + team * C::TEAM_SMEM;
-  double* buf = sm + C::O_BUF;
+  double* bufs = sm + C::O_BUF;
   double* X = sm + C::O_X;
   double* XV = sm + C::O_XV;
   double* ec = sm + C::O_EC;
   double* Iv = sm + C::O_I;
   double* E = sm + C::O_E;
   int* pivslot = reinterpret_cast<int*>(sm + C::O_PIV);
+  constexpr int RS = C::RS, BS = C::BS;
+  double* ring = sm + C::O_RING;
+  auto RF = [&](int l) { return ring + (l % 3) * RS; };        // going down: layer l's record
+  auto RB = [&](int l) { return ring + (l & 1) * (RS + BS); };  // going up: layer record, then W_l
 
   double cur[N], nxt[N], rhs = 0.0;
 #pragma unroll
@@ -135,31 +158,51 @@ __global__ void __launch_bounds__(RCfg<N>::CTA) flux_bvp_reg_kernel(FluxParams p
   bool singular = false;
 
   // ------------------------------------------------------------------ forward
-  if (t < NN) E[t] = exp(LR(0)[lrec_eig(N) + t] * dtau_s[0]);
+  team_copy_async<TEAM>(RF(0), LR(0), RS, t);
+  cp_async_commit();
+  if (ncut > 1) team_copy_async<TEAM>(RF(1), LR(1), RS, t);
+  cp_async_commit();
+  cp_async_wait<1>();
+  __syncwarp(msk);
+  if (t < NN) E[t] = exp(RF(0)[lrec_eig(N) + t] * dtau_s[0]);
   __syncwarp(msk);
   // top boundary rows in slots 0..NN-1 (setMatrix :890-907, solve0 :978-990)
   if (t < NN) {
-    const double* l0 = LR(0);
+    const double* l0 = RF(0);
     const int jq = NN - 1 - t;
 #pragma unroll
     for (int iq = 0; iq < N; ++iq) {
-      const double g = __ldg(l0 + lrec_G(N) + jq * N + iq);
+      const double g = ld_rec(l0 + lrec_G(N) + jq * N + iq);
       cur[iq] = (iq < NN) ? g * E[iq] : g;
     }
     double s = 0.0;
-    if (beam) s -= __ldg(l0 + lrec_zb(N) + jq);
-    if (thermal) s -= __ldg(l0 + lrec_z0(N) + jq);
+    if (beam) s -= ld_rec(l0 + lrec_zb(N) + jq);
+    if (thermal) s -= ld_rec(l0 + lrec_z0(N) + jq);
     s += fisot + ptop;
     rhs = s;
   }
   unsigned carried = (1u << NN) - 1u;  // slots holding carried (un-pivoted) rows
 
+  double rdiag = 0.0;  // 1 / pivot of this thread's pivot row
+  // per-layer scalars of the instance record, loaded one layer ahead
+  double dts_n = ncut > 1 ? dtau_s[1] : 0.0, btr_n = btr[1], tau_n = taus[1];
   for (int l = 0; l < ncut; ++l) {
     const bool last = (l == ncut - 1);
-    const double* lr = LR(l);
+    const double dts1 = dts_n, btr1 = btr_n, tau1 = tau_n;  // values at l + 1
+    if (l + 2 <= ncut) {
+      dts_n = (l + 2 < ncut) ? dtau_s[l + 2] : 0.0;
+      btr_n = btr[l + 2];
+      tau_n = taus[l + 2];
+    }
+    // record l+2 starts loading into the slot of record l-1; record l+1 is waited for
+    if (l + 2 < ncut) team_copy_async<TEAM>(RF(l + 2), LR(l + 2), RS, t);
+    cp_async_commit();
+    cp_async_wait<1>();
+    __syncwarp(msk);
+    const double* lr = RF(l);
     const double* Ecur = E + (l & 1) * NN;
     double* Enext = E + ((l & 1) ^ 1) * NN;
-    if (!last && t < NN) Enext[t] = exp(LR(l + 1)[lrec_eig(N) + t] * dtau_s[l + 1]);
+    if (!last && t < NN) Enext[t] = exp(RF(l + 1)[lrec_eig(N) + t] * dts1);
     __syncwarp(msk);
     // new rows into the free slots, in slot order
     const unsigned freem = ((PR == 32) ? 0xffffffffu : ((1u << PR) - 1u)) & ~carried;
@@ -171,25 +214,25 @@ __global__ void __launch_bounds__(RCfg<N>::CTA) flux_bvp_reg_kernel(FluxParams p
       if (!last) {
         // continuity row jq of interface (l, l+1) (setMatrix :852-887, solve0 :1080-1104)
         const int jq = rank;
-        const double* ln = LR(l + 1);
+        const double* ln = RF(l + 1);
         const double* Gl = lr + lrec_G(N) + jq * N;
         const double* Gn = ln + lrec_G(N) + jq * N;
 #pragma unroll
         for (int iq = 0; iq < N; ++iq) {
-          const double g = __ldg(Gl + iq);
+          const double g = ld_rec(Gl + iq);
           cur[iq] = (iq < NN) ? g : g * Ecur[N - 1 - iq];
-          const double h = __ldg(Gn + iq);
+          const double h = ld_rec(Gn + iq);
           nxt[iq] = (iq < NN) ? -h * Enext[iq] : -h;
         }
-        const double T = btr[l + 1], tau = taus[l + 1];
+        const double T = btr1, tau = tau1;
         double sum = 0.0;
         if (beam) {
-          sum += __ldg(ln + lrec_zb(N) + jq) * T;
-          sum -= __ldg(lr + lrec_zb(N) + jq) * T;
+          sum += ld_rec(ln + lrec_zb(N) + jq) * T;
+          sum -= ld_rec(lr + lrec_zb(N) + jq) * T;
         }
         if (thermal) {
-          sum += __ldg(ln + lrec_z0(N) + jq) - __ldg(lr + lrec_z0(N) + jq);
-          sum += (__ldg(ln + lrec_z1(N) + jq) - __ldg(lr + lrec_z1(N) + jq)) * tau;
+          sum += ld_rec(ln + lrec_z0(N) + jq) - ld_rec(lr + lrec_z0(N) + jq);
+          sum += (ld_rec(ln + lrec_z1(N) + jq) - ld_rec(lr + lrec_z1(N) + jq)) * tau;
         }
         rhs = sum;
       } else {
@@ -199,22 +242,22 @@ __global__ void __launch_bounds__(RCfg<N>::CTA) flux_bvp_reg_kernel(FluxParams p
         const double* Gl = lr + lrec_G(N);
 #pragma unroll
         for (int iq = 0; iq < N; ++iq) {
-          double base = __ldg(Gl + jq * N + iq);
+          double base = ld_rec(Gl + jq * N + iq);
           if (!plain) {
             double refl = 0.0;
-            for (int k = 0; k < NN; ++k) refl += wt[k] * mu[k] * alb * __ldg(Gl + (NN - 1 - k) * N + iq);
+            for (int k = 0; k < NN; ++k) refl += wt[k] * mu[k] * alb * ld_rec(Gl + (NN - 1 - k) * N + iq);
             base = base - 2.0 * refl;
           }
           cur[iq] = (iq < NN) ? base : base * Ecur[N - 1 - iq];
           nxt[iq] = 0.0;
         }
-        const double T = btr[ncut], tau = taus[ncut];
+        const double T = btr1, tau = tau1;
         double sum = 0.0;
         if (dlbc) {
-          if (beam) sum -= __ldg(lr + lrec_zb(N) + NN + rb) * T;
+          if (beam) sum -= ld_rec(lr + lrec_zb(N) + NN + rb) * T;
           if (thermal) {
-            sum -= __ldg(lr + lrec_z0(N) + NN + rb);
-            sum -= __ldg(lr + lrec_z1(N) + NN + rb) * tau;
+            sum -= ld_rec(lr + lrec_z0(N) + NN + rb);
+            sum -= ld_rec(lr + lrec_z1(N) + NN + rb) * tau;
           }
           sum += pbot + mu[rb] * pbotd;
         } else {
@@ -222,19 +265,19 @@ __global__ void __launch_bounds__(RCfg<N>::CTA) flux_bvp_reg_kernel(FluxParams p
             double refl = 0.0;
             for (int jj = 0; jj < NN; ++jj) {
               double ps = 0.0;
-              if (beam) ps += __ldg(lr + lrec_zb(N) + NN - 1 - jj) * T;
-              if (thermal) ps += __ldg(lr + lrec_z0(N) + NN - 1 - jj) + __ldg(lr + lrec_z1(N) + NN - 1 - jj) * tau;
+              if (beam) ps += ld_rec(lr + lrec_zb(N) + NN - 1 - jj) * T;
+              if (thermal) ps += ld_rec(lr + lrec_z0(N) + NN - 1 - jj) + ld_rec(lr + lrec_z1(N) + NN - 1 - jj) * tau;
               refl += wt[jj] * mu[jj] * alb * ps;
             }
             sum += 2.0 * refl;
           }
           if (beam) {
-            sum -= __ldg(lr + lrec_zb(N) + NN + rb) * T;
+            sum -= ld_rec(lr + lrec_zb(N) + NN + rb) * T;
             if (!lyrcut) sum += alb * umu0 * fbeam * T / PI;
           }
           if (thermal) {
-            sum -= __ldg(lr + lrec_z0(N) + NN + rb);
-            sum -= __ldg(lr + lrec_z1(N) + NN + rb) * tau;
+            sum -= ld_rec(lr + lrec_z0(N) + NN + rb);
+            sum -= ld_rec(lr + lrec_z1(N) + NN + rb) * tau;
           }
           sum += fisob;
           if (thermal) sum += (1.0 - alb) * pbot;
@@ -255,36 +298,42 @@ __global__ void __launch_bounds__(RCfg<N>::CTA) flux_bvp_reg_kernel(FluxParams p
     int myc = -1;  // pivot column of this thread's row, if it becomes a pivot row
 #pragma unroll
     for (int c = 0; c < N; ++c) {
-      double v = -1.0;
-      int idx = PR;
-      if (t < PR && ((cand >> t) & 1u)) {
-        double a = fabs(cur[c]);
-        if (isnan(a)) a = __longlong_as_double(0x7ff0000000000000ll);  // NaN ranks as +inf: one total order
-        v = a;
-        idx = t;
+      const bool isc = t < PR && ((cand >> t) & 1u);
+      double a = fabs(cur[c]);
+      if (isnan(a)) a = __longlong_as_double(0x7ff0000000000000ll);  // NaN ranks as +inf: one total order
+      int idx;
+      bool zero_piv;
+      if constexpr (TEAM == 32) {
+        idx = warp_argmax_nonneg(a, isc, zero_piv);
+      } else {
+        double v = isc ? a : -1.0;
+        idx = isc ? t : PR;
+        team_argmax<TEAM>(v, idx, nullptr);
+        zero_piv = v == 0.0;
       }
-      team_argmax<TEAM>(v, idx, nullptr);
       const int ps = idx < PR ? idx : 0;
-      const double pv = __shfl_sync(msk, cur[c], ps, TEAM);
       cand &= ~(1u << ps);
       if (t == ps) myc = c;
       if (t == 0) pivslot[c] = ps;
-      if (idx >= PR || pv == 0.0) {  // LINPACK skips a zero pivot column (BandSolver.hpp:76-78)
+      if (idx >= PR || zero_piv) {  // LINPACK skips a zero pivot column (BandSolver.hpp:76-78)
         singular = true;
         continue;
       }
-      const double tinv = -1.0 / pv;
+      double* buf = bufs + (c & 1) * (2 * N + 2);  // alternate buffers: no barrier after the update
       if (t == ps) {
+        const double tinv = -1.0 / cur[c];
+        rdiag = -tinv;
 #pragma unroll
         for (int j = c + 1; j < N; ++j) buf[j] = cur[j];
         if (!last)
 #pragma unroll
           for (int j = 0; j < N; ++j) buf[N + j] = nxt[j];
         buf[2 * N] = rhs;
+        buf[2 * N + 1] = tinv;
       }
       __syncwarp(msk);
       if ((cand >> t) & 1u) {
-        const double m = cur[c] * tinv;
+        const double m = cur[c] * buf[2 * N + 1];
 #pragma unroll
         for (int j = c + 1; j < N; ++j) cur[j] += m * buf[j];
         if (!last)
@@ -292,7 +341,6 @@ __global__ void __launch_bounds__(RCfg<N>::CTA) flux_bvp_reg_kernel(FluxParams p
           for (int j = 0; j < N; ++j) nxt[j] += m * buf[N + j];
         rhs += m * buf[2 * N];
       }
-      __syncwarp(msk);
     }
     DSP_PHASE(21)
 
@@ -301,7 +349,7 @@ __global__ void __launch_bounds__(RCfg<N>::CTA) flux_bvp_reg_kernel(FluxParams p
 #pragma unroll
       for (int c = N - 1; c >= 0; --c) {
         if (myc == c) {
-          const double rinv = 1.0 / cur[c];
+          const double rinv = rdiag;
 #pragma unroll
           for (int j = 0; j < N; ++j) {
             const double x = nxt[j] * rinv;
@@ -354,13 +402,15 @@ __global__ void __launch_bounds__(RCfg<N>::CTA) flux_bvp_reg_kernel(FluxParams p
     DSP_PHASE(22)
   }
   if (singular && t == 0) set_status(p.status, i, DSP_ERR_SINGULAR);
+  cp_async_wait<0>();
+  __syncwarp(msk);
 
   // ----------------------------------------------------------------- backward
   bool nonfinite = false;
   // fluxes at output level lu of layer l (computeFluxes, FluxSolver.cpp:1138-1287;
   // DisortSolver.cpp:1980-2124): utaupr scaled depth, utau unscaled depth
   auto eval_level = [&](int l, const double* x, int lu, double utaupr, double utau) {
-    const double* lr = LR(l);
+    const double* lr = RB(l);
     const double* eig = lr + lrec_eig(N);
     const double* Gl = lr + lrec_G(N);
     if (t < N) {
@@ -372,9 +422,9 @@ __global__ void __launch_bounds__(RCfg<N>::CTA) flux_bvp_reg_kernel(FluxParams p
     if (t < N) {
       double s = 0.0;
 #pragma unroll
-      for (int j = 0; j < N; ++j) s += __ldg(Gl + t * N + j) * ec[j];
-      if (beam) s += __ldg(lr + lrec_zb(N) + t) * fact;
-      if (thermal) s += __ldg(lr + lrec_z0(N) + t) + __ldg(lr + lrec_z1(N) + t) * utaupr;
+      for (int j = 0; j < N; ++j) s += ld_rec(Gl + t * N + j) * ec[j];
+      if (beam) s += ld_rec(lr + lrec_zb(N) + t) * fact;
+      if (thermal) s += ld_rec(lr + lrec_z0(N) + t) + ld_rec(lr + lrec_z1(N) + t) * utaupr;
       Iv[t] = s;
     }
     __syncwarp(msk);
@@ -437,11 +487,21 @@ __global__ void __launch_bounds__(RCfg<N>::CTA) flux_bvp_reg_kernel(FluxParams p
         if ((int)lyr_l[lu] > ncut - 1)
           for (int f = 0; f < 8; ++f) outp[f][oidx(lu)] = 0.0;
   }
+  team_copy_async<TEAM>(RB(ncut - 1), LR(ncut - 1), RS, t);
+  cp_async_commit();
   for (int l = ncut - 1; l >= 0; --l) {
+    // layer l-1's records start loading into the slot of layer l+1
+    if (l > 0) {
+      team_copy_async<TEAM>(RB(l - 1), LR(l - 1), RS, t);
+      team_copy_async<TEAM>(RB(l - 1) + RS, brec0 + (long long)(l - 1) * BS, BS, t);
+    }
+    cp_async_commit();
+    cp_async_wait<1>();
+    __syncwarp(msk);
     double* x = XV + (l & 1) * N;
     if (l < ncut - 1) {
       const double* xn = XV + ((l & 1) ^ 1) * N;
-      const double* br = brec0 + (long long)l * brec_stride(N);
+      const double* br = RB(l) + RS;
       if (t < N) {
         double s = br[N * N + t];
 #pragma unroll

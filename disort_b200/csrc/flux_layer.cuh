@@ -39,7 +39,7 @@ struct LCfg {
   static constexpr int O_CC = 0;                     // cc_top[NN][N]
   static constexpr int O_GL = O_CC + NN * N;         // gl[N]
   static constexpr int O_W = O_GL + N;               // work area
-  static constexpr int W_SIZE = 7 * MAT;
+  static constexpr int W_SIZE = 6 * MAT;
   static constexpr int O_LAM = O_W + W_SIZE;         // NN: k = sqrt|lambda|
   static constexpr int O_LAMR = O_LAM + NN;          // NN: lambda
   static constexpr int O_ROT = O_LAMR + NN;          // c, s, t per pair
@@ -137,18 +137,28 @@ __device__ __forceinline__ bool team_chol(const double* M, double* Lc, double* f
 
 // Jacobi rotation (Golub & Van Loan, Alg. 8.4.1) annihilating S[p][q]; tt = 0
 // when |apq| is negligible.  Small angles skip the square roots.
+// Whether the rotation of pair (p, q) is applied: the off-diagonal element is
+// not negligible against the diagonal ones.
+__device__ __forceinline__ bool jacobi_needed(double apq, double app, double aqq) {
+  return fabs(apq) > 1e-300 && apq * apq > 1.0e-34 * fabs(app * aqq);
+}
+
+// Rotation zeroing apq: t = tan(theta) is the smaller root of t^2 + 2 th t - 1
+// with th = d / e, d = aqq - app, e = 2 apq, written as
+// t = sgn(th) |e| / (|d| + sqrt(d^2 + e^2)) (one square root, one division).
 __device__ __forceinline__ void jacobi_rot(double apq, double app, double aqq, double& c, double& s,
                                            double& tt) {
   c = 1.0;
   s = 0.0;
   tt = 0.0;
-  if (fabs(apq) > 1e-300 && apq * apq > 1.0e-34 * fabs(app * aqq)) {
-    const double th = (aqq - app) / (2.0 * apq);
-    if (fabs(th) > 1e8) {
-      tt = 0.5 / th;
+  if (jacobi_needed(apq, app, aqq)) {
+    const double d = aqq - app, e = 2.0 * apq;
+    if (fabs(d) > 1e8 * fabs(e)) {
+      tt = e / (2.0 * d);
       c = 1.0 - 0.5 * tt * tt;
     } else {
-      tt = (th >= 0.0 ? 1.0 : -1.0) / (fabs(th) + sqrt(th * th + 1.0));
+      const double num = d > 0.0 ? e : (d < 0.0 ? -e : fabs(e));  // sgn(th) |e|, sgn(0) = +1
+      tt = num / (fabs(d) + sqrt(d * d + e * e));
       c = rsqrt(tt * tt + 1.0);
     }
     s = tt * c;
@@ -378,7 +388,7 @@ __global__ void __launch_bounds__(LCfg<N, GEN>::CTA) flux_layer_kernel(FluxParam
   double* S1 = W + 3 * C::MAT;
   double* V = W + 4 * C::MAT;
   double* LC = W + 5 * C::MAT;
-  double* EV = W + 6 * C::MAT;
+  double* EV = S0;  // eigenvectors of (a+b)(a-b); S0 is dead by then
   double* lam = sm + C::O_LAM;
   double* lamraw = sm + C::O_LAMR;
   double* rot = sm + C::O_ROT;
@@ -464,7 +474,7 @@ __global__ void __launch_bounds__(LCfg<N, GEN>::CTA) flux_layer_kernel(FluxParam
     }
   }
   DSP_PHASE(2)
-  // S = L^T M L with M = -A_s (primary) or -B_s (fallback); EV used as scratch
+  // S = L^T M L with M = -A_s (primary) or -B_s (fallback); V used as scratch
   for (int it = t; it < NN * NN; it += TEAM) {
     const int r = it / NN, c = it % NN;
     double s = 0.0;
@@ -472,29 +482,30 @@ __global__ void __launch_bounds__(LCfg<N, GEN>::CTA) flux_layer_kernel(FluxParam
       for (int k = 0; k < NN; ++k) s += -S0[r * NS + k] * LC[k * NS + c];
     else
       for (int k = 0; k < NN; ++k) s += S1[r * NS + k] * LC[k * NS + c];
-    EV[r * NS + c] = s;
+    V[r * NS + c] = s;
   }
   team_sync<TEAM>();
   for (int it = t; it < NN * NN; it += TEAM) {
     const int r = it / NN, c = it % NN;
     double s = 0.0;
-    for (int k = 0; k < NN; ++k) s += LC[k * NS + r] * EV[k * NS + c];
+    for (int k = 0; k < NN; ++k) s += LC[k * NS + r] * V[k * NS + c];
     S0[r * NS + c] = s;
-    V[r * NS + c] = (r == c) ? 1.0 : 0.0;
   }
   team_sync<TEAM>();
   // ---- cyclic Jacobi on S (symmetrised from its lower triangle) -----------
   for (int it = t; it < NN * NN; it += TEAM) {
     const int r = it / NN, c = it % NN;
     S1[r * NS + c] = (c > r) ? S0[c * NS + r] : S0[r * NS + c];
+    V[r * NS + c] = (r == c) ? 1.0 : 0.0;
   }
   team_sync<TEAM>();
   DSP_PHASE(3)
-  double* Sc = S1;
-  double* Sn = S0;
+  // In place: in a round every 2x2 block of S is read and written by its owner
+  // only, and the diagonal blocks a rotation is computed from are written by
+  // their owner after it has received that rotation.
+  double* const Sc = S1;
+  double* const Sn = S1;
   for (int sweep = 0; sweep < 20; ++sweep) {
-    if (t == 0) misc[1] = 0.0;
-    team_sync<TEAM>();
     for (int r = 0; r < NNP - 1; ++r) {
       // rotation of pair a is computed by thread a; each thread then needs the
       // rotations of its block's two pairs only (blocks are assigned statically)
@@ -503,7 +514,6 @@ __global__ void __launch_bounds__(LCfg<N, GEN>::CTA) flux_layer_kernel(FluxParam
         const int pp = rr_player<NNP>(r, t), qq = rr_player<NNP>(r, NNP - 1 - t);
         if (pp < NN && qq < NN) {
           jacobi_rot(Sc[pp * NS + qq], Sc[pp * NS + pp], Sc[qq * NS + qq], c, sn, tt);
-          if (tt != 0.0) misc[1] = 1.0;
         }
       }
       if constexpr (TEAM > 32) {
@@ -602,13 +612,19 @@ __global__ void __launch_bounds__(LCfg<N, GEN>::CTA) flux_layer_kernel(FluxParam
         }
       }
       team_sync<TEAM>();
-      double* tmp = Sc;
-      Sc = Sn;
-      Sn = tmp;
     }
-    const bool rotated = misc[1] != 0.0;
+    // stop when a further sweep would rotate no pair (the sweep that finds
+    // nothing to do is not run)
+    if (t == 0) misc[1] = 0.0;
     team_sync<TEAM>();
-    if (!rotated) break;
+    for (int it = t; it < NN * NN; it += TEAM) {
+      const int r = it / NN, c = it % NN;
+      if (c > r && jacobi_needed(Sc[r * NS + c], Sc[r * NS + r], Sc[c * NS + c])) misc[1] = 1.0;
+    }
+    team_sync<TEAM>();
+    const bool more = misc[1] != 0.0;
+    team_sync<TEAM>();
+    if (!more) break;
   }
   DSP_PHASE(4)
   // ---- sort ascending; eigenvectors of (a+b)(a-b) ------------------------
@@ -620,14 +636,20 @@ __global__ void __launch_bounds__(LCfg<N, GEN>::CTA) flux_layer_kernel(FluxParam
       if (lj < lk || (lj == lk && j < k)) ++rank;
     }
     lam[rank] = lk;
-    for (int row = 0; row < NN; ++row) Sn[row * NS + rank] = V[row * NS + k];
+    piv[rank] = k;
+  }
+  team_sync<TEAM>();
+  double* Wm = S1;  // sorted eigenvectors of S (columns), over the diagonalised S
+  for (int it = t; it < NN * NN; it += TEAM) {
+    const int row = it / NN, rank = it % NN;
+    Wm[row * NS + rank] = V[row * NS + piv[rank]];
   }
   team_sync<TEAM>();
   // primary: evec = D^{-1} L^{-T} w ; fallback: evec = D^{-1} L' w
   for (int c = t; c < NN; c += TEAM) {
     if (primary) {
       for (int r = NN - 1; r >= 0; --r) {
-        double s = Sn[r * NS + c];
+        double s = Wm[r * NS + c];
         for (int k = r + 1; k < NN; ++k) s -= LC[k * NS + r] * EV[k * NS + c];
         EV[r * NS + c] = s / LC[r * NS + r];
       }
@@ -635,7 +657,7 @@ __global__ void __launch_bounds__(LCfg<N, GEN>::CTA) flux_layer_kernel(FluxParam
     } else {
       for (int r = NN - 1; r >= 0; --r) {
         double s = 0.0;
-        for (int k = 0; k <= r; ++k) s += LC[r * NS + k] * Sn[k * NS + c];
+        for (int k = 0; k <= r; ++k) s += LC[r * NS + k] * Wm[k * NS + c];
         EV[r * NS + c] = dinv[r] * s;
       }
     }
@@ -682,7 +704,6 @@ __global__ void __launch_bounds__(LCfg<N, GEN>::CTA) flux_layer_kernel(FluxParam
   // diagonal in the same basis: B_s A_s = L W Lam W^T L^{-1} (primary) or
   // L^{-T} W Lam W^T L^T (fallback); its singular points are the reference's
   // dithering condition |1 - mu0^2 k^2| ~ 0 (FluxSolver.cpp:610-618).
-  double* Wm = Sn;  // sorted eigenvectors of S (columns)
   double* scratch = zv;
   const double dt_ = (t < NN) ? dsim[t] : 1.0;
   const double di_ = (t < NN) ? dinv[t] : 1.0;
