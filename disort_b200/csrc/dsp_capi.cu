@@ -16,7 +16,7 @@
 #include "../../include/dsp.h"
 #include "dsp_device.cuh"
 #include "dsp_host.hpp"
-#include "flux_bvp.cuh"
+#include "flux_bvp_tile.cuh"
 #include "flux_bvp_reg.cuh"
 #include "flux_layer.cuh"
 #include "flux_setup.cuh"
@@ -53,16 +53,16 @@ dsp_status launch_flux_chunk(dsp_context ctx, const FluxParams& p) {
     KernelTimer kt(ctx, "flux_bvp_kernel");
     flux_bvp_reg_kernel<N><<<grid, C::CTA, sm, s>>>(p);
   } else {
-    using C = BCfg<N>;
+    using C = TCfg<N>;
     const size_t sm = C::smem_bytes();
     static bool attr = false;
     if (!attr) {
-      cudaFuncSetAttribute(flux_bvp_kernel<N>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+      cudaFuncSetAttribute(flux_bvp_tile_kernel<N>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
       attr = true;
     }
     const int grid = (p.n + C::TPC - 1) / C::TPC;
     KernelTimer kt(ctx, "flux_bvp_kernel");
-    flux_bvp_kernel<N><<<grid, C::CTA, sm, s>>>(p);
+    flux_bvp_tile_kernel<N><<<grid, C::CTA, sm, s>>>(p);
   }
   cudaError_t e = cudaGetLastError();
   if (e != cudaSuccess) return cuda_fail(ctx, e, "flux kernel launch");

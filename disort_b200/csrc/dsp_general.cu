@@ -10,7 +10,7 @@
 // Instances whose series has ended (last mode, or converged) skip the later
 // mode launches on the device.
 #include "dsp_host.hpp"
-#include "flux_bvp.cuh"
+#include "flux_bvp_tile.cuh"
 #include "flux_bvp_reg.cuh"
 #include "flux_layer.cuh"
 #include "gen_kernels.cuh"
@@ -83,8 +83,8 @@ dsp_status launch_general_chunk(dsp_context ctx, FluxParams p, long long layers,
     cudaFuncSetAttribute(flux_layer_kernel<N, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                          (int)LC::smem_bytes());
     if constexpr (N > 16)
-      cudaFuncSetAttribute(flux_bvp_kernel<N, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                           (int)BCfg<N>::smem_bytes());
+      cudaFuncSetAttribute(flux_bvp_tile_kernel<N, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                           (int)TCfg<N>::smem_bytes());
     attr = true;
   }
   p.tables = tabs;
@@ -105,9 +105,9 @@ dsp_status launch_general_chunk(dsp_context ctx, FluxParams p, long long layers,
       KernelTimer kt(ctx, "gen_bvp_kernel");
       flux_bvp_reg_kernel<N, true><<<(p.n + C::TPC - 1) / C::TPC, C::CTA, C::smem_bytes(), s>>>(p);
     } else {
-      using C = BCfg<N>;
+      using C = TCfg<N>;
       KernelTimer kt(ctx, "gen_bvp_kernel");
-      flux_bvp_kernel<N, true><<<(p.n + C::TPC - 1) / C::TPC, C::CTA, C::smem_bytes(), s>>>(p);
+      flux_bvp_tile_kernel<N, true><<<(p.n + C::TPC - 1) / C::TPC, C::CTA, C::smem_bytes(), s>>>(p);
     }
     if (p.g.numu > 0) {
       KernelTimer kt(ctx, "gen_intensity_kernel");

@@ -34,7 +34,7 @@
 
 #include "../../include/dsp.h"
 #include "dsp_device.cuh"
-#include "flux_bvp.cuh"
+#include "flux_bvp_tile.cuh"
 #include "flux_bvp_reg.cuh"
 #include "flux_layer.cuh"
 #include "flux_setup.cuh"
@@ -104,8 +104,8 @@ void set_attrs() {
   cudaFuncSetAttribute(flux_layer_kernel<N>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                        (int)LCfg<N>::smem_bytes());
   if constexpr (N > 16)
-    cudaFuncSetAttribute(flux_bvp_kernel<N>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                         (int)BCfg<N>::smem_bytes());
+    cudaFuncSetAttribute(flux_bvp_tile_kernel<N>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                         (int)TCfg<N>::smem_bytes());
 }
 
 template <int N>
@@ -120,8 +120,8 @@ void launch(const FluxParams& p, cudaStream_t s) {
     using C = RCfg<N>;
     flux_bvp_reg_kernel<N><<<(p.n + C::TPC - 1) / C::TPC, C::CTA, C::smem_bytes(), s>>>(p);
   } else {
-    using C = BCfg<N>;
-    flux_bvp_kernel<N><<<(p.n + C::TPC - 1) / C::TPC, C::CTA, C::smem_bytes(), s>>>(p);
+    using C = TCfg<N>;
+    flux_bvp_tile_kernel<N><<<(p.n + C::TPC - 1) / C::TPC, C::CTA, C::smem_bytes(), s>>>(p);
   }
 }
 

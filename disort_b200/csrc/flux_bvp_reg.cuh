@@ -1,7 +1,7 @@
 // flux_bvp_reg.cuh — boundary-value problem and fluxes for N <= 16 with the
 // elimination panel held in registers (one panel row per thread).
 //
-// Same algorithm as flux_bvp.cuh (the staircase form of the LINPACK band LU,
+// Same algorithm as flux_bvp_tile.cuh (the staircase form of the LINPACK band LU,
 // setMatrix/solve0/computeFluxes of FluxSolver.cpp:838-1287), mapped so that
 // the sgbfa row operations are register FMAs:
 //  - slot thread s holds its row as cur[N] (columns of x_l), nxt[N] (columns of

@@ -135,15 +135,14 @@ __device__ __forceinline__ bool team_chol(const double* M, double* Lc, double* f
   else return team_cholesky<NN, NS, TEAM>(M, Lc, flag, t);
 }
 
-// Jacobi rotation (Golub & Van Loan, Alg. 8.4.1) annihilating S[p][q]; tt = 0
-// when |apq| is negligible.  Small angles skip the square roots.
-// Whether the rotation of pair (p, q) is applied: the off-diagonal element is
-// not negligible against the diagonal ones.
+// Whether the Jacobi rotation of pair (p, q) is applied: the off-diagonal
+// element is not negligible against the diagonal ones.
 __device__ __forceinline__ bool jacobi_needed(double apq, double app, double aqq) {
   return fabs(apq) > 1e-300 && apq * apq > 1.0e-34 * fabs(app * aqq);
 }
 
-// Rotation zeroing apq: t = tan(theta) is the smaller root of t^2 + 2 th t - 1
+// Jacobi rotation (Golub & Van Loan, Alg. 8.4.1) zeroing apq; tt = 0 when apq
+// is negligible.  t = tan(theta) is the smaller root of t^2 + 2 th t - 1
 // with th = d / e, d = aqq - app, e = 2 apq, written as
 // t = sgn(th) |e| / (|d| + sqrt(d^2 + e^2)) (one square root, one division).
 __device__ __forceinline__ void jacobi_rot(double apq, double app, double aqq, double& c, double& s,
@@ -624,6 +623,7 @@ __global__ void __launch_bounds__(LCfg<N, GEN>::CTA) flux_layer_kernel(FluxParam
     team_sync<TEAM>();
     const bool more = misc[1] != 0.0;
     team_sync<TEAM>();
+    DSP_PHASE(6)
     if (!more) break;
   }
   DSP_PHASE(4)
