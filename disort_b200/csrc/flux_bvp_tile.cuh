@@ -47,12 +47,12 @@ struct TCfg {
   static constexpr int MINB = 65536 / (CTA * 128);
   static constexpr int NW = (PR + 31) / 32;  // words of a slot mask
   static constexpr int LDU = 2 * N + 2;   // staged pivot row: both blocks, rhs, pad
-  static constexpr int LDX = N + 1;       // back-substitution solution, column-major [N + 1][LDX]
+  static constexpr int RL = 2 * N + 1;    // row of the layer's elimination record: [U | V | rhs]
   // shared memory (doubles)
   static constexpr int O_TAB = 0;              // mu[N], wt[N]
   static constexpr int O_U = 2 * N;            // U rows in pivot order [N][LDU]
-  static constexpr int O_XS = O_U + N * LDU;   // back substitution [N + 1][LDX]
-  static constexpr int O_M = O_XS + (N + 1) * LDX;  // multipliers, two buffers [2][PR]
+  static constexpr int O_R = O_U + N * LDU;    // right-hand side of the upward solve [N]
+  static constexpr int O_M = O_R + N;          // multipliers, two buffers [2][PR]
   static constexpr int O_X = O_M + 2 * PR;     // x ping-pong [2][N]
   static constexpr int O_EC = O_X + 2 * N;     // [N]
   static constexpr int O_I = O_EC + N;         // intensities [N]
@@ -88,7 +88,7 @@ template <int N, bool GEN = false>
 __global__ void __launch_bounds__(TCfg<N>::CTA, TCfg<N>::MINB) flux_bvp_tile_kernel(FluxParams p) {
   using C = TCfg<N>;
   constexpr int NN = C::NN, PR = C::PR, RG = C::RG, RPT = C::RPT, CPT = C::CPT, NW = C::NW;
-  constexpr int LDU = C::LDU, LDX = C::LDX;
+  constexpr int LDU = C::LDU, RL = C::RL;
   constexpr double PI = 3.14159265358979323846;
   constexpr int TEAM = C::CTA;
   extern __shared__ double smem[];
@@ -99,7 +99,7 @@ __global__ void __launch_bounds__(TCfg<N>::CTA, TCfg<N>::MINB) flux_bvp_tile_ker
   const double* mu = smem + C::O_TAB;
   const double* wt = smem + C::O_TAB + N;
   double* U = smem + C::O_U;
-  double* XS = smem + C::O_XS;
+  double* Rv = smem + C::O_R;
   double* mltb = smem + C::O_M;
   double* X = smem + C::O_X;
   double* ec = smem + C::O_EC;
@@ -436,36 +436,19 @@ __global__ void __launch_bounds__(TCfg<N>::CTA, TCfg<N>::MINB) flux_bvp_tile_ker
     __syncthreads();
     DSP_PHASE(11)
 
-    // ---- back substitution over the staged U rows --------------------------
-    // U[c][cbk*N + c'] (c' >= c) is the triangle, U[c][(cbk^1)*N + n] and
-    // U[c][2N] the right-hand sides; one column per thread, x kept in XS.
-    const int cb = cbk * N, nb = (cbk ^ 1) * N;
-    const int ncol = last ? 1 : N + 1;
-    if (t < ncol) {
-      const int jc = last ? 2 * N : (t < N ? nb + t : 2 * N);
-      double* xs = XS + t * LDX;
-#pragma unroll 1
-      for (int c = N - 1; c >= 0; --c) {
-        const double* uc = U + c * LDU + cb;
-        double s0 = U[c * LDU + jc], s1 = 0.0, s2 = 0.0, s3 = 0.0;
-        int k = c + 1;
-        for (; k + 3 < N; k += 4) {
-          s0 -= uc[k] * xs[k];
-          s1 -= uc[k + 1] * xs[k + 1];
-          s2 -= uc[k + 2] * xs[k + 2];
-          s3 -= uc[k + 3] * xs[k + 3];
-        }
-        for (; k < N; ++k) s0 -= uc[k] * xs[k];
-        xs[c] = ((s0 + s1) + (s2 + s3)) * rdg[c];
+    // ---- the layer's elimination record ------------------------------------
+    // Row c of U (the pivot row of column c): [x_l block | x_{l+1} block | rhs],
+    // blocks in x order, then 1 / pivot; the upward sweep solves
+    // U_l x_l = rhs_l - V_l x_{l+1} with it.
+    {
+      const int cb = cbk * N, nb = (cbk ^ 1) * N;
+      double* br = brec0 + (long long)l * brec_stride(N);
+      for (int idx = t; idx < N * RL; idx += TEAM) {
+        const int c = idx / RL, col = idx % RL;
+        const int src = col < N ? cb + col : (col < 2 * N ? nb + (col - N) : 2 * N);
+        br[idx] = U[c * LDU + src];
       }
-      if (!last) {
-        // W_l transposed (Wt[n][c]) and d_l
-        double* br = brec0 + (long long)l * brec_stride(N) + (t < N ? t * N : N * N);
-        for (int c = 0; c < N; ++c) br[c] = xs[c];
-      } else {
-        double* x = X + (l & 1) * N;
-        for (int c = 0; c < N; ++c) x[c] = xs[c];
-      }
+      for (int c = t; c < N; c += TEAM) br[N * RL + c] = rdg[c];
     }
     // the pivot rows are done; the others are carried into the next layer
     carried = cand;
@@ -549,18 +532,44 @@ __global__ void __launch_bounds__(TCfg<N>::CTA, TCfg<N>::MINB) flux_bvp_tile_ker
         if ((int)lyr_l[lu] > ncut - 1)
           for (int f = 0; f < 8; ++f) outp[f][oidx(lu)] = 0.0;
   }
+  constexpr int TPR = TEAM / N;  // threads per row of the matrix-vector product
+  static_assert(TPR >= 1 && (TPR & (TPR - 1)) == 0 && TPR <= 32, "row groups within a warp");
   for (int l = ncut - 1; l >= 0; --l) {
     double* x = X + (l & 1) * N;
-    if (l < ncut - 1) {
-      const double* xn = X + ((l & 1) ^ 1) * N;
+    // stage the layer's record (U rows in RL-strided rows, then 1 / pivot)
+    {
       const double* br = brec0 + (long long)l * brec_stride(N);
-      for (int c = t; c < N; c += TEAM) {
-        double s = br[N * N + c];
-        for (int n = 0; n < N; ++n) s -= br[n * N + c] * xn[n];
-        x[c] = s;
-      }
-      __syncthreads();
+      for (int idx = t; idx < N * RL + N; idx += TEAM) U[idx] = br[idx];
     }
+    __syncthreads();
+    // rhs - V x_{l+1} (x_{l+1} = 0 below the last layer)
+    {
+      const int c = t / TPR, r = t % TPR;
+      const double* xn = X + ((l & 1) ^ 1) * N;
+      double s = 0.0;
+      if (l < ncut - 1)
+        for (int n = r; n < N; n += TPR) s += U[c * RL + N + n] * xn[n];
+#pragma unroll
+      for (int off = TPR / 2; off > 0; off >>= 1) s += __shfl_xor_sync(0xffffffffu, s, off, TPR);
+      if (r == 0) Rv[c] = U[c * RL + 2 * N] - s;
+    }
+    __syncthreads();
+    // U x_l = r: column-oriented back substitution in one warp, rows t and t + 32
+    if (t < 32) {
+      const double* rdiag = U + N * RL;
+      double r0 = Rv[t], r1 = (N > 32) ? Rv[(t + 32) % N] : 0.0;
+#pragma unroll 4
+      for (int c = N - 1; c >= 0; --c) {
+        const double u0 = U[t * RL + c];
+        const double u1 = (N > 32) ? U[((t + 32) % N) * RL + c] : 0.0;
+        const double mine = (c < 32) ? r0 : r1;
+        const double xc = __shfl_sync(0xffffffffu, mine * rdiag[c], c & 31);
+        if (t == (c & 31)) x[c] = xc;
+        if (t < c) r0 -= u0 * xc;
+        if (N > 32 && t + 32 < c) r1 -= u1 * xc;
+      }
+    }
+    __syncthreads();
     DSP_PHASE(13)
     if constexpr (GEN) {
       for (int c = t; c < N; c += TEAM) cc0[(long long)l * N + c] = x[c];
