@@ -27,7 +27,8 @@ namespace dsp {
 template <int N, bool GEN = false>
 struct LCfg {
   static constexpr int NN = N / 2;
-  static constexpr int TEAM = pow2ceil(N) < 4 ? 4 : pow2ceil(N);
+  // 64 streams: a 128-thread team per layer (two threads per stream)
+  static constexpr int TEAM = N >= 64 ? 2 * N : (pow2ceil(N) < 4 ? 4 : pow2ceil(N));
   static constexpr int CTA = TEAM >= 32 ? TEAM : 128;
   static constexpr int TPC = CTA / TEAM;
   static constexpr int NNP = NN + (NN & 1);
@@ -53,7 +54,10 @@ struct LCfg {
   // user angles whose P_l^m columns fit next to W[N][N] in the work area
   static constexpr int UCH = (W_SIZE - N * N) / N;
   static_assert(!GEN || UCH >= 1, "work area too small for the user-angle tables");
-  static constexpr int TAB = tab_size(N);
+  // the Legendre table stays in global memory (L1) for N >= 32, where it would
+  // take more shared memory than a team
+  static constexpr bool Y_GLOBAL = N >= 32;
+  static constexpr int TAB = Y_GLOBAL ? tab_ylm(N) : tab_size(N);
   static constexpr size_t smem_bytes() { return sizeof(double) * (size_t)(TAB + TPC * TEAM_SMEM); }
 };
 
@@ -339,7 +343,7 @@ __global__ void __launch_bounds__(LCfg<N, GEN>::CTA) flux_layer_kernel(FluxParam
   const double* wt = smem + tab_wt(N);
   const double* dsim = smem + tab_dsim(N);
   const double* dinv = smem + tab_dinv(N);
-  const double* Y = smem + tab_ylm(N);
+  const double* Y = C::Y_GLOBAL ? p.tables + tab_ylm(N) : smem + tab_ylm(N);
 
   const int team = threadIdx.x / TEAM, t = threadIdx.x % TEAM;
   const long long task = (long long)blockIdx.x * C::TPC + team;
