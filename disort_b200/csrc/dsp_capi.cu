@@ -3,6 +3,7 @@
 // general solve lives in dsp_general.cu; shared host internals in dsp_host.hpp.
 #include <cuda_runtime.h>
 
+#include <algorithm>
 #include <cfloat>
 #include <cmath>
 #include <cstdio>
@@ -141,6 +142,11 @@ dsp_status dsp_context_destroy(dsp_context ctx) {
   cudaStreamSynchronize(ctx->stream);
   drain_timing(ctx);
   for (cudaEvent_t e : ctx->free_events) cudaEventDestroy(e);
+  if (ctx->s_in) cudaStreamSynchronize(ctx->s_in);
+  if (ctx->s_out) cudaStreamSynchronize(ctx->s_out);
+  for (cudaEvent_t e : ctx->pipe_ev) cudaEventDestroy(e);
+  if (ctx->s_in) cudaStreamDestroy(ctx->s_in);
+  if (ctx->s_out) cudaStreamDestroy(ctx->s_out);
   if (ctx->ws) cudaFree(ctx->ws);
   if (ctx->stage_in) cudaFree(ctx->stage_in);
   if (ctx->stage_out) cudaFree(ctx->stage_out);
@@ -233,6 +239,7 @@ dsp_status dsp_flux_bands_solve(dsp_context ctx, const dsp_flux_batch* batch_in,
 
   // ---- stage host inputs (and defaults) into device memory ---------------
   dsp_darray* arr = batch_arrays(&b);
+  const double* host_in[14] = {};  // per-instance host arrays still to be copied
   {
     size_t need = 0;
     for (int k = 0; k < 14; ++k) {
@@ -257,8 +264,12 @@ dsp_status dsp_flux_bands_solve(dsp_context ctx, const dsp_flux_batch* batch_in,
       }
       if (dev) continue;
       const size_t elems = arr[k].stride == 0 ? (size_t)cnt[k] : (size_t)((n - 1) * arr[k].stride + cnt[k]);
-      e = cudaMemcpyAsync(cur, arr[k].ptr, elems * sizeof(double), cudaMemcpyHostToDevice, s);
-      if (e != cudaSuccess) return cuda_fail(ctx, e, "cudaMemcpyAsync(input)");
+      if (arr[k].stride == 0) {  // shared by every instance: copied now
+        e = cudaMemcpyAsync(cur, arr[k].ptr, elems * sizeof(double), cudaMemcpyHostToDevice, s);
+        if (e != cudaSuccess) return cuda_fail(ctx, e, "cudaMemcpyAsync(input)");
+      } else {  // per instance: copied piece by piece below
+        host_in[k] = arr[k].ptr;
+      }
       arr[k].ptr = reinterpret_cast<const double*>(cur);
       cur += ((elems * sizeof(double) + 255) / 256) * 256;
     }
@@ -316,40 +327,91 @@ dsp_status dsp_flux_bands_solve(dsp_context ctx, const dsp_flux_batch* batch_in,
   p.il = InstLayout::make(L, N);
   DArr* pa[14] = {&p.wlo, &p.whi, &p.dtau, &p.ssa, &p.pmom, &p.temp, &p.alb,
                   &p.emis, &p.fbeam, &p.umu0, &p.fisot, &p.fisob, &p.ttop, &p.tbot};
-  for (int64_t off = 0; off < n; off += chunk) {
-    const int64_t m = (n - off < chunk) ? (n - off) : chunk;
-    p.n = (int)m;
-    for (int k = 0; k < 14; ++k) {
-      pa[k]->p = arr[k].ptr ? arr[k].ptr + arr[k].stride * off : nullptr;
-      pa[k]->s = arr[k].stride;
+  auto run_range = [&](int64_t r0, int64_t r1) -> dsp_status {
+    for (int64_t off = r0; off < r1; off += chunk) {
+      const int64_t m = (r1 - off < chunk) ? (r1 - off) : chunk;
+      p.n = (int)m;
+      for (int k = 0; k < 14; ++k) {
+        pa[k]->p = arr[k].ptr ? arr[k].ptr + arr[k].stride * off : nullptr;
+        pa[k]->s = arr[k].stride;
+      }
+      double* w = static_cast<double*>(ctx->ws);
+      p.inst_rec = w;
+      p.layer_rec = w + (size_t)m * sz.inst;
+      p.bvp_rec = p.layer_rec + (size_t)m * sz.layer;
+      for (int f = 0; f < 8; ++f) p.out[f] = dout[f] + off * nlev;
+      p.status = dstatus + off;
+      dsp_status rs = launch_flux(ctx, N, p);
+      if (rs != DSP_OK) return rs;
     }
-    double* w = static_cast<double*>(ctx->ws);
-    p.inst_rec = w;
-    p.layer_rec = w + (size_t)m * sz.inst;
-    p.bvp_rec = p.layer_rec + (size_t)m * sz.layer;
-    for (int f = 0; f < 8; ++f) p.out[f] = dout[f] + off * nlev;
-    p.status = dstatus + off;
-    if ((st = launch_flux(ctx, N, p)) != DSP_OK) return st;
-  }
+    return DSP_OK;
+  };
+  if (dev) return run_range(0, n);
 
-  if (dev) return DSP_OK;
-  // ---- copy back ---------------------------------------------------------
+  // ---- host buffers: copies overlapped with the solves ----------------------
+  // The batch is cut into pieces; piece k's inputs go up on a copy stream while
+  // piece k-1 is solved on the context's stream and the outputs of piece k-2 come
+  // back on a second copy stream.  (With pageable host memory the copies do not
+  // overlap, but the results are the same.)
   double* host_out[8] = {out->flux_direct_beam, out->flux_down, out->flux_up, out->flux_tau_divergence,
                          out->mean_intensity, out->mean_intensity_down, out->mean_intensity_up,
                          out->mean_intensity_direct_beam};
-  for (int f = 0; f < 8; ++f) {
-    e = cudaMemcpyAsync(host_out[f], dout[f], (size_t)n * nlev * sizeof(double), cudaMemcpyDeviceToHost, s);
-    if (e != cudaSuccess) return cuda_fail(ctx, e, "cudaMemcpyAsync(output)");
-  }
   std::vector<int32_t> hst;
   int32_t* hs = out->status;
   if (!hs) {
     hst.resize(n);
     hs = hst.data();
   }
-  e = cudaMemcpyAsync(hs, dstatus, (size_t)n * sizeof(int32_t), cudaMemcpyDeviceToHost, s);
-  if (e != cudaSuccess) return cuda_fail(ctx, e, "cudaMemcpyAsync(status)");
-  e = cudaStreamSynchronize(s);
+  constexpr int kMaxPieces = 8;
+  // pieces of at least two waves of the one-warp-per-instance boundary-value
+  // kernel (16 resident per SM), so that launch tails stay small
+  const int64_t min_piece = 32 * (int64_t)ctx->sm_count;
+  const int pieces = (int)std::max<int64_t>(1, std::min<int64_t>(kMaxPieces, n / min_piece));
+  if (!ctx->s_in) {
+    e = cudaStreamCreateWithFlags(&ctx->s_in, cudaStreamNonBlocking);
+    if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&ctx->s_out, cudaStreamNonBlocking);
+    if (e != cudaSuccess) return cuda_fail(ctx, e, "copy streams");
+  }
+  while ((int)ctx->pipe_ev.size() < 2 * kMaxPieces + 1) {
+    cudaEvent_t ev;
+    e = cudaEventCreateWithFlags(&ev, cudaEventDisableTiming);
+    if (e != cudaSuccess) return cuda_fail(ctx, e, "pipeline events");
+    ctx->pipe_ev.push_back(ev);
+  }
+  cudaEvent_t* ev_in = ctx->pipe_ev.data();
+  cudaEvent_t* ev_done = ev_in + kMaxPieces;
+  cudaEvent_t ev_start = ctx->pipe_ev[2 * kMaxPieces];
+  // the staging areas may still be read by earlier work on the context's stream
+  e = cudaEventRecord(ev_start, s);
+  if (e == cudaSuccess) e = cudaStreamWaitEvent(ctx->s_in, ev_start, 0);
+  if (e != cudaSuccess) return cuda_fail(ctx, e, "pipeline start");
+  for (int k = 0; k < pieces; ++k) {
+    const int64_t r0 = n * k / pieces, r1 = n * (k + 1) / pieces;
+    for (int a = 0; a < 14; ++a) {
+      if (!host_in[a]) continue;
+      const int64_t e0 = r0 * arr[a].stride, e1 = (r1 - 1) * arr[a].stride + cnt[a];
+      e = cudaMemcpyAsync(const_cast<double*>(arr[a].ptr) + e0, host_in[a] + e0, (size_t)(e1 - e0) * sizeof(double),
+                          cudaMemcpyHostToDevice, ctx->s_in);
+      if (e != cudaSuccess) return cuda_fail(ctx, e, "cudaMemcpyAsync(input)");
+    }
+    e = cudaEventRecord(ev_in[k], ctx->s_in);
+    if (e == cudaSuccess) e = cudaStreamWaitEvent(s, ev_in[k], 0);
+    if (e != cudaSuccess) return cuda_fail(ctx, e, "pipeline input");
+    if ((st = run_range(r0, r1)) != DSP_OK) return st;
+    e = cudaEventRecord(ev_done[k], s);
+    if (e == cudaSuccess) e = cudaStreamWaitEvent(ctx->s_out, ev_done[k], 0);
+    if (e != cudaSuccess) return cuda_fail(ctx, e, "pipeline output");
+    for (int f = 0; f < 8; ++f) {
+      e = cudaMemcpyAsync(host_out[f] + r0 * nlev, dout[f] + r0 * nlev, (size_t)(r1 - r0) * nlev * sizeof(double),
+                          cudaMemcpyDeviceToHost, ctx->s_out);
+      if (e != cudaSuccess) return cuda_fail(ctx, e, "cudaMemcpyAsync(output)");
+    }
+    e = cudaMemcpyAsync(hs + r0, dstatus + r0, (size_t)(r1 - r0) * sizeof(int32_t), cudaMemcpyDeviceToHost,
+                        ctx->s_out);
+    if (e != cudaSuccess) return cuda_fail(ctx, e, "cudaMemcpyAsync(status)");
+  }
+  e = cudaStreamSynchronize(ctx->s_out);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(s);
   if (e != cudaSuccess) return cuda_fail(ctx, e, "flux solve");
   return DSP_OK;
 }

@@ -36,6 +36,9 @@ struct dsp_context_s {
   std::map<int, double*> mode_tables;  // general solver: one table per azimuth mode
   void* meta = nullptr;                // general solver: chunk index arrays
   size_t meta_bytes = 0;
+  // host-buffer solves: copy streams and events of the copy/compute pipeline
+  cudaStream_t s_in = nullptr, s_out = nullptr;
+  std::vector<cudaEvent_t> pipe_ev;
   // optional per-kernel timing
   bool timing = false;
   struct Pending {
