@@ -36,17 +36,21 @@ struct LCfg {
   static constexpr int BPT = (NPAIR * NPAIR + TEAM - 1) / TEAM;  // Jacobi 2x2 blocks per thread
   static constexpr int NS = NN + 1;  // padded row stride of NN x NN matrices
   static constexpr int MAT = NN * NS;
-  // team shared-memory layout (doubles)
+  // team shared-memory layout (doubles).  The phase matrix is dead once
+  // alpha -/+ beta are formed; where it is large enough (N >= 10) the
+  // eigenvector matrix V and the vectors b, z are placed over it.
+  static constexpr bool OVL = MAT + 2 * N <= NN * N;
   static constexpr int O_CC = 0;                     // cc_top[NN][N]
   static constexpr int O_GL = O_CC + NN * N;         // gl[N]
-  static constexpr int O_W = O_GL + N;               // work area
-  static constexpr int W_SIZE = 6 * MAT;
+  static constexpr int O_W = O_GL + N;               // work area: AMB, APB, S0, S1, LC (, V)
+  static constexpr int W_SIZE = (OVL ? 5 : 6) * MAT;
+  static constexpr int O_V = OVL ? O_CC : O_W + 5 * MAT;
   static constexpr int O_LAM = O_W + W_SIZE;         // NN: k = sqrt|lambda|
   static constexpr int O_LAMR = O_LAM + NN;          // NN: lambda
   static constexpr int O_ROT = O_LAMR + NN;          // c, s, t per pair
-  static constexpr int O_B = O_ROT + 3 * NPAIR;      // b[N]
+  static constexpr int O_B = OVL ? O_CC + MAT : O_ROT + 3 * NPAIR;  // b[N]
   static constexpr int O_Z = O_B + N;                // z[N]
-  static constexpr int O_MISC = O_Z + N;             // flags, reduction scratch
+  static constexpr int O_MISC = OVL ? O_ROT + 3 * NPAIR : O_Z + N;  // flags, reduction scratch
   static constexpr int O_PIV = O_MISC + 8;           // N ints
   // general solver: P_l^m(-mu0), then psi0 / p0 / p1 source moments [N] each
   static constexpr int O_GX = O_PIV + N / 2 + 1;
@@ -54,11 +58,16 @@ struct LCfg {
   // user angles whose P_l^m columns fit next to W[N][N] in the work area
   static constexpr int UCH = (W_SIZE - N * N) / N;
   static_assert(!GEN || UCH >= 1, "work area too small for the user-angle tables");
-  // the Legendre table stays in global memory (L1) for N >= 32, where it would
-  // take more shared memory than a team
-  static constexpr bool Y_GLOBAL = N >= 32;
+  // the Legendre table stays in global memory (L1) for N >= 16, where it would
+  // take about as much shared memory as a team
+  static constexpr bool Y_GLOBAL = N >= 16;
   static constexpr int TAB = Y_GLOBAL ? tab_ylm(N) : tab_size(N);
   static constexpr size_t smem_bytes() { return sizeof(double) * (size_t)(TAB + TPC * TEAM_SMEM); }
+  // resident CTAs per SM the register budget is sized for: as many as shared
+  // memory admits (228 KB, 1 KB reserved per CTA), never below 80 registers
+  static constexpr int MINB_SMEM = (int)((228u * 1024u) / (smem_bytes() + 1024u));
+  static constexpr int MINB_REGS = 65536 / (CTA * 80);
+  static constexpr int MINB = MINB_SMEM < 1 ? 1 : (MINB_SMEM < MINB_REGS ? MINB_SMEM : MINB_REGS);
 };
 
 // Round-robin pairing of NNP players in round r: (arr[a], arr[NNP-1-a]),
@@ -331,7 +340,7 @@ __device__ void gen_user_angles(const FluxParams& p, int i, double* sm, const do
 }
 
 template <int N, bool GEN = false>
-__global__ void __launch_bounds__(LCfg<N, GEN>::CTA) flux_layer_kernel(FluxParams p) {
+__global__ void __launch_bounds__(LCfg<N, GEN>::CTA, LCfg<N, GEN>::MINB) flux_layer_kernel(FluxParams p) {
   using C = LCfg<N, GEN>;
   constexpr int NN = C::NN, TEAM = C::TEAM, NNP = C::NNP, NPAIR = C::NPAIR, NS = C::NS, BPT = C::BPT;
   constexpr int BPA = NPAIR;  // blocks (a, b) per column pair b
@@ -389,8 +398,8 @@ __global__ void __launch_bounds__(LCfg<N, GEN>::CTA) flux_layer_kernel(FluxParam
   double* APB = W + 1 * C::MAT;
   double* S0 = W + 2 * C::MAT;
   double* S1 = W + 3 * C::MAT;
-  double* V = W + 4 * C::MAT;
-  double* LC = W + 5 * C::MAT;
+  double* LC = W + 4 * C::MAT;
+  double* V = sm + C::O_V;  // over the phase matrix when C::OVL (first written after alpha -/+ beta)
   double* EV = S0;  // eigenvectors of (a+b)(a-b); S0 is dead by then
   double* lam = sm + C::O_LAM;
   double* lamraw = sm + C::O_LAMR;
@@ -399,12 +408,6 @@ __global__ void __launch_bounds__(LCfg<N, GEN>::CTA) flux_layer_kernel(FluxParam
   double* zv = sm + C::O_Z;
   double* misc = sm + C::O_MISC;
   int* piv = reinterpret_cast<int*>(sm + C::O_PIV);
-  // full phase matrix element C(r, j) from its unique half
-  auto Cfull = [&](int r, int j) -> double {
-    const int rr = r < NN ? r : r - NN;
-    const int jj = (r < NN) ? j : (j < NN ? j + NN : j - NN);
-    return CC[rr * N + jj];
-  };
 
   DSP_PHASE_BEGIN
   const double ws = rec[il.ssa_s + lc];
