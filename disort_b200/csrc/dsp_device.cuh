@@ -97,10 +97,11 @@ __host__ __device__ constexpr int lrec_z0(int N) { return N * N + 2 * N; }
 __host__ __device__ constexpr int lrec_z1(int N) { return N * N + 3 * N; }
 __host__ __device__ constexpr int lrec_xr(int N) { return N * N + 4 * N; }
 __host__ __device__ constexpr int lrec_stride(int N) { return round4(N * N + 4 * N + 2); }
-// Elimination record (doubles) written by the BVP kernels, per layer.
-// N <= 16: Wt[N][N] (W_l = U^{-1} V transposed) | d[N] (U^{-1} rhs).
-// N >= 32: U rows [N][2N+1] ([x_l block | x_{l+1} block | rhs]) | 1 / pivot [N].
-__host__ __device__ constexpr int brec_stride(int N) { return N <= 16 ? round4(N * N + N) : round4(N * (2 * N + 2)); }
+// Elimination record (doubles) written by the BVP kernels, per layer: the N
+// pivot rows [U | V | c] of U x_l + V x_{l+1} = c and the pivot reciprocals.
+// N <= 16: rows of 2N + 2 ([U | V | c | 1/pivot]); N >= 32: rows of 2N + 1
+// ([U | V | c]), then 1 / pivot [N].
+__host__ __device__ constexpr int brec_stride(int N) { return round4(N * (2 * N + 2)); }
 
 // General-solver layer record: the flux layer record, then the eigenvectors
 // and sources at the user polar angles of the current mode:

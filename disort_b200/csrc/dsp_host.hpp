@@ -232,7 +232,7 @@ inline Sizes sizes_for(int N, int L) {
 
 inline size_t workspace_budget() {
   const char* e = std::getenv("DSP_WORKSPACE_MB");
-  size_t mb = e ? (size_t)std::strtoull(e, nullptr, 10) : 8192;
+  size_t mb = e ? (size_t)std::strtoull(e, nullptr, 10) : 16384;
   if (mb < 16) mb = 16;
   return mb << 20;
 }

@@ -14,7 +14,7 @@
 //  - Every pointer in the batch and in the output must be device memory; the
 //    batch must carry DSP_FLAG_DEVICE_POINTERS.
 //  - One instance's workspace must fit in the array (a 60-layer, 16-stream
-//    instance needs about 0.3 MB; the limit is reached near 330 layers at 64
+//    instance needs about 0.4 MB; the limit is reached near 330 layers at 64
 //    streams); larger instances are rejected with DSP_ERR_NO_MEMORY before any
 //    work is queued.  Bigger batches run as several launches that reuse the array.
 //  - The array is shared by every call on a device and keeps the last call's

@@ -12,11 +12,14 @@
 //    through shared memory;
 //  - free slots (last layer's pivot rows) receive the new continuity rows in
 //    slot order, each thread finding its row index by a popcount;
-//  - W_l = U^{-1}[V | c] is a column-oriented back substitution across the
-//    pivot-row owners, one row of X broadcast per step;
-//  - the layer records (and, going back up, the W_l records) are brought into
-//    a shared-memory ring with cp.async one layer ahead of their use, so the
-//    elimination of a layer hides the memory latency of the next one.
+//  - the N pivot rows of a layer, [U | V | c] with U x_l + V x_{l+1} = c, go
+//    to the layer's elimination record as they are; going back up, x_l is the
+//    solution of U x_l = c - V x_{l+1}, a 16-step triangular solve across the
+//    lanes (one row each) instead of a back substitution over N + 1 columns on
+//    the way down;
+//  - the layer records (and, going back up, the elimination records) are
+//    brought into a shared-memory ring with cp.async one layer ahead of their
+//    use, so the work on a layer hides the memory latency of the next one.
 #pragma once
 
 #include "dsp_device.cuh"
@@ -37,11 +40,9 @@ struct RCfg {
   static constexpr int TEAM = pow2ceil(PR) < 8 ? 8 : pow2ceil(PR);
   static constexpr int CTA = TEAM >= 32 ? TEAM : 32;
   static constexpr int TPC = CTA / TEAM;
-  static constexpr int XS = N + 1;  // row stride of the X matrix (next block + rhs)
   // team shared memory (doubles)
   static constexpr int O_BUF = 0;                  // 2 x pivot row: cur[N] nxt[N] rhs, -1/pivot
-  static constexpr int O_X = O_BUF + 2 * (2 * N + 2);  // X[N][N+1]
-  static constexpr int O_XV = O_X + N * XS;    // x ping-pong [2][N]
+  static constexpr int O_XV = O_BUF + 2 * (2 * N + 2);  // x ping-pong [2][N]
   static constexpr int O_EC = O_XV + 2 * N;    // [N]
   static constexpr int O_I = O_EC + N;         // intensities [N]
   static constexpr int O_E = O_I + N;          // exp(eig*dtau) of layers l, l+1 [2][NN]
@@ -50,8 +51,10 @@ struct RCfg {
   // record ring: 3 layer records going down; 2 x (layer record + W record) going up
   static constexpr int RS = lrec_stride(N);
   static constexpr int BS = brec_stride(N);
+  static constexpr int RL = 2 * N + 2;  // record row: U[N] | V[N] | c | 1/pivot
   static constexpr int O_RING = round4(O_PIV + N / 2 + 1);
-  static constexpr int RING = imax(3 * RS, 2 * (RS + BS));
+  // going down: 3 layer records; going up: 2 layer records and 1 elimination record
+  static constexpr int RING = imax(3 * RS, 2 * RS + BS);
   static constexpr int TEAM_SMEM = round4(O_RING + RING);
   static constexpr int TAB = 2 * N;  // mu and wt of the constant tables
   // register budget per thread: 128 keeps 16 single-warp CTAs resident per SM
@@ -62,7 +65,7 @@ struct RCfg {
 template <int N, bool GEN = false>
 __global__ void __launch_bounds__(RCfg<N>::CTA, RCfg<N>::MINB) flux_bvp_reg_kernel(FluxParams p) {
   using C = RCfg<N>;
-  constexpr int NN = C::NN, TEAM = C::TEAM, PR = C::PR, XS = C::XS;
+  constexpr int NN = C::NN, TEAM = C::TEAM, PR = C::PR;
   constexpr double PI = 3.14159265358979323846;
   static_assert(PR <= 32 && TEAM <= 32, "register panel needs one warp");
   extern __shared__ double smem[];
@@ -141,7 +144,6 @@ __global__ void __launch_bounds__(RCfg<N>::CTA, RCfg<N>::MINB) flux_bvp_reg_kern
 
   double* sm = smem + C::TAB + team * C::TEAM_SMEM;
   double* bufs = sm + C::O_BUF;
-  double* X = sm + C::O_X;
   double* XV = sm + C::O_XV;
   double* ec = sm + C::O_EC;
   double* Iv = sm + C::O_I;
@@ -150,7 +152,8 @@ __global__ void __launch_bounds__(RCfg<N>::CTA, RCfg<N>::MINB) flux_bvp_reg_kern
   constexpr int RS = C::RS, BS = C::BS;
   double* ring = sm + C::O_RING;
   auto RF = [&](int l) { return ring + (l % 3) * RS; };        // going down: layer l's record
-  auto RB = [&](int l) { return ring + (l & 1) * (RS + BS); };  // going up: layer record, then W_l
+  auto RB = [&](int l) { return ring + (l & 1) * RS; };  // going up: layer records
+  double* const EB = ring + 2 * RS;                        // going up: the elimination record
 
   double cur[N], nxt[N], rhs = 0.0;
 #pragma unroll
@@ -345,37 +348,16 @@ __global__ void __launch_bounds__(RCfg<N>::CTA, RCfg<N>::MINB) flux_bvp_reg_kern
     DSP_PHASE(21)
 
     if (!last) {
-      // X = U^{-1} [nxt | rhs]: column-oriented back substitution over the pivot rows
+      // the pivot row of column c is row c of the layer's elimination record
+      if (myc >= 0) {
+        double* row = brec0 + (long long)l * BS + myc * C::RL;
 #pragma unroll
-      for (int c = N - 1; c >= 0; --c) {
-        if (myc == c) {
-          const double rinv = rdiag;
-#pragma unroll
-          for (int j = 0; j < N; ++j) {
-            const double x = nxt[j] * rinv;
-            nxt[j] = x;
-            X[c * XS + j] = x;
-          }
-          const double x = rhs * rinv;
-          rhs = x;
-          X[c * XS + N] = x;
+        for (int j = 0; j < N; j += 2) {
+          *reinterpret_cast<double2*>(row + j) = make_double2(cur[j], cur[j + 1]);
+          *reinterpret_cast<double2*>(row + N + j) = make_double2(nxt[j], nxt[j + 1]);
         }
-        __syncwarp(msk);
-        if (myc >= 0 && myc < c) {
-          const double u = cur[c];
-#pragma unroll
-          for (int j = 0; j < N; ++j) nxt[j] -= u * X[c * XS + j];
-          rhs -= u * X[c * XS + N];
-        }
+        *reinterpret_cast<double2*>(row + 2 * N) = make_double2(rhs, rdiag);
       }
-      __syncwarp(msk);
-      // W_l transposed (Wt[n][c]) and d_l, coalesced
-      double* br = brec0 + (long long)l * brec_stride(N);
-      for (int it = t; it < N * N; it += TEAM) {
-        const int n = it / N, c = it % N;
-        br[it] = X[c * XS + n];
-      }
-      for (int c = t; c < N; c += TEAM) br[N * N + c] = X[c * XS + N];
       // carried rows become the next layer's current block
 #pragma unroll
       for (int k = 0; k < N; ++k) {
@@ -490,26 +472,36 @@ __global__ void __launch_bounds__(RCfg<N>::CTA, RCfg<N>::MINB) flux_bvp_reg_kern
   team_copy_async<TEAM>(RB(ncut - 1), LR(ncut - 1), RS, t);
   cp_async_commit();
   for (int l = ncut - 1; l >= 0; --l) {
-    // layer l-1's records start loading into the slot of layer l+1
-    if (l > 0) {
-      team_copy_async<TEAM>(RB(l - 1), LR(l - 1), RS, t);
-      team_copy_async<TEAM>(RB(l - 1) + RS, brec0 + (long long)(l - 1) * BS, BS, t);
-    }
-    cp_async_commit();
-    cp_async_wait<1>();
+    cp_async_wait<0>();
     __syncwarp(msk);
     double* x = XV + (l & 1) * N;
     if (l < ncut - 1) {
+      // U x_l = c - V x_{l+1}: lane t holds row t; column c's unknown is
+      // formed by lane c and broadcast, the rows above it are updated
       const double* xn = XV + ((l & 1) ^ 1) * N;
-      const double* br = RB(l) + RS;
+      const double* row = EB + (t < N ? t : 0) * C::RL;
+      double r = 0.0, rd = 0.0;
       if (t < N) {
-        double s = br[N * N + t];
+        r = row[2 * N];
 #pragma unroll
-        for (int n = 0; n < N; ++n) s -= br[n * N + t] * xn[n];
-        x[t] = s;
+        for (int n = 0; n < N; ++n) r -= row[N + n] * xn[n];
+        rd = row[2 * N + 1];
+      }
+#pragma unroll
+      for (int c = N - 1; c >= 0; --c) {
+        const double xc = __shfl_sync(msk, r * rd, c, TEAM);
+        if (t == c) x[c] = xc;
+        if (t < c) r -= row[c] * xc;
       }
       __syncwarp(msk);
     }
+    // the records of layer l-1 start loading (the elimination record is used
+    // up; the layer-record slot held layer l+1)
+    if (l > 0) {
+      team_copy_async<TEAM>(RB(l - 1), LR(l - 1), RS, t);
+      team_copy_async<TEAM>(EB, brec0 + (long long)(l - 1) * BS, BS, t);
+    }
+    cp_async_commit();
     if constexpr (GEN) {
       if (t < N) cc0[(long long)l * N + t] = x[t];
       if (m == 0)
