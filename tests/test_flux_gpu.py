@@ -108,6 +108,28 @@ def test_device_pointers_match_host_pointers():
         np.testing.assert_array_equal(got[f], dgot[f])
 
 
+def test_host_pipeline_pieces_match_device_pointers():
+    """Host-buffer batches large enough to be cut into pieces (upload, solve and
+    download overlapped on copy streams) give the device-pointer results bit for
+    bit, with pinned and with pageable host memory."""
+    import torch
+    n = 12000  # several pieces on a 148-SM GPU (pieces of at least 32 instances per SM)
+    w = workloads.subset(workloads.thermal_sweep(), np.arange(n))
+    dgot, dgst, rc = gpu_lib.flux_solve_device(w)
+    assert rc == 0 and not dgst.any()
+    got, gst, rc = gpu_lib.flux_solve(w)  # pageable numpy buffers
+    assert rc == 0 and not gst.any()
+    for f in capi.FLUX_OUT_FIELDS:
+        np.testing.assert_array_equal(got[f], dgot[f])
+    pinned = dict(w)
+    pinned["arrays"] = {k: (torch.from_numpy(np.ascontiguousarray(a)).pin_memory().numpy()
+                            if isinstance(a, np.ndarray) else a) for k, a in w["arrays"].items()}
+    pgot, pgst, rc = gpu_lib.flux_solve(pinned)
+    assert rc == 0 and not pgst.any()
+    for f in capi.FLUX_OUT_FIELDS:
+        np.testing.assert_array_equal(pgot[f], dgot[f])
+
+
 def test_invalid_instances_are_flagged_not_fatal():
     w = workloads.subset(workloads.thermal_sweep(), np.arange(8))
     w["arrays"]["single_scat_albedo"] = w["arrays"]["single_scat_albedo"].copy()
