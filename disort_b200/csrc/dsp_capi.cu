@@ -35,17 +35,15 @@ dsp_status launch_flux_chunk(dsp_context ctx, const FluxParams& p) {
     flux_setup_kernel<<<(p.n + 3) / 4, 128, 0, s>>>(p);
   }
   {
-    KernelTimer kt(ctx, "flux_layer_kernel");
-    using C = LCfg<N>;
-    const size_t sm = C::smem_bytes();
     static bool attr = false;
     if (!attr) {
-      cudaFuncSetAttribute(flux_layer_kernel<N>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+      flux_layer_set_attrs<N>();
       attr = true;
     }
-    const long long tasks = (long long)p.n * p.L;
-    const long long grid = (tasks + C::TPC - 1) / C::TPC;
-    flux_layer_kernel<N><<<(unsigned)grid, C::CTA, sm, s>>>(p);
+    flux_layer_launch<N>(p, s, [&](const char* name, auto&& launch) {
+      KernelTimer kt(ctx, name);
+      launch();
+    });
   }
   if constexpr (N <= 16) {
     using C = RCfg<N>;

@@ -101,8 +101,7 @@ bool tables_for(int N, std::vector<double>& tab) {
 
 template <int N>
 void set_attrs() {
-  cudaFuncSetAttribute(flux_layer_kernel<N>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                       (int)LCfg<N>::smem_bytes());
+  flux_layer_set_attrs<N>();
   if constexpr (N > 16)
     cudaFuncSetAttribute(flux_bvp_tile_kernel<N>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                          (int)TCfg<N>::smem_bytes());
@@ -111,11 +110,7 @@ void set_attrs() {
 template <int N>
 void launch(const FluxParams& p, cudaStream_t s) {
   flux_setup_kernel<<<(p.n + 3) / 4, 128, 0, s>>>(p);
-  {
-    using C = LCfg<N>;
-    const long long tasks = (long long)p.n * p.L;
-    flux_layer_kernel<N><<<(unsigned)((tasks + C::TPC - 1) / C::TPC), C::CTA, C::smem_bytes(), s>>>(p);
-  }
+  flux_layer_launch<N>(p, s, [](const char*, auto&& launch) { launch(); });
   if constexpr (N <= 16) {
     using C = RCfg<N>;
     flux_bvp_reg_kernel<N><<<(p.n + C::TPC - 1) / C::TPC, C::CTA, C::smem_bytes(), s>>>(p);

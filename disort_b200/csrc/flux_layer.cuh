@@ -70,6 +70,48 @@ struct LCfg {
   static constexpr int MINB = MINB_SMEM < 1 ? 1 : (MINB_SMEM < MINB_REGS ? MINB_SMEM : MINB_REGS);
 };
 
+// Whether the layer stage of an N-stream flux solve is split in three launches:
+// the front of the layer kernel (phase matrix, alpha -/+ beta, Cholesky,
+// S = L^T M L), the eigensolver with one thread per layer task
+// (flux_jacobi_kernel), and the back of the layer kernel (eigenvectors, G,
+// particular solutions).  A thread that owns a whole 8 x 8 S and its eigenvector
+// matrix in registers runs the rotations of a sweep with no shuffles or
+// barriers; the team form spends most of its time waiting on them.
+template <int N>
+__host__ __device__ constexpr bool layer_split() { return N >= 10 && N <= 16; }
+
+// packed lower-triangle index of the symmetric element (r, c)
+__host__ __device__ constexpr int tri_idx(int r, int c) {
+  return r >= c ? r * (r + 1) / 2 + c : c * (c + 1) / 2 + r;
+}
+
+// Hand-off between the three launches of a split layer stage, kept in the
+// boundary-value records' area (dead until the boundary-value kernel runs):
+//   per task j, contiguous at bvp_rec + j HA: flag (0 skipped, 1 primary
+//     factorisation, 2 fallback), alpha - beta, alpha + beta (row-major NN x NN,
+//     the latter only with a beam) and the Cholesky factor L (packed lower);
+//   then, at bvp_rec + nt HA, blocks of 32 tasks with element e of the block's
+//     lane k at 32 HS b + e w + k (w = tasks in the block): flag, S (packed
+//     lower), then the eigensolver's diagonal and eigenvector matrix (row-major).
+template <int NN>
+struct Handoff {
+  static constexpr int TRI = NN * (NN + 1) / 2;
+  static constexpr int A_AMB = 1, A_APB = 1 + NN * NN, A_L = 1 + 2 * NN * NN;
+  static constexpr int HA = (A_L + TRI + 1) & ~1;
+  static constexpr int S_FLAG = 0, S_S = 1, S_D = 1 + TRI, S_V = 1 + TRI + NN;
+  static constexpr int HS = S_V + NN * NN;
+};
+
+// address of element e of task j in the lane-interleaved blocks
+template <int NN>
+__device__ __forceinline__ double* handoff_lane(double* bvp_rec, long long nt, long long j, int e) {
+  using H = Handoff<NN>;
+  const long long b = j >> 5;
+  const long long left = nt - (b << 5);
+  const int w = left < 32 ? (int)left : 32;
+  return bvp_rec + nt * H::HA + b * 32 * H::HS + (long long)e * w + (j & 31);
+}
+
 // Round-robin pairing of NNP players in round r: (arr[a], arr[NNP-1-a]),
 // arr[0] = 0, arr[j] = 1 + (j - 1 + r) mod (NNP - 1).
 template <int NNP>
@@ -339,9 +381,13 @@ __device__ void gen_user_angles(const FluxParams& p, int i, double* sm, const do
   }
 }
 
-template <int N, bool GEN = false>
+// STAGE 0: the whole layer task; 1: through S = L^T M L, written to the
+// hand-off; 2: from the eigenpairs in the hand-off to the layer record.
+template <int N, bool GEN = false, int STAGE = 0>
 __global__ void __launch_bounds__(LCfg<N, GEN>::CTA, LCfg<N, GEN>::MINB) flux_layer_kernel(FluxParams p) {
+  static_assert(STAGE == 0 || (!GEN && layer_split<N>()), "split layer stages are for flux solves, N 10..16");
   using C = LCfg<N, GEN>;
+  using H = Handoff<N / 2>;
   constexpr int NN = C::NN, TEAM = C::TEAM, NNP = C::NNP, NPAIR = C::NPAIR, NS = C::NS, BPT = C::BPT;
   constexpr int BPA = NPAIR;  // blocks (a, b) per column pair b
   extern __shared__ double smem[];
@@ -382,9 +428,25 @@ __global__ void __launch_bounds__(LCfg<N, GEN>::CTA, LCfg<N, GEN>::MINB) flux_la
     pml = p.pmom.row(i) + (long long)lin * p.pc;
   }
   const InstLayout& il = GEN ? il_gen : p.il;
-  if (p.status && p.status[i] == DSP_ERR_INVALID_INPUT) return;
+  // the front of a split stage marks the tasks it does not solve, for the
+  // eigensolver and the back (which skip them)
+  auto mark_skipped = [&]() {
+    if constexpr (STAGE == 1) {
+      if (t == 0) {
+        p.bvp_rec[task * H::HA] = 0.0;
+        *handoff_lane<N / 2>(p.bvp_rec, (long long)p.n * p.L, task, H::S_FLAG) = 0.0;
+      }
+    }
+  };
+  if (p.status && p.status[i] == DSP_ERR_INVALID_INPUT) {
+    mark_skipped();
+    return;
+  }
   const int ncut = (int)rec[H_NCUT];
-  if (lc >= ncut) return;  // layers below the absorption cut are never used
+  if (lc >= ncut) {  // layers below the absorption cut are never used
+    mark_skipped();
+    return;
+  }
   if constexpr (GEN) {
     // modes past the instance's last one, or after its azimuthal series converged
     if (p.g.m > (int)rec[H_NAZ] || rec[H_DONE] != 0.0) return;
@@ -431,207 +493,252 @@ __global__ void __launch_bounds__(LCfg<N, GEN>::CTA, LCfg<N, GEN>::MINB) flux_la
   }
   team_sync<TEAM>();
   DSP_PHASE(0)
-  // ---- phase matrix, unique half (FluxSolver.cpp:466-482) ---------------
-  // thread t owns column jq = t; its Legendre column is held in registers
-  if (t < N) {
-    const int jq = t;
-    double yj[N];
-#pragma unroll
-    for (int l = 0; l < N; ++l) yj[l] = Y[l * N + jq];
-    const double wj = wt[jq];
-    for (int iq = 0; iq < NN; ++iq) {
-      double s = 0.0;
-#pragma unroll
-      for (int l = 0; l < N; ++l) s += (gl[l] * Y[l * N + iq]) * yj[l];
-      CC[iq * N + jq] = (s * 0.5) * wj;
-    }
-  }
-  team_sync<TEAM>();
-  DSP_PHASE(1)
-  // ---- alpha -/+ beta and the similarity transform (:485-514) ------------
-  for (int it = t; it < NN * NN; it += TEAM) {
-    const int iq = it / NN, jq = it % NN;
-    const double inv_cmu = 1.0 / mu[iq];
-    const double a = CC[iq * N + jq], b = CC[iq * N + NN + jq];
-    double amb = inv_cmu * (a - b), apb = inv_cmu * (a + b);
-    if (iq == jq) { amb -= inv_cmu; apb -= inv_cmu; }
-    AMB[iq * NS + jq] = amb;
-    APB[iq * NS + jq] = apb;
-    S0[iq * NS + jq] = dsim[iq] * apb * dinv[jq];     // A_s
-    S1[iq * NS + jq] = -dsim[iq] * amb * dinv[jq];    // -B_s
-  }
-  team_sync<TEAM>();
-  // ---- Cholesky of -B_s, else of -A_s (:521-558) -------------------------
-  bool primary = ws < 1.0 - 1e-12;
-  if (primary) primary = team_chol<NN, NS, TEAM>(S1, LC, misc, t);
-  if (!primary) {
-    for (int it = t; it < NN * NN; it += TEAM) {
-      const int r = it / NN, c = it % NN;
-      V[r * NS + c] = -S0[r * NS + c];
+  bool primary = true;
+  if constexpr (STAGE != 2) {
+    // ---- phase matrix, unique half (FluxSolver.cpp:466-482) ---------------
+    // thread t owns column jq = t; its Legendre column is held in registers
+    if (t < N) {
+      const int jq = t;
+      double yj[N];
+  #pragma unroll
+      for (int l = 0; l < N; ++l) yj[l] = Y[l * N + jq];
+      const double wj = wt[jq];
+      for (int iq = 0; iq < NN; ++iq) {
+        double s = 0.0;
+  #pragma unroll
+        for (int l = 0; l < N; ++l) s += (gl[l] * Y[l * N + iq]) * yj[l];
+        CC[iq * N + jq] = (s * 0.5) * wj;
+      }
     }
     team_sync<TEAM>();
-    if (!team_chol<NN, NS, TEAM>(V, LC, misc, t)) {
-      // -A_s not SPD either: try the primary factorisation regardless of omega'
-      primary = team_chol<NN, NS, TEAM>(S1, LC, misc, t);
-      if (!primary) {
-        if (t == 0) set_status(p.status, i, DSP_ERR_EIGEN);
-        return;
-      }
+    DSP_PHASE(1)
+    // ---- alpha -/+ beta and the similarity transform (:485-514) ------------
+    for (int it = t; it < NN * NN; it += TEAM) {
+      const int iq = it / NN, jq = it % NN;
+      const double inv_cmu = 1.0 / mu[iq];
+      const double a = CC[iq * N + jq], b = CC[iq * N + NN + jq];
+      double amb = inv_cmu * (a - b), apb = inv_cmu * (a + b);
+      if (iq == jq) { amb -= inv_cmu; apb -= inv_cmu; }
+      AMB[iq * NS + jq] = amb;
+      APB[iq * NS + jq] = apb;
+      S0[iq * NS + jq] = dsim[iq] * apb * dinv[jq];     // A_s
+      S1[iq * NS + jq] = -dsim[iq] * amb * dinv[jq];    // -B_s
     }
-  }
-  DSP_PHASE(2)
-  // S = L^T M L with M = -A_s (primary) or -B_s (fallback); V used as scratch
-  for (int it = t; it < NN * NN; it += TEAM) {
-    const int r = it / NN, c = it % NN;
-    double s = 0.0;
-    if (primary)
-      for (int k = 0; k < NN; ++k) s += -S0[r * NS + k] * LC[k * NS + c];
-    else
-      for (int k = 0; k < NN; ++k) s += S1[r * NS + k] * LC[k * NS + c];
-    V[r * NS + c] = s;
-  }
-  team_sync<TEAM>();
-  for (int it = t; it < NN * NN; it += TEAM) {
-    const int r = it / NN, c = it % NN;
-    double s = 0.0;
-    for (int k = 0; k < NN; ++k) s += LC[k * NS + r] * V[k * NS + c];
-    S0[r * NS + c] = s;
-  }
-  team_sync<TEAM>();
-  // ---- cyclic Jacobi on S (symmetrised from its lower triangle) -----------
-  for (int it = t; it < NN * NN; it += TEAM) {
-    const int r = it / NN, c = it % NN;
-    S1[r * NS + c] = (c > r) ? S0[c * NS + r] : S0[r * NS + c];
-    V[r * NS + c] = (r == c) ? 1.0 : 0.0;
-  }
-  team_sync<TEAM>();
-  DSP_PHASE(3)
-  // In place: in a round every 2x2 block of S is read and written by its owner
-  // only, and the diagonal blocks a rotation is computed from are written by
-  // their owner after it has received that rotation.
-  double* const Sc = S1;
-  double* const Sn = S1;
-  for (int sweep = 0; sweep < 20; ++sweep) {
-    for (int r = 0; r < NNP - 1; ++r) {
-      // rotation of pair a is computed by thread a; each thread then needs the
-      // rotations of its block's two pairs only (blocks are assigned statically)
-      double c = 1.0, sn = 0.0, tt = 0.0;
-      if (t < NPAIR) {
-        const int pp = rr_player<NNP>(r, t), qq = rr_player<NNP>(r, NNP - 1 - t);
-        if (pp < NN && qq < NN) {
-          jacobi_rot(Sc[pp * NS + qq], Sc[pp * NS + pp], Sc[qq * NS + qq], c, sn, tt);
+    team_sync<TEAM>();
+    // ---- Cholesky of -B_s, else of -A_s (:521-558) -------------------------
+    primary = ws < 1.0 - 1e-12;
+    if (primary) primary = team_chol<NN, NS, TEAM>(S1, LC, misc, t);
+    if (!primary) {
+      for (int it = t; it < NN * NN; it += TEAM) {
+        const int r = it / NN, c = it % NN;
+        V[r * NS + c] = -S0[r * NS + c];
+      }
+      team_sync<TEAM>();
+      if (!team_chol<NN, NS, TEAM>(V, LC, misc, t)) {
+        // -A_s not SPD either: try the primary factorisation regardless of omega'
+        primary = team_chol<NN, NS, TEAM>(S1, LC, misc, t);
+        if (!primary) {
+          if (t == 0) set_status(p.status, i, DSP_ERR_EIGEN);
+          mark_skipped();
+          return;
         }
       }
-      if constexpr (TEAM > 32) {
+    }
+    DSP_PHASE(2)
+    // S = L^T M L with M = -A_s (primary) or -B_s (fallback); V used as scratch
+    for (int it = t; it < NN * NN; it += TEAM) {
+      const int r = it / NN, c = it % NN;
+      double s = 0.0;
+      if (primary)
+        for (int k = 0; k < NN; ++k) s += -S0[r * NS + k] * LC[k * NS + c];
+      else
+        for (int k = 0; k < NN; ++k) s += S1[r * NS + k] * LC[k * NS + c];
+      V[r * NS + c] = s;
+    }
+    team_sync<TEAM>();
+    for (int it = t; it < NN * NN; it += TEAM) {
+      const int r = it / NN, c = it % NN;
+      double s = 0.0;
+      for (int k = 0; k < NN; ++k) s += LC[k * NS + r] * V[k * NS + c];
+      S0[r * NS + c] = s;
+    }
+    team_sync<TEAM>();
+  }
+  if constexpr (STAGE == 1) {
+    // ---- hand-off to the eigensolver and the back of the stage ----------
+    const long long nt = (long long)p.n * p.L;
+    double* st = p.bvp_rec + task * H::HA;
+    const bool beam = rec[H_FBEAM] > 0.0;
+    for (int it = t; it < NN * NN; it += TEAM) {
+      const int r = it / NN, c = it % NN;
+      st[H::A_AMB + it] = AMB[r * NS + c];
+      if (beam) st[H::A_APB + it] = APB[r * NS + c];
+    }
+    for (int r = 0; r < NN; ++r)
+      for (int c = t; c <= r; c += TEAM) {
+        st[H::A_L + tri_idx(r, c)] = LC[r * NS + c];
+        *handoff_lane<NN>(p.bvp_rec, nt, task, H::S_S + tri_idx(r, c)) = S0[r * NS + c];
+      }
+    if (t == 0) {
+      st[0] = primary ? 1.0 : 2.0;
+      *handoff_lane<NN>(p.bvp_rec, nt, task, H::S_FLAG) = 1.0;
+    }
+    return;
+  }
+  double* const Sc = S1;
+  if constexpr (STAGE == 2) {
+    // ---- eigenpairs of S and the front's matrices from the hand-off -----
+    const long long nt = (long long)p.n * p.L;
+    const double* st = p.bvp_rec + task * H::HA;
+    const double flag = st[0];
+    if (flag == 0.0) return;  // the front did not solve this task
+    primary = flag == 1.0;
+    const bool beam = rec[H_FBEAM] > 0.0;
+    for (int it = t; it < NN * NN; it += TEAM) {
+      const int r = it / NN, c = it % NN;
+      AMB[r * NS + c] = st[H::A_AMB + it];
+      if (beam) APB[r * NS + c] = st[H::A_APB + it];
+      LC[r * NS + c] = c <= r ? st[H::A_L + tri_idx(r, c)] : 0.0;
+      V[r * NS + c] = *handoff_lane<NN>(p.bvp_rec, nt, task, H::S_V + it);
+    }
+    for (int k = t; k < NN; k += TEAM) Sc[k * NS + k] = *handoff_lane<NN>(p.bvp_rec, nt, task, H::S_D + k);
+    team_sync<TEAM>();
+  }
+  if constexpr (STAGE == 0) {
+    // ---- cyclic Jacobi on S (symmetrised from its lower triangle) -----------
+    for (int it = t; it < NN * NN; it += TEAM) {
+      const int r = it / NN, c = it % NN;
+      S1[r * NS + c] = (c > r) ? S0[c * NS + r] : S0[r * NS + c];
+      V[r * NS + c] = (r == c) ? 1.0 : 0.0;
+    }
+    team_sync<TEAM>();
+    DSP_PHASE(3)
+    // In place: in a round every 2x2 block of S is read and written by its owner
+    // only, and the diagonal blocks a rotation is computed from are written by
+    // their owner after it has received that rotation.
+    double* const Sn = S1;
+    for (int sweep = 0; sweep < 20; ++sweep) {
+      for (int r = 0; r < NNP - 1; ++r) {
+        // rotation of pair a is computed by thread a; each thread then needs the
+        // rotations of its block's two pairs only (blocks are assigned statically)
+        double c = 1.0, sn = 0.0, tt = 0.0;
         if (t < NPAIR) {
-          rot[3 * t] = c;
-          rot[3 * t + 1] = sn;
-          rot[3 * t + 2] = tt;
+          const int pp = rr_player<NNP>(r, t), qq = rr_player<NNP>(r, NNP - 1 - t);
+          if (pp < NN && qq < NN) {
+            jacobi_rot(Sc[pp * NS + qq], Sc[pp * NS + pp], Sc[qq * NS + qq], c, sn, tt);
+          }
+        }
+        if constexpr (TEAM > 32) {
+          if (t < NPAIR) {
+            rot[3 * t] = c;
+            rot[3 * t + 1] = sn;
+            rot[3 * t + 2] = tt;
+          }
+          team_sync<TEAM>();
+        }
+  #pragma unroll
+        for (int k = 0; k < BPT; ++k) {
+          const int blk = t + k * TEAM;
+          const bool act = blk < NPAIR * NPAIR;
+          const int a = act ? blk / NPAIR : 0, b = act ? blk % NPAIR : 0;  // NPAIR is a power of two or small
+          double ca, sa, ta, cb, sb;
+          if constexpr (TEAM <= 32) {
+            const unsigned m = team_mask<TEAM>();
+            ca = __shfl_sync(m, c, a, TEAM);
+            sa = __shfl_sync(m, sn, a, TEAM);
+            ta = __shfl_sync(m, tt, a, TEAM);
+            cb = __shfl_sync(m, c, b, TEAM);
+            sb = __shfl_sync(m, sn, b, TEAM);
+          } else {
+            ca = rot[3 * a]; sa = rot[3 * a + 1]; ta = rot[3 * a + 2];
+            cb = rot[3 * b]; sb = rot[3 * b + 1];
+          }
+          if (!act) continue;
+          const int pa = rr_player<NNP>(r, a), qa = rr_player<NNP>(r, NNP - 1 - a);
+          const int pb = rr_player<NNP>(r, b), qb = rr_player<NNP>(r, NNP - 1 - b);
+          const bool va = qa < NN && pa < NN, vb = qb < NN && pb < NN;
+          if (a == b) {
+            if (va) {
+              const double apq = Sc[pa * NS + qa];
+              Sn[pa * NS + pa] = Sc[pa * NS + pa] - ta * apq;
+              Sn[qa * NS + qa] = Sc[qa * NS + qa] + ta * apq;
+              const double off = (ta != 0.0) ? 0.0 : apq;
+              Sn[pa * NS + qa] = off;
+              Sn[qa * NS + pa] = off;
+            } else {
+              const int x = pa < NN ? pa : qa;
+              if (x < NN) Sn[x * NS + x] = Sc[x * NS + x];
+            }
+          } else {
+            // rows of pair a (rotated), columns of pair b (rotated); absent
+            // (padding) indices act as the identity
+            const int ri[2] = {pa, qa}, cj[2] = {pb, qb};
+            double X[2][2];
+  #pragma unroll
+            for (int u = 0; u < 2; ++u)
+  #pragma unroll
+              for (int v = 0; v < 2; ++v) {
+                const int rr = ri[u], cc = cj[v];
+                X[u][v] = (rr < NN && cc < NN) ? Sc[rr * NS + cc] : 0.0;
+              }
+            double Y2[2][2];
+            if (va) {
+  #pragma unroll
+              for (int v = 0; v < 2; ++v) {
+                Y2[0][v] = ca * X[0][v] - sa * X[1][v];
+                Y2[1][v] = sa * X[0][v] + ca * X[1][v];
+              }
+            } else {
+  #pragma unroll
+              for (int v = 0; v < 2; ++v) { Y2[0][v] = X[0][v]; Y2[1][v] = X[1][v]; }
+            }
+            double Z2[2][2];
+            if (vb) {
+  #pragma unroll
+              for (int u = 0; u < 2; ++u) {
+                Z2[u][0] = cb * Y2[u][0] - sb * Y2[u][1];
+                Z2[u][1] = sb * Y2[u][0] + cb * Y2[u][1];
+              }
+            } else {
+  #pragma unroll
+              for (int u = 0; u < 2; ++u) { Z2[u][0] = Y2[u][0]; Z2[u][1] = Y2[u][1]; }
+            }
+  #pragma unroll
+            for (int u = 0; u < 2; ++u)
+  #pragma unroll
+              for (int v = 0; v < 2; ++v) {
+                const int rr = ri[u], cc = cj[v];
+                if (rr < NN && cc < NN) Sn[rr * NS + cc] = Z2[u][v];
+              }
+          }
+          // eigenvectors V <- V J for pair b: this thread's share of the rows
+          if (vb) {
+            const int rows_per = (NN + BPA - 1) / BPA;  // blocks sharing pair b split its rows
+            const int r0 = a * rows_per;
+  #pragma unroll 4
+            for (int row = r0; row < r0 + rows_per && row < NN; ++row) {
+              const double vp = V[row * NS + pb], vq = V[row * NS + qb];
+              V[row * NS + pb] = cb * vp - sb * vq;
+              V[row * NS + qb] = sb * vp + cb * vq;
+            }
+          }
         }
         team_sync<TEAM>();
       }
-#pragma unroll
-      for (int k = 0; k < BPT; ++k) {
-        const int blk = t + k * TEAM;
-        const bool act = blk < NPAIR * NPAIR;
-        const int a = act ? blk / NPAIR : 0, b = act ? blk % NPAIR : 0;  // NPAIR is a power of two or small
-        double ca, sa, ta, cb, sb;
-        if constexpr (TEAM <= 32) {
-          const unsigned m = team_mask<TEAM>();
-          ca = __shfl_sync(m, c, a, TEAM);
-          sa = __shfl_sync(m, sn, a, TEAM);
-          ta = __shfl_sync(m, tt, a, TEAM);
-          cb = __shfl_sync(m, c, b, TEAM);
-          sb = __shfl_sync(m, sn, b, TEAM);
-        } else {
-          ca = rot[3 * a]; sa = rot[3 * a + 1]; ta = rot[3 * a + 2];
-          cb = rot[3 * b]; sb = rot[3 * b + 1];
-        }
-        if (!act) continue;
-        const int pa = rr_player<NNP>(r, a), qa = rr_player<NNP>(r, NNP - 1 - a);
-        const int pb = rr_player<NNP>(r, b), qb = rr_player<NNP>(r, NNP - 1 - b);
-        const bool va = qa < NN && pa < NN, vb = qb < NN && pb < NN;
-        if (a == b) {
-          if (va) {
-            const double apq = Sc[pa * NS + qa];
-            Sn[pa * NS + pa] = Sc[pa * NS + pa] - ta * apq;
-            Sn[qa * NS + qa] = Sc[qa * NS + qa] + ta * apq;
-            const double off = (ta != 0.0) ? 0.0 : apq;
-            Sn[pa * NS + qa] = off;
-            Sn[qa * NS + pa] = off;
-          } else {
-            const int x = pa < NN ? pa : qa;
-            if (x < NN) Sn[x * NS + x] = Sc[x * NS + x];
-          }
-        } else {
-          // rows of pair a (rotated), columns of pair b (rotated); absent
-          // (padding) indices act as the identity
-          const int ri[2] = {pa, qa}, cj[2] = {pb, qb};
-          double X[2][2];
-#pragma unroll
-          for (int u = 0; u < 2; ++u)
-#pragma unroll
-            for (int v = 0; v < 2; ++v) {
-              const int rr = ri[u], cc = cj[v];
-              X[u][v] = (rr < NN && cc < NN) ? Sc[rr * NS + cc] : 0.0;
-            }
-          double Y2[2][2];
-          if (va) {
-#pragma unroll
-            for (int v = 0; v < 2; ++v) {
-              Y2[0][v] = ca * X[0][v] - sa * X[1][v];
-              Y2[1][v] = sa * X[0][v] + ca * X[1][v];
-            }
-          } else {
-#pragma unroll
-            for (int v = 0; v < 2; ++v) { Y2[0][v] = X[0][v]; Y2[1][v] = X[1][v]; }
-          }
-          double Z2[2][2];
-          if (vb) {
-#pragma unroll
-            for (int u = 0; u < 2; ++u) {
-              Z2[u][0] = cb * Y2[u][0] - sb * Y2[u][1];
-              Z2[u][1] = sb * Y2[u][0] + cb * Y2[u][1];
-            }
-          } else {
-#pragma unroll
-            for (int u = 0; u < 2; ++u) { Z2[u][0] = Y2[u][0]; Z2[u][1] = Y2[u][1]; }
-          }
-#pragma unroll
-          for (int u = 0; u < 2; ++u)
-#pragma unroll
-            for (int v = 0; v < 2; ++v) {
-              const int rr = ri[u], cc = cj[v];
-              if (rr < NN && cc < NN) Sn[rr * NS + cc] = Z2[u][v];
-            }
-        }
-        // eigenvectors V <- V J for pair b: this thread's share of the rows
-        if (vb) {
-          const int rows_per = (NN + BPA - 1) / BPA;  // blocks sharing pair b split its rows
-          const int r0 = a * rows_per;
-#pragma unroll 4
-          for (int row = r0; row < r0 + rows_per && row < NN; ++row) {
-            const double vp = V[row * NS + pb], vq = V[row * NS + qb];
-            V[row * NS + pb] = cb * vp - sb * vq;
-            V[row * NS + qb] = sb * vp + cb * vq;
-          }
-        }
+      // stop when a further sweep would rotate no pair (the sweep that finds
+      // nothing to do is not run)
+      if (t == 0) misc[1] = 0.0;
+      team_sync<TEAM>();
+      for (int it = t; it < NN * NN; it += TEAM) {
+        const int r = it / NN, c = it % NN;
+        if (c > r && jacobi_needed(Sc[r * NS + c], Sc[r * NS + r], Sc[c * NS + c])) misc[1] = 1.0;
       }
       team_sync<TEAM>();
+      const bool more = misc[1] != 0.0;
+      team_sync<TEAM>();
+      DSP_PHASE(6)
+      if (!more) break;
     }
-    // stop when a further sweep would rotate no pair (the sweep that finds
-    // nothing to do is not run)
-    if (t == 0) misc[1] = 0.0;
-    team_sync<TEAM>();
-    for (int it = t; it < NN * NN; it += TEAM) {
-      const int r = it / NN, c = it % NN;
-      if (c > r && jacobi_needed(Sc[r * NS + c], Sc[r * NS + r], Sc[c * NS + c])) misc[1] = 1.0;
-    }
-    team_sync<TEAM>();
-    const bool more = misc[1] != 0.0;
-    team_sync<TEAM>();
-    DSP_PHASE(6)
-    if (!more) break;
   }
   DSP_PHASE(4)
   // ---- sort ascending; eigenvectors of (a+b)(a-b) ------------------------
@@ -831,6 +938,123 @@ __global__ void __launch_bounds__(LCfg<N, GEN>::CTA, LCfg<N, GEN>::MINB) flux_la
   DSP_PHASE(7)
   if constexpr (GEN) {
     if (p.g.numu > 0) gen_user_angles<N>(p, i, sm, Y, wt, gl, lrec, rec[H_FBEAM], ws, thermal_src, t);
+  }
+}
+
+
+// Rotation of the pair (p, q) applied to S (packed lower, both sides) and to the
+// columns p, q of V; the same update as the team form's 2x2 blocks:
+// column p' = c col p - s col q, column q' = s col p + c col q, and on the
+// diagonal block a_pp - t a_pq, a_qq + t a_pq, a_pq -> 0.
+template <int NN>
+__device__ __forceinline__ void jacobi_apply(double* S, double* V, int p, int q, double c, double s,
+                                             double t) {
+  const double apq = S[tri_idx(p, q)];
+#pragma unroll
+  for (int k = 0; k < NN; ++k) {
+    if (k == p || k == q) continue;
+    const double x = S[tri_idx(k, p)], y = S[tri_idx(k, q)];
+    S[tri_idx(k, p)] = c * x - s * y;
+    S[tri_idx(k, q)] = s * x + c * y;
+  }
+  S[tri_idx(p, p)] -= t * apq;
+  S[tri_idx(q, q)] += t * apq;
+  S[tri_idx(p, q)] = (t != 0.0) ? 0.0 : apq;
+#pragma unroll
+  for (int k = 0; k < NN; ++k) {
+    const double x = V[k * NN + p], y = V[k * NN + q];
+    V[k * NN + p] = c * x - s * y;
+    V[k * NN + q] = s * x + c * y;
+  }
+}
+
+// Cyclic Jacobi eigensolver of the split layer stage: one thread per layer task,
+// S (packed lower) and the eigenvector matrix in registers, every index a
+// compile-time constant (rounds and pairs unrolled).  The sweeps, the
+// round-robin pair order, the rotation (jacobi_rot) and the stopping rule (a
+// sweep is run while some pair still needs a rotation, at most 20) are those of
+// the team form in flux_layer_kernel; a warp runs until its last task has
+// converged, and a converged task's rotations are the identity.
+template <int NN>
+__global__ void __launch_bounds__(128) flux_jacobi_kernel(FluxParams p) {
+  using H = Handoff<NN>;
+  constexpr int NNP = NN + (NN & 1), NPAIR = NNP / 2;
+  const long long nt = (long long)p.n * p.L;
+  const long long j = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (j - (threadIdx.x & 31) >= nt) return;  // whole warp past the end (warp-uniform)
+  const bool in = j < nt;
+  double* const flag = handoff_lane<NN>(p.bvp_rec, nt, in ? j : nt - 1, H::S_FLAG);
+  const bool act = in && *flag != 0.0;
+  double S[H::TRI], V[NN * NN];
+#pragma unroll
+  for (int e = 0; e < H::TRI; ++e) S[e] = act ? *handoff_lane<NN>(p.bvp_rec, nt, j, H::S_S + e) : 0.0;
+#pragma unroll
+  for (int e = 0; e < NN * NN; ++e) V[e] = (e / NN == e % NN) ? 1.0 : 0.0;
+  for (int sweep = 0; sweep < 20; ++sweep) {
+#pragma unroll
+    for (int r = 0; r < NNP - 1; ++r) {
+      double c[NPAIR], s[NPAIR], tt[NPAIR];
+#pragma unroll
+      for (int a = 0; a < NPAIR; ++a) {
+        const int pp = rr_player<NNP>(r, a), qq = rr_player<NNP>(r, NNP - 1 - a);
+        c[a] = 1.0;
+        s[a] = 0.0;
+        tt[a] = 0.0;
+        if (pp < NN && qq < NN)
+          jacobi_rot(S[tri_idx(pp, qq)], S[tri_idx(pp, pp)], S[tri_idx(qq, qq)], c[a], s[a], tt[a]);
+      }
+#pragma unroll
+      for (int a = 0; a < NPAIR; ++a) {
+        const int pp = rr_player<NNP>(r, a), qq = rr_player<NNP>(r, NNP - 1 - a);
+        if (pp < NN && qq < NN) jacobi_apply<NN>(S, V, pp, qq, c[a], s[a], tt[a]);
+      }
+    }
+    bool more = false;
+#pragma unroll
+    for (int r = 1; r < NN; ++r)
+#pragma unroll
+      for (int q = 0; q < r; ++q)
+        if (jacobi_needed(S[tri_idx(r, q)], S[tri_idx(r, r)], S[tri_idx(q, q)])) more = true;
+    if (!__any_sync(0xffffffffu, act && more)) break;
+  }
+  if (!act) return;
+#pragma unroll
+  for (int k = 0; k < NN; ++k) *handoff_lane<NN>(p.bvp_rec, nt, j, H::S_D + k) = S[tri_idx(k, k)];
+#pragma unroll
+  for (int e = 0; e < NN * NN; ++e) *handoff_lane<NN>(p.bvp_rec, nt, j, H::S_V + e) = V[e];
+}
+
+// Host side of the layer stage: launches (through `wrap(name, launch)`, which
+// may time them) one layer kernel, or the three launches of a split stage.
+template <int N>
+inline void flux_layer_set_attrs() {
+  using C = LCfg<N>;
+  if constexpr (layer_split<N>()) {
+    static_assert(Handoff<N / 2>::HA + Handoff<N / 2>::HS <= brec_stride(N),
+                  "the hand-off must fit in the boundary-value records");
+    cudaFuncSetAttribute(flux_layer_kernel<N, false, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                         (int)C::smem_bytes());
+    cudaFuncSetAttribute(flux_layer_kernel<N, false, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                         (int)C::smem_bytes());
+  } else {
+    cudaFuncSetAttribute(flux_layer_kernel<N>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                         (int)C::smem_bytes());
+  }
+}
+
+template <int N, class Wrap>
+inline void flux_layer_launch(const FluxParams& p, cudaStream_t s, Wrap&& wrap) {
+  using C = LCfg<N>;
+  const long long tasks = (long long)p.n * p.L;
+  const unsigned grid = (unsigned)((tasks + C::TPC - 1) / C::TPC);
+  const size_t sm = C::smem_bytes();
+  if constexpr (layer_split<N>()) {
+    wrap("flux_layer_kernel", [&] { flux_layer_kernel<N, false, 1><<<grid, C::CTA, sm, s>>>(p); });
+    wrap("flux_jacobi_kernel",
+         [&] { flux_jacobi_kernel<N / 2><<<(unsigned)((tasks + 127) / 128), 128, 0, s>>>(p); });
+    wrap("flux_layer_kernel", [&] { flux_layer_kernel<N, false, 2><<<grid, C::CTA, sm, s>>>(p); });
+  } else {
+    wrap("flux_layer_kernel", [&] { flux_layer_kernel<N><<<grid, C::CTA, sm, s>>>(p); });
   }
 }
 
