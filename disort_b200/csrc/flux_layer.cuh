@@ -942,6 +942,29 @@ __global__ void __launch_bounds__(LCfg<N, GEN>::CTA, LCfg<N, GEN>::MINB) flux_la
 }
 
 
+// The rotation of jacobi_rot from two reciprocal square roots, without branches
+// or divisions (a sweep is then one scheduling region): with
+// r = 1/sqrt(d^2 + e^2), cos 2theta = |d| r and sin 2theta = sgn(d) e r, so
+// h = cos^2 theta = (1 + |d| r) / 2, g = 1/sqrt(h) = 1/cos theta,
+// c = h g, s = sin 2theta g / 2 and t = tan theta = s g (the same angle as
+// jacobi_rot's t = sgn(d) |e| / (|d| + sqrt(d^2 + e^2)); no cancellation for
+// small angles).  A pair whose d^2 + e^2 is below 1e-280 is left unrotated:
+// S's norm is at least its largest eigenvalue, far above that.
+__device__ __forceinline__ void jacobi_rot_rsq(double apq, double app, double aqq, double& c, double& s,
+                                               double& tt) {
+  const double d = aqq - app, e = 2.0 * apq;
+  const double q = fma(d, d, e * e);
+  const bool rot = jacobi_needed(apq, app, aqq) && q > 1e-280;
+  const double r = rsqrt(rot ? q : 1.0);
+  const double num = d > 0.0 ? e : (d < 0.0 ? -e : fabs(e));  // sgn(d) e, sgn(0) = +1
+  const double h = fma(0.5 * fabs(d), r, 0.5);
+  const double g = rsqrt(h);
+  const double sv = (0.5 * num * r) * g;
+  c = rot ? h * g : 1.0;
+  s = rot ? sv : 0.0;
+  tt = rot ? sv * g : 0.0;
+}
+
 // Rotation of the pair (p, q) applied to S (packed lower, both sides) and to the
 // columns p, q of V; the same update as the team form's 2x2 blocks:
 // column p' = c col p - s col q, column q' = s col p + c col q, and on the
@@ -1001,7 +1024,7 @@ __global__ void __launch_bounds__(128) flux_jacobi_kernel(FluxParams p) {
         s[a] = 0.0;
         tt[a] = 0.0;
         if (pp < NN && qq < NN)
-          jacobi_rot(S[tri_idx(pp, qq)], S[tri_idx(pp, pp)], S[tri_idx(qq, qq)], c[a], s[a], tt[a]);
+          jacobi_rot_rsq(S[tri_idx(pp, qq)], S[tri_idx(pp, pp)], S[tri_idx(qq, qq)], c[a], s[a], tt[a]);
       }
 #pragma unroll
       for (int a = 0; a < NPAIR; ++a) {
