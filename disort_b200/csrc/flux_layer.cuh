@@ -87,18 +87,19 @@ __host__ __device__ constexpr int tri_idx(int r, int c) {
 
 // Hand-off between the three launches of a split layer stage, kept in the
 // boundary-value records' area (dead until the boundary-value kernel runs):
-//   per task j, contiguous at bvp_rec + j HA: flag (0 skipped, 1 primary
-//     factorisation, 2 fallback), alpha - beta, alpha + beta (row-major NN x NN,
-//     the latter only with a beam) and the Cholesky factor L (packed lower);
-//   then, at bvp_rec + nt HA, blocks of 32 tasks with element e of the block's
-//     lane k at 32 HS b + e w + k (w = tasks in the block): flag, S (packed
-//     lower), then the eigensolver's diagonal and eigenvector matrix (row-major).
+// blocks of 32 layer tasks, element e of the block's lane k at
+// 32 HS b + e w + k (w = tasks in the block), so that a warp of the
+// one-thread-per-task kernels reads or writes an element of 32 tasks in one
+// coalesced access.  Per task: flag (0 skipped, 1 primary factorisation,
+// 2 fallback), S (packed lower), the Cholesky factor L (packed lower),
+// alpha - beta and alpha + beta (row-major NN x NN, the latter only with a beam),
+// then the eigensolver's diagonal and eigenvector matrix (row-major, column j
+// the eigenvector of diagonal entry j).
 template <int NN>
 struct Handoff {
   static constexpr int TRI = NN * (NN + 1) / 2;
-  static constexpr int A_AMB = 1, A_APB = 1 + NN * NN, A_L = 1 + 2 * NN * NN;
-  static constexpr int HA = (A_L + TRI + 1) & ~1;
-  static constexpr int S_FLAG = 0, S_S = 1, S_D = 1 + TRI, S_V = 1 + TRI + NN;
+  static constexpr int S_FLAG = 0, S_S = 1, S_L = 1 + TRI, S_AMB = 1 + 2 * TRI, S_APB = S_AMB + NN * NN;
+  static constexpr int S_D = S_APB + NN * NN, S_V = S_D + NN;
   static constexpr int HS = S_V + NN * NN;
 };
 
@@ -109,7 +110,7 @@ __device__ __forceinline__ double* handoff_lane(double* bvp_rec, long long nt, l
   const long long b = j >> 5;
   const long long left = nt - (b << 5);
   const int w = left < 32 ? (int)left : 32;
-  return bvp_rec + nt * H::HA + b * 32 * H::HS + (long long)e * w + (j & 31);
+  return bvp_rec + b * 32 * H::HS + (long long)e * w + (j & 31);
 }
 
 // Round-robin pairing of NNP players in round r: (arr[a], arr[NNP-1-a]),
@@ -382,7 +383,7 @@ __device__ void gen_user_angles(const FluxParams& p, int i, double* sm, const do
 }
 
 // STAGE 0: the whole layer task; 1: through S = L^T M L, written to the
-// hand-off; 2: from the eigenpairs in the hand-off to the layer record.
+// hand-off (the front of a split stage).
 template <int N, bool GEN = false, int STAGE = 0>
 __global__ void __launch_bounds__(LCfg<N, GEN>::CTA, LCfg<N, GEN>::MINB) flux_layer_kernel(FluxParams p) {
   static_assert(STAGE == 0 || (!GEN && layer_split<N>()), "split layer stages are for flux solves, N 10..16");
@@ -432,10 +433,7 @@ __global__ void __launch_bounds__(LCfg<N, GEN>::CTA, LCfg<N, GEN>::MINB) flux_la
   // eigensolver and the back (which skip them)
   auto mark_skipped = [&]() {
     if constexpr (STAGE == 1) {
-      if (t == 0) {
-        p.bvp_rec[task * H::HA] = 0.0;
-        *handoff_lane<N / 2>(p.bvp_rec, (long long)p.n * p.L, task, H::S_FLAG) = 0.0;
-      }
+      if (t == 0) *handoff_lane<N / 2>(p.bvp_rec, (long long)p.n * p.L, task, H::S_FLAG) = 0.0;
     }
   };
   if (p.status && p.status[i] == DSP_ERR_INVALID_INPUT) {
@@ -494,7 +492,7 @@ __global__ void __launch_bounds__(LCfg<N, GEN>::CTA, LCfg<N, GEN>::MINB) flux_la
   team_sync<TEAM>();
   DSP_PHASE(0)
   bool primary = true;
-  if constexpr (STAGE != 2) {
+  {
     // ---- phase matrix, unique half (FluxSolver.cpp:466-482) ---------------
     // thread t owns column jq = t; its Legendre column is held in registers
     if (t < N) {
@@ -567,43 +565,21 @@ __global__ void __launch_bounds__(LCfg<N, GEN>::CTA, LCfg<N, GEN>::MINB) flux_la
   if constexpr (STAGE == 1) {
     // ---- hand-off to the eigensolver and the back of the stage ----------
     const long long nt = (long long)p.n * p.L;
-    double* st = p.bvp_rec + task * H::HA;
     const bool beam = rec[H_FBEAM] > 0.0;
     for (int it = t; it < NN * NN; it += TEAM) {
       const int r = it / NN, c = it % NN;
-      st[H::A_AMB + it] = AMB[r * NS + c];
-      if (beam) st[H::A_APB + it] = APB[r * NS + c];
+      *handoff_lane<NN>(p.bvp_rec, nt, task, H::S_AMB + it) = AMB[r * NS + c];
+      if (beam) *handoff_lane<NN>(p.bvp_rec, nt, task, H::S_APB + it) = APB[r * NS + c];
     }
     for (int r = 0; r < NN; ++r)
       for (int c = t; c <= r; c += TEAM) {
-        st[H::A_L + tri_idx(r, c)] = LC[r * NS + c];
+        *handoff_lane<NN>(p.bvp_rec, nt, task, H::S_L + tri_idx(r, c)) = LC[r * NS + c];
         *handoff_lane<NN>(p.bvp_rec, nt, task, H::S_S + tri_idx(r, c)) = S0[r * NS + c];
       }
-    if (t == 0) {
-      st[0] = primary ? 1.0 : 2.0;
-      *handoff_lane<NN>(p.bvp_rec, nt, task, H::S_FLAG) = 1.0;
-    }
+    if (t == 0) *handoff_lane<NN>(p.bvp_rec, nt, task, H::S_FLAG) = primary ? 1.0 : 2.0;
     return;
   }
   double* const Sc = S1;
-  if constexpr (STAGE == 2) {
-    // ---- eigenpairs of S and the front's matrices from the hand-off -----
-    const long long nt = (long long)p.n * p.L;
-    const double* st = p.bvp_rec + task * H::HA;
-    const double flag = st[0];
-    if (flag == 0.0) return;  // the front did not solve this task
-    primary = flag == 1.0;
-    const bool beam = rec[H_FBEAM] > 0.0;
-    for (int it = t; it < NN * NN; it += TEAM) {
-      const int r = it / NN, c = it % NN;
-      AMB[r * NS + c] = st[H::A_AMB + it];
-      if (beam) APB[r * NS + c] = st[H::A_APB + it];
-      LC[r * NS + c] = c <= r ? st[H::A_L + tri_idx(r, c)] : 0.0;
-      V[r * NS + c] = *handoff_lane<NN>(p.bvp_rec, nt, task, H::S_V + it);
-    }
-    for (int k = t; k < NN; k += TEAM) Sc[k * NS + k] = *handoff_lane<NN>(p.bvp_rec, nt, task, H::S_D + k);
-    team_sync<TEAM>();
-  }
   if constexpr (STAGE == 0) {
     // ---- cyclic Jacobi on S (symmetrised from its lower triangle) -----------
     for (int it = t; it < NN * NN; it += TEAM) {
@@ -1047,17 +1023,352 @@ __global__ void __launch_bounds__(128) flux_jacobi_kernel(FluxParams p) {
   for (int e = 0; e < NN * NN; ++e) *handoff_lane<NN>(p.bvp_rec, nt, j, H::S_V + e) = V[e];
 }
 
+// ---------------------------------------------------------------------------
+// Back of a split layer stage, one thread per layer task: from the eigenpairs
+// of S to the layer record (the STAGE 0 kernel's steps after its Jacobi loop:
+// FluxSolver.cpp:561-587 for k and G+/-, :595-643 and :745-787 for the
+// particular solutions, in the eigen basis described there).  NN x NN operands
+// are held in registers with compile-time indices or read from the
+// lane-interleaved hand-off, whose loads are coalesced across the warp; the
+// Cholesky factor is read again by each phase that needs it (registers, not
+// bandwidth, bound a one-thread task).  Eigenpairs stay in the eigensolver's
+// order: the rank of each eigenvalue in the ascending order places its column
+// of G and its k, and the sums over eigenpairs (W Lam^{-1} W^T) do not depend
+// on the order.
+// ---------------------------------------------------------------------------
+template <int NN>
+struct BackOps {
+  const double* L;    // packed lower
+  const double* rdg;  // 1 / L_kk
+  // x <- L^{-1} x
+  __device__ __forceinline__ void fwd(double* x) const {
+#pragma unroll
+    for (int k = 0; k < NN; ++k) {
+      x[k] *= rdg[k];
+#pragma unroll
+      for (int r = k + 1; r < NN; ++r) x[r] -= L[tri_idx(r, k)] * x[k];
+    }
+  }
+  // x <- L^{-T} x
+  __device__ __forceinline__ void bwd(double* x) const {
+#pragma unroll
+    for (int k = NN - 1; k >= 0; --k) {
+      x[k] *= rdg[k];
+#pragma unroll
+      for (int r = 0; r < k; ++r) x[r] -= L[tri_idx(k, r)] * x[k];
+    }
+  }
+  // x <- L x
+  __device__ __forceinline__ void lmul(double* x) const {
+#pragma unroll
+    for (int r = NN - 1; r >= 0; --r) {
+      double s = 0.0;
+#pragma unroll
+      for (int c = 0; c <= r; ++c) s += L[tri_idx(r, c)] * x[c];
+      x[r] = s;
+    }
+  }
+  // x <- L^T x
+  __device__ __forceinline__ void ltmul(double* x) const {
+#pragma unroll
+    for (int r = 0; r < NN; ++r) {
+      double s = 0.0;
+#pragma unroll
+      for (int k = r; k < NN; ++k) s += L[tri_idx(k, r)] * x[k];
+      x[r] = s;
+    }
+  }
+};
+
+// The warp's 32 tasks have consecutive layer records; a row of W doubles that
+// each lane has put at stg[lane * RS + k] is written for every task of `ok`
+// with consecutive lanes on consecutive doubles (32 / W tasks per store).
+template <int RS>
+__device__ __forceinline__ void warp_flush_rows(const double* stg, double* rec0, int rstride, int W, int off,
+                                                unsigned ok, int lane) {
+  __syncwarp();
+  const int tpi = 32 / W;
+  const int tl = lane / W, k = lane - tl * W;
+  if (tl < tpi)
+    for (int b = tl; b < 32; b += tpi)
+      if ((ok >> b) & 1u) rec0[(long long)b * rstride + off + k] = stg[b * RS + k];
+  __syncwarp();
+}
+
+template <int N>
+__global__ void __launch_bounds__(128) flux_layer_back_kernel(FluxParams p) {
+  constexpr int NN = N / 2;
+  constexpr int RS = N + 3;  // staging row stride: a row of N (+2 for xr after z1)
+  constexpr int LS = lrec_stride(N);
+  using H = Handoff<NN>;
+  constexpr double PI = 3.14159265358979323846;
+  __shared__ double stage[4][2][32 * RS];
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+  const double* const stA = stage[wid][0];
+  const double* const stB = stage[wid][1];
+  double* const sA = stage[wid][0] + lane * RS;
+  double* const sB = stage[wid][1] + lane * RS;
+  const long long nt = (long long)p.n * p.L;
+  const long long j = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  const long long j0 = j - lane;
+  if (j0 >= nt) return;  // whole warp past the end (warp-uniform)
+  // lanes past the end or skipped by the front compute on a valid task's
+  // addresses and write nothing (no early exit: the warp writes rows together)
+  const long long jj = j < nt ? j : nt - 1;
+  auto hv = [&](int e) { return *handoff_lane<NN>(p.bvp_rec, nt, jj, e); };
+  const double flag = hv(H::S_FLAG);
+  const bool act = j < nt && flag != 0.0;  // skipped: cut layer, invalid input, no factorisation
+  const unsigned okm = __ballot_sync(0xffffffffu, act);
+  if (okm == 0u) return;  // warp-uniform
+  const bool primary = flag == 1.0;
+  const int i = (int)(jj / p.L), lc = (int)(jj % p.L);
+  const double* rec = p.inst_rec + (long long)i * p.il.stride;
+  const InstLayout& il = p.il;
+  const double* mu = p.tables + tab_mu(N);
+  const double* dsim = p.tables + tab_dsim(N);
+  const double* dinv = p.tables + tab_dinv(N);
+  double* const rec0 = p.layer_rec + j0 * LS;
+
+  // ---- ascending order of the eigenvalues; k = sqrt|lambda| ----------------
+  double kr[NN], rk[NN];
+  int rank[NN];
+  {
+    double d[NN];
+#pragma unroll
+    for (int k = 0; k < NN; ++k) d[k] = hv(H::S_D + k);
+#pragma unroll
+    for (int k = 0; k < NN; ++k) {
+      int r = 0;
+#pragma unroll
+      for (int q = 0; q < NN; ++q)
+        if (d[q] < d[k] || (d[q] == d[k] && q < k)) ++r;
+      rank[k] = r;
+      kr[k] = sqrt(fabs(d[k]));
+      rk[k] = 1.0 / kr[k];
+      sA[NN + r] = kr[k];
+      sA[NN - 1 - r] = -kr[k];
+    }
+  }
+  warp_flush_rows<RS>(stA, rec0, LS, N, lrec_eig(N), okm, lane);
+  double L[H::TRI], rdg[NN];
+  auto load_L = [&]() {
+#pragma unroll
+    for (int e = 0; e < H::TRI; ++e) L[e] = hv(H::S_L + e);
+#pragma unroll
+    for (int k = 0; k < NN; ++k) rdg[k] = 1.0 / L[tri_idx(k, k)];
+  };
+  const BackOps<NN> ops{L, rdg};
+  {
+    // ---- eigenvectors of (a+b)(a-b): D^{-1} L^{-T} w (primary), D^{-1} L w --
+    double EV[NN][NN];  // EV[c][r]: column c
+    load_L();
+#pragma unroll
+    for (int c = 0; c < NN; ++c) {
+#pragma unroll
+      for (int r = 0; r < NN; ++r) EV[c][r] = hv(H::S_V + r * NN + c);
+      if (primary) ops.bwd(EV[c]);
+      else ops.lmul(EV[c]);
+#pragma unroll
+      for (int r = 0; r < NN; ++r) EV[c][r] *= dinv[r];
+    }
+    // ---- G+/- (FluxSolver.cpp:575-587), two rows per step -------------------
+#pragma unroll 1
+    for (int iq = 0; iq < NN; ++iq) {
+      double arow[NN];
+#pragma unroll
+      for (int k = 0; k < NN; ++k) arow[k] = hv(H::S_AMB + iq * NN + k);
+      double* g0 = sA;  // row NN + iq
+      double* g1 = sB;  // row NN - iq - 1
+#pragma unroll
+      for (int c = 0; c < NN; ++c) {
+        double s = 0.0, gpmigm = 0.0;
+#pragma unroll
+        for (int k = 0; k < NN; ++k) {
+          s += arow[k] * EV[c][k];
+          gpmigm = (k == iq) ? EV[c][k] : gpmigm;
+        }
+        const double gpplgm = s * rk[c];
+        const int jq = rank[c];
+        g0[NN + jq] = 0.5 * (gpplgm + gpmigm);
+        g1[NN + jq] = 0.5 * (gpplgm - gpmigm);
+        g0[NN - jq - 1] = 0.5 * (-gpplgm + gpmigm);
+        g1[NN - jq - 1] = 0.5 * (-gpplgm - gpmigm);
+      }
+      warp_flush_rows<RS>(stA, rec0, LS, N, lrec_G(N) + (NN + iq) * N, okm, lane);
+      warp_flush_rows<RS>(stB, rec0, LS, N, lrec_G(N) + (NN - iq - 1) * N, okm, lane);
+    }
+  }
+  // x <- V diag(1 / (d - shift)) V^T x, one eigenpair at a time
+  auto vsolve = [&](double* x, double shift) {
+    double acc[NN];
+#pragma unroll
+    for (int r = 0; r < NN; ++r) acc[r] = 0.0;
+#pragma unroll 1
+    for (int c = 0; c < NN; ++c) {
+      double v[NN], s = 0.0;
+#pragma unroll
+      for (int r = 0; r < NN; ++r) {
+        v[r] = hv(H::S_V + r * NN + c);
+        s += v[r] * x[r];
+      }
+      const double coef = s / (hv(H::S_D + c) - shift);
+#pragma unroll
+      for (int r = 0; r < NN; ++r) acc[r] += coef * v[r];
+    }
+#pragma unroll
+    for (int r = 0; r < NN; ++r) x[r] = acc[r];
+  };
+  // X1 x = -L^{-T} L^{-1} x ;  X2 x = -L W Lam^{-1} W^T L^T x
+  auto applyX1 = [&](double* x) {
+    ops.fwd(x);
+    ops.bwd(x);
+#pragma unroll
+    for (int r = 0; r < NN; ++r) x[r] = -x[r];
+  };
+  auto applyX2 = [&](double* x) {
+    ops.ltmul(x);
+    vsolve(x, 0.0);
+    ops.lmul(x);
+#pragma unroll
+    for (int r = 0; r < NN; ++r) x[r] = -x[r];
+  };
+
+  const double ws = rec[il.ssa_s + lc];
+  const double dts = rec[il.dtau_s + lc];
+  const double fbeam = rec[H_FBEAM];
+  const unsigned beamm = __ballot_sync(0xffffffffu, act && fbeam > 0.0);
+  if (beamm != 0u && fbeam > 0.0) {
+    // ---- beam (computeBeamSource, FluxSolver.cpp:595-643) -------------------
+    load_L();
+    const double umu0 = rec[H_UMU0];
+    double beam_mu = umu0;
+    const double mu0sq = umu0 * umu0;
+    const double dither = 1000.0 * 2.220446049250313e-16;
+    bool dith = false;
+#pragma unroll
+    for (int k = 0; k < NN; ++k)
+      if (fabs(1.0 - mu0sq * kr[k] * kr[k]) < dither) dith = true;
+    if (dith) beam_mu = 0.999 * umu0;
+    // scaled phase coefficients g'_k (disortSet, FluxSolver.cpp:336-386) times
+    // P_k(-mu0), summed against P_k(+/-mu_r)
+    const int lin = (p.flags & DSP_FLAG_INDEX_FROM_BOTTOM) ? p.L - 1 - lc : lc;
+    const double* pml = p.pmom.row(i) + (long long)lin * p.pc;
+    const int mode = (int)rec[il.mode + lc];
+    const double f = rec[il.fsc + lc], sig = rec[il.sig + lc];
+    const double* yb = rec + il.yb;
+    const double* Y = p.tables + tab_ylm(N);
+    double sp[NN], sm[NN];
+#pragma unroll
+    for (int r = 0; r < NN; ++r) sp[r] = sm[r] = 0.0;
+#pragma unroll 1
+    for (int k = 0; k < N; ++k) {
+      const double pk = pml[k];
+      double g;
+      if (mode == 0) g = (2.0 * k + 1.0) * ws * pk;
+      else if (mode == 1) g = (2.0 * k + 1.0) * ws * (pk - f) / (1.0 - f);
+      else {
+        const double kd = (double)k;
+        g = (2.0 * k + 1.0) * ws * (pk - f * exp(-kd * kd / (2.0 * sig))) / (1.0 - f);
+      }
+      const double gy = g * yb[k];
+#pragma unroll
+      for (int r = 0; r < NN; ++r) {
+        sp[r] += gy * Y[k * N + r];
+        sm[r] += gy * Y[k * N + NN + r];
+      }
+    }
+    double m1[NN], y[NN];
+#pragma unroll
+    for (int r = 0; r < NN; ++r) {
+      const double bp = fbeam * sp[r] / (4.0 * PI), bm = fbeam * sm[r] / (4.0 * PI);
+      m1[r] = (bp + bm) / mu[r];
+      y[r] = (bp - bm) / mu[r];  // M^{-1} r2
+    }
+    // rhs = mu0^{-1} M^{-1} r2 + (a-b) M^{-1} r1, then D rhs
+#pragma unroll
+    for (int r = 0; r < NN; ++r) {
+      double s = 0.0;
+#pragma unroll
+      for (int k = 0; k < NN; ++k) s += hv(H::S_AMB + r * NN + k) * m1[k];
+      y[r] = dsim[r] * (y[r] / beam_mu + s);
+    }
+    // s = -(D^{-1} (B_s A_s - mu0^{-2})^{-1} D) rhs
+    const double shift = 1.0 / (beam_mu * beam_mu);
+    if (primary) {
+      ops.fwd(y);
+      vsolve(y, shift);
+      ops.lmul(y);
+    } else {
+      ops.ltmul(y);
+      vsolve(y, shift);
+      ops.bwd(y);
+    }
+#pragma unroll
+    for (int r = 0; r < NN; ++r) y[r] = -dinv[r] * y[r];
+    // d = mu0 ((a+b) s + M^{-1} r1)
+#pragma unroll
+    for (int r = 0; r < NN; ++r) {
+      double s = 0.0;
+#pragma unroll
+      for (int k = 0; k < NN; ++k) s += hv(H::S_APB + r * NN + k) * y[k];
+      const double dv = beam_mu * (s + m1[r]);
+      sA[NN + r] = 0.5 * (y[r] + dv);
+      sA[NN - r - 1] = 0.5 * (y[r] - dv);
+    }
+  }
+  if (beamm != 0u) warp_flush_rows<RS>(stA, rec0, LS, N, lrec_zb(N), beamm, lane);
+  if (p.flags & DSP_FLAG_THERMAL) {
+    // ---- thermal (computeIsotropicSource, FluxSolver.cpp:745-787) -----------
+    load_L();
+    const double taus_top = rec[il.tau_s + lc];
+    const double pk0 = rec[il.pkag + lc], pk1 = rec[il.pkag + lc + 1];
+    double xr1 = 0.0;
+    if (dts > 1e-4) xr1 = (pk1 - pk0) / dts;
+    const double xr0 = pk0 - xr1 * taus_top;
+    // omega' = 1: no thermal source ((a+b) is singular there)
+    const bool src = (1.0 - ws) != 0.0;
+    double u[NN], dd[NN];
+    // u = -(a+b)^{-1} M^{-1} 1 with (a+b)^{-1} y = D^{-1} X D y (X2 primary, X1 fallback)
+#pragma unroll
+    for (int r = 0; r < NN; ++r) u[r] = dsim[r] * (1.0 / mu[r]);
+    if (src) {
+      if (primary) applyX2(u);
+      else applyX1(u);
+    }
+#pragma unroll
+    for (int r = 0; r < NN; ++r) u[r] = src ? -dinv[r] * u[r] : 0.0;
+    const double c1 = 2.0 * (1.0 - ws) * xr1, c0 = 2.0 * (1.0 - ws) * xr0;
+    // d0 = -(a-b)^{-1} s1 with (a-b)^{-1} y = D^{-1} X D y (X1 primary, X2 fallback)
+#pragma unroll
+    for (int r = 0; r < NN; ++r) dd[r] = dsim[r] * (c1 * u[r]);
+    if (src) {
+      if (primary) applyX1(dd);
+      else applyX2(dd);
+    }
+#pragma unroll
+    for (int r = 0; r < NN; ++r) {
+      const double s1 = c1 * u[r], s0 = c0 * u[r];
+      const double d0 = src ? -dinv[r] * dd[r] : 0.0;
+      sB[NN + r] = 0.5 * s1;
+      sB[NN - r - 1] = 0.5 * s1;
+      sA[NN + r] = 0.5 * (s0 + d0);
+      sA[NN - r - 1] = 0.5 * (s0 - d0);
+    }
+    sB[N] = xr0;  // xr0, xr1 follow z1 in the record
+    sB[N + 1] = xr1;
+    warp_flush_rows<RS>(stA, rec0, LS, N, lrec_z0(N), okm, lane);
+    warp_flush_rows<RS>(stB, rec0, LS, N + 2, lrec_z1(N), okm, lane);
+  }
+}
+
 // Host side of the layer stage: launches (through `wrap(name, launch)`, which
 // may time them) one layer kernel, or the three launches of a split stage.
 template <int N>
 inline void flux_layer_set_attrs() {
   using C = LCfg<N>;
   if constexpr (layer_split<N>()) {
-    static_assert(Handoff<N / 2>::HA + Handoff<N / 2>::HS <= brec_stride(N),
-                  "the hand-off must fit in the boundary-value records");
+    static_assert(Handoff<N / 2>::HS <= brec_stride(N), "the hand-off must fit in the boundary-value records");
     cudaFuncSetAttribute(flux_layer_kernel<N, false, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                         (int)C::smem_bytes());
-    cudaFuncSetAttribute(flux_layer_kernel<N, false, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                          (int)C::smem_bytes());
   } else {
     cudaFuncSetAttribute(flux_layer_kernel<N>, cudaFuncAttributeMaxDynamicSharedMemorySize,
@@ -1075,7 +1386,8 @@ inline void flux_layer_launch(const FluxParams& p, cudaStream_t s, Wrap&& wrap) 
     wrap("flux_layer_kernel", [&] { flux_layer_kernel<N, false, 1><<<grid, C::CTA, sm, s>>>(p); });
     wrap("flux_jacobi_kernel",
          [&] { flux_jacobi_kernel<N / 2><<<(unsigned)((tasks + 127) / 128), 128, 0, s>>>(p); });
-    wrap("flux_layer_kernel", [&] { flux_layer_kernel<N, false, 2><<<grid, C::CTA, sm, s>>>(p); });
+    wrap("flux_layer_kernel",
+         [&] { flux_layer_back_kernel<N><<<(unsigned)((tasks + 127) / 128), 128, 0, s>>>(p); });
   } else {
     wrap("flux_layer_kernel", [&] { flux_layer_kernel<N><<<grid, C::CTA, sm, s>>>(p); });
   }
