@@ -40,7 +40,7 @@ dsp_status launch_flux_chunk(dsp_context ctx, const FluxParams& p) {
       flux_layer_set_attrs<N>();
       attr = true;
     }
-    flux_layer_launch<N>(p, s, [&](const char* name, auto&& launch) {
+    flux_layer_launch<N>(p, ctx->host_tables.at(N).data(), s, [&](const char* name, auto&& launch) {
       KernelTimer kt(ctx, name);
       launch();
     });

@@ -33,6 +33,7 @@ struct dsp_context_s {
   void* stage_out = nullptr;
   size_t stage_out_bytes = 0;
   std::map<int, double*> tables;
+  std::map<int, std::vector<double>> host_tables;  // host copies of `tables`
   std::map<int, double*> mode_tables;  // general solver: one table per azimuth mode
   void* meta = nullptr;                // general solver: chunk index arrays
   size_t meta_bytes = 0;
@@ -204,6 +205,7 @@ inline dsp_status get_tables(dsp_context ctx, int N, const double** out) {
   e = cudaMemcpy(d, tab.data(), tab.size() * sizeof(double), cudaMemcpyHostToDevice);
   if (e != cudaSuccess) return cuda_fail(ctx, e, "cudaMemcpy(tables)");
   ctx->tables[N] = d;
+  ctx->host_tables[N] = tab;
   *out = d;
   return DSP_OK;
 }

@@ -108,9 +108,9 @@ void set_attrs() {
 }
 
 template <int N>
-void launch(const FluxParams& p, cudaStream_t s) {
+void launch(const FluxParams& p, const double* host_tab, cudaStream_t s) {
   flux_setup_kernel<<<(p.n + 3) / 4, 128, 0, s>>>(p);
-  flux_layer_launch<N>(p, s, [](const char*, auto&& launch) { launch(); });
+  flux_layer_launch<N>(p, host_tab, s, [](const char*, auto&& launch) { launch(); });
   if constexpr (N <= 16) {
     using C = RCfg<N>;
     flux_bvp_reg_kernel<N><<<(p.n + C::TPC - 1) / C::TPC, C::CTA, C::smem_bytes(), s>>>(p);
@@ -121,22 +121,22 @@ void launch(const FluxParams& p, cudaStream_t s) {
 }
 
 template <int N>
-void dispatch_attrs_or_launch(bool attrs, const FluxParams* p, cudaStream_t s) {
+void dispatch_attrs_or_launch(bool attrs, const FluxParams* p, const double* host_tab, cudaStream_t s) {
   if (attrs) set_attrs<N>();
-  else launch<N>(*p, s);
+  else launch<N>(*p, host_tab, s);
 }
 
-bool run_for(int N, bool attrs, const FluxParams* p, cudaStream_t s) {
+bool run_for(int N, bool attrs, const FluxParams* p, const double* host_tab, cudaStream_t s) {
   switch (N) {
-    case 4: dispatch_attrs_or_launch<4>(attrs, p, s); return true;
-    case 6: dispatch_attrs_or_launch<6>(attrs, p, s); return true;
-    case 8: dispatch_attrs_or_launch<8>(attrs, p, s); return true;
-    case 10: dispatch_attrs_or_launch<10>(attrs, p, s); return true;
-    case 12: dispatch_attrs_or_launch<12>(attrs, p, s); return true;
-    case 14: dispatch_attrs_or_launch<14>(attrs, p, s); return true;
-    case 16: dispatch_attrs_or_launch<16>(attrs, p, s); return true;
-    case 32: dispatch_attrs_or_launch<32>(attrs, p, s); return true;
-    case 64: dispatch_attrs_or_launch<64>(attrs, p, s); return true;
+    case 4: dispatch_attrs_or_launch<4>(attrs, p, host_tab, s); return true;
+    case 6: dispatch_attrs_or_launch<6>(attrs, p, host_tab, s); return true;
+    case 8: dispatch_attrs_or_launch<8>(attrs, p, host_tab, s); return true;
+    case 10: dispatch_attrs_or_launch<10>(attrs, p, host_tab, s); return true;
+    case 12: dispatch_attrs_or_launch<12>(attrs, p, host_tab, s); return true;
+    case 14: dispatch_attrs_or_launch<14>(attrs, p, host_tab, s); return true;
+    case 16: dispatch_attrs_or_launch<16>(attrs, p, host_tab, s); return true;
+    case 32: dispatch_attrs_or_launch<32>(attrs, p, host_tab, s); return true;
+    case 64: dispatch_attrs_or_launch<64>(attrs, p, host_tab, s); return true;
   }
   return false;
 }
@@ -194,7 +194,7 @@ dsp_status dsp_flux_bands_solve_noalloc(const dsp_flux_batch* batch_in, const ds
       g_scratch_ptr[dev] = ptr;
     }
     if (!g_attr_done[dev]) {
-      for (int sN : kSupported) run_for(sN, true, nullptr, nullptr);
+      for (int sN : kSupported) run_for(sN, true, nullptr, nullptr, nullptr);
       g_attr_done[dev] = true;
     }
     base = static_cast<unsigned char*>(g_scratch_ptr[dev]);
@@ -252,7 +252,7 @@ dsp_status dsp_flux_bands_solve_noalloc(const dsp_flux_batch* batch_in, const ds
     // statuses start at zero: in the caller's array when given, else in the scratch
     p.status = out->status ? out->status + off : d_status;
     if (cudaMemsetAsync(p.status, 0, (size_t)m * sizeof(int32_t), s) != cudaSuccess) return DSP_ERR_CUDA;
-    run_for(N, false, &p, s);
+    run_for(N, false, &p, tab.data(), s);
     if (cudaGetLastError() != cudaSuccess) return DSP_ERR_CUDA;
   }
   return DSP_OK;

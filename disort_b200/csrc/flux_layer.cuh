@@ -91,17 +91,46 @@ __host__ __device__ constexpr int tri_idx(int r, int c) {
 // 32 HS b + e w + k (w = tasks in the block), so that a warp of the
 // one-thread-per-task kernels reads or writes an element of 32 tasks in one
 // coalesced access.  Per task: flag (0 skipped, 1 primary factorisation,
-// 2 fallback), S (packed lower), the Cholesky factor L (packed lower),
-// alpha - beta and alpha + beta (row-major NN x NN, the latter only with a beam),
-// then the eigensolver's diagonal and eigenvector matrix (row-major, column j
-// the eigenvector of diagonal entry j).
+// 2 fallback), S, the Cholesky factor L, and the odd- and even-order halves
+// O, E of the phase sums (all symmetric NN x NN, packed lower; E only with a
+// beam), then the eigensolver's diagonal and eigenvector matrix (row-major,
+// column j the eigenvector of diagonal entry j).
+//   O_ij = sum_{l odd} g'_l P_l(mu_i) P_l(mu_j),  E_ij = sum_{l even} (...),
+//   alpha - beta = M^{-1} (O W - I),  alpha + beta = M^{-1} (E W - I)
+// with M = diag(mu_1..mu_NN), W = diag(w_1..w_NN): the quadrature is
+// symmetric (mu_{NN+j} = -mu_j, P_l(-mu) = (-1)^l P_l(mu)), so the sums over
+// the other hemisphere only flip the sign of the odd orders.
 template <int NN>
 struct Handoff {
   static constexpr int TRI = NN * (NN + 1) / 2;
-  static constexpr int S_FLAG = 0, S_S = 1, S_L = 1 + TRI, S_AMB = 1 + 2 * TRI, S_APB = S_AMB + NN * NN;
-  static constexpr int S_D = S_APB + NN * NN, S_V = S_D + NN;
+  static constexpr int S_FLAG = 0, S_S = 1, S_L = 1 + TRI, S_O = 1 + 2 * TRI, S_E = 1 + 3 * TRI;
+  static constexpr int S_D = 1 + 4 * TRI, S_V = S_D + NN;
   static constexpr int HS = S_V + NN * NN;
 };
+
+// Quadrature tables of an N-stream solve passed by value: kernel parameters
+// live in the constant bank, so the one-thread-per-task kernels read them as
+// uniform operands with compile-time offsets, no loads.
+template <int N>
+struct ConstTab {
+  double mu[N / 2], rmu[N / 2], wt[N / 2], dsim[N / 2], dinv[N / 2];
+  double y[N * N];  // P_l(mu_i) at [l * N + i]
+};
+
+// ConstTab from a host copy of the tab_* table layout
+template <int N>
+inline ConstTab<N> make_const_tab(const double* tab) {
+  ConstTab<N> c;
+  for (int k = 0; k < N / 2; ++k) {
+    c.mu[k] = tab[tab_mu(N) + k];
+    c.rmu[k] = 1.0 / c.mu[k];
+    c.wt[k] = tab[tab_wt(N) + k];
+    c.dsim[k] = tab[tab_dsim(N) + k];
+    c.dinv[k] = tab[tab_dinv(N) + k];
+  }
+  for (int k = 0; k < N * N; ++k) c.y[k] = tab[tab_ylm(N) + k];
+  return c;
+}
 
 // address of element e of task j in the lane-interleaved blocks
 template <int NN>
@@ -382,13 +411,9 @@ __device__ void gen_user_angles(const FluxParams& p, int i, double* sm, const do
   }
 }
 
-// STAGE 0: the whole layer task; 1: through S = L^T M L, written to the
-// hand-off (the front of a split stage).
-template <int N, bool GEN = false, int STAGE = 0>
+template <int N, bool GEN = false>
 __global__ void __launch_bounds__(LCfg<N, GEN>::CTA, LCfg<N, GEN>::MINB) flux_layer_kernel(FluxParams p) {
-  static_assert(STAGE == 0 || (!GEN && layer_split<N>()), "split layer stages are for flux solves, N 10..16");
   using C = LCfg<N, GEN>;
-  using H = Handoff<N / 2>;
   constexpr int NN = C::NN, TEAM = C::TEAM, NNP = C::NNP, NPAIR = C::NPAIR, NS = C::NS, BPT = C::BPT;
   constexpr int BPA = NPAIR;  // blocks (a, b) per column pair b
   extern __shared__ double smem[];
@@ -429,22 +454,9 @@ __global__ void __launch_bounds__(LCfg<N, GEN>::CTA, LCfg<N, GEN>::MINB) flux_la
     pml = p.pmom.row(i) + (long long)lin * p.pc;
   }
   const InstLayout& il = GEN ? il_gen : p.il;
-  // the front of a split stage marks the tasks it does not solve, for the
-  // eigensolver and the back (which skip them)
-  auto mark_skipped = [&]() {
-    if constexpr (STAGE == 1) {
-      if (t == 0) *handoff_lane<N / 2>(p.bvp_rec, (long long)p.n * p.L, task, H::S_FLAG) = 0.0;
-    }
-  };
-  if (p.status && p.status[i] == DSP_ERR_INVALID_INPUT) {
-    mark_skipped();
-    return;
-  }
+  if (p.status && p.status[i] == DSP_ERR_INVALID_INPUT) return;
   const int ncut = (int)rec[H_NCUT];
-  if (lc >= ncut) {  // layers below the absorption cut are never used
-    mark_skipped();
-    return;
-  }
+  if (lc >= ncut) return;  // layers below the absorption cut are never used
   if constexpr (GEN) {
     // modes past the instance's last one, or after its azimuthal series converged
     if (p.g.m > (int)rec[H_NAZ] || rec[H_DONE] != 0.0) return;
@@ -491,230 +503,207 @@ __global__ void __launch_bounds__(LCfg<N, GEN>::CTA, LCfg<N, GEN>::MINB) flux_la
   }
   team_sync<TEAM>();
   DSP_PHASE(0)
-  bool primary = true;
-  {
-    // ---- phase matrix, unique half (FluxSolver.cpp:466-482) ---------------
-    // thread t owns column jq = t; its Legendre column is held in registers
-    if (t < N) {
-      const int jq = t;
-      double yj[N];
-  #pragma unroll
-      for (int l = 0; l < N; ++l) yj[l] = Y[l * N + jq];
-      const double wj = wt[jq];
-      for (int iq = 0; iq < NN; ++iq) {
-        double s = 0.0;
-  #pragma unroll
-        for (int l = 0; l < N; ++l) s += (gl[l] * Y[l * N + iq]) * yj[l];
-        CC[iq * N + jq] = (s * 0.5) * wj;
-      }
-    }
-    team_sync<TEAM>();
-    DSP_PHASE(1)
-    // ---- alpha -/+ beta and the similarity transform (:485-514) ------------
-    for (int it = t; it < NN * NN; it += TEAM) {
-      const int iq = it / NN, jq = it % NN;
-      const double inv_cmu = 1.0 / mu[iq];
-      const double a = CC[iq * N + jq], b = CC[iq * N + NN + jq];
-      double amb = inv_cmu * (a - b), apb = inv_cmu * (a + b);
-      if (iq == jq) { amb -= inv_cmu; apb -= inv_cmu; }
-      AMB[iq * NS + jq] = amb;
-      APB[iq * NS + jq] = apb;
-      S0[iq * NS + jq] = dsim[iq] * apb * dinv[jq];     // A_s
-      S1[iq * NS + jq] = -dsim[iq] * amb * dinv[jq];    // -B_s
-    }
-    team_sync<TEAM>();
-    // ---- Cholesky of -B_s, else of -A_s (:521-558) -------------------------
-    primary = ws < 1.0 - 1e-12;
-    if (primary) primary = team_chol<NN, NS, TEAM>(S1, LC, misc, t);
-    if (!primary) {
-      for (int it = t; it < NN * NN; it += TEAM) {
-        const int r = it / NN, c = it % NN;
-        V[r * NS + c] = -S0[r * NS + c];
-      }
-      team_sync<TEAM>();
-      if (!team_chol<NN, NS, TEAM>(V, LC, misc, t)) {
-        // -A_s not SPD either: try the primary factorisation regardless of omega'
-        primary = team_chol<NN, NS, TEAM>(S1, LC, misc, t);
-        if (!primary) {
-          if (t == 0) set_status(p.status, i, DSP_ERR_EIGEN);
-          mark_skipped();
-          return;
-        }
-      }
-    }
-    DSP_PHASE(2)
-    // S = L^T M L with M = -A_s (primary) or -B_s (fallback); V used as scratch
-    for (int it = t; it < NN * NN; it += TEAM) {
-      const int r = it / NN, c = it % NN;
+  // ---- phase matrix, unique half (FluxSolver.cpp:466-482) ---------------
+  // thread t owns column jq = t; its Legendre column is held in registers
+  if (t < N) {
+    const int jq = t;
+    double yj[N];
+#pragma unroll
+    for (int l = 0; l < N; ++l) yj[l] = Y[l * N + jq];
+    const double wj = wt[jq];
+    for (int iq = 0; iq < NN; ++iq) {
       double s = 0.0;
-      if (primary)
-        for (int k = 0; k < NN; ++k) s += -S0[r * NS + k] * LC[k * NS + c];
-      else
-        for (int k = 0; k < NN; ++k) s += S1[r * NS + k] * LC[k * NS + c];
-      V[r * NS + c] = s;
+#pragma unroll
+      for (int l = 0; l < N; ++l) s += (gl[l] * Y[l * N + iq]) * yj[l];
+      CC[iq * N + jq] = (s * 0.5) * wj;
     }
-    team_sync<TEAM>();
-    for (int it = t; it < NN * NN; it += TEAM) {
-      const int r = it / NN, c = it % NN;
-      double s = 0.0;
-      for (int k = 0; k < NN; ++k) s += LC[k * NS + r] * V[k * NS + c];
-      S0[r * NS + c] = s;
-    }
-    team_sync<TEAM>();
   }
-  if constexpr (STAGE == 1) {
-    // ---- hand-off to the eigensolver and the back of the stage ----------
-    const long long nt = (long long)p.n * p.L;
-    const bool beam = rec[H_FBEAM] > 0.0;
+  team_sync<TEAM>();
+  DSP_PHASE(1)
+  // ---- alpha -/+ beta and the similarity transform (:485-514) ------------
+  for (int it = t; it < NN * NN; it += TEAM) {
+    const int iq = it / NN, jq = it % NN;
+    const double inv_cmu = 1.0 / mu[iq];
+    const double a = CC[iq * N + jq], b = CC[iq * N + NN + jq];
+    double amb = inv_cmu * (a - b), apb = inv_cmu * (a + b);
+    if (iq == jq) { amb -= inv_cmu; apb -= inv_cmu; }
+    AMB[iq * NS + jq] = amb;
+    APB[iq * NS + jq] = apb;
+    S0[iq * NS + jq] = dsim[iq] * apb * dinv[jq];     // A_s
+    S1[iq * NS + jq] = -dsim[iq] * amb * dinv[jq];    // -B_s
+  }
+  team_sync<TEAM>();
+  // ---- Cholesky of -B_s, else of -A_s (:521-558) -------------------------
+  bool primary = ws < 1.0 - 1e-12;
+  if (primary) primary = team_chol<NN, NS, TEAM>(S1, LC, misc, t);
+  if (!primary) {
     for (int it = t; it < NN * NN; it += TEAM) {
       const int r = it / NN, c = it % NN;
-      *handoff_lane<NN>(p.bvp_rec, nt, task, H::S_AMB + it) = AMB[r * NS + c];
-      if (beam) *handoff_lane<NN>(p.bvp_rec, nt, task, H::S_APB + it) = APB[r * NS + c];
+      V[r * NS + c] = -S0[r * NS + c];
     }
-    for (int r = 0; r < NN; ++r)
-      for (int c = t; c <= r; c += TEAM) {
-        *handoff_lane<NN>(p.bvp_rec, nt, task, H::S_L + tri_idx(r, c)) = LC[r * NS + c];
-        *handoff_lane<NN>(p.bvp_rec, nt, task, H::S_S + tri_idx(r, c)) = S0[r * NS + c];
+    team_sync<TEAM>();
+    if (!team_chol<NN, NS, TEAM>(V, LC, misc, t)) {
+      // -A_s not SPD either: try the primary factorisation regardless of omega'
+      primary = team_chol<NN, NS, TEAM>(S1, LC, misc, t);
+      if (!primary) {
+        if (t == 0) set_status(p.status, i, DSP_ERR_EIGEN);
+        return;
       }
-    if (t == 0) *handoff_lane<NN>(p.bvp_rec, nt, task, H::S_FLAG) = primary ? 1.0 : 2.0;
-    return;
+    }
   }
+  DSP_PHASE(2)
+  // S = L^T M L with M = -A_s (primary) or -B_s (fallback); V used as scratch
+  for (int it = t; it < NN * NN; it += TEAM) {
+    const int r = it / NN, c = it % NN;
+    double s = 0.0;
+    if (primary)
+      for (int k = 0; k < NN; ++k) s += -S0[r * NS + k] * LC[k * NS + c];
+    else
+      for (int k = 0; k < NN; ++k) s += S1[r * NS + k] * LC[k * NS + c];
+    V[r * NS + c] = s;
+  }
+  team_sync<TEAM>();
+  for (int it = t; it < NN * NN; it += TEAM) {
+    const int r = it / NN, c = it % NN;
+    double s = 0.0;
+    for (int k = 0; k < NN; ++k) s += LC[k * NS + r] * V[k * NS + c];
+    S0[r * NS + c] = s;
+  }
+  team_sync<TEAM>();
+  // ---- cyclic Jacobi on S (symmetrised from its lower triangle) -----------
+  for (int it = t; it < NN * NN; it += TEAM) {
+    const int r = it / NN, c = it % NN;
+    S1[r * NS + c] = (c > r) ? S0[c * NS + r] : S0[r * NS + c];
+    V[r * NS + c] = (r == c) ? 1.0 : 0.0;
+  }
+  team_sync<TEAM>();
+  DSP_PHASE(3)
+  // In place: in a round every 2x2 block of S is read and written by its owner
+  // only, and the diagonal blocks a rotation is computed from are written by
+  // their owner after it has received that rotation.
   double* const Sc = S1;
-  if constexpr (STAGE == 0) {
-    // ---- cyclic Jacobi on S (symmetrised from its lower triangle) -----------
-    for (int it = t; it < NN * NN; it += TEAM) {
-      const int r = it / NN, c = it % NN;
-      S1[r * NS + c] = (c > r) ? S0[c * NS + r] : S0[r * NS + c];
-      V[r * NS + c] = (r == c) ? 1.0 : 0.0;
-    }
-    team_sync<TEAM>();
-    DSP_PHASE(3)
-    // In place: in a round every 2x2 block of S is read and written by its owner
-    // only, and the diagonal blocks a rotation is computed from are written by
-    // their owner after it has received that rotation.
-    double* const Sn = S1;
-    for (int sweep = 0; sweep < 20; ++sweep) {
-      for (int r = 0; r < NNP - 1; ++r) {
-        // rotation of pair a is computed by thread a; each thread then needs the
-        // rotations of its block's two pairs only (blocks are assigned statically)
-        double c = 1.0, sn = 0.0, tt = 0.0;
+  double* const Sn = S1;
+  for (int sweep = 0; sweep < 20; ++sweep) {
+    for (int r = 0; r < NNP - 1; ++r) {
+      // rotation of pair a is computed by thread a; each thread then needs the
+      // rotations of its block's two pairs only (blocks are assigned statically)
+      double c = 1.0, sn = 0.0, tt = 0.0;
+      if (t < NPAIR) {
+        const int pp = rr_player<NNP>(r, t), qq = rr_player<NNP>(r, NNP - 1 - t);
+        if (pp < NN && qq < NN) {
+          jacobi_rot(Sc[pp * NS + qq], Sc[pp * NS + pp], Sc[qq * NS + qq], c, sn, tt);
+        }
+      }
+      if constexpr (TEAM > 32) {
         if (t < NPAIR) {
-          const int pp = rr_player<NNP>(r, t), qq = rr_player<NNP>(r, NNP - 1 - t);
-          if (pp < NN && qq < NN) {
-            jacobi_rot(Sc[pp * NS + qq], Sc[pp * NS + pp], Sc[qq * NS + qq], c, sn, tt);
-          }
-        }
-        if constexpr (TEAM > 32) {
-          if (t < NPAIR) {
-            rot[3 * t] = c;
-            rot[3 * t + 1] = sn;
-            rot[3 * t + 2] = tt;
-          }
-          team_sync<TEAM>();
-        }
-  #pragma unroll
-        for (int k = 0; k < BPT; ++k) {
-          const int blk = t + k * TEAM;
-          const bool act = blk < NPAIR * NPAIR;
-          const int a = act ? blk / NPAIR : 0, b = act ? blk % NPAIR : 0;  // NPAIR is a power of two or small
-          double ca, sa, ta, cb, sb;
-          if constexpr (TEAM <= 32) {
-            const unsigned m = team_mask<TEAM>();
-            ca = __shfl_sync(m, c, a, TEAM);
-            sa = __shfl_sync(m, sn, a, TEAM);
-            ta = __shfl_sync(m, tt, a, TEAM);
-            cb = __shfl_sync(m, c, b, TEAM);
-            sb = __shfl_sync(m, sn, b, TEAM);
-          } else {
-            ca = rot[3 * a]; sa = rot[3 * a + 1]; ta = rot[3 * a + 2];
-            cb = rot[3 * b]; sb = rot[3 * b + 1];
-          }
-          if (!act) continue;
-          const int pa = rr_player<NNP>(r, a), qa = rr_player<NNP>(r, NNP - 1 - a);
-          const int pb = rr_player<NNP>(r, b), qb = rr_player<NNP>(r, NNP - 1 - b);
-          const bool va = qa < NN && pa < NN, vb = qb < NN && pb < NN;
-          if (a == b) {
-            if (va) {
-              const double apq = Sc[pa * NS + qa];
-              Sn[pa * NS + pa] = Sc[pa * NS + pa] - ta * apq;
-              Sn[qa * NS + qa] = Sc[qa * NS + qa] + ta * apq;
-              const double off = (ta != 0.0) ? 0.0 : apq;
-              Sn[pa * NS + qa] = off;
-              Sn[qa * NS + pa] = off;
-            } else {
-              const int x = pa < NN ? pa : qa;
-              if (x < NN) Sn[x * NS + x] = Sc[x * NS + x];
-            }
-          } else {
-            // rows of pair a (rotated), columns of pair b (rotated); absent
-            // (padding) indices act as the identity
-            const int ri[2] = {pa, qa}, cj[2] = {pb, qb};
-            double X[2][2];
-  #pragma unroll
-            for (int u = 0; u < 2; ++u)
-  #pragma unroll
-              for (int v = 0; v < 2; ++v) {
-                const int rr = ri[u], cc = cj[v];
-                X[u][v] = (rr < NN && cc < NN) ? Sc[rr * NS + cc] : 0.0;
-              }
-            double Y2[2][2];
-            if (va) {
-  #pragma unroll
-              for (int v = 0; v < 2; ++v) {
-                Y2[0][v] = ca * X[0][v] - sa * X[1][v];
-                Y2[1][v] = sa * X[0][v] + ca * X[1][v];
-              }
-            } else {
-  #pragma unroll
-              for (int v = 0; v < 2; ++v) { Y2[0][v] = X[0][v]; Y2[1][v] = X[1][v]; }
-            }
-            double Z2[2][2];
-            if (vb) {
-  #pragma unroll
-              for (int u = 0; u < 2; ++u) {
-                Z2[u][0] = cb * Y2[u][0] - sb * Y2[u][1];
-                Z2[u][1] = sb * Y2[u][0] + cb * Y2[u][1];
-              }
-            } else {
-  #pragma unroll
-              for (int u = 0; u < 2; ++u) { Z2[u][0] = Y2[u][0]; Z2[u][1] = Y2[u][1]; }
-            }
-  #pragma unroll
-            for (int u = 0; u < 2; ++u)
-  #pragma unroll
-              for (int v = 0; v < 2; ++v) {
-                const int rr = ri[u], cc = cj[v];
-                if (rr < NN && cc < NN) Sn[rr * NS + cc] = Z2[u][v];
-              }
-          }
-          // eigenvectors V <- V J for pair b: this thread's share of the rows
-          if (vb) {
-            const int rows_per = (NN + BPA - 1) / BPA;  // blocks sharing pair b split its rows
-            const int r0 = a * rows_per;
-  #pragma unroll 4
-            for (int row = r0; row < r0 + rows_per && row < NN; ++row) {
-              const double vp = V[row * NS + pb], vq = V[row * NS + qb];
-              V[row * NS + pb] = cb * vp - sb * vq;
-              V[row * NS + qb] = sb * vp + cb * vq;
-            }
-          }
+          rot[3 * t] = c;
+          rot[3 * t + 1] = sn;
+          rot[3 * t + 2] = tt;
         }
         team_sync<TEAM>();
       }
-      // stop when a further sweep would rotate no pair (the sweep that finds
-      // nothing to do is not run)
-      if (t == 0) misc[1] = 0.0;
-      team_sync<TEAM>();
-      for (int it = t; it < NN * NN; it += TEAM) {
-        const int r = it / NN, c = it % NN;
-        if (c > r && jacobi_needed(Sc[r * NS + c], Sc[r * NS + r], Sc[c * NS + c])) misc[1] = 1.0;
+#pragma unroll
+      for (int k = 0; k < BPT; ++k) {
+        const int blk = t + k * TEAM;
+        const bool act = blk < NPAIR * NPAIR;
+        const int a = act ? blk / NPAIR : 0, b = act ? blk % NPAIR : 0;  // NPAIR is a power of two or small
+        double ca, sa, ta, cb, sb;
+        if constexpr (TEAM <= 32) {
+          const unsigned m = team_mask<TEAM>();
+          ca = __shfl_sync(m, c, a, TEAM);
+          sa = __shfl_sync(m, sn, a, TEAM);
+          ta = __shfl_sync(m, tt, a, TEAM);
+          cb = __shfl_sync(m, c, b, TEAM);
+          sb = __shfl_sync(m, sn, b, TEAM);
+        } else {
+          ca = rot[3 * a]; sa = rot[3 * a + 1]; ta = rot[3 * a + 2];
+          cb = rot[3 * b]; sb = rot[3 * b + 1];
+        }
+        if (!act) continue;
+        const int pa = rr_player<NNP>(r, a), qa = rr_player<NNP>(r, NNP - 1 - a);
+        const int pb = rr_player<NNP>(r, b), qb = rr_player<NNP>(r, NNP - 1 - b);
+        const bool va = qa < NN && pa < NN, vb = qb < NN && pb < NN;
+        if (a == b) {
+          if (va) {
+            const double apq = Sc[pa * NS + qa];
+            Sn[pa * NS + pa] = Sc[pa * NS + pa] - ta * apq;
+            Sn[qa * NS + qa] = Sc[qa * NS + qa] + ta * apq;
+            const double off = (ta != 0.0) ? 0.0 : apq;
+            Sn[pa * NS + qa] = off;
+            Sn[qa * NS + pa] = off;
+          } else {
+            const int x = pa < NN ? pa : qa;
+            if (x < NN) Sn[x * NS + x] = Sc[x * NS + x];
+          }
+        } else {
+          // rows of pair a (rotated), columns of pair b (rotated); absent
+          // (padding) indices act as the identity
+          const int ri[2] = {pa, qa}, cj[2] = {pb, qb};
+          double X[2][2];
+#pragma unroll
+          for (int u = 0; u < 2; ++u)
+#pragma unroll
+            for (int v = 0; v < 2; ++v) {
+              const int rr = ri[u], cc = cj[v];
+              X[u][v] = (rr < NN && cc < NN) ? Sc[rr * NS + cc] : 0.0;
+            }
+          double Y2[2][2];
+          if (va) {
+#pragma unroll
+            for (int v = 0; v < 2; ++v) {
+              Y2[0][v] = ca * X[0][v] - sa * X[1][v];
+              Y2[1][v] = sa * X[0][v] + ca * X[1][v];
+            }
+          } else {
+#pragma unroll
+            for (int v = 0; v < 2; ++v) { Y2[0][v] = X[0][v]; Y2[1][v] = X[1][v]; }
+          }
+          double Z2[2][2];
+          if (vb) {
+#pragma unroll
+            for (int u = 0; u < 2; ++u) {
+              Z2[u][0] = cb * Y2[u][0] - sb * Y2[u][1];
+              Z2[u][1] = sb * Y2[u][0] + cb * Y2[u][1];
+            }
+          } else {
+#pragma unroll
+            for (int u = 0; u < 2; ++u) { Z2[u][0] = Y2[u][0]; Z2[u][1] = Y2[u][1]; }
+          }
+#pragma unroll
+          for (int u = 0; u < 2; ++u)
+#pragma unroll
+            for (int v = 0; v < 2; ++v) {
+              const int rr = ri[u], cc = cj[v];
+              if (rr < NN && cc < NN) Sn[rr * NS + cc] = Z2[u][v];
+            }
+        }
+        // eigenvectors V <- V J for pair b: this thread's share of the rows
+        if (vb) {
+          const int rows_per = (NN + BPA - 1) / BPA;  // blocks sharing pair b split its rows
+          const int r0 = a * rows_per;
+#pragma unroll 4
+          for (int row = r0; row < r0 + rows_per && row < NN; ++row) {
+            const double vp = V[row * NS + pb], vq = V[row * NS + qb];
+            V[row * NS + pb] = cb * vp - sb * vq;
+            V[row * NS + qb] = sb * vp + cb * vq;
+          }
+        }
       }
       team_sync<TEAM>();
-      const bool more = misc[1] != 0.0;
-      team_sync<TEAM>();
-      DSP_PHASE(6)
-      if (!more) break;
     }
+    // stop when a further sweep would rotate no pair (the sweep that finds
+    // nothing to do is not run)
+    if (t == 0) misc[1] = 0.0;
+    team_sync<TEAM>();
+    for (int it = t; it < NN * NN; it += TEAM) {
+      const int r = it / NN, c = it % NN;
+      if (c > r && jacobi_needed(Sc[r * NS + c], Sc[r * NS + r], Sc[c * NS + c])) misc[1] = 1.0;
+    }
+    team_sync<TEAM>();
+    const bool more = misc[1] != 0.0;
+    team_sync<TEAM>();
+    DSP_PHASE(6)
+    if (!more) break;
   }
   DSP_PHASE(4)
   // ---- sort ascending; eigenvectors of (a+b)(a-b) ------------------------
@@ -941,6 +930,157 @@ __device__ __forceinline__ void jacobi_rot_rsq(double apq, double app, double aq
   tt = rot ? sv * g : 0.0;
 }
 
+// ---------------------------------------------------------------------------
+// Front of a split layer stage, one thread per layer task (the STAGE before the
+// eigensolver): scaled phase coefficients (disortSet, FluxSolver.cpp:336-386),
+// the phase sums, alpha -/+ beta in the symmetric form of the reference
+// (FluxSolver.cpp:466-514), the Cholesky factorisation of -B_s, else of -A_s
+// (:521-558), and S = L^T M L, written to the hand-off.  Every matrix is a
+// packed symmetric NN x NN in registers; the tables are constant-bank operands.
+// ---------------------------------------------------------------------------
+// Cholesky of a packed lower triangle in place; false when a pivot is not
+// positive (the factor is then not used).  The updates are subtracted in the
+// order of the right-looking form and the column is divided by its pivot, as
+// the reference's LLT does: at omega' = 1 one pivot is rounding noise around
+// zero, and the factor's other entries should carry the same rounding.
+template <int NN>
+__device__ __forceinline__ bool chol_packed(double* A) {
+  bool ok = true;
+#pragma unroll
+  for (int j = 0; j < NN; ++j) {
+    double s = A[tri_idx(j, j)];
+#pragma unroll
+    for (int k = 0; k < j; ++k) s -= A[tri_idx(j, k)] * A[tri_idx(j, k)];
+    ok = ok && s > 0.0;
+    const double ljj = sqrt(ok ? s : 1.0);
+    A[tri_idx(j, j)] = ljj;
+#pragma unroll
+    for (int i = j + 1; i < NN; ++i) {
+      double t = A[tri_idx(i, j)];
+#pragma unroll
+      for (int k = 0; k < j; ++k) t -= A[tri_idx(i, k)] * A[tri_idx(j, k)];
+      A[tri_idx(i, j)] = t / ljj;
+    }
+  }
+  return ok;
+}
+
+template <int N>
+__global__ void __launch_bounds__(128) flux_layer_front_kernel(FluxParams p, ConstTab<N> tc) {
+  constexpr int NN = N / 2;
+  using H = Handoff<NN>;
+  constexpr int TRI = H::TRI;
+  const long long nt = (long long)p.n * p.L;
+  const long long j = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (j >= nt) return;
+  auto hp = [&](int e) { return handoff_lane<NN>(p.bvp_rec, nt, j, e); };
+  const int i = (int)(j / p.L), lc = (int)(j % p.L);
+  const double* rec = p.inst_rec + (long long)i * p.il.stride;
+  const InstLayout& il = p.il;
+  // invalid instances and layers below the absorption cut are not solved
+  if ((p.status && p.status[i] == DSP_ERR_INVALID_INPUT) || lc >= (int)rec[H_NCUT]) {
+    *hp(H::S_FLAG) = 0.0;
+    return;
+  }
+  const double ws = rec[il.ssa_s + lc];
+  const bool beam = rec[H_FBEAM] > 0.0;
+  // ---- phase sums O (odd orders) and E (even orders) ----------------------
+  double O[TRI], E[TRI];
+  {
+    const int lin = (p.flags & DSP_FLAG_INDEX_FROM_BOTTOM) ? p.L - 1 - lc : lc;
+    const double* pml = p.pmom.row(i) + (long long)lin * p.pc;
+    const int mode = (int)rec[il.mode + lc];
+    const double f = rec[il.fsc + lc], sig = rec[il.sig + lc];
+    double gl[N];
+#pragma unroll
+    for (int k = 0; k < N; ++k) {
+      const double pk = pml[k];
+      double g;
+      if (mode == 0) g = (2.0 * k + 1.0) * ws * pk;
+      else if (mode == 1) g = (2.0 * k + 1.0) * ws * (pk - f) / (1.0 - f);
+      else {
+        const double kd = (double)k;
+        g = (2.0 * k + 1.0) * ws * (pk - f * exp(-kd * kd / (2.0 * sig))) / (1.0 - f);
+      }
+      gl[k] = g;
+    }
+#pragma unroll
+    for (int a = 0; a < NN; ++a) {
+      double z[N];
+#pragma unroll
+      for (int l = 0; l < N; ++l) z[l] = gl[l] * tc.y[l * N + a];
+#pragma unroll
+      for (int b = 0; b <= a; ++b) {
+        double se = 0.0, so = 0.0;
+#pragma unroll
+        for (int l = 0; l < N; l += 2) se += z[l] * tc.y[l * N + b];
+#pragma unroll
+        for (int l = 1; l < N; l += 2) so += z[l] * tc.y[l * N + b];
+        E[tri_idx(a, b)] = se;
+        O[tri_idx(a, b)] = so;
+      }
+    }
+  }
+#pragma unroll
+  for (int e = 0; e < TRI; ++e) {
+    *hp(H::S_O + e) = O[e];
+    if (beam) *hp(H::S_E + e) = E[e];
+  }
+  // -B_s = -D (a-b) D^{-1} and -A_s = -D (a+b) D^{-1} (packed lower; both symmetric)
+  auto minus_s = [&](const double* P, double* X) {
+#pragma unroll
+    for (int r = 0; r < NN; ++r)
+#pragma unroll
+      for (int c = 0; c <= r; ++c) {
+        const double a = (tc.wt[c] * P[tri_idx(r, c)]) * tc.rmu[r] - (r == c ? tc.rmu[r] : 0.0);
+        X[tri_idx(r, c)] = -tc.dsim[r] * a * tc.dinv[c];
+      }
+  };
+  // ---- Cholesky of -B_s, else of -A_s, else of -B_s regardless of omega' --
+  double Lf[TRI];
+  bool primary = ws < 1.0 - 1e-12;
+  if (primary) {
+    minus_s(O, Lf);
+    primary = chol_packed<NN>(Lf);
+  }
+  if (!primary) {
+    minus_s(E, Lf);
+    if (!chol_packed<NN>(Lf)) {
+      minus_s(O, Lf);
+      primary = chol_packed<NN>(Lf);
+      if (!primary) {
+        set_status(p.status, i, DSP_ERR_EIGEN);
+        *hp(H::S_FLAG) = 0.0;
+        return;
+      }
+    }
+  }
+  // ---- S = L^T M L, M = -A_s (primary) or -B_s (fallback), by columns ----
+  double M[TRI];
+  minus_s(primary ? E : O, M);
+#pragma unroll
+  for (int c = 0; c < NN; ++c) {
+    double t[NN];  // (M L)[:, c]; L[k][c] = 0 for k < c
+#pragma unroll
+    for (int r = 0; r < NN; ++r) {
+      double s = 0.0;
+#pragma unroll
+      for (int k = c; k < NN; ++k) s += M[tri_idx(r, k)] * Lf[tri_idx(k, c)];
+      t[r] = s;
+    }
+#pragma unroll
+    for (int r = c; r < NN; ++r) {
+      double s = 0.0;
+#pragma unroll
+      for (int k = r; k < NN; ++k) s += Lf[tri_idx(k, r)] * t[k];
+      *hp(H::S_S + tri_idx(r, c)) = s;
+    }
+  }
+#pragma unroll
+  for (int e = 0; e < TRI; ++e) *hp(H::S_L + e) = Lf[e];
+  *hp(H::S_FLAG) = primary ? 1.0 : 2.0;
+}
+
 // Rotation of the pair (p, q) applied to S (packed lower, both sides) and to the
 // columns p, q of V; the same update as the team form's 2x2 blocks:
 // column p' = c col p - s col q, column q' = s col p + c col q, and on the
@@ -1096,7 +1236,7 @@ __device__ __forceinline__ void warp_flush_rows(const double* stg, double* rec0,
 }
 
 template <int N>
-__global__ void __launch_bounds__(128) flux_layer_back_kernel(FluxParams p) {
+__global__ void __launch_bounds__(128) flux_layer_back_kernel(FluxParams p, ConstTab<N> tc) {
   constexpr int NN = N / 2;
   constexpr int RS = N + 3;  // staging row stride: a row of N (+2 for xr after z1)
   constexpr int LS = lrec_stride(N);
@@ -1124,9 +1264,6 @@ __global__ void __launch_bounds__(128) flux_layer_back_kernel(FluxParams p) {
   const int i = (int)(jj / p.L), lc = (int)(jj % p.L);
   const double* rec = p.inst_rec + (long long)i * p.il.stride;
   const InstLayout& il = p.il;
-  const double* mu = p.tables + tab_mu(N);
-  const double* dsim = p.tables + tab_dsim(N);
-  const double* dinv = p.tables + tab_dinv(N);
   double* const rec0 = p.layer_rec + j0 * LS;
 
   // ---- ascending order of the eigenvalues; k = sqrt|lambda| ----------------
@@ -1169,14 +1306,18 @@ __global__ void __launch_bounds__(128) flux_layer_back_kernel(FluxParams p) {
       if (primary) ops.bwd(EV[c]);
       else ops.lmul(EV[c]);
 #pragma unroll
-      for (int r = 0; r < NN; ++r) EV[c][r] *= dinv[r];
+      for (int r = 0; r < NN; ++r) EV[c][r] *= tc.dinv[r];
     }
     // ---- G+/- (FluxSolver.cpp:575-587), two rows per step -------------------
 #pragma unroll 1
     for (int iq = 0; iq < NN; ++iq) {
-      double arow[NN];
+      // row iq of alpha - beta = M^{-1} (O W - I)
+      double rm = 0.0, arow[NN];
 #pragma unroll
-      for (int k = 0; k < NN; ++k) arow[k] = hv(H::S_AMB + iq * NN + k);
+      for (int k = 0; k < NN; ++k) rm = (k == iq) ? tc.rmu[k] : rm;
+#pragma unroll
+      for (int k = 0; k < NN; ++k)
+        arow[k] = (tc.wt[k] * hv(H::S_O + tri_idx(iq, k))) * rm - (k == iq ? rm : 0.0);
       double* g0 = sA;  // row NN + iq
       double* g1 = sB;  // row NN - iq - 1
 #pragma unroll
@@ -1256,7 +1397,6 @@ __global__ void __launch_bounds__(128) flux_layer_back_kernel(FluxParams p) {
     const int mode = (int)rec[il.mode + lc];
     const double f = rec[il.fsc + lc], sig = rec[il.sig + lc];
     const double* yb = rec + il.yb;
-    const double* Y = p.tables + tab_ylm(N);
     double sp[NN], sm[NN];
 #pragma unroll
     for (int r = 0; r < NN; ++r) sp[r] = sm[r] = 0.0;
@@ -1273,24 +1413,25 @@ __global__ void __launch_bounds__(128) flux_layer_back_kernel(FluxParams p) {
       const double gy = g * yb[k];
 #pragma unroll
       for (int r = 0; r < NN; ++r) {
-        sp[r] += gy * Y[k * N + r];
-        sm[r] += gy * Y[k * N + NN + r];
+        sp[r] += gy * tc.y[k * N + r];
+        sm[r] += gy * tc.y[k * N + NN + r];
       }
     }
     double m1[NN], y[NN];
 #pragma unroll
     for (int r = 0; r < NN; ++r) {
       const double bp = fbeam * sp[r] / (4.0 * PI), bm = fbeam * sm[r] / (4.0 * PI);
-      m1[r] = (bp + bm) / mu[r];
-      y[r] = (bp - bm) / mu[r];  // M^{-1} r2
+      m1[r] = (bp + bm) * tc.rmu[r];
+      y[r] = (bp - bm) * tc.rmu[r];  // M^{-1} r2
     }
     // rhs = mu0^{-1} M^{-1} r2 + (a-b) M^{-1} r1, then D rhs
 #pragma unroll
     for (int r = 0; r < NN; ++r) {
       double s = 0.0;
 #pragma unroll
-      for (int k = 0; k < NN; ++k) s += hv(H::S_AMB + r * NN + k) * m1[k];
-      y[r] = dsim[r] * (y[r] / beam_mu + s);
+      for (int k = 0; k < NN; ++k)
+        s += ((tc.wt[k] * hv(H::S_O + tri_idx(r, k))) * tc.rmu[r] - (k == r ? tc.rmu[r] : 0.0)) * m1[k];
+      y[r] = tc.dsim[r] * (y[r] / beam_mu + s);
     }
     // s = -(D^{-1} (B_s A_s - mu0^{-2})^{-1} D) rhs
     const double shift = 1.0 / (beam_mu * beam_mu);
@@ -1304,13 +1445,14 @@ __global__ void __launch_bounds__(128) flux_layer_back_kernel(FluxParams p) {
       ops.bwd(y);
     }
 #pragma unroll
-    for (int r = 0; r < NN; ++r) y[r] = -dinv[r] * y[r];
+    for (int r = 0; r < NN; ++r) y[r] = -tc.dinv[r] * y[r];
     // d = mu0 ((a+b) s + M^{-1} r1)
 #pragma unroll
     for (int r = 0; r < NN; ++r) {
       double s = 0.0;
 #pragma unroll
-      for (int k = 0; k < NN; ++k) s += hv(H::S_APB + r * NN + k) * y[k];
+      for (int k = 0; k < NN; ++k)
+        s += ((tc.wt[k] * hv(H::S_E + tri_idx(r, k))) * tc.rmu[r] - (k == r ? tc.rmu[r] : 0.0)) * y[k];
       const double dv = beam_mu * (s + m1[r]);
       sA[NN + r] = 0.5 * (y[r] + dv);
       sA[NN - r - 1] = 0.5 * (y[r] - dv);
@@ -1330,17 +1472,17 @@ __global__ void __launch_bounds__(128) flux_layer_back_kernel(FluxParams p) {
     double u[NN], dd[NN];
     // u = -(a+b)^{-1} M^{-1} 1 with (a+b)^{-1} y = D^{-1} X D y (X2 primary, X1 fallback)
 #pragma unroll
-    for (int r = 0; r < NN; ++r) u[r] = dsim[r] * (1.0 / mu[r]);
+    for (int r = 0; r < NN; ++r) u[r] = tc.dsim[r] * tc.rmu[r];
     if (src) {
       if (primary) applyX2(u);
       else applyX1(u);
     }
 #pragma unroll
-    for (int r = 0; r < NN; ++r) u[r] = src ? -dinv[r] * u[r] : 0.0;
+    for (int r = 0; r < NN; ++r) u[r] = src ? -tc.dinv[r] * u[r] : 0.0;
     const double c1 = 2.0 * (1.0 - ws) * xr1, c0 = 2.0 * (1.0 - ws) * xr0;
     // d0 = -(a-b)^{-1} s1 with (a-b)^{-1} y = D^{-1} X D y (X1 primary, X2 fallback)
 #pragma unroll
-    for (int r = 0; r < NN; ++r) dd[r] = dsim[r] * (c1 * u[r]);
+    for (int r = 0; r < NN; ++r) dd[r] = tc.dsim[r] * (c1 * u[r]);
     if (src) {
       if (primary) applyX1(dd);
       else applyX2(dd);
@@ -1348,7 +1490,7 @@ __global__ void __launch_bounds__(128) flux_layer_back_kernel(FluxParams p) {
 #pragma unroll
     for (int r = 0; r < NN; ++r) {
       const double s1 = c1 * u[r], s0 = c0 * u[r];
-      const double d0 = src ? -dinv[r] * dd[r] : 0.0;
+      const double d0 = src ? -tc.dinv[r] * dd[r] : 0.0;
       sB[NN + r] = 0.5 * s1;
       sB[NN - r - 1] = 0.5 * s1;
       sA[NN + r] = 0.5 * (s0 + d0);
@@ -1362,14 +1504,13 @@ __global__ void __launch_bounds__(128) flux_layer_back_kernel(FluxParams p) {
 }
 
 // Host side of the layer stage: launches (through `wrap(name, launch)`, which
-// may time them) one layer kernel, or the three launches of a split stage.
+// may time them) one layer kernel, or the three launches of a split stage;
+// `host_tab` is a host copy of the tab_* tables of N.
 template <int N>
 inline void flux_layer_set_attrs() {
   using C = LCfg<N>;
   if constexpr (layer_split<N>()) {
     static_assert(Handoff<N / 2>::HS <= brec_stride(N), "the hand-off must fit in the boundary-value records");
-    cudaFuncSetAttribute(flux_layer_kernel<N, false, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                         (int)C::smem_bytes());
   } else {
     cudaFuncSetAttribute(flux_layer_kernel<N>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                          (int)C::smem_bytes());
@@ -1377,19 +1518,18 @@ inline void flux_layer_set_attrs() {
 }
 
 template <int N, class Wrap>
-inline void flux_layer_launch(const FluxParams& p, cudaStream_t s, Wrap&& wrap) {
+inline void flux_layer_launch(const FluxParams& p, const double* host_tab, cudaStream_t s, Wrap&& wrap) {
   using C = LCfg<N>;
   const long long tasks = (long long)p.n * p.L;
-  const unsigned grid = (unsigned)((tasks + C::TPC - 1) / C::TPC);
-  const size_t sm = C::smem_bytes();
   if constexpr (layer_split<N>()) {
-    wrap("flux_layer_kernel", [&] { flux_layer_kernel<N, false, 1><<<grid, C::CTA, sm, s>>>(p); });
-    wrap("flux_jacobi_kernel",
-         [&] { flux_jacobi_kernel<N / 2><<<(unsigned)((tasks + 127) / 128), 128, 0, s>>>(p); });
-    wrap("flux_layer_kernel",
-         [&] { flux_layer_back_kernel<N><<<(unsigned)((tasks + 127) / 128), 128, 0, s>>>(p); });
+    const ConstTab<N> tc = make_const_tab<N>(host_tab);
+    const unsigned g = (unsigned)((tasks + 127) / 128);
+    wrap("flux_layer_kernel", [&] { flux_layer_front_kernel<N><<<g, 128, 0, s>>>(p, tc); });
+    wrap("flux_jacobi_kernel", [&] { flux_jacobi_kernel<N / 2><<<g, 128, 0, s>>>(p); });
+    wrap("flux_layer_kernel", [&] { flux_layer_back_kernel<N><<<g, 128, 0, s>>>(p, tc); });
   } else {
-    wrap("flux_layer_kernel", [&] { flux_layer_kernel<N><<<grid, C::CTA, sm, s>>>(p); });
+    const unsigned grid = (unsigned)((tasks + C::TPC - 1) / C::TPC);
+    wrap("flux_layer_kernel", [&] { flux_layer_kernel<N><<<grid, C::CTA, C::smem_bytes(), s>>>(p); });
   }
 }
 
