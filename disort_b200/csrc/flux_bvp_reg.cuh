@@ -288,12 +288,9 @@ __global__ void __launch_bounds__(RCfg<N>::CTA, RCfg<N>::MINB) flux_bvp_reg_kern
         rhs = sum;
       }
     }
-    unsigned newm = 0u;
-#pragma unroll
-    for (int s = 0; s < PR; ++s) {
-      const int rk = __popc(freem & ((1u << s) - 1u));
-      if (((freem >> s) & 1u) && rk < nnew) newm |= 1u << s;
-    }
+    // slots receiving a new row: this team's bits of the ballot of `fresh`
+    const unsigned newm = (__ballot_sync(msk, fresh) >> (threadIdx.x & 31u & ~(unsigned)(TEAM - 1))) &
+                          (TEAM == 32 ? 0xffffffffu : ((1u << TEAM) - 1u));
     unsigned cand = carried | newm;
     DSP_PHASE(20)
 
@@ -389,18 +386,26 @@ __global__ void __launch_bounds__(RCfg<N>::CTA, RCfg<N>::MINB) flux_bvp_reg_kern
 
   // ----------------------------------------------------------------- backward
   bool nonfinite = false;
+  const double rumu0 = beam ? 1.0 / umu0 : 0.0;
+  auto ssa_of = [&](int l) {
+    const int lin = ifb ? L - 1 - l : l;
+    return GEN ? p.g.ssa[p.g.in_off[i] + lin] : p.ssa(i, lin);
+  };
   // fluxes at output level lu of layer l (computeFluxes, FluxSolver.cpp:1138-1287;
   // DisortSolver.cpp:1980-2124): utaupr scaled depth, utau unscaled depth
-  auto eval_level = [&](int l, const double* x, int lu, double utaupr, double utau) {
+  // tau_top, tau_bot: scaled depths of the layer's top and bottom; w0: its
+  // single-scattering albedo (loaded ahead by the caller)
+  auto eval_level = [&](int l, const double* x, int lu, double utaupr, double utau, double tau_top,
+                        double tau_bot, double w0) {
     const double* lr = RB(l);
     const double* eig = lr + lrec_eig(N);
     const double* Gl = lr + lrec_G(N);
     if (t < N) {
-      const double d = (t < NN) ? (utaupr - taus[l + 1]) : (utaupr - taus[l]);
+      const double d = (t < NN) ? (utaupr - tau_bot) : (utaupr - tau_top);
       ec[t] = x[t] * exp(-eig[t] * d);
     }
     __syncwarp(msk);
-    const double fact = beam ? exp(-utaupr / umu0) : 0.0;
+    const double fact = beam ? exp(-utaupr * rumu0) : 0.0;
     if (t < N) {
       double s = 0.0;
 #pragma unroll
@@ -415,7 +420,7 @@ __global__ void __launch_bounds__(RCfg<N>::CTA, RCfg<N>::MINB) flux_bvp_reg_kern
       if (beam) {
         dirint = fbeam * fact;
         fldir = umu0 * fbeam * fact;
-        fdir = umu0 * fbeam * exp(-utau / umu0);
+        fdir = umu0 * fbeam * exp(-utau * rumu0);
       }
       double iv[N];
 #pragma unroll
@@ -438,14 +443,13 @@ __global__ void __launch_bounds__(RCfg<N>::CTA, RCfg<N>::MINB) flux_bvp_reg_kern
       fup *= 2.0 * PI;
       fldn *= 2.0 * PI;
       const double fdn = (fldn + fldir) - fdir;
-      ua = (2.0 * PI * ua + dirint) / (4.0 * PI);
-      const double uaso = dirint / (4.0 * PI);
-      uad = (2.0 * PI * uad) / (4.0 * PI);
-      uau = (2.0 * PI * uau) / (4.0 * PI);
+      constexpr double R4PI = 1.0 / (4.0 * PI);
+      ua = (2.0 * PI * ua + dirint) * R4PI;
+      const double uaso = dirint * R4PI;
+      uad = (2.0 * PI * uad) * R4PI;
+      uau = (2.0 * PI * uau) * R4PI;
       double plsorc = 0.0;
       if (thermal) plsorc = lr[lrec_xr(N)] + lr[lrec_xr(N) + 1] * utaupr;
-      const int lin = ifb ? L - 1 - l : l;
-      const double w0 = GEN ? p.g.ssa[p.g.in_off[i] + lin] : p.ssa(i, lin);
       const double dfdt = (1.0 - w0) * 4.0 * PI * (ua - plsorc);
       const double o[8] = {fdir, fdn, fup, dfdt, ua, uad, uau, uaso};
 #pragma unroll
@@ -471,7 +475,12 @@ __global__ void __launch_bounds__(RCfg<N>::CTA, RCfg<N>::MINB) flux_bvp_reg_kern
   }
   team_copy_async<TEAM>(RB(ncut - 1), LR(ncut - 1), RS, t);
   cp_async_commit();
+  // per-layer scalars of layer l, loaded one layer ahead
+  double tau_top = taus[ncut - 1], tau_bot = taus[ncut], tauc_bot = GEN ? 0.0 : rec[il.tauc + ncut];
+  double w0 = ssa_of(ncut - 1);
   for (int l = ncut - 1; l >= 0; --l) {
+    const double tau_top_n = l > 0 ? taus[l - 1] : 0.0, w0_n = l > 0 ? ssa_of(l - 1) : 0.0;
+    const double tauc_top = GEN ? 0.0 : rec[il.tauc + l];
     cp_async_wait<0>();
     __syncwarp(msk);
     double* x = XV + (l & 1) * N;
@@ -506,11 +515,15 @@ __global__ void __launch_bounds__(RCfg<N>::CTA, RCfg<N>::MINB) flux_bvp_reg_kern
       if (t < N) cc0[(long long)l * N + t] = x[t];
       if (m == 0)
         for (int lu = 0; lu < NT; ++lu)
-          if ((int)lyr_l[lu] == l) eval_level(l, x, lu, utaus_l[lu], utau_l[lu]);
+          if ((int)lyr_l[lu] == l) eval_level(l, x, lu, utaus_l[lu], utau_l[lu], tau_top, tau_bot, w0);
     } else {
-      eval_level(l, x, l + 1, taus[l + 1], rec[il.tauc + l + 1]);
-      if (l == 0) eval_level(0, x, 0, taus[0], rec[il.tauc]);
+      eval_level(l, x, l + 1, tau_bot, tauc_bot, tau_top, tau_bot, w0);
+      if (l == 0) eval_level(0, x, 0, tau_top, tauc_top, tau_top, tau_bot, w0);
     }
+    tau_bot = tau_top;
+    tau_top = tau_top_n;
+    tauc_bot = tauc_top;
+    w0 = w0_n;
     DSP_PHASE(23)
   }
   if (nonfinite && t == 0) set_status(p.status, i, DSP_ERR_NONFINITE);
