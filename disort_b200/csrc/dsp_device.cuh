@@ -13,6 +13,9 @@
 #ifndef DSP_PHASE
 #define DSP_PHASE(k)
 #endif
+#ifndef DSP_PHASE_END
+#define DSP_PHASE_END
+#endif
 
 namespace dsp {
 
@@ -269,6 +272,31 @@ __device__ __forceinline__ void team_copy_async(double* dst, const double* src, 
       asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(s0 + 16u * k), "l"(src + 2 * k) : "memory");
   } else {
     for (int k = t; k < nd; k += TEAM) dst[k] = src[k];
+  }
+}
+// Team copy of `rows` rows of `cols` doubles (cols even) from global memory
+// (row stride sstride) into shared memory (row stride dstride), 16-byte cp.async
+// chunks when both layouts keep every chunk 16-byte aligned, plain loads and
+// stores otherwise; waited for like team_copy_async.
+template <int TEAM>
+__device__ __forceinline__ void team_copy_rows_async(double* dst, int dstride, const double* src, int sstride,
+                                                     int rows, int cols, int t) {
+  const bool al = ((reinterpret_cast<uintptr_t>(dst) | reinterpret_cast<uintptr_t>(src)) & 15u) == 0 &&
+                  ((dstride | sstride | cols) & 1) == 0;
+  const int cpr = cols / 2;
+  if (al) {
+    const unsigned s0 = static_cast<unsigned>(__cvta_generic_to_shared(dst));
+    for (int k = t; k < rows * cpr; k += TEAM) {
+      const int r = k / cpr, c2 = k - r * cpr;
+      asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(s0 + 8u * (unsigned)(r * dstride + 2 * c2)),
+                   "l"(src + (long long)r * sstride + 2 * c2)
+                   : "memory");
+    }
+  } else {
+    for (int k = t; k < rows * cols; k += TEAM) {
+      const int r = k / cols, c = k - r * cols;
+      dst[r * dstride + c] = src[(long long)r * sstride + c];
+    }
   }
 }
 __device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }

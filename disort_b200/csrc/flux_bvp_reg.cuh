@@ -52,9 +52,17 @@ struct RCfg {
   static constexpr int RS = lrec_stride(N);
   static constexpr int BS = brec_stride(N);
   static constexpr int RL = 2 * N + 2;  // record row: U[N] | V[N] | c | 1/pivot
+  // A layer record in the ring keeps its layout except that the rows of G are
+  // GS doubles apart: GS = 2 mod 4 (and even, for the 16-byte copies), so that
+  // lanes reading one row each of G hit different shared-memory banks (row
+  // stride N would put them all on one bank).
+  static constexpr int GS = (N + 2) % 4 == 2 ? N + 2 : N + 4;
+  static constexpr int SEIG = N * GS, SZB = SEIG + N, SZ0 = SZB + N, SZ1 = SZ0 + N, SXR = SZ1 + N;
+  static constexpr int RSP = round4(SXR + 2);
+  static_assert(RS - N * N == round4(N * N + 4 * N + 2) - N * N, "layer record: G then eig, zb, z0, z1, xr");
   static constexpr int O_RING = round4(O_PIV + N / 2 + 1);
   // going down: 3 layer records; going up: 2 layer records and 1 elimination record
-  static constexpr int RING = imax(3 * RS, 2 * RS + BS);
+  static constexpr int RING = imax(3 * RSP, 2 * RSP + BS);
   static constexpr int TEAM_SMEM = round4(O_RING + RING);
   static constexpr int TAB = 2 * N;  // mu and wt of the constant tables
   // register budget per thread: 128 keeps 16 single-warp CTAs resident per SM
@@ -151,9 +159,15 @@ __global__ void __launch_bounds__(RCfg<N>::CTA, RCfg<N>::MINB) flux_bvp_reg_kern
   int* pivslot = reinterpret_cast<int*>(sm + C::O_PIV);
   constexpr int RS = C::RS, BS = C::BS;
   double* ring = sm + C::O_RING;
-  auto RF = [&](int l) { return ring + (l % 3) * RS; };        // going down: layer l's record
-  auto RB = [&](int l) { return ring + (l & 1) * RS; };  // going up: layer records
-  double* const EB = ring + 2 * RS;                        // going up: the elimination record
+  constexpr int RSP = C::RSP, GS = C::GS;
+  auto RF = [&](int l) { return ring + (l % 3) * RSP; };  // going down: layer l's record
+  auto RB = [&](int l) { return ring + (l & 1) * RSP; };  // going up: layer records
+  double* const EB = ring + 2 * RSP;                      // going up: the elimination record
+  // a layer record into a ring slot, G's rows GS apart
+  auto copy_lrec = [&](double* dst, const double* src) {
+    team_copy_rows_async<TEAM>(dst, GS, src, N, N, N, t);
+    team_copy_async<TEAM>(dst + C::SEIG, src + N * N, RS - N * N, t);
+  };
 
   double cur[N], nxt[N], rhs = 0.0;
 #pragma unroll
@@ -161,13 +175,13 @@ __global__ void __launch_bounds__(RCfg<N>::CTA, RCfg<N>::MINB) flux_bvp_reg_kern
   bool singular = false;
 
   // ------------------------------------------------------------------ forward
-  team_copy_async<TEAM>(RF(0), LR(0), RS, t);
+  copy_lrec(RF(0), LR(0));
   cp_async_commit();
-  if (ncut > 1) team_copy_async<TEAM>(RF(1), LR(1), RS, t);
+  if (ncut > 1) copy_lrec(RF(1), LR(1));
   cp_async_commit();
   cp_async_wait<1>();
   __syncwarp(msk);
-  if (t < NN) E[t] = exp(RF(0)[lrec_eig(N) + t] * dtau_s[0]);
+  if (t < NN) E[t] = exp(RF(0)[C::SEIG + t] * dtau_s[0]);
   __syncwarp(msk);
   // top boundary rows in slots 0..NN-1 (setMatrix :890-907, solve0 :978-990)
   if (t < NN) {
@@ -175,12 +189,12 @@ __global__ void __launch_bounds__(RCfg<N>::CTA, RCfg<N>::MINB) flux_bvp_reg_kern
     const int jq = NN - 1 - t;
 #pragma unroll
     for (int iq = 0; iq < N; ++iq) {
-      const double g = ld_rec(l0 + lrec_G(N) + jq * N + iq);
+      const double g = ld_rec(l0 + jq * GS + iq);
       cur[iq] = (iq < NN) ? g * E[iq] : g;
     }
     double s = 0.0;
-    if (beam) s -= ld_rec(l0 + lrec_zb(N) + jq);
-    if (thermal) s -= ld_rec(l0 + lrec_z0(N) + jq);
+    if (beam) s -= ld_rec(l0 + C::SZB + jq);
+    if (thermal) s -= ld_rec(l0 + C::SZ0 + jq);
     s += fisot + ptop;
     rhs = s;
   }
@@ -198,14 +212,14 @@ __global__ void __launch_bounds__(RCfg<N>::CTA, RCfg<N>::MINB) flux_bvp_reg_kern
       tau_n = taus[l + 2];
     }
     // record l+2 starts loading into the slot of record l-1; record l+1 is waited for
-    if (l + 2 < ncut) team_copy_async<TEAM>(RF(l + 2), LR(l + 2), RS, t);
+    if (l + 2 < ncut) copy_lrec(RF(l + 2), LR(l + 2));
     cp_async_commit();
     cp_async_wait<1>();
     __syncwarp(msk);
     const double* lr = RF(l);
     const double* Ecur = E + (l & 1) * NN;
     double* Enext = E + ((l & 1) ^ 1) * NN;
-    if (!last && t < NN) Enext[t] = exp(RF(l + 1)[lrec_eig(N) + t] * dts1);
+    if (!last && t < NN) Enext[t] = exp(RF(l + 1)[C::SEIG + t] * dts1);
     __syncwarp(msk);
     // new rows into the free slots, in slot order
     const unsigned freem = ((PR == 32) ? 0xffffffffu : ((1u << PR) - 1u)) & ~carried;
@@ -218,8 +232,8 @@ __global__ void __launch_bounds__(RCfg<N>::CTA, RCfg<N>::MINB) flux_bvp_reg_kern
         // continuity row jq of interface (l, l+1) (setMatrix :852-887, solve0 :1080-1104)
         const int jq = rank;
         const double* ln = RF(l + 1);
-        const double* Gl = lr + lrec_G(N) + jq * N;
-        const double* Gn = ln + lrec_G(N) + jq * N;
+        const double* Gl = lr + jq * GS;
+        const double* Gn = ln + jq * GS;
 #pragma unroll
         for (int iq = 0; iq < N; ++iq) {
           const double g = ld_rec(Gl + iq);
@@ -230,25 +244,25 @@ __global__ void __launch_bounds__(RCfg<N>::CTA, RCfg<N>::MINB) flux_bvp_reg_kern
         const double T = btr1, tau = tau1;
         double sum = 0.0;
         if (beam) {
-          sum += ld_rec(ln + lrec_zb(N) + jq) * T;
-          sum -= ld_rec(lr + lrec_zb(N) + jq) * T;
+          sum += ld_rec(ln + C::SZB + jq) * T;
+          sum -= ld_rec(lr + C::SZB + jq) * T;
         }
         if (thermal) {
-          sum += ld_rec(ln + lrec_z0(N) + jq) - ld_rec(lr + lrec_z0(N) + jq);
-          sum += (ld_rec(ln + lrec_z1(N) + jq) - ld_rec(lr + lrec_z1(N) + jq)) * tau;
+          sum += ld_rec(ln + C::SZ0 + jq) - ld_rec(lr + C::SZ0 + jq);
+          sum += (ld_rec(ln + C::SZ1 + jq) - ld_rec(lr + C::SZ1 + jq)) * tau;
         }
         rhs = sum;
       } else {
         // bottom boundary row (setMatrix :909-958, solve0 :993-1076)
         const int rb = rank, jq = NN + rb;
         const bool plain = lyrcut || dlbc;
-        const double* Gl = lr + lrec_G(N);
+        const double* Gl = lr;
 #pragma unroll
         for (int iq = 0; iq < N; ++iq) {
-          double base = ld_rec(Gl + jq * N + iq);
+          double base = ld_rec(Gl + jq * GS + iq);
           if (!plain) {
             double refl = 0.0;
-            for (int k = 0; k < NN; ++k) refl += wt[k] * mu[k] * alb * ld_rec(Gl + (NN - 1 - k) * N + iq);
+            for (int k = 0; k < NN; ++k) refl += wt[k] * mu[k] * alb * ld_rec(Gl + (NN - 1 - k) * GS + iq);
             base = base - 2.0 * refl;
           }
           cur[iq] = (iq < NN) ? base : base * Ecur[N - 1 - iq];
@@ -257,10 +271,10 @@ __global__ void __launch_bounds__(RCfg<N>::CTA, RCfg<N>::MINB) flux_bvp_reg_kern
         const double T = btr1, tau = tau1;
         double sum = 0.0;
         if (dlbc) {
-          if (beam) sum -= ld_rec(lr + lrec_zb(N) + NN + rb) * T;
+          if (beam) sum -= ld_rec(lr + C::SZB + NN + rb) * T;
           if (thermal) {
-            sum -= ld_rec(lr + lrec_z0(N) + NN + rb);
-            sum -= ld_rec(lr + lrec_z1(N) + NN + rb) * tau;
+            sum -= ld_rec(lr + C::SZ0 + NN + rb);
+            sum -= ld_rec(lr + C::SZ1 + NN + rb) * tau;
           }
           sum += pbot + mu[rb] * pbotd;
         } else {
@@ -268,19 +282,19 @@ __global__ void __launch_bounds__(RCfg<N>::CTA, RCfg<N>::MINB) flux_bvp_reg_kern
             double refl = 0.0;
             for (int jj = 0; jj < NN; ++jj) {
               double ps = 0.0;
-              if (beam) ps += ld_rec(lr + lrec_zb(N) + NN - 1 - jj) * T;
-              if (thermal) ps += ld_rec(lr + lrec_z0(N) + NN - 1 - jj) + ld_rec(lr + lrec_z1(N) + NN - 1 - jj) * tau;
+              if (beam) ps += ld_rec(lr + C::SZB + NN - 1 - jj) * T;
+              if (thermal) ps += ld_rec(lr + C::SZ0 + NN - 1 - jj) + ld_rec(lr + C::SZ1 + NN - 1 - jj) * tau;
               refl += wt[jj] * mu[jj] * alb * ps;
             }
             sum += 2.0 * refl;
           }
           if (beam) {
-            sum -= ld_rec(lr + lrec_zb(N) + NN + rb) * T;
+            sum -= ld_rec(lr + C::SZB + NN + rb) * T;
             if (!lyrcut) sum += alb * umu0 * fbeam * T / PI;
           }
           if (thermal) {
-            sum -= ld_rec(lr + lrec_z0(N) + NN + rb);
-            sum -= ld_rec(lr + lrec_z1(N) + NN + rb) * tau;
+            sum -= ld_rec(lr + C::SZ0 + NN + rb);
+            sum -= ld_rec(lr + C::SZ1 + NN + rb) * tau;
           }
           sum += fisob;
           if (thermal) sum += (1.0 - alb) * pbot;
@@ -311,6 +325,7 @@ __global__ void __launch_bounds__(RCfg<N>::CTA, RCfg<N>::MINB) flux_bvp_reg_kern
         team_argmax<TEAM>(v, idx, nullptr);
         zero_piv = v == 0.0;
       }
+      DSP_PHASE(27)
       const int ps = idx < PR ? idx : 0;
       cand &= ~(1u << ps);
       if (t == ps) myc = c;
@@ -332,6 +347,7 @@ __global__ void __launch_bounds__(RCfg<N>::CTA, RCfg<N>::MINB) flux_bvp_reg_kern
         buf[2 * N + 1] = tinv;
       }
       __syncwarp(msk);
+      DSP_PHASE(28)
       if ((cand >> t) & 1u) {
         const double m = cur[c] * buf[2 * N + 1];
 #pragma unroll
@@ -398,8 +414,8 @@ __global__ void __launch_bounds__(RCfg<N>::CTA, RCfg<N>::MINB) flux_bvp_reg_kern
   auto eval_level = [&](int l, const double* x, int lu, double utaupr, double utau, double tau_top,
                         double tau_bot, double w0) {
     const double* lr = RB(l);
-    const double* eig = lr + lrec_eig(N);
-    const double* Gl = lr + lrec_G(N);
+    const double* eig = lr + C::SEIG;
+    const double* Gl = lr;
     if (t < N) {
       const double d = (t < NN) ? (utaupr - tau_bot) : (utaupr - tau_top);
       ec[t] = x[t] * exp(-eig[t] * d);
@@ -409,9 +425,9 @@ __global__ void __launch_bounds__(RCfg<N>::CTA, RCfg<N>::MINB) flux_bvp_reg_kern
     if (t < N) {
       double s = 0.0;
 #pragma unroll
-      for (int j = 0; j < N; ++j) s += ld_rec(Gl + t * N + j) * ec[j];
-      if (beam) s += ld_rec(lr + lrec_zb(N) + t) * fact;
-      if (thermal) s += ld_rec(lr + lrec_z0(N) + t) + ld_rec(lr + lrec_z1(N) + t) * utaupr;
+      for (int j = 0; j < N; ++j) s += ld_rec(Gl + t * GS + j) * ec[j];
+      if (beam) s += ld_rec(lr + C::SZB + t) * fact;
+      if (thermal) s += ld_rec(lr + C::SZ0 + t) + ld_rec(lr + C::SZ1 + t) * utaupr;
       Iv[t] = s;
     }
     __syncwarp(msk);
@@ -449,7 +465,7 @@ __global__ void __launch_bounds__(RCfg<N>::CTA, RCfg<N>::MINB) flux_bvp_reg_kern
       uad = (2.0 * PI * uad) * R4PI;
       uau = (2.0 * PI * uau) * R4PI;
       double plsorc = 0.0;
-      if (thermal) plsorc = lr[lrec_xr(N)] + lr[lrec_xr(N) + 1] * utaupr;
+      if (thermal) plsorc = lr[C::SXR] + lr[C::SXR + 1] * utaupr;
       const double dfdt = (1.0 - w0) * 4.0 * PI * (ua - plsorc);
       const double o[8] = {fdir, fdn, fup, dfdt, ua, uad, uau, uaso};
 #pragma unroll
@@ -473,7 +489,7 @@ __global__ void __launch_bounds__(RCfg<N>::CTA, RCfg<N>::MINB) flux_bvp_reg_kern
         if ((int)lyr_l[lu] > ncut - 1)
           for (int f = 0; f < 8; ++f) outp[f][oidx(lu)] = 0.0;
   }
-  team_copy_async<TEAM>(RB(ncut - 1), LR(ncut - 1), RS, t);
+  copy_lrec(RB(ncut - 1), LR(ncut - 1));
   cp_async_commit();
   // per-layer scalars of layer l, loaded one layer ahead
   double tau_top = taus[ncut - 1], tau_bot = taus[ncut], tauc_bot = GEN ? 0.0 : rec[il.tauc + ncut];
@@ -483,6 +499,7 @@ __global__ void __launch_bounds__(RCfg<N>::CTA, RCfg<N>::MINB) flux_bvp_reg_kern
     const double tauc_top = GEN ? 0.0 : rec[il.tauc + l];
     cp_async_wait<0>();
     __syncwarp(msk);
+    DSP_PHASE(24)
     double* x = XV + (l & 1) * N;
     if (l < ncut - 1) {
       // U x_l = c - V x_{l+1}: lane t holds row t; column c's unknown is
@@ -504,13 +521,15 @@ __global__ void __launch_bounds__(RCfg<N>::CTA, RCfg<N>::MINB) flux_bvp_reg_kern
       }
       __syncwarp(msk);
     }
+    DSP_PHASE(25)
     // the records of layer l-1 start loading (the elimination record is used
     // up; the layer-record slot held layer l+1)
     if (l > 0) {
-      team_copy_async<TEAM>(RB(l - 1), LR(l - 1), RS, t);
+      copy_lrec(RB(l - 1), LR(l - 1));
       team_copy_async<TEAM>(EB, brec0 + (long long)(l - 1) * BS, BS, t);
     }
     cp_async_commit();
+    DSP_PHASE(26)
     if constexpr (GEN) {
       if (t < N) cc0[(long long)l * N + t] = x[t];
       if (m == 0)
@@ -526,6 +545,7 @@ __global__ void __launch_bounds__(RCfg<N>::CTA, RCfg<N>::MINB) flux_bvp_reg_kern
     w0 = w0_n;
     DSP_PHASE(23)
   }
+  DSP_PHASE_END
   if (nonfinite && t == 0) set_status(p.status, i, DSP_ERR_NONFINITE);
 }
 
