@@ -99,6 +99,36 @@ def test_layer_cut_and_index_from_bottom():
     assert_parity(got2, ref2, "index_from_bottom")
 
 
+@pytest.mark.parametrize("nstr", [10, 12, 14, 16])
+def test_split_layer_stage_cut_bottom_index_and_conservative_layers(nstr):
+    """The three-launch layer stage of 10-16 streams: layers below the absorption
+    cut and whole instances marked skipped, bottom-up layer indexing, omega = 1
+    layers (the fallback factorisation) among ordinary ones, and a task count
+    that leaves a partial block of 32 in the hand-off."""
+    rng = np.random.default_rng(300 + nstr)
+    n, L = 37, 13  # 481 layer tasks
+    pc = nstr + 1
+    w = dict(n_inst=n, num_streams=nstr, num_layers=L, num_phase_func_moments=0, pmom_count=pc, flags=0,
+             arrays=dict(delta_tau=rng.uniform(0.5, 3.0, (n, L)), single_scat_albedo=rng.uniform(0, 0.7, (n, L)),
+                         phase_function_moments=workloads.hg_moments(rng.uniform(0, 0.8, (n, L)), pc),
+                         surface_albedo=0.2, direct_beam_flux=1.0, direct_beam_mu=0.6))
+    got, gst, ref, rst = both(w)
+    assert np.all(gst == 0)
+    assert np.any(got["flux_up"][:, -1] == 0.0)  # absorption cut reached
+    assert_parity(got, ref, f"nstr={nstr} lyrcut")
+    got, gst, ref, rst = both(w, extra_flags=capi.FLAG_INDEX_FROM_BOTTOM)
+    assert_parity(got, ref, f"nstr={nstr} index_from_bottom")
+    # conservative layers: the reference's own tolerance for omega = 1 (1e-8 relative
+    # with 2e-9 absolute, test_flux_solver.cpp:46-60, 135-136)
+    ssa = w["arrays"]["single_scat_albedo"].copy()
+    ssa[::3, ::4] = 1.0
+    w["arrays"]["single_scat_albedo"] = ssa
+    got, gst, ref, rst = both(w)
+    assert np.all(gst == rst)
+    for f in capi.FLUX_OUT_FIELDS:
+        np.testing.assert_allclose(got[f], ref[f], rtol=1e-8, atol=2e-9)
+
+
 def test_device_pointers_match_host_pointers():
     w = workloads.subset(workloads.thermal_sweep(), np.arange(64))
     got, gst, _ = gpu_lib.flux_solve(w)
