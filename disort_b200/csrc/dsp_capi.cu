@@ -28,10 +28,9 @@ using namespace dsp_host;
 namespace {
 
 template <int N>
-dsp_status launch_flux_chunk(dsp_context ctx, const FluxParams& p) {
-  cudaStream_t s = ctx->stream;
+dsp_status launch_flux_chunk(dsp_context ctx, const FluxParams& p, cudaStream_t s) {
   {
-    KernelTimer kt(ctx, "flux_setup_kernel");
+    KernelTimer kt(ctx, "flux_setup_kernel", s);
     flux_setup_kernel<<<(p.n + 3) / 4, 128, 0, s>>>(p);
   }
   {
@@ -41,7 +40,7 @@ dsp_status launch_flux_chunk(dsp_context ctx, const FluxParams& p) {
       attr = true;
     }
     flux_layer_launch<N>(p, ctx->host_tables.at(N).data(), s, [&](const char* name, auto&& launch) {
-      KernelTimer kt(ctx, name);
+      KernelTimer kt(ctx, name, s);
       launch();
     });
   }
@@ -49,7 +48,7 @@ dsp_status launch_flux_chunk(dsp_context ctx, const FluxParams& p) {
     using C = RCfg<N>;
     const size_t sm = C::smem_bytes();
     const int grid = (p.n + C::TPC - 1) / C::TPC;
-    KernelTimer kt(ctx, "flux_bvp_kernel");
+    KernelTimer kt(ctx, "flux_bvp_kernel", s);
     flux_bvp_reg_kernel<N><<<grid, C::CTA, sm, s>>>(p);
   } else {
     using C = TCfg<N>;
@@ -60,7 +59,7 @@ dsp_status launch_flux_chunk(dsp_context ctx, const FluxParams& p) {
       attr = true;
     }
     const int grid = (p.n + C::TPC - 1) / C::TPC;
-    KernelTimer kt(ctx, "flux_bvp_kernel");
+    KernelTimer kt(ctx, "flux_bvp_kernel", s);
     flux_bvp_tile_kernel<N><<<grid, C::CTA, sm, s>>>(p);
   }
   cudaError_t e = cudaGetLastError();
@@ -68,17 +67,49 @@ dsp_status launch_flux_chunk(dsp_context ctx, const FluxParams& p) {
   return DSP_OK;
 }
 
-dsp_status launch_flux(dsp_context ctx, int N, const FluxParams& p) {
+// Instances the boundary-value kernel of N streams keeps resident on the whole
+// GPU at once (one wave).
+template <int N>
+int64_t bvp_wave_n(int sm_count) {
+  int blocks = 0;
+  if constexpr (N <= 16) {
+    using C = RCfg<N>;
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&blocks, flux_bvp_reg_kernel<N>, C::CTA, C::smem_bytes());
+    return (int64_t)std::max(blocks, 1) * C::TPC * sm_count;
+  } else {
+    using C = TCfg<N>;
+    cudaFuncSetAttribute(flux_bvp_tile_kernel<N>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)C::smem_bytes());
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&blocks, flux_bvp_tile_kernel<N>, C::CTA, C::smem_bytes());
+    return (int64_t)std::max(blocks, 1) * C::TPC * sm_count;
+  }
+}
+
+int64_t bvp_wave(int N, int sm_count) {
   switch (N) {
-    case 4: return launch_flux_chunk<4>(ctx, p);
-    case 6: return launch_flux_chunk<6>(ctx, p);
-    case 8: return launch_flux_chunk<8>(ctx, p);
-    case 10: return launch_flux_chunk<10>(ctx, p);
-    case 12: return launch_flux_chunk<12>(ctx, p);
-    case 14: return launch_flux_chunk<14>(ctx, p);
-    case 16: return launch_flux_chunk<16>(ctx, p);
-    case 32: return launch_flux_chunk<32>(ctx, p);
-    case 64: return launch_flux_chunk<64>(ctx, p);
+    case 4: return bvp_wave_n<4>(sm_count);
+    case 6: return bvp_wave_n<6>(sm_count);
+    case 8: return bvp_wave_n<8>(sm_count);
+    case 10: return bvp_wave_n<10>(sm_count);
+    case 12: return bvp_wave_n<12>(sm_count);
+    case 14: return bvp_wave_n<14>(sm_count);
+    case 16: return bvp_wave_n<16>(sm_count);
+    case 32: return bvp_wave_n<32>(sm_count);
+    case 64: return bvp_wave_n<64>(sm_count);
+  }
+  return sm_count;
+}
+
+dsp_status launch_flux(dsp_context ctx, int N, const FluxParams& p, cudaStream_t s) {
+  switch (N) {
+    case 4: return launch_flux_chunk<4>(ctx, p, s);
+    case 6: return launch_flux_chunk<6>(ctx, p, s);
+    case 8: return launch_flux_chunk<8>(ctx, p, s);
+    case 10: return launch_flux_chunk<10>(ctx, p, s);
+    case 12: return launch_flux_chunk<12>(ctx, p, s);
+    case 14: return launch_flux_chunk<14>(ctx, p, s);
+    case 16: return launch_flux_chunk<16>(ctx, p, s);
+    case 32: return launch_flux_chunk<32>(ctx, p, s);
+    case 64: return launch_flux_chunk<64>(ctx, p, s);
   }
   return fail(ctx, DSP_ERR_UNSUPPORTED, "unsupported num_streams");
 }
@@ -142,9 +173,11 @@ dsp_status dsp_context_destroy(dsp_context ctx) {
   for (cudaEvent_t e : ctx->free_events) cudaEventDestroy(e);
   if (ctx->s_in) cudaStreamSynchronize(ctx->s_in);
   if (ctx->s_out) cudaStreamSynchronize(ctx->s_out);
+  if (ctx->s_c2) cudaStreamSynchronize(ctx->s_c2);
   for (cudaEvent_t e : ctx->pipe_ev) cudaEventDestroy(e);
   if (ctx->s_in) cudaStreamDestroy(ctx->s_in);
   if (ctx->s_out) cudaStreamDestroy(ctx->s_out);
+  if (ctx->s_c2) cudaStreamDestroy(ctx->s_c2);
   if (ctx->ws) cudaFree(ctx->ws);
   if (ctx->stage_in) cudaFree(ctx->stage_in);
   if (ctx->stage_out) cudaFree(ctx->stage_out);
@@ -304,6 +337,7 @@ dsp_status dsp_flux_bands_solve(dsp_context ctx, const dsp_flux_batch* batch_in,
 
   // ---- workspace and chunking -------------------------------------------
   const Sizes sz = sizes_for(N, L);
+  const size_t inst_doubles = sz.inst + sz.layer + sz.bvp;
   size_t budget = workspace_budget();
   size_t freeb = 0, totalb = 0;
   if (cudaMemGetInfo(&freeb, &totalb) == cudaSuccess && freeb / 2 < budget + ctx->ws_bytes)
@@ -311,46 +345,52 @@ dsp_status dsp_flux_bands_solve(dsp_context ctx, const dsp_flux_batch* batch_in,
   int64_t chunk = (int64_t)(budget / sz.per_inst_bytes());
   if (chunk < 1) chunk = 1;
   if (chunk > n) chunk = n;
-  const size_t ws_need = (size_t)chunk * (sz.inst + sz.layer + sz.bvp) * sizeof(double) + 1024;
-  if ((st = ensure(ctx, &ctx->ws, &ctx->ws_bytes, ws_need, "workspace")) != DSP_OK) return st;
 
-  FluxParams p;
-  p.N = N;
-  p.L = L;
-  p.pc = b.pmom_count;
-  p.nmom = b.num_phase_func_moments;
-  p.flags = b.flags;
-  p.tables = tables;
-  p.pk = planck_consts();
-  p.il = InstLayout::make(L, N);
-  DArr* pa[14] = {&p.wlo, &p.whi, &p.dtau, &p.ssa, &p.pmom, &p.temp, &p.alb,
-                  &p.emis, &p.fbeam, &p.umu0, &p.fisot, &p.fisob, &p.ttop, &p.tbot};
-  auto run_range = [&](int64_t r0, int64_t r1) -> dsp_status {
-    for (int64_t off = r0; off < r1; off += chunk) {
-      const int64_t m = (r1 - off < chunk) ? (r1 - off) : chunk;
+  FluxParams p0;
+  p0.N = N;
+  p0.L = L;
+  p0.pc = b.pmom_count;
+  p0.nmom = b.num_phase_func_moments;
+  p0.flags = b.flags;
+  p0.tables = tables;
+  p0.pk = planck_consts();
+  p0.il = InstLayout::make(L, N);
+  // solves instances [r0, r1) on stream `cs`, `ch` at a time, in the workspace at `wsb`
+  auto run_range = [&](int64_t r0, int64_t r1, cudaStream_t cs, double* wsb, int64_t ch) -> dsp_status {
+    FluxParams p = p0;
+    DArr* pa[14] = {&p.wlo, &p.whi, &p.dtau, &p.ssa, &p.pmom, &p.temp, &p.alb,
+                    &p.emis, &p.fbeam, &p.umu0, &p.fisot, &p.fisob, &p.ttop, &p.tbot};
+    for (int64_t off = r0; off < r1; off += ch) {
+      const int64_t m = (r1 - off < ch) ? (r1 - off) : ch;
       p.n = (int)m;
       for (int k = 0; k < 14; ++k) {
         pa[k]->p = arr[k].ptr ? arr[k].ptr + arr[k].stride * off : nullptr;
         pa[k]->s = arr[k].stride;
       }
-      double* w = static_cast<double*>(ctx->ws);
-      p.inst_rec = w;
-      p.layer_rec = w + (size_t)m * sz.inst;
+      p.inst_rec = wsb;
+      p.layer_rec = wsb + (size_t)m * sz.inst;
       p.bvp_rec = p.layer_rec + (size_t)m * sz.layer;
       for (int f = 0; f < 8; ++f) p.out[f] = dout[f] + off * nlev;
       p.status = dstatus + off;
-      dsp_status rs = launch_flux(ctx, N, p);
+      dsp_status rs = launch_flux(ctx, N, p, cs);
       if (rs != DSP_OK) return rs;
     }
     return DSP_OK;
   };
-  if (dev) return run_range(0, n);
+  if (dev) {
+    const size_t ws_need = (size_t)chunk * inst_doubles * sizeof(double) + 1024;
+    if ((st = ensure(ctx, &ctx->ws, &ctx->ws_bytes, ws_need, "workspace")) != DSP_OK) return st;
+    return run_range(0, n, s, static_cast<double*>(ctx->ws), chunk);
+  }
 
   // ---- host buffers: copies overlapped with the solves ----------------------
-  // The batch is cut into pieces; piece k's inputs go up on a copy stream while
-  // piece k-1 is solved on the context's stream and the outputs of piece k-2 come
-  // back on a second copy stream.  (With pageable host memory the copies do not
-  // overlap, but the results are the same.)
+  // The batch is cut into pieces of whole boundary-value waves (the instances
+  // that kernel keeps resident at once), about a quarter of the batch each, the
+  // remainder last.  Piece k's inputs go up on a copy stream, it is solved on
+  // one of two solve streams (alternating, each with its own half of the
+  // workspace) and its outputs come back on a second copy stream, so the next
+  // piece's kernels fill the GPU while a piece's last wave drains.  (With
+  // pageable host memory the copies do not overlap, but the results are the same.)
   double* host_out[8] = {out->flux_direct_beam, out->flux_down, out->flux_up, out->flux_tau_divergence,
                          out->mean_intensity, out->mean_intensity_down, out->mean_intensity_up,
                          out->mean_intensity_direct_beam};
@@ -361,13 +401,22 @@ dsp_status dsp_flux_bands_solve(dsp_context ctx, const dsp_flux_batch* batch_in,
     hs = hst.data();
   }
   constexpr int kMaxPieces = 8;
-  // pieces of at least two waves of the one-warp-per-instance boundary-value
-  // kernel (16 resident per SM), so that launch tails stay small
-  const int64_t min_piece = 32 * (int64_t)ctx->sm_count;
-  const int pieces = (int)std::max<int64_t>(1, std::min<int64_t>(kMaxPieces, n / min_piece));
+  const int64_t wave = std::max<int64_t>(1, bvp_wave(N, ctx->sm_count));
+  const int64_t waves = (n + wave - 1) / wave;
+  int64_t piece = wave * std::max<int64_t>(1, waves / 4);
+  while ((n + piece - 1) / piece > kMaxPieces) piece += wave;
+  piece = std::min<int64_t>(piece, n);
+  const int pieces = (int)((n + piece - 1) / piece);
+  // two workspace halves when they fit the budget, else one stream and `chunk`
+  const bool dual = pieces > 1 && piece <= chunk / 2;
+  const int64_t ch = dual ? piece : chunk;
+  const size_t half = (size_t)ch * inst_doubles;
+  const size_t ws_need = (dual ? 2 : 1) * half * sizeof(double) + 1024;
+  if ((st = ensure(ctx, &ctx->ws, &ctx->ws_bytes, ws_need, "workspace")) != DSP_OK) return st;
   if (!ctx->s_in) {
     e = cudaStreamCreateWithFlags(&ctx->s_in, cudaStreamNonBlocking);
     if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&ctx->s_out, cudaStreamNonBlocking);
+    if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&ctx->s_c2, cudaStreamNonBlocking);
     if (e != cudaSuccess) return cuda_fail(ctx, e, "copy streams");
   }
   while ((int)ctx->pipe_ev.size() < 2 * kMaxPieces + 1) {
@@ -379,12 +428,16 @@ dsp_status dsp_flux_bands_solve(dsp_context ctx, const dsp_flux_batch* batch_in,
   cudaEvent_t* ev_in = ctx->pipe_ev.data();
   cudaEvent_t* ev_done = ev_in + kMaxPieces;
   cudaEvent_t ev_start = ctx->pipe_ev[2 * kMaxPieces];
-  // the staging areas may still be read by earlier work on the context's stream
+  // the staging areas and the workspace may still be used by earlier work on
+  // the context's stream (and the status memset above runs there)
   e = cudaEventRecord(ev_start, s);
   if (e == cudaSuccess) e = cudaStreamWaitEvent(ctx->s_in, ev_start, 0);
+  if (e == cudaSuccess) e = cudaStreamWaitEvent(ctx->s_c2, ev_start, 0);
   if (e != cudaSuccess) return cuda_fail(ctx, e, "pipeline start");
+  double* const ws0 = static_cast<double*>(ctx->ws);
   for (int k = 0; k < pieces; ++k) {
-    const int64_t r0 = n * k / pieces, r1 = n * (k + 1) / pieces;
+    const int64_t r0 = piece * k, r1 = std::min<int64_t>(n, piece * (k + 1));
+    cudaStream_t cs = (dual && (k & 1)) ? ctx->s_c2 : s;
     for (int a = 0; a < 14; ++a) {
       if (!host_in[a]) continue;
       const int64_t e0 = r0 * arr[a].stride, e1 = (r1 - 1) * arr[a].stride + cnt[a];
@@ -393,10 +446,10 @@ dsp_status dsp_flux_bands_solve(dsp_context ctx, const dsp_flux_batch* batch_in,
       if (e != cudaSuccess) return cuda_fail(ctx, e, "cudaMemcpyAsync(input)");
     }
     e = cudaEventRecord(ev_in[k], ctx->s_in);
-    if (e == cudaSuccess) e = cudaStreamWaitEvent(s, ev_in[k], 0);
+    if (e == cudaSuccess) e = cudaStreamWaitEvent(cs, ev_in[k], 0);
     if (e != cudaSuccess) return cuda_fail(ctx, e, "pipeline input");
-    if ((st = run_range(r0, r1)) != DSP_OK) return st;
-    e = cudaEventRecord(ev_done[k], s);
+    if ((st = run_range(r0, r1, cs, ws0 + ((dual && (k & 1)) ? half : 0), ch)) != DSP_OK) return st;
+    e = cudaEventRecord(ev_done[k], cs);
     if (e == cudaSuccess) e = cudaStreamWaitEvent(ctx->s_out, ev_done[k], 0);
     if (e != cudaSuccess) return cuda_fail(ctx, e, "pipeline output");
     for (int f = 0; f < 8; ++f) {
@@ -408,7 +461,10 @@ dsp_status dsp_flux_bands_solve(dsp_context ctx, const dsp_flux_batch* batch_in,
                         ctx->s_out);
     if (e != cudaSuccess) return cuda_fail(ctx, e, "cudaMemcpyAsync(status)");
   }
-  e = cudaStreamSynchronize(ctx->s_out);
+  // later work on the context's stream sees the whole solve
+  e = cudaEventRecord(ev_start, ctx->s_c2);
+  if (e == cudaSuccess) e = cudaStreamWaitEvent(s, ev_start, 0);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(ctx->s_out);
   if (e == cudaSuccess) e = cudaStreamSynchronize(s);
   if (e != cudaSuccess) return cuda_fail(ctx, e, "flux solve");
   return DSP_OK;

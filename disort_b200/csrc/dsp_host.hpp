@@ -39,6 +39,7 @@ struct dsp_context_s {
   size_t meta_bytes = 0;
   // host-buffer solves: copy streams and events of the copy/compute pipeline
   cudaStream_t s_in = nullptr, s_out = nullptr;
+  cudaStream_t s_c2 = nullptr;  // second solve stream of the host-buffer pipeline
   std::vector<cudaEvent_t> pipe_ev;
   // optional per-kernel timing
   bool timing = false;
@@ -77,18 +78,19 @@ inline int kernel_id(dsp_context c, const char* name) {
 // Brackets one launch with events when timing is on.
 struct KernelTimer {
   dsp_context c;
+  cudaStream_t s;
   int id = -1;
   cudaEvent_t a = nullptr, b = nullptr;
-  KernelTimer(dsp_context ctx, const char* name) : c(ctx) {
+  KernelTimer(dsp_context ctx, const char* name, cudaStream_t st = nullptr) : c(ctx), s(st ? st : ctx->stream) {
     if (!c->timing) return;
     id = kernel_id(c, name);
     a = take_event(c);
     b = take_event(c);
-    cudaEventRecord(a, c->stream);
+    cudaEventRecord(a, s);
   }
   ~KernelTimer() {
     if (id < 0) return;
-    cudaEventRecord(b, c->stream);
+    cudaEventRecord(b, s);
     c->pending.push_back({id, a, b});
   }
 };
