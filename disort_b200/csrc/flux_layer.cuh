@@ -1277,7 +1277,18 @@ __global__ void __launch_bounds__(128) flux_layer_back_kernel(FluxParams p, Cons
   // addresses and write nothing (no early exit: the warp writes rows together)
   const long long jj = j < nt ? j : nt - 1;
   auto hv = [&](int e) { return *handoff_lane<NN>(p.bvp_rec, nt, jj, e); };
+  // the hand-off operands of the eigenvector phase are all requested up front,
+  // so that their latency overlaps the ordering of the eigenvalues
+  double d[NN], L[H::TRI], rdg[NN], EV[NN][NN];  // EV[c][r]: column c
   const double flag = hv(H::S_FLAG);
+#pragma unroll
+  for (int k = 0; k < NN; ++k) d[k] = hv(H::S_D + k);
+#pragma unroll
+  for (int e = 0; e < H::TRI; ++e) L[e] = hv(H::S_L + e);
+#pragma unroll
+  for (int c = 0; c < NN; ++c)
+#pragma unroll
+    for (int r = 0; r < NN; ++r) EV[c][r] = hv(H::S_V + r * NN + c);
   const bool act = j < nt && flag != 0.0;  // skipped: cut layer, invalid input, no factorisation
   const unsigned okm = __ballot_sync(0xffffffffu, act);
   if (okm == 0u) return;  // warp-uniform
@@ -1291,9 +1302,6 @@ __global__ void __launch_bounds__(128) flux_layer_back_kernel(FluxParams p, Cons
   double kr[NN], rk[NN];
   int rank[NN];
   {
-    double d[NN];
-#pragma unroll
-    for (int k = 0; k < NN; ++k) d[k] = hv(H::S_D + k);
 #pragma unroll
     for (int k = 0; k < NN; ++k) {
       int r = 0;
@@ -1308,7 +1316,6 @@ __global__ void __launch_bounds__(128) flux_layer_back_kernel(FluxParams p, Cons
     }
   }
   warp_flush_rows<RS>(stA, rec0, LS, N, lrec_eig(N), okm, lane);
-  double L[H::TRI], rdg[NN];
   auto load_L = [&]() {
 #pragma unroll
     for (int e = 0; e < H::TRI; ++e) L[e] = hv(H::S_L + e);
@@ -1318,12 +1325,10 @@ __global__ void __launch_bounds__(128) flux_layer_back_kernel(FluxParams p, Cons
   const BackOps<NN> ops{L, rdg};
   {
     // ---- eigenvectors of (a+b)(a-b): D^{-1} L^{-T} w (primary), D^{-1} L w --
-    double EV[NN][NN];  // EV[c][r]: column c
-    load_L();
+#pragma unroll
+    for (int k = 0; k < NN; ++k) rdg[k] = 1.0 / L[tri_idx(k, k)];
 #pragma unroll
     for (int c = 0; c < NN; ++c) {
-#pragma unroll
-      for (int r = 0; r < NN; ++r) EV[c][r] = hv(H::S_V + r * NN + c);
       if (primary) ops.bwd(EV[c]);
       else ops.lmul(EV[c]);
 #pragma unroll
