@@ -987,24 +987,28 @@ __global__ void __launch_bounds__(128) flux_layer_front_kernel(FluxParams p, Con
   const int i = (int)(j / p.L), lc = (int)(j % p.L);
   const double* rec = p.inst_rec + (long long)i * p.il.stride;
   const InstLayout& il = p.il;
+  // the layer's inputs are requested before the test that may skip it
+  const int lin = (p.flags & DSP_FLAG_INDEX_FROM_BOTTOM) ? p.L - 1 - lc : lc;
+  const double* pml = p.pmom.row(i) + (long long)lin * p.pc;
+  double pmk[N];
+#pragma unroll
+  for (int k = 0; k < N; ++k) pmk[k] = pml[k];
+  const double ws = rec[il.ssa_s + lc];
+  const bool beam = rec[H_FBEAM] > 0.0;
+  const int mode = (int)rec[il.mode + lc];
+  const double f = rec[il.fsc + lc], sig = rec[il.sig + lc];
   // invalid instances and layers below the absorption cut are not solved
   if ((p.status && p.status[i] == DSP_ERR_INVALID_INPUT) || lc >= (int)rec[H_NCUT]) {
     *hp(H::S_FLAG) = 0.0;
     return;
   }
-  const double ws = rec[il.ssa_s + lc];
-  const bool beam = rec[H_FBEAM] > 0.0;
   // ---- phase sums O (odd orders) and E (even orders) ----------------------
   double O[TRI], E[TRI];
   {
-    const int lin = (p.flags & DSP_FLAG_INDEX_FROM_BOTTOM) ? p.L - 1 - lc : lc;
-    const double* pml = p.pmom.row(i) + (long long)lin * p.pc;
-    const int mode = (int)rec[il.mode + lc];
-    const double f = rec[il.fsc + lc], sig = rec[il.sig + lc];
     double gl[N];
 #pragma unroll
     for (int k = 0; k < N; ++k) {
-      const double pk = pml[k];
+      const double pk = pmk[k];
       double g;
       if (mode == 0) g = (2.0 * k + 1.0) * ws * pk;
       else if (mode == 1) g = (2.0 * k + 1.0) * ws * (pk - f) / (1.0 - f);
@@ -1370,7 +1374,7 @@ __global__ void __launch_bounds__(128) flux_layer_back_kernel(FluxParams p, Cons
     double acc[NN];
 #pragma unroll
     for (int r = 0; r < NN; ++r) acc[r] = 0.0;
-#pragma unroll 1
+#pragma unroll 2
     for (int c = 0; c < NN; ++c) {
       double v[NN], s = 0.0;
 #pragma unroll
