@@ -404,9 +404,12 @@ dsp_status dsp_flux_bands_solve(dsp_context ctx, const dsp_flux_batch* batch_in,
   const int64_t wave = std::max<int64_t>(1, bvp_wave(N, ctx->sm_count));
   const int64_t waves = (n + wave - 1) / wave;
   int64_t piece = wave * std::max<int64_t>(1, waves / 4);
-  while ((n + piece - 1) / piece > kMaxPieces) piece += wave;
+  while ((n + piece - 1) / piece > kMaxPieces - 1) piece += wave;
   piece = std::min<int64_t>(piece, n);
-  const int pieces = (int)((n + piece - 1) / piece);
+  // the first piece is one wave when the others are larger: the solves start
+  // after a shorter upload
+  const int64_t first = std::min<int64_t>(piece, wave);
+  const int pieces = 1 + (int)((n - first + piece - 1) / piece);
   // two workspace halves when they fit the budget, else one stream and `chunk`
   const bool dual = pieces > 1 && piece <= chunk / 2;
   const int64_t ch = dual ? piece : chunk;
@@ -436,7 +439,7 @@ dsp_status dsp_flux_bands_solve(dsp_context ctx, const dsp_flux_batch* batch_in,
   if (e != cudaSuccess) return cuda_fail(ctx, e, "pipeline start");
   double* const ws0 = static_cast<double*>(ctx->ws);
   for (int k = 0; k < pieces; ++k) {
-    const int64_t r0 = piece * k, r1 = std::min<int64_t>(n, piece * (k + 1));
+    const int64_t r0 = k == 0 ? 0 : first + piece * (k - 1), r1 = std::min<int64_t>(n, first + piece * k);
     cudaStream_t cs = (dual && (k & 1)) ? ctx->s_c2 : s;
     for (int a = 0; a < 14; ++a) {
       if (!host_in[a]) continue;
