@@ -1339,6 +1339,10 @@ __global__ void __launch_bounds__(128) flux_layer_back_kernel(FluxParams p, Cons
       for (int r = 0; r < NN; ++r) EV[c][r] *= tc.dinv[r];
     }
     // ---- G+/- (FluxSolver.cpp:575-587), two rows per step -------------------
+    // row iq of O is loaded one step ahead
+    double orow[NN];
+#pragma unroll
+    for (int k = 0; k < NN; ++k) orow[k] = hv(H::S_O + tri_idx(0, k));
 #pragma unroll 1
     for (int iq = 0; iq < NN; ++iq) {
       // row iq of alpha - beta = M^{-1} (O W - I)
@@ -1346,8 +1350,10 @@ __global__ void __launch_bounds__(128) flux_layer_back_kernel(FluxParams p, Cons
 #pragma unroll
       for (int k = 0; k < NN; ++k) rm = (k == iq) ? tc.rmu[k] : rm;
 #pragma unroll
-      for (int k = 0; k < NN; ++k)
-        arow[k] = (tc.wt[k] * hv(H::S_O + tri_idx(iq, k))) * rm - (k == iq ? rm : 0.0);
+      for (int k = 0; k < NN; ++k) arow[k] = (tc.wt[k] * orow[k]) * rm - (k == iq ? rm : 0.0);
+      const int iqn = iq + 1 < NN ? iq + 1 : iq;
+#pragma unroll
+      for (int k = 0; k < NN; ++k) orow[k] = hv(H::S_O + tri_idx(iqn, k));
       double* g0 = sA;  // row NN + iq
       double* g1 = sB;  // row NN - iq - 1
 #pragma unroll
