@@ -220,19 +220,14 @@ __device__ __forceinline__ bool team_chol(const double* M, double* Lc, double* f
   else return team_cholesky<NN, NS, TEAM>(M, Lc, flag, t);
 }
 
-// Whether the Jacobi rotation of pair (p, q) is applied: the off-diagonal
-// element is not negligible against the diagonal ones.
+// Whether the Jacobi rotation of pair (p, q) is applied: |apq| above 1e-15 of
+// sqrt|app aqq| (about 4.5 ulp).  With the quadratic convergence of cyclic
+// Jacobi a threshold at this level rather than 1e-17 saves the last sweep of
+// many tasks (one-thread eigensolver at 16 streams: 2.02 -> 1.82 ms per
+// 20,000-band thermal step); an off-diagonal left at that level moves
+// eigenvalues by its square and eigenvectors by it over the eigenvalue gap, far
+// below the 1e-9 parity bound.
 __device__ __forceinline__ bool jacobi_needed(double apq, double app, double aqq) {
-  return fabs(apq) > 1e-300 && apq * apq > 1.0e-34 * fabs(app * aqq);
-}
-
-// The test of the one-thread-per-task eigensolver: |apq| above 1e-15 of
-// sqrt|app aqq| (about 4.5 ulp) instead of 1e-17.  With the quadratic
-// convergence of cyclic Jacobi this saves the last sweep of many tasks (2.02 ->
-// 1.82 ms per 20,000-band thermal step); an off-diagonal left at that level
-// moves eigenvalues by its square and eigenvectors by it over the eigenvalue
-// gap, far below the 1e-9 parity bound.
-__device__ __forceinline__ bool jacobi_needed_t(double apq, double app, double aqq) {
   return fabs(apq) > 1e-300 && apq * apq > 1.0e-30 * fabs(app * aqq);
 }
 
@@ -929,7 +924,7 @@ __device__ __forceinline__ void jacobi_rot_rsq(double apq, double app, double aq
                                                double& tt) {
   const double d = aqq - app, e = 2.0 * apq;
   const double q = fma(d, d, e * e);
-  const bool rot = jacobi_needed_t(apq, app, aqq) && q > 1e-280;
+  const bool rot = jacobi_needed(apq, app, aqq) && q > 1e-280;
   const double r = rsqrt(rot ? q : 1.0);
   const double num = d > 0.0 ? e : (d < 0.0 ? -e : fabs(e));  // sgn(d) e, sgn(0) = +1
   const double h = fma(0.5 * fabs(d), r, 0.5);
@@ -1155,7 +1150,7 @@ __device__ __forceinline__ void jacobi_sweeps(double* S, double* V, bool act) {
     for (int r = 1; r < NN; ++r)
 #pragma unroll
       for (int q = 0; q < r; ++q)
-        if (jacobi_needed_t(S[tri_idx(r, q)], S[tri_idx(r, r)], S[tri_idx(q, q)])) more = true;
+        if (jacobi_needed(S[tri_idx(r, q)], S[tri_idx(r, r)], S[tri_idx(q, q)])) more = true;
     if (!__any_sync(0xffffffffu, act && more)) break;
   }
 }
