@@ -78,7 +78,7 @@ struct LCfg {
 // matrix in registers runs the rotations of a sweep with no shuffles or
 // barriers; the team form spends most of its time waiting on them.
 template <int N>
-__host__ __device__ constexpr bool layer_split() { return N >= 10 && N <= 16; }
+__host__ __device__ constexpr bool layer_split() { return N <= 16; }
 
 // packed lower-triangle index of the symmetric element (r, c)
 __host__ __device__ constexpr int tri_idx(int r, int c) {
