@@ -2,9 +2,8 @@
 //
 // Some callers cannot let a library allocate GPU memory: a host application
 // that hands the whole device to its own pooled allocator (and must account for
-// every byte), code that runs while a CUDA graph is being built from its
-// stream, or an embedding that forbids allocation after start-up.  For them,
-// dsp_flux_bands_solve_noalloc runs the same three kernels as
+// every byte), or an embedding that forbids allocation after start-up.  For
+// them, dsp_flux_bands_solve_noalloc runs the same kernels as
 // dsp_flux_bands_solve, but its workspace is a fixed array compiled into the
 // library (g_noalloc_scratch, 32 MiB of device memory that every GPU which loads
 // libdsp.so keeps until the process exits), and it needs no dsp_context (a
@@ -21,15 +20,19 @@
 //    contents; the per-instance status words are cleared at the start of each
 //    launch.  Calls that can overlap on the GPU (different streams, or
 //    different host threads without ordering) race on the array; serialise them.
-//  - The first call on a device looks up the array's device address with
-//    cudaGetSymbolAddress and sets kernel attributes; make that first call
-//    before any stream capture begins.
+//  - Every call looks up the array's device address on the current device with
+//    cudaGetSymbolAddress (no allocation, not a stream operation), so a device
+//    reset or a new primary context between calls is harmless, and sets the
+//    kernel attributes of its stream count.
+//  - Every call copies the quadrature tables and the defaults of absent scalar
+//    inputs from pageable host memory into the array; such copies are staged by
+//    the driver before the call returns, so the call is not fully asynchronous
+//    with respect to the host.
 #include <cuda_runtime.h>
 
 #include <cfloat>
 #include <cmath>
 #include <cstring>
-#include <mutex>
 #include <vector>
 
 #include "../../include/dsp.h"
@@ -47,11 +50,6 @@ constexpr size_t kScratchBytes = size_t(32) << 20;
 // The workspace.  In host code this name is only a stand-in symbol, never a
 // device address: the address comes from cudaGetSymbolAddress below.
 static __device__ __align__(256) unsigned char g_noalloc_scratch[kScratchBytes];
-
-constexpr int kMaxDevices = 64;
-std::mutex g_mu;
-void* g_scratch_ptr[kMaxDevices] = {};
-bool g_attr_done[kMaxDevices] = {};
 
 const int kSupported[] = {4, 6, 8, 10, 12, 14, 16, 32, 64};
 
@@ -176,33 +174,26 @@ dsp_status dsp_flux_bands_solve_noalloc(const dsp_flux_batch* batch_in, const ds
   const size_t per_inst = (size_t)il.stride + (size_t)L * lrec_stride(N) + (size_t)L * brec_stride(N);
   const size_t head = align256(16 * sizeof(double)) + align256((size_t)tab_size(N) * sizeof(double));
   const size_t per_inst_bytes = per_inst * sizeof(double) + sizeof(int32_t);
-  if (head + align256(per_inst_bytes) + 256 > kScratchBytes) return DSP_ERR_NO_MEMORY;  // one instance too big
-  const size_t room = kScratchBytes - head - 512;
-  const int64_t chunk = (int64_t)(room / per_inst_bytes) < n ? (int64_t)(room / per_inst_bytes) : n;
+  // room for the status words (rounded up to 256 bytes) and the records of
+  // `chunk` instances; at least one instance must fit before any work is queued
+  const size_t room = kScratchBytes > head + 512 ? kScratchBytes - head - 512 : 0;
+  const int64_t fit = (int64_t)(room / per_inst_bytes);
+  if (fit < 1) return DSP_ERR_NO_MEMORY;  // one instance is too big for the array
+  const int64_t chunk = fit < n ? fit : n;
 
-  int dev = 0;
-  if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= kMaxDevices) return DSP_ERR_CUDA;
-  unsigned char* base = nullptr;
-  {
-    std::lock_guard<std::mutex> lk(g_mu);
-    if (!g_scratch_ptr[dev]) {
-      void* ptr = nullptr;
-      if (cudaGetSymbolAddress(&ptr, g_noalloc_scratch) != cudaSuccess || !ptr) {
-        cudaGetLastError();
-        return DSP_ERR_CUDA;
-      }
-      g_scratch_ptr[dev] = ptr;
-    }
-    if (!g_attr_done[dev]) {
-      for (int sN : kSupported) run_for(sN, true, nullptr, nullptr, nullptr);
-      g_attr_done[dev] = true;
-    }
-    base = static_cast<unsigned char*>(g_scratch_ptr[dev]);
+  // the array's address on the current device, looked up on every call
+  void* ptr = nullptr;
+  if (cudaGetSymbolAddress(&ptr, g_noalloc_scratch) != cudaSuccess || !ptr) {
+    cudaGetLastError();
+    return DSP_ERR_CUDA;
   }
+  unsigned char* base = static_cast<unsigned char*>(ptr);
+  run_for(N, true, nullptr, nullptr, nullptr);  // kernel attributes of this stream count
+  if (cudaGetLastError() != cudaSuccess) return DSP_ERR_CUDA;
   cudaStream_t s = static_cast<cudaStream_t>(stream);
 
   // defaults of absent scalar fields (DisortFluxConfig.hpp:30-44) and the tables;
-  // the copies read pageable host memory, so they complete before returning
+  // the copies read pageable host memory, so the driver stages them before returning
   static const double kDefaults[14] = {0, 0, 0, 0, 0, 0, 0.0, 1.0, 0.0, 0.5, 0.0, 0.0, 0.0, 0.0};
   double* d_def = reinterpret_cast<double*>(base);
   double* d_tab = reinterpret_cast<double*>(base + align256(16 * sizeof(double)));

@@ -5,7 +5,7 @@ These published coefficient tables must be identical to the reference's for the
 phase-function helpers to agree, so they are extracted from DisORT++
 src/PhaseFunction.cpp (fillHazeGarciaSiewert / fillCloudGarciaSiewert):
 
-    python disort_b200/csrc/host/make_phase_tables.py [/path/to/DisORT]
+    python disort_b200/csrc/host/make_phase_tables.py /path/to/DisORT
 """
 import os
 import re
@@ -18,7 +18,9 @@ def table(src: str, func: str, name: str) -> list:
 
 
 def main():
-    ref = sys.argv[1] if len(sys.argv) > 1 else "/root/reference"
+    if len(sys.argv) != 2:
+        sys.exit("usage: make_phase_tables.py /path/to/DisORT (the DisORT++ source tree)")
+    ref = sys.argv[1]
     src = open(os.path.join(ref, "src", "PhaseFunction.cpp")).read()
     haze = table(src, "fillHazeGarciaSiewert", "hazelm")
     cloud = table(src, "fillCloudGarciaSiewert", "cldmom")

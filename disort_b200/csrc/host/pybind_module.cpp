@@ -2,7 +2,7 @@
 //
 // Mirrors the reference module (src/python_bindings.cpp:213-763): the same
 // class, property, function and keyword names, the same immutable-tuple
-// getters for vector fields (RO_VEC1D/RO_VEC2D, :21-44), the GIL released around
+// getters for vector fields (:21-44), the GIL released around
 // solves.  Added: solve_flux_spectral_bands_arrays, which takes numpy arrays and
 // returns numpy arrays [n_bands, num_layers+1] without per-band objects.
 #include <pybind11/numpy.h>
@@ -14,20 +14,27 @@
 namespace py = pybind11;
 using namespace disortpp;
 
-#define RO_VEC1D(cls, field)                                                   \
-  def_property(                                                                \
-      #field, [](const cls& c) { return py::tuple(py::cast(c.field)); },       \
-      [](cls& c, const std::vector<double>& v) { c.field = v; })
+namespace {
 
-#define RO_VEC2D(cls, field)                                                    \
-  def_property(                                                                 \
-      #field,                                                                   \
-      [](const cls& c) {                                                        \
-        py::list outer;                                                         \
-        for (const auto& row : c.field) outer.append(py::tuple(py::cast(row))); \
-        return py::tuple(outer);                                                \
-      },                                                                        \
-      [](cls& c, const std::vector<std::vector<double>>& v) { c.field = v; })
+// Vector members read back as immutable tuples (a snapshot: element assignment on
+// the result cannot silently edit a temporary copy) and are replaced whole on
+// assignment, which is how the reference module exposes them.
+py::tuple as_tuple(const std::vector<double>& v) { return py::tuple(py::cast(v)); }
+py::tuple as_tuple(const std::vector<std::vector<double>>& v) {
+  py::tuple t(v.size());
+  for (size_t i = 0; i < v.size(); ++i) t[i] = as_tuple(v[i]);
+  return t;
+}
+template <class C, class V>
+auto tuple_getter(V C::*member) {
+  return [member](const C& c) { return as_tuple(c.*member); };
+}
+template <class C, class V>
+auto whole_setter(V C::*member) {
+  return [member](C& c, const V& v) { c.*member = v; };
+}
+
+}  // namespace
 
 namespace {
 
@@ -200,16 +207,16 @@ PYBIND11_MODULE(_disortpp, m) {
       .def_readwrite("wavenumber_high", &DisortConfig::wavenumber_high)
       .def_readwrite("accuracy_fourier_series", &DisortConfig::accuracy_fourier_series)
       .def_readwrite("bottom_radius", &DisortConfig::bottom_radius)
-      .RO_VEC1D(DisortConfig, delta_tau)
-      .RO_VEC1D(DisortConfig, single_scat_albedo)
-      .RO_VEC2D(DisortConfig, phase_function_moments)
-      .RO_VEC1D(DisortConfig, temperature)
-      .RO_VEC1D(DisortConfig, level_altitudes)
-      .RO_VEC1D(DisortConfig, tau_user)
-      .RO_VEC1D(DisortConfig, mu_user)
-      .RO_VEC1D(DisortConfig, phi_user)
-      .RO_VEC1D(DisortConfig, mu_phase_function)
-      .RO_VEC2D(DisortConfig, phase_function)
+      .def_property("delta_tau", tuple_getter(&DisortConfig::delta_tau), whole_setter(&DisortConfig::delta_tau))
+      .def_property("single_scat_albedo", tuple_getter(&DisortConfig::single_scat_albedo), whole_setter(&DisortConfig::single_scat_albedo))
+      .def_property("phase_function_moments", tuple_getter(&DisortConfig::phase_function_moments), whole_setter(&DisortConfig::phase_function_moments))
+      .def_property("temperature", tuple_getter(&DisortConfig::temperature), whole_setter(&DisortConfig::temperature))
+      .def_property("level_altitudes", tuple_getter(&DisortConfig::level_altitudes), whole_setter(&DisortConfig::level_altitudes))
+      .def_property("tau_user", tuple_getter(&DisortConfig::tau_user), whole_setter(&DisortConfig::tau_user))
+      .def_property("mu_user", tuple_getter(&DisortConfig::mu_user), whole_setter(&DisortConfig::mu_user))
+      .def_property("phi_user", tuple_getter(&DisortConfig::phi_user), whole_setter(&DisortConfig::phi_user))
+      .def_property("mu_phase_function", tuple_getter(&DisortConfig::mu_phase_function), whole_setter(&DisortConfig::mu_phase_function))
+      .def_property("phase_function", tuple_getter(&DisortConfig::phase_function), whole_setter(&DisortConfig::phase_function))
       .def("nmom_nstr", &DisortConfig::nmomNstr)
       .def("allocate", &DisortConfig::allocate)
       .def("validate", &DisortConfig::validate)
@@ -291,11 +298,11 @@ PYBIND11_MODULE(_disortpp, m) {
       .def_readwrite("wavenumber_low", &DisortFluxConfig::wavenumber_low)
       .def_readwrite("wavenumber_high", &DisortFluxConfig::wavenumber_high)
       .def_readwrite("bottom_radius", &DisortFluxConfig::bottom_radius)
-      .RO_VEC1D(DisortFluxConfig, delta_tau)
-      .RO_VEC1D(DisortFluxConfig, single_scat_albedo)
-      .RO_VEC2D(DisortFluxConfig, phase_function_moments)
-      .RO_VEC1D(DisortFluxConfig, temperature)
-      .RO_VEC1D(DisortFluxConfig, level_altitudes)
+      .def_property("delta_tau", tuple_getter(&DisortFluxConfig::delta_tau), whole_setter(&DisortFluxConfig::delta_tau))
+      .def_property("single_scat_albedo", tuple_getter(&DisortFluxConfig::single_scat_albedo), whole_setter(&DisortFluxConfig::single_scat_albedo))
+      .def_property("phase_function_moments", tuple_getter(&DisortFluxConfig::phase_function_moments), whole_setter(&DisortFluxConfig::phase_function_moments))
+      .def_property("temperature", tuple_getter(&DisortFluxConfig::temperature), whole_setter(&DisortFluxConfig::temperature))
+      .def_property("level_altitudes", tuple_getter(&DisortFluxConfig::level_altitudes), whole_setter(&DisortFluxConfig::level_altitudes))
       .def("nmom_nstr", &DisortFluxConfig::nmomNstr)
       .def("allocate", &DisortFluxConfig::allocate)
       .def("validate", &DisortFluxConfig::validate)

@@ -6,9 +6,10 @@
  *
  * The entry points replace these reference interfaces (DisORT++):
  *   dsp_flux_bands_solve     <- solveFluxSpectralBandsImpl<N> / DisortFluxSolver<N>::solve
- *                               (src/python_bindings.cpp:170-211, src/FluxSolver.hpp:49)
- *   dsp_flux_spectral_solve  <- solveFluxSpectralImpl<N> (src/python_bindings.cpp:148-168);
- *                               same batch with wavenumber_low == wavenumber_high
+ *                               (src/python_bindings.cpp:170-211, src/FluxSolver.hpp:49);
+ *                               also solveFluxSpectralImpl<N> (src/python_bindings.cpp:148-168):
+ *                               a single-wavenumber loop is the same call with
+ *                               wavenumber_low == wavenumber_high per instance
  *   dsp_general_bands_solve  <- solveSpectralBands / DisortSolver::solve
  *                               (src/python_bindings.cpp:108-127, src/DisortSolver.hpp:87)
  *
@@ -200,14 +201,16 @@ dsp_status dsp_general_bands_solve(dsp_context ctx, const dsp_general_batch* bat
  * kernels as dsp_flux_bands_solve with a workspace compiled into libdsp.so: a
  * 32 MiB device array (dsp_noalloc_scratch_bytes()) that each GPU loading the
  * library keeps until exit.  Needs no context; all batch and output pointers
- * must be device memory (DSP_FLAG_DEVICE_POINTERS).  Work is queued on `stream`
- * (a cudaStream_t, NULL = legacy default) and not waited for.  An instance whose
- * workspace exceeds the array is rejected with DSP_ERR_NO_MEMORY before anything
- * runs; larger batches reuse the array in several launches.  All calls share the
- * array and it keeps the last call's contents: calls that may overlap on the GPU
- * race and must be serialised by the caller.  The first call on a device looks
- * up the array's address and sets kernel attributes; make it before any stream
- * capture.
+ * must be device memory (DSP_FLAG_DEVICE_POINTERS).  The kernels are queued on
+ * `stream` (a cudaStream_t, NULL = legacy default) and not waited for; the small
+ * copies of the quadrature tables and of the defaults of absent scalar inputs come
+ * from pageable host memory, which the driver stages before the call returns.  An
+ * instance whose workspace exceeds the array is rejected with DSP_ERR_NO_MEMORY
+ * before anything is queued; larger batches reuse the array in several launches.
+ * All calls share the array and it keeps the last call's contents: calls that may
+ * overlap on the GPU race and must be serialised by the caller.  Every call looks
+ * up the array's address on the current device (cudaGetSymbolAddress), so no
+ * per-device state outlives a device reset.
  */
 int64_t dsp_noalloc_scratch_bytes(void);
 dsp_status dsp_flux_bands_solve_noalloc(const dsp_flux_batch* batch, const dsp_flux_out* out, void* stream);

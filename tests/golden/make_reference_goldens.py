@@ -1,8 +1,8 @@
 """Generate tests/golden/reference_goldens.json from the reference's own tests.
 
-Run in a container that has the DisORT++ sources (default path below):
+Run where the DisORT++ sources are available, giving their path:
 
-    python tests/golden/make_reference_goldens.py [/path/to/DisORT]
+    python tests/golden/make_reference_goldens.py /path/to/DisORT
 
 The reference's known-answer tests are C++ code (tests/test_solver.cpp).  This
 script pairs each selected TEST with a transcription of its configuration (the
@@ -162,7 +162,9 @@ def moments(phase, nmom_nstr: int, cloud: list) -> list:
 
 
 def main():
-    ref = sys.argv[1] if len(sys.argv) > 1 else "/root/reference"
+    if len(sys.argv) != 2:
+        sys.exit("usage: make_reference_goldens.py /path/to/DisORT (the DisORT++ source tree)")
+    ref = sys.argv[1]
     text = open(os.path.join(ref, "tests", "test_solver.cpp")).read()
     cloud = cloud_table(open(os.path.join(ref, "src", "PhaseFunction.cpp")).read())
     bodies = test_bodies(text)
