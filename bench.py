@@ -88,29 +88,51 @@ def cpu_oracle():
     return lib
 
 
-def cpu_time(lib, w, threads):
+def cpu_time(lib, w, threads, keep_outputs=False):
     batch, keep = workloads.make_batch(w)
     outs, status = capi.alloc_flux_out_numpy(w["n_inst"], w["num_layers"])
     o, keep2 = capi.make_flux_out(outs, status)
     t0 = time.perf_counter()
     lib.oracle_flux_bands_solve(ctypes.byref(batch), ctypes.byref(o), threads)
-    return time.perf_counter() - t0
+    t = time.perf_counter() - t0
+    return (t, outs, status) if keep_outputs else t
 
 
 def cpu_baseline(w, target_s: float):
+    """The oracle on the host's threads over the whole sweep when that takes at
+    most a few times `target_s` (else an evenly spaced sample sized to it).
+    Returns (cpu_baseline dict, band indices solved, oracle outputs)."""
     lib = cpu_oracle()
     threads = os.cpu_count() or 1
     probe = workloads.subset(w, np.arange(0, w["n_inst"], max(1, w["n_inst"] // (4 * threads)))[: 4 * threads])
     cpu_time(lib, probe, threads)  # warm-up
     t = cpu_time(lib, probe, threads)
     rate = probe["n_inst"] / t
-    m = int(min(w["n_inst"], max(threads, rate * target_s)))
+    m = w["n_inst"] if w["n_inst"] / rate <= 4 * target_s else int(max(threads, rate * target_s))
     idx = np.linspace(0, w["n_inst"] - 1, m).astype(np.int64)
-    sample = workloads.subset(w, idx)
-    t = cpu_time(lib, sample, threads)
+    sample = workloads.subset(w, idx) if m < w["n_inst"] else w
+    t, outs, status = cpu_time(lib, sample, threads, keep_outputs=True)
+    what = "all" if m == w["n_inst"] else f"{m} of"
     return dict(value=m / t, unit="solves/s", cores=threads, kind="port",
-                sample=f"{m} of {w['n_inst']} bands evenly spaced across the sweep, "
-                       f"oracle built -march=native, {threads} OpenMP threads, {t:.1f} s"), lib
+                sample=f"{what} {w['n_inst']} bands{'' if m == w['n_inst'] else ' evenly spaced across the sweep'}, "
+                       f"oracle built -march=native, {threads} OpenMP threads, {t:.1f} s"), idx, (outs, status)
+
+
+def parity_of(gpu_outs: dict, idx, ref, rtol=1e-9, atol=1e-12) -> dict:
+    """Element-wise |gpu - oracle| / (rtol |oracle| + atol) over the solved bands
+    (<= 1 passes), every FluxResult field."""
+    outs, status = ref
+    worst, where = 0.0, None
+    for f in capi.FLUX_OUT_FIELDS:
+        a, b = np.asarray(gpu_outs[f])[idx], np.asarray(outs[f])
+        r = np.abs(a - b) / (rtol * np.abs(b) + atol)
+        r = np.where(np.isnan(a) & np.isnan(b), 0.0, np.where(np.isnan(r), np.inf, r))
+        k = float(r.max())
+        if k > worst:
+            worst, where = k, f + str(tuple(int(x) for x in np.unravel_index(int(np.argmax(r)), r.shape)))
+    return {"max_ratio": worst, "at": where, "rtol": rtol, "atol": atol, "bands_compared": int(len(idx)),
+            "fields": list(capi.FLUX_OUT_FIELDS), "oracle_bad_status": int((np.asarray(status) != 0).sum()),
+            "passes": worst <= 1.0}
 
 
 def run_reference(args):
@@ -217,6 +239,9 @@ def committed_traffic(workload_name: str, kernel: str):
 
 
 def run_e2e(args, ctx, w, douts, stream, dev, world):
+    """Same solve through the C ABI with pinned host buffers: inputs up, results
+    down, inside the timed region.  Returns (solves/s, h2d bytes, d2h bytes,
+    results equal to the device-resident run)."""
     import torch
     n, L, N = w["n_inst"], w["num_layers"], w["num_streams"]
     host_arrays = {}
@@ -332,10 +357,19 @@ def run_ours(args):
     value = replicas.job_rate(n, args.steps, world, ms_max)
 
     # ---- e2e: through the C ABI with pinned host buffers ----------------------
+    # the headline e2e sends one Henyey-Greenstein g per layer (DSP_FLAG_HG_G; the
+    # engine forms the moments on the device, bit-identical results); the same
+    # call with the full [L][17] moment array is reported beside it
     if args.no_e2e:
-        e2e_value, h2d, d2h, same = None, 0, 0, None
+        e2e_value, h2d, d2h, same, e2e_mom = None, 0, 0, None, None
     else:
-        e2e_value, h2d, d2h, same = run_e2e(args, ctx, w, douts, stream, dev, world)
+        w_e2e = workloads.as_hg(w) if "hg_g" in w else w
+        e2e_value, h2d, d2h, same = run_e2e(args, ctx, w_e2e, douts, stream, dev, world)
+        e2e_mom = None
+        if w_e2e is not w:
+            v, h, d, sm = run_e2e(args, ctx, w, douts, stream, dev, world)
+            e2e_mom = {"value": v, "unit": "solves/s", "h2d_bytes_per_step": h, "d2h_bytes_per_step": d,
+                       "matches_device_result": sm, "inputs": "full phase-function moments [L][17]"}
 
     # ---- roofline of the dominant kernel -----------------------------------
     beam = bool(np.any(np.asarray(w["arrays"]["direct_beam_flux"]) > 0))
@@ -356,16 +390,22 @@ def run_ours(args):
     }
 
     if rank == 0:
-        cpu = None if args.no_cpu else cpu_baseline(w, args.cpu_seconds)[0]
+        cpu, parity = None, None
+        if not args.no_cpu:
+            cpu, idx, ref = cpu_baseline(w, args.cpu_seconds)
+            parity = parity_of({f: v.cpu().numpy() for f, v in douts.items()}, idx, ref)
         line = {
             "metric": METRIC, "value": value, "unit": "solves/s", "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": ms_max / args.steps, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded PCG64)",
             "config": config_of(w, args, world),
             "e2e": {"value": e2e_value, "unit": "solves/s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
-                    "matches_device_result": same},
+                    "matches_device_result": same,
+                    "inputs": "one HG asymmetry factor per layer (DSP_FLAG_HG_G)" if "hg_g" in w else "moments"},
+            "e2e_full_moments": e2e_mom,
             "gpu_launches": int(sum(v[1] for v in ktimes.values())),
-            "roofline": roofline, "cpu_baseline": cpu, "clocks": clk, "bad_status_instances": bad,
+            "roofline": roofline, "cpu_baseline": cpu, "parity": parity, "clocks": clk,
+            "bad_status_instances": bad,
         }
         if not args.no_surrogate and world == 1:
             line["surrogate"] = surrogate_leg(ctx)
@@ -419,13 +459,36 @@ def general_oracle_lib():
     return lib
 
 
-def general_cpu_time(lib, insts, flags, threads):
+def general_cpu_time(lib, insts, flags, threads, keep_outputs=False):
     d = capi.pack_general(insts, flags, pmom_count=66)
     b, keep = capi.make_general_batch(d)
     outs, o, keep2 = capi.alloc_general_out_numpy(d)
     t0 = time.perf_counter()
     lib.oracle_general_bands_solve(ctypes.byref(b), ctypes.byref(o), threads)
-    return time.perf_counter() - t0
+    t = time.perf_counter() - t0
+    return (t, outs) if keep_outputs else t
+
+
+def general_parity(gpu: dict, idx, ref: dict, rtol=1e-9, atol=1e-12) -> dict:
+    """Fluxes element-wise; intensities against max(|value|, the instance's
+    largest |intensity|) (a Fourier sum whose terms cancel); <= 1 passes."""
+    worst, where = 0.0, None
+    for f in capi.FLUX_OUT_FIELDS + ("intensity", "intensity_azimuth_avg"):
+        a = np.asarray(gpu[f])[idx]
+        b = np.asarray(ref[f])
+        if f.startswith("intensity"):
+            flat = np.abs(np.nan_to_num(b)).reshape(b.shape[0], -1)
+            scale = flat.max(axis=1).reshape((-1,) + (1,) * (b.ndim - 1))
+            denom = rtol * np.maximum(np.abs(b), scale) + atol
+        else:
+            denom = rtol * np.abs(b) + atol
+        r = np.abs(a - b) / denom
+        r = np.where(np.isnan(a) & np.isnan(b), 0.0, np.where(np.isnan(r), np.inf, r))
+        k = float(r.max()) if r.size else 0.0
+        if k > worst:
+            worst, where = k, f + str(tuple(int(x) for x in np.unravel_index(int(np.argmax(r)), r.shape)))
+    return {"max_ratio": worst, "at": where, "rtol": rtol, "atol": atol, "instances_compared": int(len(idx)),
+            "passes": worst <= 1.0}
 
 
 def general_cpu_sample(insts, target_s: float):
@@ -438,7 +501,7 @@ def general_cpu_sample(insts, target_s: float):
     t = general_cpu_time(lib, probe, flags, threads)
     m = int(min(n, max(threads, len(probe) * target_s / max(t, 1e-6))))
     idx = np.linspace(0, n - 1, m).astype(int)
-    return lib, [insts[k] for k in idx], flags, threads
+    return lib, [insts[k] for k in idx], flags, threads, idx
 
 
 def run_general(args):
@@ -449,7 +512,7 @@ def run_general(args):
         if rank != 0:
             return
         insts, flags = workloads.general_mix(n, seed=3)
-        lib, sample, flags, threads = general_cpu_sample(insts, min(20.0, 150.0 / max(1, args.steps + args.warmup)))
+        lib, sample, flags, threads, _ = general_cpu_sample(insts, min(20.0, 150.0 / max(1, args.steps + args.warmup)))
         for _ in range(args.warmup):
             general_cpu_time(lib, sample, flags, threads)
         ts = [general_cpu_time(lib, sample, flags, threads) for _ in range(args.steps)]
@@ -565,13 +628,14 @@ def run_general(args):
                 "kernel_ms_per_step": {k: v[0] / args.steps for k, v in ktimes.items()},
                 "all_kernels_tflops": fl["total"] * args.steps / (ms_max / 1000.0) / 1e12}
     if rank == 0:
-        cpu = None
+        cpu, parity = None, None
         if not args.no_cpu:
-            lib, sample, flags, threads = general_cpu_sample(insts, args.cpu_seconds)
-            tcpu = general_cpu_time(lib, sample, flags, threads)
+            lib, sample, flags, threads, idx = general_cpu_sample(insts, args.cpu_seconds)
+            tcpu, ref = general_cpu_time(lib, sample, flags, threads, keep_outputs=True)
             cpu = {"value": len(sample) / tcpu, "unit": "solves/s", "cores": threads, "kind": "port",
                    "sample": f"{len(sample)} of {n} instances evenly spaced, oracle -march=native, "
                              f"{threads} OpenMP threads, {tcpu:.1f} s"}
+            parity = general_parity({k: v.cpu().numpy() for k, v in douts.items()}, idx, ref)
         print(json.dumps({
             "metric": GENERAL_METRIC, "value": value, "unit": "solves/s", "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": ms_max / args.steps, "higher_is_better": True, "scaling": "weak",
@@ -580,7 +644,7 @@ def run_general(args):
                        "parallelism": f"replicas x{world}" if world > 1 else "single GPU",
                        "l2": "workspace larger than L2; no flush needed"},
             "e2e": e2e, "gpu_launches": int(sum(v[1] for v in ktimes.values())), "roofline": roofline,
-            "cpu_baseline": cpu, "clocks": clk, "bad_status_instances": bad}), flush=True)
+            "cpu_baseline": cpu, "parity": parity, "clocks": clk, "bad_status_instances": bad}), flush=True)
     ctx.close()
     replicas.finish()
 

@@ -40,6 +40,7 @@ FLAG_INDEX_FROM_BOTTOM = 1 << 3
 FLAG_DEVICE_POINTERS = 1 << 4
 FLAG_SPHERICAL_BEAM = 1 << 5
 FLAG_TEMPERATURE_JAC = 1 << 6
+FLAG_HG_G = 1 << 7
 
 GFLAG_USER_TAU = 1 << 8
 GFLAG_USER_MU = 1 << 9
@@ -109,6 +110,8 @@ def make_flux_batch(n_inst: int, num_streams: int, num_layers: int, num_phase_fu
     per_ndim = {  # dimensions of one instance's value
         "delta_tau": 1, "single_scat_albedo": 1, "phase_function_moments": 2, "temperature": 1,
     }
+    if flags & FLAG_HG_G:  # one asymmetry factor per layer instead of moments
+        per_ndim["phase_function_moments"] = 1
     b = FluxBatch()
     b.n_inst = n_inst
     b.num_streams = num_streams

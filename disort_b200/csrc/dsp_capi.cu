@@ -117,7 +117,8 @@ dsp_status launch_flux(dsp_context ctx, int N, const FluxParams& p, cudaStream_t
 // elements of one instance's value for each batch array, in FLUX field order
 void per_inst_counts(const dsp_flux_batch* b, int64_t cnt[14]) {
   const int L = b->num_layers;
-  const int64_t c[14] = {1, 1, L, L, (int64_t)L * b->pmom_count, L + 1, 1, 1, 1, 1, 1, 1, 1, 1};
+  const int64_t pm = (b->flags & DSP_FLAG_HG_G) ? (int64_t)L : (int64_t)L * b->pmom_count;
+  const int64_t c[14] = {1, 1, L, L, pm, L + 1, 1, 1, 1, 1, 1, 1, 1, 1};
   for (int k = 0; k < 14; ++k) cnt[k] = c[k];
 }
 
@@ -229,7 +230,8 @@ dsp_status dsp_context_timing_get(dsp_context ctx, int32_t idx, const char** nam
 
 int64_t dsp_flux_workspace_bytes(const dsp_flux_batch* b) {
   if (!b || b->num_layers <= 0 || !supported_nstr(b->num_streams)) return -1;
-  const Sizes s = sizes_for(b->num_streams, b->num_layers);
+  Sizes s = sizes_for(b->num_streams, b->num_layers);
+  if (b->flags & DSP_FLAG_HG_G) s.inst += (size_t)round4(b->num_layers * b->pmom_count);
   return (int64_t)s.per_inst_bytes() * (int64_t)b->n_inst;
 }
 
@@ -336,7 +338,11 @@ dsp_status dsp_flux_bands_solve(dsp_context ctx, const dsp_flux_batch* batch_in,
   if ((st = get_tables(ctx, N, &tables)) != DSP_OK) return st;
 
   // ---- workspace and chunking -------------------------------------------
-  const Sizes sz = sizes_for(N, L);
+  // with DSP_FLAG_HG_G every instance also holds its formed moments [L][pc]
+  const bool hg = (b.flags & DSP_FLAG_HG_G) != 0;
+  const size_t hg_doubles = hg ? (size_t)round4(L * b.pmom_count) : 0;  // keeps the records 32-byte aligned
+  Sizes sz = sizes_for(N, L);
+  sz.inst += hg_doubles;
   const size_t inst_doubles = sz.inst + sz.layer + sz.bvp;
   size_t budget = workspace_budget();
   size_t freeb = 0, totalb = 0;
@@ -372,6 +378,17 @@ dsp_status dsp_flux_bands_solve(dsp_context ctx, const dsp_flux_batch* batch_in,
       p.bvp_rec = p.layer_rec + (size_t)m * sz.layer;
       for (int f = 0; f < 8; ++f) p.out[f] = dout[f] + off * nlev;
       p.status = dstatus + off;
+      if (hg) {  // g per layer -> moments at the end of the instance-record area
+        double* mom = wsb + (size_t)m * (sz.inst - hg_doubles);
+        const long long rows = m * (long long)L;
+        const long long threads = rows * p.pc;
+        {
+          KernelTimer kt(ctx, "hg_moments_kernel", cs);
+          hg_moments_kernel<<<(unsigned)((threads + 255) / 256), 256, 0, cs>>>(p.pmom, rows, L, p.pc, mom);
+        }
+        p.pmom.p = mom;
+        p.pmom.s = (long long)L * p.pc;
+      }
       dsp_status rs = launch_flux(ctx, N, p, cs);
       if (rs != DSP_OK) return rs;
     }

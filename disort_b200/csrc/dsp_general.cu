@@ -186,6 +186,8 @@ extern "C" dsp_status dsp_general_bands_solve(dsp_context ctx, const dsp_general
   const uint32_t fl = b.flags;
   if (fl & (DSP_FLAG_SPHERICAL_BEAM | DSP_FLAG_TEMPERATURE_JAC))
     return fail(ctx, DSP_ERR_UNSUPPORTED, "spherical beam and temperature Jacobians are not in this engine");
+  if (fl & DSP_FLAG_HG_G)
+    return fail(ctx, DSP_ERR_UNSUPPORTED, "the Henyey-Greenstein g fast path is a flux-batch option");
   const bool thermal = (fl & DSP_FLAG_THERMAL) != 0;
   const bool user_tau = (fl & DSP_GFLAG_USER_TAU) != 0, user_mu = (fl & DSP_GFLAG_USER_MU) != 0;
   const bool only_fluxes = (fl & DSP_GFLAG_ONLY_FLUXES) != 0;

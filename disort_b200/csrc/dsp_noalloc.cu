@@ -157,7 +157,7 @@ dsp_status dsp_flux_bands_solve_noalloc(const dsp_flux_batch* batch_in, const ds
   bool ok = false;
   for (int sN : kSupported) ok = ok || sN == N;
   if (!ok) return DSP_ERR_UNSUPPORTED;
-  if (b.flags & (DSP_FLAG_SPHERICAL_BEAM | DSP_FLAG_TEMPERATURE_JAC)) return DSP_ERR_UNSUPPORTED;
+  if (b.flags & (DSP_FLAG_SPHERICAL_BEAM | DSP_FLAG_TEMPERATURE_JAC | DSP_FLAG_HG_G)) return DSP_ERR_UNSUPPORTED;
   const int nmomnstr = b.num_phase_func_moments > N ? b.num_phase_func_moments : N;
   if (b.num_phase_func_moments < 0 || b.pmom_count < nmomnstr + 1) return DSP_ERR_INVALID_INPUT;
   if (!b.delta_tau.ptr || !b.single_scat_albedo.ptr || !b.phase_function_moments.ptr) return DSP_ERR_INVALID_INPUT;

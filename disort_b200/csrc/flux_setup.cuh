@@ -68,6 +68,24 @@ static __device__ double planck2(double lo, double hi, double T, const PlanckCon
   return ans;
 }
 
+// Henyey-Greenstein moments of a DSP_FLAG_HG_G batch: moment k of (instance i,
+// layer lc) is g^k formed by k successive products from 1, the order of
+// fillHenyeyGreenstein (PhaseFunction.cpp:6-19), so it equals a host-side fill
+// bit for bit.  One thread per output element: consecutive threads write
+// consecutive doubles of out[i][lc][k].
+static __global__ void __launch_bounds__(256) hg_moments_kernel(DArr g, long long n_rows, int L, int pc,
+                                                                double* out) {
+  const long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  if (t >= n_rows * pc) return;
+  const long long row = t / pc;
+  const int k = (int)(t - row * pc);
+  const long long i = row / L;
+  const double gv = g(i, row - i * L);
+  double gk = 1.0;
+  for (int j = 0; j < k; ++j) gk *= gv;
+  out[t] = gk;
+}
+
 // Four instances per 128-thread CTA, one warp each.
 static __global__ void __launch_bounds__(128) flux_setup_kernel(FluxParams p) {
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;

@@ -75,7 +75,7 @@ def thermal_sweep(n_bands: int = 20000, num_layers: int = 60, num_streams: int =
     return dict(
         name=f"thermal_sweep_{n_bands}x{L}L_{N}str",
         n_inst=n_bands, num_streams=N, num_layers=L, num_phase_func_moments=0, pmom_count=pc,
-        flags=capi.FLAG_THERMAL,
+        flags=capi.FLAG_THERMAL, hg_g=g,
         arrays=dict(
             wavenumber_low=lo, wavenumber_high=hi, delta_tau=dtau, single_scat_albedo=ssa,
             phase_function_moments=pmom, temperature=temp, surface_albedo=0.05,
@@ -102,6 +102,20 @@ def subset(w: dict, idx) -> dict:
                 continue
         arrs[k] = a
     out["arrays"] = arrs
+    if isinstance(w.get("hg_g"), np.ndarray) and w["hg_g"].shape[0] == n:
+        out["hg_g"] = np.ascontiguousarray(w["hg_g"][idx])
+    return out
+
+
+def as_hg(w: dict) -> dict:
+    """The same workload through the Henyey-Greenstein fast path (DSP_FLAG_HG_G):
+    one asymmetry factor per layer instead of the moments g**k."""
+    out = dict(w)
+    out["flags"] = w["flags"] | capi.FLAG_HG_G
+    arrs = dict(w["arrays"])
+    arrs["phase_function_moments"] = w["hg_g"]
+    out["arrays"] = arrs
+    out["name"] = w["name"] + "_hg"
     return out
 
 

@@ -63,6 +63,16 @@ typedef enum dsp_status {
 #define DSP_FLAG_DEVICE_POINTERS    (1u << 4) /* every pointer is device memory */
 #define DSP_FLAG_SPHERICAL_BEAM     (1u << 5) /* use_spherical_beam: rejected, DSP_ERR_UNSUPPORTED */
 #define DSP_FLAG_TEMPERATURE_JAC    (1u << 6) /* compute_temperature_jacobian: rejected, DSP_ERR_UNSUPPORTED */
+/*
+ * Henyey-Greenstein fast path (flux batches): phase_function_moments holds ONE
+ * asymmetry factor g per layer ([L] per instance) instead of [L][pmom_count]
+ * moments, and the engine forms the moments g^k, k = 0 .. pmom_count-1, on the
+ * device with the products of setHenyeyGreenstein (fillHenyeyGreenstein,
+ * src/PhaseFunction.cpp:6-19), so the result equals the moment path fed with
+ * those moments bit for bit.  Cuts the upload of a host-buffer solve by a factor
+ * of about pmom_count on the moment array.
+ */
+#define DSP_FLAG_HG_G               (1u << 7)
 
 /* A strided double array: element (instance i, index k) = ptr[i * stride + k]. */
 typedef struct dsp_darray {

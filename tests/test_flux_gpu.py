@@ -196,3 +196,54 @@ def test_invalid_instances_are_flagged_not_fatal():
     assert np.all(np.isnan(got["flux_up"][[3, 6]]))
     ok = [0, 1, 2, 4, 5, 7]
     assert_parity({k: v[ok] for k, v in got.items()}, {k: v[ok] for k, v in ref.items()}, "valid rows")
+
+
+@pytest.mark.parametrize("nstr,L", [(32, 60), (32, 120), (64, 90), (64, 120)])
+def test_deep_columns_at_32_and_64_streams(nstr, L):
+    """The 32/64-stream kernels on deep columns: thermal sweep columns (no cut)
+    and beam-only delta-M+ columns where the absorption cut fires."""
+    w = workloads.thermal_sweep(n_bands=6, num_layers=L, num_streams=nstr, seed=60 + L)
+    got, gst, ref, rst = both(w)
+    assert np.all(gst == 0) and np.all(rst == 0)
+    assert_parity(got, ref, f"thermal N={nstr} L={L}")
+    rng = np.random.default_rng(70 + L + nstr)
+    n, pc = 6, nstr + 2
+    w = dict(n_inst=n, num_streams=nstr, num_layers=L, num_phase_func_moments=nstr + 1, pmom_count=pc,
+             flags=capi.FLAG_DELTA_M_PLUS,
+             arrays=dict(delta_tau=np.clip(rng.lognormal(-3, 2, (n, L)), 1e-6, 50),
+                         single_scat_albedo=rng.uniform(0, 0.99, (n, L)),
+                         phase_function_moments=workloads.hg_moments(rng.uniform(0.5, 0.95, (n, L)), pc),
+                         surface_albedo=rng.uniform(0, 0.6, n), direct_beam_flux=1.0,
+                         direct_beam_mu=rng.uniform(0.1, 1.0, n)))
+    got, gst, ref, rst = both(w)
+    assert np.all(gst == 0) and np.all(rst == 0)
+    assert_parity(got, ref, f"beam DM+ N={nstr} L={L}")
+
+
+def test_hg_fast_path_equals_moment_path():
+    """DSP_FLAG_HG_G (one g per layer, moments formed on the device) gives the
+    moment path's results bit for bit, through host and device pointers, and
+    with bottom-up indexing."""
+    w = workloads.subset(workloads.thermal_sweep(), np.arange(0, 20000, 50))
+    wh = workloads.as_hg(w)
+    for extra in (0, capi.FLAG_INDEX_FROM_BOTTOM):
+        ref, rst, rc = gpu_lib.flux_solve(w, extra_flags=extra)
+        assert rc == 0 and not rst.any()
+        got, gst, rc = gpu_lib.flux_solve(wh, extra_flags=extra)
+        assert rc == 0, gpu_lib.context().last_error()
+        assert not gst.any()
+        dgot, dgst, rc = gpu_lib.flux_solve_device(wh, extra_flags=extra)
+        assert rc == 0 and not dgst.any()
+        for f in capi.FLUX_OUT_FIELDS:
+            np.testing.assert_array_equal(got[f], ref[f])
+            np.testing.assert_array_equal(dgot[f], ref[f])
+    # a g shared by every instance (stride 0) and the 64-stream kernels
+    w = workloads.thermal_sweep(n_bands=8, num_layers=30, num_streams=64, seed=5)
+    wh = workloads.as_hg(w)
+    wh["arrays"]["phase_function_moments"] = w["hg_g"][0]
+    w["arrays"]["phase_function_moments"] = w["arrays"]["phase_function_moments"][0]
+    ref, rst, rc = gpu_lib.flux_solve(w)
+    got, gst, rc2 = gpu_lib.flux_solve(wh)
+    assert rc == rc2 == 0 and not gst.any()
+    for f in capi.FLUX_OUT_FIELDS:
+        np.testing.assert_array_equal(got[f], ref[f])

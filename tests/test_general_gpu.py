@@ -164,3 +164,36 @@ def test_general_device_pointers_match_host():
     assert rc2 == 0, gpu_lib.context().last_error()
     for f in host:
         np.testing.assert_array_equal(dev[f], host[f], err_msg=f)
+
+
+def config3_sample():
+    """A stratified sample of the ragged general mix at its own sizes: the mix's
+    real distribution (N in {4, 8, 16, 32, 64}, 10-120 layers, delta-M+, beam
+    only so the absorption cut fires, user optical depths top/middle/bottom, five
+    polar angles, four azimuths, every azimuth mode), four instances of each of
+    N = 4, 8, 16, and for N = 32 and 64 four deep columns (90 layers or more) and
+    one shallow one."""
+    insts, flags = workloads.general_mix(1200, seed=3)
+    pick = []
+    for N in (4, 8, 16):
+        pick += [i for i, p in enumerate(insts) if p["num_streams"] == N][:4]
+    for N in (32, 64):
+        pick += [i for i, p in enumerate(insts) if p["num_streams"] == N and p["num_layers"] >= 90][:4]
+        pick += [i for i, p in enumerate(insts) if p["num_streams"] == N and p["num_layers"] < 40][:1]
+    return [insts[i] for i in pick], flags
+
+
+def test_general_mix_at_full_sizes():
+    from disort_b200 import flops
+    insts, flags = config3_sample()
+    assert sum(p["num_layers"] >= 90 for p in insts if p["num_streams"] == 64) >= 4
+    cut = [flops.absorption_cut(p["delta_tau"], p["single_scat_albedo"], False) < p["num_layers"] for p in insts]
+    assert sum(cut) >= 5  # the absorption cut shortens several columns
+    got, ref, _ = both(insts, flags)
+    assert np.all(got["status"] == 0) and np.all(ref["status"] == 0)
+    assert_parity_general(got, ref, "general mix at full sizes")
+    # the same instances through device pointers give the same numbers
+    dgot, rc = gpu_lib.general_solve_device(capi.pack_general(insts, flags))
+    assert rc == 0
+    for f in got:
+        np.testing.assert_array_equal(got[f], dgot[f])
