@@ -16,17 +16,20 @@ from disort_b200 import capi
 
 REPO = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 ORACLE_DIR = os.path.join(REPO, "oracle")
-_LIB = None
+_LIBS = {}
 
 
-def load(native: bool = False):
-    """Load (building if needed) the oracle shared library."""
-    global _LIB
-    if _LIB is not None and not native:
-        return _LIB
-    target = "native" if native else "all"
-    path = os.path.join(ORACLE_DIR, "_native" if native else "", "liboracle_disort.so")
-    subprocess.run(["make", "-s", "-C", ORACLE_DIR, target], check=True)
+def load(native: bool = False, ext: bool = False):
+    """Load (building if needed) the oracle shared library: the portable build,
+    the -march=native build (native=True) or the extended-precision build
+    (ext=True: x87 intermediates, the checker for ill-conditioned cases)."""
+    key = "native" if native else ("ext" if ext else "all")
+    if key in _LIBS and not native:
+        return _LIBS[key]
+    path = {"native": os.path.join(ORACLE_DIR, "_native", "liboracle_disort.so"),
+            "ext": os.path.join(ORACLE_DIR, "liboracle_disort_ext.so"),
+            "all": os.path.join(ORACLE_DIR, "liboracle_disort.so")}[key]
+    subprocess.run(["make", "-s", "-C", ORACLE_DIR, key], check=True)
     lib = ctypes.CDLL(path)
     lib.oracle_flux_bands_solve.restype = c_int
     lib.oracle_flux_bands_solve.argtypes = [POINTER(capi.FluxBatch), POINTER(capi.FluxOut), c_int]
@@ -37,13 +40,13 @@ def load(native: bool = False):
     lib.oracle_general_bands_solve.restype = c_int
     lib.oracle_general_bands_solve.argtypes = [POINTER(capi.GeneralBatch), POINTER(capi.GeneralOut), c_int]
     if not native:
-        _LIB = lib
+        _LIBS[key] = lib
     return lib
 
 
-def flux_solve(w: dict, nthreads: int = 0, extra_flags: int = 0):
+def flux_solve(w: dict, nthreads: int = 0, extra_flags: int = 0, ext: bool = False):
     """Run the oracle on workload dict `w`; returns (outputs dict, status array)."""
-    lib = load()
+    lib = load(ext=ext)
     batch, keep = capi.make_flux_batch(w["n_inst"], w["num_streams"], w["num_layers"],
                                        w["num_phase_func_moments"], w["pmom_count"],
                                        w["flags"] | extra_flags, w["arrays"])
@@ -53,9 +56,9 @@ def flux_solve(w: dict, nthreads: int = 0, extra_flags: int = 0):
     return outs, status
 
 
-def general_solve(d: dict, nthreads: int = 0):
+def general_solve(d: dict, nthreads: int = 0, ext: bool = False):
     """Run the general oracle on a pack_general dict; returns the outputs dict."""
-    lib = load()
+    lib = load(ext=ext)
     batch, keep = capi.make_general_batch(d)
     outs, o, keep2 = capi.alloc_general_out_numpy(d)
     lib.oracle_general_bands_solve(ctypes.byref(batch), ctypes.byref(o), nthreads)

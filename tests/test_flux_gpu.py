@@ -17,8 +17,8 @@ pytestmark = pytest.mark.gpu
 CASES = golden_cases.load_cases()
 
 
-def both(w, extra_flags=0):
-    ref, rst = oracle_lib.flux_solve(w, extra_flags=extra_flags)
+def both(w, extra_flags=0, ext=False):
+    ref, rst = oracle_lib.flux_solve(w, extra_flags=extra_flags, ext=ext)
     got, gst, rc = gpu_lib.flux_solve(w, extra_flags=extra_flags)
     assert rc == 0, gpu_lib.context().last_error()
     return got, gst, ref, rst
@@ -201,11 +201,17 @@ def test_invalid_instances_are_flagged_not_fatal():
 @pytest.mark.parametrize("nstr,L", [(32, 60), (32, 120), (64, 90), (64, 120)])
 def test_deep_columns_at_32_and_64_streams(nstr, L):
     """The 32/64-stream kernels on deep columns: thermal sweep columns (no cut)
-    and beam-only delta-M+ columns where the absorption cut fires."""
+    and beam-only delta-M+ columns where the absorption cut fires.  The checker
+    is the oracle built with extended-precision intermediates: on these columns
+    double rounding inside the restatement itself moves small upward fluxes by
+    up to ~7e-9 relative (the GPU agrees with the extended build within 1e-9),
+    so the double build is held to 1e-8 of the extended one beside it."""
+    from parity import worst
     w = workloads.thermal_sweep(n_bands=6, num_layers=L, num_streams=nstr, seed=60 + L)
-    got, gst, ref, rst = both(w)
+    got, gst, ref, rst = both(w, ext=True)
     assert np.all(gst == 0) and np.all(rst == 0)
     assert_parity(got, ref, f"thermal N={nstr} L={L}")
+    assert worst(oracle_lib.flux_solve(w)[0], ref)[0] <= 10.0
     rng = np.random.default_rng(70 + L + nstr)
     n, pc = 6, nstr + 2
     w = dict(n_inst=n, num_streams=nstr, num_layers=L, num_phase_func_moments=nstr + 1, pmom_count=pc,
@@ -215,9 +221,10 @@ def test_deep_columns_at_32_and_64_streams(nstr, L):
                          phase_function_moments=workloads.hg_moments(rng.uniform(0.5, 0.95, (n, L)), pc),
                          surface_albedo=rng.uniform(0, 0.6, n), direct_beam_flux=1.0,
                          direct_beam_mu=rng.uniform(0.1, 1.0, n)))
-    got, gst, ref, rst = both(w)
+    got, gst, ref, rst = both(w, ext=True)
     assert np.all(gst == 0) and np.all(rst == 0)
     assert_parity(got, ref, f"beam DM+ N={nstr} L={L}")
+    assert worst(oracle_lib.flux_solve(w)[0], ref)[0] <= 10.0
 
 
 def test_hg_fast_path_equals_moment_path():

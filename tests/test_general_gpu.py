@@ -13,15 +13,15 @@ import golden_cases
 import gpu_lib
 import oracle_lib
 from disort_b200 import capi, workloads
-from parity import assert_parity_general
+from parity import assert_parity_general, worst_general
 
 pytestmark = pytest.mark.gpu
 CASES = golden_cases.load_cases()
 
 
-def both(insts, flags, accuracy=0.0):
+def both(insts, flags, accuracy=0.0, ext=False):
     d = capi.pack_general(insts, flags, accuracy_fourier_series=accuracy)
-    ref = oracle_lib.general_solve(d)
+    ref = oracle_lib.general_solve(d, ext=ext)
     got, rc = gpu_lib.general_solve(d)
     assert rc == 0, gpu_lib.context().last_error()
     return got, ref, d
@@ -189,9 +189,12 @@ def test_general_mix_at_full_sizes():
     assert sum(p["num_layers"] >= 90 for p in insts if p["num_streams"] == 64) >= 4
     cut = [flops.absorption_cut(p["delta_tau"], p["single_scat_albedo"], False) < p["num_layers"] for p in insts]
     assert sum(cut) >= 5  # the absorption cut shortens several columns
-    got, ref, _ = both(insts, flags)
+    # checker: the extended-precision oracle build (at 64 streams double rounding in
+    # the restatement reaches 1e-9 of some fluxes; the double build is held to 1e-8)
+    got, ref, d = both(insts, flags, ext=True)
     assert np.all(got["status"] == 0) and np.all(ref["status"] == 0)
     assert_parity_general(got, ref, "general mix at full sizes")
+    assert worst_general(oracle_lib.general_solve(d), ref)[0] <= 10.0
     # the same instances through device pointers give the same numbers
     dgot, rc = gpu_lib.general_solve_device(capi.pack_general(insts, flags))
     assert rc == 0

@@ -12,6 +12,7 @@ import pytest
 
 import golden_cases
 import oracle_lib
+from disort_b200 import capi
 
 CASES = golden_cases.load_cases()
 
@@ -51,3 +52,33 @@ def test_quadrature_and_planck_sanity():
     # single-wavenumber branch and zero-temperature branch
     assert lib.oracle_planck(1000.0, 1000.0, 300.0) > 0
     assert lib.oracle_planck(100.0, 200.0, 0.0) == 0.0
+
+
+def test_extended_precision_build_reproduces_goldens_and_double_build():
+    """The extended-precision build of the oracle (the checker of the deep 32/64
+    stream GPU cases) passes the same known-answer tests, and on deep 64-stream
+    columns the double build stays within 1e-8 of it (its own rounding reaches
+    ~7e-9 of small upward fluxes there)."""
+    from disort_b200 import workloads
+    from parity import worst
+    for case in CASES:
+        w = golden_cases.flux_workload(case)
+        out, st = oracle_lib.flux_solve(w, ext=True)
+        assert st[0] == 0
+        for e in case["expect_flux"]:
+            lev = golden_cases.level_of(case, e["index"])
+            if lev is not None:
+                assert abs(out[e["field"]][0, lev] - e["value"]) <= e["tol"]
+    rng = np.random.default_rng(254)
+    n, N, L = 6, 64, 120
+    pc = N + 2
+    w = dict(n_inst=n, num_streams=N, num_layers=L, num_phase_func_moments=N + 1, pmom_count=pc,
+             flags=capi.FLAG_DELTA_M_PLUS,
+             arrays=dict(delta_tau=np.clip(rng.lognormal(-3, 2, (n, L)), 1e-6, 50),
+                         single_scat_albedo=rng.uniform(0, 0.99, (n, L)),
+                         phase_function_moments=workloads.hg_moments(rng.uniform(0.5, 0.95, (n, L)), pc),
+                         surface_albedo=rng.uniform(0, 0.6, n), direct_beam_flux=1.0,
+                         direct_beam_mu=rng.uniform(0.1, 1.0, n)))
+    a, _ = oracle_lib.flux_solve(w)
+    b, _ = oracle_lib.flux_solve(w, ext=True)
+    assert worst(a, b)[0] <= 10.0
