@@ -77,6 +77,32 @@ class FluxOut(ctypes.Structure):
     _fields_ = [(f, POINTER(c_double)) for f in FLUX_OUT_FIELDS] + [("status", POINTER(c_int32))]
 
 
+# dsp_flux_jac_out: temperature Jacobians, each [n_inst][L+1][L+2]
+JAC_FIELDS = ("flux_up", "flux_down", "mean_intensity", "mean_intensity_down", "mean_intensity_up",
+              "flux_divergence")
+# the FluxResult output each Jacobian differentiates
+JAC_OF = dict(zip(JAC_FIELDS, ("flux_up", "flux_down", "mean_intensity", "mean_intensity_down",
+                               "mean_intensity_up", "flux_tau_divergence")))
+
+
+class FluxJacOut(ctypes.Structure):
+    _fields_ = [(f, POINTER(c_double)) for f in JAC_FIELDS]
+
+
+def make_flux_jac_out(arrays: dict) -> tuple[FluxJacOut, list]:
+    o = FluxJacOut()
+    keep = []
+    for f in JAC_FIELDS:
+        a = arrays[f]
+        keep.append(a)
+        setattr(o, f, ctypes.cast(c_void_p(_ptr(a)), POINTER(c_double)))
+    return o, keep
+
+
+def alloc_flux_jac_numpy(n_inst: int, num_layers: int) -> dict:
+    return {f: np.full((n_inst, num_layers + 1, num_layers + 2), np.nan) for f in JAC_FIELDS}
+
+
 def _ptr(a) -> int:
     if a is None:
         return 0

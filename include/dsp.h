@@ -62,7 +62,7 @@ typedef enum dsp_status {
 #define DSP_FLAG_INDEX_FROM_BOTTOM  (1u << 3) /* index_from_bottom (layer/level arrays reversed) */
 #define DSP_FLAG_DEVICE_POINTERS    (1u << 4) /* every pointer is device memory */
 #define DSP_FLAG_SPHERICAL_BEAM     (1u << 5) /* use_spherical_beam: rejected, DSP_ERR_UNSUPPORTED */
-#define DSP_FLAG_TEMPERATURE_JAC    (1u << 6) /* compute_temperature_jacobian: rejected, DSP_ERR_UNSUPPORTED */
+#define DSP_FLAG_TEMPERATURE_JAC    (1u << 6) /* compute_temperature_jacobian: use dsp_flux_bands_solve_jac */
 /*
  * Henyey-Greenstein fast path (flux batches): phase_function_moments holds ONE
  * asymmetry factor g per layer ([L] per instance) instead of [L][pmom_count]
@@ -120,6 +120,24 @@ typedef struct dsp_flux_out {
   double* mean_intensity_direct_beam;
   int32_t* status; /* [n_inst] or NULL */
 } dsp_flux_out;
+
+/*
+ * Temperature Jacobians of a flux solve (FluxResult's *_temperature_jac fields,
+ * FluxResult.hpp; computeThermalJacobian, src/FluxSolver.cpp:1294-1497).  Each
+ * array is [n_inst][L+1][L+2]: row = output level (indexed like the fluxes),
+ * column = level temperature 0..L (reversed with the levels under
+ * DSP_FLAG_INDEX_FROM_BOTTOM), then the surface temperature (temperature_bottom)
+ * in column L+1.  Units: output per kelvin.  Without DSP_FLAG_THERMAL every entry
+ * is zero (the reference returns empty Jacobians there).
+ */
+typedef struct dsp_flux_jac_out {
+  double* flux_up;
+  double* flux_down;
+  double* mean_intensity;
+  double* mean_intensity_down;
+  double* mean_intensity_up;
+  double* flux_divergence;
+} dsp_flux_jac_out;
 
 /*
  * General batch (DisortConfig, DisortConfig.hpp:119-243): the full DisortSolver
@@ -198,6 +216,15 @@ dsp_status dsp_context_timing_get(dsp_context ctx, int32_t idx, const char** nam
 /* Flux-only spectral-band solve (DisortFluxSolver<N> over every instance). */
 dsp_status dsp_flux_bands_solve(dsp_context ctx, const dsp_flux_batch* batch,
                                 const dsp_flux_out* out);
+
+/*
+ * Flux solve with temperature Jacobians (DisortFluxSolver<N>::solve with
+ * compute_temperature_jacobian, src/FluxSolver.cpp:1294-1497): the fluxes of
+ * dsp_flux_bands_solve plus `jac`.  The batch flag DSP_FLAG_TEMPERATURE_JAC is
+ * implied; dsp_flux_bands_solve itself rejects that flag.
+ */
+dsp_status dsp_flux_bands_solve_jac(dsp_context ctx, const dsp_flux_batch* batch,
+                                    const dsp_flux_out* out, const dsp_flux_jac_out* jac);
 
 /* General spectral-band solve (DisortSolver::solve over every instance). */
 dsp_status dsp_general_bands_solve(dsp_context ctx, const dsp_general_batch* batch,

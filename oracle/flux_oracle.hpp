@@ -18,6 +18,7 @@ struct FluxInstance {
   int num_layers = 0, num_streams = 0, num_phase_func_moments = 0;
   int pmom_count = 0;  // stride of pmom per layer
   bool thermal = false, delta_m_plus = false, diffusion_lower_bc = false, index_from_bottom = false;
+  bool temperature_jac = false;  // compute_temperature_jacobian
   double wavenumber_low = 0, wavenumber_high = 0;
   double surface_albedo = 0, emissivity_top = 1, direct_beam_flux = 0, direct_beam_mu = 0.5;
   double isotropic_flux_top = 0, isotropic_flux_bottom = 0, temperature_top = 0, temperature_bottom = 0;
@@ -29,6 +30,10 @@ struct FluxInstance {
 
 struct FluxOutput {  // each [L+1]
   double *fdir, *fdn, *fup, *dfdt, *uavg, *uavgdn, *uavgup, *uavgso;
+  // temperature Jacobians (FluxResult *_temperature_jac), each [L+1][L+2] or null:
+  // flux_up, flux_down, mean_intensity, mean_intensity_down, mean_intensity_up,
+  // flux_divergence
+  double* jac[6] = {nullptr, nullptr, nullptr, nullptr, nullptr, nullptr};
 };
 
 // DisortFluxConfig::validate (DisortFluxConfig.cpp:43-143) for the fields the
@@ -224,6 +229,7 @@ class FluxOracle {
   int solve(const FluxInstance& cfg_in, const FluxOutput& out);
 
  private:
+  void thermal_jacobian(const FluxInstance& cfg, const FluxOutput& out, int lda, int nc, int ncd);
   int N = 0, NN = 0, L = 0, ncut = 0;
   bool lyrcut = false, deltam = false, deltam_plus = false;
   // quadrature (FluxSolver.cpp:257-290, 442-445)
@@ -232,6 +238,10 @@ class FluxOracle {
   std::vector<double> beam_tr;                  // [L+1]
   std::vector<double> kk, G, C;                 // kk[L][N], G[L][N][N], C[L][N][N]
   std::vector<double> zb, z0, z1, xr0, xr1;     // particular solutions
+  // derivatives of the thermal source w.r.t. the layer's top / bottom level
+  // Planck values (computeIsotropicSource, FluxSolver.cpp:786-829)
+  std::vector<double> dz0t, dz0b, dz1t, dz1b, dxr0t, dxr0b, dxr1t, dxr1b;
+  std::vector<double> jb, jll;  // Jacobian right-hand side and its reordered solution
   std::vector<double> band, rhs, cc;            // BVP
   std::vector<int> ipvt;
   double planck_top = 0, planck_bottom = 0, planck_bottom_deriv = 0;
@@ -250,6 +260,8 @@ inline int FluxOracle::solve(const FluxInstance& cfg_in, const FluxOutput& out) 
       out.fdir[i] = out.fdn[i] = out.fup[i] = out.dfdt[i] = std::nan("");
       out.uavg[i] = out.uavgdn[i] = out.uavgup[i] = out.uavgso[i] = std::nan("");
     }
+    if (out.jac[0])
+      for (double* J : out.jac) std::fill(J, J + (size_t)nlev * (L + 2), std::nan(""));
   };
   if (L <= 0 || N < 4 || N % 2 != 0 || N > 64) { if (L > 0) fill_nan(); return DSP_ERR_INVALID_INPUT; }
   // index_from_bottom: reverse layer/level inputs (IndexConversion.hpp:42-52)
@@ -462,6 +474,11 @@ inline int FluxOracle::solve(const FluxInstance& cfg_in, const FluxOutput& out) 
 
   // Thermal particular solution (computeIsotropicSource, FluxSolver.cpp:745-831)
   z0.assign((size_t)L * N, 0.0); z1.assign((size_t)L * N, 0.0); xr0.assign(L, 0.0); xr1.assign(L, 0.0);
+  const bool want_jac = cfg.temperature_jac && cfg.thermal && out.jac[0];
+  if (want_jac) {
+    for (auto* v : {&dz0t, &dz0b, &dz1t, &dz1b}) v->assign((size_t)L * N, 0.0);
+    for (auto* v : {&dxr0t, &dxr0b, &dxr1t, &dxr1b}) v->assign(L, 0.0);
+  }
   if (cfg.thermal) {
     std::vector<double> pkag(L + 1), b(N), zz1(N);
     for (int lev = 0; lev <= L; ++lev)
@@ -486,6 +503,33 @@ inline int FluxOracle::solve(const FluxInstance& cfg_in, const FluxOutput& out) 
         z0[(size_t)lc * N + NN - iq - 1] = b[iq + NN];
         z1[(size_t)lc * N + NN + iq] = zz1[iq];
         z1[(size_t)lc * N + NN - iq - 1] = zz1[iq + NN];
+      }
+      if (want_jac) {
+        // d/d(pkag[lc]) and d/d(pkag[lc+1]) with the same factorisation
+        // (FluxSolver.cpp:789-829)
+        const double omm = 1.0 - ssa_s[lc], tc = tau_s[lc];
+        double d1t = 0.0, d1b = 0.0;
+        if (dtau_s[lc] > 1e-4) {
+          d1t = -1.0 / dtau_s[lc];
+          d1b = 1.0 / dtau_s[lc];
+        }
+        const double d0t = 1.0 - d1t * tc, d0b = -d1b * tc;
+        dxr0t[lc] = d0t; dxr0b[lc] = d0b; dxr1t[lc] = d1t; dxr1b[lc] = d1b;
+        for (int side = 0; side < 2; ++side) {
+          const double d1 = side ? d1b : d1t, d0 = side ? d0b : d0t;
+          for (int i = 0; i < N; ++i) zz1[i] = omm * d1;
+          lu_solve(A.data(), N, N, piv.data(), zz1.data());
+          for (int i = 0; i < N; ++i) b[i] = omm * d0 + mu[i] * zz1[i];
+          lu_solve(A.data(), N, N, piv.data(), b.data());
+          std::vector<double>& D0 = side ? dz0b : dz0t;
+          std::vector<double>& D1 = side ? dz1b : dz1t;
+          for (int iq = 0; iq < NN; ++iq) {
+            D0[(size_t)lc * N + NN + iq] = b[iq];
+            D0[(size_t)lc * N + NN - iq - 1] = b[iq + NN];
+            D1[(size_t)lc * N + NN + iq] = zz1[iq];
+            D1[(size_t)lc * N + NN - iq - 1] = zz1[iq + NN];
+          }
+        }
       }
     }
   }
@@ -705,11 +749,174 @@ inline int FluxOracle::solve(const FluxInstance& cfg_in, const FluxOutput& out) 
     out.uavg[lu] = ua; out.uavgdn[lu] = uad; out.uavgup[lu] = uau; out.uavgso[lu] = uaso;
     if (lu < L) tauc_lu += cfg.delta_tau[lu];
   }
+  if (out.jac[0]) {
+    const int ndof = L + 2;
+    for (double* J : out.jac) std::fill(J, J + (size_t)nlev * ndof, 0.0);
+    if (want_jac) thermal_jacobian(cfg, out, lda, nc, ncd);
+  }
   if (cfg.index_from_bottom) {
     for (double* a : {out.fdir, out.fdn, out.fup, out.dfdt, out.uavg, out.uavgdn, out.uavgup, out.uavgso})
       std::reverse(a, a + nlev);
+    // Jacobian rows reversed like the fluxes; level columns reversed, the
+    // surface column kept last (IndexConversion.hpp:55-68)
+    if (out.jac[0]) {
+      const int ndof = L + 2;
+      for (double* J : out.jac) {
+        for (int r = 0; r < nlev / 2; ++r)
+          std::swap_ranges(J + (size_t)r * ndof, J + (size_t)(r + 1) * ndof, J + (size_t)(L - r) * ndof);
+        for (int r = 0; r < nlev; ++r) std::reverse(J + (size_t)r * ndof, J + (size_t)r * ndof + L + 1);
+      }
+    }
   }
   return nonsing ? DSP_OK : DSP_ERR_SINGULAR;
+}
+
+// computeThermalJacobian (FluxSolver.cpp:1294-1497): dC = A^{-1} dB for every
+// level-Planck degree of freedom k = 0..L and the surface (column L+1), with the
+// band LU left by solve0, propagated to the six outputs per level and chained
+// with dB/dT (planckFunctionDeriv2).  Fills out.jac (top-down indexing).
+inline void FluxOracle::thermal_jacobian(const FluxInstance& cfg, const FluxOutput& out, int lda, int nc,
+                                         int ncd) {
+  const int ndof = L + 2, surf = L + 1;
+  auto at = [&](const std::vector<double>& v, int lc, int iq) { return v[(size_t)lc * N + iq]; };
+  auto dz0 = [&](int lc, int iq, int k) {
+    double r = 0.0;
+    if (k == lc) r += at(dz0t, lc, iq);
+    if (k == lc + 1) r += at(dz0b, lc, iq);
+    return r;
+  };
+  auto dz1 = [&](int lc, int iq, int k) {
+    double r = 0.0;
+    if (k == lc) r += at(dz1t, lc, iq);
+    if (k == lc + 1) r += at(dz1b, lc, iq);
+    return r;
+  };
+  auto dintc = [&](int lc, int k) {
+    double r = 0.0;
+    if (k == lc) r += dxr0t[lc];
+    if (k == lc + 1) r += dxr0b[lc];
+    return r;
+  };
+  auto dslp = [&](int lc, int k) {
+    double r = 0.0;
+    if (k == lc) r += dxr1t[lc];
+    if (k == lc + 1) r += dxr1b[lc];
+    return r;
+  };
+  const double dtau_last = dtau_s[L - 1];
+  const double tauc_bot = tau_s[ncut];
+  jb.assign(nc, 0.0);
+  jll.assign((size_t)N * L, 0.0);
+  std::vector<double> dexp(N), dval(N);
+  auto reorder = [&]() {
+    std::fill(jll.begin(), jll.end(), 0.0);
+    for (int lc = 0; lc < ncut; ++lc) {
+      const int ipnt = (lc + 1) * N - NN - 1;
+      for (int iq = 0; iq < NN; ++iq) {
+        const int b_idx = ipnt - iq;
+        if (b_idx >= 0 && b_idx < nc) jll[(size_t)lc * N + NN - iq - 1] = jb[b_idx];
+      }
+      for (int iq = 0; iq < NN; ++iq) {
+        const int b_idx = ipnt + iq + 1;
+        if (b_idx >= 0 && b_idx < nc) jll[(size_t)lc * N + NN + iq] = jb[b_idx];
+      }
+    }
+  };
+  auto propagate = [&](int k, int col, double chain) {
+    for (int lu = 0; lu <= L; ++lu) {
+      int lyu = (lu == 0) ? 0 : lu - 1;
+      if (lyrcut && lyu > ncut - 1) continue;
+      if (lyu >= ncut) lyu = ncut - 1;
+      const double utaupr = tau_s[lu];
+      const double tb = tau_s[lyu + 1], tt = tau_s[lyu];
+      for (int jq = 0; jq < NN; ++jq) dexp[jq] = jll[(size_t)lyu * N + jq] * std::exp(-kk[(size_t)lyu * N + jq] * (utaupr - tb));
+      for (int jq = NN; jq < N; ++jq) dexp[jq] = jll[(size_t)lyu * N + jq] * std::exp(-kk[(size_t)lyu * N + jq] * (utaupr - tt));
+      for (int i = 0; i < N; ++i) {
+        double sacc = 0.0;
+        for (int j = 0; j < N; ++j) sacc += G[(size_t)lyu * N * N + i * N + j] * dexp[j];
+        dval[i] = sacc;
+      }
+      if (k >= 0)
+        for (int iq = 0; iq < N; ++iq) dval[iq] += dz0(lyu, iq, k) + dz1(lyu, iq, k) * utaupr;
+      double dmi = 0.0, dmidn = 0.0, dmiup = 0.0, dfdn = 0.0, dfup = 0.0;
+      for (int iq = 0; iq < NN; ++iq) {
+        const int c = NN - iq - 1;
+        const double v = dval[iq], w = wt[c];
+        dmi += w * v; dmidn += w * v; dfdn += w * v * mu[c];
+      }
+      for (int iq = NN; iq < N; ++iq) {
+        const int c = iq - NN;
+        const double v = dval[iq], w = wt[c];
+        dmi += w * v; dmiup += w * v; dfup += w * v * mu[c];
+      }
+      dfup *= 2.0 * M_PI;
+      dfdn *= 2.0 * M_PI;
+      const double dmi_t = (2.0 * M_PI * dmi) / (4.0 * M_PI);
+      const double dmi_d = (2.0 * M_PI * dmidn) / (4.0 * M_PI);
+      const double dmi_u = (2.0 * M_PI * dmiup) / (4.0 * M_PI);
+      double dpls = 0.0;
+      if (k >= 0) dpls = dintc(lyu, k) + dslp(lyu, k) * utaupr;
+      const double dfdiv = (1.0 - cfg.ssa[lyu]) * 4.0 * M_PI * (dmi_t - dpls);
+      const size_t o = (size_t)lu * ndof + col;
+      out.jac[0][o] = chain * dfup;
+      out.jac[1][o] = chain * dfdn;
+      out.jac[2][o] = chain * dmi_t;
+      out.jac[3][o] = chain * dmi_d;
+      out.jac[4][o] = chain * dmi_u;
+      out.jac[5][o] = chain * dfdiv;
+    }
+  };
+  const double alb = cfg.surface_albedo;
+  for (int k = 0; k <= L; ++k) {
+    std::fill(jb.begin(), jb.end(), 0.0);
+    for (int iq = 0; iq < NN; ++iq) jb[iq] = -dz0(0, NN - 1 - iq, k);
+    if (cfg.diffusion_lower_bc) {
+      for (int iq = 0; iq < NN; ++iq) {
+        double sacc = -dz0(ncut - 1, NN + iq, k) - dz1(ncut - 1, NN + iq, k) * tauc_bot;
+        if (k == L - 1 && dtau_last > 0.0) sacc += mu[iq] * (-1.0 / dtau_last);
+        jb[nc - NN + iq] = sacc;
+      }
+    } else {
+      for (int iq = 0; iq < NN; ++iq) {
+        double sacc = 0.0;
+        if (!lyrcut) {
+          double refl = 0.0;
+          for (int jq = 0; jq < NN; ++jq) {
+            const double ps = dz0(ncut - 1, NN - 1 - jq, k) + dz1(ncut - 1, NN - 1 - jq, k) * tauc_bot;
+            refl += wt[jq] * mu[jq] * alb * ps;
+          }
+          sacc += 2.0 * refl;
+        }
+        sacc -= dz0(ncut - 1, NN + iq, k) + dz1(ncut - 1, NN + iq, k) * tauc_bot;
+        jb[nc - NN + iq] = sacc;
+      }
+    }
+    for (int lc = 1; lc < ncut; ++lc) {
+      const int ipnt = lc * N - NN;
+      const double tc = tau_s[lc];
+      for (int iq = 0; iq < N; ++iq)
+        jb[ipnt + iq] = dz0(lc, iq, k) - dz0(lc - 1, iq, k) + (dz1(lc, iq, k) - dz1(lc - 1, iq, k)) * tc;
+    }
+    band_solve(band.data(), lda, nc, ncd, ncd, ipvt.data(), jb.data());
+    reorder();
+    propagate(k, k, planck_function_deriv2(cfg.wavenumber_low, cfg.wavenumber_high, cfg.temperature[k]));
+  }
+  // surface degree of freedom: the emission (1 - albedo) B(T_bottom), or the
+  // diffusion boundary's B and its gradient
+  std::fill(jb.begin(), jb.end(), 0.0);
+  for (int iq = 0; iq < NN; ++iq) {
+    double sacc;
+    if (cfg.diffusion_lower_bc) {
+      sacc = 1.0;
+      if (dtau_last > 0.0) sacc += mu[iq] * (1.0 / dtau_last);
+    } else {
+      sacc = 1.0 - alb;  // Lambertian emissivity (FluxSolver.cpp:147-154)
+    }
+    jb[nc - NN + iq] = sacc;
+  }
+  band_solve(band.data(), lda, nc, ncd, ncd, ipvt.data(), jb.data());
+  reorder();
+  propagate(-1, surf, planck_function_deriv2(cfg.wavenumber_low, cfg.wavenumber_high, cfg.temperature_bottom));
 }
 
 }  // namespace oracle

@@ -23,7 +23,17 @@ inline double scalar(const dsp_darray& a, int64_t i, double dflt) {
 
 extern "C" {
 
+int oracle_flux_bands_solve_jac(const dsp_flux_batch* b, const dsp_flux_out* o, const dsp_flux_jac_out* jac,
+                                int nthreads);
+
 int oracle_flux_bands_solve(const dsp_flux_batch* b, const dsp_flux_out* o, int nthreads) {
+  if (b && (b->flags & DSP_FLAG_TEMPERATURE_JAC)) return DSP_ERR_UNSUPPORTED;
+  return oracle_flux_bands_solve_jac(b, o, nullptr, nthreads);
+}
+
+// The flux batch with optional temperature Jacobians (jac may be null).
+int oracle_flux_bands_solve_jac(const dsp_flux_batch* b, const dsp_flux_out* o, const dsp_flux_jac_out* jac,
+                                int nthreads) {
   if (!b || !o) return DSP_ERR_INVALID_INPUT;
   const int n = b->n_inst;
   const int L = b->num_layers;
@@ -63,8 +73,15 @@ int oracle_flux_bands_solve(const dsp_flux_batch* b, const dsp_flux_out* o, int 
                             o->flux_up + nlev * i, o->flux_tau_divergence + nlev * i,
                             o->mean_intensity + nlev * i, o->mean_intensity_down + nlev * i,
                             o->mean_intensity_up + nlev * i, o->mean_intensity_direct_beam + nlev * i};
+      if (jac) {
+        const int64_t js = nlev * (L + 2);
+        double* const jp[6] = {jac->flux_up, jac->flux_down, jac->mean_intensity, jac->mean_intensity_down,
+                               jac->mean_intensity_up, jac->flux_divergence};
+        for (int f = 0; f < 6; ++f) fo.jac[f] = jp[f] + js * i;
+        c.temperature_jac = true;
+      }
       int st;
-      if ((b->flags & (DSP_FLAG_SPHERICAL_BEAM | DSP_FLAG_TEMPERATURE_JAC)) != 0) {
+      if ((b->flags & DSP_FLAG_SPHERICAL_BEAM) != 0) {
         st = DSP_ERR_UNSUPPORTED;
       } else if (!c.delta_tau || !c.ssa || !c.pmom) {
         st = DSP_ERR_INVALID_INPUT;
@@ -174,6 +191,10 @@ int oracle_quadrature(int nstr, double* mu, double* w, double* ylm) {
 
 double oracle_planck(double wnumlo, double wnumhi, double temp) {
   return oracle::planck_function2(wnumlo, wnumhi, temp);
+}
+
+double oracle_planck_deriv(double wnumlo, double wnumhi, double temp) {
+  return oracle::planck_function_deriv2(wnumlo, wnumhi, temp);
 }
 
 }  // extern "C"

@@ -118,6 +118,34 @@ inline double planck_function2(double wnumlo, double wnumhi, double temp) {
   return planck_function(wnumlo, wnumhi, temp);
 }
 
+// planckFunctionDeriv2 (Planck.cpp:171-214): dB/dT of the band (or single
+// wavenumber) Planck function, from the closed form of the derivative of the
+// band integral (4 B / T minus the boundary terms of the integration limits).
+inline double planck_function_deriv2(double wnumlo, double wnumhi, double temp) {
+  using namespace planck_const;
+  if (temp < 0.0 || wnumhi < wnumlo || wnumlo < 0.0) return std::nan("");
+  if (temp < 1.e-4) return 0.0;
+  auto fkernel = [](double v) -> double {  // v^3 / (e^v - 1), v^2 near 0
+    if (v < 1.e-6) return v * v;
+    const double em = std::exp(-v);
+    return v * v * v * em / (1.0 - em);
+  };
+  if (wnumhi == wnumlo) {
+    const double wvn = wnumhi;
+    const double x = C2 * wvn / temp;
+    const double em = std::exp(-x);
+    const double b = planck_data().c1 * wvn * wvn * wvn * em / (1.0 - em);
+    return b * (x / temp) / (1.0 - em);
+  }
+  const double sigdpi = SIGMA / M_PI;
+  const double conc = 15.0 / std::pow(M_PI, 4.0);
+  const double v0 = C2 * wnumlo / temp;
+  const double v1 = C2 * wnumhi / temp;
+  const double B = planck_function2(wnumlo, wnumhi, temp);
+  const double boundary = sigdpi * conc * temp * temp * temp * (v1 * fkernel(v1) - v0 * fkernel(v0));
+  return 4.0 * B / temp - boundary;
+}
+
 // ---------------------------------------------------------------------------
 // Gauss-Legendre quadrature on (0,1), mirrored (FluxSolver.cpp:257-290)
 // mu[0..n-1] > 0, mu[n..2n-1] = -mu[0..n-1]; w likewise.

@@ -37,6 +37,9 @@ def load(native: bool = False, ext: bool = False):
     lib.oracle_quadrature.argtypes = [c_int, POINTER(c_double), POINTER(c_double), POINTER(c_double)]
     lib.oracle_planck.restype = c_double
     lib.oracle_planck.argtypes = [c_double, c_double, c_double]
+    lib.oracle_flux_bands_solve_jac.restype = c_int
+    lib.oracle_flux_bands_solve_jac.argtypes = [POINTER(capi.FluxBatch), POINTER(capi.FluxOut),
+                                                POINTER(capi.FluxJacOut), c_int]
     lib.oracle_general_bands_solve.restype = c_int
     lib.oracle_general_bands_solve.argtypes = [POINTER(capi.GeneralBatch), POINTER(capi.GeneralOut), c_int]
     if not native:
@@ -54,6 +57,20 @@ def flux_solve(w: dict, nthreads: int = 0, extra_flags: int = 0, ext: bool = Fal
     o, keep2 = capi.make_flux_out(outs, status)
     lib.oracle_flux_bands_solve(ctypes.byref(batch), ctypes.byref(o), nthreads)
     return outs, status
+
+
+def flux_solve_jac(w: dict, nthreads: int = 0, extra_flags: int = 0, ext: bool = False):
+    """Flux solve with temperature Jacobians: (outputs, status, jacobians)."""
+    lib = load(ext=ext)
+    batch, keep = capi.make_flux_batch(w["n_inst"], w["num_streams"], w["num_layers"],
+                                       w["num_phase_func_moments"], w["pmom_count"],
+                                       w["flags"] | extra_flags, w["arrays"])
+    outs, status = capi.alloc_flux_out_numpy(w["n_inst"], w["num_layers"])
+    o, keep2 = capi.make_flux_out(outs, status)
+    jac = capi.alloc_flux_jac_numpy(w["n_inst"], w["num_layers"])
+    jo, keep3 = capi.make_flux_jac_out(jac)
+    lib.oracle_flux_bands_solve_jac(ctypes.byref(batch), ctypes.byref(o), ctypes.byref(jo), nthreads)
+    return outs, status, jac
 
 
 def general_solve(d: dict, nthreads: int = 0, ext: bool = False):
