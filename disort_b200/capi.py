@@ -360,6 +360,8 @@ def load_library(path: str | None = None):
                                            POINTER(c_double), POINTER(c_int64)]
     lib.dsp_flux_bands_solve.restype = c_int32
     lib.dsp_flux_bands_solve.argtypes = [c_void_p, POINTER(FluxBatch), POINTER(FluxOut)]
+    lib.dsp_flux_bands_solve_jac.restype = c_int32
+    lib.dsp_flux_bands_solve_jac.argtypes = [c_void_p, POINTER(FluxBatch), POINTER(FluxOut), POINTER(FluxJacOut)]
     lib.dsp_general_bands_solve.restype = c_int32
     lib.dsp_general_bands_solve.argtypes = [c_void_p, POINTER(GeneralBatch), POINTER(GeneralOut)]
     lib.dsp_noalloc_scratch_bytes.restype = c_int64
@@ -391,6 +393,9 @@ class Context:
 
     def flux_bands_solve(self, batch: FluxBatch, out: FluxOut) -> int:
         return self.lib.dsp_flux_bands_solve(self.h, ctypes.byref(batch), ctypes.byref(out))
+
+    def flux_bands_solve_jac(self, batch: FluxBatch, out: FluxOut, jac: FluxJacOut) -> int:
+        return self.lib.dsp_flux_bands_solve_jac(self.h, ctypes.byref(batch), ctypes.byref(out), ctypes.byref(jac))
 
     def general_bands_solve(self, batch: GeneralBatch, out: GeneralOut) -> int:
         return self.lib.dsp_general_bands_solve(self.h, ctypes.byref(batch), ctypes.byref(out))

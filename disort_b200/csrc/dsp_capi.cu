@@ -19,6 +19,7 @@
 #include "dsp_host.hpp"
 #include "flux_bvp_tile.cuh"
 #include "flux_bvp_reg.cuh"
+#include "flux_jac.cuh"
 #include "flux_layer.cuh"
 #include "flux_setup.cuh"
 
@@ -27,8 +28,11 @@ using namespace dsp_host;
 
 namespace {
 
-template <int N>
-dsp_status launch_flux_chunk(dsp_context ctx, const FluxParams& p, cudaStream_t s) {
+// One chunk of a flux solve.  JAC: the temperature-Jacobian forms of the layer
+// and boundary-value kernels (they also write the P/Q and multiplier records),
+// then flux_jac_kernel with the view `jv`.
+template <int N, bool JAC>
+dsp_status launch_flux_chunk(dsp_context ctx, const FluxParams& p, cudaStream_t s, const JacView* jv) {
   {
     KernelTimer kt(ctx, "flux_setup_kernel", s);
     flux_setup_kernel<<<(p.n + 3) / 4, 128, 0, s>>>(p);
@@ -36,10 +40,10 @@ dsp_status launch_flux_chunk(dsp_context ctx, const FluxParams& p, cudaStream_t 
   {
     static bool attr = false;
     if (!attr) {
-      flux_layer_set_attrs<N>();
+      flux_layer_set_attrs<N, JAC>();
       attr = true;
     }
-    flux_layer_launch<N>(p, ctx->host_tables.at(N).data(), s, [&](const char* name, auto&& launch) {
+    flux_layer_launch<N, JAC>(p, ctx->host_tables.at(N).data(), s, [&](const char* name, auto&& launch) {
       KernelTimer kt(ctx, name, s);
       launch();
     });
@@ -49,18 +53,29 @@ dsp_status launch_flux_chunk(dsp_context ctx, const FluxParams& p, cudaStream_t 
     const size_t sm = C::smem_bytes();
     const int grid = (p.n + C::TPC - 1) / C::TPC;
     KernelTimer kt(ctx, "flux_bvp_kernel", s);
-    flux_bvp_reg_kernel<N><<<grid, C::CTA, sm, s>>>(p);
+    flux_bvp_reg_kernel<N, false, JAC><<<grid, C::CTA, sm, s>>>(p);
   } else {
     using C = TCfg<N>;
     const size_t sm = C::smem_bytes();
     static bool attr = false;
     if (!attr) {
-      cudaFuncSetAttribute(flux_bvp_tile_kernel<N>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+      cudaFuncSetAttribute(flux_bvp_tile_kernel<N, false, JAC>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                           (int)sm);
       attr = true;
     }
     const int grid = (p.n + C::TPC - 1) / C::TPC;
     KernelTimer kt(ctx, "flux_bvp_kernel", s);
-    flux_bvp_tile_kernel<N><<<grid, C::CTA, sm, s>>>(p);
+    flux_bvp_tile_kernel<N, false, JAC><<<grid, C::CTA, sm, s>>>(p);
+  }
+  if (jv) {
+    using C = JCfg<N>;
+    static bool attr = false;
+    if (!attr) {
+      cudaFuncSetAttribute(flux_jac_kernel<N>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)C::smem_bytes());
+      attr = true;
+    }
+    KernelTimer kt(ctx, "flux_jac_kernel", s);
+    flux_jac_kernel<N><<<p.n, C::KB, C::smem_bytes(), s>>>(p, *jv);
   }
   cudaError_t e = cudaGetLastError();
   if (e != cudaSuccess) return cuda_fail(ctx, e, "flux kernel launch");
@@ -99,17 +114,24 @@ int64_t bvp_wave(int N, int sm_count) {
   return sm_count;
 }
 
-dsp_status launch_flux(dsp_context ctx, int N, const FluxParams& p, cudaStream_t s) {
+template <int N>
+dsp_status launch_flux_n(dsp_context ctx, const FluxParams& p, cudaStream_t s, const JacView* jv) {
+  // Jacobian records are only needed when there is a thermal source to differentiate
+  if (jv && (p.flags & DSP_FLAG_THERMAL)) return launch_flux_chunk<N, true>(ctx, p, s, jv);
+  return launch_flux_chunk<N, false>(ctx, p, s, jv);
+}
+
+dsp_status launch_flux(dsp_context ctx, int N, const FluxParams& p, cudaStream_t s, const JacView* jv) {
   switch (N) {
-    case 4: return launch_flux_chunk<4>(ctx, p, s);
-    case 6: return launch_flux_chunk<6>(ctx, p, s);
-    case 8: return launch_flux_chunk<8>(ctx, p, s);
-    case 10: return launch_flux_chunk<10>(ctx, p, s);
-    case 12: return launch_flux_chunk<12>(ctx, p, s);
-    case 14: return launch_flux_chunk<14>(ctx, p, s);
-    case 16: return launch_flux_chunk<16>(ctx, p, s);
-    case 32: return launch_flux_chunk<32>(ctx, p, s);
-    case 64: return launch_flux_chunk<64>(ctx, p, s);
+    case 4: return launch_flux_n<4>(ctx, p, s, jv);
+    case 6: return launch_flux_n<6>(ctx, p, s, jv);
+    case 8: return launch_flux_n<8>(ctx, p, s, jv);
+    case 10: return launch_flux_n<10>(ctx, p, s, jv);
+    case 12: return launch_flux_n<12>(ctx, p, s, jv);
+    case 14: return launch_flux_n<14>(ctx, p, s, jv);
+    case 16: return launch_flux_n<16>(ctx, p, s, jv);
+    case 32: return launch_flux_n<32>(ctx, p, s, jv);
+    case 64: return launch_flux_n<64>(ctx, p, s, jv);
   }
   return fail(ctx, DSP_ERR_UNSUPPORTED, "unsupported num_streams");
 }
@@ -123,6 +145,9 @@ void per_inst_counts(const dsp_flux_batch* b, int64_t cnt[14]) {
 }
 
 dsp_darray* batch_arrays(dsp_flux_batch* b) { return &b->wavenumber_low; }
+
+dsp_status flux_solve(dsp_context ctx, const dsp_flux_batch* batch_in, const dsp_flux_out* out,
+                      const dsp_flux_jac_out* jac);
 
 }  // namespace
 
@@ -237,6 +262,28 @@ int64_t dsp_flux_workspace_bytes(const dsp_flux_batch* b) {
 
 dsp_status dsp_flux_bands_solve(dsp_context ctx, const dsp_flux_batch* batch_in, const dsp_flux_out* out) {
   if (!ctx) return DSP_ERR_NOT_INITIALIZED;
+  if (batch_in && (batch_in->flags & DSP_FLAG_TEMPERATURE_JAC))
+    return fail(ctx, DSP_ERR_UNSUPPORTED, "temperature Jacobians are computed by dsp_flux_bands_solve_jac");
+  return flux_solve(ctx, batch_in, out, nullptr);
+}
+
+dsp_status dsp_flux_bands_solve_jac(dsp_context ctx, const dsp_flux_batch* batch_in, const dsp_flux_out* out,
+                                    const dsp_flux_jac_out* jac) {
+  if (!ctx) return DSP_ERR_NOT_INITIALIZED;
+  if (!jac || !jac->flux_up || !jac->flux_down || !jac->mean_intensity || !jac->mean_intensity_down ||
+      !jac->mean_intensity_up || !jac->flux_divergence)
+    return fail(ctx, DSP_ERR_INVALID_INPUT, "every Jacobian output array is required");
+  return flux_solve(ctx, batch_in, out, jac);
+}
+
+}  // extern "C"
+
+namespace {
+
+// The flux solve behind both entry points; `jac` (may be null) adds the
+// temperature Jacobians.
+dsp_status flux_solve(dsp_context ctx, const dsp_flux_batch* batch_in, const dsp_flux_out* out,
+                      const dsp_flux_jac_out* jac) {
   if (!batch_in || !out) return fail(ctx, DSP_ERR_INVALID_INPUT, "null batch or output");
   dsp_flux_batch b = *batch_in;
   const int n = b.n_inst, N = b.num_streams, L = b.num_layers;
@@ -251,8 +298,8 @@ dsp_status dsp_flux_bands_solve(dsp_context ctx, const dsp_flux_batch* batch_in,
   const int nmomnstr = b.num_phase_func_moments > N ? b.num_phase_func_moments : N;
   if (b.pmom_count < nmomnstr + 1)
     return fail(ctx, DSP_ERR_INVALID_INPUT, "phase_function_moments size < nmomNstr()+1");
-  if (b.flags & (DSP_FLAG_SPHERICAL_BEAM | DSP_FLAG_TEMPERATURE_JAC))
-    return fail(ctx, DSP_ERR_UNSUPPORTED, "spherical beam and temperature Jacobians are not in this engine");
+  if (b.flags & DSP_FLAG_SPHERICAL_BEAM)
+    return fail(ctx, DSP_ERR_UNSUPPORTED, "the spherical beam is not in this engine");
   const bool thermal = (b.flags & DSP_FLAG_THERMAL) != 0;
   if (!b.delta_tau.ptr || !b.single_scat_albedo.ptr || !b.phase_function_moments.ptr)
     return fail(ctx, DSP_ERR_INVALID_INPUT, "delta_tau, single_scat_albedo and phase_function_moments are required");
@@ -309,7 +356,12 @@ dsp_status dsp_flux_bands_solve(dsp_context ctx, const dsp_flux_batch* batch_in,
     // kDefaults is static storage; the copies above are ordered before the kernels
   }
   // ---- outputs -----------------------------------------------------------
+  const int ndof = L + 2;  // Jacobian columns: level temperatures 0..L, surface
   double* dout[8];
+  double* djac[6] = {};
+  double* const hjac[6] = {jac ? jac->flux_up : nullptr, jac ? jac->flux_down : nullptr,
+                           jac ? jac->mean_intensity : nullptr, jac ? jac->mean_intensity_down : nullptr,
+                           jac ? jac->mean_intensity_up : nullptr, jac ? jac->flux_divergence : nullptr};
   int32_t* dstatus = nullptr;
   {
     double* host_out[8] = {out->flux_direct_beam, out->flux_down, out->flux_up, out->flux_tau_divergence,
@@ -318,8 +370,9 @@ dsp_status dsp_flux_bands_solve(dsp_context ctx, const dsp_flux_batch* batch_in,
     for (int f = 0; f < 8; ++f)
       if (!host_out[f]) return fail(ctx, DSP_ERR_INVALID_INPUT, "every output array is required");
     const size_t arr_bytes = ((size_t)n * nlev * sizeof(double) + 255) / 256 * 256;
+    const size_t jac_bytes = jac ? ((size_t)n * nlev * ndof * sizeof(double) + 255) / 256 * 256 : 0;
     const size_t st_bytes = ((size_t)n * sizeof(int32_t) + 255) / 256 * 256;
-    const size_t need = (dev ? 0 : 8 * arr_bytes) + st_bytes;
+    const size_t need = (dev ? 0 : 8 * arr_bytes + 6 * jac_bytes) + st_bytes;
     if ((st = ensure(ctx, &ctx->stage_out, &ctx->stage_out_bytes, need, "output staging")) != DSP_OK) return st;
     char* cur = static_cast<char*>(ctx->stage_out);
     for (int f = 0; f < 8; ++f) {
@@ -329,6 +382,14 @@ dsp_status dsp_flux_bands_solve(dsp_context ctx, const dsp_flux_batch* batch_in,
         cur += arr_bytes;
       }
     }
+    if (jac)
+      for (int f = 0; f < 6; ++f) {
+        if (dev) djac[f] = hjac[f];
+        else {
+          djac[f] = reinterpret_cast<double*>(cur);
+          cur += jac_bytes;
+        }
+      }
     dstatus = (dev && out->status) ? out->status : reinterpret_cast<int32_t*>(cur);
   }
   e = cudaMemsetAsync(dstatus, 0, (size_t)n * sizeof(int32_t), s);
@@ -343,6 +404,13 @@ dsp_status dsp_flux_bands_solve(dsp_context ctx, const dsp_flux_batch* batch_in,
   const size_t hg_doubles = hg ? (size_t)round4(L * b.pmom_count) : 0;  // keeps the records 32-byte aligned
   Sizes sz = sizes_for(N, L);
   sz.inst += hg_doubles;
+  // with Jacobians of a thermal solve: P/Q and multiplier records, and the
+  // replayed right-hand side values [L][N][ndof]
+  const bool jrecs = jac && thermal;
+  const size_t jpq_d = jrecs ? (size_t)L * jpq_stride(N) : 0;
+  const size_t jrec_d = jrecs ? (size_t)L * jrec_stride(N) : 0;
+  const size_t jcv_d = jrecs ? (size_t)L * N * ndof : 0;
+  sz.bvp += jpq_d + jrec_d + jcv_d;
   const size_t inst_doubles = sz.inst + sz.layer + sz.bvp;
   size_t budget = workspace_budget();
   size_t freeb = 0, totalb = 0;
@@ -378,6 +446,16 @@ dsp_status dsp_flux_bands_solve(dsp_context ctx, const dsp_flux_batch* batch_in,
       p.bvp_rec = p.layer_rec + (size_t)m * sz.layer;
       for (int f = 0; f < 8; ++f) p.out[f] = dout[f] + off * nlev;
       p.status = dstatus + off;
+      JacView jv;
+      if (jac) {
+        // the Jacobian areas follow the elimination records of the chunk
+        double* jbase = p.bvp_rec + (size_t)m * (sz.bvp - jpq_d - jrec_d - jcv_d);
+        p.jac_pq = jrecs ? jbase : nullptr;
+        p.jac_rec = jrecs ? jbase + (size_t)m * jpq_d : nullptr;
+        jv.cv = jrecs ? jbase + (size_t)m * (jpq_d + jrec_d) : nullptr;
+        jv.ndof = ndof;
+        for (int f = 0; f < 6; ++f) jv.out[f] = djac[f] + off * nlev * ndof;
+      }
       if (hg) {  // g per layer -> moments at the end of the instance-record area
         double* mom = wsb + (size_t)m * (sz.inst - hg_doubles);
         const long long rows = m * (long long)L;
@@ -389,7 +467,7 @@ dsp_status dsp_flux_bands_solve(dsp_context ctx, const dsp_flux_batch* batch_in,
         p.pmom.p = mom;
         p.pmom.s = (long long)L * p.pc;
       }
-      dsp_status rs = launch_flux(ctx, N, p, cs);
+      dsp_status rs = launch_flux(ctx, N, p, cs, jac ? &jv : nullptr);
       if (rs != DSP_OK) return rs;
     }
     return DSP_OK;
@@ -480,6 +558,13 @@ dsp_status dsp_flux_bands_solve(dsp_context ctx, const dsp_flux_batch* batch_in,
     e = cudaMemcpyAsync(hs + r0, dstatus + r0, (size_t)(r1 - r0) * sizeof(int32_t), cudaMemcpyDeviceToHost,
                         ctx->s_out);
     if (e != cudaSuccess) return cuda_fail(ctx, e, "cudaMemcpyAsync(status)");
+    if (jac)
+      for (int f = 0; f < 6; ++f) {
+        const int64_t per = nlev * ndof;
+        e = cudaMemcpyAsync(hjac[f] + r0 * per, djac[f] + r0 * per, (size_t)(r1 - r0) * per * sizeof(double),
+                            cudaMemcpyDeviceToHost, ctx->s_out);
+        if (e != cudaSuccess) return cuda_fail(ctx, e, "cudaMemcpyAsync(jacobian)");
+      }
   }
   // later work on the context's stream sees the whole solve
   e = cudaEventRecord(ev_start, ctx->s_c2);
@@ -490,4 +575,4 @@ dsp_status dsp_flux_bands_solve(dsp_context ctx, const dsp_flux_batch* batch_in,
   return DSP_OK;
 }
 
-}  // extern "C"
+}  // namespace

@@ -106,6 +106,21 @@ __host__ __device__ constexpr int lrec_stride(int N) { return round4(N * N + 4 *
 // ([U | V | c]), then 1 / pivot [N].
 __host__ __device__ constexpr int brec_stride(int N) { return round4(N * (2 * N + 2)); }
 
+// Temperature-Jacobian records of the flux path (compute_temperature_jacobian).
+// Per layer, written by the layer stage: P[NN] | Q[NN], the thermal particular
+// solution per unit Planck intercept and slope: with P and Q the solution of
+// computeIsotropicSource is Z1 = xr1 P / 2 in both hemispheres and
+// Z0 = (xr0 P +/- xr1 Q) / 2 (z0's upper / lower hemisphere order), so the
+// derivatives with respect to a layer's top and bottom level Planck values
+// (FluxSolver.cpp:789-829) follow from the derivatives of xr0 and xr1.
+__host__ __device__ constexpr int jpq_stride(int N) { return N; }
+// Per layer, written by the boundary-value kernels: the multiplier applied to
+// every panel slot at every pivot column, [N][3N/2] (0 where the slot was not a
+// candidate or the column was skipped as singular), then the pivot slot of each
+// column [N] (as doubles).  Together with the pivot rows of the elimination
+// record they replay the band LU on further right-hand sides.
+__host__ __device__ constexpr int jrec_stride(int N) { return round4(N * (3 * (N / 2)) + N); }
+
 // General-solver layer record: the flux layer record, then the eigenvectors
 // and sources at the user polar angles of the current mode:
 // GU[numu][N] | zbu[numu] | z0u[numu] | z1u[numu]
@@ -151,6 +166,17 @@ struct FluxParams {
   double* out[8];
   int32_t* status;
   GenView g;  // general-solver launches only
+  double* jac_pq = nullptr;   // [n][L][jpq_stride] (temperature-Jacobian launches only)
+  double* jac_rec = nullptr;  // [n][L][jrec_stride] (temperature-Jacobian launches only)
+};
+
+// The temperature-Jacobian launch of a flux chunk: the right-hand side values
+// of the replayed elimination, per instance [L][N][ndof], and the six outputs
+// [batch][L+1][ndof] (already offset to the chunk's first instance).
+struct JacView {
+  int ndof;         // L + 2 degrees of freedom: level temperatures 0..L, surface
+  double* cv;       // [n][L][N][ndof]
+  double* out[6];   // flux_up, flux_down, mean_intensity, _down, _up, flux_divergence
 };
 
 // P_l^m(x) for l = m..lmax into y[l * stride] (rows l < m set to 0), the

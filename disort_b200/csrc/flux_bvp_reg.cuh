@@ -70,7 +70,7 @@ struct RCfg {
   static constexpr size_t smem_bytes() { return sizeof(double) * (size_t)(TAB + TPC * TEAM_SMEM); }
 };
 
-template <int N, bool GEN = false>
+template <int N, bool GEN = false, bool JAC = false>
 __global__ void __launch_bounds__(RCfg<N>::CTA, RCfg<N>::MINB) flux_bvp_reg_kernel(FluxParams p) {
   using C = RCfg<N>;
   constexpr int NN = C::NN, TEAM = C::TEAM, PR = C::PR;
@@ -310,6 +310,8 @@ __global__ void __launch_bounds__(RCfg<N>::CTA, RCfg<N>::MINB) flux_bvp_reg_kern
 
     // ---- eliminate the N columns of x_l (sgbfa steps) ----------------------
     int myc = -1;  // pivot column of this thread's row, if it becomes a pivot row
+    // temperature Jacobian: this layer's multipliers and pivot slots
+    double* const jrow = JAC ? p.jac_rec + ((long long)i * L + l) * jrec_stride(N) : nullptr;
 #pragma unroll
     for (int c = 0; c < N; ++c) {
       const bool isc = t < PR && ((cand >> t) & 1u);
@@ -332,6 +334,10 @@ __global__ void __launch_bounds__(RCfg<N>::CTA, RCfg<N>::MINB) flux_bvp_reg_kern
       if (t == 0) pivslot[c] = ps;
       if (idx >= PR || zero_piv) {  // LINPACK skips a zero pivot column (BandSolver.hpp:76-78)
         singular = true;
+        if constexpr (JAC) {
+          if (t < PR) jrow[c * PR + t] = 0.0;
+          if (t == 0) jrow[N * PR + c] = (double)ps;
+        }
         continue;
       }
       double* buf = bufs + (c & 1) * (2 * N + 2);  // alternate buffers: no barrier after the update
@@ -348,6 +354,10 @@ __global__ void __launch_bounds__(RCfg<N>::CTA, RCfg<N>::MINB) flux_bvp_reg_kern
       }
       __syncwarp(msk);
       DSP_PHASE(28)
+      if constexpr (JAC) {
+        if (t < PR) jrow[c * PR + t] = ((cand >> t) & 1u) ? cur[c] * buf[2 * N + 1] : 0.0;
+        if (t == 0) jrow[N * PR + c] = (double)ps;
+      }
       if ((cand >> t) & 1u) {
         const double m = cur[c] * buf[2 * N + 1];
 #pragma unroll
@@ -360,6 +370,17 @@ __global__ void __launch_bounds__(RCfg<N>::CTA, RCfg<N>::MINB) flux_bvp_reg_kern
     }
     DSP_PHASE(21)
 
+    if (JAC && last && myc >= 0) {
+      // the Jacobian's upward solve also needs the last layer's pivot rows
+      double* row = brec0 + (long long)l * BS + myc * C::RL;
+#pragma unroll
+      for (int j = 0; j < N; ++j) {
+        row[j] = cur[j];
+        row[N + j] = 0.0;
+      }
+      row[2 * N] = rhs;
+      row[2 * N + 1] = rdiag;
+    }
     if (!last) {
       // the pivot row of column c is row c of the layer's elimination record
       if (myc >= 0) {

@@ -84,7 +84,7 @@ struct TMask {
   }
 };
 
-template <int N, bool GEN = false>
+template <int N, bool GEN = false, bool JAC = false>
 __global__ void __launch_bounds__(TCfg<N>::CTA, TCfg<N>::MINB) flux_bvp_tile_kernel(FluxParams p) {
   using C = TCfg<N>;
   constexpr int NN = C::NN, PR = C::PR, RG = C::RG, RPT = C::RPT, CPT = C::CPT, NW = C::NW;
@@ -344,6 +344,8 @@ __global__ void __launch_bounds__(TCfg<N>::CTA, TCfg<N>::MINB) flux_bvp_tile_ker
 
     // ---- eliminate the N columns of x_l (sgbfa steps) ----------------------
     const int cgo0 = cbk * (N / CPT);  // first column group of the current block
+    // temperature Jacobian: this layer's multipliers and pivot slots
+    double* const jrow = JAC ? p.jac_rec + ((long long)i * L + l) * jrec_stride(N) : nullptr;
 #pragma unroll 1
     for (int cb8 = 0; cb8 < N / CPT; ++cb8) {
       const int cgo = cgo0 + cb8;  // column group owning the next CPT pivot columns
@@ -398,6 +400,10 @@ __global__ void __launch_bounds__(TCfg<N>::CTA, TCfg<N>::MINB) flux_bvp_tile_ker
         const int pcode = psb[c & 1];
         const bool sing = pcode < 0;
         const int ps = sing ? -1 - pcode : pcode;
+        if constexpr (JAC) {
+          if (t < PR) jrow[c * PR + t] = (!sing && cand.test(t) && t != ps) ? mlt[t] : 0.0;
+          if (t == 0) jrow[N * PR + c] = (double)ps;
+        }
         if (rg == ps % RG) {
           const int kp = ps / RG;
 #pragma unroll

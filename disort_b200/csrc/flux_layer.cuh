@@ -416,7 +416,7 @@ __device__ void gen_user_angles(const FluxParams& p, int i, double* sm, const do
   }
 }
 
-template <int N, bool GEN = false>
+template <int N, bool GEN = false, bool JAC = false>
 __global__ void __launch_bounds__(LCfg<N, GEN>::CTA, LCfg<N, GEN>::MINB) flux_layer_kernel(FluxParams p) {
   using C = LCfg<N, GEN>;
   constexpr int NN = C::NN, TEAM = C::TEAM, NNP = C::NNP, NPAIR = C::NPAIR, NS = C::NS, BPT = C::BPT;
@@ -904,6 +904,16 @@ __global__ void __launch_bounds__(LCfg<N, GEN>::CTA, LCfg<N, GEN>::MINB) flux_la
       lrec[lrec_xr(N)] = xr0;
       lrec[lrec_xr(N) + 1] = xr1;
     }
+    if constexpr (JAC) {
+      // the source per unit intercept (P) and slope (Q) for the temperature
+      // Jacobian: s0 = xr0 P, d0 = xr1 Q
+      const double P = 2.0 * (1.0 - ws) * u;
+      const double Q = src ? -inv_amb(P) : 0.0;
+      if (t < NN) {
+        p.jac_pq[task * jpq_stride(N) + t] = P;
+        p.jac_pq[task * jpq_stride(N) + NN + t] = Q;
+      }
+    }
   }
   DSP_PHASE(7)
   if constexpr (GEN) {
@@ -1255,7 +1265,7 @@ __device__ __forceinline__ void warp_flush_rows(const double* stg, double* rec0,
   __syncwarp();
 }
 
-template <int N>
+template <int N, bool JAC = false>
 __global__ void __launch_bounds__(128) flux_layer_back_kernel(FluxParams p, ConstTab<N> tc) {
   constexpr int NN = N / 2;
   constexpr int RS = N + 3;  // staging row stride: a row of N (+2 for xr after z1)
@@ -1531,24 +1541,44 @@ __global__ void __launch_bounds__(128) flux_layer_back_kernel(FluxParams p, Cons
     sB[N + 1] = xr1;
     warp_flush_rows<RS>(stA, rec0, LS, N, lrec_z0(N), okm, lane);
     warp_flush_rows<RS>(stB, rec0, LS, N + 2, lrec_z1(N), okm, lane);
+    if constexpr (JAC) {
+      // the source per unit intercept (P) and slope (Q) for the temperature
+      // Jacobian: s0 = xr0 P, d0 = xr1 Q
+      const double cu = 2.0 * (1.0 - ws);
+      double qq[NN];
+#pragma unroll
+      for (int r = 0; r < NN; ++r) qq[r] = tc.dsim[r] * (cu * u[r]);
+      if (src) {
+        if (primary) applyX1(qq);
+        else applyX2(qq);
+      }
+      if (act) {
+        double* pq = p.jac_pq + jj * jpq_stride(N);
+#pragma unroll
+        for (int r = 0; r < NN; ++r) {
+          pq[r] = cu * u[r];
+          pq[NN + r] = src ? -tc.dinv[r] * qq[r] : 0.0;
+        }
+      }
+    }
   }
 }
 
 // Host side of the layer stage: launches (through `wrap(name, launch)`, which
 // may time them) one layer kernel, or the three launches of a split stage;
 // `host_tab` is a host copy of the tab_* tables of N.
-template <int N>
+template <int N, bool JAC = false>
 inline void flux_layer_set_attrs() {
   using C = LCfg<N>;
   if constexpr (layer_split<N>()) {
     static_assert(Handoff<N / 2>::HS <= brec_stride(N), "the hand-off must fit in the boundary-value records");
   } else {
-    cudaFuncSetAttribute(flux_layer_kernel<N>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+    cudaFuncSetAttribute(flux_layer_kernel<N, false, JAC>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                          (int)C::smem_bytes());
   }
 }
 
-template <int N, class Wrap>
+template <int N, bool JAC = false, class Wrap>
 inline void flux_layer_launch(const FluxParams& p, const double* host_tab, cudaStream_t s, Wrap&& wrap) {
   using C = LCfg<N>;
   const long long tasks = (long long)p.n * p.L;
@@ -1557,10 +1587,10 @@ inline void flux_layer_launch(const FluxParams& p, const double* host_tab, cudaS
     const unsigned g = (unsigned)((tasks + 127) / 128);
     wrap("flux_layer_kernel", [&] { flux_layer_front_kernel<N><<<g, 128, 0, s>>>(p, tc); });
     wrap("flux_jacobi_kernel", [&] { flux_jacobi_kernel<N / 2><<<g, 128, 0, s>>>(p); });
-    wrap("flux_layer_kernel", [&] { flux_layer_back_kernel<N><<<g, 128, 0, s>>>(p, tc); });
+    wrap("flux_layer_kernel", [&] { flux_layer_back_kernel<N, JAC><<<g, 128, 0, s>>>(p, tc); });
   } else {
     const unsigned grid = (unsigned)((tasks + C::TPC - 1) / C::TPC);
-    wrap("flux_layer_kernel", [&] { flux_layer_kernel<N><<<grid, C::CTA, C::smem_bytes(), s>>>(p); });
+    wrap("flux_layer_kernel", [&] { flux_layer_kernel<N, false, JAC><<<grid, C::CTA, C::smem_bytes(), s>>>(p); });
   }
 }
 

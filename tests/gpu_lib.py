@@ -27,6 +27,50 @@ def flux_solve(w: dict, extra_flags: int = 0):
     return outs, status, rc
 
 
+def flux_solve_jac(w: dict, extra_flags: int = 0):
+    """Host-pointer solve with temperature Jacobians: (outputs, status, jacobians, rc)."""
+    ctx = context()
+    batch, keep = capi.make_flux_batch(w["n_inst"], w["num_streams"], w["num_layers"],
+                                       w["num_phase_func_moments"], w["pmom_count"],
+                                       w["flags"] | extra_flags, w["arrays"])
+    outs, status = capi.alloc_flux_out_numpy(w["n_inst"], w["num_layers"])
+    o, keep2 = capi.make_flux_out(outs, status)
+    jac = capi.alloc_flux_jac_numpy(w["n_inst"], w["num_layers"])
+    jo, keep3 = capi.make_flux_jac_out(jac)
+    rc = ctx.flux_bands_solve_jac(batch, o, jo)
+    return outs, status, jac, rc
+
+
+def flux_solve_jac_device(w: dict, extra_flags: int = 0):
+    """Device-pointer solve with temperature Jacobians (torch CUDA tensors in and out)."""
+    import torch
+    ctx = context()
+    dev_arrays = {}
+    for k, a in w["arrays"].items():
+        if a is None:
+            dev_arrays[k] = None
+        elif isinstance(a, np.ndarray):
+            dev_arrays[k] = torch.from_numpy(np.ascontiguousarray(a)).cuda()
+        else:
+            dev_arrays[k] = torch.tensor([float(a)], dtype=torch.float64, device="cuda")
+    batch, keep = capi.make_flux_batch(w["n_inst"], w["num_streams"], w["num_layers"],
+                                       w["num_phase_func_moments"], w["pmom_count"],
+                                       w["flags"] | extra_flags | capi.FLAG_DEVICE_POINTERS, dev_arrays)
+    n, L = w["n_inst"], w["num_layers"]
+    outs = {f: torch.full((n, L + 1), float("nan"), dtype=torch.float64, device="cuda")
+            for f in capi.FLUX_OUT_FIELDS}
+    status = torch.full((n,), -1, dtype=torch.int32, device="cuda")
+    o, keep2 = capi.make_flux_out(outs, status)
+    jac = {f: torch.full((n, L + 1, L + 2), float("nan"), dtype=torch.float64, device="cuda")
+           for f in capi.JAC_FIELDS}
+    jo, keep3 = capi.make_flux_jac_out(jac)
+    ctx.set_stream(torch.cuda.current_stream().cuda_stream)
+    rc = ctx.flux_bands_solve_jac(batch, o, jo)
+    torch.cuda.synchronize()
+    return ({k: v.cpu().numpy() for k, v in outs.items()}, status.cpu().numpy(),
+            {k: v.cpu().numpy() for k, v in jac.items()}, rc)
+
+
 def flux_solve_device(w: dict, extra_flags: int = 0):
     """Device-pointer solve (torch CUDA tensors in and out)."""
     import torch

@@ -1,0 +1,104 @@
+"""GPU temperature Jacobians (dsp_flux_bands_solve_jac) against the oracle.
+
+The oracle's analytic Jacobian is itself checked against finite differences of
+the forward solve (test_jacobian_oracle.py, after the reference's
+tests/test_jacobian.cpp).  Here every Jacobian entry of the GPU must satisfy
+|gpu - oracle| <= 1e-9 * max(|oracle|, 1e-6 * s) + 1e-15, where s is the
+largest |entry| of that output's Jacobian in the instance: entries many orders
+below the instance's scale (sensitivities of levels far from a temperature,
+attenuated by exp(-k tau)) carry the absolute rounding of the larger ones.
+The fluxes of the same call are held to the usual 1e-9 / 1e-12 parity.
+"""
+import numpy as np
+import pytest
+
+import gpu_lib
+import oracle_lib
+from disort_b200 import capi, workloads
+from parity import assert_parity
+from test_jacobian_oracle import thermal_column
+
+pytestmark = pytest.mark.gpu
+
+RTOL = 1e-9
+
+
+def jac_ratio(got: dict, ref: dict) -> tuple[float, str]:
+    worst, where = 0.0, ""
+    for f in capi.JAC_FIELDS:
+        a, b = got[f], ref[f]
+        scale = np.nanmax(np.abs(b).reshape(b.shape[0], -1), axis=1)[:, None, None]
+        denom = RTOL * np.maximum(np.abs(b), 1e-6 * scale) + 1e-15
+        r = np.where(np.isnan(a) & np.isnan(b), 0.0, np.abs(a - b) / denom)
+        r = np.where(np.isnan(r), np.inf, r)
+        k = float(r.max())
+        if k > worst:
+            idx = np.unravel_index(int(np.argmax(r)), r.shape)
+            worst, where = k, f"{f}{tuple(int(x) for x in idx)} gpu={a[idx]!r} ref={b[idx]!r}"
+    return worst, where
+
+
+def check(w, extra_flags=0, label=""):
+    out, st, jac, rc = gpu_lib.flux_solve_jac(w, extra_flags)
+    assert rc == 0, gpu_lib.context().last_error()
+    rout, rst, rjac = oracle_lib.flux_solve_jac(w, extra_flags=extra_flags)
+    assert np.all(st == rst)
+    ok = st == 0
+    assert_parity({k: v[ok] for k, v in out.items()}, {k: v[ok] for k, v in rout.items()}, label)
+    r, where = jac_ratio(jac, rjac)
+    assert r <= 1.0, f"{label}: Jacobian parity ratio {r:.3g} at {where}"
+    return out, st, jac
+
+
+@pytest.mark.parametrize("name,Tlev,Tsurf,nstr,ssa,beam", [
+    ("flux_single_layer", [200.0, 260.0], 280.0, 8, 0.0, 0.0),
+    ("flux_multilayer_scattering", [205.0 + 9.0 * i for i in range(9)], 290.0, 16, 0.7, 0.0),
+    ("thermal_plus_beam", [200.0, 240.0, 270.0], 288.0, 16, 0.6, 1.0),
+    ("four_streams", [220.0, 240.0, 260.0, 275.0], 285.0, 4, 0.4, 0.0),
+    ("scattering_high_12", [210.0, 235.0, 255.0, 270.0, 280.0], 290.0, 12, 0.9, 0.0),
+])
+def test_reference_jacobian_problems(name, Tlev, Tsurf, nstr, ssa, beam):
+    check(thermal_column(Tlev, Tsurf, nstr, ssa, beam), label=name)
+
+
+@pytest.mark.parametrize("extra", [0, capi.FLAG_INDEX_FROM_BOTTOM, capi.FLAG_DIFFUSION_LOWER_BC,
+                                   capi.FLAG_DELTA_M_PLUS])
+def test_thermal_sweep_jacobians(extra):
+    """Thermal-sweep columns (60 layers, 16 streams), also bottom-up, with the
+    diffusion lower boundary, and delta-M+ (moments g^k: the global fallback
+    keeps delta-M)."""
+    w = workloads.subset(workloads.thermal_sweep(), np.arange(0, 20000, 800))
+    check(w, extra, label=f"thermal sweep flags={extra}")
+
+
+@pytest.mark.parametrize("nstr", [6, 10, 14, 32, 64])
+def test_jacobians_other_stream_counts(nstr):
+    w = workloads.thermal_sweep(n_bands=5, num_layers=30 if nstr < 64 else 20, num_streams=nstr, seed=80 + nstr)
+    check(w, label=f"N={nstr}")
+
+
+def test_deep_column_more_degrees_of_freedom_than_a_pass():
+    """90 layers: 92 degrees of freedom, two passes of the 64-thread Jacobian CTA."""
+    w = workloads.thermal_sweep(n_bands=3, num_layers=90, num_streams=8, seed=91)
+    check(w, label="L=90")
+
+
+def test_jacobian_device_pointers_equal_host_pointers_and_edge_cases():
+    w = workloads.subset(workloads.thermal_sweep(), np.arange(0, 20000, 1000))
+    w["arrays"]["single_scat_albedo"] = w["arrays"]["single_scat_albedo"].copy()
+    w["arrays"]["single_scat_albedo"][3, 7] = 1.5  # invalid instance: NaN Jacobian
+    out, st, jac = check(w, label="with an invalid instance")
+    assert st[3] == capi.DSP_ERR_INVALID_INPUT and np.all(np.isnan(jac["flux_up"][3]))
+    dout, dst, djac, rc = gpu_lib.flux_solve_jac_device(w)
+    assert rc == 0
+    for f in capi.JAC_FIELDS:
+        np.testing.assert_array_equal(jac[f], djac[f])
+    # without thermal emission the Jacobians are zero
+    w2 = workloads.beam_sweep(16)
+    out, st, jac, rc = gpu_lib.flux_solve_jac(w2)
+    assert rc == 0 and not st.any()
+    for f in capi.JAC_FIELDS:
+        assert np.all(jac[f] == 0.0)
+    # the plain entry point rejects the Jacobian flag
+    _, _, rc = gpu_lib.flux_solve(w, extra_flags=capi.FLAG_TEMPERATURE_JAC)
+    assert rc == capi.DSP_ERR_UNSUPPORTED
