@@ -345,14 +345,14 @@ dsp_flux_batch pack(const DisortFluxConfig& c, const std::vector<std::pair<doubl
   return b;
 }
 
+// jac6 (null unless compute_temperature_jacobian): the six Jacobian arrays,
+// each [n][L+1][L+2]
 void run(const DisortFluxConfig& c, const std::vector<std::pair<double, double>>& bands, const SpectralOverrides& ov,
-         double* out8[8]) {
+         double* out8[8], double* jac6[6] = nullptr) {
   if (!supported(c.num_streams))
     throw std::invalid_argument("Unsupported num_streams=" + std::to_string(c.num_streams) +
                                 ". Supported values: 4, 6, 8, 10, 12, 14, 16, 32, 64");
   if (c.use_spherical_beam) throw std::invalid_argument("use_spherical_beam is not supported by the B200 engine");
-  if (c.compute_temperature_jacobian)
-    throw std::invalid_argument("compute_temperature_jacobian is not supported by the B200 engine");
   const size_t n = bands.size();
   auto check = [&](size_t got, const char* name) {
     if (got != 0 && got != n)
@@ -376,7 +376,13 @@ void run(const DisortFluxConfig& c, const std::vector<std::pair<double, double>>
   dsp_flux_out o{out8[0], out8[1], out8[2], out8[3], out8[4], out8[5], out8[6], out8[7], status.data()};
   std::lock_guard<std::mutex> lk(g_mu);
   dsp_context ctx = context_locked();
-  const dsp_status st = dsp_flux_bands_solve(ctx, &b, &o);
+  dsp_status st;
+  if (jac6) {
+    const dsp_flux_jac_out j{jac6[0], jac6[1], jac6[2], jac6[3], jac6[4], jac6[5]};
+    st = dsp_flux_bands_solve_jac(ctx, &b, &o, &j);
+  } else {
+    st = dsp_flux_bands_solve(ctx, &b, &o);
+  }
   if (st != DSP_OK)
     throw std::runtime_error(std::string("disortpp: GPU solve failed: ") + dsp_status_string(st) + ": " +
                              dsp_context_last_error(ctx));
@@ -385,9 +391,11 @@ void run(const DisortFluxConfig& c, const std::vector<std::pair<double, double>>
       throw std::invalid_argument("band " + std::to_string(i) + ": " + dsp_status_string((dsp_status)status[i]));
 }
 
-std::vector<FluxResult> to_results(size_t n, int L, const std::vector<double>& buf) {
+// jbuf: the six Jacobian arrays back to back ([6][n][L+1][L+2]), or empty
+std::vector<FluxResult> to_results(size_t n, int L, const std::vector<double>& buf,
+                                   const std::vector<double>& jbuf = {}) {
   std::vector<FluxResult> res(n);
-  const size_t nlev = static_cast<size_t>(L) + 1;
+  const size_t nlev = static_cast<size_t>(L) + 1, ndof = static_cast<size_t>(L) + 2;
   for (size_t i = 0; i < n; ++i) {
     FluxResult& r = res[i];
     std::vector<double>* dst[8] = {&r.flux_direct_beam, &r.flux_down, &r.flux_up, &r.flux_tau_divergence,
@@ -396,6 +404,20 @@ std::vector<FluxResult> to_results(size_t n, int L, const std::vector<double>& b
     for (int f = 0; f < 8; ++f) {
       const double* src = buf.data() + (static_cast<size_t>(f) * n + i) * nlev;
       dst[f]->assign(src, src + nlev);
+    }
+    if (!jbuf.empty()) {
+      std::vector<std::vector<double>>* jd[6] = {&r.flux_up_temperature_jac, &r.flux_down_temperature_jac,
+                                                 &r.mean_intensity_temperature_jac,
+                                                 &r.mean_intensity_down_temperature_jac,
+                                                 &r.mean_intensity_up_temperature_jac,
+                                                 &r.flux_divergence_temperature_jac};
+      for (int f = 0; f < 6; ++f) {
+        jd[f]->resize(nlev);
+        for (size_t lu = 0; lu < nlev; ++lu) {
+          const double* src = jbuf.data() + ((static_cast<size_t>(f) * n + i) * nlev + lu) * ndof;
+          (*jd[f])[lu].assign(src, src + ndof);
+        }
+      }
     }
   }
   return res;
@@ -406,6 +428,8 @@ std::vector<FluxResult> to_results(size_t n, int L, const std::vector<double>& b
 void solveFluxSpectralBandsInto(const DisortFluxConfig& config,
                                 const std::vector<std::pair<double, double>>& bands, const SpectralOverrides& ov,
                                 double* out8[8]) {
+  if (config.compute_temperature_jacobian)
+    throw std::invalid_argument("temperature Jacobians are returned by solve_flux_spectral_bands");
   run(config, bands, ov, out8);
 }
 
@@ -417,8 +441,19 @@ std::vector<FluxResult> solveFluxSpectralBands(const DisortFluxConfig& config,
   std::vector<double> buf(8 * n * nlev);
   double* out8[8];
   for (int f = 0; f < 8; ++f) out8[f] = buf.data() + static_cast<size_t>(f) * n * nlev;
-  run(config, bands, ov, out8);
-  return to_results(n, config.num_layers, buf);
+  // Jacobians are returned when asked for with thermal emission on; otherwise
+  // they stay empty, as the reference clears them (FluxSolver.cpp:1299-1307)
+  const bool jac = config.compute_temperature_jacobian;
+  std::vector<double> jbuf;
+  double* jac6[6];
+  if (jac) {
+    const size_t per = n * nlev * (nlev + 1);
+    jbuf.resize(6 * per);
+    for (int f = 0; f < 6; ++f) jac6[f] = jbuf.data() + f * per;
+  }
+  run(config, bands, ov, out8, jac ? jac6 : nullptr);
+  if (jac && !config.use_thermal_emission) jbuf.clear();
+  return to_results(n, config.num_layers, buf, jbuf);
 }
 
 std::vector<FluxResult> solveFluxSpectral(const DisortFluxConfig& config, const std::vector<double>& wavenumbers,

@@ -118,3 +118,18 @@ def test_no_thermal_gives_zero_jacobian():
     assert st[0] == 0
     for f in capi.JAC_FIELDS:
         assert np.all(jac[f] == 0.0)
+
+
+def test_double_and_extended_oracle_jacobians_agree():
+    """The double build of the oracle against its extended-precision build (the
+    GPU Jacobians' checker): within 3e-8 of max(|entry|, 1e-3 of the output's
+    largest entry in the instance) on thermal-sweep columns -- double rounding
+    alone moves single entries by up to ~1.4e-8 there."""
+    from disort_b200 import workloads
+    w = workloads.subset(workloads.thermal_sweep(), np.arange(0, 20000, 800))
+    for extra in (0, capi.FLAG_DIFFUSION_LOWER_BC):
+        _, _, a = oracle_lib.flux_solve_jac(w, extra_flags=extra)
+        _, _, b = oracle_lib.flux_solve_jac(w, extra_flags=extra, ext=True)
+        for f in capi.JAC_FIELDS:
+            scale = np.abs(b[f]).reshape(b[f].shape[0], -1).max(axis=1)[:, None, None]
+            assert np.all(np.abs(a[f] - b[f]) <= 3e-8 * np.maximum(np.abs(b[f]), 1e-3 * scale)), f
