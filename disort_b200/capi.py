@@ -57,7 +57,7 @@ FLUX_ARRAY_FIELDS = (
     "wavenumber_low", "wavenumber_high", "delta_tau", "single_scat_albedo",
     "phase_function_moments", "temperature", "surface_albedo", "emissivity_top",
     "direct_beam_flux", "direct_beam_mu", "isotropic_flux_top", "isotropic_flux_bottom",
-    "temperature_top", "temperature_bottom",
+    "temperature_top", "temperature_bottom", "level_altitudes", "bottom_radius",
 )
 
 FLUX_OUT_FIELDS = (
@@ -135,6 +135,7 @@ def make_flux_batch(n_inst: int, num_streams: int, num_layers: int, num_phase_fu
     keep: list = []
     per_ndim = {  # dimensions of one instance's value
         "delta_tau": 1, "single_scat_albedo": 1, "phase_function_moments": 2, "temperature": 1,
+        "level_altitudes": 1,
     }
     if flags & FLAG_HG_G:  # one asymmetry factor per layer instead of moments
         per_ndim["phase_function_moments"] = 1

@@ -22,6 +22,7 @@
 #include "flux_jac.cuh"
 #include "flux_layer.cuh"
 #include "flux_setup.cuh"
+#include "flux_sph.cuh"
 
 using namespace dsp;
 using namespace dsp_host;
@@ -31,11 +32,15 @@ namespace {
 // One chunk of a flux solve.  JAC: the temperature-Jacobian forms of the layer
 // and boundary-value kernels (they also write the P/Q and multiplier records),
 // then flux_jac_kernel with the view `jv`.
-template <int N, bool JAC>
+template <int N, bool JAC, bool SPH>
 dsp_status launch_flux_chunk(dsp_context ctx, const FluxParams& p, cudaStream_t s, const JacView* jv) {
   {
     KernelTimer kt(ctx, "flux_setup_kernel", s);
     flux_setup_kernel<<<(p.n + 3) / 4, 128, 0, s>>>(p);
+  }
+  if constexpr (SPH) {
+    KernelTimer kt(ctx, "flux_sph_chapman_kernel", s);
+    flux_sph_chapman_kernel<<<(p.n + 3) / 4, 128, 0, s>>>(p);
   }
   {
     static bool attr = false;
@@ -48,24 +53,37 @@ dsp_status launch_flux_chunk(dsp_context ctx, const FluxParams& p, cudaStream_t 
       launch();
     });
   }
+  if constexpr (SPH) {
+    // the spherical particular solution replaces the layer stage's plane-parallel one
+    using C = SCfg<N>;
+    static bool attr = false;
+    if (!attr) {
+      cudaFuncSetAttribute(flux_sph_source_kernel<N>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                           (int)C::smem_bytes());
+      attr = true;
+    }
+    const long long tasks = (long long)p.n * p.L;
+    KernelTimer kt(ctx, "flux_sph_source_kernel", s);
+    flux_sph_source_kernel<N><<<(unsigned)((tasks + C::WPC - 1) / C::WPC), 32 * C::WPC, C::smem_bytes(), s>>>(p);
+  }
   if constexpr (N <= 16) {
     using C = RCfg<N>;
     const size_t sm = C::smem_bytes();
     const int grid = (p.n + C::TPC - 1) / C::TPC;
     KernelTimer kt(ctx, "flux_bvp_kernel", s);
-    flux_bvp_reg_kernel<N, false, JAC><<<grid, C::CTA, sm, s>>>(p);
+    flux_bvp_reg_kernel<N, false, JAC, SPH><<<grid, C::CTA, sm, s>>>(p);
   } else {
     using C = TCfg<N>;
     const size_t sm = C::smem_bytes();
     static bool attr = false;
     if (!attr) {
-      cudaFuncSetAttribute(flux_bvp_tile_kernel<N, false, JAC>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+      cudaFuncSetAttribute(flux_bvp_tile_kernel<N, false, JAC, SPH>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                            (int)sm);
       attr = true;
     }
     const int grid = (p.n + C::TPC - 1) / C::TPC;
     KernelTimer kt(ctx, "flux_bvp_kernel", s);
-    flux_bvp_tile_kernel<N, false, JAC><<<grid, C::CTA, sm, s>>>(p);
+    flux_bvp_tile_kernel<N, false, JAC, SPH><<<grid, C::CTA, sm, s>>>(p);
   }
   if (jv) {
     using C = JCfg<N>;
@@ -117,8 +135,10 @@ int64_t bvp_wave(int N, int sm_count) {
 template <int N>
 dsp_status launch_flux_n(dsp_context ctx, const FluxParams& p, cudaStream_t s, const JacView* jv) {
   // Jacobian records are only needed when there is a thermal source to differentiate
-  if (jv && (p.flags & DSP_FLAG_THERMAL)) return launch_flux_chunk<N, true>(ctx, p, s, jv);
-  return launch_flux_chunk<N, false>(ctx, p, s, jv);
+  const bool jac = jv && (p.flags & DSP_FLAG_THERMAL);
+  const bool sph = (p.flags & DSP_FLAG_SPHERICAL_BEAM) != 0;
+  if (sph) return jac ? launch_flux_chunk<N, true, true>(ctx, p, s, jv) : launch_flux_chunk<N, false, true>(ctx, p, s, jv);
+  return jac ? launch_flux_chunk<N, true, false>(ctx, p, s, jv) : launch_flux_chunk<N, false, false>(ctx, p, s, jv);
 }
 
 dsp_status launch_flux(dsp_context ctx, int N, const FluxParams& p, cudaStream_t s, const JacView* jv) {
@@ -136,12 +156,18 @@ dsp_status launch_flux(dsp_context ctx, int N, const FluxParams& p, cudaStream_t
   return fail(ctx, DSP_ERR_UNSUPPORTED, "unsupported num_streams");
 }
 
-// elements of one instance's value for each batch array, in FLUX field order
-void per_inst_counts(const dsp_flux_batch* b, int64_t cnt[14]) {
+// the batch arrays of dsp_flux_batch, in field order
+constexpr int kFluxArrays = 16;
+// scalar fields, which take the DisortFluxConfig default when absent
+constexpr bool kScalarField[kFluxArrays] = {true, true, false, false, false, false, true, true,
+                                            true, true, true, true, true, true, false, true};
+
+// elements of one instance's value for each batch array, in field order
+void per_inst_counts(const dsp_flux_batch* b, int64_t cnt[kFluxArrays]) {
   const int L = b->num_layers;
   const int64_t pm = (b->flags & DSP_FLAG_HG_G) ? (int64_t)L : (int64_t)L * b->pmom_count;
-  const int64_t c[14] = {1, 1, L, L, pm, L + 1, 1, 1, 1, 1, 1, 1, 1, 1};
-  for (int k = 0; k < 14; ++k) cnt[k] = c[k];
+  const int64_t c[kFluxArrays] = {1, 1, L, L, pm, L + 1, 1, 1, 1, 1, 1, 1, 1, 1, L + 1, 1};
+  for (int k = 0; k < kFluxArrays; ++k) cnt[k] = c[k];
 }
 
 dsp_darray* batch_arrays(dsp_flux_batch* b) { return &b->wavenumber_low; }
@@ -257,6 +283,7 @@ int64_t dsp_flux_workspace_bytes(const dsp_flux_batch* b) {
   if (!b || b->num_layers <= 0 || !supported_nstr(b->num_streams)) return -1;
   Sizes s = sizes_for(b->num_streams, b->num_layers);
   if (b->flags & DSP_FLAG_HG_G) s.inst += (size_t)round4(b->num_layers * b->pmom_count);
+  if (b->flags & DSP_FLAG_SPHERICAL_BEAM) s.bvp += (size_t)b->num_layers * sph_stride(b->num_streams);
   return (int64_t)s.per_inst_bytes() * (int64_t)b->n_inst;
 }
 
@@ -298,9 +325,10 @@ dsp_status flux_solve(dsp_context ctx, const dsp_flux_batch* batch_in, const dsp
   const int nmomnstr = b.num_phase_func_moments > N ? b.num_phase_func_moments : N;
   if (b.pmom_count < nmomnstr + 1)
     return fail(ctx, DSP_ERR_INVALID_INPUT, "phase_function_moments size < nmomNstr()+1");
-  if (b.flags & DSP_FLAG_SPHERICAL_BEAM)
-    return fail(ctx, DSP_ERR_UNSUPPORTED, "the spherical beam is not in this engine");
   const bool thermal = (b.flags & DSP_FLAG_THERMAL) != 0;
+  const bool spherical = (b.flags & DSP_FLAG_SPHERICAL_BEAM) != 0;
+  if (spherical && (!b.level_altitudes.ptr || !b.bottom_radius.ptr))
+    return fail(ctx, DSP_ERR_INVALID_INPUT, "the spherical beam needs level_altitudes and bottom_radius");
   if (!b.delta_tau.ptr || !b.single_scat_albedo.ptr || !b.phase_function_moments.ptr)
     return fail(ctx, DSP_ERR_INVALID_INPUT, "delta_tau, single_scat_albedo and phase_function_moments are required");
   if (thermal && (!b.temperature.ptr || !b.wavenumber_low.ptr || !b.wavenumber_high.ptr))
@@ -313,27 +341,27 @@ dsp_status flux_solve(dsp_context ctx, const dsp_flux_batch* batch_in, const dsp
   dsp_status st;
 
   // scalar defaults for absent per-instance scalars (DisortFluxConfig.hpp:30-44)
-  static const double kDefaults[14] = {0, 0, 0, 0, 0, 0, 0.0, 1.0, 0.0, 0.5, 0.0, 0.0, 0.0, 0.0};
-  int64_t cnt[14];
+  static const double kDefaults[kFluxArrays] = {0, 0, 0, 0, 0, 0, 0.0, 1.0, 0.0, 0.5, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0};
+  int64_t cnt[kFluxArrays];
   per_inst_counts(&b, cnt);
 
   // ---- stage host inputs (and defaults) into device memory ---------------
   dsp_darray* arr = batch_arrays(&b);
-  const double* host_in[14] = {};  // per-instance host arrays still to be copied
+  const double* host_in[kFluxArrays] = {};  // per-instance host arrays still to be copied
   {
     size_t need = 0;
-    for (int k = 0; k < 14; ++k) {
+    for (int k = 0; k < kFluxArrays; ++k) {
       size_t elems;
-      if (!arr[k].ptr) elems = (k <= 1 || k >= 6) ? 1 : 0;
+      if (!arr[k].ptr) elems = kScalarField[k] ? 1 : 0;
       else if (dev) elems = 0;
       else elems = arr[k].stride == 0 ? (size_t)cnt[k] : (size_t)((n - 1) * arr[k].stride + cnt[k]);
       need += ((elems * sizeof(double) + 255) / 256) * 256;
     }
     if ((st = ensure(ctx, &ctx->stage_in, &ctx->stage_in_bytes, need + 256, "input staging")) != DSP_OK) return st;
     char* cur = static_cast<char*>(ctx->stage_in);
-    for (int k = 0; k < 14; ++k) {
+    for (int k = 0; k < kFluxArrays; ++k) {
       if (!arr[k].ptr) {
-        if (k <= 1 || k >= 6) {  // absent scalar: the DisortFluxConfig default
+        if (kScalarField[k]) {  // absent scalar: the DisortFluxConfig default
           e = cudaMemcpyAsync(cur, &kDefaults[k], sizeof(double), cudaMemcpyHostToDevice, s);
           if (e != cudaSuccess) return cuda_fail(ctx, e, "cudaMemcpyAsync(default)");
           arr[k].ptr = reinterpret_cast<const double*>(cur);
@@ -410,7 +438,9 @@ dsp_status flux_solve(dsp_context ctx, const dsp_flux_batch* batch_in, const dsp
   const size_t jpq_d = jrecs ? (size_t)L * jpq_stride(N) : 0;
   const size_t jrec_d = jrecs ? (size_t)L * jrec_stride(N) : 0;
   const size_t jcv_d = jrecs ? (size_t)L * N * ndof : 0;
-  sz.bvp += jpq_d + jrec_d + jcv_d;
+  // with the pseudo-spherical beam: the spherical record of every layer
+  const size_t sph_d = spherical ? (size_t)L * sph_stride(N) : 0;
+  sz.bvp += jpq_d + jrec_d + jcv_d + sph_d;
   const size_t inst_doubles = sz.inst + sz.layer + sz.bvp;
   size_t budget = workspace_budget();
   size_t freeb = 0, totalb = 0;
@@ -432,12 +462,12 @@ dsp_status flux_solve(dsp_context ctx, const dsp_flux_batch* batch_in, const dsp
   // solves instances [r0, r1) on stream `cs`, `ch` at a time, in the workspace at `wsb`
   auto run_range = [&](int64_t r0, int64_t r1, cudaStream_t cs, double* wsb, int64_t ch) -> dsp_status {
     FluxParams p = p0;
-    DArr* pa[14] = {&p.wlo, &p.whi, &p.dtau, &p.ssa, &p.pmom, &p.temp, &p.alb,
-                    &p.emis, &p.fbeam, &p.umu0, &p.fisot, &p.fisob, &p.ttop, &p.tbot};
+    DArr* pa[kFluxArrays] = {&p.wlo, &p.whi, &p.dtau, &p.ssa, &p.pmom, &p.temp, &p.alb, &p.emis,
+                             &p.fbeam, &p.umu0, &p.fisot, &p.fisob, &p.ttop, &p.tbot, &p.zalt, &p.rbot};
     for (int64_t off = r0; off < r1; off += ch) {
       const int64_t m = (r1 - off < ch) ? (r1 - off) : ch;
       p.n = (int)m;
-      for (int k = 0; k < 14; ++k) {
+      for (int k = 0; k < kFluxArrays; ++k) {
         pa[k]->p = arr[k].ptr ? arr[k].ptr + arr[k].stride * off : nullptr;
         pa[k]->s = arr[k].stride;
       }
@@ -446,10 +476,12 @@ dsp_status flux_solve(dsp_context ctx, const dsp_flux_batch* batch_in, const dsp
       p.bvp_rec = p.layer_rec + (size_t)m * sz.layer;
       for (int f = 0; f < 8; ++f) p.out[f] = dout[f] + off * nlev;
       p.status = dstatus + off;
+      // the spherical and Jacobian areas follow the elimination records of the chunk
+      double* xbase = p.bvp_rec + (size_t)m * (sz.bvp - jpq_d - jrec_d - jcv_d - sph_d);
+      p.sph = spherical ? xbase : nullptr;
       JacView jv;
       if (jac) {
-        // the Jacobian areas follow the elimination records of the chunk
-        double* jbase = p.bvp_rec + (size_t)m * (sz.bvp - jpq_d - jrec_d - jcv_d);
+        double* jbase = xbase + (size_t)m * sph_d;
         p.jac_pq = jrecs ? jbase : nullptr;
         p.jac_rec = jrecs ? jbase + (size_t)m * jpq_d : nullptr;
         jv.cv = jrecs ? jbase + (size_t)m * (jpq_d + jrec_d) : nullptr;
@@ -536,7 +568,7 @@ dsp_status flux_solve(dsp_context ctx, const dsp_flux_batch* batch_in, const dsp
   for (int k = 0; k < pieces; ++k) {
     const int64_t r0 = k == 0 ? 0 : first + piece * (k - 1), r1 = std::min<int64_t>(n, first + piece * k);
     cudaStream_t cs = (dual && (k & 1)) ? ctx->s_c2 : s;
-    for (int a = 0; a < 14; ++a) {
+    for (int a = 0; a < kFluxArrays; ++a) {
       if (!host_in[a]) continue;
       const int64_t e0 = r0 * arr[a].stride, e1 = (r1 - 1) * arr[a].stride + cnt[a];
       e = cudaMemcpyAsync(const_cast<double*>(arr[a].ptr) + e0, host_in[a] + e0, (size_t)(e1 - e0) * sizeof(double),

@@ -106,6 +106,14 @@ __host__ __device__ constexpr int lrec_stride(int N) { return round4(N * N + 4 *
 // ([U | V | c]), then 1 / pivot [N].
 __host__ __device__ constexpr int brec_stride(int N) { return round4(N * (2 * N + 2)); }
 
+// Pseudo-spherical beam record of the flux path, per layer: the slope Z1 of the
+// beam particular solution Z(tau) = exp(-xba tau) (Z0 + Z1 tau) (Z0 is the layer
+// record's zb), its attenuation xba, and the layer's Chapman factor
+// (computeBeamSourceSpherical, FluxSolver.cpp:650-738; :391-419).
+__host__ __device__ constexpr int sph_stride(int N) { return round4(N + 2); }
+__host__ __device__ constexpr int sph_xba(int N) { return N; }
+__host__ __device__ constexpr int sph_ch(int N) { return N + 1; }
+
 // Temperature-Jacobian records of the flux path (compute_temperature_jacobian).
 // Per layer, written by the layer stage: P[NN] | Q[NN], the thermal particular
 // solution per unit Planck intercept and slope: with P and Q the solution of
@@ -156,7 +164,7 @@ struct FluxParams {
   int n;          // instances in this launch
   int N, L, pc, nmom;
   uint32_t flags;
-  DArr wlo, whi, dtau, ssa, pmom, temp, alb, emis, fbeam, umu0, fisot, fisob, ttop, tbot;
+  DArr wlo, whi, dtau, ssa, pmom, temp, alb, emis, fbeam, umu0, fisot, fisob, ttop, tbot, zalt, rbot;
   const double* tables;  // tab_* layout for N
   PlanckConsts pk;
   double* inst_rec;
@@ -166,6 +174,7 @@ struct FluxParams {
   double* out[8];
   int32_t* status;
   GenView g;  // general-solver launches only
+  double* sph = nullptr;      // [n][L][sph_stride] (pseudo-spherical beam launches only)
   double* jac_pq = nullptr;   // [n][L][jpq_stride] (temperature-Jacobian launches only)
   double* jac_rec = nullptr;  // [n][L][jrec_stride] (temperature-Jacobian launches only)
 };

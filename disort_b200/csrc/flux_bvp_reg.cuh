@@ -70,7 +70,7 @@ struct RCfg {
   static constexpr size_t smem_bytes() { return sizeof(double) * (size_t)(TAB + TPC * TEAM_SMEM); }
 };
 
-template <int N, bool GEN = false, bool JAC = false>
+template <int N, bool GEN = false, bool JAC = false, bool SPH = false>
 __global__ void __launch_bounds__(RCfg<N>::CTA, RCfg<N>::MINB) flux_bvp_reg_kernel(FluxParams p) {
   using C = RCfg<N>;
   constexpr int NN = C::NN, TEAM = C::TEAM, PR = C::PR;
@@ -149,6 +149,13 @@ __global__ void __launch_bounds__(RCfg<N>::CTA, RCfg<N>::MINB) flux_bvp_reg_kern
   const double* btr = rec + il.btr;
   const double* dtau_s = rec + il.dtau_s;
   auto LR = [&](int l) { return lrec0 + (long long)l * lstride; };
+  // pseudo-spherical beam: layer l's record [Z1 | xba | ch], and its particular
+  // solution exp(-xba tau) (Z0 + Z1 tau) at stream iq (solve0, FluxSolver.cpp:1001-1090)
+  auto SR = [&](int l) { return p.sph + ((long long)i * L + l) * sph_stride(N); };
+  auto zsph = [&](const double* lrl, int l, int iq, double tau) {
+    const double* sr = SR(l);
+    return exp(-sr[sph_xba(N)] * tau) * (ld_rec(lrl + C::SZB + iq) + sr[iq] * tau);
+  };
 
   double* sm = smem + C::TAB + team * C::TEAM_SMEM;
   double* bufs = sm + C::O_BUF;
@@ -244,8 +251,13 @@ __global__ void __launch_bounds__(RCfg<N>::CTA, RCfg<N>::MINB) flux_bvp_reg_kern
         const double T = btr1, tau = tau1;
         double sum = 0.0;
         if (beam) {
-          sum += ld_rec(ln + C::SZB + jq) * T;
-          sum -= ld_rec(lr + C::SZB + jq) * T;
+          if constexpr (SPH) {
+            sum += zsph(ln, l + 1, jq, tau);
+            sum -= zsph(lr, l, jq, tau);
+          } else {
+            sum += ld_rec(ln + C::SZB + jq) * T;
+            sum -= ld_rec(lr + C::SZB + jq) * T;
+          }
         }
         if (thermal) {
           sum += ld_rec(ln + C::SZ0 + jq) - ld_rec(lr + C::SZ0 + jq);
@@ -271,7 +283,7 @@ __global__ void __launch_bounds__(RCfg<N>::CTA, RCfg<N>::MINB) flux_bvp_reg_kern
         const double T = btr1, tau = tau1;
         double sum = 0.0;
         if (dlbc) {
-          if (beam) sum -= ld_rec(lr + C::SZB + NN + rb) * T;
+          if (beam) sum -= SPH ? zsph(lr, l, NN + rb, tau) : ld_rec(lr + C::SZB + NN + rb) * T;
           if (thermal) {
             sum -= ld_rec(lr + C::SZ0 + NN + rb);
             sum -= ld_rec(lr + C::SZ1 + NN + rb) * tau;
@@ -282,14 +294,14 @@ __global__ void __launch_bounds__(RCfg<N>::CTA, RCfg<N>::MINB) flux_bvp_reg_kern
             double refl = 0.0;
             for (int jj = 0; jj < NN; ++jj) {
               double ps = 0.0;
-              if (beam) ps += ld_rec(lr + C::SZB + NN - 1 - jj) * T;
+              if (beam) ps += SPH ? zsph(lr, l, NN - 1 - jj, tau) : ld_rec(lr + C::SZB + NN - 1 - jj) * T;
               if (thermal) ps += ld_rec(lr + C::SZ0 + NN - 1 - jj) + ld_rec(lr + C::SZ1 + NN - 1 - jj) * tau;
               refl += wt[jj] * mu[jj] * alb * ps;
             }
             sum += 2.0 * refl;
           }
           if (beam) {
-            sum -= ld_rec(lr + C::SZB + NN + rb) * T;
+            sum -= SPH ? zsph(lr, l, NN + rb, tau) : ld_rec(lr + C::SZB + NN + rb) * T;
             if (!lyrcut) sum += alb * umu0 * fbeam * T / PI;
           }
           if (thermal) {
@@ -442,12 +454,15 @@ __global__ void __launch_bounds__(RCfg<N>::CTA, RCfg<N>::MINB) flux_bvp_reg_kern
       ec[t] = x[t] * exp(-eig[t] * d);
     }
     __syncwarp(msk);
-    const double fact = beam ? exp(-utaupr * rumu0) : 0.0;
+    // pseudo-spherical: the Chapman factor of the layer replaces mu0
+    // (computeFluxes, FluxSolver.cpp:1184-1188, 1216-1219)
+    const double ch = SPH && beam ? SR(l)[sph_ch(N)] : 0.0;
+    const double fact = beam ? (SPH ? exp(-utaupr / ch) : exp(-utaupr * rumu0)) : 0.0;
     if (t < N) {
       double s = 0.0;
 #pragma unroll
       for (int j = 0; j < N; ++j) s += ld_rec(Gl + t * GS + j) * ec[j];
-      if (beam) s += ld_rec(lr + C::SZB + t) * fact;
+      if (beam) s += SPH ? zsph(lr, l, t, utaupr) : ld_rec(lr + C::SZB + t) * fact;
       if (thermal) s += ld_rec(lr + C::SZ0 + t) + ld_rec(lr + C::SZ1 + t) * utaupr;
       Iv[t] = s;
     }
@@ -457,7 +472,7 @@ __global__ void __launch_bounds__(RCfg<N>::CTA, RCfg<N>::MINB) flux_bvp_reg_kern
       if (beam) {
         dirint = fbeam * fact;
         fldir = umu0 * fbeam * fact;
-        fdir = umu0 * fbeam * exp(-utau * rumu0);
+        fdir = SPH ? fabs(umu0) * fbeam * exp(-utau / ch) : umu0 * fbeam * exp(-utau * rumu0);
       }
       double iv[N];
 #pragma unroll

@@ -84,7 +84,7 @@ struct TMask {
   }
 };
 
-template <int N, bool GEN = false, bool JAC = false>
+template <int N, bool GEN = false, bool JAC = false, bool SPH = false>
 __global__ void __launch_bounds__(TCfg<N>::CTA, TCfg<N>::MINB) flux_bvp_tile_kernel(FluxParams p) {
   using C = TCfg<N>;
   constexpr int NN = C::NN, PR = C::PR, RG = C::RG, RPT = C::RPT, CPT = C::CPT, NW = C::NW;
@@ -172,6 +172,13 @@ __global__ void __launch_bounds__(TCfg<N>::CTA, TCfg<N>::MINB) flux_bvp_tile_ker
   const double* btr = rec + il.btr;
   const double* dtau_s = rec + il.dtau_s;
   auto LR = [&](int l) { return lrec0 + (long long)l * lstride; };
+  // pseudo-spherical beam: layer l's record [Z1 | xba | ch], and its particular
+  // solution exp(-xba tau) (Z0 + Z1 tau) at stream iq (solve0, FluxSolver.cpp:1001-1090)
+  auto SR = [&](int l) { return p.sph + ((long long)i * L + l) * sph_stride(N); };
+  auto zsph = [&](int l, int iq, double tau) {
+    const double* sr = SR(l);
+    return exp(-sr[sph_xba(N)] * tau) * (__ldg(LR(l) + lrec_zb(N) + iq) + sr[iq] * tau);
+  };
 
   // this thread's tile
   double a[RPT][CPT], rh[RPT];
@@ -268,8 +275,13 @@ __global__ void __launch_bounds__(TCfg<N>::CTA, TCfg<N>::MINB) flux_bvp_tile_ker
             const double T = btr[l + 1], tau = taus[l + 1];
             double sum = 0.0;
             if (beam) {
-              sum += __ldg(ln + lrec_zb(N) + jq) * T;
-              sum -= __ldg(lr + lrec_zb(N) + jq) * T;
+              if constexpr (SPH) {
+                sum += zsph(l + 1, jq, tau);
+                sum -= zsph(l, jq, tau);
+              } else {
+                sum += __ldg(ln + lrec_zb(N) + jq) * T;
+                sum -= __ldg(lr + lrec_zb(N) + jq) * T;
+              }
             }
             if (thermal) {
               sum += __ldg(ln + lrec_z0(N) + jq) - __ldg(lr + lrec_z0(N) + jq);
@@ -302,7 +314,7 @@ __global__ void __launch_bounds__(TCfg<N>::CTA, TCfg<N>::MINB) flux_bvp_tile_ker
             const double fisob = mode_m == 0 ? rec[H_FISOB] : 0.0;
             double sum = 0.0;
             if (dlbc) {
-              if (beam) sum -= __ldg(lr + lrec_zb(N) + NN + rb) * T;
+              if (beam) sum -= SPH ? zsph(l, NN + rb, tau) : __ldg(lr + lrec_zb(N) + NN + rb) * T;
               if (thermal) {
                 sum -= __ldg(lr + lrec_z0(N) + NN + rb);
                 sum -= __ldg(lr + lrec_z1(N) + NN + rb) * tau;
@@ -313,7 +325,7 @@ __global__ void __launch_bounds__(TCfg<N>::CTA, TCfg<N>::MINB) flux_bvp_tile_ker
                 double refl = 0.0;
                 for (int jj = 0; jj < NN; ++jj) {
                   double ps = 0.0;
-                  if (beam) ps += __ldg(lr + lrec_zb(N) + NN - 1 - jj) * T;
+                  if (beam) ps += SPH ? zsph(l, NN - 1 - jj, tau) : __ldg(lr + lrec_zb(N) + NN - 1 - jj) * T;
                   if (thermal)
                     ps += __ldg(lr + lrec_z0(N) + NN - 1 - jj) + __ldg(lr + lrec_z1(N) + NN - 1 - jj) * tau;
                   refl += wt[jj] * mu[jj] * alb * ps;
@@ -321,7 +333,7 @@ __global__ void __launch_bounds__(TCfg<N>::CTA, TCfg<N>::MINB) flux_bvp_tile_ker
                 sum += 2.0 * refl;
               }
               if (beam) {
-                sum -= __ldg(lr + lrec_zb(N) + NN + rb) * T;
+                sum -= SPH ? zsph(l, NN + rb, tau) : __ldg(lr + lrec_zb(N) + NN + rb) * T;
                 if (!lyrcut) sum += alb * umu0 * fbeam * T / PI;
               }
               if (thermal) {
@@ -476,11 +488,14 @@ __global__ void __launch_bounds__(TCfg<N>::CTA, TCfg<N>::MINB) flux_bvp_tile_ker
       ec[j] = x[j] * exp(-eig[j] * d);
     }
     __syncthreads();
-    const double fact = beam ? exp(-utaupr / umu0) : 0.0;
+    // pseudo-spherical: the Chapman factor of the layer replaces mu0
+    // (computeFluxes, FluxSolver.cpp:1184-1188, 1216-1219)
+    const double ch = SPH && beam ? SR(l)[sph_ch(N)] : 0.0;
+    const double fact = beam ? (SPH ? exp(-utaupr / ch) : exp(-utaupr / umu0)) : 0.0;
     for (int r = t; r < N; r += TEAM) {
       double s = 0.0;
       for (int j = 0; j < N; ++j) s += Gl[r * N + j] * ec[j];
-      if (beam) s += lr[lrec_zb(N) + r] * fact;
+      if (beam) s += SPH ? zsph(l, r, utaupr) : lr[lrec_zb(N) + r] * fact;
       if (thermal) s += lr[lrec_z0(N) + r] + lr[lrec_z1(N) + r] * utaupr;
       Iv[r] = s;
     }
@@ -490,7 +505,7 @@ __global__ void __launch_bounds__(TCfg<N>::CTA, TCfg<N>::MINB) flux_bvp_tile_ker
       if (beam) {
         dirint = fbeam * fact;
         fldir = umu0 * fbeam * fact;
-        fdir = umu0 * fbeam * exp(-utau / umu0);
+        fdir = SPH ? fabs(umu0) * fbeam * exp(-utau / ch) : umu0 * fbeam * exp(-utau / umu0);
       }
       double ua = 0.0, uad = 0.0, uau = 0.0, fldn = 0.0, fup = 0.0;
       for (int iq = 0; iq < NN; ++iq) {

@@ -131,6 +131,8 @@ static __global__ void __launch_bounds__(128) flux_setup_kernel(FluxParams p) {
       if (emis < 0.0 || emis > 1.0) bad = true;
     }
     if ((p.flags & DSP_FLAG_DELTA_M_PLUS) && p.nmom < N + 1) bad = true;
+    // bottom_radius > 0 with the pseudo-spherical beam (DisortFluxConfig.cpp:127-133)
+    if ((p.flags & DSP_FLAG_SPHERICAL_BEAM) && !(p.rbot(i) > 0.0)) bad = true;
   }
   if (__any_sync(0xffffffffu, bad)) {
     if (lane == 0) set_status(p.status, i, DSP_ERR_INVALID_INPUT);

@@ -93,7 +93,8 @@ def subset(w: dict, idx) -> dict:
     out = dict(w)
     out["n_inst"] = int(idx.size)
     arrs = {}
-    per_ndim = {"delta_tau": 1, "single_scat_albedo": 1, "phase_function_moments": 2, "temperature": 1}
+    per_ndim = {"delta_tau": 1, "single_scat_albedo": 1, "phase_function_moments": 2, "temperature": 1,
+                "level_altitudes": 1}
     for k, a in w["arrays"].items():
         if isinstance(a, np.ndarray):
             nd = per_ndim.get(k, 0)

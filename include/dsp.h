@@ -40,7 +40,7 @@
 extern "C" {
 #endif
 
-#define DSP_API_VERSION 1
+#define DSP_API_VERSION 2
 
 typedef enum dsp_status {
   DSP_OK = 0,
@@ -61,7 +61,7 @@ typedef enum dsp_status {
 #define DSP_FLAG_DIFFUSION_LOWER_BC (1u << 2) /* use_diffusion_lower_bc */
 #define DSP_FLAG_INDEX_FROM_BOTTOM  (1u << 3) /* index_from_bottom (layer/level arrays reversed) */
 #define DSP_FLAG_DEVICE_POINTERS    (1u << 4) /* every pointer is device memory */
-#define DSP_FLAG_SPHERICAL_BEAM     (1u << 5) /* use_spherical_beam: rejected, DSP_ERR_UNSUPPORTED */
+#define DSP_FLAG_SPHERICAL_BEAM     (1u << 5) /* use_spherical_beam (flux batches; the general batch rejects it) */
 #define DSP_FLAG_TEMPERATURE_JAC    (1u << 6) /* compute_temperature_jacobian: use dsp_flux_bands_solve_jac */
 /*
  * Henyey-Greenstein fast path (flux batches): phase_function_moments holds ONE
@@ -106,6 +106,9 @@ typedef struct dsp_flux_batch {
   dsp_darray isotropic_flux_bottom;   /* [1] */
   dsp_darray temperature_top;         /* [1] */
   dsp_darray temperature_bottom;      /* [1] */
+  /* pseudo-spherical beam (DSP_FLAG_SPHERICAL_BEAM; may be NULL otherwise) */
+  dsp_darray level_altitudes;         /* [L+1], top down, the units of bottom_radius */
+  dsp_darray bottom_radius;           /* [1] */
 } dsp_flux_batch;
 
 /* FluxResult (FluxResult.hpp:14-22): each array is [n_inst][L+1]. */

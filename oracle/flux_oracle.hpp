@@ -19,6 +19,9 @@ struct FluxInstance {
   int pmom_count = 0;  // stride of pmom per layer
   bool thermal = false, delta_m_plus = false, diffusion_lower_bc = false, index_from_bottom = false;
   bool temperature_jac = false;  // compute_temperature_jacobian
+  bool spherical = false;        // use_spherical_beam
+  double bottom_radius = 0;
+  const double* level_altitudes = nullptr;  // [L+1] (spherical only)
   double wavenumber_low = 0, wavenumber_high = 0;
   double surface_albedo = 0, emissivity_top = 1, direct_beam_flux = 0, direct_beam_mu = 0.5;
   double isotropic_flux_top = 0, isotropic_flux_bottom = 0, temperature_top = 0, temperature_bottom = 0;
@@ -61,6 +64,7 @@ inline int validate_flux_instance(const FluxInstance& c) {
     if (c.temperature_top < 0.0 || c.temperature_bottom < 0.0) return DSP_ERR_INVALID_INPUT;
     if (c.emissivity_top < 0.0 || c.emissivity_top > 1.0) return DSP_ERR_INVALID_INPUT;
   }
+  if (c.spherical && (c.bottom_radius <= 0.0 || c.level_altitudes == nullptr)) return DSP_ERR_INVALID_INPUT;
   if (c.delta_m_plus && c.num_phase_func_moments < N + 1) return DSP_ERR_INVALID_INPUT;
   return DSP_OK;
 }
@@ -220,6 +224,47 @@ inline int layer_eigen(int nn, const double* amb, const double* apb, const doubl
   return DSP_OK;
 }
 
+// The Chapman function of the pseudo-spherical beam (chapmanImpl,
+// FluxSolver.cpp:1503-1566): the slant optical depth from the top to a point
+// a fraction tau_frac from the bottom of layer lc (1-based) along the beam
+// through a spherical shell atmosphere of level altitudes zd[0..L] (top down)
+// above radius r, with dtau_lyr the layers' optical depths.
+inline double chapman(int lc, double tau_frac, const double* zd, const double* dtau_lyr, int num_layers, double r,
+                      double direct_beam_mu) {
+  const double DEG = M_PI / 180.0;
+  const double zenang = std::acos(direct_beam_mu) * 180.0 / M_PI;
+  const double zenrad = zenang * DEG;
+  auto ZD = [&](int j) { return zd[j]; };
+  auto DT = [&](int j) { return dtau_lyr[j - 1]; };
+  const double xp = r + ZD(lc) + (ZD(lc - 1) - ZD(lc)) * tau_frac;
+  const double xpsinz = xp * std::sin(zenrad);
+  if (zenang > 90.0 && xpsinz < r) return 1.0e+20;
+  int id = lc;
+  if (zenang > 90.0)
+    for (int j = lc; j <= num_layers; ++j)
+      if (xpsinz < (ZD(j - 1) + r) && xpsinz >= (ZD(j) + r)) id = j;
+  double sum = 0.0;
+  for (int j = 1; j <= id; ++j) {
+    double fact = 1.0, fact2 = 1.0;
+    if (j > lc) fact = 2.0;
+    else if (j == lc && lc == id && zenang > 90.0) fact2 = -1.0;
+    const double rj = r + ZD(j - 1);
+    double rjp1 = r + ZD(j);
+    if (j == lc && id == lc) rjp1 = xp;
+    const double dhj = ZD(j - 1) - ZD(j);
+    double dsj;
+    if (id > lc && j == id) dsj = std::sqrt(rj * rj - xpsinz * xpsinz);
+    else dsj = std::sqrt(rj * rj - xpsinz * xpsinz) - fact2 * std::sqrt(rjp1 * rjp1 - xpsinz * xpsinz);
+    sum += DT(j) * fact * dsj / dhj;
+  }
+  if (id > lc) {
+    const double dhj = ZD(lc - 1) - ZD(lc);
+    const double dsj = std::sqrt(xp * xp - xpsinz * xpsinz) - std::sqrt((ZD(lc) + r) * (ZD(lc) + r) - xpsinz * xpsinz);
+    sum += DT(lc) * dsj / dhj;
+  }
+  return sum;
+}
+
 // ---------------------------------------------------------------------------
 // The flux solver.  One object per thread, reused across instances, like the
 // reference spectral loop (python_bindings.cpp:170-190).
@@ -236,6 +281,10 @@ class FluxOracle {
   std::vector<double> mu, wt, dsim, dinv, ylm;  // ylm[(N+1) x N]
   std::vector<double> dtau_s, tau_s, ssa_s, gl;  // gl[L][N]
   std::vector<double> beam_tr;                  // [L+1]
+  // pseudo-spherical beam: Chapman factor per layer, the slope of the beam
+  // particular solution and its attenuation (FluxSolver.cpp:391-419, 650-738)
+  std::vector<double> chap, zbs1, xba;
+  std::vector<double> rev_zalt;
   std::vector<double> kk, G, C;                 // kk[L][N], G[L][N][N], C[L][N][N]
   std::vector<double> zb, z0, z1, xr0, xr1;     // particular solutions
   // derivatives of the thermal source w.r.t. the layer's top / bottom level
@@ -281,6 +330,11 @@ inline int FluxOracle::solve(const FluxInstance& cfg_in, const FluxOutput& out) 
       rev_temp.assign(cfg.temperature, cfg.temperature + L + 1);
       std::reverse(rev_temp.begin(), rev_temp.end());
       cfg.temperature = rev_temp.data();
+    }
+    if (cfg.level_altitudes) {
+      rev_zalt.assign(cfg.level_altitudes, cfg.level_altitudes + L + 1);
+      std::reverse(rev_zalt.begin(), rev_zalt.end());
+      cfg.level_altitudes = rev_zalt.data();
     }
   }
   int st = validate_flux_instance(cfg);
@@ -355,9 +409,26 @@ inline int FluxOracle::solve(const FluxInstance& cfg_in, const FluxOutput& out) 
     }
     // Beam transmission for lc < ncut of the absorption loop (FluxSolver.cpp:391-412).
     // Entries past that cut are left at zero, as on a freshly constructed solver.
+    chap.assign(L, 0.0);
     if (cfg.direct_beam_flux > 0.0) {
       beam_tr[0] = 1.0;
-      for (int lc = 0; lc < ncut; ++lc) beam_tr[lc + 1] = std::exp(-tau_s[lc + 1] / cfg.direct_beam_mu);
+      if (cfg.spherical) {
+        // Chapman factors on the scaled depths (FluxSolver.cpp:396-415)
+        for (int lc = 0; lc < ncut; ++lc) {
+          const double taup_mid = tau_s[lc] + dtau_s[lc] / 2.0;
+          const double chtau_mid = chapman(lc + 1, 0.5, cfg.level_altitudes, dtau_s.data(), L, cfg.bottom_radius,
+                                           cfg.direct_beam_mu);
+          chap[lc] = taup_mid / chtau_mid;
+          const double chtau = chapman(lc + 1, 0.0, cfg.level_altitudes, dtau_s.data(), L, cfg.bottom_radius,
+                                       cfg.direct_beam_mu);
+          beam_tr[lc + 1] = std::exp(-chtau);
+        }
+      } else {
+        for (int lc = 0; lc < ncut; ++lc) {
+          chap[lc] = cfg.direct_beam_mu;
+          beam_tr[lc + 1] = std::exp(-tau_s[lc + 1] / cfg.direct_beam_mu);
+        }
+      }
     }
     lyrcut = (abstau >= abscut && !cfg.thermal && L > 1);
     if (!lyrcut) ncut = L;
@@ -440,9 +511,69 @@ inline int FluxOracle::solve(const FluxInstance& cfg_in, const FluxOutput& out) 
 
   // Beam particular solution (computeBeamSource, FluxSolver.cpp:595-643)
   zb.assign((size_t)L * N, 0.0);
+  zbs1.assign((size_t)L * N, 0.0);
+  xba.assign(L, 0.0);
   std::vector<double> A((size_t)N * N), x(N);
   std::vector<int> piv(N);
-  if (cfg.direct_beam_flux > 0.0) {
+  if (cfg.direct_beam_flux > 0.0 && cfg.spherical) {
+    // pseudo-spherical source (computeBeamSourceSpherical, FluxSolver.cpp:650-738):
+    // Z(tau) = exp(-xba tau) (Z0 + Z1 tau) with xba = 1 / Chapman factor
+    std::vector<double> yb(N + 1), zj(N), xb0(N), xb1(N), z1v(N), z0v(N);
+    const double umu0 = -cfg.direct_beam_mu;
+    legendre_flat(1, 0, 1, N - 1, &umu0, yb.data());
+    const double big = std::sqrt(std::numeric_limits<double>::max()) / 1.0e10;
+    for (int lc = 0; lc < ncut; ++lc) {
+      for (int iq = 0; iq < N; ++iq) {
+        double sum = 0.0;
+        for (int k = 0; k < N; ++k) sum += gl[(size_t)lc * N + k] * Y(k, iq) * yb[k];
+        zj[iq] = cfg.direct_beam_flux * sum / (4.0 * M_PI);
+      }
+      const double q0a = beam_tr[lc], q2a = beam_tr[lc + 1];
+      double xb = 1.0 / chap[lc];
+      if (std::abs(xb) > big && tau_s[lc + 1] > 1.0) xb = 0.0;
+      if (std::abs(xb * tau_s[lc + 1]) > std::log(big)) xb = 0.0;
+      if (std::abs(xb) > 1.0e-5)
+        for (int iq = 0; iq < NN; ++iq)
+          if (std::abs((std::abs(xb) - 1.0 / mu[iq]) / xb) < 0.05) {
+            xb *= 1.001;
+            break;
+          }
+      const double deltat = tau_s[lc + 1] - tau_s[lc];
+      for (int iq = 0; iq < N; ++iq) {
+        const double q0 = q0a * zj[iq], q2 = q2a * zj[iq];
+        xb1[iq] = (q2 * std::exp(xb * tau_s[lc + 1]) - q0 * std::exp(xb * tau_s[lc])) / deltat;
+        xb0[iq] = q0 * std::exp(xb * tau_s[lc]) - xb1[iq] * tau_s[lc];
+      }
+      const double* Cl = &C[(size_t)lc * N * N];
+      auto build = [&]() {
+        for (int i = 0; i < N; ++i)
+          for (int j = 0; j < N; ++j) A[i * N + j] = -Cl[i * N + j];
+        for (int iq = 0; iq < N; ++iq) A[iq * N + iq] += 1.0 + xb * mu[iq];
+      };
+      build();
+      // dither when near-singular: 1 / Frobenius norm of the system (FluxSolver.cpp:707-718)
+      double fro = 0.0;
+      for (int e = 0; e < N * N; ++e) fro += A[e] * A[e];
+      const double rcond_approx = 1.0 / std::sqrt(fro);
+      if (rcond_approx < 1.0e-4) {
+        if (xb == 0.0) xb = 5.0e-9;
+        xb *= 1.00000005;
+        build();
+      }
+      xba[lc] = xb;
+      lu_factor(A.data(), N, N, piv.data());
+      for (int iq = 0; iq < N; ++iq) z1v[iq] = xb1[iq];
+      lu_solve(A.data(), N, N, piv.data(), z1v.data());
+      for (int iq = 0; iq < N; ++iq) z0v[iq] = xb0[iq] + mu[iq] * z1v[iq];
+      lu_solve(A.data(), N, N, piv.data(), z0v.data());
+      for (int iq = 0; iq < NN; ++iq) {
+        zb[(size_t)lc * N + NN + iq] = z0v[iq];
+        zb[(size_t)lc * N + NN - 1 - iq] = z0v[iq + NN];
+        zbs1[(size_t)lc * N + NN + iq] = z1v[iq];
+        zbs1[(size_t)lc * N + NN - 1 - iq] = z1v[iq + NN];
+      }
+    }
+  } else if (cfg.direct_beam_flux > 0.0) {
     std::vector<double> yb(N + 1);
     const double umu0 = -cfg.direct_beam_mu;
     legendre_flat(1, 0, 1, N - 1, &umu0, yb.data());
@@ -621,6 +752,14 @@ inline int FluxOracle::solve(const FluxInstance& cfg_in, const FluxOutput& out) 
   rhs.assign(nc, 0.0);
   const bool beam = cfg.direct_beam_flux > 0.0;
   auto ZB = [&](int lc, int i) { return zb[(size_t)lc * N + i]; };
+  // the beam particular solution of layer lc at scaled depth tau: plane-parallel
+  // zb(lc) T (T the transmission at that level), pseudo-spherical
+  // exp(-xba tau) (zb + zbs1 tau) (solve0, FluxSolver.cpp:1001-1090)
+  const bool sph = cfg.spherical;
+  auto ZBT = [&](int lc, int i, double tau, double T) {
+    if (sph) return std::exp(-xba[lc] * tau) * (zb[(size_t)lc * N + i] + zbs1[(size_t)lc * N + i] * tau);
+    return ZB(lc, i) * T;
+  };
   auto Z0 = [&](int lc, int i) { return z0[(size_t)lc * N + i]; };
   auto Z1 = [&](int lc, int i) { return z1[(size_t)lc * N + i]; };
   for (int iq = 0; iq < NN; ++iq) {
@@ -634,7 +773,7 @@ inline int FluxOracle::solve(const FluxInstance& cfg_in, const FluxOutput& out) 
   if (cfg.diffusion_lower_bc) {
     for (int iq = 0; iq < NN; ++iq) {
       double s = 0.0;
-      if (beam) s -= ZB(lb, NN + iq) * beam_tr[ncut];
+      if (beam) s -= ZBT(lb, NN + iq, tau_s[ncut], beam_tr[ncut]);
       if (cfg.thermal) { s -= Z0(lb, NN + iq); s -= Z1(lb, NN + iq) * tau_s[ncut]; }
       s += planck_bottom + mu[iq] * planck_bottom_deriv;
       rhs[nc - NN + iq] = s;
@@ -646,14 +785,14 @@ inline int FluxOracle::solve(const FluxInstance& cfg_in, const FluxOutput& out) 
         double refl = 0.0;
         for (int jq = 0; jq < NN; ++jq) {
           double ps = 0.0;
-          if (beam) ps += ZB(lb, NN - 1 - jq) * beam_tr[ncut];
+          if (beam) ps += ZBT(lb, NN - 1 - jq, tau_s[ncut], beam_tr[ncut]);
           if (cfg.thermal) ps += Z0(lb, NN - 1 - jq) + Z1(lb, NN - 1 - jq) * tau_s[ncut];
           refl += wt[jq] * mu[jq] * cfg.surface_albedo * ps;
         }
         s += 2.0 * refl;
       }
       if (beam) {
-        s -= ZB(lb, NN + iq) * beam_tr[ncut];
+        s -= ZBT(lb, NN + iq, tau_s[ncut], beam_tr[ncut]);
         if (!lyrcut) s += cfg.surface_albedo * cfg.direct_beam_mu * cfg.direct_beam_flux * beam_tr[ncut] / M_PI;
       }
       if (cfg.thermal) { s -= Z0(lb, NN + iq); s -= Z1(lb, NN + iq) * tau_s[ncut]; }
@@ -666,7 +805,7 @@ inline int FluxOracle::solve(const FluxInstance& cfg_in, const FluxOutput& out) 
     const int ipnt = lc * N - NN;
     for (int iq = 0; iq < N; ++iq) {
       double s = 0.0;
-      if (beam) { s += ZB(lc, iq) * beam_tr[lc]; s -= ZB(lc - 1, iq) * beam_tr[lc]; }
+      if (beam) { s += ZBT(lc, iq, tau_s[lc], beam_tr[lc]); s -= ZBT(lc - 1, iq, tau_s[lc], beam_tr[lc]); }
       if (cfg.thermal) {
         s += Z0(lc, iq) - Z0(lc - 1, iq);
         s += (Z1(lc, iq) - Z1(lc - 1, iq)) * tau_s[lc];
@@ -704,8 +843,14 @@ inline int FluxOracle::solve(const FluxInstance& cfg_in, const FluxOutput& out) 
     const double utaupr = tau_s[lu];
     double fact = 0.0, dirint = 0.0, fldir = 0.0, fdir = 0.0;
     if (beam) {
-      fact = std::exp(-utaupr / cfg.direct_beam_mu);
-      fdir = cfg.direct_beam_mu * cfg.direct_beam_flux * std::exp(-tauc_lu / cfg.direct_beam_mu);
+      if (sph) {  // FluxSolver.cpp:1184-1188
+        const double ch = chap[lyu];
+        fact = std::exp(-utaupr / ch);
+        fdir = std::abs(cfg.direct_beam_mu) * cfg.direct_beam_flux * std::exp(-tauc_lu / ch);
+      } else {
+        fact = std::exp(-utaupr / cfg.direct_beam_mu);
+        fdir = cfg.direct_beam_mu * cfg.direct_beam_flux * std::exp(-tauc_lu / cfg.direct_beam_mu);
+      }
       dirint = cfg.direct_beam_flux * fact;
       fldir = cfg.direct_beam_mu * cfg.direct_beam_flux * fact;
     }
@@ -717,8 +862,14 @@ inline int FluxOracle::solve(const FluxInstance& cfg_in, const FluxOutput& out) 
       for (int j = 0; j < N; ++j) s += Gv(lyu, i, j) * ec[j];
       inten[i] = s;
     }
-    if (beam)
-      for (int i = 0; i < N; ++i) inten[i] += ZB(lyu, i) * fact;
+    if (beam) {
+      if (sph) {
+        const double be = std::exp(-xba[lyu] * utaupr);
+        for (int i = 0; i < N; ++i) inten[i] += be * (ZB(lyu, i) + zbs1[(size_t)lyu * N + i] * utaupr);
+      } else {
+        for (int i = 0; i < N; ++i) inten[i] += ZB(lyu, i) * fact;
+      }
+    }
     if (cfg.thermal)
       for (int i = 0; i < N; ++i) inten[i] += Z0(lyu, i) + Z1(lyu, i) * utaupr;
     double ua = 0.0, uad = 0.0, uau = 0.0, fldn = 0.0, fup = 0.0;

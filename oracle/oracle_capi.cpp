@@ -81,9 +81,10 @@ int oracle_flux_bands_solve_jac(const dsp_flux_batch* b, const dsp_flux_out* o, 
         c.temperature_jac = true;
       }
       int st;
-      if ((b->flags & DSP_FLAG_SPHERICAL_BEAM) != 0) {
-        st = DSP_ERR_UNSUPPORTED;
-      } else if (!c.delta_tau || !c.ssa || !c.pmom) {
+      c.spherical = (b->flags & DSP_FLAG_SPHERICAL_BEAM) != 0;
+      c.level_altitudes = at(b->level_altitudes, i);
+      c.bottom_radius = scalar(b->bottom_radius, i, 0.0);
+      if (!c.delta_tau || !c.ssa || !c.pmom) {
         st = DSP_ERR_INVALID_INPUT;
       } else {
         st = solver.solve(c, fo);

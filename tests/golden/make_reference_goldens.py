@@ -89,6 +89,10 @@ CASES = [
     dict(test="CloudGarciaSiewert", suite="DeltaMPlus", N=16, L=1, nmom=298, dtau=[5.0], ssa=[1.0],
          phase=[("cloud",)], fbeam=1.0, umu0=0.5, albedo=0.0, dm_plus=True, utau=[0.0, 5.0],
          umu=[-1.0, -0.5, 0.5, 1.0], phi=[0.0]),
+    # pseudo-spherical beam (test_solver.cpp:4459-4533): altitudes 60/30/0 km, radius 6371 km
+    dict(test="SphericalGeometry", N=16, L=2, nmom=0, dtau=[0.5, 1.0], ssa=[0.9, 0.8], phase=[("hg", 0.8)],
+         fbeam=1.0, umu0=0.5, albedo=0.1, spherical=True, zalt=[60.0, 30.0, 0.0], radius=6371.0,
+         umu=[-0.5, 0.1, 0.5, 1.0], phi=[0.0]),
 ]
 
 FIELDS = ("flux_direct_beam", "flux_down", "flux_up", "flux_tau_divergence", "mean_intensity",
@@ -190,6 +194,8 @@ def main():
             temperature_top=c.get("ttemp", 0.0), temperature_bottom=c.get("btemp", 0.0),
             emissivity_top=1.0, use_delta_m_plus=bool(c.get("dm_plus", False)),
             tau_user=c.get("utau"), mu_user=c.get("umu"), phi_user=c.get("phi"),
+            use_spherical_beam=bool(c.get("spherical", False)), level_altitudes=c.get("zalt"),
+            bottom_radius=c.get("radius", 0.0),
             expect_flux=fl, expect_intensity=it,
         ))
     out = dict(generated_by="tests/golden/make_reference_goldens.py",

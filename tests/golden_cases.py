@@ -12,8 +12,15 @@ GOLDEN = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden", "ref
 
 
 def load_cases() -> list:
+    """The plane-parallel cases (every solver path supports them)."""
     with open(GOLDEN) as f:
-        return json.load(f)["cases"]
+        return [c for c in json.load(f)["cases"] if not c.get("use_spherical_beam")]
+
+
+def load_spherical_cases() -> list:
+    """The pseudo-spherical beam cases (flux path)."""
+    with open(GOLDEN) as f:
+        return [c for c in json.load(f)["cases"] if c.get("use_spherical_beam")]
 
 
 def flux_workload(c: dict) -> dict:
@@ -35,6 +42,10 @@ def flux_workload(c: dict) -> dict:
         isotropic_flux_top=c["isotropic_flux_top"], isotropic_flux_bottom=0.0,
         temperature_top=c["temperature_top"], temperature_bottom=c["temperature_bottom"],
     )
+    if c.get("use_spherical_beam"):
+        flags |= capi.FLAG_SPHERICAL_BEAM
+        arrays["level_altitudes"] = np.array(c["level_altitudes"], dtype=np.float64)
+        arrays["bottom_radius"] = c["bottom_radius"]
     return dict(name=c["name"], n_inst=1, num_streams=c["num_streams"], num_layers=L,
                 num_phase_func_moments=c["num_phase_func_moments"], pmom_count=pm.shape[1],
                 flags=flags, arrays=arrays)

@@ -217,3 +217,33 @@ def test_general_spectral_bands_with_overrides_match_oracle():
     assert_parity_general(_as_outputs(res, True), ref, "solve_spectral_bands")
     # the caller's config is not modified by the spectral loop
     assert c.num_user_tau == 3 and list(c.delta_tau) == [0.1, 0.5, 1.0, 2.0]
+
+
+def test_flux_solver_temperature_jacobians():
+    """compute_temperature_jacobian through the DisORT++ API: FluxResult's six
+    *_temperature_jac fields ([L+1][L+2]) equal the oracle's within the
+    Jacobian tolerance of test_jacobian_gpu.py; empty without thermal emission,
+    as the reference clears them."""
+    c = _flux_cfg()
+    c.compute_temperature_jacobian = True
+    r = disortpp.DisortFluxSolver16().solve(c)
+    out, st, jac = oracle_lib.flux_solve_jac(_as_workload(c, 500.0, 520.0))
+    assert st[0] == 0
+    names = dict(flux_up="flux_up_temperature_jac", flux_down="flux_down_temperature_jac",
+                 mean_intensity="mean_intensity_temperature_jac",
+                 mean_intensity_down="mean_intensity_down_temperature_jac",
+                 mean_intensity_up="mean_intensity_up_temperature_jac",
+                 flux_divergence="flux_divergence_temperature_jac")
+    for f, attr in names.items():
+        got = np.array(getattr(r, attr))
+        assert got.shape == (6, 7)
+        ref = jac[f][0]
+        scale = np.abs(ref).max()
+        assert np.all(np.abs(got - ref) <= 3e-8 * np.maximum(np.abs(ref), 1e-3 * scale)), f
+    # spectral loop: one Jacobian per band
+    res = disortpp.solve_flux_spectral_bands(c, [(500.0, 520.0), (600.0, 610.0)])
+    assert len(res[1].flux_up_temperature_jac) == 6 and len(res[1].flux_up_temperature_jac[0]) == 7
+    np.testing.assert_array_equal(np.array(res[0].flux_up_temperature_jac), np.array(r.flux_up_temperature_jac))
+    c.use_thermal_emission = False
+    r = disortpp.DisortFluxSolver16().solve(c)
+    assert len(r.flux_up_temperature_jac) == 0

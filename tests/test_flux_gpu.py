@@ -254,3 +254,78 @@ def test_hg_fast_path_equals_moment_path():
     assert rc == rc2 == 0 and not gst.any()
     for f in capi.FLUX_OUT_FIELDS:
         np.testing.assert_array_equal(got[f], ref[f])
+
+
+SPH_CASES = golden_cases.load_spherical_cases()
+
+
+@pytest.mark.parametrize("case", SPH_CASES, ids=[c["name"] for c in SPH_CASES])
+def test_spherical_golden(case):
+    w = golden_cases.flux_workload(case)
+    got, gst, ref, rst = both(w)
+    assert gst[0] == rst[0] == 0
+    assert_parity(got, ref, case["name"])
+    for e in case["expect_flux"]:
+        assert abs(got[e["field"]][0, golden_cases.level_of(case, e["index"])] - e["value"]) <= e["tol"]
+
+
+def spherical_columns(nstr, L, n, seed, thermal=False):
+    """Beam columns through spherical shells (altitudes L*2 km .. 0 over a
+    6371 km radius), mu0 down to 0.1 so the slant paths matter, delta-M+,
+    ragged optical depths so the absorption cut fires on some columns."""
+    rng = np.random.default_rng(seed)
+    pc = nstr + 2
+    w = dict(n_inst=n, num_streams=nstr, num_layers=L, num_phase_func_moments=nstr + 1, pmom_count=pc,
+             flags=capi.FLAG_SPHERICAL_BEAM | capi.FLAG_DELTA_M_PLUS | (capi.FLAG_THERMAL if thermal else 0),
+             arrays=dict(delta_tau=np.clip(rng.lognormal(-2, 1.5, (n, L)), 1e-6, 20),
+                         single_scat_albedo=rng.uniform(0, 0.99, (n, L)),
+                         phase_function_moments=workloads.hg_moments(rng.uniform(0.5, 0.9, (n, L)), pc),
+                         surface_albedo=rng.uniform(0, 0.6, n), direct_beam_flux=1.0,
+                         direct_beam_mu=rng.uniform(0.1, 1.0, n),
+                         level_altitudes=np.linspace(2.0 * L, 0.0, L + 1), bottom_radius=6371.0))
+    if thermal:
+        w["arrays"].update(wavenumber_low=rng.uniform(300, 1500, n), temperature=200 + 100 * rng.random(L + 1),
+                           temperature_bottom=300.0, temperature_top=0.0)
+        w["arrays"]["wavenumber_high"] = w["arrays"]["wavenumber_low"] * 1.01
+    return w
+
+
+@pytest.mark.parametrize("nstr", capi.SUPPORTED_NSTR)
+def test_spherical_beam_all_stream_counts(nstr):
+    """The reference's SphericalBeam4/16 column (test_flux_solver.cpp:309-358:
+    five isotropic layers of optical depth 0.1, mu0 0.3, altitudes 100..0 km)
+    at every stream count, then ragged delta-M+ columns, bottom-up indexing
+    and a thermal source with them."""
+    pc = nstr + 1
+    w = dict(n_inst=1, num_streams=nstr, num_layers=5, num_phase_func_moments=0, pmom_count=pc,
+             flags=capi.FLAG_SPHERICAL_BEAM,
+             arrays=dict(delta_tau=np.full(5, 0.1), single_scat_albedo=np.full(5, 0.9),
+                         phase_function_moments=workloads.hg_moments(np.zeros(5), pc), surface_albedo=0.1,
+                         direct_beam_flux=1.0, direct_beam_mu=0.3,
+                         level_altitudes=np.array([100.0, 80.0, 60.0, 40.0, 20.0, 0.0]), bottom_radius=6371.0))
+    got, gst, ref, rst = both(w)
+    assert gst[0] == rst[0] == 0
+    assert_parity(got, ref, f"SphericalBeam N={nstr}")
+    L = 24 if nstr < 32 else 12
+    w = spherical_columns(nstr, L, 12, seed=400 + nstr)
+    got, gst, ref, rst = both(w)
+    assert np.all(gst == 0) and np.all(rst == 0)
+    assert_parity(got, ref, f"spherical columns N={nstr}")
+    got, gst, ref, rst = both(w, extra_flags=capi.FLAG_INDEX_FROM_BOTTOM)
+    assert_parity(got, ref, f"spherical columns N={nstr} bottom-up")
+    w = spherical_columns(nstr, L, 6, seed=500 + nstr, thermal=True)
+    got, gst, ref, rst = both(w)
+    assert np.all(gst == 0)
+    assert_parity(got, ref, f"spherical thermal columns N={nstr}")
+
+
+def test_spherical_beam_invalid_radius_and_missing_altitudes():
+    w = spherical_columns(8, 6, 4, seed=7)
+    w["arrays"]["bottom_radius"] = np.array([6371.0, -1.0, 6371.0, 0.0])
+    got, gst, ref, rst = both(w)
+    assert list(gst) == [0, capi.DSP_ERR_INVALID_INPUT, 0, capi.DSP_ERR_INVALID_INPUT] and np.all(gst == rst)
+    ok = [0, 2]
+    assert_parity({k: v[ok] for k, v in got.items()}, {k: v[ok] for k, v in ref.items()}, "valid rows")
+    w["arrays"]["level_altitudes"] = None
+    _, _, rc = gpu_lib.flux_solve(w)
+    assert rc == capi.DSP_ERR_INVALID_INPUT

@@ -8,8 +8,9 @@ derivative from the mean-intensity one): two builds of the same oracle source,
 double and extended-precision intermediates, differ by up to 1.4e-8 of an
 entry on thermal-sweep columns, and theoretically-zero entries (the downward
 flux at the top) are rounding noise of the larger entries of their output.  So
-every GPU entry must satisfy |gpu - oracle| <= 1e-8 * max(|oracle|, 1e-3 * s),
-s the largest |entry| of that output's Jacobian in the instance -- two orders
+every GPU entry must satisfy |gpu - oracle| <= 3e-8 * max(|oracle|, 1e-3 * s),
+s the largest |entry| of that output's Jacobian in the instance -- the bound the
+two oracle builds are held to (test_jacobian_oracle.py), and thirty times
 tighter than the reference's own cross-solver Jacobian check (1e-6 relative,
 test_jacobian.cpp:381-409).  The fluxes of the same call are held to the usual
 1e-9 / 1e-12 parity.
@@ -25,7 +26,7 @@ from test_jacobian_oracle import thermal_column
 
 pytestmark = pytest.mark.gpu
 
-RTOL = 1e-8
+RTOL = 3e-8
 FLOOR = 1e-3
 
 
@@ -109,3 +110,10 @@ def test_jacobian_device_pointers_equal_host_pointers_and_edge_cases():
     # the plain entry point rejects the Jacobian flag
     _, _, rc = gpu_lib.flux_solve(w, extra_flags=capi.FLAG_TEMPERATURE_JAC)
     assert rc == capi.DSP_ERR_UNSUPPORTED
+
+
+def test_jacobians_with_spherical_beam():
+    """Thermal Jacobians are unchanged in form under the pseudo-spherical beam
+    (its source does not depend on temperature)."""
+    from test_flux_gpu import spherical_columns
+    check(spherical_columns(16, 20, 6, seed=77, thermal=True), label="spherical + thermal")

@@ -82,3 +82,43 @@ def test_extended_precision_build_reproduces_goldens_and_double_build():
     a, _ = oracle_lib.flux_solve(w)
     b, _ = oracle_lib.flux_solve(w, ext=True)
     assert worst(a, b)[0] <= 10.0
+
+
+SPH = golden_cases.load_spherical_cases()
+
+
+@pytest.mark.parametrize("case", SPH, ids=[c["name"] for c in SPH])
+def test_oracle_spherical_goldens(case):
+    """The reference's pseudo-spherical known-answer test (C-DISORT values, the
+    general solver's fluxes, which the flux solver reproduces): Chapman factors,
+    beam transmission and the spherical particular solution."""
+    w = golden_cases.flux_workload(case)
+    out, status = oracle_lib.flux_solve(w)
+    assert status[0] == 0
+    for e in case["expect_flux"]:
+        got = out[e["field"]][0, golden_cases.level_of(case, e["index"])]
+        assert abs(got - e["value"]) <= e["tol"], (e, got)
+    # the plane-parallel solve of the same column differs (the Chapman correction)
+    w["flags"] &= ~capi.FLAG_SPHERICAL_BEAM
+    pp, _ = oracle_lib.flux_solve(w)
+    assert pp["flux_direct_beam"][0, 2] < 2.49e-2 < out["flux_direct_beam"][0, 2]
+
+
+def test_oracle_spherical_tends_to_plane_parallel():
+    """A very large radius makes the shells flat: the spherical fluxes approach
+    the plane-parallel ones."""
+    from disort_b200 import workloads
+    from parity import worst
+    w = workloads.subset(workloads.beam_sweep(64), np.arange(64))
+    L = w["num_layers"]
+    w["arrays"]["level_altitudes"] = np.linspace(40.0, 0.0, L + 1)
+    pp, _ = oracle_lib.flux_solve(w)
+    prev = np.inf
+    for radius in (6.371e3, 6.371e5, 6.371e7):  # km: the Earth, then flatter shells
+        w["arrays"]["bottom_radius"] = radius
+        sp, st = oracle_lib.flux_solve(w, extra_flags=capi.FLAG_SPHERICAL_BEAM)
+        assert not st.any()
+        gap = worst(sp, pp)[0]
+        assert gap < prev / 50.0  # the Chapman correction shrinks like 1 / radius
+        prev = gap
+    assert prev < 1e4  # within ~1e-5 relative at 6.4e7 km
