@@ -307,16 +307,24 @@ def test_spherical_beam_all_stream_counts(nstr):
     assert gst[0] == rst[0] == 0
     assert_parity(got, ref, f"SphericalBeam N={nstr}")
     L = 24 if nstr < 32 else 12
+    # At 32 and 64 streams the spherical particular solution (an N x N LU of
+    # I + xba M - C, xba = 1 / Chapman factor often within a few percent of a
+    # 1 / mu_i) carries rounding of ~2e-8 relative: the double build of the
+    # oracle differs from its extended-precision build by up to 2e-8 on these
+    # columns.  There the checker is the extended build, at 5e-8.
+    ext = nstr >= 32
+    rtol = 5e-8 if ext else 1e-9
+
+    def check(w, extra=0, label=""):
+        got, gst, ref, rst = both(w, extra_flags=extra, ext=ext)
+        assert np.all(gst == 0) and np.all(rst == 0)
+        for f in capi.FLUX_OUT_FIELDS:
+            np.testing.assert_allclose(got[f], ref[f], rtol=rtol, atol=1e-12, err_msg=label)
+
     w = spherical_columns(nstr, L, 12, seed=400 + nstr)
-    got, gst, ref, rst = both(w)
-    assert np.all(gst == 0) and np.all(rst == 0)
-    assert_parity(got, ref, f"spherical columns N={nstr}")
-    got, gst, ref, rst = both(w, extra_flags=capi.FLAG_INDEX_FROM_BOTTOM)
-    assert_parity(got, ref, f"spherical columns N={nstr} bottom-up")
-    w = spherical_columns(nstr, L, 6, seed=500 + nstr, thermal=True)
-    got, gst, ref, rst = both(w)
-    assert np.all(gst == 0)
-    assert_parity(got, ref, f"spherical thermal columns N={nstr}")
+    check(w, label=f"spherical columns N={nstr}")
+    check(w, capi.FLAG_INDEX_FROM_BOTTOM, label=f"spherical columns N={nstr} bottom-up")
+    check(spherical_columns(nstr, L, 6, seed=500 + nstr, thermal=True), label=f"spherical thermal N={nstr}")
 
 
 def test_spherical_beam_invalid_radius_and_missing_altitudes():

@@ -122,3 +122,17 @@ def test_oracle_spherical_tends_to_plane_parallel():
         assert gap < prev / 50.0  # the Chapman correction shrinks like 1 / radius
         prev = gap
     assert prev < 1e4  # within ~1e-5 relative at 6.4e7 km
+
+
+def test_spherical_double_and_extended_builds_agree():
+    """The rounding floor of the pseudo-spherical source at 32 and 64 streams:
+    the double build of the oracle within 3e-8 of its extended-precision build
+    (the checker of those GPU cases)."""
+    from test_flux_gpu import spherical_columns
+    for nstr in (32, 64):
+        w = spherical_columns(nstr, 12, 12, seed=400 + nstr)
+        for extra in (0, capi.FLAG_INDEX_FROM_BOTTOM):
+            a, _ = oracle_lib.flux_solve(w, extra_flags=extra)
+            b, _ = oracle_lib.flux_solve(w, extra_flags=extra, ext=True)
+            for f in capi.FLUX_OUT_FIELDS:
+                np.testing.assert_allclose(a[f], b[f], rtol=3e-8, atol=1e-12)
