@@ -323,6 +323,8 @@ def test_spherical_beam_all_stream_counts(nstr):
 
     w = spherical_columns(nstr, L, 12, seed=400 + nstr)
     check(w, label=f"spherical columns N={nstr}")
+    # bottom-up: every level array is given from the surface up, altitudes too
+    w["arrays"]["level_altitudes"] = w["arrays"]["level_altitudes"][::-1].copy()
     check(w, capi.FLAG_INDEX_FROM_BOTTOM, label=f"spherical columns N={nstr} bottom-up")
     check(spherical_columns(nstr, L, 6, seed=500 + nstr, thermal=True), label=f"spherical thermal N={nstr}")
 

@@ -132,6 +132,8 @@ def test_spherical_double_and_extended_builds_agree():
     for nstr in (32, 64):
         w = spherical_columns(nstr, 12, 12, seed=400 + nstr)
         for extra in (0, capi.FLAG_INDEX_FROM_BOTTOM):
+            if extra:
+                w["arrays"]["level_altitudes"] = w["arrays"]["level_altitudes"][::-1].copy()
             a, _ = oracle_lib.flux_solve(w, extra_flags=extra)
             b, _ = oracle_lib.flux_solve(w, extra_flags=extra, ext=True)
             for f in capi.FLUX_OUT_FIELDS:
