@@ -312,6 +312,22 @@ def alloc_general_out_numpy(d: dict) -> tuple[dict, GeneralOut, list]:
     return outs, o, [outs]
 
 
+class GeneralJacOut(ctypes.Structure):
+    _fields_ = [(f, POINTER(c_double)) for f in JAC_FIELDS] + [("ndof_out", c_int32)]
+
+
+def alloc_general_jac_numpy(d: dict) -> tuple[dict, GeneralJacOut, list]:
+    """NaN-filled Jacobian outputs [n][ntau_out][max L + 2] for a pack_general batch."""
+    n, nt = d["n_inst"], d["ntau_out"]
+    ndof = int(np.max(d["num_layers"])) + 2 if n else 2
+    jac = {f: np.full((n, nt, ndof), np.nan) for f in JAC_FIELDS}
+    o = GeneralJacOut()
+    for f in JAC_FIELDS:
+        setattr(o, f, ctypes.cast(c_void_p(_ptr(jac[f])), POINTER(c_double)))
+    o.ndof_out = ndof
+    return jac, o, [jac]
+
+
 def alloc_flux_out_numpy(n_inst: int, num_layers: int) -> tuple[dict, np.ndarray]:
     outs = {f: np.full((n_inst, num_layers + 1), np.nan) for f in FLUX_OUT_FIELDS}
     status = np.full(n_inst, -1, dtype=np.int32)
@@ -365,6 +381,9 @@ def load_library(path: str | None = None):
     lib.dsp_flux_bands_solve_jac.argtypes = [c_void_p, POINTER(FluxBatch), POINTER(FluxOut), POINTER(FluxJacOut)]
     lib.dsp_general_bands_solve.restype = c_int32
     lib.dsp_general_bands_solve.argtypes = [c_void_p, POINTER(GeneralBatch), POINTER(GeneralOut)]
+    lib.dsp_general_bands_solve_jac.restype = c_int32
+    lib.dsp_general_bands_solve_jac.argtypes = [c_void_p, POINTER(GeneralBatch), POINTER(GeneralOut),
+                                                POINTER(GeneralJacOut)]
     lib.dsp_noalloc_scratch_bytes.restype = c_int64
     lib.dsp_noalloc_scratch_bytes.argtypes = []
     lib.dsp_flux_bands_solve_noalloc.restype = c_int32
@@ -400,6 +419,9 @@ class Context:
 
     def general_bands_solve(self, batch: GeneralBatch, out: GeneralOut) -> int:
         return self.lib.dsp_general_bands_solve(self.h, ctypes.byref(batch), ctypes.byref(out))
+
+    def general_bands_solve_jac(self, batch: GeneralBatch, out: GeneralOut, jac: GeneralJacOut) -> int:
+        return self.lib.dsp_general_bands_solve_jac(self.h, ctypes.byref(batch), ctypes.byref(out), ctypes.byref(jac))
 
     def set_timing(self, enable: bool):
         self.lib.dsp_context_set_timing(self.h, 1 if enable else 0)

@@ -179,6 +179,23 @@ typedef struct dsp_general_batch {
       temperature_bottom; /* [1] each */
 } dsp_general_batch;
 
+/*
+ * Temperature Jacobians of a general solve (DisortResult's *_temperature_jac,
+ * computeThermalJacobian, src/DisortSolver.cpp:2130-2358): each array is
+ * [n_inst][ntau_out][ndof_out]; row = output optical depth (indexed like the
+ * fluxes), column = level temperature 0..L_i, then the surface temperature in
+ * column L_i + 1 (columns past it are untouched).  ndof_out >= max L_i + 2.
+ */
+typedef struct dsp_general_jac_out {
+  double* flux_up;
+  double* flux_down;
+  double* mean_intensity;
+  double* mean_intensity_down;
+  double* mean_intensity_up;
+  double* flux_divergence;
+  int32_t ndof_out;
+} dsp_general_jac_out;
+
 /* DisortResult (DisortResult.hpp:16-125) for the general batch. */
 typedef struct dsp_general_out {
   double* flux[8];                /* FluxResult order, each [n_inst][ntau_out] */
@@ -232,6 +249,14 @@ dsp_status dsp_flux_bands_solve_jac(dsp_context ctx, const dsp_flux_batch* batch
 /* General spectral-band solve (DisortSolver::solve over every instance). */
 dsp_status dsp_general_bands_solve(dsp_context ctx, const dsp_general_batch* batch,
                                    const dsp_general_out* out);
+
+/*
+ * General solve with temperature Jacobians (DisortSolver::solve with
+ * compute_temperature_jacobian, src/DisortSolver.cpp:2130-2358).  The batch flag
+ * DSP_FLAG_TEMPERATURE_JAC is implied; dsp_general_bands_solve rejects it.
+ */
+dsp_status dsp_general_bands_solve_jac(dsp_context ctx, const dsp_general_batch* batch,
+                                       const dsp_general_out* out, const dsp_general_jac_out* jac);
 
 /*
  * Flux solve without any allocation (no counterpart in the reference: DisORT++

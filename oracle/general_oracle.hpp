@@ -17,6 +17,7 @@ struct GeneralInstance {
   int L = 0, N = 0, nmom = 0, pc = 0;
   bool thermal = false, dmplus = false, dlbc = false, ifb = false;
   bool user_tau = false, user_mu = false, only_fluxes = false;
+  bool temperature_jac = false;  // compute_temperature_jacobian
   double accur = 0.0;
   double wlo = 0, whi = 0, alb = 0, emis = 1, fbeam = 0, umu0 = 0.5, phi0 = 0, fisot = 0, fisob = 0, ttop = 0, tbot = 0;
   const double *dtau = nullptr, *ssa = nullptr, *pmom = nullptr, *temp = nullptr;
@@ -29,6 +30,10 @@ struct GeneralOutput {
   double* intensity; // [ntau_out][numu_out][nphi]
   double* iavg;      // [ntau_out][numu_out]
   int ntau_out = 0, numu_out = 0;
+  // temperature Jacobians (DisortResult *_temperature_jac), each [ntau_out][jac_stride]
+  // or null: flux_up, flux_down, mean_intensity, _down, _up, flux_divergence
+  double* jac[6] = {nullptr, nullptr, nullptr, nullptr, nullptr, nullptr};
+  int jac_stride = 0;
 };
 
 // DisortConfig::validate (DisortConfig.cpp:72-249) for the fields carried here,
@@ -247,6 +252,16 @@ inline int GeneralOracle::solve(const GeneralInstance& cin, const GeneralOutput&
   std::vector<int> piv(N);
   int kconv = 0;
   int status = DSP_OK;
+  // temperature Jacobian: derivative sources of the thermal particular solution
+  // with respect to each layer's top / bottom level Planck value
+  const bool want_jac = c.temperature_jac && c.thermal && out.jac[0];
+  std::vector<double> dz0t, dz0b, dz1t, dz1b, dxr0t, dxr0b, dxr1t, dxr1b;
+  if (want_jac) {
+    for (auto* v : {&dz0t, &dz0b, &dz1t, &dz1b}) v->assign((size_t)L * N, 0.0);
+    for (auto* v : {&dxr0t, &dxr0b, &dxr1t, &dxr1b}) v->assign(L, 0.0);
+  }
+  if (out.jac[0])
+    for (double* J : out.jac) std::fill(J, J + (size_t)ntau * out.jac_stride, 0.0);
 
   for (int m = 0; m <= naz; ++m) {
     const double d0 = (m == 0) ? 1.0 : 0.0;
@@ -378,6 +393,33 @@ inline int GeneralOracle::solve(const GeneralInstance& cin, const GeneralOutput&
           z0[(size_t)lc * N + NN - iq - 1] = bvec[iq + NN];
           z1[(size_t)lc * N + NN + iq] = zz1[iq];
           z1[(size_t)lc * N + NN - iq - 1] = zz1[iq + NN];
+        }
+        if (want_jac) {
+          // d/d(pkag[lc]) and d/d(pkag[lc+1]) with the same factorisation
+          // (DisortSolver.cpp:1588-1640)
+          const double omm = 1.0 - ws[lc], tc = taus[lc];
+          double d1t = 0.0, d1b = 0.0;
+          if (dts[lc] > 1e-4) {
+            d1t = -1.0 / dts[lc];
+            d1b = 1.0 / dts[lc];
+          }
+          const double d0t = 1.0 - d1t * tc, d0b = -d1b * tc;
+          dxr0t[lc] = d0t; dxr0b[lc] = d0b; dxr1t[lc] = d1t; dxr1b[lc] = d1b;
+          for (int side = 0; side < 2; ++side) {
+            const double d1 = side ? d1b : d1t, d0 = side ? d0b : d0t;
+            for (int i = 0; i < N; ++i) zz1[i] = omm * d1;
+            lu_solve(A.data(), N, N, piv.data(), zz1.data());
+            for (int i = 0; i < N; ++i) bvec[i] = omm * d0 + mu[i] * zz1[i];
+            lu_solve(A.data(), N, N, piv.data(), bvec.data());
+            std::vector<double>& D0 = side ? dz0b : dz0t;
+            std::vector<double>& D1 = side ? dz1b : dz1t;
+            for (int iq = 0; iq < NN; ++iq) {
+              D0[(size_t)lc * N + NN + iq] = bvec[iq];
+              D0[(size_t)lc * N + NN - iq - 1] = bvec[iq + NN];
+              D1[(size_t)lc * N + NN + iq] = zz1[iq];
+              D1[(size_t)lc * N + NN - iq - 1] = zz1[iq + NN];
+            }
+          }
         }
       }
     }
@@ -616,6 +658,92 @@ inline int GeneralOracle::solve(const GeneralInstance& cin, const GeneralOutput&
         const double o[8] = {fdir, fdn, fup, dfdt, ua, uad, uau, uaso};
         for (int f = 0; f < 8; ++f) out.flux[f][lu] = o[f];
       }
+      // computeThermalJacobian (DisortSolver.cpp:2130-2358): dC = A^{-1} dB with
+      // the mode-0 band LU, for every level Planck value and the surface, at
+      // the output optical depths, chained with dB/dT
+      if (want_jac) {
+        auto pick = [&](const std::vector<double>& v, int lc, int iq) { return v[(size_t)lc * N + iq]; };
+        auto dz0 = [&](int lc, int iq, int k) {
+          return (k == lc ? pick(dz0t, lc, iq) : 0.0) + (k == lc + 1 ? pick(dz0b, lc, iq) : 0.0);
+        };
+        auto dz1 = [&](int lc, int iq, int k) {
+          return (k == lc ? pick(dz1t, lc, iq) : 0.0) + (k == lc + 1 ? pick(dz1b, lc, iq) : 0.0);
+        };
+        auto dint = [&](int lc, int k) { return (k == lc ? dxr0t[lc] : 0.0) + (k == lc + 1 ? dxr0b[lc] : 0.0); };
+        auto dslp = [&](int lc, int k) { return (k == lc ? dxr1t[lc] : 0.0) + (k == lc + 1 ? dxr1b[lc] : 0.0); };
+        const double dtau_last = dts[L - 1], tauc_bot = taus[ncut];
+        std::vector<double> jb(nc), dexp(N), dval(N);
+        auto propagate = [&](int k, int col, double chain) {
+          for (int lu = 0; lu < ntau; ++lu) {
+            const int y = lyr[lu];
+            if (lyrcut && y > ncut - 1) continue;
+            const double u = utaus[lu];
+            for (int jq = 0; jq < NN; ++jq) dexp[jq] = jb[(size_t)y * N + jq] * std::exp(-kk[(size_t)y * N + jq] * (u - taus[y + 1]));
+            for (int jq = NN; jq < N; ++jq) dexp[jq] = jb[(size_t)y * N + jq] * std::exp(-kk[(size_t)y * N + jq] * (u - taus[y]));
+            for (int i = 0; i < N; ++i) {
+              double sacc = 0.0;
+              for (int j = 0; j < N; ++j) sacc += Gv(y, i, j) * dexp[j];
+              dval[i] = sacc;
+            }
+            if (k >= 0)
+              for (int i = 0; i < N; ++i) dval[i] += dz0(y, i, k) + dz1(y, i, k) * u;
+            double dmi = 0, dmidn = 0, dmiup = 0, dfdn = 0, dfup = 0;
+            for (int iq = 0; iq < NN; ++iq) {
+              const int cw = NN - iq - 1;
+              dmi += wt[cw] * dval[iq]; dmidn += wt[cw] * dval[iq]; dfdn += wt[cw] * dval[iq] * mu[cw];
+            }
+            for (int iq = NN; iq < N; ++iq) {
+              const int cw = iq - NN;
+              dmi += wt[cw] * dval[iq]; dmiup += wt[cw] * dval[iq]; dfup += wt[cw] * dval[iq] * mu[cw];
+            }
+            dfup *= 2.0 * M_PI;
+            dfdn *= 2.0 * M_PI;
+            const double dmt = (2.0 * M_PI * dmi) / (4.0 * M_PI);
+            const double dmd = (2.0 * M_PI * dmidn) / (4.0 * M_PI);
+            const double dmu = (2.0 * M_PI * dmiup) / (4.0 * M_PI);
+            const double dpls = k >= 0 ? dint(y, k) + dslp(y, k) * u : 0.0;
+            const double dfdiv = (1.0 - c.ssa[y]) * 4.0 * M_PI * (dmt - dpls);
+            const double v[6] = {dfup, dfdn, dmt, dmd, dmu, dfdiv};
+            for (int f = 0; f < 6; ++f) out.jac[f][(size_t)lu * out.jac_stride + col] = chain * v[f];
+          }
+        };
+        for (int k = 0; k <= L + 1; ++k) {
+          const bool surf = k == L + 1;
+          std::fill(jb.begin(), jb.end(), 0.0);
+          if (!surf)
+            for (int iq = 0; iq < NN; ++iq) jb[iq] = -dz0(0, NN - 1 - iq, k);
+          for (int iq = 0; iq < NN; ++iq) {
+            double sacc = 0.0;
+            if (surf) {
+              if (c.dlbc) {
+                sacc = 1.0;
+                if (dtau_last > 0.0) sacc += mu[iq] * (1.0 / dtau_last);
+              } else {
+                sacc = 1.0 - c.alb;  // Lambertian emissivity
+              }
+            } else if (c.dlbc) {
+              sacc = -dz0(ncut - 1, NN + iq, k) - dz1(ncut - 1, NN + iq, k) * tauc_bot;
+              if (k == L - 1 && dtau_last > 0.0) sacc += mu[iq] * (-1.0 / dtau_last);
+            } else {
+              if (!lyrcut) {
+                double refl = 0.0;
+                for (int jq = 0; jq < NN; ++jq)
+                  refl += wt[jq] * mu[jq] * c.alb * (dz0(ncut - 1, NN - 1 - jq, k) + dz1(ncut - 1, NN - 1 - jq, k) * tauc_bot);
+                sacc += 2.0 * refl;
+              }
+              sacc -= dz0(ncut - 1, NN + iq, k) + dz1(ncut - 1, NN + iq, k) * tauc_bot;
+            }
+            jb[nc - NN + iq] = sacc;
+          }
+          if (!surf)
+            for (int lc = 1; lc < ncut; ++lc)
+              for (int iq = 0; iq < N; ++iq)
+                jb[lc * N - NN + iq] = dz0(lc, iq, k) - dz0(lc - 1, iq, k) + (dz1(lc, iq, k) - dz1(lc - 1, iq, k)) * taus[lc];
+          band_solve(band.data(), lda, nc, ncd, ncd, ipvt.data(), jb.data());
+          const double T = surf ? c.tbot : c.temp[k];
+          propagate(surf ? -1 : k, k, planck_function_deriv2(c.wlo, c.whi, T));
+        }
+      }
     }
 
     // computeUserIntensities (DisortSolver.cpp:2938-3268)
@@ -777,6 +905,14 @@ inline int GeneralOracle::solve(const GeneralInstance& cin, const GeneralOutput&
   }
   if (c.ifb) {  // reverseOutputArrays (IndexConversion.hpp:60-80): the level axis
     for (int f = 0; f < 8; ++f) std::reverse(out.flux[f], out.flux[f] + ntau);
+    if (out.jac[0]) {  // rows reversed; level columns reversed, the surface column kept last
+      const size_t js = out.jac_stride;
+      for (double* J : out.jac) {
+        for (int a = 0, z = ntau - 1; a < z; ++a, --z)
+          std::swap_ranges(J + a * js, J + a * js + L + 2, J + z * js);
+        for (int r = 0; r < ntau; ++r) std::reverse(J + r * js, J + r * js + L + 1);
+      }
+    }
     if (do_int) {
       const size_t row3 = (size_t)out.numu_out * nphi, row2 = out.numu_out;
       for (int a = 0, z = ntau - 1; a < z; ++a, --z) {

@@ -102,7 +102,17 @@ int oracle_flux_bands_solve_jac(const dsp_flux_batch* b, const dsp_flux_out* o, 
 // OpenMP loop as the flux batch.  Instances are ragged: instance i owns layers
 // layer_offset[i] .. layer_offset[i+1]-1 and levels layer_offset[i] + i ..
 // layer_offset[i+1] + i.
+int oracle_general_bands_solve_jac(const dsp_general_batch* b, const dsp_general_out* o,
+                                   const dsp_general_jac_out* jac, int nthreads);
+
 int oracle_general_bands_solve(const dsp_general_batch* b, const dsp_general_out* o, int nthreads) {
+  if (b && (b->flags & DSP_FLAG_TEMPERATURE_JAC)) return DSP_ERR_UNSUPPORTED;
+  return oracle_general_bands_solve_jac(b, o, nullptr, nthreads);
+}
+
+// The general batch with optional temperature Jacobians (jac may be null).
+int oracle_general_bands_solve_jac(const dsp_general_batch* b, const dsp_general_out* o,
+                                   const dsp_general_jac_out* jac, int nthreads) {
   if (!b || !o || b->n_inst < 0) return DSP_ERR_INVALID_INPUT;
   const int n = b->n_inst;
   const uint32_t fl = b->flags;
@@ -157,12 +167,21 @@ int oracle_general_bands_solve(const dsp_general_batch* b, const dsp_general_out
         c.phi = at(b->phi_user, i);
         const int ntau = c.user_tau ? c.ntau : c.L + 1;
         const int numu = (c.user_mu && !c.only_fluxes) ? c.numu : c.N;
-        if ((fl & (DSP_FLAG_SPHERICAL_BEAM | DSP_FLAG_TEMPERATURE_JAC)) != 0) st = DSP_ERR_UNSUPPORTED;
+        if ((fl & DSP_FLAG_SPHERICAL_BEAM) != 0) st = DSP_ERR_UNSUPPORTED;
         else if (c.L > 0 && b->layer_offset[i + 1] - l0 != c.L) st = DSP_ERR_INVALID_INPUT;
         else if (ntau > ntau_o || numu > numu_o || c.N > 64) st = DSP_ERR_INVALID_INPUT;
+        else if (jac && jac->ndof_out < c.L + 2) st = DSP_ERR_INVALID_INPUT;
         else {
           oracle::GeneralOutput go;
           for (int f = 0; f < 8; ++f) go.flux[f] = o->flux[f] + ntau_o * i;
+          if (jac) {
+            const int64_t js = ntau_o * jac->ndof_out;
+            double* const jp[6] = {jac->flux_up, jac->flux_down, jac->mean_intensity, jac->mean_intensity_down,
+                                   jac->mean_intensity_up, jac->flux_divergence};
+            for (int f = 0; f < 6; ++f) go.jac[f] = jp[f] + js * i;
+            go.jac_stride = jac->ndof_out;
+            c.temperature_jac = true;
+          }
           go.intensity = o->intensity ? o->intensity + (ntau_o * numu_o * nphi) * i : nullptr;
           go.iavg = o->intensity_azimuth_avg ? o->intensity_azimuth_avg + (ntau_o * numu_o) * i : nullptr;
           go.ntau_out = (int)ntau_o;

@@ -40,6 +40,9 @@ def load(native: bool = False, ext: bool = False):
     lib.oracle_flux_bands_solve_jac.restype = c_int
     lib.oracle_flux_bands_solve_jac.argtypes = [POINTER(capi.FluxBatch), POINTER(capi.FluxOut),
                                                 POINTER(capi.FluxJacOut), c_int]
+    lib.oracle_general_bands_solve_jac.restype = c_int
+    lib.oracle_general_bands_solve_jac.argtypes = [POINTER(capi.GeneralBatch), POINTER(capi.GeneralOut),
+                                                   POINTER(capi.GeneralJacOut), c_int]
     lib.oracle_general_bands_solve.restype = c_int
     lib.oracle_general_bands_solve.argtypes = [POINTER(capi.GeneralBatch), POINTER(capi.GeneralOut), c_int]
     if not native:
@@ -80,3 +83,13 @@ def general_solve(d: dict, nthreads: int = 0, ext: bool = False):
     outs, o, keep2 = capi.alloc_general_out_numpy(d)
     lib.oracle_general_bands_solve(ctypes.byref(batch), ctypes.byref(o), nthreads)
     return outs
+
+
+def general_solve_jac(d: dict, nthreads: int = 0, ext: bool = False):
+    """General solve with temperature Jacobians: (outputs, jacobians)."""
+    lib = load(ext=ext)
+    batch, keep = capi.make_general_batch(d)
+    outs, o, keep2 = capi.alloc_general_out_numpy(d)
+    jac, jo, keep3 = capi.alloc_general_jac_numpy(d)
+    lib.oracle_general_bands_solve_jac(ctypes.byref(batch), ctypes.byref(o), ctypes.byref(jo), nthreads)
+    return outs, jac

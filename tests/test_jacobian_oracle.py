@@ -133,3 +133,93 @@ def test_double_and_extended_oracle_jacobians_agree():
         for f in capi.JAC_FIELDS:
             scale = np.abs(b[f]).reshape(b[f].shape[0], -1).max(axis=1)[:, None, None]
             assert np.all(np.abs(a[f] - b[f]) <= 3e-8 * np.maximum(np.abs(b[f]), 1e-3 * scale)), f
+
+
+# ---------------------------------------------------------------------------
+# DisortSolver (general path): test_jacobian.cpp:19-115, 206-249, 284-409
+# ---------------------------------------------------------------------------
+def general_thermal(Tlev, Tsurf, nstr, ssa, beam=0.0, flags=0):
+    """buildThermalConfig (test_jacobian.cpp:19-70): outputs at the layer
+    boundaries, intensities at the quadrature angles, one azimuth, accuracy 1e-4."""
+    L = len(Tlev) - 1
+    pm = np.zeros((L, nstr + 1))
+    pm[:, 0] = 1.0
+    pm[:, 1] = 0.3 * ssa
+    inst = dict(num_streams=nstr, num_layers=L, num_phase_func_moments=0, delta_tau=np.full(L, 0.4),
+                single_scat_albedo=np.full(L, ssa), phase_function_moments=pm,
+                temperature=np.array(Tlev, dtype=np.float64), wavenumber_low=500.0, wavenumber_high=800.0,
+                surface_albedo=0.1, emissivity_top=1.0, direct_beam_flux=beam, direct_beam_mu=0.5,
+                direct_beam_phi=0.0, temperature_top=0.0, temperature_bottom=Tsurf, phi_user=[0.0])
+    return capi.pack_general([inst], capi.FLAG_THERMAL | flags, accuracy_fourier_series=1e-4)
+
+
+def general_fd_check(Tlev, Tsurf, nstr, ssa, beam, rtol, atol=1e-9):
+    L = len(Tlev) - 1
+    out, jac = oracle_lib.general_solve_jac(general_thermal(Tlev, Tsurf, nstr, ssa, beam))
+    assert out["status"][0] == 0
+    for dof in range(L + 2):
+        T0 = Tlev[dof] if dof <= L else Tsurf
+        h = 1e-3 * max(abs(T0), 1.0)
+        Tp, Tm = list(Tlev), list(Tlev)
+        Tsp = Tsm = Tsurf
+        if dof <= L:
+            Tp[dof] += h
+            Tm[dof] -= h
+        else:
+            Tsp += h
+            Tsm -= h
+        op = oracle_lib.general_solve(general_thermal(Tp, Tsp, nstr, ssa, beam))
+        om = oracle_lib.general_solve(general_thermal(Tm, Tsm, nstr, ssa, beam))
+        for jf, of in capi.JAC_OF.items():
+            fd = (op[of][0] - om[of][0]) / (2.0 * h)
+            ana = jac[jf][0, :, dof]
+            assert np.all(np.abs(ana - fd) <= rtol * np.maximum(np.abs(fd), np.abs(ana)) + atol), (jf, dof)
+
+
+@pytest.mark.parametrize("name,Tlev,Tsurf,nstr,ssa,beam,rtol", [
+    ("single_layer", [200.0, 260.0], 280.0, 8, 0.0, 0.0, 1e-3),                   # :206-210
+    ("multilayer_profile", [200.0 + 8.0 * i for i in range(11)], 285.0, 16, 0.0, 0.0, 1e-3),  # :216-222
+    ("scattering_half", [210.0, 235.0, 255.0, 270.0, 280.0], 290.0, 16, 0.5, 0.0, 1.5e-3),  # :228-232
+    ("scattering_high", [210.0, 235.0, 255.0, 270.0, 280.0], 290.0, 16, 0.9, 0.0, 2e-3),  # :234-238
+    ("thermal_plus_beam", [200.0, 240.0, 270.0], 288.0, 16, 0.6, 1.0, 1.5e-3),  # :244-248
+])
+def test_general_jacobian_vs_finite_differences(name, Tlev, Tsurf, nstr, ssa, beam, rtol):
+    general_fd_check(Tlev, Tsurf, nstr, ssa, beam, rtol)
+
+
+def test_general_and_flux_jacobians_agree():
+    """FluxSolverMatchesDisortSolver (test_jacobian.cpp:381-409): 1e-6 relative, 1e-9 absolute."""
+    Tlev = [210.0, 240.0, 265.0, 282.0]
+    _, jg = oracle_lib.general_solve_jac(general_thermal(Tlev, 290.0, 16, 0.0))
+    _, _, jf = oracle_lib.flux_solve_jac(thermal_column(Tlev, 290.0, 16, 0.0))
+    for f in ("flux_up", "flux_down", "flux_divergence"):
+        a, b = jg[f][0], jf[f][0]
+        assert np.all(np.abs(a - b) <= 1e-6 * np.maximum(np.abs(a), np.abs(b)) + 1e-9), f
+
+
+def test_general_jacobian_index_from_bottom_and_user_taus():
+    """IndexFromBottomReversal (test_jacobian.cpp:316-352) on the general solver,
+    and Jacobians at user optical depths inside layers (the rows follow the
+    user depths, scaled like the fluxes)."""
+    Tlev = [210.0, 240.0, 265.0, 285.0]
+    L = 3
+    _, j0 = oracle_lib.general_solve_jac(general_thermal(Tlev, 295.0, 16, 0.3))
+    _, j1 = oracle_lib.general_solve_jac(general_thermal(Tlev[::-1], 295.0, 16, 0.3,
+                                                         flags=capi.FLAG_INDEX_FROM_BOTTOM))
+    for f in capi.JAC_FIELDS:
+        a = j1[f][0]
+        b = j0[f][0][::-1]
+        b = np.concatenate([b[:, L::-1], b[:, L + 1:]], axis=1)
+        assert np.all(np.abs(a - b) <= 1e-9 * np.maximum(np.abs(a), np.abs(b)) + 1e-12), f
+    # user taus at the layer boundaries reproduce the level rows
+    taus = np.concatenate([[0.0], np.cumsum([0.4] * L)])
+    d2 = capi.pack_general([dict(num_streams=16, num_layers=L, num_phase_func_moments=0,
+                                 delta_tau=np.full(L, 0.4), single_scat_albedo=np.full(L, 0.3),
+                                 phase_function_moments=np.c_[np.ones(L), np.full(L, 0.09), np.zeros((L, 15))],
+                                 temperature=np.array(Tlev), wavenumber_low=500.0, wavenumber_high=800.0,
+                                 surface_albedo=0.1, temperature_bottom=295.0, phi_user=[0.0],
+                                 tau_user=taus)], capi.FLAG_THERMAL | capi.GFLAG_USER_TAU,
+                           accuracy_fourier_series=1e-4)
+    _, ju = oracle_lib.general_solve_jac(d2)
+    for f in capi.JAC_FIELDS:
+        np.testing.assert_allclose(ju[f][0], j0[f][0], rtol=1e-12, atol=1e-18)
