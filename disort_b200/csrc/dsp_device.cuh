@@ -183,9 +183,11 @@ struct FluxParams {
 // of the replayed elimination, per instance [L][N][ndof], and the six outputs
 // [batch][L+1][ndof] (already offset to the chunk's first instance).
 struct JacView {
-  int ndof;         // L + 2 degrees of freedom: level temperatures 0..L, surface
-  double* cv;       // [n][L][N][ndof]
+  int ndof;         // flux path: L + 2 degrees of freedom (level temperatures 0..L,
+                    // surface); general path: the largest L + 2 of the batch
+  double* cv;       // [n][L][N][ndof] (general path: [chunk layers][N][ndof])
   double* out[6];   // flux_up, flux_down, mean_intensity, _down, _up, flux_divergence
+  int ndof_out;     // general path: column stride of out (>= L + 2 of every instance)
 };
 
 // P_l^m(x) for l = m..lmax into y[l * stride] (rows l < m set to 0), the

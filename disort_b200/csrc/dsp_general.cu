@@ -12,6 +12,7 @@
 #include "dsp_host.hpp"
 #include "flux_bvp_tile.cuh"
 #include "flux_bvp_reg.cuh"
+#include "flux_jac.cuh"
 #include "flux_layer.cuh"
 #include "gen_kernels.cuh"
 
@@ -74,40 +75,64 @@ dsp_status get_mode_tables(dsp_context ctx, int N, const double** out) {
   return DSP_OK;
 }
 
-template <int N>
-dsp_status launch_general_chunk(dsp_context ctx, FluxParams p, long long layers, int maxm, const double* tabs) {
-  cudaStream_t s = ctx->stream;
+// The mode-m layer and boundary-value launches of a chunk; JAC: their
+// temperature-Jacobian forms (mode 0 with Jacobians asked for).
+template <int N, bool JAC>
+void launch_general_mode(dsp_context ctx, const FluxParams& p, long long lgrid, cudaStream_t s) {
   using LC = LCfg<N, true>;
   static bool attr = false;
   if (!attr) {
-    cudaFuncSetAttribute(flux_layer_kernel<N, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+    cudaFuncSetAttribute(flux_layer_kernel<N, true, JAC>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                          (int)LC::smem_bytes());
     if constexpr (N > 16)
-      cudaFuncSetAttribute(flux_bvp_tile_kernel<N, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+      cudaFuncSetAttribute(flux_bvp_tile_kernel<N, true, JAC>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                            (int)TCfg<N>::smem_bytes());
     attr = true;
   }
+  if (lgrid > 0) {
+    KernelTimer kt(ctx, "gen_layer_kernel");
+    flux_layer_kernel<N, true, JAC><<<(unsigned)lgrid, LC::CTA, LC::smem_bytes(), s>>>(p);
+  }
+  if constexpr (N <= 16) {
+    using C = RCfg<N>;
+    KernelTimer kt(ctx, "gen_bvp_kernel");
+    flux_bvp_reg_kernel<N, true, JAC><<<(p.n + C::TPC - 1) / C::TPC, C::CTA, C::smem_bytes(), s>>>(p);
+  } else {
+    using C = TCfg<N>;
+    KernelTimer kt(ctx, "gen_bvp_kernel");
+    flux_bvp_tile_kernel<N, true, JAC><<<(p.n + C::TPC - 1) / C::TPC, C::CTA, C::smem_bytes(), s>>>(p);
+  }
+}
+
+template <int N>
+dsp_status launch_general_chunk(dsp_context ctx, FluxParams p, long long layers, int maxm, const double* tabs,
+                                const JacView* jv) {
+  cudaStream_t s = ctx->stream;
+  using LC = LCfg<N, true>;
   p.tables = tabs;
   {
     KernelTimer kt(ctx, "gen_setup_kernel");
     gen_setup_kernel<<<(p.n + 3) / 4, 128, 0, s>>>(p);
   }
   const long long lgrid = (layers + LC::TPC - 1) / LC::TPC;
+  // Jacobian records only when there is a thermal source to differentiate
+  const bool jrecs = jv && (p.flags & DSP_FLAG_THERMAL);
   for (int m = 0; m <= maxm; ++m) {
     p.g.m = m;
     p.tables = tabs + (size_t)m * tab_size(N);
-    if (lgrid > 0) {
-      KernelTimer kt(ctx, "gen_layer_kernel");
-      flux_layer_kernel<N, true><<<(unsigned)lgrid, LC::CTA, LC::smem_bytes(), s>>>(p);
-    }
-    if constexpr (N <= 16) {
-      using C = RCfg<N>;
-      KernelTimer kt(ctx, "gen_bvp_kernel");
-      flux_bvp_reg_kernel<N, true><<<(p.n + C::TPC - 1) / C::TPC, C::CTA, C::smem_bytes(), s>>>(p);
-    } else {
-      using C = TCfg<N>;
-      KernelTimer kt(ctx, "gen_bvp_kernel");
-      flux_bvp_tile_kernel<N, true><<<(p.n + C::TPC - 1) / C::TPC, C::CTA, C::smem_bytes(), s>>>(p);
+    if (m == 0 && jrecs) launch_general_mode<N, true>(ctx, p, lgrid, s);
+    else launch_general_mode<N, false>(ctx, p, lgrid, s);
+    if (m == 0 && jv) {
+      // the Jacobians use the mode-0 elimination before the next mode replaces it
+      using C = JCfg<N>;
+      static bool attr = false;
+      if (!attr) {
+        cudaFuncSetAttribute(flux_jac_kernel<N, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             (int)C::smem_bytes());
+        attr = true;
+      }
+      KernelTimer kt(ctx, "gen_jac_kernel");
+      flux_jac_kernel<N, true><<<p.n, C::KB, C::smem_bytes(), s>>>(p, *jv);
     }
     if (p.g.numu > 0) {
       KernelTimer kt(ctx, "gen_intensity_kernel");
@@ -120,17 +145,17 @@ dsp_status launch_general_chunk(dsp_context ctx, FluxParams p, long long layers,
 }
 
 dsp_status launch_general(dsp_context ctx, int N, const FluxParams& p, long long layers, int maxm,
-                          const double* tabs) {
+                          const double* tabs, const JacView* jv) {
   switch (N) {
-    case 4: return launch_general_chunk<4>(ctx, p, layers, maxm, tabs);
-    case 6: return launch_general_chunk<6>(ctx, p, layers, maxm, tabs);
-    case 8: return launch_general_chunk<8>(ctx, p, layers, maxm, tabs);
-    case 10: return launch_general_chunk<10>(ctx, p, layers, maxm, tabs);
-    case 12: return launch_general_chunk<12>(ctx, p, layers, maxm, tabs);
-    case 14: return launch_general_chunk<14>(ctx, p, layers, maxm, tabs);
-    case 16: return launch_general_chunk<16>(ctx, p, layers, maxm, tabs);
-    case 32: return launch_general_chunk<32>(ctx, p, layers, maxm, tabs);
-    case 64: return launch_general_chunk<64>(ctx, p, layers, maxm, tabs);
+    case 4: return launch_general_chunk<4>(ctx, p, layers, maxm, tabs, jv);
+    case 6: return launch_general_chunk<6>(ctx, p, layers, maxm, tabs, jv);
+    case 8: return launch_general_chunk<8>(ctx, p, layers, maxm, tabs, jv);
+    case 10: return launch_general_chunk<10>(ctx, p, layers, maxm, tabs, jv);
+    case 12: return launch_general_chunk<12>(ctx, p, layers, maxm, tabs, jv);
+    case 14: return launch_general_chunk<14>(ctx, p, layers, maxm, tabs, jv);
+    case 16: return launch_general_chunk<16>(ctx, p, layers, maxm, tabs, jv);
+    case 32: return launch_general_chunk<32>(ctx, p, layers, maxm, tabs, jv);
+    case 64: return launch_general_chunk<64>(ctx, p, layers, maxm, tabs, jv);
   }
   return fail(ctx, DSP_ERR_UNSUPPORTED, "unsupported num_streams");
 }
@@ -173,19 +198,42 @@ struct DevFlux {
 
 inline size_t align256(size_t b) { return (b + 255) / 256 * 256; }
 
+dsp_status general_solve(dsp_context ctx, const dsp_general_batch* bin, const dsp_general_out* out,
+                         const dsp_general_jac_out* jac);
+
 }  // namespace
 
 extern "C" dsp_status dsp_general_bands_solve(dsp_context ctx, const dsp_general_batch* bin,
                                               const dsp_general_out* out) {
   if (!ctx) return DSP_ERR_NOT_INITIALIZED;
+  if (bin && (bin->flags & DSP_FLAG_TEMPERATURE_JAC))
+    return fail(ctx, DSP_ERR_UNSUPPORTED, "temperature Jacobians are computed by dsp_general_bands_solve_jac");
+  return general_solve(ctx, bin, out, nullptr);
+}
+
+extern "C" dsp_status dsp_general_bands_solve_jac(dsp_context ctx, const dsp_general_batch* bin,
+                                                  const dsp_general_out* out, const dsp_general_jac_out* jac) {
+  if (!ctx) return DSP_ERR_NOT_INITIALIZED;
+  if (!jac || !jac->flux_up || !jac->flux_down || !jac->mean_intensity || !jac->mean_intensity_down ||
+      !jac->mean_intensity_up || !jac->flux_divergence)
+    return fail(ctx, DSP_ERR_INVALID_INPUT, "every Jacobian output array is required");
+  return general_solve(ctx, bin, out, jac);
+}
+
+namespace {
+
+// The general solve behind both entry points; `jac` (may be null) adds the
+// temperature Jacobians of mode 0.
+dsp_status general_solve(dsp_context ctx, const dsp_general_batch* bin, const dsp_general_out* out,
+                         const dsp_general_jac_out* jac) {
   if (!bin || !out) return fail(ctx, DSP_ERR_INVALID_INPUT, "null batch or output");
   const dsp_general_batch& b = *bin;
   const int n = b.n_inst;
   if (n < 0) return fail(ctx, DSP_ERR_INVALID_INPUT, "n_inst must be >= 0");
   if (n == 0) return DSP_OK;
   const uint32_t fl = b.flags;
-  if (fl & (DSP_FLAG_SPHERICAL_BEAM | DSP_FLAG_TEMPERATURE_JAC))
-    return fail(ctx, DSP_ERR_UNSUPPORTED, "spherical beam and temperature Jacobians are not in this engine");
+  if (fl & DSP_FLAG_SPHERICAL_BEAM)
+    return fail(ctx, DSP_ERR_UNSUPPORTED, "the general solver takes no pseudo-spherical beam in this engine");
   if (fl & DSP_FLAG_HG_G)
     return fail(ctx, DSP_ERR_UNSUPPORTED, "the Henyey-Greenstein g fast path is a flux-batch option");
   const bool thermal = (fl & DSP_FLAG_THERMAL) != 0;
@@ -247,6 +295,11 @@ extern "C" dsp_status dsp_general_bands_solve(dsp_context ctx, const dsp_general
   const int64_t total_layers = hoff[n];
   const int nphi = only_fluxes ? (b.num_phi > 0 ? b.num_phi : 0) : b.num_phi;
   const int64_t ntau_o = out->ntau_out, numu_o = out->numu_out;
+  // Jacobian columns: the largest L + 2 (the replay's column stride), the output stride
+  const int jdof = maxL + 2;
+  if (jac && jac->ndof_out < jdof)
+    return fail(ctx, DSP_ERR_INVALID_INPUT, "ndof_out is smaller than num_layers + 2");
+  const int64_t jdof_o = jac ? jac->ndof_out : 0;
 
   // ---- stage inputs --------------------------------------------------------
   static const double kDefaults[11] = {0.0, 0.0, 0.0, 1.0, 0.0, 0.5, 0.0, 0.0, 0.0, 0.0, 0.0};
@@ -330,8 +383,14 @@ extern "C" dsp_status dsp_general_bands_solve(dsp_context ctx, const dsp_general
   double* dint = nullptr;
   double* diavg = nullptr;
   int32_t* dstatus = nullptr;
+  const size_t jac_elems = jac ? (size_t)n * ntau_o * jdof_o : 0;
+  double* djac[6] = {};
+  double* const hjac[6] = {jac ? jac->flux_up : nullptr, jac ? jac->flux_down : nullptr,
+                           jac ? jac->mean_intensity : nullptr, jac ? jac->mean_intensity_down : nullptr,
+                           jac ? jac->mean_intensity_up : nullptr, jac ? jac->flux_divergence : nullptr};
   {
-    const size_t need = (dev ? 0 : 8 * align256(flux_elems * 8) + align256(int_elems * 8) + align256(iavg_elems * 8)) +
+    const size_t need = (dev ? 0 : 8 * align256(flux_elems * 8) + align256(int_elems * 8) + align256(iavg_elems * 8) +
+                                       6 * align256(jac_elems * 8)) +
                         2 * align256(n * sizeof(int32_t)) + align256(8 * sizeof(double*));
     if ((st = ensure(ctx, &ctx->stage_out, &ctx->stage_out_bytes, need, "output staging")) != DSP_OK) return st;
     char* cur = static_cast<char*>(ctx->stage_out);
@@ -351,6 +410,13 @@ extern "C" dsp_status dsp_general_bands_solve(dsp_context ctx, const dsp_general
       if (iavg_elems) diavg = reinterpret_cast<double*>(cur);
       cur += align256(iavg_elems * 8);
     }
+    for (int f = 0; f < 6 && jac; ++f) {
+      if (dev) djac[f] = hjac[f];
+      else {
+        djac[f] = reinterpret_cast<double*>(cur);
+        cur += align256(jac_elems * 8);
+      }
+    }
     dstatus = (dev && out->status) ? out->status : reinterpret_cast<int32_t*>(cur);
     cur += align256(n * sizeof(int32_t));
     double** dfp = reinterpret_cast<double**>(cur);
@@ -360,6 +426,7 @@ extern "C" dsp_status dsp_general_bands_solve(dsp_context ctx, const dsp_general
     for (int f = 0; f < 8 && e == cudaSuccess; ++f) e = cudaMemsetAsync(dflux[f], 0, flux_elems * 8, s);
     if (e == cudaSuccess && dint) e = cudaMemsetAsync(dint, 0, int_elems * 8, s);
     if (e == cudaSuccess && diavg) e = cudaMemsetAsync(diavg, 0, iavg_elems * 8, s);
+    for (int f = 0; f < 6 && jac && e == cudaSuccess; ++f) e = cudaMemsetAsync(djac[f], 0, jac_elems * 8, s);
     if (e != cudaSuccess) return cuda_fail(ctx, e, "output initialisation");
 
     // status: 0, or the verdict on instances no kernel takes
@@ -404,9 +471,15 @@ extern "C" dsp_status dsp_general_bands_solve(dsp_context ctx, const dsp_general
   const double* h_fbeam = (!dev && b.direct_beam_flux.ptr) ? b.direct_beam_flux.ptr : nullptr;
   const double* h_umu0 = (!dev && b.direct_beam_mu.ptr) ? b.direct_beam_mu.ptr : nullptr;
   const double* h_mu = (!dev && user_mu) ? b.mu_user.ptr : nullptr;
+  // with Jacobians of a thermal solve, per layer: P/Q, multiplier records and
+  // the replayed right-hand side values [N][jdof]
+  const bool jrecs = jac && thermal;
+  auto jac_per_layer = [&](int N) -> int64_t {
+    return jrecs ? (int64_t)jpq_stride(N) + jrec_stride(N) + (int64_t)N * jdof : 0;
+  };
   for (int N : kSupported) {
     const int64_t lstride = glrec_stride(N, numu_eff);
-    const int64_t per_layer = lstride + brec_stride(N) + N;
+    const int64_t per_layer = lstride + brec_stride(N) + N + jac_per_layer(N);
     Chunk c;
     c.N = N;
     size_t bytes = 0;
@@ -450,7 +523,8 @@ extern "C" dsp_status dsp_general_bands_solve(dsp_context ctx, const dsp_general
       meta_need += align256(c.ids.size() * 4) + align256(c.ids.size() * 8) + align256((c.ids.size() + 1) * 8) +
                    align256(c.layers * 4);
       const int64_t lstride = glrec_stride(c.N, numu_eff);
-      const size_t w = (size_t)(c.inst_doubles + c.layers * (lstride + brec_stride(c.N) + c.N)) * sizeof(double);
+      const size_t w =
+          (size_t)(c.inst_doubles + c.layers * (lstride + brec_stride(c.N) + c.N + jac_per_layer(c.N))) * sizeof(double);
       if (w > ws_need) ws_need = w;
     }
     if ((st = ensure(ctx, &ctx->meta, &ctx->meta_bytes, meta_need, "chunk index")) != DSP_OK) return st;
@@ -530,9 +604,20 @@ extern "C" dsp_status dsp_general_bands_solve(dsp_context ctx, const dsp_general
       p.layer_rec = w + c.inst_doubles;
       p.bvp_rec = p.layer_rec + c.layers * g.lstride;
       g.cc = p.bvp_rec + c.layers * brec_stride(c.N);
+      JacView jv;
+      if (jac) {
+        // after the solution coefficients: P/Q, multipliers, replayed values
+        double* jb = g.cc + c.layers * c.N;
+        p.jac_pq = jrecs ? jb : nullptr;
+        p.jac_rec = jrecs ? jb + c.layers * jpq_stride(c.N) : nullptr;
+        jv.cv = jrecs ? p.jac_rec + c.layers * jrec_stride(c.N) : nullptr;
+        jv.ndof = jdof;
+        jv.ndof_out = (int)jdof_o;
+        for (int f = 0; f < 6; ++f) jv.out[f] = djac[f];
+      }
       const double* tabs = nullptr;
       if ((st = get_mode_tables(ctx, c.N, &tabs)) != DSP_OK) return st;
-      if ((st = launch_general(ctx, c.N, p, c.layers, c.maxm, tabs)) != DSP_OK) return st;
+      if ((st = launch_general(ctx, c.N, p, c.layers, c.maxm, tabs, jac ? &jv : nullptr)) != DSP_OK) return st;
     }
   }
 
@@ -550,6 +635,10 @@ copy_back:
     e = cudaMemcpyAsync(out->intensity_azimuth_avg, diavg, iavg_elems * 8, cudaMemcpyDeviceToHost, s);
     if (e != cudaSuccess) return cuda_fail(ctx, e, "cudaMemcpyAsync(intensity_azimuth_avg)");
   }
+  for (int f = 0; f < 6 && jac; ++f) {
+    e = cudaMemcpyAsync(hjac[f], djac[f], jac_elems * 8, cudaMemcpyDeviceToHost, s);
+    if (e != cudaSuccess) return cuda_fail(ctx, e, "cudaMemcpyAsync(jacobian)");
+  }
   std::vector<int32_t> hs_tmp;
   int32_t* hs = out->status;
   if (!hs) {
@@ -562,3 +651,5 @@ copy_back:
   if (e != cudaSuccess) return cuda_fail(ctx, e, "general solve");
   return DSP_OK;
 }
+
+}  // namespace

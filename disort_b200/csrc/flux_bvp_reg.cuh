@@ -323,7 +323,8 @@ __global__ void __launch_bounds__(RCfg<N>::CTA, RCfg<N>::MINB) flux_bvp_reg_kern
     // ---- eliminate the N columns of x_l (sgbfa steps) ----------------------
     int myc = -1;  // pivot column of this thread's row, if it becomes a pivot row
     // temperature Jacobian: this layer's multipliers and pivot slots
-    double* const jrow = JAC ? p.jac_rec + ((long long)i * L + l) * jrec_stride(N) : nullptr;
+    double* const jrow = !JAC ? nullptr
+        : p.jac_rec + ((GEN ? (long long)p.g.lay_off[slot] : (long long)i * L) + l) * jrec_stride(N);
 #pragma unroll
     for (int c = 0; c < N; ++c) {
       const bool isc = t < PR && ((cand >> t) & 1u);

@@ -357,7 +357,8 @@ __global__ void __launch_bounds__(TCfg<N>::CTA, TCfg<N>::MINB) flux_bvp_tile_ker
     // ---- eliminate the N columns of x_l (sgbfa steps) ----------------------
     const int cgo0 = cbk * (N / CPT);  // first column group of the current block
     // temperature Jacobian: this layer's multipliers and pivot slots
-    double* const jrow = JAC ? p.jac_rec + ((long long)i * L + l) * jrec_stride(N) : nullptr;
+    double* const jrow = !JAC ? nullptr
+        : p.jac_rec + ((GEN ? (long long)p.g.lay_off[slot] : (long long)i * L) + l) * jrec_stride(N);
 #pragma unroll 1
     for (int cb8 = 0; cb8 < N / CPT; ++cb8) {
       const int cgo = cgo0 + cb8;  // column group owning the next CPT pivot columns

@@ -71,7 +71,9 @@ struct JCfg {
   static constexpr int NW = (PR + 31) / 32;
 };
 
-template <int N>
+// GEN: the general path (mode 0 of a ragged chunk): outputs at the instance's
+// output depths (user optical depths or the levels), rows of ndof_out columns.
+template <int N, bool GEN = false>
 __global__ void __launch_bounds__(64) flux_jac_kernel(FluxParams p, JacView jv) {
   using C = JCfg<N>;
   constexpr int NN = C::NN, PR = C::PR, KB = C::KB, NW = C::NW;
@@ -84,40 +86,70 @@ __global__ void __launch_bounds__(64) flux_jac_kernel(FluxParams p, JacView jv) 
   const int tid = threadIdx.x;
   for (int k = tid; k < 2 * N; k += KB) smem[C::O_TAB + k] = p.tables[k];  // tab_mu, tab_wt
   __syncthreads();
-  const int i = blockIdx.x;  // chunk-local instance
-  if (i >= p.n) return;
-  const int L = p.L, ndof = jv.ndof;
-  const long long nlev = L + 1;
+  const int slot = blockIdx.x;  // chunk-local instance
+  if (slot >= p.n) return;
+  // i: batch index; L: layers; NT: output depths; cvs: column stride of cv
+  int i, L, NT;
+  const double *rec, *lrec0, *brec0, *jrec0, *pq0;
+  double* cv0;
+  InstLayout il_gen;
+  long long lstride;
+  const int cvs = jv.ndof;
+  if constexpr (GEN) {
+    i = p.g.ids[slot];
+    L = p.g.Ls[i];
+    NT = p.g.user_tau ? p.g.user_tau : L + 1;
+    il_gen = InstLayout::make(L, N);
+    rec = p.inst_rec + p.g.inst_off[slot];
+    const long long l0 = p.g.lay_off[slot];
+    lstride = p.g.lstride;
+    lrec0 = p.layer_rec + l0 * lstride;
+    brec0 = p.bvp_rec + l0 * brec_stride(N);
+    jrec0 = p.jac_rec + l0 * jrec_stride(N);
+    pq0 = p.jac_pq + l0 * jpq_stride(N);
+    cv0 = jv.cv + l0 * N * cvs;
+  } else {
+    i = slot;
+    L = p.L;
+    NT = L + 1;
+    rec = p.inst_rec + (long long)i * p.il.stride;
+    lstride = lrec_stride(N);
+    lrec0 = p.layer_rec + (long long)i * L * lstride;
+    brec0 = p.bvp_rec + (long long)i * L * brec_stride(N);
+    jrec0 = p.jac_rec + (long long)i * L * jrec_stride(N);
+    pq0 = p.jac_pq + (long long)i * L * jpq_stride(N);
+    cv0 = jv.cv + (long long)i * L * N * cvs;
+  }
+  const InstLayout& il = GEN ? il_gen : p.il;
+  const int ndof = L + 2;
   const bool ifb = (p.flags & DSP_FLAG_INDEX_FROM_BOTTOM) != 0;
   auto store = [&](int f, int lu, int k, double v) {
-    const int row = ifb ? L - lu : lu;
+    const int row = ifb ? NT - 1 - lu : lu;
     const int col = (ifb && k <= L) ? L - k : k;
-    jv.out[f][((long long)i * nlev + row) * ndof + col] = v;
+    if constexpr (GEN) jv.out[f][((long long)i * p.g.ntau_out + row) * jv.ndof_out + col] = v;
+    else jv.out[f][((long long)i * NT + row) * ndof + col] = v;
   };
   const int st = p.status ? p.status[i] : 0;
   const bool thermal = (p.flags & DSP_FLAG_THERMAL) != 0;
   if (st == DSP_ERR_INVALID_INPUT || st == DSP_ERR_EIGEN || !thermal) {
     // invalid instances: NaN like their fluxes; no thermal emission: zero
     const double v = thermal ? __longlong_as_double(0x7ff8000000000000ll) : 0.0;
-    for (long long e = tid; e < nlev * ndof; e += KB) {
+    for (long long e = tid; e < (long long)NT * ndof; e += KB) {
       const int lu = (int)(e / ndof), k = (int)(e % ndof);
       for (int f = 0; f < 6; ++f) store(f, lu, k, v);
     }
     return;
   }
-  const double* rec = p.inst_rec + (long long)i * p.il.stride;
-  const InstLayout& il = p.il;
   const double* taus = rec + il.tau_s;
   const double* dtau_s = rec + il.dtau_s;
-  const double* lrec0 = p.layer_rec + (long long)i * L * lrec_stride(N);
-  const double* brec0 = p.bvp_rec + (long long)i * L * brec_stride(N);
-  const double* jrec0 = p.jac_rec + (long long)i * L * jrec_stride(N);
-  const double* pq0 = p.jac_pq + (long long)i * L * jpq_stride(N);
-  double* cv0 = jv.cv + (long long)i * L * N * ndof;
+  // output depth lu: its layer and scaled depth (general path: the user depths)
+  const GenLayout gl_ = GenLayout::make(L, N, NT);
+  auto out_layer = [&](int lu) { return GEN ? (int)rec[gl_.lyr + lu] : (lu == 0 ? 0 : lu - 1); };
+  auto out_taus = [&](int lu) { return GEN ? rec[gl_.utaus + lu] : taus[lu]; };
   const bool dlbc = (p.flags & DSP_FLAG_DIFFUSION_LOWER_BC) != 0;
   const double alb = rec[H_ALB];
   const double wlo = p.wlo(i), whi = p.whi(i);
-  const double* temp_in = p.temp.row(i);
+  const double* temp_in = GEN ? p.g.temp + p.g.in_off[i] + i : p.temp.row(i);
   const double dtau_last = dtau_s[L - 1];
   // row width and 1/pivot position of the elimination record (flux_bvp_reg /
   // flux_bvp_tile layouts)
@@ -236,12 +268,12 @@ __global__ void __launch_bounds__(64) flux_jac_kernel(FluxParams p, JacView jv) 
 #pragma unroll
       for (int w = 0; w < NW; ++w) cand[w] = carried[w];
       const double* jr = jrec0 + (long long)l * jrec_stride(N);
-      double* cvl = cv0 + (long long)l * N * ndof;
+      double* cvl = cv0 + (long long)l * N * cvs;
       for (int c = 0; c < N; ++c) {
         int ps = (int)jr[N * PR + c];
         ps = ps < 0 ? 0 : (ps >= PR ? PR - 1 : ps);  // a record slot always, whatever was stored
         const double rp = R[ps * KB];
-        if (act) cvl[c * ndof + k] = rp;
+        if (act) cvl[c * cvs + k] = rp;
         cand[ps >> 5] &= ~(1u << (ps & 31));
         const double* m = jr + c * PR;
         for (int s = 0; s < PR; ++s) R[s * KB] += m[s] * rp;
@@ -264,26 +296,29 @@ __global__ void __launch_bounds__(64) flux_jac_kernel(FluxParams p, JacView jv) 
       double* x = X + b * N * KB;
       const double* xn = X + (b ^ 1) * N * KB;
       const double* br = brec0 + (long long)l * brec_stride(N);
-      const double* cvl = cv0 + (long long)l * N * ndof;
+      const double* cvl = cv0 + (long long)l * N * cvs;
       for (int c = N - 1; c >= 0; --c) {
-        double s = act ? cvl[c * ndof + k] : 0.0;
+        double s = act ? cvl[c * cvs + k] : 0.0;
         const double* row = br + c * RL;
         for (int j = c + 1; j < N; ++j) s -= row[j] * x[j * KB];
         if (l < L - 1)
           for (int j = 0; j < N; ++j) s -= row[N + j] * xn[j * KB];
         x[c * KB] = s * rdiag(br, c);
       }
-      // outputs at the levels of layer l: its bottom, and the top for l = 0
-      const double* lr = lrec0 + (long long)l * lrec_stride(N);
+      // outputs at the depths of layer l (flux path: its bottom level, and the
+      // top for l = 0)
+      const double* lr = lrec0 + (long long)l * lstride;
       const double* eig = lr + lrec_eig(N);
       const double* G = lr + lrec_G(N);
       double a0, a1;
       coef(l, a0, a1);
       const int lin = ifb ? L - 1 - l : l;
-      const double w0 = p.ssa(i, lin);
-      for (int pass = 0; pass < (l == 0 ? 2 : 1); ++pass) {
-        const int lu = pass == 0 ? l + 1 : 0;
-        const double utaupr = taus[lu];
+      const double w0 = GEN ? p.g.ssa[p.g.in_off[i] + lin] : p.ssa(i, lin);
+      const int npass = GEN ? NT : (l == 0 ? 2 : 1);
+      for (int pass = 0; pass < npass; ++pass) {
+        const int lu = GEN ? pass : (pass == 0 ? l + 1 : 0);
+        if (GEN && out_layer(lu) != l) continue;  // uniform over the CTA
+        const double utaupr = out_taus(lu);
         __syncthreads();
         for (int j = tid; j < N; j += KB) {
           const double d = (j < NN) ? (utaupr - taus[l + 1]) : (utaupr - taus[l]);

@@ -117,3 +117,67 @@ def test_jacobians_with_spherical_beam():
     (its source does not depend on temperature)."""
     from test_flux_gpu import spherical_columns
     check(spherical_columns(16, 20, 6, seed=77, thermal=True), label="spherical + thermal")
+
+
+# ---------------------------------------------------------------------------
+# general path (dsp_general_bands_solve_jac, DisortSolver)
+# ---------------------------------------------------------------------------
+def general_check(insts, flags, label, accuracy=0.0):
+    d = capi.pack_general(insts, flags, accuracy_fourier_series=accuracy)
+    batch, keep = capi.make_general_batch(d)
+    outs, o, keep2 = capi.alloc_general_out_numpy(d)
+    jac, jo, keep3 = capi.alloc_general_jac_numpy(d)
+    rc = gpu_lib.context().general_bands_solve_jac(batch, o, jo)
+    assert rc == 0, gpu_lib.context().last_error()
+    rout, rjac = oracle_lib.general_solve_jac(d)
+    assert np.all(outs["status"] == rout["status"])
+    from parity import assert_parity_general
+    ok = outs["status"] == 0
+    assert_parity_general({k: v[ok] for k, v in outs.items() if k != "status"},
+                          {k: v[ok] for k, v in rout.items() if k != "status"}, label)
+    # compare each instance's own columns (L_i + 2) and rows
+    for i in np.nonzero(ok)[0]:
+        L = insts[i]["num_layers"]
+        nt = d["num_user_tau"] if flags & capi.GFLAG_USER_TAU else L + 1
+        got = {f: jac[f][i:i + 1, :nt, :L + 2] for f in capi.JAC_FIELDS}
+        ref = {f: rjac[f][i:i + 1, :nt, :L + 2] for f in capi.JAC_FIELDS}
+        r, where = jac_ratio(got, ref)
+        assert r <= 1.0, f"{label} instance {i}: Jacobian parity ratio {r:.3g} at {where}"
+    return outs, jac
+
+
+def general_thermal_mix(n, seed, nstr=(4, 8, 16, 32), user_tau=True):
+    rng = np.random.default_rng(seed)
+    insts = []
+    for k in range(n):
+        N = nstr[k % len(nstr)]
+        L = int(rng.integers(3, 25 if N < 32 else 12))
+        g = rng.uniform(0.0, 0.9, L)
+        dtau = np.clip(rng.lognormal(-2.0, 1.5, L), 1e-6, 20.0)
+        inst = dict(num_streams=N, num_layers=L, num_phase_func_moments=0, delta_tau=dtau,
+                    single_scat_albedo=rng.uniform(0.0, 0.95, L), phase_function_moments=workloads.hg_moments(g, N + 1),
+                    temperature=200.0 + 100.0 * rng.random(L + 1), wavenumber_low=float(rng.uniform(300, 1500)),
+                    surface_albedo=float(rng.uniform(0, 0.5)), temperature_bottom=300.0, temperature_top=50.0,
+                    emissivity_top=0.9, direct_beam_flux=float(rng.uniform(0, 1)), direct_beam_mu=0.6,
+                    mu_user=[-0.7, -0.2, 0.3, 0.9], phi_user=[0.0, 45.0])
+        inst["wavenumber_high"] = inst["wavenumber_low"] * 1.02
+        if user_tau:
+            tot = float(dtau.sum())
+            inst["tau_user"] = [0.0, 0.37 * tot, tot]
+        insts.append(inst)
+    return insts
+
+
+@pytest.mark.parametrize("extra", [0, capi.FLAG_INDEX_FROM_BOTTOM, capi.FLAG_DIFFUSION_LOWER_BC])
+def test_general_jacobians_ragged_batch(extra):
+    """A ragged batch of thermal (and beam) instances at 4-32 streams, outputs
+    at user optical depths inside layers, intensities on (all azimuth modes
+    run; the Jacobians come from mode 0)."""
+    insts = general_thermal_mix(12, seed=90 + extra)
+    general_check(insts, capi.FLAG_THERMAL | capi.GFLAG_USER_TAU | capi.GFLAG_USER_MU | extra,
+                  f"general Jacobians flags={extra}")
+
+
+def test_general_jacobians_at_levels_and_64_streams():
+    insts = general_thermal_mix(4, seed=95, nstr=(64, 8), user_tau=False)
+    general_check(insts, capi.FLAG_THERMAL | capi.GFLAG_ONLY_FLUXES, "general Jacobians at the levels")
