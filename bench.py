@@ -52,6 +52,9 @@ def parse():
     ap.add_argument("--no-e2e", action="store_true", help="profiling: skip the host-buffer pass")
     ap.add_argument("--no-surrogate", action="store_true",
                     help="skip the gated-emulator leg (solver-labelled training + gated inference)")
+    ap.add_argument("--no-general", action="store_true",
+                    help="skip the general-solver leg (65,536-instance mixed batch)")
+    ap.add_argument("--general-instances", type=int, default=65536)
     return ap.parse_args()
 
 
@@ -409,6 +412,8 @@ def run_ours(args):
         }
         if not args.no_surrogate and world == 1:
             line["surrogate"] = surrogate_leg(ctx)
+        if not args.no_general and world == 1:
+            line["general"] = general_leg(ctx, stream, dev, args)
         print(json.dumps(line), flush=True)
     ctx.close()
     replicas.finish()
@@ -427,6 +432,19 @@ def surrogate_leg(ctx) -> dict:
         return {"metric": "gated surrogate solves/s vs plain FP64 GPU solves/s, same instances",
                 "workload": "4096 columns x 256 bands, 40 layers, 16 streams, thermal + solar", "training": rep,
                 "inference": ev}
+    except Exception as e:  # the plain-solver line stands on its own
+        return {"error": f"{type(e).__name__}: {e}"}
+
+
+def general_leg(ctx, stream, dev, args) -> dict:
+    """The general solver (DisortSolver) on the 65,536-instance mixed batch
+    (N 4-64, L 10-120, all azimuth modes, intensities): one warm-up and one
+    timed solve with inputs in HBM, the oracle on an evenly spaced sample (CPU
+    baseline and parity, the parity also against the extended-precision
+    oracle build, the checker of the 64-stream instances)."""
+    try:
+        return measure_general(ctx, stream, dev, args.general_instances, 3, 1, 1, e2e=False,
+                               cpu_seconds=None if args.no_cpu else args.cpu_seconds, ext_parity=True)
     except Exception as e:  # the plain-solver line stands on its own
         return {"error": f"{type(e).__name__}: {e}"}
 
@@ -450,9 +468,11 @@ def general_batch(n: int, seed: int):
     return insts, d, fl
 
 
-def general_oracle_lib():
-    subprocess.run(["make", "-s", "-C", os.path.join(REPO, "oracle"), "native"], check=True)
-    lib = ctypes.CDLL(os.path.join(REPO, "oracle", "_native", "liboracle_disort.so"))
+def general_oracle_lib(ext: bool = False):
+    """The oracle built for this host (-march=native), or its extended-precision build."""
+    subprocess.run(["make", "-s", "-C", os.path.join(REPO, "oracle"), "ext" if ext else "native"], check=True)
+    lib = ctypes.CDLL(os.path.join(REPO, "oracle", "liboracle_disort_ext.so") if ext else
+                      os.path.join(REPO, "oracle", "_native", "liboracle_disort.so"))
     lib.oracle_general_bands_solve.restype = ctypes.c_int
     lib.oracle_general_bands_solve.argtypes = [ctypes.POINTER(capi.GeneralBatch), ctypes.POINTER(capi.GeneralOut),
                                                ctypes.c_int]
@@ -531,8 +551,26 @@ def run_general(args):
     replicas.init("nccl", 300.0)
     dev = torch.device("cuda", local)
     stream = torch.cuda.current_stream()
-    insts, d, fl = general_batch(n, replicas.replica_seed(3, rank))
     ctx = capi.Context(local, stream.cuda_stream)
+    line = measure_general(ctx, stream, dev, n, replicas.replica_seed(3, rank), args.steps, args.warmup,
+                           world, rank, e2e=not args.no_e2e, cpu_seconds=None if args.no_cpu else args.cpu_seconds)
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    ctx.close()
+    replicas.finish()
+
+
+def measure_general(ctx, stream, dev, n, seed, steps, warmup, world=1, rank=0, e2e=True, cpu_seconds=10.0,
+                    ext_parity=False):
+    """The general solver on n instances of the mixed batch: device-resident
+    solves/s over `steps` timed solves (CUDA events), optionally the host-buffer
+    e2e rate, the oracle on an evenly spaced CPU sample (baseline and parity)
+    and the roofline of the dominant kernel.  Returns the bench line."""
+    import torch
+    from types import SimpleNamespace
+    args = SimpleNamespace(steps=steps, warmup=warmup, no_e2e=not e2e, no_cpu=cpu_seconds is None,
+                           cpu_seconds=cpu_seconds)
+    insts, d, fl = general_batch(n, seed)
     dd = dict(d)
     for k in ("num_streams", "num_layers", "layer_offset", "num_phase_func_moments", "delta_tau",
               "single_scat_albedo", "phase_function_moments", "temperature") + capi.GENERAL_SCALAR_FIELDS:
@@ -627,16 +665,21 @@ def run_general(args):
                 "avg_launch_ms": dom_ms / max(1, dom_launches), "traffic": None,
                 "kernel_ms_per_step": {k: v[0] / args.steps for k, v in ktimes.items()},
                 "all_kernels_tflops": fl["total"] * args.steps / (ms_max / 1000.0) / 1e12}
+    cpu, parity = None, None
     if rank == 0:
-        cpu, parity = None, None
         if not args.no_cpu:
             lib, sample, flags, threads, idx = general_cpu_sample(insts, args.cpu_seconds)
             tcpu, ref = general_cpu_time(lib, sample, flags, threads, keep_outputs=True)
             cpu = {"value": len(sample) / tcpu, "unit": "solves/s", "cores": threads, "kind": "port",
                    "sample": f"{len(sample)} of {n} instances evenly spaced, oracle -march=native, "
                              f"{threads} OpenMP threads, {tcpu:.1f} s"}
-            parity = general_parity({k: v.cpu().numpy() for k, v in douts.items()}, idx, ref)
-        print(json.dumps({
+            got = {k: v.cpu().numpy() for k, v in douts.items()}
+            parity = general_parity(got, idx, ref)
+            parity["checker"] = "oracle (double)"
+            if ext_parity:
+                _, ref_ext = general_cpu_time(general_oracle_lib(ext=True), sample, flags, threads, keep_outputs=True)
+                parity["vs_extended_precision_oracle"] = general_parity(got, idx, ref_ext)
+    return {
             "metric": GENERAL_METRIC, "value": value, "unit": "solves/s", "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": ms_max / args.steps, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded PCG64)",
@@ -644,9 +687,9 @@ def run_general(args):
                        "parallelism": f"replicas x{world}" if world > 1 else "single GPU",
                        "l2": "workspace larger than L2; no flush needed"},
             "e2e": e2e, "gpu_launches": int(sum(v[1] for v in ktimes.values())), "roofline": roofline,
-            "cpu_baseline": cpu, "parity": parity, "clocks": clk, "bad_status_instances": bad}), flush=True)
-    ctx.close()
-    replicas.finish()
+            "cpu_baseline": cpu, "parity": parity, "clocks": clk, "bad_status_instances": bad}
+
+
 
 
 # ---------------------------------------------------------------------------

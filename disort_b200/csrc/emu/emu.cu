@@ -3,6 +3,8 @@
 // Training step (batch B, layers i = 1..nl, H_0 = X):
 //   forward   Z_i = H_{i-1} W_i^T + b_i,  H_i = GELU(Z_i)  (last layer: P = Z_nl)
 //   loss      sum over heads h of w_mh * mean_k (P_mhk - Y_mk)^2, averaged over m
+//             (the gradient); the reported epoch loss is the same sum with the
+//             82 outputs summed rather than averaged
 //   backward  dZ_nl from the loss (fused into the output GEMM's epilogue),
 //             dW_i = dZ_i^T H_{i-1},  dZ_{i-1} = (dZ_i W_i) * GELU'(Z_{i-1}),
 //             db_i = column sums of dZ_i

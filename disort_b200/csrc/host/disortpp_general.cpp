@@ -197,8 +197,6 @@ void check_engine(const DisortConfig& c) {
   if (f.intensity_corr_buras || f.intensity_corr_nakajima)
     throw std::invalid_argument("intensity corrections are not supported by the B200 engine");
   if (f.use_spherical_beam) throw std::invalid_argument("use_spherical_beam is not supported by the B200 engine");
-  if (f.compute_temperature_jacobian)
-    throw std::invalid_argument("compute_temperature_jacobian is not supported by the B200 engine");
   if (f.output_fourier_expansion)
     throw std::invalid_argument("output_fourier_expansion is not supported by the B200 engine");
   // validate() does not look at the user optical depths; the reference reads
@@ -459,6 +457,19 @@ std::vector<DisortResult> run_general(const DisortConfig& c, const std::vector<s
     iavg.resize(n * static_cast<size_t>(ntau) * numu);
   }
   std::vector<int32_t> status(n, 0);
+  // temperature Jacobians (DisortSolver.cpp:2130-2358): [n][ntau][L+2] per output
+  const bool jac = f.compute_temperature_jacobian;
+  const int ndof = c.num_layers + 2;
+  std::vector<double> jbuf;
+  dsp_general_jac_out jo{};
+  if (jac) {
+    const size_t per = n * static_cast<size_t>(ntau) * ndof;
+    jbuf.resize(6 * per);
+    double** jp[6] = {&jo.flux_up, &jo.flux_down, &jo.mean_intensity, &jo.mean_intensity_down,
+                      &jo.mean_intensity_up, &jo.flux_divergence};
+    for (int k = 0; k < 6; ++k) *jp[k] = jbuf.data() + k * per;
+    jo.ndof_out = ndof;
+  }
   dsp_general_out o{};
   for (int k = 0; k < 8; ++k) o.flux[k] = flux.data() + static_cast<size_t>(k) * n * ntau;
   o.intensity = do_int ? inten.data() : nullptr;
@@ -469,7 +480,7 @@ std::vector<DisortResult> run_general(const DisortConfig& c, const std::vector<s
   {
     std::lock_guard<std::mutex> lk(detail::engine_mutex());
     dsp_context ctx = detail::engine_context_locked();
-    const dsp_status st = dsp_general_bands_solve(ctx, &b, &o);
+    const dsp_status st = jac ? dsp_general_bands_solve_jac(ctx, &b, &o, &jo) : dsp_general_bands_solve(ctx, &b, &o);
     if (st != DSP_OK)
       throw std::runtime_error(std::string("disortpp: GPU solve failed: ") + dsp_status_string(st) + ": " +
                                dsp_context_last_error(ctx));
@@ -495,6 +506,20 @@ std::vector<DisortResult> run_general(const DisortConfig& c, const std::vector<s
           std::copy(inten.begin() + row * nphi, inten.begin() + (row + 1) * nphi, r.intensity[lu][iu].begin());
           r.intensity_azimuth_avg[lu][iu] = iavg[row];
         }
+    }
+    // Jacobians when asked for with thermal emission on; otherwise empty, as the
+    // reference clears them (DisortSolver.cpp:2143-2151)
+    std::vector<std::vector<double>>* jd[6] = {&r.flux_up_temperature_jac, &r.flux_down_temperature_jac,
+                                               &r.mean_intensity_temperature_jac,
+                                               &r.mean_intensity_down_temperature_jac,
+                                               &r.mean_intensity_up_temperature_jac,
+                                               &r.flux_divergence_temperature_jac};
+    for (int k = 0; k < 6; ++k) {
+      jd[k]->clear();
+      if (!jac || !f.use_thermal_emission) continue;
+      const double* src = jbuf.data() + static_cast<size_t>(k) * n * ntau * ndof + i * static_cast<size_t>(ntau) * ndof;
+      jd[k]->resize(ntau);
+      for (int lu = 0; lu < ntau; ++lu) (*jd[k])[lu].assign(src + lu * ndof, src + (lu + 1) * ndof);
     }
   }
   return res;

@@ -6,28 +6,38 @@ Instances are 40-layer, 16-stream thermal + solar columns.  Per (column, band):
   level T    linear from T_top U[180, 220] to T_surf U[280, 320] plus U(-10, 10)
   albedo U[0, 0.6], beam F0 = 1 at mu0 U[0.1, 1], emissivity_top 1, T_top 0 K,
   T_bottom = T_surf level, and one of 256 contiguous bands over 100-2,900 cm^-1.
-Features (165 + 82): log delta_tau, ssa, g (40 each), the 41 level
-temperatures, albedo, mu0, and the band edges nu_lo, nu_hi (the band is needed
-because the thermal source depends on it); then physics features computed from
-the same inputs: log cumulative optical depth at levels 1..40, the level Planck
-fluxes pi B(T) / S and the thermal share of S, where S = pi B(T_surface) + mu0 F0
-is the instance's flux scale (B: band Planck radiance, midpoint rule).
-Targets (82): flux_up and the diffuse downward flux at the 41 levels divided by
-S, as log(x + 1e-3) standardised per output (the offset sits at the error
-metric's floor, so fluxes far below it do not dominate the loss).  The
-standardised features enter the network as hi/lo BF16 pairs (x_hi = bf16(x),
-x_lo = bf16(x - x_hi)), 494 inputs carrying about 16 mantissa bits: a single
-BF16 feature (8 bits) alone perturbs optical depths by ~1 %.  The direct beam
-mu0 F0 exp(-tau/mu0) is exact and added back, so the emulated total downward
-flux is direct + S * diffuse.
+
+The emulator corrects a cheap physical solve instead of predicting fluxes from
+scratch: every instance is first solved in FP64 on the GPU with 4 streams
+(about ten times faster than 16), and the network predicts the difference
+between the 16-stream and the 4-stream fluxes.  A network trained to predict
+the fluxes themselves from the same inputs (same architecture, same data)
+reaches a held-out MSE of 0.007 per standardised output -- and the plain
+PyTorch FP32 training of that network reaches the same -- but that leaves
+~25 % median per-instance maximum error: the map from 40 layers of optical
+properties to 82 fluxes is too sharp for the network to reach the 0.5 % bar.
+The 4-stream solve carries the physics; the network learns its smooth bias.
+
+Features (165 + 82 + 82): log delta_tau, ssa, g (40 each), the 41 level
+temperatures, albedo, mu0, and the band edges nu_lo, nu_hi; physics features
+computed from the same inputs: log cumulative optical depth at levels 1..40,
+the level Planck fluxes pi B(T) / S and the thermal share of S, where
+S = pi B(T_surface) + mu0 F0 is the instance's flux scale (B: band Planck
+radiance, midpoint rule); and the 4-stream solution t4 = log(x4 + 1e-3) for the
+82 fluxes x4 (flux_up and the diffuse downward flux at the 41 levels, over S).
+Targets (82): t16 - t4, t16 the same transform of the 16-stream solution,
+standardised per output.  The standardised features enter the network as
+hi/lo BF16 pairs (x_hi = bf16(x), x_lo = bf16(x - x_hi)), 658 inputs carrying
+about 16 mantissa bits.  The direct beam mu0 F0 exp(-tau/mu0) is exact and
+added back, so the emulated total downward flux is direct + S * diffuse.
 
 Relative flux error: |F - F_ref| / max(|F_ref|, 1e-3 max_k |F_ref,k|) over the
 82 fluxes of an instance (flux_up and direct + diffuse down); the floor keeps
 near-zero fluxes of an instance from dominating its error.
 
-The gate sends an instance to the FP64 solver when a raw feature lies outside
-the training envelope or the two heads disagree by more than 0.2 % in the same
-floored relative measure.
+The gate sends an instance to the 16-stream FP64 solver when a raw feature
+lies outside the training envelope or the two heads disagree by more than
+0.2 % in the same floored relative measure.
 """
 from __future__ import annotations
 
@@ -39,10 +49,11 @@ import numpy as np
 from . import capi
 
 L, N = 40, 16
+N_LOW = 4  # streams of the cheap physical solve the network corrects
 NLEV = L + 1
-N_RAW = 3 * L + NLEV + 4  # 165 input features
-N_IN = N_RAW + L + NLEV + 1  # + physics features = 247
 N_OUT = 2 * NLEV  # 82
+N_RAW = 3 * L + NLEV + 4  # 165 input features
+N_IN = N_RAW + L + NLEV + 1 + N_OUT  # + physics features + the 4-stream solution = 329
 NBANDS = 256
 BAND_W = 2800.0 / NBANDS
 FLOOR_FRAC = 1e-3
@@ -126,28 +137,39 @@ def physics(arrays: dict):
     return S.reshape(n), fdir, feats
 
 
-def features_device(arrays: dict):
-    """The 247 raw features from the device flux-batch arrays (float32 [n][247])."""
+def log_diffuse(F, S, fdir):
+    """t = log(diffuse / S + 1e-3) of fluxes [n][82] (the direct beam removed)."""
+    import torch
+    diffuse = F.clone()
+    diffuse[:, NLEV:] -= fdir
+    return torch.log((diffuse / S.reshape(-1, 1)).clamp_min(0.0) + EPS)
+
+
+def features_device(arrays: dict, t4):
+    """The 329 features from the device flux-batch arrays and the 4-stream
+    solution t4 [n][82] (float32 [n][329])."""
     import torch
     n = arrays["delta_tau"].shape[0]
     pm = arrays["phase_function_moments"]
     cols = [torch.log(arrays["delta_tau"]), arrays["single_scat_albedo"], pm[:, :, 1], arrays["temperature"],
             arrays["surface_albedo"].reshape(n, 1), arrays["direct_beam_mu"].reshape(n, 1),
-            arrays["wavenumber_low"].reshape(n, 1), arrays["wavenumber_high"].reshape(n, 1), physics(arrays)[2]]
+            arrays["wavenumber_low"].reshape(n, 1), arrays["wavenumber_high"].reshape(n, 1), physics(arrays)[2],
+            t4]
     return torch.cat(cols, dim=1).float().contiguous()
 
 
-def reconstruct(y, mu, sd, S, fdir):
-    """Fluxes [n][82] from standardised predictions of one head."""
+def reconstruct(y, mu, sd, S, fdir, t4):
+    """Fluxes [n][82] from the standardised correction predicted by one head."""
     import torch
-    x = torch.exp(y.double() * sd.double() + mu.double()) - EPS
+    x = torch.exp(t4.double() + y.double() * sd.double() + mu.double()) - EPS
     F = S.double().reshape(-1, 1) * x
     F[:, NLEV:] += fdir
     return F
 
 
-def solve_fp64(ctx: capi.Context, arrays: dict, n: int, chunk: int = 262144):
-    """FP64 GPU solves of n instances: fluxes [n][82] (flux_up, direct + diffuse down)."""
+def solve_fp64(ctx: capi.Context, arrays: dict, n: int, chunk: int = 262144, nstr: int = N):
+    """FP64 GPU solves of n instances with `nstr` streams: fluxes [n][82]
+    (flux_up, direct + diffuse down)."""
     import torch
     dev = arrays["delta_tau"].device
     out = torch.empty((n, N_OUT), dtype=torch.float64, device=dev)
@@ -157,7 +179,9 @@ def solve_fp64(ctx: capi.Context, arrays: dict, n: int, chunk: int = 262144):
         part = {}
         for k, v in arrays.items():
             part[k] = v[r0:r0 + m] if hasattr(v, "shape") and v.dim() >= 1 and v.shape[0] == n else v
-        batch, keep = capi.make_flux_batch(m, N, L, 0, N + 1, capi.FLAG_THERMAL | capi.FLAG_DEVICE_POINTERS, part)
+        # the moment array holds N + 1 = 17 moments; a 4-stream solve reads the first 5
+        batch, keep = capi.make_flux_batch(m, nstr, L, 0, N + 1, capi.FLAG_THERMAL | capi.FLAG_DEVICE_POINTERS,
+                                           part)
         outs = {f: torch.empty((m, NLEV), dtype=torch.float64, device=dev) for f in capi.FLUX_OUT_FIELDS}
         st = torch.empty((m,), dtype=torch.int32, device=dev)
         o, keep2 = capi.make_flux_out(outs, st)
@@ -204,15 +228,15 @@ def train(ctx: capi.Context, n_columns: int = 1 << 20, epochs: int = 50, batch: 
     d = sample(n_columns, seed)
     arrays = device_inputs(d)
     F, st = solve_fp64(ctx, arrays, n_columns)
+    F4, st4 = solve_fp64(ctx, arrays, n_columns, nstr=N_LOW)
     torch.cuda.synchronize()
     t_label = time.perf_counter() - t0
-    bad = int((st != 0).sum())
-    raw = features_device(arrays)
+    bad = int((st != 0).sum()) + int((st4 != 0).sum())
     S, fdir, _ = physics(arrays)
+    t4 = log_diffuse(F4, S, fdir)
+    raw = features_device(arrays, t4)
     ntr = int(n_columns * (1.0 - holdout)) // batch * batch
-    diffuse = F.clone()
-    diffuse[:, NLEV:] -= fdir
-    t = torch.log((diffuse / S.reshape(-1, 1)).clamp_min(0.0) + EPS)
+    t = log_diffuse(F, S, fdir) - t4
     mu = t[:ntr].mean(dim=0)
     sd = t[:ntr].std(dim=0).clamp_min(1e-6)
     y = ((t - mu) / sd).float()
@@ -233,32 +257,53 @@ def train(ctx: capi.Context, n_columns: int = 1 << 20, epochs: int = 50, batch: 
     losses = emu.train(epochs, lr=1e-3, lr_min=1e-5, seed=seed + 2)
     torch.cuda.synchronize()
     t_train = time.perf_counter() - t1
-    # held-out error of the raw emulator (head mean)
+    # held-out error of the corrected solve (head mean) and of the 4-stream solve alone
     Xh = X[ntr:].contiguous()
     preds = torch.empty((Xh.shape[0], 2 * N_OUT), dtype=torch.float32, device="cuda")
     emu.forward(Xh, preds)
-    Sh, fh = S[ntr:], fdir[ntr:]
-    Fe = 0.5 * (reconstruct(preds[:, :N_OUT], mu, sd, Sh, fh) + reconstruct(preds[:, N_OUT:], mu, sd, Sh, fh))
+    Sh, fh, t4h = S[ntr:], fdir[ntr:], t4[ntr:]
+    Fe = 0.5 * (reconstruct(preds[:, :N_OUT], mu, sd, Sh, fh, t4h) + reconstruct(preds[:, N_OUT:], mu, sd, Sh, fh, t4h))
     emax = rel_err(Fe, F[ntr:]).amax(dim=1)
+    e4 = rel_err(F4[ntr:], F[ntr:]).amax(dim=1)
+    per_out = 1.0 / (2 * N_OUT)  # the training loss sums the squared errors of 82 outputs over 2 heads
     report = dict(columns=n_columns, train_columns=ntr, holdout_columns=n_columns - ntr, epochs=epochs, batch=batch,
                   label_seconds=t_label, train_seconds=t_train, bad_label_status=bad, first_loss=losses[0],
-                  last_loss=losses[-1], holdout_max_rel_err=float(emax.max()),
+                  last_loss=losses[-1], last_loss_per_output=losses[-1] * per_out,
+                  holdout_max_rel_err=float(emax.max()),
                   holdout_p99_rel_err=float(torch.quantile(emax.float(), 0.99)),
-                  holdout_median_rel_err=float(emax.median()))
+                  holdout_median_rel_err=float(emax.median()),
+                  four_stream_alone=dict(max_rel_err=float(e4.max()),
+                                         p99_rel_err=float(torch.quantile(e4.float(), 0.99)),
+                                         median_rel_err=float(e4.median())))
     log(f"emulator: labels {t_label:.1f} s, training {t_train:.1f} s, loss {losses[0]:.4g} -> {losses[-1]:.4g}, "
         f"held-out max/p99/median rel err {report['holdout_max_rel_err']:.3g}/{report['holdout_p99_rel_err']:.3g}/"
-        f"{report['holdout_median_rel_err']:.3g}")
+        f"{report['holdout_median_rel_err']:.3g} (4-stream alone: median {report['four_stream_alone']['median_rel_err']:.3g})")
     return sur, report
 
 
-def gated_run(ctx: capi.Context, sur: Surrogate, arrays: dict, raw, n: int, tol: float = GATE_TOL):
-    """Emulate every instance, re-solve the gated ones in FP64, merge.  Returns the
-    fluxes [n][82], the fallback count and the fallback flags [n] (int32)."""
+def emulate(ctx: capi.Context, sur: Surrogate, arrays: dict, n: int):
+    """The 4-stream solve, the features and both heads' predictions, shifted so
+    that pred * sd + mu is the corrected log flux (t4 folded in).  Returns
+    (raw features, predictions [n][164], S, direct beam, t4)."""
     import torch
+    S, fdir, _ = physics(arrays)
+    F4, _ = solve_fp64(ctx, arrays, n, nstr=N_LOW)
+    t4 = log_diffuse(F4, S, fdir)
+    raw = features_device(arrays, t4)
     X = sur.encode(raw)
     preds = torch.empty((n, 2 * N_OUT), dtype=torch.float32, device="cuda")
     sur.emu.forward(X, preds)
-    S, fdir, _ = physics(arrays)
+    shift = (t4 / sur.sd).float()
+    preds[:, :N_OUT] += shift
+    preds[:, N_OUT:] += shift
+    return raw, preds, S, fdir, t4
+
+
+def gated_run(ctx: capi.Context, sur: Surrogate, arrays: dict, n: int, tol: float = GATE_TOL):
+    """Emulate every instance, re-solve the gated ones in FP64, merge.  Returns the
+    fluxes [n][82], the fallback count and the fallback flags [n] (int32)."""
+    import torch
+    raw, preds, S, fdir, _ = emulate(ctx, sur, arrays, n)
     add = torch.zeros((n, N_OUT), dtype=torch.float32, device="cuda")
     add[:, NLEV:] = fdir
     flux = torch.empty((n, N_OUT), dtype=torch.float32, device="cuda")
@@ -298,13 +343,13 @@ def evaluate(ctx: capi.Context, sur: Surrogate, columns: int = 4096, seed: int =
     b.record()
     torch.cuda.synchronize()
     t_plain = a.elapsed_time(b) / 1000.0 / repeats
-    # gated: features -> emulator -> gate -> FP64 solve of the fallback instances
-    F_g, k, _ = gated_run(ctx, sur, arrays, features_device(arrays), n)
+    # gated: 4-stream solve -> features -> emulator -> gate -> 16-stream FP64 solve of the fallback instances
+    F_g, k, _ = gated_run(ctx, sur, arrays, n)
     torch.cuda.synchronize()
     a, b = ev()
     a.record()
     for _ in range(repeats):
-        F_g, k, _ = gated_run(ctx, sur, arrays, features_device(arrays), n)
+        F_g, k, _ = gated_run(ctx, sur, arrays, n)
     b.record()
     torch.cuda.synchronize()
     t_gated = a.elapsed_time(b) / 1000.0 / repeats
@@ -320,7 +365,7 @@ def evaluate(ctx: capi.Context, sur: Surrogate, columns: int = 4096, seed: int =
     for tol in tols:
         a, b = ev()
         a.record()
-        F_t, k_t, _ = gated_run(ctx, sur, arrays, features_device(arrays), n, tol)
+        F_t, k_t, _ = gated_run(ctx, sur, arrays, n, tol)
         b.record()
         torch.cuda.synchronize()
         tt = a.elapsed_time(b) / 1000.0
@@ -328,13 +373,25 @@ def evaluate(ctx: capi.Context, sur: Surrogate, columns: int = 4096, seed: int =
         sweep.append(dict(gate_tol=tol, fallback_fraction=k_t / n, speedup=t_plain / tt,
                           max_rel_err=float(et.max()), p99_rel_err=float(torch.quantile(et.float(), 0.99))))
     res["gate_sweep"] = sweep
-    # the raw emulator alone (no gate) on the in-envelope instances
-    X = sur.encode(features_device(arrays))
-    preds = torch.empty((n, 2 * N_OUT), dtype=torch.float32, device="cuda")
-    sur.emu.forward(X, preds)
-    S, fdir, _ = physics(arrays)
-    Fe = 0.5 * (reconstruct(preds[:, :N_OUT], sur.mu, sur.sd, S, fdir) + reconstruct(preds[:, N_OUT:], sur.mu, sur.sd, S, fdir))
+    # the corrected solve alone (no gate) on the in-envelope instances, beside the
+    # 4-stream solve it corrects: what the network gains
+    raw, preds, S, fdir, t4 = emulate(ctx, sur, arrays, n)
+    zero = torch.zeros_like(t4)
+    Fe = 0.5 * (reconstruct(preds[:, :N_OUT], sur.mu, sur.sd, S, fdir, zero) +
+                reconstruct(preds[:, N_OUT:], sur.mu, sur.sd, S, fdir, zero))
     ee = rel_err(Fe, F_ref).amax(dim=1)[~ooe_mask]
+    F4, _ = solve_fp64(ctx, arrays, n, nstr=N_LOW)
+    e4 = rel_err(F4, F_ref).amax(dim=1)[~ooe_mask]
     res["emulator_only_in_envelope"] = dict(max_rel_err=float(ee.max()), p99_rel_err=float(torch.quantile(ee.float(), 0.99)),
                                             median_rel_err=float(ee.median()))
+    res["four_stream_alone_in_envelope"] = dict(max_rel_err=float(e4.max()),
+                                                p99_rel_err=float(torch.quantile(e4.float(), 0.99)),
+                                                median_rel_err=float(e4.median()))
+    # the 4-stream solve's own rate on these instances (the floor of the gated path's cost)
+    a, b = ev()
+    a.record()
+    solve_fp64(ctx, arrays, n, nstr=N_LOW)
+    b.record()
+    torch.cuda.synchronize()
+    res["four_stream_solves_per_s"] = n / (a.elapsed_time(b) / 1000.0)
     return res

@@ -49,7 +49,9 @@ dsp_status dsp_emu_set_data(dsp_emu emu, const uint16_t* feats, const float* tar
 
 /* Adam (beta 0.9 / 0.999, eps 1e-8), cosine learning-rate decay from lr to
  * lr_min over all steps of all epochs; one pass over shuffled batches per epoch.
- * epoch_loss (host, [epochs] or NULL) receives the mean training loss. */
+ * epoch_loss (host, [epochs] or NULL) receives the epoch's training loss per row: the
+ * squared errors of the n_out outputs summed (not averaged), weighted and summed over
+ * the heads, averaged over the rows. */
 dsp_status dsp_emu_train(dsp_emu emu, int32_t epochs, float lr, float lr_min, uint64_t shuffle_seed,
                          float* epoch_loss);
 

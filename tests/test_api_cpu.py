@@ -154,7 +154,6 @@ def test_general_engine_rejections_before_any_gpu_work():
         (lambda c: setattr(c.flags, "use_lambertian_surface", False), "BRDF surfaces"),
         (lambda c: setattr(c.flags, "intensity_corr_nakajima", True), "intensity corrections"),
         (lambda c: setattr(c.flags, "output_fourier_expansion", True), "output_fourier_expansion"),
-        (lambda c: setattr(c.flags, "compute_temperature_jacobian", True), "compute_temperature_jacobian"),
     ]
     for mutate, msg in cases:
         c = _general_cfg()

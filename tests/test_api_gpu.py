@@ -247,3 +247,39 @@ def test_flux_solver_temperature_jacobians():
     c.use_thermal_emission = False
     r = disortpp.DisortFluxSolver16().solve(c)
     assert len(r.flux_up_temperature_jac) == 0
+
+
+def test_general_solver_temperature_jacobians():
+    """DisortSolver with compute_temperature_jacobian (the reference's
+    buildThermalConfig, test_jacobian.cpp:19-70): DisortResult's Jacobians
+    ([ntau][L+2]) equal the oracle's, and agree with the flux solver's
+    (FluxSolverMatchesDisortSolver, 1e-6 relative)."""
+    from test_jacobian_oracle import general_thermal
+    Tlev = [210.0, 240.0, 265.0, 282.0]
+    c = disortpp.DisortConfig(3, 16)
+    c.flags.use_thermal_emission = True
+    c.flags.use_user_tau = False
+    c.flags.use_user_mu = False
+    c.flags.comp_only_fluxes = False
+    c.flags.compute_temperature_jacobian = True
+    c.bc.direct_beam_flux = 0.0
+    c.bc.surface_albedo = 0.1
+    c.bc.temperature_bottom = 290.0
+    c.bc.temperature_top = 0.0
+    c.bc.emissivity_top = 1.0
+    c.wavenumber_low, c.wavenumber_high = 500.0, 800.0
+    c.accuracy_fourier_series = 1e-4
+    c.num_phi = 1
+    c.allocate()
+    c.phi_user = [0.0]
+    c.delta_tau = [0.4] * 3
+    c.single_scat_albedo = [0.3] * 3
+    c.phase_function_moments = [[1.0, 0.09] + [0.0] * 15 for _ in range(3)]
+    c.temperature = Tlev
+    r = disortpp.DisortSolver().solve(c)
+    _, jac = oracle_lib.general_solve_jac(general_thermal(Tlev, 290.0, 16, 0.3))
+    got = np.array(r.flux_up_temperature_jac)
+    assert got.shape == (4, 5)
+    ref = jac["flux_up"][0][:4, :5]
+    scale = np.abs(ref).max()
+    assert np.all(np.abs(got - ref) <= 3e-8 * np.maximum(np.abs(ref), 1e-3 * scale))
