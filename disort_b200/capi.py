@@ -201,7 +201,7 @@ class GeneralBatch(ctypes.Structure):
         ("delta_tau", c_void_p), ("single_scat_albedo", c_void_p), ("phase_function_moments", c_void_p),
         ("temperature", c_void_p),
         ("tau_user", DArray), ("mu_user", DArray), ("phi_user", DArray),
-    ] + [(f, DArray) for f in GENERAL_SCALAR_FIELDS]
+    ] + [(f, DArray) for f in GENERAL_SCALAR_FIELDS] + [("level_altitudes", c_void_p), ("bottom_radius", DArray)]
 
 
 class GeneralOut(ctypes.Structure):
@@ -254,6 +254,14 @@ def pack_general(insts: list, flags: int, accuracy_fourier_series: float = 0.0,
     d = dict(n_inst=n, flags=flags, num_streams=N, num_layers=L, layer_offset=off,
              num_phase_func_moments=nmom, pmom_count=pmom_count, accuracy=float(accuracy_fourier_series),
              delta_tau=dtau, single_scat_albedo=ssa, phase_function_moments=pm, temperature=temp)
+    if flags & FLAG_SPHERICAL_BEAM:  # level altitudes [L+1] per instance (like temperature), radius per instance
+        zalt = np.zeros(tot + n)
+        for i, c in enumerate(insts):
+            za = c.get("level_altitudes")
+            if za is not None:
+                zalt[off[i] + i:off[i + 1] + i + 1] = za
+        d["level_altitudes"] = zalt
+        d["bottom_radius"] = np.array([float(c.get("bottom_radius", 0.0)) for c in insts])
     for f in GENERAL_SCALAR_FIELDS:
         d[f] = np.array([float(c.get(f, GENERAL_SCALAR_DEFAULTS[f])) for c in insts])
     ntau = numu = nphi = 0
@@ -292,6 +300,10 @@ def make_general_batch(d: dict) -> tuple[GeneralBatch, list]:
     for f in GENERAL_SCALAR_FIELDS:
         a = d[f]
         setattr(b, f, DArray(_ptr(a), 1 if a.shape[0] > 1 else 0))
+    if "level_altitudes" in d:
+        b.level_altitudes = _ptr(d["level_altitudes"])
+        a = d["bottom_radius"]
+        b.bottom_radius = DArray(_ptr(a), 1 if a.shape[0] > 1 else 0)
     return b, keep
 
 

@@ -40,7 +40,7 @@ dsp_status launch_flux_chunk(dsp_context ctx, const FluxParams& p, cudaStream_t 
   }
   if constexpr (SPH) {
     KernelTimer kt(ctx, "flux_sph_chapman_kernel", s);
-    flux_sph_chapman_kernel<<<(p.n + 3) / 4, 128, 0, s>>>(p);
+    flux_sph_chapman_kernel<false><<<(p.n + 3) / 4, 128, 0, s>>>(p);
   }
   {
     static bool attr = false;

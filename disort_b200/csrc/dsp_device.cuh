@@ -152,6 +152,7 @@ struct GenView {
   const long long* in_off;     // batch layer_offset (CSR)
   const int* nmoms;            // batch num_phase_func_moments
   const double *dtau, *ssa, *pmom, *temp;  // CSR inputs
+  const double* zalt;          // level altitudes, laid out like temp (pseudo-spherical beam only)
   DArr utau, umu, phi, phi0;
   long long lstride;           // layer record stride (glrec_stride)
   double* cc;                  // [layers][N] boundary-value solution of the mode
@@ -174,7 +175,7 @@ struct FluxParams {
   double* out[8];
   int32_t* status;
   GenView g;  // general-solver launches only
-  double* sph = nullptr;      // [n][L][sph_stride] (pseudo-spherical beam launches only)
+  double* sph = nullptr;      // [n][L][sph_stride], general: [layers][sph_stride] (pseudo-spherical beam only)
   double* jac_pq = nullptr;   // [n][L][jpq_stride] (temperature-Jacobian launches only)
   double* jac_rec = nullptr;  // [n][L][jrec_stride] (temperature-Jacobian launches only)
 };

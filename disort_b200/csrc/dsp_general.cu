@@ -14,6 +14,7 @@
 #include "flux_bvp_reg.cuh"
 #include "flux_jac.cuh"
 #include "flux_layer.cuh"
+#include "flux_sph.cuh"
 #include "gen_kernels.cuh"
 
 using namespace dsp;
@@ -76,52 +77,67 @@ dsp_status get_mode_tables(dsp_context ctx, int N, const double** out) {
 }
 
 // The mode-m layer and boundary-value launches of a chunk; JAC: their
-// temperature-Jacobian forms (mode 0 with Jacobians asked for).
-template <int N, bool JAC>
-void launch_general_mode(dsp_context ctx, const FluxParams& p, long long lgrid, cudaStream_t s) {
+// temperature-Jacobian forms (mode 0 with Jacobians asked for); SPH: with the
+// pseudo-spherical beam, whose particular solution of the mode is formed
+// between the two.
+template <int N, bool JAC, bool SPH>
+void launch_general_mode(dsp_context ctx, const FluxParams& p, long long layers, cudaStream_t s) {
   using LC = LCfg<N, true>;
   static bool attr = false;
   if (!attr) {
     cudaFuncSetAttribute(flux_layer_kernel<N, true, JAC>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                          (int)LC::smem_bytes());
     if constexpr (N > 16)
-      cudaFuncSetAttribute(flux_bvp_tile_kernel<N, true, JAC>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+      cudaFuncSetAttribute(flux_bvp_tile_kernel<N, true, JAC, SPH>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                            (int)TCfg<N>::smem_bytes());
+    if constexpr (SPH)
+      cudaFuncSetAttribute(flux_sph_source_kernel<N, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                           (int)SCfg<N>::smem_bytes());
     attr = true;
   }
-  if (lgrid > 0) {
+  if (layers > 0) {
     KernelTimer kt(ctx, "gen_layer_kernel");
-    flux_layer_kernel<N, true, JAC><<<(unsigned)lgrid, LC::CTA, LC::smem_bytes(), s>>>(p);
+    flux_layer_kernel<N, true, JAC><<<(unsigned)((layers + LC::TPC - 1) / LC::TPC), LC::CTA, LC::smem_bytes(), s>>>(p);
+  }
+  if constexpr (SPH) {
+    if (layers > 0) {
+      using C = SCfg<N>;
+      KernelTimer kt(ctx, "gen_sph_source_kernel");
+      flux_sph_source_kernel<N, true><<<(unsigned)((layers + C::WPC - 1) / C::WPC), 32 * C::WPC, C::smem_bytes(), s>>>(p);
+    }
   }
   if constexpr (N <= 16) {
     using C = RCfg<N>;
     KernelTimer kt(ctx, "gen_bvp_kernel");
-    flux_bvp_reg_kernel<N, true, JAC><<<(p.n + C::TPC - 1) / C::TPC, C::CTA, C::smem_bytes(), s>>>(p);
+    flux_bvp_reg_kernel<N, true, JAC, SPH><<<(p.n + C::TPC - 1) / C::TPC, C::CTA, C::smem_bytes(), s>>>(p);
   } else {
     using C = TCfg<N>;
     KernelTimer kt(ctx, "gen_bvp_kernel");
-    flux_bvp_tile_kernel<N, true, JAC><<<(p.n + C::TPC - 1) / C::TPC, C::CTA, C::smem_bytes(), s>>>(p);
+    flux_bvp_tile_kernel<N, true, JAC, SPH><<<(p.n + C::TPC - 1) / C::TPC, C::CTA, C::smem_bytes(), s>>>(p);
   }
 }
 
-template <int N>
+template <int N, bool SPH>
 dsp_status launch_general_chunk(dsp_context ctx, FluxParams p, long long layers, int maxm, const double* tabs,
                                 const JacView* jv) {
   cudaStream_t s = ctx->stream;
-  using LC = LCfg<N, true>;
   p.tables = tabs;
   {
     KernelTimer kt(ctx, "gen_setup_kernel");
     gen_setup_kernel<<<(p.n + 3) / 4, 128, 0, s>>>(p);
   }
-  const long long lgrid = (layers + LC::TPC - 1) / LC::TPC;
+  if constexpr (SPH) {
+    // Chapman factors and the beam transmission through the spherical shells
+    KernelTimer kt(ctx, "gen_sph_chapman_kernel");
+    flux_sph_chapman_kernel<true><<<(p.n + 3) / 4, 128, 0, s>>>(p);
+  }
   // Jacobian records only when there is a thermal source to differentiate
   const bool jrecs = jv && (p.flags & DSP_FLAG_THERMAL);
   for (int m = 0; m <= maxm; ++m) {
     p.g.m = m;
     p.tables = tabs + (size_t)m * tab_size(N);
-    if (m == 0 && jrecs) launch_general_mode<N, true>(ctx, p, lgrid, s);
-    else launch_general_mode<N, false>(ctx, p, lgrid, s);
+    if (m == 0 && jrecs) launch_general_mode<N, true, SPH>(ctx, p, layers, s);
+    else launch_general_mode<N, false, SPH>(ctx, p, layers, s);
     if (m == 0 && jv) {
       // the Jacobians use the mode-0 elimination before the next mode replaces it
       using C = JCfg<N>;
@@ -144,18 +160,25 @@ dsp_status launch_general_chunk(dsp_context ctx, FluxParams p, long long layers,
   return DSP_OK;
 }
 
+template <int N>
+dsp_status launch_general_n(dsp_context ctx, const FluxParams& p, long long layers, int maxm, const double* tabs,
+                            const JacView* jv) {
+  if (p.flags & DSP_FLAG_SPHERICAL_BEAM) return launch_general_chunk<N, true>(ctx, p, layers, maxm, tabs, jv);
+  return launch_general_chunk<N, false>(ctx, p, layers, maxm, tabs, jv);
+}
+
 dsp_status launch_general(dsp_context ctx, int N, const FluxParams& p, long long layers, int maxm,
                           const double* tabs, const JacView* jv) {
   switch (N) {
-    case 4: return launch_general_chunk<4>(ctx, p, layers, maxm, tabs, jv);
-    case 6: return launch_general_chunk<6>(ctx, p, layers, maxm, tabs, jv);
-    case 8: return launch_general_chunk<8>(ctx, p, layers, maxm, tabs, jv);
-    case 10: return launch_general_chunk<10>(ctx, p, layers, maxm, tabs, jv);
-    case 12: return launch_general_chunk<12>(ctx, p, layers, maxm, tabs, jv);
-    case 14: return launch_general_chunk<14>(ctx, p, layers, maxm, tabs, jv);
-    case 16: return launch_general_chunk<16>(ctx, p, layers, maxm, tabs, jv);
-    case 32: return launch_general_chunk<32>(ctx, p, layers, maxm, tabs, jv);
-    case 64: return launch_general_chunk<64>(ctx, p, layers, maxm, tabs, jv);
+    case 4: return launch_general_n<4>(ctx, p, layers, maxm, tabs, jv);
+    case 6: return launch_general_n<6>(ctx, p, layers, maxm, tabs, jv);
+    case 8: return launch_general_n<8>(ctx, p, layers, maxm, tabs, jv);
+    case 10: return launch_general_n<10>(ctx, p, layers, maxm, tabs, jv);
+    case 12: return launch_general_n<12>(ctx, p, layers, maxm, tabs, jv);
+    case 14: return launch_general_n<14>(ctx, p, layers, maxm, tabs, jv);
+    case 16: return launch_general_n<16>(ctx, p, layers, maxm, tabs, jv);
+    case 32: return launch_general_n<32>(ctx, p, layers, maxm, tabs, jv);
+    case 64: return launch_general_n<64>(ctx, p, layers, maxm, tabs, jv);
   }
   return fail(ctx, DSP_ERR_UNSUPPORTED, "unsupported num_streams");
 }
@@ -232,11 +255,10 @@ dsp_status general_solve(dsp_context ctx, const dsp_general_batch* bin, const ds
   if (n < 0) return fail(ctx, DSP_ERR_INVALID_INPUT, "n_inst must be >= 0");
   if (n == 0) return DSP_OK;
   const uint32_t fl = b.flags;
-  if (fl & DSP_FLAG_SPHERICAL_BEAM)
-    return fail(ctx, DSP_ERR_UNSUPPORTED, "the general solver takes no pseudo-spherical beam in this engine");
   if (fl & DSP_FLAG_HG_G)
     return fail(ctx, DSP_ERR_UNSUPPORTED, "the Henyey-Greenstein g fast path is a flux-batch option");
   const bool thermal = (fl & DSP_FLAG_THERMAL) != 0;
+  const bool spherical = (fl & DSP_FLAG_SPHERICAL_BEAM) != 0;
   const bool user_tau = (fl & DSP_GFLAG_USER_TAU) != 0, user_mu = (fl & DSP_GFLAG_USER_MU) != 0;
   const bool only_fluxes = (fl & DSP_GFLAG_ONLY_FLUXES) != 0;
   const bool do_int = user_mu && !only_fluxes;
@@ -246,6 +268,8 @@ dsp_status general_solve(dsp_context ctx, const dsp_general_batch* bin, const ds
     return fail(ctx, DSP_ERR_INVALID_INPUT, "num_streams, num_layers, layer_offset, num_phase_func_moments, "
                                             "delta_tau, single_scat_albedo and phase_function_moments are required");
   if (thermal && !b.temperature) return fail(ctx, DSP_ERR_INVALID_INPUT, "thermal emission needs temperature");
+  if (spherical && (!b.level_altitudes || !b.bottom_radius.ptr))
+    return fail(ctx, DSP_ERR_INVALID_INPUT, "the spherical beam needs level_altitudes and bottom_radius");
   if (b.pmom_count < 1) return fail(ctx, DSP_ERR_INVALID_INPUT, "pmom_count must be >= 1");
   if (user_tau && (b.num_user_tau <= 0 || !b.tau_user.ptr))
     return fail(ctx, DSP_ERR_INVALID_INPUT, "use_user_tau needs num_user_tau > 0 and tau_user");
@@ -315,6 +339,8 @@ dsp_status general_solve(dsp_context ctx, const dsp_general_batch* bin, const ds
   const double* d_ssa;
   const double* d_pmom;
   const double* d_temp = nullptr;
+  const double* d_zalt = nullptr;
+  dsp_darray d_rbot = b.bottom_radius;
   const int32_t* d_L;
   const int64_t* d_off;
   const int32_t* d_nmom;
@@ -325,6 +351,8 @@ dsp_status general_solve(dsp_context ctx, const dsp_general_batch* bin, const ds
       need += align256(n * sizeof(int32_t)) * 2 + align256((n + 1) * sizeof(int64_t));
       need += align256(total_layers * sizeof(double)) * 2 + align256(total_layers * b.pmom_count * sizeof(double));
       if (thermal) need += align256((total_layers + n) * sizeof(double));
+      if (spherical)
+        need += align256((total_layers + n) * sizeof(double)) + align256(darray_elems(b.bottom_radius, 1) * sizeof(double));
       for (int k = 0; k < 3; ++k)
         if (lists[k]->ptr && list_n[k] > 0) need += align256(darray_elems(*lists[k], list_n[k]) * sizeof(double));
     }
@@ -347,6 +375,7 @@ dsp_status general_solve(dsp_context ctx, const dsp_general_batch* bin, const ds
       d_ssa = b.single_scat_albedo;
       d_pmom = b.phase_function_moments;
       d_temp = thermal ? b.temperature : nullptr;
+      d_zalt = spherical ? b.level_altitudes : nullptr;
       for (int k = 0; k < 3; ++k) dlists[k] = *lists[k];
     } else {
       d_L = static_cast<const int32_t*>(put(b.num_layers, n * sizeof(int32_t)));
@@ -356,6 +385,11 @@ dsp_status general_solve(dsp_context ctx, const dsp_general_batch* bin, const ds
       d_ssa = static_cast<const double*>(put(b.single_scat_albedo, total_layers * sizeof(double)));
       d_pmom = static_cast<const double*>(put(b.phase_function_moments, total_layers * b.pmom_count * sizeof(double)));
       if (thermal) d_temp = static_cast<const double*>(put(b.temperature, (total_layers + n) * sizeof(double)));
+      if (spherical) {
+        d_zalt = static_cast<const double*>(put(b.level_altitudes, (total_layers + n) * sizeof(double)));
+        d_rbot.ptr =
+            static_cast<const double*>(put(b.bottom_radius.ptr, darray_elems(b.bottom_radius, 1) * sizeof(double)));
+      }
       for (int k = 0; k < 3; ++k) {
         dlists[k] = *lists[k];
         if (lists[k]->ptr && list_n[k] > 0)
@@ -477,9 +511,11 @@ dsp_status general_solve(dsp_context ctx, const dsp_general_batch* bin, const ds
   auto jac_per_layer = [&](int N) -> int64_t {
     return jrecs ? (int64_t)jpq_stride(N) + jrec_stride(N) + (int64_t)N * jdof : 0;
   };
+  // with the pseudo-spherical beam: the spherical record of every layer
+  auto sph_per_layer = [&](int N) -> int64_t { return spherical ? (int64_t)sph_stride(N) : 0; };
   for (int N : kSupported) {
     const int64_t lstride = glrec_stride(N, numu_eff);
-    const int64_t per_layer = lstride + brec_stride(N) + N + jac_per_layer(N);
+    const int64_t per_layer = lstride + brec_stride(N) + N + sph_per_layer(N) + jac_per_layer(N);
     Chunk c;
     c.N = N;
     size_t bytes = 0;
@@ -524,7 +560,9 @@ dsp_status general_solve(dsp_context ctx, const dsp_general_batch* bin, const ds
                    align256(c.layers * 4);
       const int64_t lstride = glrec_stride(c.N, numu_eff);
       const size_t w =
-          (size_t)(c.inst_doubles + c.layers * (lstride + brec_stride(c.N) + c.N + jac_per_layer(c.N))) * sizeof(double);
+          (size_t)(c.inst_doubles +
+                   c.layers * (lstride + brec_stride(c.N) + c.N + sph_per_layer(c.N) + jac_per_layer(c.N))) *
+          sizeof(double);
       if (w > ws_need) ws_need = w;
     }
     if ((st = ensure(ctx, &ctx->meta, &ctx->meta_bytes, meta_need, "chunk index")) != DSP_OK) return st;
@@ -579,6 +617,9 @@ dsp_status general_solve(dsp_context ctx, const dsp_general_batch* bin, const ds
     g.ssa = d_ssa;
     g.pmom = d_pmom;
     g.temp = d_temp;
+    g.zalt = d_zalt;
+    p.rbot.p = d_rbot.ptr;
+    p.rbot.s = d_rbot.stride;
     g.utau = {dlists[0].ptr, dlists[0].stride};
     g.umu = {dlists[1].ptr, dlists[1].stride};
     g.phi = {dlists[2].ptr, dlists[2].stride};
@@ -604,10 +645,12 @@ dsp_status general_solve(dsp_context ctx, const dsp_general_batch* bin, const ds
       p.layer_rec = w + c.inst_doubles;
       p.bvp_rec = p.layer_rec + c.layers * g.lstride;
       g.cc = p.bvp_rec + c.layers * brec_stride(c.N);
+      // after the solution coefficients: the spherical records
+      p.sph = spherical ? g.cc + c.layers * c.N : nullptr;
       JacView jv;
       if (jac) {
-        // after the solution coefficients: P/Q, multipliers, replayed values
-        double* jb = g.cc + c.layers * c.N;
+        // then P/Q, multipliers, replayed values
+        double* jb = g.cc + c.layers * (c.N + sph_per_layer(c.N));
         p.jac_pq = jrecs ? jb : nullptr;
         p.jac_rec = jrecs ? jb + c.layers * jpq_stride(c.N) : nullptr;
         jv.cv = jrecs ? p.jac_rec + c.layers * jrec_stride(c.N) : nullptr;

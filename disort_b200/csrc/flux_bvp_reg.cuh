@@ -151,7 +151,9 @@ __global__ void __launch_bounds__(RCfg<N>::CTA, RCfg<N>::MINB) flux_bvp_reg_kern
   auto LR = [&](int l) { return lrec0 + (long long)l * lstride; };
   // pseudo-spherical beam: layer l's record [Z1 | xba | ch], and its particular
   // solution exp(-xba tau) (Z0 + Z1 tau) at stream iq (solve0, FluxSolver.cpp:1001-1090)
-  auto SR = [&](int l) { return p.sph + ((long long)i * L + l) * sph_stride(N); };
+  // (general solver: one record per layer task of the chunk)
+  const long long sph0 = GEN ? (long long)p.g.lay_off[slot] : (long long)i * L;
+  auto SR = [&](int l) { return p.sph + (sph0 + l) * sph_stride(N); };
   auto zsph = [&](const double* lrl, int l, int iq, double tau) {
     const double* sr = SR(l);
     return exp(-sr[sph_xba(N)] * tau) * (ld_rec(lrl + C::SZB + iq) + sr[iq] * tau);

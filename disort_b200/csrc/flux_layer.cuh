@@ -820,16 +820,8 @@ __global__ void __launch_bounds__(LCfg<N, GEN>::CTA, LCfg<N, GEN>::MINB) flux_la
   const double fbeam = rec[H_FBEAM];
   if (fbeam > 0.0) {
     // ---- beam (computeBeamSource, FluxSolver.cpp:595-643) -----------------
+    // source coefficients zj in bv
     const double umu0 = rec[H_UMU0];
-    double beam_mu = umu0;
-    const double mu0sq = umu0 * umu0;
-    const double dither = 1000.0 * 2.220446049250313e-16;
-    bool dith = false;
-    for (int k = 0; k < NN; ++k) {
-      const double kk = lam[k];
-      if (fabs(1.0 - mu0sq * kk * kk) < dither) dith = true;
-    }
-    if (dith) beam_mu = 0.999 * umu0;
     const double* yb;
     if constexpr (GEN) {
       // P_l^m(-mu0) of this mode (DisortSolver.cpp:1334-1335); Y rows l < m are zero
@@ -848,6 +840,29 @@ __global__ void __launch_bounds__(LCfg<N, GEN>::CTA, LCfg<N, GEN>::MINB) flux_la
       bv[r] = bfac * sacc / (4.0 * 3.14159265358979323846);
     }
     team_sync<TEAM>();
+  }
+  if (fbeam > 0.0 && GEN && (p.flags & DSP_FLAG_SPHERICAL_BEAM)) {
+    // pseudo-spherical beam (general solver): the source coefficients zj go to
+    // the particular-solution slot in its row order, where the user-angle
+    // interpolation reads them (computeBeamSourceSpherical keeps the raw zj
+    // for interpSource, DisortSolver.cpp:1524-1527); gen_sph_source_kernel
+    // then replaces them with Z0
+    if (t < NN) {
+      lrec[lrec_zb(N) + NN + t] = bv[t];
+      lrec[lrec_zb(N) + NN - t - 1] = bv[NN + t];
+    }
+    team_sync<TEAM>();
+  } else if (fbeam > 0.0) {
+    const double umu0 = rec[H_UMU0];
+    double beam_mu = umu0;
+    const double mu0sq = umu0 * umu0;
+    const double dither = 1000.0 * 2.220446049250313e-16;
+    bool dith = false;
+    for (int k = 0; k < NN; ++k) {
+      const double kk = lam[k];
+      if (fabs(1.0 - mu0sq * kk * kk) < dither) dith = true;
+    }
+    if (dith) beam_mu = 0.999 * umu0;
     const double bp = (t < NN) ? bv[t] : 0.0, bm = (t < NN) ? bv[NN + t] : 0.0;
     const double m1 = (bp + bm) / mui;  // M^{-1} r1
     const double m2 = (bp - bm) / mui;  // M^{-1} r2

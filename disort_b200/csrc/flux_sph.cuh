@@ -16,6 +16,9 @@
 //    quadrature angle or a near-singular system).
 // Z0 replaces the layer record's plane-parallel zb; Z1, xba and ch go to the
 // layer's spherical record (sph_stride).
+// The general solver (DisortSolver.cpp:740-790, 1396-1530) runs the same two
+// kernels in their GEN form: the Chapman factors once per chunk after its
+// setup, the particular solution once per azimuth mode after the layer kernel.
 #pragma once
 
 #include "dsp_device.cuh"
@@ -60,40 +63,61 @@ __device__ double chapman_slant(int lc, double tau_frac, ZD zd, DT dt, int num_l
   return sum;
 }
 
-// One warp per instance (4 per CTA).
-static __global__ void __launch_bounds__(128) flux_sph_chapman_kernel(FluxParams p) {
+// One warp per instance (4 per CTA).  GEN: the general solver's chunk
+// addressing (ragged layers; one spherical record per layer task of the chunk;
+// level altitudes laid out like the level temperatures).
+template <bool GEN = false>
+__global__ void __launch_bounds__(128) flux_sph_chapman_kernel(FluxParams p) {
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  const int i = blockIdx.x * 4 + warp;
-  if (i >= p.n) return;
+  const int slot = blockIdx.x * 4 + warp;
+  if (slot >= p.n) return;
+  int i, L;
+  double* rec;
+  InstLayout il;
+  const double* zin;
+  double* sph0;
+  if constexpr (GEN) {
+    i = p.g.ids[slot];
+    L = p.g.Ls[i];
+    il = InstLayout::make(L, p.N);
+    rec = p.inst_rec + p.g.inst_off[slot];
+    zin = p.g.zalt + p.g.in_off[i] + i;
+    sph0 = p.sph + p.g.lay_off[slot] * sph_stride(p.N);
+  } else {
+    i = slot;
+    L = p.L;
+    il = p.il;
+    rec = p.inst_rec + (long long)i * p.il.stride;
+    zin = p.zalt.row(i);
+    sph0 = p.sph + (long long)i * L * sph_stride(p.N);
+  }
   if (p.status && p.status[i] == DSP_ERR_INVALID_INPUT) return;
-  const int L = p.L, N = p.N;
-  double* rec = p.inst_rec + (long long)i * p.il.stride;
-  const InstLayout& il = p.il;
+  const int N = p.N;
   const double fbeam = rec[H_FBEAM], mu0 = rec[H_UMU0];
   if (!(fbeam > 0.0)) return;
   const bool ifb = (p.flags & DSP_FLAG_INDEX_FROM_BOTTOM) != 0;
-  const double* zin = p.zalt.row(i);
   const double r = p.rbot(i);
   const double* dts = rec + il.dtau_s;
   const double* taus = rec + il.tau_s;
-  // the layers of the absorption loop (FluxSolver.cpp:312-331): the
-  // transmission is computed down to that cut even without a layer cut
+  // the layers of the absorption loop (FluxSolver.cpp:312-331; DisortSolver.cpp:
+  // 749-790): the transmission is computed down to that cut even without a
+  // layer cut
   int ncut_abs = L;
   if (lane == 0) {
-    const double* dtau_in = p.dtau.row(i);
-    const double* ssa_in = p.ssa.row(i);
     double abstau = 0.0;
     for (int lc = 0; lc < L; ++lc) {
       if (abstau < 10.0) ncut_abs = lc + 1;
       const int lin = ifb ? L - 1 - lc : lc;
-      abstau += (1.0 - ssa_in[lin]) * dtau_in[lin];
+      const double w = GEN ? p.g.ssa[p.g.in_off[i] + lin] : p.ssa.row(i)[lin];
+      const double d = GEN ? p.g.dtau[p.g.in_off[i] + lin] : p.dtau.row(i)[lin];
+      abstau += (1.0 - w) * d;
     }
   }
   ncut_abs = __shfl_sync(0xffffffffu, ncut_abs, 0);
   auto zd = [&](int j) { return zin[ifb ? L - j : j]; };
   auto dt = [&](int j) { return dts[j - 1]; };
   for (int lc = lane; lc < L; lc += 32) {
-    double* sr = p.sph + ((long long)i * L + lc) * sph_stride(N);
+    double* sr = sph0 + (long long)lc * sph_stride(N);
     if (lc < ncut_abs) {
       const double taup_mid = taus[lc] + dts[lc] / 2.0;
       const double chtau_mid = chapman_slant(lc + 1, 0.5, zd, dt, L, r, mu0);
@@ -116,7 +140,10 @@ struct SCfg {
   static constexpr size_t smem_bytes() { return sizeof(double) * (size_t)WPC * WARP_SMEM; }
 };
 
-template <int N>
+// GEN: one azimuth mode of the general solver (P_l^m tables of the mode; the
+// source coefficients zj, with the (2 - delta_m0) factor, are read from the
+// particular-solution slot where the layer kernel left them).
+template <int N, bool GEN = false>
 __global__ void __launch_bounds__(128) flux_sph_source_kernel(FluxParams p) {
   using C = SCfg<N>;
   constexpr int NN = C::NN, LDA = C::LDA;
@@ -124,13 +151,39 @@ __global__ void __launch_bounds__(128) flux_sph_source_kernel(FluxParams p) {
   extern __shared__ double smem[];
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const long long task = (long long)blockIdx.x * C::WPC + warp;
-  if (task >= (long long)p.n * p.L) return;
-  const int i = (int)(task / p.L), lc = (int)(task % p.L);
+  int i, lc, Lin;
+  const double* rec;
+  InstLayout il;
+  double* lrec;
+  const double* pml;
+  if constexpr (GEN) {
+    if (task >= p.g.lay_off[p.n]) return;
+    const int ci = p.g.layer_inst[task];
+    i = p.g.ids[ci];
+    lc = (int)(task - p.g.lay_off[ci]);
+    Lin = p.g.Ls[i];
+    il = InstLayout::make(Lin, N);
+    rec = p.inst_rec + p.g.inst_off[ci];
+    lrec = p.layer_rec + task * p.g.lstride;
+    const int lin = (p.flags & DSP_FLAG_INDEX_FROM_BOTTOM) ? Lin - 1 - lc : lc;
+    pml = p.g.pmom + (p.g.in_off[i] + lin) * (long long)p.pc;
+  } else {
+    if (task >= (long long)p.n * p.L) return;
+    i = (int)(task / p.L);
+    lc = (int)(task % p.L);
+    Lin = p.L;
+    il = p.il;
+    rec = p.inst_rec + (long long)i * p.il.stride;
+    lrec = p.layer_rec + task * lrec_stride(N);
+    const int lin = (p.flags & DSP_FLAG_INDEX_FROM_BOTTOM) ? p.L - 1 - lc : lc;
+    pml = p.pmom.row(i) + (long long)lin * p.pc;
+  }
   if (p.status && p.status[i] == DSP_ERR_INVALID_INPUT) return;
-  const double* rec = p.inst_rec + (long long)i * p.il.stride;
-  const InstLayout& il = p.il;
   const double fbeam = rec[H_FBEAM];
   if (!(fbeam > 0.0) || lc >= (int)rec[H_NCUT]) return;
+  if constexpr (GEN) {
+    if (p.g.m > (int)rec[H_NAZ] || rec[H_DONE] != 0.0) return;
+  }
   double* sm = smem + warp * C::WARP_SMEM;
   double* A = sm + C::O_A;
   double* gl = sm + C::O_GL;
@@ -139,21 +192,19 @@ __global__ void __launch_bounds__(128) flux_sph_source_kernel(FluxParams p) {
   double* z1 = sm + C::O_Z1;
   int* piv = reinterpret_cast<int*>(sm + C::O_PIV);
   const double* mu = p.tables + tab_mu(N);
-  const double* Y = p.tables + tab_ylm(N);  // Y[l * N + i] = P_l(mu_i)
+  const double* Y = p.tables + tab_ylm(N);  // Y[l * N + i] = P_l^m(mu_i)
   const double* taus = rec + il.tau_s;
   const double* btr = rec + il.btr;
   double* sr = p.sph + task * sph_stride(N);
-  double* lrec = p.layer_rec + task * lrec_stride(N);
 
-  // scaled phase coefficients g'_k (disortSet, FluxSolver.cpp:336-386)
+  // scaled phase coefficients g'_k (disortSet, FluxSolver.cpp:336-386;
+  // DisortSolver.cpp:663-747, where P_0 is normalised to 1)
   {
-    const int lin = (p.flags & DSP_FLAG_INDEX_FROM_BOTTOM) ? p.L - 1 - lc : lc;
-    const double* pml = p.pmom.row(i) + (long long)lin * p.pc;
     const double ws = rec[il.ssa_s + lc];
     const int mode = (int)rec[il.mode + lc];
     const double f = rec[il.fsc + lc], sig = rec[il.sig + lc];
     for (int k = lane; k < N; k += 32) {
-      const double pk = pml[k];
+      const double pk = (GEN && k == 0) ? 1.0 : pml[k];
       double g;
       if (mode == 0) g = (2.0 * k + 1.0) * ws * pk;
       else if (mode == 1) g = (2.0 * k + 1.0) * ws * (pk - f) / (1.0 - f);
@@ -167,11 +218,18 @@ __global__ void __launch_bounds__(128) flux_sph_source_kernel(FluxParams p) {
   __syncwarp();
   // source coefficients zj (FluxSolver.cpp:660-667) and the phase matrix C:
   // rows iq < NN from the quadrature sums, the other half by symmetry
-  const double* yb = rec + il.yb;
-  for (int iq = lane; iq < N; iq += 32) {
-    double s = 0.0;
-    for (int k = 0; k < N; ++k) s += gl[k] * Y[k * N + iq] * yb[k];
-    zj[iq] = fbeam * s / (4.0 * PI);
+  if constexpr (GEN) {
+    for (int iq = lane; iq < NN; iq += 32) {
+      zj[iq] = lrec[lrec_zb(N) + NN + iq];
+      zj[NN + iq] = lrec[lrec_zb(N) + NN - 1 - iq];
+    }
+  } else {
+    const double* yb = rec + il.yb;
+    for (int iq = lane; iq < N; iq += 32) {
+      double s = 0.0;
+      for (int k = 0; k < N; ++k) s += gl[k] * Y[k * N + iq] * yb[k];
+      zj[iq] = fbeam * s / (4.0 * PI);
+    }
   }
   const double* wt = p.tables + tab_wt(N);
   for (int e = lane; e < NN * N; e += 32) {

@@ -76,6 +76,8 @@ static __global__ void __launch_bounds__(128) gen_setup_kernel(FluxParams p) {
       if ((umu0 <= 0.0 || umu0 > 1.0) && fbeam > 0.0) bad = true;
       if (alb < 0.0 || alb > 1.0) bad = true;
       if ((fl & DSP_FLAG_DELTA_M_PLUS) && nmom < N + 1) bad = true;
+      // bottom_radius > 0 with the pseudo-spherical beam (DisortConfig.cpp:189-196)
+      if ((fl & DSP_FLAG_SPHERICAL_BEAM) && !(p.rbot(i) > 0.0)) bad = true;
       if (thermal) {
         if (wlo < 0.0 || whi <= wlo) bad = true;
         if (ttop < 0.0 || tbot < 0.0) bad = true;

@@ -265,8 +265,8 @@ void validate_base(const DisortFluxConfig& c, const SpectralOverrides& ov) {
 }
 
 struct Packed {
-  std::vector<double> lo, hi, dtau, ssa, pmom, temp, alb, emis, fbeam, fisot, fisob;
-  double mu0 = 0.5, ttop = 0.0, tbot = 0.0;
+  std::vector<double> lo, hi, dtau, ssa, pmom, temp, alb, emis, fbeam, fisot, fisob, zalt;
+  double mu0 = 0.5, ttop = 0.0, tbot = 0.0, rbot = 0.0;
 };
 
 // Build a dsp_flux_batch for the whole loop: overrides become per-instance
@@ -284,7 +284,8 @@ dsp_flux_batch pack(const DisortFluxConfig& c, const std::vector<std::pair<doubl
   b.pmom_count = pc;
   b.flags = (c.use_thermal_emission ? DSP_FLAG_THERMAL : 0u) | (c.use_delta_m_plus ? DSP_FLAG_DELTA_M_PLUS : 0u) |
             (c.use_diffusion_lower_bc ? DSP_FLAG_DIFFUSION_LOWER_BC : 0u) |
-            (c.index_from_bottom ? DSP_FLAG_INDEX_FROM_BOTTOM : 0u);
+            (c.index_from_bottom ? DSP_FLAG_INDEX_FROM_BOTTOM : 0u) |
+            (c.use_spherical_beam ? DSP_FLAG_SPHERICAL_BEAM : 0u);
   pk.lo.resize(n);
   pk.hi.resize(n);
   for (int i = 0; i < n; ++i) {
@@ -323,6 +324,12 @@ dsp_flux_batch pack(const DisortFluxConfig& c, const std::vector<std::pair<doubl
     pk.temp.assign(c.temperature.begin(), c.temperature.begin() + L + 1);
     b.temperature = {pk.temp.data(), 0};
   }
+  if (c.use_spherical_beam) {  // one column geometry for every band
+    pk.zalt.assign(c.level_altitudes.begin(), c.level_altitudes.begin() + L + 1);
+    pk.rbot = c.bottom_radius;
+    b.level_altitudes = {pk.zalt.data(), 0};
+    b.bottom_radius = {&pk.rbot, 0};
+  }
   auto scalar = [&](const std::vector<double>& per, double base, std::vector<double>& dst) -> dsp_darray {
     if (per.empty()) {
       dst.assign(1, base);
@@ -352,7 +359,6 @@ void run(const DisortFluxConfig& c, const std::vector<std::pair<double, double>>
   if (!supported(c.num_streams))
     throw std::invalid_argument("Unsupported num_streams=" + std::to_string(c.num_streams) +
                                 ". Supported values: 4, 6, 8, 10, 12, 14, 16, 32, 64");
-  if (c.use_spherical_beam) throw std::invalid_argument("use_spherical_beam is not supported by the B200 engine");
   const size_t n = bands.size();
   auto check = [&](size_t got, const char* name) {
     if (got != 0 && got != n)

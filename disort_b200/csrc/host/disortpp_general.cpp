@@ -196,7 +196,6 @@ void check_engine(const DisortConfig& c) {
   if (!f.use_lambertian_surface) throw std::invalid_argument("BRDF surfaces are not supported by the B200 engine");
   if (f.intensity_corr_buras || f.intensity_corr_nakajima)
     throw std::invalid_argument("intensity corrections are not supported by the B200 engine");
-  if (f.use_spherical_beam) throw std::invalid_argument("use_spherical_beam is not supported by the B200 engine");
   if (f.output_fourier_expansion)
     throw std::invalid_argument("output_fourier_expansion is not supported by the B200 engine");
   // validate() does not look at the user optical depths; the reference reads
@@ -273,9 +272,9 @@ void fill_automatic(DisortConfig& c) {
 struct GenPacked {
   std::vector<int32_t> nstr, nlyr, nmom;
   std::vector<int64_t> off;
-  std::vector<double> dtau, ssa, pmom, temp, utau, umu, phi;
+  std::vector<double> dtau, ssa, pmom, temp, zalt, utau, umu, phi;
   std::vector<double> lo, hi, alb, emis, fbeam, fisot, fisob;
-  double mu0 = 0.5, phi0 = 0.0, ttop = 0.0, tbot = 0.0;
+  double mu0 = 0.5, phi0 = 0.0, ttop = 0.0, tbot = 0.0, rbot = 0.0;
 };
 
 // One batch for the whole loop.  `c` already carries the automatic fields.
@@ -292,7 +291,8 @@ dsp_general_batch pack_general(const DisortConfig& c, const std::vector<std::pai
             (f.use_diffusion_lower_bc ? DSP_FLAG_DIFFUSION_LOWER_BC : 0u) |
             (f.index_from_bottom ? DSP_FLAG_INDEX_FROM_BOTTOM : 0u) | (f.use_user_tau ? DSP_GFLAG_USER_TAU : 0u) |
             (f.use_user_mu && !f.comp_only_fluxes ? DSP_GFLAG_USER_MU : 0u) |
-            (f.comp_only_fluxes ? DSP_GFLAG_ONLY_FLUXES : 0u);
+            (f.comp_only_fluxes ? DSP_GFLAG_ONLY_FLUXES : 0u) |
+            (f.use_spherical_beam ? DSP_FLAG_SPHERICAL_BEAM : 0u);
   pk.nstr.assign(n, c.num_streams);
   pk.nlyr.assign(n, L);
   pk.nmom.assign(n, c.num_phase_func_moments);
@@ -328,6 +328,15 @@ dsp_general_batch pack_general(const DisortConfig& c, const std::vector<std::pai
     for (int i = 0; i < n; ++i)
       std::copy(c.temperature.begin(), c.temperature.begin() + L + 1, pk.temp.begin() + static_cast<size_t>(i) * (L + 1));
     b.temperature = pk.temp.data();
+  }
+  if (f.use_spherical_beam) {  // the same column geometry for every band
+    pk.zalt.resize(static_cast<size_t>(n) * (L + 1));
+    for (int i = 0; i < n; ++i)
+      std::copy(c.level_altitudes.begin(), c.level_altitudes.begin() + L + 1,
+                pk.zalt.begin() + static_cast<size_t>(i) * (L + 1));
+    pk.rbot = c.bottom_radius;
+    b.level_altitudes = pk.zalt.data();
+    b.bottom_radius = {&pk.rbot, 0};
   }
   if (f.use_user_tau) {
     pk.utau.assign(c.tau_user.begin(), c.tau_user.begin() + c.num_user_tau);

@@ -61,7 +61,7 @@ typedef enum dsp_status {
 #define DSP_FLAG_DIFFUSION_LOWER_BC (1u << 2) /* use_diffusion_lower_bc */
 #define DSP_FLAG_INDEX_FROM_BOTTOM  (1u << 3) /* index_from_bottom (layer/level arrays reversed) */
 #define DSP_FLAG_DEVICE_POINTERS    (1u << 4) /* every pointer is device memory */
-#define DSP_FLAG_SPHERICAL_BEAM     (1u << 5) /* use_spherical_beam (flux batches; the general batch rejects it) */
+#define DSP_FLAG_SPHERICAL_BEAM     (1u << 5) /* use_spherical_beam */
 #define DSP_FLAG_TEMPERATURE_JAC    (1u << 6) /* compute_temperature_jacobian: use dsp_flux_bands_solve_jac */
 /*
  * Henyey-Greenstein fast path (flux batches): phase_function_moments holds ONE
@@ -177,6 +177,9 @@ typedef struct dsp_general_batch {
   dsp_darray wavenumber_low, wavenumber_high, surface_albedo, emissivity_top, direct_beam_flux,
       direct_beam_mu, direct_beam_phi, isotropic_flux_top, isotropic_flux_bottom, temperature_top,
       temperature_bottom; /* [1] each */
+  /* pseudo-spherical beam (DSP_FLAG_SPHERICAL_BEAM; may be NULL otherwise) */
+  const double* level_altitudes;        /* [total layers + n_inst], top down, levels like temperature */
+  dsp_darray bottom_radius;             /* [1] */
 } dsp_general_batch;
 
 /*

@@ -18,6 +18,9 @@ struct GeneralInstance {
   bool thermal = false, dmplus = false, dlbc = false, ifb = false;
   bool user_tau = false, user_mu = false, only_fluxes = false;
   bool temperature_jac = false;  // compute_temperature_jacobian
+  bool spherical = false;        // use_spherical_beam
+  double radius = 0.0;           // bottom_radius
+  const double* zalt = nullptr;  // level_altitudes [L+1] (spherical only)
   double accur = 0.0;
   double wlo = 0, whi = 0, alb = 0, emis = 1, fbeam = 0, umu0 = 0.5, phi0 = 0, fisot = 0, fisob = 0, ttop = 0, tbot = 0;
   const double *dtau = nullptr, *ssa = nullptr, *pmom = nullptr, *temp = nullptr;
@@ -68,6 +71,7 @@ inline int validate_general(const GeneralInstance& c) {
     for (int j = 0; j < c.nphi; ++j)
       if (c.phi[j] < 0.0 || c.phi[j] > 360.0) return DSP_ERR_INVALID_INPUT;
   }
+  if (c.spherical && (c.radius <= 0.0 || !c.zalt)) return DSP_ERR_INVALID_INPUT;
   if (c.dmplus && c.nmom < c.N + 1) return DSP_ERR_INVALID_INPUT;
   if (c.accur < 0.0) return DSP_ERR_INVALID_INPUT;
   if (c.thermal) {
@@ -88,7 +92,7 @@ class GeneralOracle {
 inline int GeneralOracle::solve(const GeneralInstance& cin, const GeneralOutput& out) {
   GeneralInstance c = cin;
   const int L = c.L, N = c.N, NN = N / 2;
-  std::vector<double> rdt, rss, rpm, rtp, rut;
+  std::vector<double> rdt, rss, rpm, rtp, rut, rza;
   if (c.ifb) {  // reverseInputArrays (IndexConversion.hpp:16-40)
     rdt.assign(c.dtau, c.dtau + L);
     rss.assign(c.ssa, c.ssa + L);
@@ -104,6 +108,11 @@ inline int GeneralOracle::solve(const GeneralInstance& cin, const GeneralOutput&
       rtp.assign(c.temp, c.temp + L + 1);
       std::reverse(rtp.begin(), rtp.end());
       c.temp = rtp.data();
+    }
+    if (c.zalt) {
+      rza.assign(c.zalt, c.zalt + L + 1);
+      std::reverse(rza.begin(), rza.end());
+      c.zalt = rza.data();
     }
     if (c.user_tau && c.utau && c.ntau > 0) {
       double total = 0.0;
@@ -181,9 +190,23 @@ inline int GeneralOracle::solve(const GeneralInstance& cin, const GeneralOutput&
     }
     fsc[lc] = f;
   }
+  // Chapman factor per layer (the pseudo-spherical beam, DisortSolver.cpp:740-782)
+  std::vector<double> chap(L, 0.0);
   if (c.fbeam > 0.0) {
     btr[0] = 1.0;
-    for (int lc = 0; lc < ncut; ++lc) btr[lc + 1] = std::exp(-taus[lc + 1] / c.umu0);
+    if (c.spherical) {
+      for (int lc = 0; lc < ncut; ++lc) {
+        const double taup_mid = taus[lc] + dts[lc] / 2.0;
+        const double chtau_mid = chapman(lc + 1, 0.5, c.zalt, dts.data(), L, c.radius, c.umu0);
+        chap[lc] = taup_mid / chtau_mid;
+        btr[lc + 1] = std::exp(-chapman(lc + 1, 0.0, c.zalt, dts.data(), L, c.radius, c.umu0));
+      }
+    } else {
+      for (int lc = 0; lc < ncut; ++lc) {
+        chap[lc] = c.umu0;
+        btr[lc + 1] = std::exp(-taus[lc + 1] / c.umu0);
+      }
+    }
   }
   const bool lyrcut = (abstau >= 10.0 && !c.thermal && L > 1);
   if (!lyrcut) ncut = L;
@@ -249,6 +272,7 @@ inline int GeneralOracle::solve(const GeneralInstance& cin, const GeneralOutput&
       cc((size_t)N * L), Im((size_t)ntau * numu);
   std::vector<double> cc_top((size_t)NN * N), amb(NN * NN), apb(NN * NN), evec(NN * NN), kred(NN), gpg(NN * NN);
   std::vector<double> A((size_t)N * N), xv(N), bvec(N);
+  std::vector<double> zbs1((size_t)L * N, 0.0), xba(L, 0.0);  // pseudo-spherical beam source
   std::vector<int> piv(N);
   int kconv = 0;
   int status = DSP_OK;
@@ -339,8 +363,67 @@ inline int GeneralOracle::solve(const GeneralInstance& cin, const GeneralOutput&
           }
       }
     }
+    // pseudo-spherical beam source of mode m (computeBeamSourceSpherical,
+    // DisortSolver.cpp:1396-1530): Z(tau) = exp(-xba tau) (Z0 + Z1 tau); the
+    // user-angle interpolation then reads the source coefficients zj themselves
+    if (c.fbeam > 0.0 && c.spherical) {
+      const double umu0n = -c.umu0;
+      legendre_flat(1, m, 1, N - 1, &umu0n, ylb.data());
+      const double big = std::sqrt(std::numeric_limits<double>::max()) / 1.0e10;
+      std::vector<double> zj(N), xb0(N), xb1(N), z1v(N);
+      for (int lc = 0; lc < L; ++lc) {
+        for (int iq = 0; iq < N; ++iq) {
+          double s = 0.0;
+          for (int k = m; k < N; ++k) s += gl[(size_t)lc * N + k] * Yq(k, iq) * ylb[k];
+          zj[iq] = (2.0 - d0) * c.fbeam * s / (4.0 * M_PI);
+        }
+        const double q0a = btr[lc], q2a = btr[lc + 1];
+        double xb = 1.0 / chap[lc];
+        if (std::abs(xb) > big && taus[lc + 1] > 1.0) xb = 0.0;
+        if (std::abs(xb * taus[lc + 1]) > std::log(big)) xb = 0.0;
+        if (std::abs(xb) > 1.0e-5)
+          for (int iq = 0; iq < NN; ++iq)
+            if (std::abs((std::abs(xb) - 1.0 / mu[iq]) / xb) < 0.05) {
+              xb *= 1.001;
+              break;
+            }
+        const double deltat = taus[lc + 1] - taus[lc];
+        for (int iq = 0; iq < N; ++iq) {
+          const double q0 = q0a * zj[iq], q2 = q2a * zj[iq];
+          xb1[iq] = (q2 * std::exp(xb * taus[lc + 1]) - q0 * std::exp(xb * taus[lc])) / deltat;
+          xb0[iq] = q0 * std::exp(xb * taus[lc]) - xb1[iq] * taus[lc];
+        }
+        const double* Cl = &C[(size_t)lc * N * N];
+        auto build = [&]() {
+          for (int i = 0; i < N; ++i)
+            for (int j = 0; j < N; ++j) A[i * N + j] = -Cl[i * N + j];
+          for (int iq = 0; iq < N; ++iq) A[iq * N + iq] += 1.0 + xb * mu[iq];
+        };
+        build();
+        double fro = 0.0;
+        for (int e = 0; e < N * N; ++e) fro += A[e] * A[e];
+        if (1.0 / std::sqrt(fro) < 1.0e-4) {
+          if (xb == 0.0) xb = 5.0e-9;
+          xb *= 1.00000005;
+          build();
+        }
+        xba[lc] = xb;
+        lu_factor(A.data(), N, N, piv.data());
+        for (int iq = 0; iq < N; ++iq) z1v[iq] = xb1[iq];
+        lu_solve(A.data(), N, N, piv.data(), z1v.data());
+        for (int iq = 0; iq < N; ++iq) xv[iq] = xb0[iq] + mu[iq] * z1v[iq];
+        lu_solve(A.data(), N, N, piv.data(), xv.data());
+        for (int iq = 0; iq < N; ++iq) zbraw[(size_t)lc * N + iq] = zj[iq];
+        for (int iq = 0; iq < NN; ++iq) {
+          zb[(size_t)lc * N + NN + iq] = xv[iq];
+          zb[(size_t)lc * N + NN - iq - 1] = xv[iq + NN];
+          zbs1[(size_t)lc * N + NN + iq] = z1v[iq];
+          zbs1[(size_t)lc * N + NN - iq - 1] = z1v[iq + NN];
+        }
+      }
+    }
     // beam particular solution (DisortSolver.cpp:1319-1395)
-    if (c.fbeam > 0.0) {
+    if (c.fbeam > 0.0 && !c.spherical) {
       const double umu0n = -c.umu0;
       legendre_flat(1, m, 1, N - 1, &umu0n, ylb.data());
       const double dither = 1000.0 * std::numeric_limits<double>::epsilon();
@@ -549,12 +632,21 @@ inline int GeneralOracle::solve(const GeneralInstance& cin, const GeneralOutput&
     auto Z0 = [&](int lc, int i) { return z0[(size_t)lc * N + i]; };
     auto Z1 = [&](int lc, int i) { return z1[(size_t)lc * N + i]; };
     const bool beam = c.fbeam > 0.0;
+    // the beam particular solution of layer lc at scaled depth tau (T: the
+    // transmission there); pseudo-spherical: exp(-xba tau) (Z0 + Z1 tau)
+    // (DisortSolver.cpp:1722-1760, 1800-1905)
+    auto ZBT = [&](int lc, int i, double tau, double T) {
+      if (c.spherical) return std::exp(-xba[lc] * tau) * (ZB(lc, i) + zbs1[(size_t)lc * N + i] * tau);
+      return ZB(lc, i) * T;
+    };
     if (m > 0) {
       if (beam) {
         for (int iq = 0; iq < NN; ++iq) b[iq] = -ZB(0, NN - 1 - iq);
-        for (int iq = 0; iq < NN; ++iq) b[nc - NN + iq] = -ZB(lb, NN + iq) * btr[ncut];
+        for (int iq = 0; iq < NN; ++iq) b[nc - NN + iq] = -ZBT(lb, NN + iq, taus[ncut], btr[ncut]);
         for (int lc = 1; lc < ncut; ++lc)
-          for (int iq = 0; iq < N; ++iq) b[lc * N - NN + iq] = (ZB(lc, iq) - ZB(lc - 1, iq)) * btr[lc];
+          for (int iq = 0; iq < N; ++iq)
+            b[lc * N - NN + iq] = c.spherical ? ZBT(lc, iq, taus[lc], 0.0) - ZBT(lc - 1, iq, taus[lc], 0.0)
+                                              : (ZB(lc, iq) - ZB(lc - 1, iq)) * btr[lc];
       }
     } else {
       for (int iq = 0; iq < NN; ++iq) {
@@ -567,7 +659,7 @@ inline int GeneralOracle::solve(const GeneralInstance& cin, const GeneralOutput&
       if (c.dlbc) {
         for (int iq = 0; iq < NN; ++iq) {
           double s = 0.0;
-          if (beam) s -= ZB(lb, NN + iq) * btr[ncut];
+          if (beam) s -= ZBT(lb, NN + iq, taus[ncut], btr[ncut]);
           if (c.thermal) { s -= Z0(lb, NN + iq); s -= Z1(lb, NN + iq) * taus[ncut]; }
           s += pbot + mu[iq] * pbotd;
           b[nc - NN + iq] = s;
@@ -579,14 +671,14 @@ inline int GeneralOracle::solve(const GeneralInstance& cin, const GeneralOutput&
             double refl = 0.0;
             for (int jq = 0; jq < NN; ++jq) {
               double ps = 0.0;
-              if (beam) ps += ZB(lb, NN - 1 - jq) * btr[ncut];
+              if (beam) ps += ZBT(lb, NN - 1 - jq, taus[ncut], btr[ncut]);
               if (c.thermal) ps += Z0(lb, NN - 1 - jq) + Z1(lb, NN - 1 - jq) * taus[ncut];
               refl += wt[jq] * mu[jq] * c.alb * ps;
             }
             s += 2.0 * refl;
           }
           if (beam) {
-            s -= ZB(lb, NN + iq) * btr[ncut];
+            s -= ZBT(lb, NN + iq, taus[ncut], btr[ncut]);
             if (!lyrcut) s += c.alb * c.umu0 * c.fbeam * btr[ncut] / M_PI;
           }
           if (c.thermal) { s -= Z0(lb, NN + iq); s -= Z1(lb, NN + iq) * taus[ncut]; }
@@ -598,7 +690,7 @@ inline int GeneralOracle::solve(const GeneralInstance& cin, const GeneralOutput&
       for (int lc = 1; lc < ncut; ++lc)
         for (int iq = 0; iq < N; ++iq) {
           double s = 0.0;
-          if (beam) { s += ZB(lc, iq) * btr[lc]; s -= ZB(lc - 1, iq) * btr[lc]; }
+          if (beam) { s += ZBT(lc, iq, taus[lc], btr[lc]); s -= ZBT(lc - 1, iq, taus[lc], btr[lc]); }
           if (c.thermal) {
             s += Z0(lc, iq) - Z0(lc - 1, iq);
             s += (Z1(lc, iq) - Z1(lc - 1, iq)) * taus[lc];
@@ -621,8 +713,13 @@ inline int GeneralOracle::solve(const GeneralInstance& cin, const GeneralOutput&
         const double u = utaus[lu];
         double fact = 0, dirint = 0, fldir = 0, fdir = 0;
         if (beam) {
-          fact = std::exp(-u / c.umu0);
-          fdir = c.umu0 * c.fbeam * std::exp(-utau[lu] / c.umu0);
+          if (c.spherical) {  // DisortSolver.cpp:2022-2025
+            fact = std::exp(-u / chap[y]);
+            fdir = std::abs(c.umu0) * c.fbeam * std::exp(-utau[lu] / chap[y]);
+          } else {
+            fact = std::exp(-u / c.umu0);
+            fdir = c.umu0 * c.fbeam * std::exp(-utau[lu] / c.umu0);
+          }
           dirint = c.fbeam * fact;
           fldir = c.umu0 * c.fbeam * fact;
         }
@@ -634,7 +731,14 @@ inline int GeneralOracle::solve(const GeneralInstance& cin, const GeneralOutput&
           for (int j = 0; j < N; ++j) s += Gv(y, i, j) * ec[j];
           in[i] = s;
         }
-        if (beam) for (int i = 0; i < N; ++i) in[i] += ZB(y, i) * fact;
+        if (beam) {
+          if (c.spherical) {
+            const double be = std::exp(-xba[y] * u);
+            for (int i = 0; i < N; ++i) in[i] += be * (ZB(y, i) + zbs1[(size_t)y * N + i] * u);
+          } else {
+            for (int i = 0; i < N; ++i) in[i] += ZB(y, i) * fact;
+          }
+        }
         if (c.thermal) for (int i = 0; i < N; ++i) in[i] += Z0(y, i) + Z1(y, i) * u;
         double ua = 0, uad = 0, uau = 0, fldn = 0, fup = 0;
         for (int iq = 0; iq < NN; ++iq) {

@@ -167,8 +167,10 @@ int oracle_general_bands_solve_jac(const dsp_general_batch* b, const dsp_general
         c.phi = at(b->phi_user, i);
         const int ntau = c.user_tau ? c.ntau : c.L + 1;
         const int numu = (c.user_mu && !c.only_fluxes) ? c.numu : c.N;
-        if ((fl & DSP_FLAG_SPHERICAL_BEAM) != 0) st = DSP_ERR_UNSUPPORTED;
-        else if (c.L > 0 && b->layer_offset[i + 1] - l0 != c.L) st = DSP_ERR_INVALID_INPUT;
+        c.spherical = (fl & DSP_FLAG_SPHERICAL_BEAM) != 0;
+        c.zalt = b->level_altitudes ? b->level_altitudes + l0 + i : nullptr;
+        c.radius = scalar(b->bottom_radius, i, 0.0);
+        if (c.L > 0 && b->layer_offset[i + 1] - l0 != c.L) st = DSP_ERR_INVALID_INPUT;
         else if (ntau > ntau_o || numu > numu_o || c.N > 64) st = DSP_ERR_INVALID_INPUT;
         else if (jac && jac->ndof_out < c.L + 2) st = DSP_ERR_INVALID_INPUT;
         else {

@@ -283,3 +283,47 @@ def test_general_solver_temperature_jacobians():
     ref = jac["flux_up"][0][:4, :5]
     scale = np.abs(ref).max()
     assert np.all(np.abs(got - ref) <= 3e-8 * np.maximum(np.abs(ref), 1e-3 * scale))
+
+
+# ---------------------------------------------------------------------------
+# pseudo-spherical beam through both solver objects
+# ---------------------------------------------------------------------------
+def test_flux_solver_spherical_beam():
+    """SphericalBeam16 (test_flux_solver.cpp:309-358) through DisortFluxSolver16
+    and the spectral-band loop."""
+    c = disortpp.DisortFluxConfig(5, 16)
+    c.use_spherical_beam = True
+    c.direct_beam_flux, c.direct_beam_mu, c.surface_albedo = 1.0, 0.3, 0.1
+    c.bottom_radius = 6371.0
+    c.allocate()
+    c.delta_tau = [0.1] * 5
+    c.single_scat_albedo = [0.9] * 5
+    c.set_isotropic()
+    c.level_altitudes = [100.0, 80.0, 60.0, 40.0, 20.0, 0.0]
+    r = disortpp.DisortFluxSolver16().solve(c)
+    w = _as_workload(c, 0.0, 0.0)
+    w["flags"] |= capi.FLAG_SPHERICAL_BEAM
+    w["arrays"].update(level_altitudes=np.array(c.level_altitudes), bottom_radius=6371.0, temperature=None)
+    ref, st = oracle_lib.flux_solve(w)
+    assert st[0] == 0
+    assert_parity({f: np.array(getattr(r, f))[None, :] for f in capi.FLUX_OUT_FIELDS}, ref, "spherical flux")
+    res = disortpp.solve_flux_spectral_bands(c, [(500.0, 510.0), (600.0, 610.0)])
+    assert_parity({f: np.array(getattr(res[1], f))[None, :] for f in capi.FLUX_OUT_FIELDS}, ref, "spherical bands")
+    c.bottom_radius = 0.0
+    with pytest.raises(ValueError, match="bottom_radius"):
+        disortpp.DisortFluxSolver16().solve(c)
+
+
+@pytest.mark.parametrize("ifb", [False, True])
+def test_disort_solver_spherical_beam(ifb):
+    c = _general_cfg()
+    c.flags.use_spherical_beam = True
+    c.flags.index_from_bottom = ifb
+    c.bottom_radius = 6371.0
+    z = [8.0, 6.0, 4.0, 2.0, 0.0]
+    c.level_altitudes = z[::-1] if ifb else z
+    r = disortpp.DisortSolver().solve(c)
+    inst = _oracle_inst(c, 500.0, 520.0, level_altitudes=list(c.level_altitudes), bottom_radius=6371.0)
+    ref = oracle_lib.general_solve(capi.pack_general([inst], _general_flags(c) | capi.FLAG_SPHERICAL_BEAM))
+    assert (ref["status"] == 0).all()
+    assert_parity_general(_as_outputs([r], True), ref, f"DisortSolver spherical ifb={ifb}")

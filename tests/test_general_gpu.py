@@ -200,3 +200,88 @@ def test_general_mix_at_full_sizes():
     assert rc == 0
     for f in got:
         np.testing.assert_array_equal(got[f], dgot[f])
+
+
+# ---------------------------------------------------------------------------
+# pseudo-spherical beam (DisortSolver.cpp:740-790, 1396-1530)
+# ---------------------------------------------------------------------------
+def spherical_mix(n, seed, nstr, layers=(3, 16), bottom_up=False, thermal=False):
+    """Beam instances of the mixed batch through spherical shells (altitudes
+    2 km per layer over a 6371 km radius), intensities at user angles in every
+    azimuth mode; bottom_up gives the layer arrays and altitudes bottom-up."""
+    insts, flags = workloads.general_mix(n, seed=seed, nstr=(4,), layers=layers)
+    insts = with_streams(insts, nstr)
+    rng = np.random.default_rng(seed + 1)
+    for p in insts:
+        L = p["num_layers"]
+        z = np.linspace(2.0 * L, 0.0, L + 1)
+        p.update(level_altitudes=z[::-1] if bottom_up else z, bottom_radius=6371.0,
+                 direct_beam_phi=float(rng.uniform(0, 90)))
+        if thermal:
+            lo = float(rng.uniform(300, 1500))
+            p.update(temperature=200 + 100 * rng.random(L + 1), wavenumber_low=lo, wavenumber_high=lo * 1.01,
+                     temperature_bottom=300.0)
+    flags |= capi.FLAG_SPHERICAL_BEAM
+    if bottom_up:
+        flags |= capi.FLAG_INDEX_FROM_BOTTOM
+    if thermal:
+        flags |= capi.FLAG_THERMAL
+    return insts, flags
+
+
+def test_general_spherical_golden():
+    """SphericalGeometry (tests/test_solver.cpp:4459-4533) through the general path."""
+    case = golden_cases.load_spherical_cases()[0]
+    inst, flags = golden_cases.general_instance(case)
+    inst.update(level_altitudes=case["level_altitudes"], bottom_radius=case["bottom_radius"])
+    got, ref, _ = both([inst], flags | capi.FLAG_SPHERICAL_BEAM)
+    assert got["status"][0] == ref["status"][0] == 0
+    assert_parity_general(got, ref, case["name"])
+    for e in case["expect_flux"]:
+        assert abs(got[e["field"]][0, e["index"]] - e["value"]) <= e["tol"]
+
+
+@pytest.mark.parametrize("nstr", [(4, 8), (16,), (6, 10, 12, 14), (32,), (64,)])
+def test_general_spherical_beam(nstr):
+    """Spherical-shell instances at every stream count, with all azimuth modes
+    (each mode has its own spherical particular solution), then bottom-up
+    indexing and a thermal source with them.  At 32 and 64 streams the N x N
+    LU of I + xba M - C (xba = 1 / Chapman factor, often within a few percent of
+    a 1 / mu_i) carries rounding of ~2e-8 relative: there the checker is the
+    extended-precision oracle build, at 5e-8."""
+    big = max(nstr) >= 32
+    rtol = 5e-8 if big else 1e-9
+    n = 2 if 64 in nstr else 12
+    for kw in (dict(), dict(bottom_up=True), dict(thermal=True)):
+        insts, flags = spherical_mix(n, seed=600 + sum(nstr), nstr=nstr, layers=(3, 5) if 64 in nstr else (3, 16),
+                                     **kw)
+        got, ref, _ = both(insts, flags, ext=big)
+        assert np.all(got["status"] == 0) and np.all(ref["status"] == 0), (got["status"], ref["status"])
+        assert_parity_general(got, ref, f"spherical N={nstr} {kw}", rtol=rtol)
+
+
+def test_general_spherical_invalid_radius_and_missing_altitudes():
+    insts, flags = spherical_mix(4, seed=7, nstr=(8,))
+    insts[1]["bottom_radius"] = -1.0
+    insts[3]["bottom_radius"] = 0.0
+    got, ref, _ = both(insts, flags)
+    assert list(got["status"]) == [0, capi.DSP_ERR_INVALID_INPUT, 0, capi.DSP_ERR_INVALID_INPUT]
+    assert np.all(got["status"] == ref["status"])
+    ok = [0, 2]
+    assert_parity_general({k: v[ok] for k, v in got.items() if k != "status"},
+                          {k: v[ok] for k, v in ref.items() if k != "status"}, "valid rows")
+    d = capi.pack_general(insts, flags)
+    batch, keep = capi.make_general_batch(d)
+    batch.level_altitudes = None
+    outs, o, keep2 = capi.alloc_general_out_numpy(d)
+    assert gpu_lib.context().general_bands_solve(batch, o) == capi.DSP_ERR_INVALID_INPUT
+
+
+def test_general_spherical_device_pointers_match_host():
+    insts, flags = spherical_mix(6, seed=11, nstr=(4, 16))
+    d = capi.pack_general(insts, flags)
+    host, rc = gpu_lib.general_solve(d)
+    dev, rc2 = gpu_lib.general_solve_device(d)
+    assert rc == 0 and rc2 == 0, gpu_lib.context().last_error()
+    for f in capi.FLUX_OUT_FIELDS + ("intensity", "intensity_azimuth_avg", "status"):
+        np.testing.assert_array_equal(host[f], dev[f], err_msg=f)

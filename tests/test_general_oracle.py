@@ -150,3 +150,42 @@ def test_general_validation(mutate):
         d = capi.pack_general([inst], flags)
     o = oracle_lib.general_solve(d)
     assert o["status"][0] == capi.DSP_ERR_INVALID_INPUT
+
+
+# ---------------------------------------------------------------------------
+# pseudo-spherical beam of the general solver
+# ---------------------------------------------------------------------------
+def test_general_spherical_golden():
+    """SphericalGeometry (tests/test_solver.cpp:4459-4533): the C-DISORT
+    fluxes of the general solver with the Chapman correction, 1e-3."""
+    case = gc.load_spherical_cases()[0]
+    inst, flags = gc.general_instance(case)
+    inst.update(level_altitudes=case["level_altitudes"], bottom_radius=case["bottom_radius"])
+    o = oracle_lib.general_solve(capi.pack_general([inst], flags | capi.FLAG_SPHERICAL_BEAM))
+    assert o["status"][0] == 0
+    for e in case["expect_flux"]:
+        v = o[e["field"]][0, e["index"]]
+        assert abs(v - e["value"]) <= e["tol"], (e, v)
+
+
+@pytest.mark.parametrize("nstr", [4, 16])
+def test_general_spherical_equals_flux_spherical(nstr):
+    """SphericalBeam4/16 (test_flux_solver.cpp:309-358): the flux solver and
+    the general solver agree to 1e-12 on a spherical-shell column."""
+    from disort_b200 import workloads
+    L = 5
+    zalt = [100.0, 80.0, 60.0, 40.0, 20.0, 0.0]
+    pm = workloads.hg_moments(np.zeros(L), nstr + 1)
+    inst = dict(num_streams=nstr, num_layers=L, num_phase_func_moments=0, delta_tau=np.full(L, 0.1),
+                single_scat_albedo=np.full(L, 0.9), phase_function_moments=pm, surface_albedo=0.1,
+                direct_beam_flux=1.0, direct_beam_mu=0.3, level_altitudes=zalt, bottom_radius=6371.0)
+    o = oracle_lib.general_solve(capi.pack_general([inst], capi.FLAG_SPHERICAL_BEAM | capi.GFLAG_ONLY_FLUXES))
+    w = dict(n_inst=1, num_streams=nstr, num_layers=L, num_phase_func_moments=0, pmom_count=nstr + 1,
+             flags=capi.FLAG_SPHERICAL_BEAM,
+             arrays=dict(delta_tau=np.full(L, 0.1), single_scat_albedo=np.full(L, 0.9), phase_function_moments=pm,
+                         surface_albedo=0.1, direct_beam_flux=1.0, direct_beam_mu=0.3,
+                         level_altitudes=np.array(zalt), bottom_radius=6371.0))
+    f, st = oracle_lib.flux_solve(w)
+    assert o["status"][0] == 0 and st[0] == 0
+    for k in capi.FLUX_OUT_FIELDS:
+        np.testing.assert_allclose(o[k][0, :L + 1], f[k][0], rtol=1e-12, atol=1e-14, err_msg=k)
