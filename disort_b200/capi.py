@@ -42,6 +42,8 @@ FLAG_SPHERICAL_BEAM = 1 << 5
 FLAG_TEMPERATURE_JAC = 1 << 6
 FLAG_HG_G = 1 << 7
 
+DEBUG_POISON_SCRATCH = 1  # dsp_context_set_debug
+
 GFLAG_USER_TAU = 1 << 8
 GFLAG_USER_MU = 1 << 9
 GFLAG_ONLY_FLUXES = 1 << 10
@@ -378,6 +380,8 @@ def load_library(path: str | None = None):
     lib.dsp_context_last_error.argtypes = [c_void_p]
     lib.dsp_flux_workspace_bytes.restype = c_int64
     lib.dsp_flux_workspace_bytes.argtypes = [POINTER(FluxBatch)]
+    lib.dsp_context_set_debug.restype = c_int32
+    lib.dsp_context_set_debug.argtypes = [c_void_p, c_uint32]
     lib.dsp_context_set_timing.restype = c_int32
     lib.dsp_context_set_timing.argtypes = [c_void_p, c_int32]
     lib.dsp_context_timing_reset.restype = c_int32
@@ -434,6 +438,10 @@ class Context:
 
     def general_bands_solve_jac(self, batch: GeneralBatch, out: GeneralOut, jac: GeneralJacOut) -> int:
         return self.lib.dsp_general_bands_solve_jac(self.h, ctypes.byref(batch), ctypes.byref(out), ctypes.byref(jac))
+
+    def set_debug(self, flags: int) -> int:
+        """DSP_DEBUG_* flags (DEBUG_POISON_SCRATCH: NaN-filled workspace before each chunk)."""
+        return int(self.lib.dsp_context_set_debug(self.h, flags))
 
     def set_timing(self, enable: bool):
         self.lib.dsp_context_set_timing(self.h, 1 if enable else 0)

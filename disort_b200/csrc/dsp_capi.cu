@@ -254,6 +254,13 @@ dsp_status dsp_context_set_timing(dsp_context ctx, int32_t enable) {
   return DSP_OK;
 }
 
+dsp_status dsp_context_set_debug(dsp_context ctx, uint32_t flags) {
+  if (!ctx) return DSP_ERR_NOT_INITIALIZED;
+  if (flags & ~DSP_DEBUG_POISON_SCRATCH) return fail(ctx, DSP_ERR_INVALID_INPUT, "unknown debug flag");
+  ctx->debug = flags;
+  return DSP_OK;
+}
+
 dsp_status dsp_context_timing_reset(dsp_context ctx) {
   if (!ctx) return DSP_ERR_NOT_INITIALIZED;
   drain_timing(ctx);
@@ -289,6 +296,7 @@ int64_t dsp_flux_workspace_bytes(const dsp_flux_batch* b) {
 
 dsp_status dsp_flux_bands_solve(dsp_context ctx, const dsp_flux_batch* batch_in, const dsp_flux_out* out) {
   if (!ctx) return DSP_ERR_NOT_INITIALIZED;
+  NvtxRange r("dsp_flux_bands_solve");
   if (batch_in && (batch_in->flags & DSP_FLAG_TEMPERATURE_JAC))
     return fail(ctx, DSP_ERR_UNSUPPORTED, "temperature Jacobians are computed by dsp_flux_bands_solve_jac");
   return flux_solve(ctx, batch_in, out, nullptr);
@@ -297,6 +305,7 @@ dsp_status dsp_flux_bands_solve(dsp_context ctx, const dsp_flux_batch* batch_in,
 dsp_status dsp_flux_bands_solve_jac(dsp_context ctx, const dsp_flux_batch* batch_in, const dsp_flux_out* out,
                                     const dsp_flux_jac_out* jac) {
   if (!ctx) return DSP_ERR_NOT_INITIALIZED;
+  NvtxRange r("dsp_flux_bands_solve_jac");
   if (!jac || !jac->flux_up || !jac->flux_down || !jac->mean_intensity || !jac->mean_intensity_down ||
       !jac->mean_intensity_up || !jac->flux_divergence)
     return fail(ctx, DSP_ERR_INVALID_INPUT, "every Jacobian output array is required");
@@ -467,6 +476,10 @@ dsp_status flux_solve(dsp_context ctx, const dsp_flux_batch* batch_in, const dsp
     for (int64_t off = r0; off < r1; off += ch) {
       const int64_t m = (r1 - off < ch) ? (r1 - off) : ch;
       p.n = (int)m;
+      if (ctx->debug & DSP_DEBUG_POISON_SCRATCH) {
+        const cudaError_t pe = cudaMemsetAsync(wsb, 0xFF, (size_t)m * inst_doubles * sizeof(double), cs);
+        if (pe != cudaSuccess) return cuda_fail(ctx, pe, "scratch poison");
+      }
       for (int k = 0; k < kFluxArrays; ++k) {
         pa[k]->p = arr[k].ptr ? arr[k].ptr + arr[k].stride * off : nullptr;
         pa[k]->s = arr[k].stride;

@@ -229,6 +229,7 @@ dsp_status general_solve(dsp_context ctx, const dsp_general_batch* bin, const ds
 extern "C" dsp_status dsp_general_bands_solve(dsp_context ctx, const dsp_general_batch* bin,
                                               const dsp_general_out* out) {
   if (!ctx) return DSP_ERR_NOT_INITIALIZED;
+  NvtxRange r("dsp_general_bands_solve");
   if (bin && (bin->flags & DSP_FLAG_TEMPERATURE_JAC))
     return fail(ctx, DSP_ERR_UNSUPPORTED, "temperature Jacobians are computed by dsp_general_bands_solve_jac");
   return general_solve(ctx, bin, out, nullptr);
@@ -237,6 +238,7 @@ extern "C" dsp_status dsp_general_bands_solve(dsp_context ctx, const dsp_general
 extern "C" dsp_status dsp_general_bands_solve_jac(dsp_context ctx, const dsp_general_batch* bin,
                                                   const dsp_general_out* out, const dsp_general_jac_out* jac) {
   if (!ctx) return DSP_ERR_NOT_INITIALIZED;
+  NvtxRange r("dsp_general_bands_solve_jac");
   if (!jac || !jac->flux_up || !jac->flux_down || !jac->mean_intensity || !jac->mean_intensity_down ||
       !jac->mean_intensity_up || !jac->flux_divergence)
     return fail(ctx, DSP_ERR_INVALID_INPUT, "every Jacobian output array is required");
@@ -660,6 +662,13 @@ dsp_status general_solve(dsp_context ctx, const dsp_general_batch* bin, const ds
       }
       const double* tabs = nullptr;
       if ((st = get_mode_tables(ctx, c.N, &tabs)) != DSP_OK) return st;
+      if (ctx->debug & DSP_DEBUG_POISON_SCRATCH) {
+        const size_t wb = (size_t)(c.inst_doubles + c.layers * (g.lstride + brec_stride(c.N) + c.N +
+                                                                 sph_per_layer(c.N) + jac_per_layer(c.N))) *
+                          sizeof(double);
+        e = cudaMemsetAsync(ctx->ws, 0xFF, wb, s);
+        if (e != cudaSuccess) return cuda_fail(ctx, e, "scratch poison");
+      }
       if ((st = launch_general(ctx, c.N, p, c.layers, c.maxm, tabs, jac ? &jv : nullptr)) != DSP_OK) return st;
     }
   }

@@ -4,6 +4,7 @@
 #pragma once
 
 #include <cuda_runtime.h>
+#include <nvtx3/nvToolsExt.h>
 
 #include <cfloat>
 #include <cmath>
@@ -43,6 +44,7 @@ struct dsp_context_s {
   std::vector<cudaEvent_t> pipe_ev;
   // optional per-kernel timing
   bool timing = false;
+  uint32_t debug = 0;  // DSP_DEBUG_* flags
   struct Pending {
     int kernel;
     cudaEvent_t a, b;
@@ -76,12 +78,24 @@ inline int kernel_id(dsp_context c, const char* name) {
 }
 
 // Brackets one launch with events when timing is on.
+// An NVTX range over a host scope (an entry-point call, a chunk, a launch):
+// header-only NVTX v3, a no-op unless a profiler's injection library is loaded.
+struct NvtxRange {
+  explicit NvtxRange(const char* name) { nvtxRangePushA(name); }
+  ~NvtxRange() { nvtxRangePop(); }
+  NvtxRange(const NvtxRange&) = delete;
+  NvtxRange& operator=(const NvtxRange&) = delete;
+};
+
+// One launch: its NVTX range, and with timing on a pair of CUDA events around it.
 struct KernelTimer {
   dsp_context c;
   cudaStream_t s;
   int id = -1;
   cudaEvent_t a = nullptr, b = nullptr;
-  KernelTimer(dsp_context ctx, const char* name, cudaStream_t st = nullptr) : c(ctx), s(st ? st : ctx->stream) {
+  NvtxRange range;
+  KernelTimer(dsp_context ctx, const char* name, cudaStream_t st = nullptr)
+      : c(ctx), s(st ? st : ctx->stream), range(name) {
     if (!c->timing) return;
     id = kernel_id(c, name);
     a = take_event(c);

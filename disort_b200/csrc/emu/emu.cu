@@ -791,6 +791,26 @@ dsp_status dsp_emu_gemm_bf16(dsp_emu e, const uint16_t* A, const uint16_t* B, fl
   return read_err_flag(e);
 }
 
+dsp_status dsp_emu_wait_selftest(dsp_emu e, int64_t cycles) {
+  if (!e) return DSP_ERR_NOT_INITIALIZED;
+  if (cycles <= 0 || cycles > (1ll << 31)) return efail(e, DSP_ERR_INVALID_INPUT, "cycles out of (0, 2^31]");
+  cudaSetDevice(e->device);
+  int h = 0;
+  cudaError_t ce = cudaMemcpyAsync(&h, e->err_d, sizeof(int), cudaMemcpyDeviceToHost, e->stream);
+  if (ce == cudaSuccess) ce = cudaStreamSynchronize(e->stream);
+  if (ce != cudaSuccess) return check_err(e, ce, "wait self-test");
+  if (h) return efail(e, DSP_ERR_TIMEOUT, "the error flag was already set");
+  dsp_tc::wait_selftest_kernel<<<1, 32, 0, e->stream>>>(e->err_d, (long long)cycles);
+  ce = cudaGetLastError();
+  if (ce != cudaSuccess) return check_err(e, ce, "wait self-test launch");
+  const dsp_status st = read_err_flag(e);
+  // the self-test's own timeout leaves the emulator usable: clear the flag it set
+  ce = cudaMemsetAsync(e->err_d, 0, sizeof(int), e->stream);
+  if (ce == cudaSuccess) ce = cudaStreamSynchronize(e->stream);
+  if (ce != cudaSuccess) return check_err(e, ce, "wait self-test");
+  return st;
+}
+
 dsp_status dsp_emu_gate(dsp_emu e, const float* raw, int32_t raw_stride, const float* lo, const float* hi,
                         const float* preds, const float* mu, const float* sd, const float* scale, const float* add,
                         float eps, float rel_tol, float floor_frac, int64_t rows, float* flux, int32_t* fallback,

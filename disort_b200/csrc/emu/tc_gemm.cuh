@@ -51,15 +51,32 @@ __device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, uint32_t parity) {
   return ok != 0;
 }
 
-// Bounded wait: false when the phase did not complete within ~2^31 cycles or
-// another role of the CTA has aborted.
-__device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity, volatile int* abort_flag) {
+// Bounded wait: false when the phase did not complete within `limit` cycles
+// (~2^31 by default, about a second) or another role of the CTA has aborted.
+__device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity, volatile int* abort_flag,
+                                          long long limit = (1ll << 31)) {
   const long long t0 = clock64();
   while (!mbar_try_wait(bar, parity)) {
     if (*abort_flag) return false;
-    if (clock64() - t0 > (1ll << 31)) return false;
+    if (clock64() - t0 > limit) return false;
   }
   return true;
+}
+
+// Self-test of the bounded wait: one mbarrier that nothing arrives on (no copy
+// or MMA is issued against it), waited on by every thread with a short limit.
+// The wait runs out and the CTA reports it through the error flag the GEMMs use.
+static __global__ void __launch_bounds__(32) wait_selftest_kernel(int* err, long long limit) {
+  __shared__ __align__(8) uint64_t bar;
+  __shared__ int abort_flag;
+  if (threadIdx.x == 0) {
+    mbar_init(&bar, 1);
+    abort_flag = 0;
+    fence_mbar_init();
+  }
+  __syncthreads();
+  const bool ok = __all_sync(0xffffffffu, mbar_wait(&bar, 0, &abort_flag, limit) ? 1 : 0) != 0;
+  if (threadIdx.x == 0 && !ok) atomicExch(err, 1);
 }
 
 __device__ __forceinline__ void tma_load_2d(void* dst, const CUtensorMap* map, uint64_t* bar, int x, int y) {

@@ -57,6 +57,8 @@ def load_library():
     lib.dsp_emu_set_params.argtypes = [c_void_p, c_void_p]
     lib.dsp_emu_gemm_bf16.restype = c_int32
     lib.dsp_emu_gemm_bf16.argtypes = [c_void_p, c_void_p, c_void_p, c_void_p, c_int32, c_int32, c_int32]
+    lib.dsp_emu_wait_selftest.restype = c_int32
+    lib.dsp_emu_wait_selftest.argtypes = [c_void_p, c_int64]
     lib.dsp_emu_gate.restype = c_int32
     lib.dsp_emu_gate.argtypes = [c_void_p, c_void_p, c_int32, c_void_p, c_void_p, c_void_p, c_void_p, c_void_p,
                                  c_void_p, c_void_p, c_float, c_float, c_float, c_int64, c_void_p, c_void_p,
@@ -128,6 +130,10 @@ class Emulator:
     def gemm(self, A, B, C):
         self._check(self.lib.dsp_emu_gemm_bf16(self.h, _p(A), _p(B), _p(C), A.shape[0], B.shape[0], A.shape[1]),
                     "dsp_emu_gemm_bf16")
+
+    def wait_selftest(self, cycles: int) -> int:
+        """Status of the bounded-wait self-test (DSP_ERR_TIMEOUT when the wait ran out)."""
+        return int(self.lib.dsp_emu_wait_selftest(self.h, cycles))
 
     def gate(self, raw, lo, hi, preds, mu, sd, scale, add, eps, rel_tol, floor_frac, flux, fallback, idx, count):
         self._check(self.lib.dsp_emu_gate(self.h, _p(raw), raw.shape[1], _p(lo), _p(hi), _p(preds), _p(mu), _p(sd),

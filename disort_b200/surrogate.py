@@ -395,3 +395,89 @@ def evaluate(ctx: capi.Context, sur: Surrogate, columns: int = 4096, seed: int =
     torch.cuda.synchronize()
     res["four_stream_solves_per_s"] = n / (a.elapsed_time(b) / 1000.0)
     return res
+
+
+# ---------------------------------------------------------------------------
+# save / load: a JSON header and one little-endian binary blob
+# ---------------------------------------------------------------------------
+SAVE_FORMAT = "disort_b200.surrogate"
+SAVE_VERSION = 1
+_VECTORS = ("fmean", "fstd", "lo", "hi", "mu", "sd")
+
+
+def write_blob(path: str, header: dict, blocks: list) -> None:
+    """`path`.json holds `header` plus the list of blocks (name, dtype, shape,
+    byte offset); `path`.bin holds the blocks back to back, little-endian."""
+    import json
+    meta, off = [], 0
+    with open(path + ".bin", "wb") as f:
+        for name, a in blocks:
+            a = np.ascontiguousarray(a)
+            a = a.astype(a.dtype.newbyteorder("<"), copy=False)
+            f.write(a.tobytes())
+            meta.append(dict(name=name, dtype=a.dtype.str, shape=list(a.shape), offset=off, nbytes=a.nbytes))
+            off += a.nbytes
+    h = dict(header)
+    h["blocks"] = meta
+    h["blob_bytes"] = off
+    with open(path + ".json", "w") as f:
+        json.dump(h, f, indent=1)
+
+
+def read_blob(path: str, fmt: str, version: int) -> tuple[dict, dict]:
+    """Header and {name: array} of a write_blob pair; ValueError when the format,
+    version or blob size does not match."""
+    import json
+    with open(path + ".json") as f:
+        h = json.load(f)
+    if h.get("format") != fmt or h.get("version") != version:
+        raise ValueError(f"{path}.json: format {h.get('format')!r} version {h.get('version')!r}, "
+                         f"expected {fmt!r} version {version}")
+    with open(path + ".bin", "rb") as f:
+        raw = f.read()
+    if len(raw) != h["blob_bytes"]:
+        raise ValueError(f"{path}.bin: {len(raw)} bytes, header says {h['blob_bytes']}")
+    out = {}
+    for b in h["blocks"]:
+        a = np.frombuffer(raw, dtype=np.dtype(b["dtype"]), count=int(np.prod(b["shape"], dtype=np.int64)),
+                          offset=b["offset"])
+        out[b["name"]] = a.reshape(b["shape"]).copy()
+    return h, out
+
+
+def save(sur: Surrogate, path: str) -> None:
+    """The trained emulator's FP32 master weights, its configuration and the
+    normalisation and envelope vectors, to `path`.json + `path`.bin."""
+    e = sur.emu
+    params = np.empty(e.param_count(), dtype=np.float32)
+    e.get_params(params)
+    c = e.cfg
+    header = dict(format=SAVE_FORMAT, version=SAVE_VERSION,
+                  emulator=dict(n_in=c.n_in, hidden=c.hidden, n_hidden_layers=c.n_hidden_layers, n_out=c.n_out,
+                                n_heads=c.n_heads, batch=c.batch, seed=c.seed),
+                  layer_dims=[list(d) for d in e.layer_dims()],
+                  instances=dict(layers=L, streams=N, low_streams=N_LOW, features=N_IN, outputs=N_OUT,
+                                 bands=NBANDS, floor_frac=FLOOR_FRAC, gate_tol=GATE_TOL, eps=EPS))
+    blocks = [("params", params)] + [(k, getattr(sur, k).detach().cpu().numpy()) for k in _VECTORS]
+    write_blob(path, header, blocks)
+
+
+def load(path: str, device: int = 0, stream: int = 0) -> Surrogate:
+    """A Surrogate from a save() pair: a new emulator with the stored weights."""
+    import torch
+    from .emu import Emulator
+    h, b = read_blob(path, SAVE_FORMAT, SAVE_VERSION)
+    inst = h["instances"]
+    if (inst["layers"], inst["streams"], inst["low_streams"], inst["features"], inst["outputs"]) != \
+            (L, N, N_LOW, N_IN, N_OUT):
+        raise ValueError(f"{path}.json: saved for a different instance layout ({inst})")
+    c = h["emulator"]
+    emu = Emulator(n_in=c["n_in"], hidden=c["hidden"], n_hidden_layers=c["n_hidden_layers"], n_out=c["n_out"],
+                   n_heads=c["n_heads"], batch=c["batch"], seed=c["seed"], device=device, stream=stream)
+    if emu.param_count() != b["params"].size or [list(d) for d in emu.layer_dims()] != h["layer_dims"]:
+        emu.close()
+        raise ValueError(f"{path}: parameter layout does not match the emulator's")
+    emu.set_params(np.ascontiguousarray(b["params"], dtype=np.float32))
+    dev = torch.device("cuda", device)
+    vec = {k: torch.from_numpy(b[k]).to(dev) for k in _VECTORS}
+    return Surrogate(emu, vec["fmean"], vec["fstd"], vec["lo"], vec["hi"], vec["mu"], vec["sd"])

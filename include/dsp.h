@@ -236,6 +236,15 @@ int32_t dsp_context_timing_count(dsp_context ctx);
 dsp_status dsp_context_timing_get(dsp_context ctx, int32_t idx, const char** name, double* total_ms,
                                   int64_t* launches);
 
+/*
+ * Debug options of a context (no reference counterpart).  With
+ * DSP_DEBUG_POISON_SCRATCH every chunk's workspace is filled with NaN (all bits
+ * set) before its kernels run, so that a kernel reading scratch it did not
+ * write shows up as NaN outputs.  Costs one memset of the workspace per chunk.
+ */
+#define DSP_DEBUG_POISON_SCRATCH 1u
+dsp_status dsp_context_set_debug(dsp_context ctx, uint32_t flags);
+
 /* Flux-only spectral-band solve (DisortFluxSolver<N> over every instance). */
 dsp_status dsp_flux_bands_solve(dsp_context ctx, const dsp_flux_batch* batch,
                                 const dsp_flux_out* out);

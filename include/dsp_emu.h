@@ -75,6 +75,13 @@ dsp_status dsp_emu_set_params(dsp_emu emu, const float* host);
 dsp_status dsp_emu_gemm_bf16(dsp_emu emu, const uint16_t* A, const uint16_t* B, float* C, int32_t M, int32_t N,
                              int32_t K);
 
+/* Self-test of the device-side bounded waits: a kernel waits `cycles` clock
+ * cycles (at most 2^31) on an mbarrier that nothing arrives on, with no copy or
+ * MMA in flight, gives up and sets the error flag the GEMMs use; the call
+ * returns DSP_ERR_TIMEOUT read from that flag, then clears the flag so that the
+ * emulator stays usable. */
+dsp_status dsp_emu_wait_selftest(dsp_emu emu, int64_t cycles);
+
 /* Gate: a row falls back to the FP64 solver when any raw feature lies outside
  * [lo, hi] (per feature, n_in values each) or when its heads disagree on the
  * reconstructed fluxes F_h,k = scale_r * (exp(pred_h,k * sd_k + mu_k) - eps) + add_r,k

@@ -7,6 +7,7 @@
    gradients are re-rounded on both sides; the rest is accumulation order).
 3. The training loop (fused loss gradient, tensor-core backward, fused Adam,
    cosine schedule) tracks a plain PyTorch FP32 run from the same initial weights.
+4. A bounded device wait that runs out returns DSP_ERR_TIMEOUT to the host.
 """
 import os
 import sys
@@ -47,6 +48,17 @@ def test_tc_gemm_matches_fp64(emu_small, M, N, K):
     got = C.cpu().numpy().astype(np.float64)
     err = np.abs(got - ref).max() / np.abs(ref).max()
     assert err < 1e-5, err
+
+
+def test_bounded_wait_times_out_and_the_emulator_stays_usable(emu_small):
+    """A device wait on an mbarrier that nothing arrives on (no copy or MMA in
+    flight) gives up after its cycle limit; the host reads DSP_ERR_TIMEOUT from
+    the GEMMs' error flag, and the context and the emulator keep working."""
+    from disort_b200 import capi
+    assert emu_small.wait_selftest(1 << 20) == capi.DSP_ERR_TIMEOUT
+    assert "ran out" in emu_small.last_error()
+    assert emu_small.wait_selftest(0) == capi.DSP_ERR_INVALID_INPUT
+    test_tc_gemm_matches_fp64(emu_small, 128, 64, 64)
 
 
 def make_data(rng, n, n_in, in_pad, n_out, n_heads):

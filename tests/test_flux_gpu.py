@@ -337,3 +337,49 @@ def test_spherical_beam_invalid_radius_and_missing_altitudes():
     w["arrays"]["level_altitudes"] = None
     _, _, rc = gpu_lib.flux_solve(w)
     assert rc == capi.DSP_ERR_INVALID_INPUT
+
+
+def test_poisoned_scratch_gives_the_same_results():
+    """With the workspace filled with NaN before each chunk (DSP_DEBUG_POISON_SCRATCH)
+    every output is bit-identical to the unpoisoned run: no kernel reads scratch
+    it did not write (thermal sweep, spherical columns at 32 streams, temperature
+    Jacobians, a spherical thermal general mix with intensities and Jacobians)."""
+    ctx = gpu_lib.context()
+    from test_general_gpu import spherical_mix
+    runs = []
+    w1 = workloads.subset(workloads.thermal_sweep(), np.arange(0, 20000, 200))
+    runs.append(lambda: gpu_lib.flux_solve(w1))
+    w2 = spherical_columns(32, 10, 4, seed=9)
+    runs.append(lambda: gpu_lib.flux_solve(w2))
+    w3 = spherical_columns(16, 20, 6, seed=5, thermal=True)
+    runs.append(lambda: gpu_lib.flux_solve_jac(w3))
+    insts, flags = spherical_mix(8, seed=3, nstr=(4, 16, 32), thermal=True)
+    d = capi.pack_general(insts, flags)
+    runs.append(lambda: gpu_lib.general_solve(d)[0])
+
+    def gen_jac():
+        batch, keep = capi.make_general_batch(d)
+        outs, o, keep2 = capi.alloc_general_out_numpy(d)
+        jac, jo, keep3 = capi.alloc_general_jac_numpy(d)
+        assert ctx.general_bands_solve_jac(batch, o, jo) == 0
+        return outs, jac
+    runs.append(gen_jac)
+
+    def flat(r):
+        if isinstance(r, dict):
+            return [np.asarray(r[k]) for k in sorted(r)]
+        if isinstance(r, (tuple, list)):
+            return [a for x in r for a in flat(x)]
+        return [np.asarray(r)]
+    try:
+        for k, run in enumerate(runs):
+            assert ctx.set_debug(0) == 0
+            a = flat(run())
+            assert ctx.set_debug(capi.DEBUG_POISON_SCRATCH) == 0
+            b = flat(run())
+            assert len(a) == len(b)
+            for x, y in zip(a, b):
+                np.testing.assert_array_equal(x, y, err_msg=f"run {k}")
+    finally:
+        ctx.set_debug(0)
+    assert ctx.set_debug(2) == capi.DSP_ERR_INVALID_INPUT

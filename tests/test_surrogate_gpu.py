@@ -75,3 +75,22 @@ def test_gate_bounds_error_and_catches_out_of_envelope(trained):
     print(f"envelope-only gate: fallback {ko / n:.3f}, in-envelope p50/p99 rel err {float(eo.median()):.3g}/"
           f"{float(torch.quantile(eo.float(), 0.99)):.3g}")
     assert float(eo.median()) < 2e-2
+
+
+def test_save_and_load_give_the_same_predictions(trained, tmp_path):
+    import torch
+    from disort_b200 import surrogate as s
+    ctx, sur, rep = trained
+    p = str(tmp_path / "emulator")
+    s.save(sur, p)
+    sur2 = s.load(p)
+    try:
+        d = s.sample(512, 33)
+        arrays = s.device_inputs(d)
+        raw, pa, *_ = s.emulate(ctx, sur, arrays, 512)
+        raw2, pb, *_ = s.emulate(ctx, sur2, arrays, 512)
+        assert torch.equal(raw, raw2) and torch.equal(pa, pb)
+        for k in ("fmean", "fstd", "lo", "hi", "mu", "sd"):
+            assert torch.equal(getattr(sur, k), getattr(sur2, k))
+    finally:
+        sur2.emu.close()
