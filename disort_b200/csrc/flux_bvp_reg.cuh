@@ -4,14 +4,20 @@
 // Same algorithm as flux_bvp_tile.cuh (the staircase form of the LINPACK band LU,
 // setMatrix/solve0/computeFluxes of FluxSolver.cpp:838-1287), mapped so that
 // the sgbfa row operations are register FMAs:
-//  - slot thread s holds its row as cur[N] (columns of x_l), nxt[N] (columns of
-//    x_{l+1}) and rhs; carried rows move nxt -> cur between layers;
+//  - slot thread s holds its row's x_l columns as cur[N]; the row's x_{l+1}
+//    columns and right-hand side go to shared memory once the layer's new rows
+//    are in the panel, and carried rows take theirs back as cur between layers;
 //  - the pivot of column c is an arg-max of |cur[c]| over candidate slots
 //    (warp reductions of the bit patterns for a full-warp team, shuffles
 //    otherwise); only the pivot row and its negated reciprocal are broadcast
 //    through shared memory;
 //  - free slots (last layer's pivot rows) receive the new continuity rows in
 //    slot order, each thread finding its row index by a popcount;
+//  - a pivot step updates the x_l columns only (the multipliers replace the
+//    pivot column's entries); the x_{l+1} columns and the right-hand side of
+//    the panel follow after the layer's N steps, one lane per column: a unit
+//    lower-triangular solve for the pivot rows, then the carried rows, each
+//    element with the same FMA sequence as inside the steps;
 //  - the N pivot rows of a layer, [U | V | c] with U x_l + V x_{l+1} = c, go
 //    to the layer's elimination record as they are; going back up, x_l is the
 //    solution of U x_l = c - V x_{l+1}, a 16-step triangular solve across the
@@ -41,8 +47,9 @@ struct RCfg {
   static constexpr int CTA = TEAM >= 32 ? TEAM : 32;
   static constexpr int TPC = CTA / TEAM;
   // team shared memory (doubles)
-  static constexpr int O_BUF = 0;                  // 2 x pivot row: cur[N] nxt[N] rhs, -1/pivot
-  static constexpr int O_XV = O_BUF + 2 * (2 * N + 2);  // x ping-pong [2][N]
+  static constexpr int BL = N + 2;                 // pivot-step buffer: cur[c+1..N-1] | rhs | -1/pivot
+  static constexpr int O_BUF = 0;                  // 2 x pivot-step buffer
+  static constexpr int O_XV = O_BUF + 2 * BL;      // x ping-pong [2][N]
   static constexpr int O_EC = O_XV + 2 * N;    // [N]
   static constexpr int O_I = O_EC + N;         // intensities [N]
   static constexpr int O_E = O_I + N;          // exp(eig*dtau) of layers l, l+1 [2][NN]
@@ -61,13 +68,24 @@ struct RCfg {
   static constexpr int RSP = round4(SXR + 2);
   static_assert(RS - N * N == round4(N * N + 4 * N + 2) - N * N, "layer record: G then eig, zb, z0, z1, xr");
   static constexpr int O_RING = round4(O_PIV + N / 2 + 1);
-  // going down: 3 layer records; going up: 2 layer records and 1 elimination record
-  static constexpr int RING = imax(3 * RSP, 2 * RSP + BS);
+  // Going down: 3 layer records, then the panel rows' right-hand blocks
+  // [x_{l+1} columns | rhs] by slot (PR rows of R0S doubles, odd so that a lane
+  // per row writing one column spreads over the banks); the multipliers of the
+  // layer's pivot steps go to the free slot of the layer's own record (packed:
+  // pivot row k's k multipliers at k(k-1)/2, carried row r's N at N(N-1)/2 + rN).
+  // Going up: 2 layer records and 1 elimination record.
+  static constexpr int R0S = N + 1;
+  static constexpr int O_R0 = 3 * RSP;
+  static constexpr int ML_CARRIED = N * (N - 1) / 2;
+  static_assert(ML_CARRIED + (PR - N) * N <= RSP, "multipliers fit a layer record's ring slot");
+  static constexpr int RING = imax(3 * RSP + PR * R0S, 2 * RSP + BS);
   static constexpr int TEAM_SMEM = round4(O_RING + RING);
   static constexpr int TAB = 2 * N;  // mu and wt of the constant tables
   // register budget per thread: 128 keeps 16 single-warp CTAs resident per SM
   static constexpr int MINB = 65536 / (CTA * DSP_BVP_REGS);
   static constexpr size_t smem_bytes() { return sizeof(double) * (size_t)(TAB + TPC * TEAM_SMEM); }
+  // 16 resident CTAs (one per warp of the register budget) fit 228 KB with 1 KB reserved each
+  static_assert(N != 16 || 16 * (smem_bytes() + 1024) <= 228 * 1024, "16 CTAs per SM at 16 streams");
 };
 
 template <int N, bool GEN = false, bool JAC = false, bool SPH = false>
@@ -320,10 +338,25 @@ __global__ void __launch_bounds__(RCfg<N>::CTA, RCfg<N>::MINB) flux_bvp_reg_kern
     const unsigned newm = (__ballot_sync(msk, fresh) >> (threadIdx.x & 31u & ~(unsigned)(TEAM - 1))) &
                           (TEAM == 32 ? 0xffffffffu : ((1u << TEAM) - 1u));
     unsigned cand = carried | newm;
+    // the panel rows' right-hand blocks [x_{l+1} columns | rhs] wait in shared
+    // memory for the column phase (carried rows have no x_{l+1} entries)
+    double* R0 = ring + C::O_R0;
+    if (!last && t < PR) {
+#pragma unroll
+      for (int j = 0; j < N; ++j) R0[t * C::R0S + j] = fresh ? nxt[j] : 0.0;
+      R0[t * C::R0S + N] = rhs;
+    }
     DSP_PHASE(20)
 
     // ---- eliminate the N columns of x_l (sgbfa steps) ----------------------
+    // Each pivot step updates the x_l columns only; the multiplier of every
+    // candidate row replaces its entry in the pivot column (LINPACK keeps L
+    // there too).  The x_{l+1} columns and the right-hand side are brought up to
+    // date afterwards, column by column (below), with the same FMA sequence per
+    // element as the row operations of the steps; the last layer, with no
+    // x_{l+1} columns, updates its right-hand side within the steps.
     int myc = -1;  // pivot column of this thread's row, if it becomes a pivot row
+    unsigned sing = 0u;  // columns whose pivot is zero: no elimination step
     // temperature Jacobian: this layer's multipliers and pivot slots
     double* const jrow = !JAC ? nullptr
         : p.jac_rec + ((GEN ? (long long)p.g.lay_off[slot] : (long long)i * L) + l) * jrec_stride(N);
@@ -349,38 +382,34 @@ __global__ void __launch_bounds__(RCfg<N>::CTA, RCfg<N>::MINB) flux_bvp_reg_kern
       if (t == 0) pivslot[c] = ps;
       if (idx >= PR || zero_piv) {  // LINPACK skips a zero pivot column (BandSolver.hpp:76-78)
         singular = true;
+        sing |= 1u << c;
         if constexpr (JAC) {
           if (t < PR) jrow[c * PR + t] = 0.0;
           if (t == 0) jrow[N * PR + c] = (double)ps;
         }
         continue;
       }
-      double* buf = bufs + (c & 1) * (2 * N + 2);  // alternate buffers: no barrier after the update
+      double* buf = bufs + (c & 1) * C::BL;  // alternate buffers: no barrier after the update
       if (t == ps) {
         const double tinv = -1.0 / cur[c];
         rdiag = -tinv;
 #pragma unroll
         for (int j = c + 1; j < N; ++j) buf[j] = cur[j];
-        if (!last)
-#pragma unroll
-          for (int j = 0; j < N; ++j) buf[N + j] = nxt[j];
-        buf[2 * N] = rhs;
-        buf[2 * N + 1] = tinv;
+        if (last) buf[N] = rhs;
+        buf[N + 1] = tinv;
       }
       __syncwarp(msk);
       DSP_PHASE(28)
       if constexpr (JAC) {
-        if (t < PR) jrow[c * PR + t] = ((cand >> t) & 1u) ? cur[c] * buf[2 * N + 1] : 0.0;
+        if (t < PR) jrow[c * PR + t] = ((cand >> t) & 1u) ? cur[c] * buf[N + 1] : 0.0;
         if (t == 0) jrow[N * PR + c] = (double)ps;
       }
       if ((cand >> t) & 1u) {
-        const double m = cur[c] * buf[2 * N + 1];
+        const double m = cur[c] * buf[N + 1];
 #pragma unroll
-        for (int j = c + 1; j < N; ++j) cur[j] += m * buf[j];
-        if (!last)
-#pragma unroll
-          for (int j = 0; j < N; ++j) nxt[j] += m * buf[N + j];
-        rhs += m * buf[2 * N];
+        for (int j = c + 1; j < N; ++j) cur[j] = fma(m, buf[j], cur[j]);
+        cur[c] = m;
+        if (last) rhs = fma(m, buf[N], rhs);
       }
     }
     DSP_PHASE(21)
@@ -397,21 +426,72 @@ __global__ void __launch_bounds__(RCfg<N>::CTA, RCfg<N>::MINB) flux_bvp_reg_kern
       row[2 * N + 1] = rdiag;
     }
     if (!last) {
-      // the pivot row of column c is row c of the layer's elimination record
-      if (myc >= 0) {
-        double* row = brec0 + (long long)l * BS + myc * C::RL;
+      // ---- the right-hand block [x_{l+1} columns | rhs] --------------------
+      // Pivot row k (slot p_k): R_k = R0[p_k] + sum_{k' < k} m[p_k][k'] R_k', a
+      // unit lower-triangular solve; carried row s: R0[s] + sum_k m[s][k] R_k.
+      // One lane per column (N + 1 lanes), the panel rows' initial right-hand
+      // blocks and multipliers in shared memory.
+      double* ML = RF(l);  // the layer's record is used up
+      double* brow = brec0 + (long long)l * BS;
+      __syncwarp(msk);  // every read of the record's slot is done
+      if (t < PR) {
+        if (myc >= 0) {
+          // pivot row of column myc: its multipliers, and [U | . | . | 1/pivot] of
+          // the elimination record (row myc)
+          double* mk = ML + myc * (myc - 1) / 2;
 #pragma unroll
-        for (int j = 0; j < N; j += 2) {
-          *reinterpret_cast<double2*>(row + j) = make_double2(cur[j], cur[j + 1]);
-          *reinterpret_cast<double2*>(row + N + j) = make_double2(nxt[j], nxt[j + 1]);
+          for (int k = 0; k < N - 1; ++k)
+            if (k < myc) mk[k] = cur[k];
+          double* row = brow + myc * C::RL;
+#pragma unroll
+          for (int j = 0; j < N; j += 2) *reinterpret_cast<double2*>(row + j) = make_double2(cur[j], cur[j + 1]);
+          row[2 * N + 1] = rdiag;
+        } else {
+          double* mk = ML + C::ML_CARRIED + __popc(cand & ((1u << t) - 1u)) * N;
+#pragma unroll
+          for (int k = 0; k < N; ++k) mk[k] = cur[k];
         }
-        *reinterpret_cast<double2*>(row + 2 * N) = make_double2(rhs, rdiag);
       }
-      // carried rows become the next layer's current block
+      __syncwarp(msk);
+      DSP_PHASE(29)
+      if (t <= N) {
+        double r[N];
 #pragma unroll
-      for (int k = 0; k < N; ++k) {
-        cur[k] = nxt[k];
-        nxt[k] = 0.0;
+        for (int k = 0; k < N; ++k) r[k] = R0[pivslot[k] * C::R0S + t];
+#pragma unroll
+        for (int k = 1; k < N; ++k) {
+          const double* mk = ML + k * (k - 1) / 2;
+#pragma unroll
+          for (int kk = 0; kk < k; ++kk)
+            if (!((sing >> kk) & 1u)) r[k] = fma(mk[kk], r[kk], r[k]);
+        }
+        // V and c of the pivot rows (columns N + t of the record rows)
+#pragma unroll
+        for (int k = 0; k < N; ++k) brow[k * C::RL + N + t] = r[k];
+        unsigned cm = cand;
+        for (int rk = 0; cm != 0u; ++rk) {
+          const int sl = __ffs(cm) - 1;
+          cm &= cm - 1u;
+          const double* mk = ML + C::ML_CARRIED + rk * N;
+          double acc = R0[sl * C::R0S + t];
+#pragma unroll
+          for (int k = 0; k < N; ++k)
+            if (!((sing >> k) & 1u)) acc = fma(mk[k], r[k], acc);
+          R0[sl * C::R0S + t] = acc;
+        }
+      }
+      __syncwarp(msk);
+      // carried rows become the next layer's current block; the other lanes'
+      // rows are replaced or unused, so cur is not live across the column phase
+      {
+        const bool keep = t < PR && ((cand >> t) & 1u);
+        const double* rr = R0 + (keep ? t : 0) * C::R0S;
+#pragma unroll
+        for (int k = 0; k < N; ++k) {
+          const double v = rr[k];
+          cur[k] = keep ? v : 0.0;
+        }
+        rhs = keep ? rr[N] : 0.0;
       }
       carried = cand;
       __syncwarp(msk);
