@@ -610,7 +610,7 @@ def measure_general(ctx, stream, dev, n, seed, steps, warmup, world=1, rank=0, e
         step(batch, dout)
     torch.cuda.synchronize()
     bad = int((douts["status"] != 0).sum())
-    clocks = ClockSampler(str(local))
+    clocks = ClockSampler(str(dev.index if dev.index is not None else 0))
     ctx.set_timing(True)
     ctx.timing_reset()
     replicas.barrier()

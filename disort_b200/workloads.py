@@ -132,6 +132,20 @@ GENERAL_MU = (-0.5, -0.1, 0.1, 0.5, 1.0)
 GENERAL_PHI = (0.0, 60.0, 120.0, 180.0)
 
 
+def column_total(dtau) -> float:
+    """Total optical depth of a column as a user output depth: the smaller of
+    the sequential top-down and bottom-up sums of delta_tau.  The solver sums
+    the layers in its own (top-down) order, and with bottom-up indexing a user
+    depth d becomes total - d, so a depth one rounding above either sum would
+    fall outside the column."""
+    down = up = 0.0
+    for x in np.asarray(dtau, dtype=np.float64):
+        down += float(x)
+    for x in np.asarray(dtau, dtype=np.float64)[::-1]:
+        up += float(x)
+    return min(down, up)
+
+
 def general_mix(n_inst: int = 65536, seed: int = 3, nstr=None, layers=(10, 120)) -> tuple[list, int]:
     """Instances of the general solver's mixed batch and its flags.
 
@@ -148,7 +162,7 @@ def general_mix(n_inst: int = 65536, seed: int = 3, nstr=None, layers=(10, 120))
         N, L = int(Nv[k]), int(Lv[k])
         dtau = np.clip(rng.lognormal(-3.0, 2.0, L), 1e-6, 50.0)
         g = rng.uniform(0.5, 0.95, L)
-        tot = float(np.sum(dtau))
+        tot = column_total(dtau)
         insts.append(dict(
             num_streams=N, num_layers=L, num_phase_func_moments=N + 1,
             delta_tau=dtau, single_scat_albedo=rng.uniform(0.0, 0.99, L),

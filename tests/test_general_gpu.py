@@ -251,13 +251,16 @@ def test_general_spherical_beam(nstr):
     extended-precision oracle build, at 5e-8."""
     big = max(nstr) >= 32
     rtol = 5e-8 if big else 1e-9
+    # theoretically-zero fluxes (the downward diffuse flux at the top) come out
+    # as cancellation noise: 1.3e-12 in the extended build itself at 64 streams
+    atol = 1e-11 if big else 1e-12
     n = 2 if 64 in nstr else 12
     for kw in (dict(), dict(bottom_up=True), dict(thermal=True)):
         insts, flags = spherical_mix(n, seed=600 + sum(nstr), nstr=nstr, layers=(3, 5) if 64 in nstr else (3, 16),
                                      **kw)
         got, ref, _ = both(insts, flags, ext=big)
         assert np.all(got["status"] == 0) and np.all(ref["status"] == 0), (got["status"], ref["status"])
-        assert_parity_general(got, ref, f"spherical N={nstr} {kw}", rtol=rtol)
+        assert_parity_general(got, ref, f"spherical N={nstr} {kw}", rtol=rtol, atol=atol)
 
 
 def test_general_spherical_invalid_radius_and_missing_altitudes():

@@ -162,7 +162,7 @@ def general_thermal_mix(n, seed, nstr=(4, 8, 16, 32), user_tau=True):
                     mu_user=[-0.7, -0.2, 0.3, 0.9], phi_user=[0.0, 45.0])
         inst["wavenumber_high"] = inst["wavenumber_low"] * 1.02
         if user_tau:
-            tot = float(dtau.sum())
+            tot = workloads.column_total(dtau)
             inst["tau_user"] = [0.0, 0.37 * tot, tot]
         insts.append(inst)
     return insts

@@ -1,4 +1,4 @@
-"""GPU test of the gated emulator pipeline (disort_b200/surrogate.py), small scale.
+"""GPU test of the gated emulator pipeline (disort_b200/surrogate.py).
 
 The emulator corrects a 4-stream FP64 solve toward the 16-stream one; it is
 trained on columns labelled by the FP64 GPU solver, then used on column x band
@@ -9,8 +9,8 @@ instances with some columns pushed out of the training envelope.  Checked here:
   itself, and every out-of-envelope instance is gated at any disagreement
   tolerance, while the emulator alone carries the in-envelope instances when
   the disagreement test is switched off.
-The throughput at each tolerance is measured at full scale by bench.py's
-surrogate leg.
+The network is trained at the bench leg's scale; the throughput at each gate
+tolerance is measured by bench.py's surrogate leg.
 """
 import numpy as np
 import pytest
@@ -23,7 +23,8 @@ def trained():
     import torch
     from disort_b200 import capi, surrogate
     ctx = capi.Context(0, torch.cuda.current_stream().cuda_stream)
-    sur, rep = surrogate.train(ctx, n_columns=1 << 17, epochs=20, log=lambda *a: None)
+    # the bench leg's scale: 2^20 solver-labelled columns, 50 epochs (about 20 s)
+    sur, rep = surrogate.train(ctx, n_columns=1 << 20, epochs=50, log=lambda *a: None)
     yield ctx, sur, rep
     sur.emu.close()
     ctx.close()
@@ -32,18 +33,19 @@ def trained():
 def test_training_on_solver_labels(trained):
     ctx, sur, rep = trained
     assert rep["bad_label_status"] == 0
-    assert rep["last_loss"] < 0.2 * rep["first_loss"], rep
+    assert rep["last_loss"] < 0.35 * rep["first_loss"], rep
 
 
 def test_network_gain_over_the_cheap_solve(trained):
-    """The network's correction cuts the 4-stream solve's held-out median and
-    p99 errors at least in half, and brings the median under 1 %."""
+    """The network's correction cuts the 4-stream solve's held-out median error
+    at least in half and its p99 error by at least 30 %, and brings the median
+    under 1 %."""
     ctx, sur, rep = trained
     four = rep["four_stream_alone"]
     print(f"held-out median/p99: corrected {rep['holdout_median_rel_err']:.4g}/{rep['holdout_p99_rel_err']:.4g}, "
           f"4-stream alone {four['median_rel_err']:.4g}/{four['p99_rel_err']:.4g}")
     assert rep["holdout_median_rel_err"] < 0.5 * four["median_rel_err"], rep
-    assert rep["holdout_p99_rel_err"] < 0.5 * four["p99_rel_err"], rep
+    assert rep["holdout_p99_rel_err"] < 0.7 * four["p99_rel_err"], rep
     assert rep["holdout_median_rel_err"] < 1e-2, rep
 
 
