@@ -85,7 +85,7 @@ def build_bench(force: bool = False) -> str:
     os.makedirs(LIB, exist_ok=True)
     target = os.path.join(LIB, "libdsp_bench.so")
     src = os.path.join(CSRC, "fp64_peak.cu")
-    if force or _stale(target, [src]):
+    if force or _stale(target, [src, os.path.join(CSRC, "dsp_device.cuh")]):
         _run([NVCC, *ARCH, "-O3", "-std=c++17", "-Xcompiler", "-fPIC", "-shared", "-o", target, src])
     return target
 

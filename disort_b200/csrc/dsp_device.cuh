@@ -284,6 +284,21 @@ __device__ __forceinline__ void team_argmax(double& v, int& idx, double* red) {
 // bit patterns, so the maximum is two 32-bit warp reductions (high words, then
 // the low words of the lanes that tie on the high word) and the winner is the
 // lowest lane of the ballot of exact matches.  `zero` reports a maximum of 0.
+// 1/x without branches: the hardware approximation (rcp.approx.ftz.f64)
+// refined by two Newton-Raphson steps y <- y + y (1 - x y), each about doubling
+// the correct bits (Muller et al., Handbook of Floating-Point Arithmetic, 2nd
+// ed., section 4.7); within an ulp or two of 1/x for normal x.  Subnormal x
+// flush to zero (result +-inf); the pivots it serves are never that small in a
+// solvable system.
+__device__ __forceinline__ double rcp_newton(double x) {
+  double y;
+  asm("rcp.approx.ftz.f64 %0, %1;" : "=d"(y) : "d"(x));
+  double e = fma(-x, y, 1.0);
+  y = fma(y, e, y);
+  e = fma(-x, y, 1.0);
+  return fma(y, e, y);
+}
+
 __device__ __forceinline__ int warp_argmax_nonneg(double a, bool cand, bool& zero) {
   const unsigned long long b = static_cast<unsigned long long>(__double_as_longlong(a));
   const unsigned hi = cand ? static_cast<unsigned>(b >> 32) : 0u;

@@ -356,13 +356,15 @@ __global__ void __launch_bounds__(RCfg<N>::CTA, RCfg<N>::MINB) flux_bvp_reg_kern
     // element as the row operations of the steps; the last layer, with no
     // x_{l+1} columns, updates its right-hand side within the steps.
     int myc = -1;  // pivot column of this thread's row, if it becomes a pivot row
-    unsigned sing = 0u;  // columns whose pivot is zero: no elimination step
     // temperature Jacobian: this layer's multipliers and pivot slots
     double* const jrow = !JAC ? nullptr
         : p.jac_rec + ((GEN ? (long long)p.g.lay_off[slot] : (long long)i * L) + l) * jrec_stride(N);
 #pragma unroll
     for (int c = 0; c < N; ++c) {
       const bool isc = t < PR && ((cand >> t) & 1u);
+      // every lane's reciprocal, branch-free, issued alongside the search: the
+      // pivot lane's is ready when the search ends
+      const double rc = -rcp_newton(cur[c]);
       double a = fabs(cur[c]);
       if (isnan(a)) a = __longlong_as_double(0x7ff0000000000000ll);  // NaN ranks as +inf: one total order
       int idx;
@@ -382,7 +384,6 @@ __global__ void __launch_bounds__(RCfg<N>::CTA, RCfg<N>::MINB) flux_bvp_reg_kern
       if (t == 0) pivslot[c] = ps;
       if (idx >= PR || zero_piv) {  // LINPACK skips a zero pivot column (BandSolver.hpp:76-78)
         singular = true;
-        sing |= 1u << c;
         if constexpr (JAC) {
           if (t < PR) jrow[c * PR + t] = 0.0;
           if (t == 0) jrow[N * PR + c] = (double)ps;
@@ -391,25 +392,27 @@ __global__ void __launch_bounds__(RCfg<N>::CTA, RCfg<N>::MINB) flux_bvp_reg_kern
       }
       double* buf = bufs + (c & 1) * C::BL;  // alternate buffers: no barrier after the update
       if (t == ps) {
-        const double tinv = -1.0 / cur[c];
-        rdiag = -tinv;
+        rdiag = -rc;
 #pragma unroll
         for (int j = c + 1; j < N; ++j) buf[j] = cur[j];
         if (last) buf[N] = rhs;
-        buf[N + 1] = tinv;
+        buf[N + 1] = rc;
       }
       __syncwarp(msk);
+      const double tinv = buf[N + 1];
+      const double* pv = buf;
+      const double prhs = buf[N];
       DSP_PHASE(28)
       if constexpr (JAC) {
-        if (t < PR) jrow[c * PR + t] = ((cand >> t) & 1u) ? cur[c] * buf[N + 1] : 0.0;
+        if (t < PR) jrow[c * PR + t] = ((cand >> t) & 1u) ? cur[c] * tinv : 0.0;
         if (t == 0) jrow[N * PR + c] = (double)ps;
       }
       if ((cand >> t) & 1u) {
-        const double m = cur[c] * buf[N + 1];
+        const double m = cur[c] * tinv;
 #pragma unroll
-        for (int j = c + 1; j < N; ++j) cur[j] = fma(m, buf[j], cur[j]);
+        for (int j = c + 1; j < N; ++j) cur[j] = fma(m, pv[j], cur[j]);
         cur[c] = m;
-        if (last) rhs = fma(m, buf[N], rhs);
+        if (last) rhs = fma(m, prhs, rhs);
       }
     }
     DSP_PHASE(21)
@@ -455,29 +458,43 @@ __global__ void __launch_bounds__(RCfg<N>::CTA, RCfg<N>::MINB) flux_bvp_reg_kern
       __syncwarp(msk);
       DSP_PHASE(29)
       if (t <= N) {
+        // A zero-pivot step left its candidates' multiplier slots at +-0, so
+        // its terms add nothing: no test per term.
         double r[N];
 #pragma unroll
         for (int k = 0; k < N; ++k) r[k] = R0[pivslot[k] * C::R0S + t];
+        // right-looking: once R_kk is final it enters every later pivot row
+        // (each row still takes its terms in step order)
 #pragma unroll
-        for (int k = 1; k < N; ++k) {
-          const double* mk = ML + k * (k - 1) / 2;
+        for (int kk = 0; kk < N - 1; ++kk)
 #pragma unroll
-          for (int kk = 0; kk < k; ++kk)
-            if (!((sing >> kk) & 1u)) r[k] = fma(mk[kk], r[kk], r[k]);
-        }
+          for (int k = kk + 1; k < N; ++k) r[k] = fma(ML[k * (k - 1) / 2 + kk], r[kk], r[k]);
         // V and c of the pivot rows (columns N + t of the record rows)
 #pragma unroll
         for (int k = 0; k < N; ++k) brow[k * C::RL + N + t] = r[k];
+        // the NN carried rows, CQ at a time interleaved
+        constexpr int NC = PR - N, CQ = NC < 4 ? NC : 4;
         unsigned cm = cand;
-        for (int rk = 0; cm != 0u; ++rk) {
-          const int sl = __ffs(cm) - 1;
-          cm &= cm - 1u;
-          const double* mk = ML + C::ML_CARRIED + rk * N;
-          double acc = R0[sl * C::R0S + t];
+#pragma unroll
+        for (int q0 = 0; q0 < NC; q0 += CQ) {
+          int sl[CQ];
+          double acc[CQ];
+#pragma unroll
+          for (int q = 0; q < CQ; ++q) {
+            if (q0 + q < NC) {  // the last group may be partial
+              sl[q] = cm ? __ffs(cm) - 1 : 0;
+              cm &= cm - 1u;
+              acc[q] = R0[sl[q] * C::R0S + t];
+            }
+          }
 #pragma unroll
           for (int k = 0; k < N; ++k)
-            if (!((sing >> k) & 1u)) acc = fma(mk[k], r[k], acc);
-          R0[sl * C::R0S + t] = acc;
+#pragma unroll
+            for (int q = 0; q < CQ; ++q)
+              if (q0 + q < NC) acc[q] = fma(ML[C::ML_CARRIED + (q0 + q) * N + k], r[k], acc[q]);
+#pragma unroll
+          for (int q = 0; q < CQ; ++q)
+            if (q0 + q < NC) R0[sl[q] * C::R0S + t] = acc[q];
         }
       }
       __syncwarp(msk);

@@ -8,6 +8,8 @@
 
 #include <cstdint>
 
+#include "dsp_device.cuh"
+
 __global__ void __launch_bounds__(256) dfma_chains(double* out, int iters, double a, double b) {
   double x[8];
 #pragma unroll
@@ -51,4 +53,23 @@ extern "C" double dsp_bench_fp64_tflops(int device, int repeats) {
   if (cudaGetLastError() != cudaSuccess) return -1.0;
   const double flops = 2.0 * 8 * 16 * (double)iters * blocks * threads;
   return flops / (best * 1e-3) / 1e12;
+}
+
+// Check of the solver's branch-free reciprocal (dsp::rcp_newton, used for the
+// pivots of the boundary-value kernel) against CUDA's division on n values:
+// y[k] = rcp_newton(x[k]), q[k] = 1 / x[k] (device arrays).  Returns 0 or the
+// CUDA error code.
+__global__ void rcp_check_kernel(const double* x, double* y, double* q, int n) {
+  const int k = blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= n) return;
+  y[k] = dsp::rcp_newton(x[k]);
+  q[k] = 1.0 / x[k];
+}
+
+extern "C" int dsp_bench_rcp_check(const double* x, double* y, double* q, int n) {
+  if (n <= 0) return 0;
+  rcp_check_kernel<<<(n + 255) / 256, 256>>>(x, y, q, n);
+  cudaError_t e = cudaGetLastError();
+  if (e == cudaSuccess) e = cudaDeviceSynchronize();
+  return (int)e;
 }
