@@ -351,6 +351,16 @@ def alloc_flux_out_numpy(n_inst: int, num_layers: int) -> tuple[dict, np.ndarray
 # ---------------------------------------------------------------------------
 # libdsp.so (the product library)
 # ---------------------------------------------------------------------------
+class Schedule(ctypes.Structure):
+    """dsp_schedule: a launch schedule for instances with N streams and
+    min_layers..max_layers layers (0 fields: the built-in choice)."""
+    _fields_ = [("num_streams", c_int32), ("min_layers", c_int32), ("max_layers", c_int32),
+                ("layer_stage", c_int32), ("layer_cta", c_int32), ("persistent", c_int32)]
+
+
+# the schedule table measured by disort_b200/autotune.py on this GPU model
+TUNING_FILE = os.path.join(os.path.dirname(os.path.abspath(__file__)), "tuning", "b200.txt")
+
 _LIB = None
 
 
@@ -380,6 +390,18 @@ def load_library(path: str | None = None):
     lib.dsp_context_last_error.argtypes = [c_void_p]
     lib.dsp_flux_workspace_bytes.restype = c_int64
     lib.dsp_flux_workspace_bytes.argtypes = [POINTER(FluxBatch)]
+    lib.dsp_context_set_schedule.restype = c_int32
+    lib.dsp_context_set_schedule.argtypes = [c_void_p, POINTER(Schedule), c_int32]
+    lib.dsp_context_load_schedule_file.restype = c_int32
+    lib.dsp_context_load_schedule_file.argtypes = [c_void_p, ctypes.c_char_p]
+    lib.dsp_context_schedule_count.restype = c_int32
+    lib.dsp_context_schedule_count.argtypes = [c_void_p]
+    lib.dsp_flux_graph_create.restype = c_int32
+    lib.dsp_flux_graph_create.argtypes = [c_int32, POINTER(FluxBatch), POINTER(FluxOut), POINTER(c_void_p)]
+    lib.dsp_graph_launch.restype = c_int32
+    lib.dsp_graph_launch.argtypes = [c_void_p, c_void_p]
+    lib.dsp_graph_destroy.restype = c_int32
+    lib.dsp_graph_destroy.argtypes = [c_void_p]
     lib.dsp_context_set_debug.restype = c_int32
     lib.dsp_context_set_debug.argtypes = [c_void_p, c_uint32]
     lib.dsp_context_set_timing.restype = c_int32
@@ -412,13 +434,29 @@ def load_library(path: str | None = None):
 class Context:
     """RAII wrapper of a dsp_context."""
 
-    def __init__(self, device: int = 0, stream: int = 0, lib=None):
+    def __init__(self, device: int = 0, stream: int = 0, lib=None, tuned: bool = True):
+        """tuned: load the committed schedule table (TUNING_FILE) when present."""
         self.lib = lib or load_library()
         h = c_void_p()
         st = self.lib.dsp_context_create(device, c_void_p(stream), ctypes.byref(h))
         if st != DSP_OK:
             raise RuntimeError(f"dsp_context_create failed: {STATUS_NAMES.get(st, st)}")
         self.h = h
+        if tuned and os.path.exists(TUNING_FILE):
+            st = self.load_schedule_file(TUNING_FILE)
+            if st != DSP_OK:
+                raise RuntimeError(f"{TUNING_FILE}: {self.last_error()}")
+
+    def set_schedule(self, entries) -> int:
+        """entries: (N, min_layers, max_layers, layer_stage, layer_cta, persistent) tuples."""
+        arr = (Schedule * max(1, len(entries)))(*[Schedule(*e) for e in entries])
+        return int(self.lib.dsp_context_set_schedule(self.h, arr, len(entries)))
+
+    def load_schedule_file(self, path: str) -> int:
+        return int(self.lib.dsp_context_load_schedule_file(self.h, path.encode()))
+
+    def schedule_count(self) -> int:
+        return int(self.lib.dsp_context_schedule_count(self.h))
 
     def set_stream(self, stream: int):
         self.lib.dsp_context_set_stream(self.h, c_void_p(stream))
@@ -463,6 +501,34 @@ class Context:
     def close(self):
         if getattr(self, "h", None):
             self.lib.dsp_context_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class FluxGraph:
+    """A device-pointer flux solve captured as a CUDA graph (dsp_flux_graph_create);
+    launch() replays it on a stream; the batch's arrays are re-read on every launch."""
+
+    def __init__(self, batch: FluxBatch, out: FluxOut, device: int = 0, lib=None):
+        self.lib = lib or load_library()
+        self._keep = (batch, out)
+        h = c_void_p()
+        st = self.lib.dsp_flux_graph_create(device, ctypes.byref(batch), ctypes.byref(out), ctypes.byref(h))
+        if st != DSP_OK:
+            raise RuntimeError(f"dsp_flux_graph_create: {STATUS_NAMES.get(st, st)}")
+        self.h = h
+
+    def launch(self, stream: int = 0) -> int:
+        return int(self.lib.dsp_graph_launch(self.h, c_void_p(stream)))
+
+    def close(self):
+        if getattr(self, "h", None):
+            self.lib.dsp_graph_destroy(self.h)
             self.h = None
 
     def __del__(self):

@@ -48,10 +48,16 @@ dsp_status launch_flux_chunk(dsp_context ctx, const FluxParams& p, cudaStream_t 
       flux_layer_set_attrs<N, JAC>();
       attr = true;
     }
-    flux_layer_launch<N, JAC>(p, ctx->host_tables.at(N).data(), s, [&](const char* name, auto&& launch) {
-      KernelTimer kt(ctx, name, s);
-      launch();
-    });
+    // the schedule for (N, L) may pick the layer stage's form and CTA size
+    const dsp_schedule sch = find_schedule(ctx, N, p.L);
+    const bool split = sch.layer_stage == 0 ? layer_split<N>() : sch.layer_stage == 1;
+    flux_layer_launch<N, JAC>(
+        p, ctx->host_tables.at(N).data(), s,
+        [&](const char* name, auto&& launch) {
+          KernelTimer kt(ctx, name, s);
+          launch();
+        },
+        split, sch.layer_cta ? sch.layer_cta : 128);
   }
   if constexpr (SPH) {
     // the spherical particular solution replaces the layer stage's plane-parallel one
@@ -236,6 +242,7 @@ dsp_status dsp_context_destroy(dsp_context ctx) {
   for (auto& kv : ctx->tables) cudaFree(kv.second);
   for (auto& kv : ctx->mode_tables) cudaFree(kv.second);
   if (ctx->meta) cudaFree(ctx->meta);
+  if (ctx->flux_defaults) cudaFree(ctx->flux_defaults);
   delete ctx;
   return DSP_OK;
 }
@@ -260,6 +267,50 @@ dsp_status dsp_context_set_debug(dsp_context ctx, uint32_t flags) {
   ctx->debug = flags;
   return DSP_OK;
 }
+
+dsp_status dsp_context_set_schedule(dsp_context ctx, const dsp_schedule* entries, int32_t count) {
+  if (!ctx) return DSP_ERR_NOT_INITIALIZED;
+  if (count < 0 || (count > 0 && !entries)) return fail(ctx, DSP_ERR_INVALID_INPUT, "schedule entries");
+  for (int32_t k = 0; k < count; ++k) {
+    const dsp_schedule& e = entries[k];
+    if (e.min_layers > e.max_layers || e.layer_stage < 0 || e.layer_stage > 2 || e.persistent < 0 ||
+        e.persistent > 2 || (e.layer_cta != 0 && e.layer_cta != 64 && e.layer_cta != 128))
+      return fail(ctx, DSP_ERR_INVALID_INPUT, "schedule entry " + std::to_string(k) + " out of range");
+  }
+  ctx->schedule.assign(entries, entries + count);
+  return DSP_OK;
+}
+
+dsp_status dsp_context_load_schedule_file(dsp_context ctx, const char* path) {
+  if (!ctx) return DSP_ERR_NOT_INITIALIZED;
+  if (!path) return fail(ctx, DSP_ERR_INVALID_INPUT, "null path");
+  FILE* f = std::fopen(path, "r");
+  if (!f) return fail(ctx, DSP_ERR_INVALID_INPUT, std::string("cannot open ") + path);
+  std::vector<dsp_schedule> v;
+  char line[512];
+  int ln = 0;
+  bool bad = false;
+  while (std::fgets(line, sizeof(line), f)) {
+    ++ln;
+    if (char* h = std::strchr(line, '#')) *h = '\0';
+    dsp_schedule e{};
+    char extra = 0;
+    const int got = std::sscanf(line, "%d %d %d %d %d %d %c", &e.num_streams, &e.min_layers, &e.max_layers,
+                                &e.layer_stage, &e.layer_cta, &e.persistent, &extra);
+    if (got <= 0) continue;  // blank or comment line
+    if (got != 6) {
+      bad = true;
+      break;
+    }
+    v.push_back(e);
+  }
+  std::fclose(f);
+  if (bad) return fail(ctx, DSP_ERR_INVALID_INPUT, std::string(path) + ": line " + std::to_string(ln) +
+                                                       " is not 'N min_layers max_layers layer_stage layer_cta persistent'");
+  return dsp_context_set_schedule(ctx, v.data(), (int32_t)v.size());
+}
+
+int32_t dsp_context_schedule_count(dsp_context ctx) { return ctx ? (int32_t)ctx->schedule.size() : 0; }
 
 dsp_status dsp_context_timing_reset(dsp_context ctx) {
   if (!ctx) return DSP_ERR_NOT_INITIALIZED;
@@ -354,14 +405,24 @@ dsp_status flux_solve(dsp_context ctx, const dsp_flux_batch* batch_in, const dsp
   int64_t cnt[kFluxArrays];
   per_inst_counts(&b, cnt);
 
-  // ---- stage host inputs (and defaults) into device memory ---------------
+  // absent scalars read the DisortFluxConfig defaults from a device copy made once
+  if (!ctx->flux_defaults) {
+    e = cudaMalloc(&ctx->flux_defaults, sizeof(kDefaults));
+    if (e == cudaSuccess) e = cudaMemcpy(ctx->flux_defaults, kDefaults, sizeof(kDefaults), cudaMemcpyHostToDevice);
+    if (e != cudaSuccess) {
+      if (ctx->flux_defaults) cudaFree(ctx->flux_defaults);
+      ctx->flux_defaults = nullptr;
+      return cuda_fail(ctx, e, "flux defaults");
+    }
+  }
+  // ---- stage host inputs into device memory --------------------------------
   dsp_darray* arr = batch_arrays(&b);
   const double* host_in[kFluxArrays] = {};  // per-instance host arrays still to be copied
   {
     size_t need = 0;
     for (int k = 0; k < kFluxArrays; ++k) {
       size_t elems;
-      if (!arr[k].ptr) elems = kScalarField[k] ? 1 : 0;
+      if (!arr[k].ptr) elems = 0;
       else if (dev) elems = 0;
       else elems = arr[k].stride == 0 ? (size_t)cnt[k] : (size_t)((n - 1) * arr[k].stride + cnt[k]);
       need += ((elems * sizeof(double) + 255) / 256) * 256;
@@ -371,11 +432,8 @@ dsp_status flux_solve(dsp_context ctx, const dsp_flux_batch* batch_in, const dsp
     for (int k = 0; k < kFluxArrays; ++k) {
       if (!arr[k].ptr) {
         if (kScalarField[k]) {  // absent scalar: the DisortFluxConfig default
-          e = cudaMemcpyAsync(cur, &kDefaults[k], sizeof(double), cudaMemcpyHostToDevice, s);
-          if (e != cudaSuccess) return cuda_fail(ctx, e, "cudaMemcpyAsync(default)");
-          arr[k].ptr = reinterpret_cast<const double*>(cur);
+          arr[k].ptr = ctx->flux_defaults + k;
           arr[k].stride = 0;
-          cur += 256;
         }
         continue;
       }
@@ -390,7 +448,6 @@ dsp_status flux_solve(dsp_context ctx, const dsp_flux_batch* batch_in, const dsp
       arr[k].ptr = reinterpret_cast<const double*>(cur);
       cur += ((elems * sizeof(double) + 255) / 256) * 256;
     }
-    // kDefaults is static storage; the copies above are ordered before the kernels
   }
   // ---- outputs -----------------------------------------------------------
   const int ndof = L + 2;  // Jacobian columns: level temperatures 0..L, surface
@@ -621,3 +678,65 @@ dsp_status flux_solve(dsp_context ctx, const dsp_flux_batch* batch_in, const dsp
 }
 
 }  // namespace
+
+// ---------------------------------------------------------------------------
+// CUDA graph of a device-pointer flux solve (no reference counterpart)
+// ---------------------------------------------------------------------------
+struct dsp_graph_s {
+  dsp_context ctx = nullptr;  // private: its workspace addresses are baked into the graph
+  cudaStream_t cs = nullptr;
+  cudaGraph_t graph = nullptr;
+  cudaGraphExec_t exec = nullptr;
+  int device = 0;
+};
+
+extern "C" dsp_status dsp_flux_graph_create(int32_t device, const dsp_flux_batch* batch, const dsp_flux_out* out,
+                                            dsp_graph* g) {
+  if (!batch || !out || !g) return DSP_ERR_INVALID_INPUT;
+  *g = nullptr;
+  if (!(batch->flags & DSP_FLAG_DEVICE_POINTERS) || (batch->flags & DSP_FLAG_TEMPERATURE_JAC)) return DSP_ERR_INVALID_INPUT;
+  dsp_graph_s* gr = new dsp_graph_s;
+  gr->device = device;
+  auto bail = [&](dsp_status st) {
+    if (gr->exec) cudaGraphExecDestroy(gr->exec);
+    if (gr->graph) cudaGraphDestroy(gr->graph);
+    if (gr->ctx) dsp_context_destroy(gr->ctx);
+    if (gr->cs) cudaStreamDestroy(gr->cs);
+    delete gr;
+    return st;
+  };
+  if (cudaSetDevice(device) != cudaSuccess || cudaStreamCreateWithFlags(&gr->cs, cudaStreamNonBlocking) != cudaSuccess)
+    return bail(DSP_ERR_CUDA);
+  dsp_status st = dsp_context_create(device, gr->cs, &gr->ctx);
+  if (st != DSP_OK) return bail(st);
+  // a first solve sizes the workspace and uploads the tables, so that the
+  // captured solve consists of memsets and kernel launches only
+  if ((st = flux_solve(gr->ctx, batch, out, nullptr)) != DSP_OK) return bail(st);
+  if (cudaStreamSynchronize(gr->cs) != cudaSuccess) return bail(DSP_ERR_CUDA);
+  if (cudaStreamBeginCapture(gr->cs, cudaStreamCaptureModeRelaxed) != cudaSuccess) return bail(DSP_ERR_CUDA);
+  st = flux_solve(gr->ctx, batch, out, nullptr);
+  const cudaError_t ec = cudaStreamEndCapture(gr->cs, &gr->graph);
+  if (st != DSP_OK) return bail(st);
+  if (ec != cudaSuccess || !gr->graph) return bail(DSP_ERR_CUDA);
+  if (cudaGraphInstantiate(&gr->exec, gr->graph, 0) != cudaSuccess) return bail(DSP_ERR_CUDA);
+  *g = gr;
+  return DSP_OK;
+}
+
+extern "C" dsp_status dsp_graph_launch(dsp_graph g, void* stream) {
+  if (!g) return DSP_ERR_INVALID_INPUT;
+  if (cudaSetDevice(g->device) != cudaSuccess) return DSP_ERR_CUDA;
+  return cudaGraphLaunch(g->exec, static_cast<cudaStream_t>(stream)) == cudaSuccess ? DSP_OK : DSP_ERR_CUDA;
+}
+
+extern "C" dsp_status dsp_graph_destroy(dsp_graph g) {
+  if (!g) return DSP_ERR_INVALID_INPUT;
+  cudaSetDevice(g->device);
+  cudaStreamSynchronize(g->cs);
+  if (g->exec) cudaGraphExecDestroy(g->exec);
+  if (g->graph) cudaGraphDestroy(g->graph);
+  if (g->ctx) dsp_context_destroy(g->ctx);
+  if (g->cs) cudaStreamDestroy(g->cs);
+  delete g;
+  return DSP_OK;
+}

@@ -80,8 +80,21 @@ dsp_status get_mode_tables(dsp_context ctx, int N, const double** out) {
 // temperature-Jacobian forms (mode 0 with Jacobians asked for); SPH: with the
 // pseudo-spherical beam, whose particular solution of the mode is formed
 // between the two.
+// Resident CTAs of a kernel on the whole GPU (persistent launches).
+template <class K>
+int resident_ctas(dsp_context ctx, K kernel, int threads, size_t smem) {
+  int per_sm = 0;
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, threads, smem) != cudaSuccess || per_sm < 1)
+    per_sm = 1;
+  return per_sm * ctx->sm_count;
+}
+
+// `order`/`head` (persistent boundary-value launch): the chunk's slots by
+// descending layer count and this mode's queue counter; null: one CTA or team
+// per slot.
 template <int N, bool JAC, bool SPH>
-void launch_general_mode(dsp_context ctx, const FluxParams& p, long long layers, cudaStream_t s) {
+void launch_general_mode(dsp_context ctx, const FluxParams& p, long long layers, cudaStream_t s, const int* order,
+                         int* head) {
   using LC = LCfg<N, true>;
   static bool attr = false;
   if (!attr) {
@@ -109,17 +122,36 @@ void launch_general_mode(dsp_context ctx, const FluxParams& p, long long layers,
   if constexpr (N <= 16) {
     using C = RCfg<N>;
     KernelTimer kt(ctx, "gen_bvp_kernel");
-    flux_bvp_reg_kernel<N, true, JAC, SPH><<<(p.n + C::TPC - 1) / C::TPC, C::CTA, C::smem_bytes(), s>>>(p);
+    const int slots = (p.n + C::TPC - 1) / C::TPC;
+    if (order) {
+      static const int cap = resident_ctas(ctx, gen_bvp_reg_persistent_kernel<N, JAC, SPH>, C::CTA, C::smem_bytes());
+      gen_bvp_reg_persistent_kernel<N, JAC, SPH><<<slots < cap ? slots : cap, C::CTA, C::smem_bytes(), s>>>(p, order,
+                                                                                                          head);
+    } else {
+      flux_bvp_reg_kernel<N, true, JAC, SPH><<<slots, C::CTA, C::smem_bytes(), s>>>(p);
+    }
   } else {
     using C = TCfg<N>;
     KernelTimer kt(ctx, "gen_bvp_kernel");
-    flux_bvp_tile_kernel<N, true, JAC, SPH><<<(p.n + C::TPC - 1) / C::TPC, C::CTA, C::smem_bytes(), s>>>(p);
+    if (order) {
+      static bool pattr = false;
+      if (!pattr) {
+        cudaFuncSetAttribute(gen_bvp_tile_persistent_kernel<N, JAC, SPH>,
+                             cudaFuncAttributeMaxDynamicSharedMemorySize, (int)C::smem_bytes());
+        pattr = true;
+      }
+      static const int cap = resident_ctas(ctx, gen_bvp_tile_persistent_kernel<N, JAC, SPH>, C::CTA, C::smem_bytes());
+      gen_bvp_tile_persistent_kernel<N, JAC, SPH><<<p.n < cap ? p.n : cap, C::CTA, C::smem_bytes(), s>>>(p, order,
+                                                                                                        head);
+    } else {
+      flux_bvp_tile_kernel<N, true, JAC, SPH><<<p.n, C::CTA, C::smem_bytes(), s>>>(p);
+    }
   }
 }
 
 template <int N, bool SPH>
 dsp_status launch_general_chunk(dsp_context ctx, FluxParams p, long long layers, int maxm, const double* tabs,
-                                const JacView* jv) {
+                                const JacView* jv, const int* order, int* heads) {
   cudaStream_t s = ctx->stream;
   p.tables = tabs;
   {
@@ -136,8 +168,9 @@ dsp_status launch_general_chunk(dsp_context ctx, FluxParams p, long long layers,
   for (int m = 0; m <= maxm; ++m) {
     p.g.m = m;
     p.tables = tabs + (size_t)m * tab_size(N);
-    if (m == 0 && jrecs) launch_general_mode<N, true, SPH>(ctx, p, layers, s);
-    else launch_general_mode<N, false, SPH>(ctx, p, layers, s);
+    int* head = order ? heads + m : nullptr;
+    if (m == 0 && jrecs) launch_general_mode<N, true, SPH>(ctx, p, layers, s, order, head);
+    else launch_general_mode<N, false, SPH>(ctx, p, layers, s, order, head);
     if (m == 0 && jv) {
       // the Jacobians use the mode-0 elimination before the next mode replaces it
       using C = JCfg<N>;
@@ -162,23 +195,24 @@ dsp_status launch_general_chunk(dsp_context ctx, FluxParams p, long long layers,
 
 template <int N>
 dsp_status launch_general_n(dsp_context ctx, const FluxParams& p, long long layers, int maxm, const double* tabs,
-                            const JacView* jv) {
-  if (p.flags & DSP_FLAG_SPHERICAL_BEAM) return launch_general_chunk<N, true>(ctx, p, layers, maxm, tabs, jv);
-  return launch_general_chunk<N, false>(ctx, p, layers, maxm, tabs, jv);
+                            const JacView* jv, const int* order, int* heads) {
+  if (p.flags & DSP_FLAG_SPHERICAL_BEAM)
+    return launch_general_chunk<N, true>(ctx, p, layers, maxm, tabs, jv, order, heads);
+  return launch_general_chunk<N, false>(ctx, p, layers, maxm, tabs, jv, order, heads);
 }
 
 dsp_status launch_general(dsp_context ctx, int N, const FluxParams& p, long long layers, int maxm,
-                          const double* tabs, const JacView* jv) {
+                          const double* tabs, const JacView* jv, const int* order, int* heads) {
   switch (N) {
-    case 4: return launch_general_n<4>(ctx, p, layers, maxm, tabs, jv);
-    case 6: return launch_general_n<6>(ctx, p, layers, maxm, tabs, jv);
-    case 8: return launch_general_n<8>(ctx, p, layers, maxm, tabs, jv);
-    case 10: return launch_general_n<10>(ctx, p, layers, maxm, tabs, jv);
-    case 12: return launch_general_n<12>(ctx, p, layers, maxm, tabs, jv);
-    case 14: return launch_general_n<14>(ctx, p, layers, maxm, tabs, jv);
-    case 16: return launch_general_n<16>(ctx, p, layers, maxm, tabs, jv);
-    case 32: return launch_general_n<32>(ctx, p, layers, maxm, tabs, jv);
-    case 64: return launch_general_n<64>(ctx, p, layers, maxm, tabs, jv);
+    case 4: return launch_general_n<4>(ctx, p, layers, maxm, tabs, jv, order, heads);
+    case 6: return launch_general_n<6>(ctx, p, layers, maxm, tabs, jv, order, heads);
+    case 8: return launch_general_n<8>(ctx, p, layers, maxm, tabs, jv, order, heads);
+    case 10: return launch_general_n<10>(ctx, p, layers, maxm, tabs, jv, order, heads);
+    case 12: return launch_general_n<12>(ctx, p, layers, maxm, tabs, jv, order, heads);
+    case 14: return launch_general_n<14>(ctx, p, layers, maxm, tabs, jv, order, heads);
+    case 16: return launch_general_n<16>(ctx, p, layers, maxm, tabs, jv, order, heads);
+    case 32: return launch_general_n<32>(ctx, p, layers, maxm, tabs, jv, order, heads);
+    case 64: return launch_general_n<64>(ctx, p, layers, maxm, tabs, jv, order, heads);
   }
   return fail(ctx, DSP_ERR_UNSUPPORTED, "unsupported num_streams");
 }
@@ -496,6 +530,8 @@ dsp_status general_solve(dsp_context ctx, const dsp_general_batch* bin, const ds
     std::vector<int64_t> inst_off, lay_off;
     int64_t inst_doubles = 0, layers = 0;
     int maxm = 0;
+    // persistent boundary-value launches: the slots by descending layer count
+    std::vector<int32_t> order;
   };
   std::vector<Chunk> chunks;
   size_t budget = workspace_budget();
@@ -554,12 +590,21 @@ dsp_status general_solve(dsp_context ctx, const dsp_general_batch* bin, const ds
     flush();
   }
   if (chunks.empty()) goto copy_back;
+  // the size-class queue of each chunk the schedule runs persistently
+  for (Chunk& c : chunks) {
+    const int meanL = c.ids.empty() ? 0 : (int)(c.layers / (int64_t)c.ids.size());
+    if (find_schedule(ctx, c.N, meanL).persistent != 1) continue;
+    c.order.resize(c.ids.size());
+    for (size_t k = 0; k < c.ids.size(); ++k) c.order[k] = (int32_t)k;
+    std::stable_sort(c.order.begin(), c.order.end(),
+                     [&](int32_t a, int32_t b) { return hL[c.ids[a]] > hL[c.ids[b]]; });
+  }
   {
     // chunk index arrays, one upload
     size_t meta_need = 0, ws_need = 0;
     for (const Chunk& c : chunks) {
       meta_need += align256(c.ids.size() * 4) + align256(c.ids.size() * 8) + align256((c.ids.size() + 1) * 8) +
-                   align256(c.layers * 4);
+                   align256(c.layers * 4) + align256(c.order.size() * 4) + align256((c.maxm + 1) * 4);
       const int64_t lstride = glrec_stride(c.N, numu_eff);
       const size_t w =
           (size_t)(c.inst_doubles +
@@ -587,6 +632,9 @@ dsp_status general_solve(dsp_context ctx, const dsp_general_batch* bin, const ds
         for (size_t ci = 0; ci < nc; ++ci)
           for (int64_t l = c.lay_off[ci]; l < c.lay_off[ci + 1]; ++l) li[l] = (int32_t)ci;
         o += align256(c.layers * 4);
+        if (!c.order.empty()) std::memcpy(hmeta.data() + o, c.order.data(), c.order.size() * 4);
+        o += align256(c.order.size() * 4);
+        o += align256((c.maxm + 1) * 4);  // queue counters, one per mode, zero
       }
     }
     e = cudaMemcpyAsync(ctx->meta, hmeta.data(), meta_need, cudaMemcpyHostToDevice, s);
@@ -639,6 +687,10 @@ dsp_status general_solve(dsp_context ctx, const dsp_general_batch* bin, const ds
       g.lay_off = reinterpret_cast<const long long*>(mb);
       mb += align256((nc + 1) * 8);
       g.layer_inst = reinterpret_cast<const int*>(mb);
+      mb += align256(c.layers * 4);
+      const int* order = c.order.empty() ? nullptr : reinterpret_cast<const int*>(mb);
+      mb += align256(c.order.size() * 4);
+      int* heads = reinterpret_cast<int*>(mb);
       g.lstride = glrec_stride(c.N, numu_eff);
       p.n = (int)nc;
       p.N = c.N;
@@ -669,7 +721,8 @@ dsp_status general_solve(dsp_context ctx, const dsp_general_batch* bin, const ds
         e = cudaMemsetAsync(ctx->ws, 0xFF, wb, s);
         if (e != cudaSuccess) return cuda_fail(ctx, e, "scratch poison");
       }
-      if ((st = launch_general(ctx, c.N, p, c.layers, c.maxm, tabs, jac ? &jv : nullptr)) != DSP_OK) return st;
+      if ((st = launch_general(ctx, c.N, p, c.layers, c.maxm, tabs, jac ? &jv : nullptr, order, heads)) != DSP_OK)
+        return st;
     }
   }
 

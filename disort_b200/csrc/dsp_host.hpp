@@ -6,6 +6,7 @@
 #include <cuda_runtime.h>
 #include <nvtx3/nvToolsExt.h>
 
+#include <algorithm>
 #include <cfloat>
 #include <cmath>
 #include <cstdio>
@@ -37,6 +38,7 @@ struct dsp_context_s {
   std::map<int, std::vector<double>> host_tables;  // host copies of `tables`
   std::map<int, double*> mode_tables;  // general solver: one table per azimuth mode
   void* meta = nullptr;                // general solver: chunk index arrays
+  double* flux_defaults = nullptr;     // defaults of absent flux-batch scalars (device, uploaded once)
   size_t meta_bytes = 0;
   // host-buffer solves: copy streams and events of the copy/compute pipeline
   cudaStream_t s_in = nullptr, s_out = nullptr;
@@ -45,6 +47,7 @@ struct dsp_context_s {
   // optional per-kernel timing
   bool timing = false;
   uint32_t debug = 0;  // DSP_DEBUG_* flags
+  std::vector<dsp_schedule> schedule;  // launch schedules, first match wins
   struct Pending {
     int kernel;
     cudaEvent_t a, b;
@@ -57,6 +60,15 @@ struct dsp_context_s {
 };
 
 namespace dsp_host {
+// The schedule entry for (N, L); a zeroed entry (built-in choices) if none matches.
+inline dsp_schedule find_schedule(dsp_context c, int N, int L) {
+  for (const dsp_schedule& e : c->schedule)
+    if (e.num_streams == N && e.min_layers <= L && L <= e.max_layers) return e;
+  dsp_schedule z{};
+  z.num_streams = N;
+  return z;
+}
+
 inline cudaEvent_t take_event(dsp_context c) {
   if (!c->free_events.empty()) {
     cudaEvent_t e = c->free_events.back();

@@ -88,21 +88,19 @@ struct RCfg {
   static_assert(N != 16 || 16 * (smem_bytes() + 1024) <= 228 * 1024, "16 CTAs per SM at 16 streams");
 };
 
-template <int N, bool GEN = false, bool JAC = false, bool SPH = false>
-__global__ void __launch_bounds__(RCfg<N>::CTA, RCfg<N>::MINB) flux_bvp_reg_kernel(FluxParams p) {
+// One instance (chunk slot `slot`) on this thread's team; the CTA's constant
+// tables are in shared memory already.
+template <int N, bool GEN, bool JAC, bool SPH>
+__device__ __forceinline__ void bvp_reg_instance(const FluxParams& p, const int slot) {
   using C = RCfg<N>;
   constexpr int NN = C::NN, TEAM = C::TEAM, PR = C::PR;
   constexpr double PI = 3.14159265358979323846;
   static_assert(PR <= 32 && TEAM <= 32, "register panel needs one warp");
   extern __shared__ double smem[];
-  for (int k = threadIdx.x; k < C::TAB; k += blockDim.x) smem[k] = p.tables[k];
-  __syncthreads();
   const double* mu = smem + tab_mu(N);
   const double* wt = smem + tab_wt(N);
 
   const int team = threadIdx.x / TEAM, t = threadIdx.x % TEAM;
-  const int slot = blockIdx.x * C::TPC + team;
-  if (slot >= p.n) return;
   const unsigned msk = team_mask<TEAM>();
   const bool ifb = (p.flags & DSP_FLAG_INDEX_FROM_BOTTOM) != 0;
   // i: status / input / output index, L: layers, NT: output levels
@@ -683,6 +681,42 @@ __global__ void __launch_bounds__(RCfg<N>::CTA, RCfg<N>::MINB) flux_bvp_reg_kern
   }
   DSP_PHASE_END
   if (nonfinite && t == 0) set_status(p.status, i, DSP_ERR_NONFINITE);
+}
+
+// One team (a warp or part of one) per instance, in chunk-slot order.
+template <int N, bool GEN = false, bool JAC = false, bool SPH = false>
+__global__ void __launch_bounds__(RCfg<N>::CTA, RCfg<N>::MINB) flux_bvp_reg_kernel(FluxParams p) {
+  using C = RCfg<N>;
+  extern __shared__ double smem[];
+  for (int k = threadIdx.x; k < C::TAB; k += blockDim.x) smem[k] = p.tables[k];
+  __syncthreads();
+  const int slot = blockIdx.x * C::TPC + threadIdx.x / C::TEAM;
+  if (slot >= p.n) return;
+  bvp_reg_instance<N, GEN, JAC, SPH>(p, slot);
+}
+
+// Persistent form (general solver): a resident grid whose teams take chunk
+// slots from a work queue -- `order`, the chunk's slots by descending layer
+// count (the size classes), consumed through the counter `head` -- so that
+// the longest instances start first and the tail of the launch is short.
+template <int N, bool JAC = false, bool SPH = false>
+__global__ void __launch_bounds__(RCfg<N>::CTA, RCfg<N>::MINB)
+    gen_bvp_reg_persistent_kernel(FluxParams p, const int* order, int* head) {
+  using C = RCfg<N>;
+  constexpr int TEAM = C::TEAM;
+  extern __shared__ double smem[];
+  for (int k = threadIdx.x; k < C::TAB; k += blockDim.x) smem[k] = p.tables[k];
+  __syncthreads();
+  const int t = threadIdx.x % TEAM;
+  const unsigned msk = team_mask<TEAM>();
+  for (;;) {
+    int k = 0;
+    if (t == 0) k = atomicAdd(head, 1);
+    k = __shfl_sync(msk, k, 0, TEAM);
+    if (k >= p.n) break;
+    bvp_reg_instance<N, true, JAC, SPH>(p, order[k]);
+    __syncwarp(msk);  // the team's shared memory serves the next instance
+  }
 }
 
 }  // namespace dsp

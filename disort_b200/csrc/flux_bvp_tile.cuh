@@ -84,8 +84,10 @@ struct TMask {
   }
 };
 
-template <int N, bool GEN = false, bool JAC = false, bool SPH = false>
-__global__ void __launch_bounds__(TCfg<N>::CTA, TCfg<N>::MINB) flux_bvp_tile_kernel(FluxParams p) {
+// One instance (chunk slot `slot`) on the whole CTA; the constant tables are in
+// shared memory already.
+template <int N, bool GEN, bool JAC, bool SPH>
+__device__ __forceinline__ void bvp_tile_instance(const FluxParams& p, const int slot) {
   using C = TCfg<N>;
   constexpr int NN = C::NN, PR = C::PR, RG = C::RG, RPT = C::RPT, CPT = C::CPT, NW = C::NW;
   constexpr int LDU = C::LDU, RL = C::RL;
@@ -95,7 +97,6 @@ __global__ void __launch_bounds__(TCfg<N>::CTA, TCfg<N>::MINB) flux_bvp_tile_ker
   const int t = threadIdx.x;
   const int cg = t / RG, rg = t % RG;
   const unsigned half = 0xffffu << (threadIdx.x & 16u);  // this thread's half-warp
-  for (int k = t; k < 2 * N; k += TEAM) smem[C::O_TAB + k] = p.tables[k];
   const double* mu = smem + C::O_TAB;
   const double* wt = smem + C::O_TAB + N;
   double* U = smem + C::O_U;
@@ -110,10 +111,7 @@ __global__ void __launch_bounds__(TCfg<N>::CTA, TCfg<N>::MINB) flux_bvp_tile_ker
   int* psb = ints;           // pivot slot, two buffers
   int* pivslot = ints + 2;   // [N]
   int* sflag = ints + 2 + N; // singular column seen
-  __syncthreads();
 
-  const int slot = blockIdx.x;
-  if (slot >= p.n) return;
   const bool ifb = (p.flags & DSP_FLAG_INDEX_FROM_BOTTOM) != 0;
   int i, L, NT;
   const double* rec;
@@ -607,6 +605,36 @@ __global__ void __launch_bounds__(TCfg<N>::CTA, TCfg<N>::MINB) flux_bvp_tile_ker
     DSP_PHASE(14)
   }
   if (nonfinite && t == 0) set_status(p.status, i, DSP_ERR_NONFINITE);
+}
+
+// One CTA per instance, in chunk-slot order.
+template <int N, bool GEN = false, bool JAC = false, bool SPH = false>
+__global__ void __launch_bounds__(TCfg<N>::CTA, TCfg<N>::MINB) flux_bvp_tile_kernel(FluxParams p) {
+  using C = TCfg<N>;
+  extern __shared__ double smem[];
+  for (int k = threadIdx.x; k < 2 * N; k += C::CTA) smem[C::O_TAB + k] = p.tables[k];
+  __syncthreads();
+  if ((int)blockIdx.x >= p.n) return;
+  bvp_tile_instance<N, GEN, JAC, SPH>(p, blockIdx.x);
+}
+
+// Persistent form (general solver): a resident grid whose CTAs take chunk slots
+// from the size-class-ordered queue `order` through the counter `head`.
+template <int N, bool JAC = false, bool SPH = false>
+__global__ void __launch_bounds__(TCfg<N>::CTA, TCfg<N>::MINB)
+    gen_bvp_tile_persistent_kernel(FluxParams p, const int* order, int* head) {
+  using C = TCfg<N>;
+  extern __shared__ double smem[];
+  __shared__ int task;
+  for (int k = threadIdx.x; k < 2 * N; k += C::CTA) smem[C::O_TAB + k] = p.tables[k];
+  for (;;) {
+    if (threadIdx.x == 0) task = atomicAdd(head, 1);
+    __syncthreads();  // the task, and (first trip) the tables, are visible
+    const int k = task;
+    if (k >= p.n) break;
+    bvp_tile_instance<N, true, JAC, SPH>(p, order[k]);
+    __syncthreads();  // every thread is done with the instance before `task` changes
+  }
 }
 
 }  // namespace dsp

@@ -1585,28 +1585,34 @@ __global__ void __launch_bounds__(128) flux_layer_back_kernel(FluxParams p, Cons
 template <int N, bool JAC = false>
 inline void flux_layer_set_attrs() {
   using C = LCfg<N>;
-  if constexpr (layer_split<N>()) {
+  if constexpr (layer_split<N>())
     static_assert(Handoff<N / 2>::HS <= brec_stride(N), "the hand-off must fit in the boundary-value records");
-  } else {
-    cudaFuncSetAttribute(flux_layer_kernel<N, false, JAC>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                         (int)C::smem_bytes());
-  }
+  // the team kernel serves every N (N <= 16: when a schedule asks for it)
+  cudaFuncSetAttribute(flux_layer_kernel<N, false, JAC>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                       (int)C::smem_bytes());
 }
 
+// The layer stage of a flux chunk.  split: the three one-thread-per-task
+// launches (N <= 16 only), with `cta` threads per CTA (64 or 128); otherwise
+// the team kernel (shared-memory eigensolver, one team per layer task).
 template <int N, bool JAC = false, class Wrap>
-inline void flux_layer_launch(const FluxParams& p, const double* host_tab, cudaStream_t s, Wrap&& wrap) {
+inline void flux_layer_launch(const FluxParams& p, const double* host_tab, cudaStream_t s, Wrap&& wrap,
+                              bool split = layer_split<N>(), int cta = 128) {
   using C = LCfg<N>;
   const long long tasks = (long long)p.n * p.L;
   if constexpr (layer_split<N>()) {
-    const ConstTab<N> tc = make_const_tab<N>(host_tab);
-    const unsigned g = (unsigned)((tasks + 127) / 128);
-    wrap("flux_layer_kernel", [&] { flux_layer_front_kernel<N><<<g, 128, 0, s>>>(p, tc); });
-    wrap("flux_jacobi_kernel", [&] { flux_jacobi_kernel<N / 2><<<g, 128, 0, s>>>(p); });
-    wrap("flux_layer_kernel", [&] { flux_layer_back_kernel<N, JAC><<<g, 128, 0, s>>>(p, tc); });
-  } else {
-    const unsigned grid = (unsigned)((tasks + C::TPC - 1) / C::TPC);
-    wrap("flux_layer_kernel", [&] { flux_layer_kernel<N, false, JAC><<<grid, C::CTA, C::smem_bytes(), s>>>(p); });
+    if (split) {
+      const int b = cta == 64 ? 64 : 128;
+      const ConstTab<N> tc = make_const_tab<N>(host_tab);
+      const unsigned g = (unsigned)((tasks + b - 1) / b);
+      wrap("flux_layer_kernel", [&] { flux_layer_front_kernel<N><<<g, b, 0, s>>>(p, tc); });
+      wrap("flux_jacobi_kernel", [&] { flux_jacobi_kernel<N / 2><<<g, b, 0, s>>>(p); });
+      wrap("flux_layer_kernel", [&] { flux_layer_back_kernel<N, JAC><<<g, b, 0, s>>>(p, tc); });
+      return;
+    }
   }
+  const unsigned grid = (unsigned)((tasks + C::TPC - 1) / C::TPC);
+  wrap("flux_layer_kernel", [&] { flux_layer_kernel<N, false, JAC><<<grid, C::CTA, C::smem_bytes(), s>>>(p); });
 }
 
 }  // namespace dsp

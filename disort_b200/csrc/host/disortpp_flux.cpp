@@ -2,7 +2,9 @@
 // of the C ABI.  Validation mirrors DisortFluxConfig::validate
 // (DisortFluxConfig.cpp:43-143) message for message; every solve is one batched
 // dsp_flux_bands_solve call.
+#include <dlfcn.h>
 #include <cmath>
+#include <cstdio>
 #include <cstdlib>
 #include <mutex>
 #include <string>
@@ -193,6 +195,26 @@ dsp_context engine_context_locked() {
     const int dev = d ? std::atoi(d) : 0;
     if (dsp_context_create(dev, nullptr, &ctx) != DSP_OK)
       throw std::runtime_error("disortpp: no CUDA device available for the B200 engine");
+    // launch schedules: DSP_SCHEDULE_FILE, else the autotuned table installed
+    // beside this library (lib/../tuning/b200.txt), when present
+    std::string path;
+    if (const char* e = std::getenv("DSP_SCHEDULE_FILE")) {
+      path = e;
+    } else {
+      Dl_info info;
+      if (dladdr(reinterpret_cast<void*>(&engine_context_locked), &info) && info.dli_fname) {
+        std::string so = info.dli_fname;
+        const size_t cut = so.find_last_of('/');
+        path = (cut == std::string::npos ? std::string(".") : so.substr(0, cut)) + "/../tuning/b200.txt";
+      }
+    }
+    if (!path.empty()) {
+      if (FILE* f = std::fopen(path.c_str(), "r")) {
+        std::fclose(f);
+        if (dsp_context_load_schedule_file(ctx, path.c_str()) != DSP_OK)
+          throw std::runtime_error(std::string("disortpp: schedule file: ") + dsp_context_last_error(ctx));
+      }
+    }
   }
   return ctx;
 }

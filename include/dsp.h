@@ -245,6 +245,49 @@ dsp_status dsp_context_timing_get(dsp_context ctx, int32_t idx, const char** nam
 #define DSP_DEBUG_POISON_SCRATCH 1u
 dsp_status dsp_context_set_debug(dsp_context ctx, uint32_t flags);
 
+/*
+ * Launch schedules (no reference counterpart; the reference has one code path
+ * per solver).  An entry applies to instances with num_streams == N and
+ * min_layers <= num_layers <= max_layers; the first matching entry wins, and
+ * without one the built-in choice stands.  Fields (0 = built-in choice):
+ *   layer_stage  flux path, N <= 16: 1 = three one-thread-per-task launches
+ *                (register-resident eigensolver), 2 = one team per layer task
+ *                (shared-memory eigensolver);
+ *   layer_cta    threads per CTA of the one-thread-per-task launches: 64 or 128;
+ *   persistent   general path: 1 = boundary-value and intensity kernels run
+ *                as resident grids that take instances from a queue ordered by
+ *                descending layer count (size class), 2 = one CTA or team per
+ *                instance in index order.
+ * dsp_context_load_schedule_file reads entries as text lines
+ *   "N min_layers max_layers layer_stage layer_cta persistent"
+ * ('#' starts a comment), as written by the autotuner (disort_b200/autotune.py),
+ * and replaces the context's table; DSP_ERR_INVALID_INPUT on a malformed file.
+ */
+typedef struct dsp_schedule {
+  int32_t num_streams, min_layers, max_layers;
+  int32_t layer_stage, layer_cta, persistent;
+} dsp_schedule;
+dsp_status dsp_context_set_schedule(dsp_context ctx, const dsp_schedule* entries, int32_t count);
+dsp_status dsp_context_load_schedule_file(dsp_context ctx, const char* path);
+int32_t dsp_context_schedule_count(dsp_context ctx);
+
+/*
+ * A spectral loop as one CUDA graph (no reference counterpart): the whole
+ * device-pointer flux solve of `batch` into `out` (DSP_FLAG_DEVICE_POINTERS
+ * required; not with DSP_FLAG_TEMPERATURE_JAC) captured once and replayed by
+ * dsp_graph_launch on any stream of `device`.  Replays read the batch's device
+ * arrays and write `out` at the addresses given here, so a caller refreshes the
+ * inputs in place between launches.  The graph owns a private context (its
+ * workspace addresses are part of the graph); creation runs the solve once
+ * eagerly, then captures it.  Destroy only after the last launch has completed
+ * (synchronize its stream first).
+ */
+typedef struct dsp_graph_s* dsp_graph;
+dsp_status dsp_flux_graph_create(int32_t device, const dsp_flux_batch* batch, const dsp_flux_out* out,
+                                 dsp_graph* graph);
+dsp_status dsp_graph_launch(dsp_graph graph, void* stream);
+dsp_status dsp_graph_destroy(dsp_graph graph);
+
 /* Flux-only spectral-band solve (DisortFluxSolver<N> over every instance). */
 dsp_status dsp_flux_bands_solve(dsp_context ctx, const dsp_flux_batch* batch,
                                 const dsp_flux_out* out);
