@@ -50,6 +50,7 @@ def parse():
     ap.add_argument("--bands", type=int, default=0, help="profiling: solve only the first N bands")
     ap.add_argument("--no-cpu", action="store_true", help="profiling: skip the CPU baseline")
     ap.add_argument("--no-e2e", action="store_true", help="profiling: skip the host-buffer pass")
+    ap.add_argument("--no-graph", action="store_true", help="profiling: skip the CUDA-graph replay pass")
     ap.add_argument("--no-surrogate", action="store_true",
                     help="skip the gated-emulator leg (solver-labelled training + gated inference)")
     ap.add_argument("--no-general", action="store_true",
@@ -374,6 +375,9 @@ def run_ours(args):
             e2e_mom = {"value": v, "unit": "solves/s", "h2d_bytes_per_step": h, "d2h_bytes_per_step": d,
                        "matches_device_result": sm, "inputs": "full phase-function moments [L][17]"}
 
+    # ---- the same device-resident step replayed as one CUDA graph ---------------
+    graph = None if args.no_graph else graph_leg(batch, out, stream, local, n, args)
+
     # ---- roofline of the dominant kernel -----------------------------------
     beam = bool(np.any(np.asarray(w["arrays"]["direct_beam_flux"]) > 0))
     thermal = bool(w["flags"] & capi.FLAG_THERMAL)
@@ -406,6 +410,7 @@ def run_ours(args):
                     "matches_device_result": same,
                     "inputs": "one HG asymmetry factor per layer (DSP_FLAG_HG_G)" if "hg_g" in w else "moments"},
             "e2e_full_moments": e2e_mom,
+            "graph": graph,
             "gpu_launches": int(sum(v[1] for v in ktimes.values())),
             "roofline": roofline, "cpu_baseline": cpu, "parity": parity, "clocks": clk,
             "bad_status_instances": bad,
@@ -417,6 +422,31 @@ def run_ours(args):
         print(json.dumps(line), flush=True)
     ctx.close()
     replicas.finish()
+
+
+def graph_leg(batch, out, stream, device, n, args) -> dict:
+    """The device-resident step as one CUDA graph (dsp_flux_graph_create),
+    replayed `steps` times after `warmup` replays; CUDA events on the stream."""
+    import torch
+    g = capi.FluxGraph(batch, out, device)
+    try:
+        for _ in range(max(1, args.warmup)):
+            g.launch(stream.cuda_stream)
+        torch.cuda.synchronize()
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record(stream)
+        for _ in range(args.steps):
+            rc = g.launch(stream.cuda_stream)
+            if rc != 0:
+                raise RuntimeError(f"dsp_graph_launch: {capi.STATUS_NAMES.get(rc, rc)}")
+        b.record(stream)
+        torch.cuda.synchronize()
+        ms = a.elapsed_time(b)
+    finally:
+        torch.cuda.synchronize()
+        g.close()
+    return {"value": n * args.steps / (ms / 1000.0), "unit": "solves/s", "ms_per_step": ms / args.steps,
+            "note": "the same device-resident solve replayed as one CUDA graph"}
 
 
 def surrogate_leg(ctx) -> dict:

@@ -23,10 +23,10 @@
 //   B. the threads holding the pivot row stage it in shared memory (it becomes
 //      row c of U);                                              barrier
 //   C. every thread updates its candidate rows: a += m * pivot row.
-// After N steps W_l = U^{-1} [V | d] is a back substitution over the staged U
-// rows, one column per thread, written to the W record for the upward sweep,
-// which evaluates the fluxes (or, for the general solver, stores the solution
-// coefficients) layer by layer.
+// After N steps the pivot rows [U | V | d] and the pivot reciprocals go to the
+// layer's elimination record; the upward sweep solves U_l x_l = d_l - V_l x_{l+1}
+// layer by layer and evaluates the fluxes (or, for the general solver, stores
+// the solution coefficients).
 #pragma once
 
 #include "dsp_device.cuh"
