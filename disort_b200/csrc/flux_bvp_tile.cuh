@@ -604,6 +604,7 @@ __device__ __forceinline__ void bvp_tile_instance(const FluxParams& p, const int
     }
     DSP_PHASE(14)
   }
+  DSP_PHASE_END
   if (nonfinite && t == 0) set_status(p.status, i, DSP_ERR_NONFINITE);
 }
 

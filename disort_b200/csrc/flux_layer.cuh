@@ -227,8 +227,11 @@ __device__ __forceinline__ bool team_chol(const double* M, double* Lc, double* f
 // 20,000-band thermal step); an off-diagonal left at that level moves
 // eigenvalues by its square and eigenvectors by it over the eigenvalue gap, far
 // below the 1e-9 parity bound.
+#ifndef DSP_JACOBI_TOL2
+#define DSP_JACOBI_TOL2 1.0e-30
+#endif
 __device__ __forceinline__ bool jacobi_needed(double apq, double app, double aqq) {
-  return fabs(apq) > 1e-300 && apq * apq > 1.0e-30 * fabs(app * aqq);
+  return fabs(apq) > 1e-300 && apq * apq > DSP_JACOBI_TOL2 * fabs(app * aqq);
 }
 
 // Jacobi rotation (Golub & Van Loan, Alg. 8.4.1) zeroing apq; tt = 0 when apq
@@ -934,6 +937,8 @@ __global__ void __launch_bounds__(LCfg<N, GEN>::CTA, LCfg<N, GEN>::MINB) flux_la
   if constexpr (GEN) {
     if (p.g.numu > 0) gen_user_angles<N>(p, i, sm, Y, wt, gl, lrec, rec[H_FBEAM], ws, thermal_src, t);
   }
+  DSP_PHASE(8)
+  DSP_PHASE_END
 }
 
 
