@@ -519,9 +519,14 @@ def general_cpu_time(lib, insts, flags, threads, keep_outputs=False):
     return (t, outs) if keep_outputs else t
 
 
-def general_parity(gpu: dict, idx, ref: dict, rtol=1e-9, atol=1e-12) -> dict:
+def general_parity(gpu: dict, idx, ref: dict, rtol=1e-9, atol=1e-12, floor_ref: dict | None = None) -> dict:
     """Fluxes element-wise; intensities against max(|value|, the instance's
-    largest |intensity|) (a Fourier sum whose terms cancel); <= 1 passes."""
+    largest |intensity|) (a Fourier sum whose terms cancel); <= 1 passes.
+
+    With `floor_ref` (the double build's outputs when `ref` is the extended-
+    precision build) an element's allowance is also at least the distance
+    between the two oracle builds there: the FP64 rounding floor of the
+    formulation itself, which no FP64 solver is held below."""
     worst, where = 0.0, None
     for f in capi.FLUX_OUT_FIELDS + ("intensity", "intensity_azimuth_avg"):
         a = np.asarray(gpu[f])[idx]
@@ -532,6 +537,8 @@ def general_parity(gpu: dict, idx, ref: dict, rtol=1e-9, atol=1e-12) -> dict:
             denom = rtol * np.maximum(np.abs(b), scale) + atol
         else:
             denom = rtol * np.abs(b) + atol
+        if floor_ref is not None:
+            denom = np.maximum(denom, np.abs(np.asarray(floor_ref[f]) - b))
         r = np.abs(a - b) / denom
         r = np.where(np.isnan(a) & np.isnan(b), 0.0, np.where(np.isnan(r), np.inf, r))
         k = float(r.max()) if r.size else 0.0
@@ -709,6 +716,10 @@ def measure_general(ctx, stream, dev, n, seed, steps, warmup, world=1, rank=0, e
             if ext_parity:
                 _, ref_ext = general_cpu_time(general_oracle_lib(ext=True), sample, flags, threads, keep_outputs=True)
                 parity["vs_extended_precision_oracle"] = general_parity(got, idx, ref_ext)
+                # the GPU against the extended build, allowed the double build's own distance from it
+                fa = general_parity(got, idx, ref_ext, floor_ref=ref)
+                parity["rounding_floor_aware"] = {"max_ratio": fa["max_ratio"], "at": fa["at"],
+                                                  "passes": fa["passes"]}
     return {
             "metric": GENERAL_METRIC, "value": value, "unit": "solves/s", "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": ms_max / args.steps, "higher_is_better": True, "scaling": "weak",

@@ -193,6 +193,11 @@ GENERAL_SCALAR_DEFAULTS = dict(wavenumber_low=0.0, wavenumber_high=0.0, surface_
                                temperature_top=0.0, temperature_bottom=0.0)
 
 
+# surface models (dsp.h DSP_BRDF_*; the BrdfType enum of the reference)
+BRDF_LAMBERTIAN, BRDF_RPV, BRDF_COX_MUNK, BRDF_AMBRALS, BRDF_HAPKE = 0, 1, 2, 3, 4
+BRDF_PARAMS = 8
+
+
 class GeneralBatch(ctypes.Structure):
     _fields_ = [
         ("n_inst", c_int32), ("flags", c_uint32),
@@ -203,7 +208,8 @@ class GeneralBatch(ctypes.Structure):
         ("delta_tau", c_void_p), ("single_scat_albedo", c_void_p), ("phase_function_moments", c_void_p),
         ("temperature", c_void_p),
         ("tau_user", DArray), ("mu_user", DArray), ("phi_user", DArray),
-    ] + [(f, DArray) for f in GENERAL_SCALAR_FIELDS] + [("level_altitudes", c_void_p), ("bottom_radius", DArray)]
+    ] + [(f, DArray) for f in GENERAL_SCALAR_FIELDS] + [("level_altitudes", c_void_p), ("bottom_radius", DArray),
+                                                        ("brdf_type", c_int32), ("brdf_params", DArray)]
 
 
 class GeneralOut(ctypes.Structure):
@@ -278,6 +284,17 @@ def pack_general(insts: list, flags: int, accuracy_fourier_series: float = 0.0,
             nphi = len(insts[0]["phi_user"])
             d["phi_user"] = _user_list(insts, "phi_user", nphi)
     d["num_user_tau"], d["num_user_mu"], d["num_phi"] = ntau, numu, nphi
+    # bidirectional surface: one type for the batch, parameters per instance
+    types = {int(c.get("brdf_type", BRDF_LAMBERTIAN)) for c in insts}
+    if len(types) != 1:
+        raise ValueError("brdf_type: one surface model per batch")
+    d["brdf_type"] = types.pop()
+    if d["brdf_type"] != BRDF_LAMBERTIAN:
+        bp = np.zeros((n, BRDF_PARAMS))
+        for i, c in enumerate(insts):
+            v = np.asarray(c.get("brdf_params", ()), dtype=np.float64).reshape(-1)
+            bp[i, :v.size] = v
+        d["brdf_params"] = bp
     d["ntau_out"] = ntau if flags & GFLAG_USER_TAU else int(L.max()) + 1
     d["numu_out"] = numu if (flags & GFLAG_USER_MU and not flags & GFLAG_ONLY_FLUXES) else int(N.max())
     return d
@@ -306,6 +323,10 @@ def make_general_batch(d: dict) -> tuple[GeneralBatch, list]:
         b.level_altitudes = _ptr(d["level_altitudes"])
         a = d["bottom_radius"]
         b.bottom_radius = DArray(_ptr(a), 1 if a.shape[0] > 1 else 0)
+    b.brdf_type = d.get("brdf_type", BRDF_LAMBERTIAN)
+    if "brdf_params" in d:
+        a = d["brdf_params"]
+        b.brdf_params = DArray(_ptr(a), BRDF_PARAMS if a.shape[0] > 1 else 0)
     return b, keep
 
 

@@ -40,7 +40,7 @@
 extern "C" {
 #endif
 
-#define DSP_API_VERSION 2
+#define DSP_API_VERSION 3
 
 typedef enum dsp_status {
   DSP_OK = 0,
@@ -145,7 +145,8 @@ typedef struct dsp_flux_jac_out {
 /*
  * General batch (DisortConfig, DisortConfig.hpp:119-243): the full DisortSolver
  * with Fourier azimuth modes and intensities at user optical depths, polar
- * angles and azimuths.  Plane-parallel geometry, Lambertian surface.
+ * angles and azimuths.  Plane-parallel or pseudo-spherical beam geometry,
+ * Lambertian or bidirectional (BRDF) surface.
  * Instances may differ in num_streams and num_layers: instance i owns layers
  * layer_offset[i] .. layer_offset[i+1]-1 of the layer arrays (CSR) and levels
  * layer_offset[i] + i .. layer_offset[i+1] + i of the level arrays.
@@ -180,7 +181,31 @@ typedef struct dsp_general_batch {
   /* pseudo-spherical beam (DSP_FLAG_SPHERICAL_BEAM; may be NULL otherwise) */
   const double* level_altitudes;        /* [total layers + n_inst], top down, levels like temperature */
   dsp_darray bottom_radius;             /* [1] */
+  /*
+   * Bidirectional surface (DisortFlags::use_lambertian_surface = false with
+   * DisortFlags::brdf_type, DisortConfig::brdf; DisortSolver.cpp:2582-2936).
+   * brdf_type 0 (DSP_BRDF_LAMBERTIAN, what a zero-initialised batch gives) keeps
+   * the Lambertian surface of surface_albedo.  Otherwise surface_albedo is not
+   * read and brdf_params holds DSP_BRDF_PARAMS doubles per instance (stride 0:
+   * shared), in the order of the reference's spec struct:
+   *   DSP_BRDF_RPV       rho0, k, theta, sigma, t1, t2, scale   (RpvBrdfSpec)
+   *   DSP_BRDF_COX_MUNK  u10, pcl, xsal, refractive_index, do_shadow (0 or 1)
+   *   DSP_BRDF_AMBRALS   iso, vol, geo                          (AmbralsBrdfSpec)
+   *   DSP_BRDF_HAPKE     b0, hh, w                              (HapkeBrdfSpec)
+   * The surface's Fourier coefficients are formed on the device at every
+   * azimuth mode with the reference's 100-node azimuth quadrature.
+   */
+  int32_t brdf_type;
+  dsp_darray brdf_params;               /* [DSP_BRDF_PARAMS] */
 } dsp_general_batch;
+
+/* brdf_type values: the BrdfType enum of DisortConfig.hpp */
+#define DSP_BRDF_LAMBERTIAN 0
+#define DSP_BRDF_RPV        1
+#define DSP_BRDF_COX_MUNK   2
+#define DSP_BRDF_AMBRALS    3
+#define DSP_BRDF_HAPKE      4
+#define DSP_BRDF_PARAMS     8
 
 /*
  * Temperature Jacobians of a general solve (DisortResult's *_temperature_jac,

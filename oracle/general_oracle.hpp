@@ -1,6 +1,6 @@
 // general_oracle.hpp — CPU restatement of DisortSolver::solve
 // (src/DisortSolver.cpp:21-399 of DisORT++) for plane-parallel geometry and a
-// Lambertian surface without intensity corrections: delta-M / delta-M+,
+// Lambertian or bidirectional (BRDF) surface, without intensity corrections: delta-M / delta-M+,
 // Fourier azimuth modes, fluxes at user optical depths and intensities at user
 // polar angles and azimuths.
 //
@@ -22,6 +22,8 @@ struct GeneralInstance {
   double radius = 0.0;           // bottom_radius
   const double* zalt = nullptr;  // level_altitudes [L+1] (spherical only)
   double accur = 0.0;
+  int brdf = 0;                  // 0: Lambertian; else the BrdfType (RPV 1, CoxMunk 2, Ambrals 3, Hapke 4)
+  const double* bp = nullptr;    // its parameters (SurfaceTables, oracle_common.hpp)
   double wlo = 0, whi = 0, alb = 0, emis = 1, fbeam = 0, umu0 = 0.5, phi0 = 0, fisot = 0, fisob = 0, ttop = 0, tbot = 0;
   const double *dtau = nullptr, *ssa = nullptr, *pmom = nullptr, *temp = nullptr;
   int ntau = 0, numu = 0, nphi = 0;
@@ -56,9 +58,10 @@ inline int validate_general(const GeneralInstance& c) {
     if (c.wlo < 0.0 || c.whi < c.wlo) return DSP_ERR_INVALID_INPUT;
   }
   if (c.dlbc && !c.thermal) return DSP_ERR_INVALID_INPUT;
+  if (c.dlbc && c.brdf != BRDF_LAMBERT) return DSP_ERR_INVALID_INPUT;  // DisortConfig.cpp:144-146
   if (c.fbeam < 0.0) return DSP_ERR_INVALID_INPUT;
   if ((c.umu0 <= 0.0 || c.umu0 > 1.0) && c.fbeam > 0.0) return DSP_ERR_INVALID_INPUT;
-  if (c.alb < 0.0 || c.alb > 1.0) return DSP_ERR_INVALID_INPUT;
+  if (c.brdf == BRDF_LAMBERT && (c.alb < 0.0 || c.alb > 1.0)) return DSP_ERR_INVALID_INPUT;
   if (c.user_mu) {
     if (c.numu <= 0 || !c.umu) return DSP_ERR_INVALID_INPUT;
     for (int iu = 0; iu < c.numu; ++iu) {
@@ -287,8 +290,13 @@ inline int GeneralOracle::solve(const GeneralInstance& cin, const GeneralOutput&
   if (out.jac[0])
     for (double* J : out.jac) std::fill(J, J + (size_t)ntau * out.jac_stride, 0.0);
 
+  // surface reflectance and emissivity of each mode (computeSurfaceBidir)
+  SurfaceTables sfc;
+  sfc.init(NN, do_int ? numu : 0);
+  const bool lamb = c.brdf == BRDF_LAMBERT;
   for (int m = 0; m <= naz; ++m) {
     const double d0 = (m == 0) ? 1.0 : 0.0;
+    sfc.fill(c.brdf, c.bp, c.alb, m, mu.data(), umu.data(), do_int, c.fbeam, c.umu0);
     legendre_flat(N, m, N, N - 1, mu.data(), ylq.data());
     auto Yq = [&](int l, int i) { return ylq[(size_t)l * N + i]; };
     if (do_int) legendre_flat(numu, m, numu, N - 1, umu.data(), ylu.data());
@@ -548,7 +556,8 @@ inline int GeneralOracle::solve(const GeneralInstance& cin, const GeneralOutput&
         }
       }
     }
-    // setMatrix (DisortSolver.cpp:1153-1317): Lambertian coupling only for m = 0
+    // setMatrix (DisortSolver.cpp:1153-1317): surface coupling at every mode of a
+    // BRDF, at mode 0 only for a Lambertian surface
     const int ncd = 3 * NN - 1, lda = 3 * ncd + 1, nshift = lda - 2 * N + 1;
     std::vector<double> band((size_t)lda * N * L, 0.0);
     auto BM = [&](int r, int col) -> double& { return band[(size_t)col * lda + r]; };
@@ -593,7 +602,7 @@ inline int GeneralOracle::solve(const GeneralInstance& cin, const GeneralOutput&
       int nncol = ncol - N - 1;
       jcol = 0;
       const int lb = ncut - 1;
-      const bool plain = lyrcut || c.dlbc || d0 == 0.0;
+      const bool plain = lyrcut || c.dlbc || (lamb && d0 == 0.0);
       for (int iq = 0; iq < NN; ++iq) {
         nncol++;
         int irow = nshift - jcol + N - 1;
@@ -601,7 +610,7 @@ inline int GeneralOracle::solve(const GeneralInstance& cin, const GeneralOutput&
           if (plain) BM(irow, nncol) = Gv(lb, jq, iq);
           else {
             double refl = 0.0;
-            for (int k = 0; k < NN; ++k) refl += wt[k] * mu[k] * c.alb * Gv(lb, NN - 1 - k, iq);
+            for (int k = 0; k < NN; ++k) refl += wt[k] * mu[k] * sfc.RQ(jq - NN, k + 1) * Gv(lb, NN - 1 - k, iq);
             BM(irow, nncol) = Gv(lb, jq, iq) - (1.0 + d0) * refl;
           }
           irow++;
@@ -616,7 +625,7 @@ inline int GeneralOracle::solve(const GeneralInstance& cin, const GeneralOutput&
           if (plain) BM(irow, nncol) = Gv(lb, jq, iq) * expa;
           else {
             double refl = 0.0;
-            for (int k = 0; k < NN; ++k) refl += wt[k] * mu[k] * c.alb * Gv(lb, NN - 1 - k, iq);
+            for (int k = 0; k < NN; ++k) refl += wt[k] * mu[k] * sfc.RQ(jq - NN, k + 1) * Gv(lb, NN - 1 - k, iq);
             BM(irow, nncol) = (Gv(lb, jq, iq) - (1.0 + d0) * refl) * expa;
           }
           irow++;
@@ -642,7 +651,16 @@ inline int GeneralOracle::solve(const GeneralInstance& cin, const GeneralOutput&
     if (m > 0) {
       if (beam) {
         for (int iq = 0; iq < NN; ++iq) b[iq] = -ZB(0, NN - 1 - iq);
-        for (int iq = 0; iq < NN; ++iq) b[nc - NN + iq] = -ZBT(lb, NN + iq, taus[ncut], btr[ncut]);
+        for (int iq = 0; iq < NN; ++iq) {
+          if (lyrcut || lamb) {
+            b[nc - NN + iq] = -ZBT(lb, NN + iq, taus[ncut], btr[ncut]);
+          } else {  // BRDF reflection of the diffuse and direct beam (DisortSolver.cpp:1729-1741)
+            double s = 0.0;
+            for (int jq = 0; jq < NN; ++jq)
+              s += wt[jq] * mu[jq] * sfc.RQ(iq, jq + 1) * ZB(lb, NN - 1 - jq) * btr[ncut];
+            b[nc - NN + iq] = s + (sfc.RQ(iq, 0) * c.umu0 * c.fbeam / M_PI - ZB(lb, NN + iq)) * btr[ncut];
+          }
+        }
         for (int lc = 1; lc < ncut; ++lc)
           for (int iq = 0; iq < N; ++iq)
             b[lc * N - NN + iq] = c.spherical ? ZBT(lc, iq, taus[lc], 0.0) - ZBT(lc - 1, iq, taus[lc], 0.0)
@@ -673,17 +691,17 @@ inline int GeneralOracle::solve(const GeneralInstance& cin, const GeneralOutput&
               double ps = 0.0;
               if (beam) ps += ZBT(lb, NN - 1 - jq, taus[ncut], btr[ncut]);
               if (c.thermal) ps += Z0(lb, NN - 1 - jq) + Z1(lb, NN - 1 - jq) * taus[ncut];
-              refl += wt[jq] * mu[jq] * c.alb * ps;
+              refl += wt[jq] * mu[jq] * sfc.RQ(iq, jq + 1) * ps;
             }
             s += 2.0 * refl;
           }
           if (beam) {
             s -= ZBT(lb, NN + iq, taus[ncut], btr[ncut]);
-            if (!lyrcut) s += c.alb * c.umu0 * c.fbeam * btr[ncut] / M_PI;
+            if (!lyrcut) s += sfc.RQ(iq, 0) * c.umu0 * c.fbeam * btr[ncut] / M_PI;
           }
           if (c.thermal) { s -= Z0(lb, NN + iq); s -= Z1(lb, NN + iq) * taus[ncut]; }
           s += c.fisob;
-          if (c.thermal) s += (1.0 - c.alb) * pbot;
+          if (c.thermal) s += sfc.eq[iq] * pbot;
           b[nc - NN + iq] = s;
         }
       }
@@ -823,7 +841,7 @@ inline int GeneralOracle::solve(const GeneralInstance& cin, const GeneralOutput&
                 sacc = 1.0;
                 if (dtau_last > 0.0) sacc += mu[iq] * (1.0 / dtau_last);
               } else {
-                sacc = 1.0 - c.alb;  // Lambertian emissivity
+                sacc = sfc.eq[iq];  // surface emissivity
               }
             } else if (c.dlbc) {
               sacc = -dz0(ncut - 1, NN + iq, k) - dz1(ncut - 1, NN + iq, k) * tauc_bot;
@@ -832,7 +850,7 @@ inline int GeneralOracle::solve(const GeneralInstance& cin, const GeneralOutput&
               if (!lyrcut) {
                 double refl = 0.0;
                 for (int jq = 0; jq < NN; ++jq)
-                  refl += wt[jq] * mu[jq] * c.alb * (dz0(ncut - 1, NN - 1 - jq, k) + dz1(ncut - 1, NN - 1 - jq, k) * tauc_bot);
+                  refl += wt[jq] * mu[jq] * sfc.RQ(iq, jq + 1) * (dz0(ncut - 1, NN - 1 - jq, k) + dz1(ncut - 1, NN - 1 - jq, k) * tauc_bot);
                 sacc += 2.0 * refl;
               }
               sacc -= dz0(ncut - 1, NN + iq, k) + dz1(ncut - 1, NN + iq, k) * tauc_bot;
@@ -953,12 +971,11 @@ inline int GeneralOracle::solve(const GeneralInstance& cin, const GeneralOutput&
             if (c.dlbc) {
               if (lyrcut || m > 0) { Iout = palint + plkint; continue; }
               bndint = (pbot + um * pbotd) * std::exp((utaus[lu] - taus[L]) / um);
-            } else if (lyrcut || m > 0) {
+            } else if (lyrcut || (lamb && m > 0)) {
               Iout = palint + plkint;
               continue;
             } else {
-              // Lambertian surface at user angles (DisortSolver.cpp:2655-2662): set only for mu > 0
-              const double rho_u = um > 0.0 ? c.alb : 0.0, emis_u = um > 0.0 ? 1.0 - c.alb : 0.0;
+              // surface at user angles (DisortSolver.cpp:3170-3220; tables set for mu > 0 only)
               for (int jq = NN; jq < N; ++jq) wkb[jq - NN] = std::exp(-kk[(size_t)(L - 1) * N + jq] * dts[L - 1]);
               double bnddfu = 0.0;
               for (int iq = NN - 1; iq >= 0; --iq) {
@@ -967,10 +984,10 @@ inline int GeneralOracle::solve(const GeneralInstance& cin, const GeneralOutput&
                 for (int jq = NN; jq < N; ++jq) dfu += Gv(L - 1, iq, jq) * CCv(L - 1, jq) * wkb[jq - NN];
                 if (beam) dfu += ZB(L - 1, iq) * btr[L];
                 dfu += d0 * (Z0(L - 1, iq) + Z1(L - 1, iq) * taus[L]);
-                bnddfu += (1.0 + d0) * rho_u * mu[NN - iq - 1] * wt[NN - iq - 1] * dfu;
+                bnddfu += (1.0 + d0) * sfc.RU(iu, NN - iq) * mu[NN - iq - 1] * wt[NN - iq - 1] * dfu;
               }
-              const double bnddir = c.umu0 * c.fbeam / M_PI * rho_u * btr[L];
-              bndint = (bnddfu + bnddir + d0 * emis_u * pbot + c.fisob) * std::exp((utaus[lu] - taus[L]) / um);
+              const double bnddir = c.umu0 * c.fbeam / M_PI * sfc.RU(iu, 0) * btr[L];
+              bndint = (bnddfu + bnddir + d0 * sfc.eu[iu] * pbot + c.fisob) * std::exp((utaus[lu] - taus[L]) / um);
             }
           }
           Iout = palint + plkint + bndint;

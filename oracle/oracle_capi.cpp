@@ -170,7 +170,10 @@ int oracle_general_bands_solve_jac(const dsp_general_batch* b, const dsp_general
         c.spherical = (fl & DSP_FLAG_SPHERICAL_BEAM) != 0;
         c.zalt = b->level_altitudes ? b->level_altitudes + l0 + i : nullptr;
         c.radius = scalar(b->bottom_radius, i, 0.0);
+        c.brdf = b->brdf_type;
+        c.bp = c.brdf ? at(b->brdf_params, i) : nullptr;
         if (c.L > 0 && b->layer_offset[i + 1] - l0 != c.L) st = DSP_ERR_INVALID_INPUT;
+        else if (c.brdf < 0 || c.brdf > 4 || (c.brdf && !c.bp)) st = DSP_ERR_INVALID_INPUT;
         else if (ntau > ntau_o || numu > numu_o || c.N > 64) st = DSP_ERR_INVALID_INPUT;
         else if (jac && jac->ndof_out < c.L + 2) st = DSP_ERR_INVALID_INPUT;
         else {

@@ -16,6 +16,7 @@
 #include <cstring>
 #include <limits>
 #include <stdexcept>
+#include <vector>
 
 namespace oracle {
 
@@ -383,5 +384,203 @@ inline void sym_eigen(const double* a_in, int n, int ld, double* evals, double* 
     }
   }
 }
+
+// ---------------------------------------------------------------------------
+// Bidirectional surface reflectance (DisortSolver.cpp:2710-2936).  `bp` holds
+// the parameters of the model in the C ABI's order (include/dsp.h,
+// dsp_general_batch::brdf_params):
+//   RPV      rho0, k, theta, sigma, t1, t2, scale
+//   CoxMunk  u10, pcl, xsal, refractive_index, do_shadow (0 / 1)
+//   Ambrals  iso, vol, geo
+//   Hapke    b0, hh, w
+// ---------------------------------------------------------------------------
+enum { BRDF_LAMBERT = 0, BRDF_RPV = 1, BRDF_COX_MUNK = 2, BRDF_AMBRALS = 3, BRDF_HAPKE = 4 };
+
+// bidirReflectivityHapke (DisortSolver.cpp:2710-2732)
+inline double brdf_hapke(const double* bp, double mu, double mup, double dphi) {
+  const double b0 = bp[0], hh = bp[1], w = bp[2];
+  const double ctheta = mu * mup + std::sqrt((1.0 - mu * mu) * (1.0 - mup * mup)) * std::cos(dphi);
+  const double thetah = std::acos(ctheta);
+  const double p = 1.0 + 0.5 * ctheta;
+  const double b = b0 * hh / (hh + std::tan(0.5 * thetah));
+  const double gam = std::sqrt(1.0 - w);
+  const double h0 = (1.0 + 2.0 * mup) / (1.0 + 2.0 * gam * mup);
+  const double h = (1.0 + 2.0 * mu) / (1.0 + 2.0 * gam * mu);
+  return 0.25 * w * ((1.0 + b) * p + h0 * h - 1.0) / (mu + mup);
+}
+
+// bidirReflectivityRpv (DisortSolver.cpp:2734-2780), called with badmu = 0
+// (DisortSolver.cpp:2915-2918): no clamping of the cosines
+inline double brdf_rpv(const double* bp, double mu1, double mu2, double phi) {
+  const double rho0 = bp[0], k = bp[1], th = bp[2], sigma = bp[3], t1 = bp[4], t2 = bp[5], scale = bp[6];
+  phi = M_PI - phi;  // RPV measures the azimuth from the backward direction
+  const double hspot = rho0 * (std::pow(2.0 * mu1 * mu1 * mu1, k - 1.0) * (1.0 - th) / ((1.0 + th) * (1.0 + th)) *
+                                   (2.0 - rho0) + sigma / mu1) *
+                       (t1 * std::exp(M_PI * t2) + 1.0);
+  if (phi == 1.0e-4 && mu1 == mu2) return hspot * scale;
+  const double m = std::pow(mu1 * mu2 * (mu1 + mu2), k - 1.0);
+  const double cosphi = std::cos(phi);
+  const double sin1 = std::sqrt(1.0 - mu1 * mu1), sin2 = std::sqrt(1.0 - mu2 * mu2);
+  const double cosg = mu1 * mu2 + sin1 * sin2 * cosphi;
+  const double g = std::acos(cosg);
+  const double f = (1.0 - th * th) / std::pow(1.0 + 2.0 * th * cosg + th * th, 1.5);
+  const double tan1 = sin1 / mu1, tan2 = sin2 / mu2;
+  const double capg = std::sqrt(tan1 * tan1 + tan2 * tan2 - 2.0 * tan1 * tan2 * cosphi);
+  const double hval = 1.0 + (1.0 - rho0) / (1.0 + capg);
+  const double t = 1.0 + t1 * std::exp(t2 * (M_PI - g));
+  const double ans = rho0 * (m * f * hval + sigma / mu1) * t * scale;
+  return ans < 0.0 ? 0.0 : ans;
+}
+
+// bidirReflectivityRossLi (DisortSolver.cpp:2782-2836): Ross-thick volume and
+// Li-sparse-reciprocal geometric kernels, crown height/base 2, branch/radius 1,
+// hot-spot width 1.5 degrees
+inline double brdf_rossli(const double* bp, double mu, double mup, double dphi) {
+  const double iso = bp[0], vol = bp[1], geo = bp[2];
+  const double hb = 2.0, br = 1.0, alpha0 = 1.5 * M_PI / 180.0;
+  const double sin_i = std::sqrt(1.0 - mup * mup), sin_r = std::sqrt(1.0 - mu * mu);
+  const double tan_i = mup > 0.0 ? sin_i / mup : 0.0, tan_r = mu > 0.0 ? sin_r / mu : 0.0;
+  double cos_a = mup * mu + sin_i * sin_r * std::cos(dphi);
+  cos_a = std::min(std::max(cos_a, -1.0), 1.0);
+  const double alpha = std::acos(cos_a), sin_a = std::sin(alpha);
+  const double cc = 1.0 + 1.0 / (1.0 + alpha / alpha0);
+  const double f_vol = 4.0 / (3.0 * M_PI) * (1.0 / (mup + mu)) * ((M_PI / 2.0 - alpha) * cos_a + sin_a) * cc - 1.0 / 3.0;
+  const double ti = br * tan_i, tr = br * tan_r;
+  const double ci = 1.0 / std::sqrt(1.0 + ti * ti), cr = 1.0 / std::sqrt(1.0 + tr * tr);
+  const double si = ti * ci, sr = tr * cr;
+  const double cos_a1 = ci * cr + si * sr * std::cos(dphi);
+  double g2 = ti * ti + tr * tr - 2.0 * ti * tr * std::cos(dphi);
+  if (g2 < 0.0) g2 = 0.0;
+  const double cos_t = hb * (ci * cr) / (ci + cr) * std::sqrt(g2 + std::pow(ti * tr * std::sin(dphi), 2));
+  double t = 0.0;
+  if (cos_t >= -1.0 && cos_t <= 1.0) t = std::acos(cos_t);
+  const double f_geo = (ci + cr) / (M_PI * ci * cr) * (t - std::sin(t) * std::cos(t) - M_PI) + (1.0 + cos_a1) / (2.0 * ci * cr);
+  return std::max(iso + vol * f_vol + geo * f_geo, 0.0);
+}
+
+// shadowEta (DisortSolver.cpp:2838-2851): Tsang's shadowing function
+inline double brdf_shadow_eta(double cos_theta, double sigma_sq) {
+  const double sin_theta = std::sqrt(1.0 - cos_theta * cos_theta);
+  if (sin_theta < 1e-15) return 0.0;
+  const double cot = cos_theta / sin_theta;
+  const double t1 = std::sqrt(sigma_sq / M_PI) / cot * std::exp(-cot * cot / sigma_sq);
+  const double t2 = std::erfc(cot / std::sqrt(sigma_sq));
+  return 0.5 * (t1 - t2);
+}
+
+// bidirReflectivityCoxMunk (DisortSolver.cpp:2853-2900)
+inline double brdf_cox_munk(const double* bp, double mu, double mup, double dphi) {
+  const double u10 = bp[0], nt = bp[3];
+  const bool shadow = bp[4] != 0.0;
+  const double sin_i = std::sqrt(1.0 - mup * mup), sin_r = std::sqrt(1.0 - mu * mu);
+  const double cos_theta = -mup * mu + sin_i * sin_r * std::cos(dphi);
+  const double omc = 1.0 - cos_theta;
+  if (omc < 1e-15) return 0.0;
+  const double mun2 = (mup + mu) * (mup + mu) / (2.0 * omc);
+  if (mun2 < 1e-15) return 0.0;
+  const double s2 = 0.003 + 0.00512 * u10;
+  const double p_slope = 1.0 / (M_PI * s2) * std::exp(-(1.0 - mun2) / (s2 * mun2));
+  const double ni = 1.0;
+  const double cos_li = std::sqrt(0.5 * (1.0 + cos_theta));
+  const double sin_li = std::sqrt(std::max(0.0, 1.0 - cos_li * cos_li));
+  const double sin_lt = ni * sin_li / nt;
+  if (sin_lt >= 1.0) return 0.0;
+  const double cos_lt = std::sqrt(1.0 - sin_lt * sin_lt);
+  const double rs = (ni * cos_li - nt * cos_lt) / (ni * cos_li + nt * cos_lt);
+  const double rp = (nt * cos_li - ni * cos_lt) / (ni * cos_lt + nt * cos_li);
+  const double rf = 0.5 * (rs * rs + rp * rp);
+  double v = (p_slope * rf) / (4.0 * mup * mu * mun2 * mun2);
+  if (shadow) v *= 1.0 / (brdf_shadow_eta(mup, s2) + brdf_shadow_eta(mu, s2) + 1.0);
+  return std::max(v, 0.0);
+}
+
+// bidirReflectivity (DisortSolver.cpp:2902-2936)
+inline double brdf_value(int type, const double* bp, double mu, double mup, double dphi) {
+  switch (type) {
+    case BRDF_HAPKE: return brdf_hapke(bp, mu, mup, dphi);
+    case BRDF_RPV: return brdf_rpv(bp, mu, mup, dphi);
+    case BRDF_COX_MUNK: return brdf_cox_munk(bp, mu, mup, dphi);
+    case BRDF_AMBRALS: return brdf_rossli(bp, mu, mup, dphi);
+  }
+  return std::numeric_limits<double>::quiet_NaN();
+}
+
+// computeSurfaceBidir (DisortSolver.cpp:2582-2708) for one azimuth mode m:
+//   rq[iq][0]      direct-beam reflectance at quadrature angle iq
+//   rq[iq][1 + jq] diffuse reflectance, incoming stream jq, outgoing iq
+//   eq[iq]         directional emissivity (mode 0)
+//   ru[iu][...], eu[iu] the same at the user polar angles (mu > 0 only)
+// with the 100-point half-range Gauss quadrature of the azimuth (NMUG = 200,
+// DisortSolver.cpp:484-496).  Lambertian: the albedo at mode 0, zero above.
+struct SurfaceTables {
+  int NN = 0, numu = 0;
+  std::vector<double> rq, eq, ru, eu;
+  std::vector<double> gmu, gwt;  // the azimuth quadrature, 200 nodes
+  void init(int nn, int nu) {
+    NN = nn;
+    numu = nu;
+    rq.assign((size_t)NN * (NN + 1), 0.0);
+    eq.assign(NN, 0.0);
+    ru.assign((size_t)std::max(numu, 1) * (NN + 1), 0.0);
+    eu.assign(std::max(numu, 1), 0.0);
+    gmu.assign(200, 0.0);
+    gwt.assign(200, 0.0);
+    gauss_quadrature(100, gmu.data(), gwt.data());
+  }
+  double& RQ(int iq, int j) { return rq[(size_t)iq * (NN + 1) + j]; }
+  double& RU(int iu, int j) { return ru[(size_t)iu * (NN + 1) + j]; }
+  void fill(int type, const double* bp, double alb, int m, const double* mu, const double* umu, bool user,
+            double fbeam, double umu0) {
+    const double d0 = m == 0 ? 1.0 : 0.0;
+    std::fill(rq.begin(), rq.end(), 0.0);
+    std::fill(eq.begin(), eq.end(), 0.0);
+    auto fourier = [&](double a, double b) {
+      double s = 0.0;
+      for (int k = 0; k < 100; ++k)
+        s += gwt[k] * brdf_value(type, bp, a, b, M_PI * gmu[k]) * std::cos(static_cast<double>(m) * M_PI * gmu[k]);
+      return (2.0 - d0) * s;
+    };
+    auto emissivity = [&](double a) {
+      double dref = 0.0;
+      for (int jg = 0; jg < 200; ++jg) {
+        double s = 0.0;
+        for (int k = 0; k < 100; ++k) s += gwt[k] * gmu[k] * brdf_value(type, bp, a, gmu[k], M_PI * gmu[jg]);
+        dref += gwt[jg] * s;
+      }
+      return 1.0 - dref;
+    };
+    if (type == BRDF_LAMBERT) {
+      if (m == 0)
+        for (int iq = 0; iq < NN; ++iq) {
+          eq[iq] = 1.0 - alb;
+          for (int j = 0; j <= NN; ++j) RQ(iq, j) = alb;
+        }
+    } else {
+      for (int iq = 0; iq < NN; ++iq) {
+        for (int jq = 0; jq < NN; ++jq) RQ(iq, jq + 1) = fourier(mu[iq], mu[jq]);
+        if (fbeam > 0.0) RQ(iq, 0) = fourier(mu[iq], umu0);
+      }
+      if (m == 0)
+        for (int iq = 0; iq < NN; ++iq) eq[iq] = emissivity(mu[iq]);
+    }
+    if (!user) return;
+    std::fill(ru.begin(), ru.end(), 0.0);
+    std::fill(eu.begin(), eu.end(), 0.0);
+    for (int iu = 0; iu < numu; ++iu) {
+      const double u = umu[iu];
+      if (u <= 0.0) continue;
+      if (type == BRDF_LAMBERT) {
+        if (m == 0) {
+          for (int j = 0; j <= NN; ++j) RU(iu, j) = alb;
+          eu[iu] = 1.0 - alb;
+        }
+      } else {
+        for (int jq = 0; jq < NN; ++jq) RU(iu, jq + 1) = fourier(u, mu[jq]);
+        if (fbeam > 0.0) RU(iu, 0) = fourier(u, umu0);
+        if (m == 0) eu[iu] = emissivity(u);
+      }
+    }
+  }
+};
 
 }  // namespace oracle

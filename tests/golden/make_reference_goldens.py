@@ -89,6 +89,41 @@ CASES = [
     dict(test="CloudGarciaSiewert", suite="DeltaMPlus", N=16, L=1, nmom=298, dtau=[5.0], ssa=[1.0],
          phase=[("cloud",)], fbeam=1.0, umu0=0.5, albedo=0.0, dm_plus=True, utau=[0.0, 5.0],
          umu=[-1.0, -0.5, 0.5, 1.0], phi=[0.0]),
+    # bidirectional surfaces (general solver only).  Hapke (makeHapkeTestConfig1Layer,
+    # test_solver.cpp:4038-4080; b0 1, hh 0.06, w 0.6 by default) and RPV (:4133-4190),
+    # no intensity correction: fluxes and intensities pin the surface Fourier terms.
+    dict(test="HapkeBRDF1", N=16, L=1, nmom=16, dtau=[1.0], ssa=[1.0], phase=[("hg", 0.75)],
+         fbeam=PI, umu0=0.5, brdf=(4, [1.0, 0.06, 0.6]), utau=[0.0, 1.0],
+         umu=[-1.0, -0.5, -0.1, 0.1, 0.5, 1.0], phi=[0.0]),
+    dict(test="HapkeBRDF2", N=16, L=1, nmom=16, dtau=[0.5], ssa=[0.5], phase=[("iso",)],
+         fbeam=1.0, umu0=0.8, brdf=(4, [1.0, 0.06, 0.6]), utau=[0.0, 0.5],
+         umu=[-1.0, -0.5, -0.1, 0.1, 0.5, 1.0], phi=[0.0]),
+    dict(test="RpvBRDF1", N=16, L=1, nmom=16, dtau=[0.3], ssa=[0.9], phase=[("iso",)],
+         fbeam=1.0, umu0=0.6, brdf=(1, [0.1, 0.9, -0.2, 0.0, 0.0, 0.0, 1.0]), utau=[0.0, 0.3],
+         umu=[-1.0, -0.5, -0.1, 0.1, 0.5, 1.0], phi=[0.0]),
+    # disotest 6d-6h (makeTest6dConfig, test_solver.cpp:2200-2250): Hapke surface under a
+    # non-scattering layer with the intensity corrections switched on; without
+    # scattering the Nakajima-Tanaka correction does not apply, the BRDF beam correction
+    # of the intensities does ("intensity_corrected": the fluxes pin the surface alone)
+    dict(test="ValidationDisotest6d", N=16, L=1, nmom=0, dtau=[1.0], ssa=[0.0], phase=[("iso",)],
+         fbeam=200.0, umu0=0.5, brdf=(4, [1.0, 0.06, 0.6]), corr=True, utau=[0.0, 0.5, 1.0],
+         umu=[-1.0, -0.1, 0.1, 1.0], phi=[90.0], wn=(0.0, 50000.0)),
+    dict(test="ValidationDisotest6e", N=16, L=1, nmom=0, dtau=[1.0], ssa=[0.0], phase=[("iso",)],
+         fbeam=200.0, umu0=0.5, brdf=(4, [1.0, 0.06, 0.6]), corr=True, utau=[0.0, 0.5, 1.0],
+         umu=[-1.0, -0.1, 0.1, 1.0], phi=[90.0], thermal=True, temperature=[0.0, 0.0], wn=(0.0, 50000.0),
+         btemp=300.0, ttemp=0.0),
+    dict(test="ValidationDisotest6f", N=16, L=1, nmom=0, dtau=[1.0], ssa=[0.0], phase=[("iso",)],
+         fbeam=200.0, umu0=0.5, brdf=(4, [1.0, 0.06, 0.6]), corr=True, utau=[0.0, 0.5, 1.0],
+         umu=[-1.0, -0.1, 0.1, 1.0], phi=[90.0], thermal=True, temperature=[0.0, 0.0], wn=(0.0, 50000.0),
+         btemp=300.0, ttemp=250.0, fisot=100.0 / PI),
+    dict(test="ValidationDisotest6g", N=16, L=1, nmom=0, dtau=[1.0], ssa=[0.0], phase=[("iso",)],
+         fbeam=200.0, umu0=0.5, brdf=(4, [1.0, 0.06, 0.6]), corr=True, utau=[0.0, 0.5, 1.0],
+         umu=[-1.0, -0.1, 0.1, 1.0], phi=[90.0], thermal=True, temperature=[250.0, 300.0], wn=(0.0, 50000.0),
+         btemp=300.0, ttemp=250.0, fisot=100.0 / PI),
+    dict(test="ValidationDisotest6h", N=16, L=1, nmom=0, dtau=[10.0], ssa=[0.0], phase=[("iso",)],
+         fbeam=200.0, umu0=0.5, brdf=(4, [1.0, 0.06, 0.6]), corr=True, utau=[0.0, 1.0, 10.0],
+         umu=[-1.0, -0.1, 0.1, 1.0], phi=[90.0], thermal=True, temperature=[250.0, 300.0], wn=(0.0, 50000.0),
+         btemp=300.0, ttemp=250.0, fisot=100.0 / PI),
     # pseudo-spherical beam (test_solver.cpp:4459-4533): altitudes 60/30/0 km, radius 6371 km
     dict(test="SphericalGeometry", N=16, L=2, nmom=0, dtau=[0.5, 1.0], ssa=[0.9, 0.8], phase=[("hg", 0.8)],
          fbeam=1.0, umu0=0.5, albedo=0.1, spherical=True, zalt=[60.0, 30.0, 0.0], radius=6371.0,
@@ -196,6 +231,9 @@ def main():
             tau_user=c.get("utau"), mu_user=c.get("umu"), phi_user=c.get("phi"),
             use_spherical_beam=bool(c.get("spherical", False)), level_altitudes=c.get("zalt"),
             bottom_radius=c.get("radius", 0.0),
+            brdf_type=c["brdf"][0] if "brdf" in c else 0,
+            brdf_params=c["brdf"][1] if "brdf" in c else [],
+            intensity_corrected=bool(c.get("corr", False)),
             expect_flux=fl, expect_intensity=it,
         ))
     out = dict(generated_by="tests/golden/make_reference_goldens.py",

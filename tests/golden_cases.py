@@ -12,9 +12,15 @@ GOLDEN = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden", "ref
 
 
 def load_cases() -> list:
-    """The plane-parallel cases (every solver path supports them)."""
+    """The plane-parallel cases over a Lambertian surface (every solver path supports them)."""
     with open(GOLDEN) as f:
-        return [c for c in json.load(f)["cases"] if not c.get("use_spherical_beam")]
+        return [c for c in json.load(f)["cases"] if not c.get("use_spherical_beam") and not c.get("brdf_type")]
+
+
+def load_brdf_cases() -> list:
+    """The cases over a bidirectional surface (general solver only)."""
+    with open(GOLDEN) as f:
+        return [c for c in json.load(f)["cases"] if c.get("brdf_type")]
 
 
 def load_spherical_cases() -> list:
@@ -83,6 +89,11 @@ def general_instance(c: dict) -> tuple[dict, int]:
         isotropic_flux_top=c["isotropic_flux_top"],
         temperature_top=c["temperature_top"], temperature_bottom=c["temperature_bottom"],
     )
+    if c.get("brdf_type"):
+        inst["brdf_type"] = c["brdf_type"]
+        inst["brdf_params"] = c["brdf_params"]
+    if c.get("isotropic_flux_bottom"):
+        inst["isotropic_flux_bottom"] = c["isotropic_flux_bottom"]
     if c["tau_user"] is not None:
         flags |= capi.GFLAG_USER_TAU
         inst["tau_user"] = c["tau_user"]

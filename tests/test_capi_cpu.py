@@ -32,7 +32,7 @@ def test_library_exports_every_declared_symbol():
     lib = capi.load_library()
     missing = [n for n in declared_functions() if not hasattr(lib, n)]
     assert not missing, missing
-    assert lib.dsp_api_version() == 2
+    assert lib.dsp_api_version() == 3
     assert lib.dsp_status_string(capi.DSP_ERR_SINGULAR) == b"SINGULAR"
 
 

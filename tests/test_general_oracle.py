@@ -189,3 +189,67 @@ def test_general_spherical_equals_flux_spherical(nstr):
     assert o["status"][0] == 0 and st[0] == 0
     for k in capi.FLUX_OUT_FIELDS:
         np.testing.assert_allclose(o[k][0, :L + 1], f[k][0], rtol=1e-12, atol=1e-14, err_msg=k)
+
+
+BRDF_CASES = gc.load_brdf_cases()
+
+
+@pytest.mark.parametrize("case", BRDF_CASES, ids=[c["name"] for c in BRDF_CASES])
+def test_general_oracle_brdf_goldens(case):
+    """Bidirectional surfaces (Hapke, RPV) against the reference's C-DISORT goldens.
+    Cases run with the intensity corrections on compare their fluxes only (the
+    corrections change intensities, not fluxes)."""
+    inst, flags = gc.general_instance(case)
+    o = oracle_lib.general_solve(capi.pack_general([inst], flags))
+    assert o["status"][0] == 0
+    assert case["expect_flux"] or case["expect_intensity"]
+    for e in case["expect_flux"]:
+        v = o[e["field"]][0, e["index"]]
+        assert abs(v - e["value"]) <= e["tol"], (e, v)
+    if case["intensity_corrected"]:
+        return
+    for e in case["expect_intensity"]:
+        v = o["intensity"][0, e["lu"], e["iu"], e["j"]]
+        assert abs(v - e["value"]) <= e["tol"], (e, v)
+
+
+@pytest.mark.parametrize("model", [capi.BRDF_RPV, capi.BRDF_COX_MUNK, capi.BRDF_AMBRALS, capi.BRDF_HAPKE])
+def test_general_oracle_brdf_conserves_energy_sense(model):
+    """Every surface model: a non-absorbing, non-emitting column over a BRDF
+    reflects no more than it receives (net flux at the surface >= 0) and the
+    surface's reflection raises the upward flux over a black surface."""
+    params = {capi.BRDF_RPV: [0.1, 0.9, -0.2, 0.0, 0.0, 0.0, 1.0],
+              capi.BRDF_COX_MUNK: [5.0, 0.0, 0.0, 1.34, 1.0],
+              capi.BRDF_AMBRALS: [0.1, 0.05, 0.02],
+              capi.BRDF_HAPKE: [1.0, 0.06, 0.6]}[model]
+    rng = np.random.default_rng(11 + model)
+    inst = random_instance(rng, 8, 5, thermal=False, beam=True)
+    inst.update(mu_user=[-0.7, -0.2, 0.3, 0.8], phi_user=[0.0, 90.0, 180.0])
+    flags = capi.GFLAG_USER_MU
+    black = oracle_lib.general_solve(capi.pack_general([dict(inst, surface_albedo=0.0)], flags))
+    o = oracle_lib.general_solve(capi.pack_general([dict(inst, brdf_type=model, brdf_params=params)], flags))
+    assert o["status"][0] == 0 and black["status"][0] == 0
+    L = inst["num_layers"]
+    down = o["flux_down"][0, L] + o["flux_direct_beam"][0, L]
+    assert o["flux_up"][0, L] <= down
+    assert o["flux_up"][0, 0] > black["flux_up"][0, 0]
+    assert np.isfinite(o["intensity"][0]).all()
+
+
+def test_general_oracle_brdf_rejections():
+    """A BRDF with the diffusion lower boundary is invalid (DisortConfig.cpp:144-146);
+    an unknown model too; a BRDF ignores surface_albedo (no [0, 1] check)."""
+    rng = np.random.default_rng(5)
+    inst = random_instance(rng, 8, 3, thermal=True, beam=False)
+    hap = dict(brdf_type=capi.BRDF_HAPKE, brdf_params=[1.0, 0.06, 0.6])
+    fl = capi.FLAG_THERMAL | capi.GFLAG_ONLY_FLUXES
+    o = oracle_lib.general_solve(capi.pack_general([dict(inst, **hap)], fl))
+    assert o["status"][0] == 0
+    o = oracle_lib.general_solve(capi.pack_general([dict(inst, **hap)], fl | capi.FLAG_DIFFUSION_LOWER_BC))
+    assert o["status"][0] == capi.DSP_ERR_INVALID_INPUT
+    o = oracle_lib.general_solve(capi.pack_general([dict(inst, brdf_type=9, brdf_params=[1.0])], fl))
+    assert o["status"][0] == capi.DSP_ERR_INVALID_INPUT
+    o = oracle_lib.general_solve(capi.pack_general([dict(inst, surface_albedo=7.0, **hap)], fl))
+    assert o["status"][0] == 0
+    o = oracle_lib.general_solve(capi.pack_general([dict(inst, surface_albedo=7.0)], fl))
+    assert o["status"][0] == capi.DSP_ERR_INVALID_INPUT
