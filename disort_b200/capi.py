@@ -301,7 +301,14 @@ def pack_general(insts: list, flags: int, accuracy_fourier_series: float = 0.0,
 
 
 def make_general_batch(d: dict) -> tuple[GeneralBatch, list]:
-    """dsp_general_batch over the arrays of pack_general (host pointers)."""
+    """dsp_general_batch over the arrays of pack_general (host pointers, or
+    CUDA tensors in place of every array with FLAG_DEVICE_POINTERS)."""
+    if d["flags"] & FLAG_DEVICE_POINTERS:
+        host = [k for k, v in d.items() if isinstance(v, np.ndarray) or
+                (isinstance(v, tuple) and v and isinstance(v[0], np.ndarray))]
+        host = [k for k in host if k not in ("ntau_out", "numu_out")]
+        if host:
+            raise ValueError(f"FLAG_DEVICE_POINTERS with host arrays: {host}")
     keep = [d]
     b = GeneralBatch()
     b.n_inst = d["n_inst"]

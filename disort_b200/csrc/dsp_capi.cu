@@ -241,6 +241,7 @@ dsp_status dsp_context_destroy(dsp_context ctx) {
   if (ctx->stage_out) cudaFree(ctx->stage_out);
   for (auto& kv : ctx->tables) cudaFree(kv.second);
   for (auto& kv : ctx->mode_tables) cudaFree(kv.second);
+  if (ctx->brdf_q) cudaFree(ctx->brdf_q);
   if (ctx->meta) cudaFree(ctx->meta);
   if (ctx->flux_defaults) cudaFree(ctx->flux_defaults);
   delete ctx;

@@ -159,7 +159,22 @@ struct GenView {
   double* out_flux[8];         // [batch][ntau_out]
   double* out_int;             // [batch][ntau_out][numu_out][nphi]
   double* out_iavg;            // [batch][ntau_out][numu_out]
+  // bidirectional surface (brdf_type != 0): the model's parameters per batch
+  // instance, the 200-node azimuth quadrature [gmu | gwt], and per chunk slot
+  // the mode's surface table (brdf_stride doubles, written by gen_brdf_kernel)
+  int brdf_type;
+  DArr brdf_par;
+  const double* brdf_q;
+  double* brdf;
 };
+
+// Surface table of one chunk slot for the current azimuth mode
+// (computeSurfaceBidir, DisortSolver.cpp:2582-2708): rows r = 0..NN-1 are the
+// quadrature angles, r = NN + iu the user polar angles; each row holds
+// [beam reflectance | diffuse reflectance of incoming stream 0..NN-1 |
+//  directional emissivity (mode 0) | the intensity kernel's reflected-field sum].
+__host__ __device__ constexpr int brdf_row(int N) { return N / 2 + 3; }
+__host__ __device__ constexpr int brdf_stride(int N, int numu) { return round4((N / 2 + numu) * brdf_row(N)); }
 
 struct FluxParams {
   int n;          // instances in this launch

@@ -15,6 +15,7 @@
 #include "flux_jac.cuh"
 #include "flux_layer.cuh"
 #include "flux_sph.cuh"
+#include "gen_brdf.cuh"
 #include "gen_kernels.cuh"
 
 using namespace dsp;
@@ -72,6 +73,51 @@ dsp_status get_mode_tables(dsp_context ctx, int N, const double** out) {
   e = cudaMemcpy(d, tab.data(), tab.size() * sizeof(double), cudaMemcpyHostToDevice);
   if (e != cudaSuccess) return cuda_fail(ctx, e, "cudaMemcpy(mode tables)");
   ctx->mode_tables[N] = d;
+  *out = d;
+  return DSP_OK;
+}
+
+// The azimuth quadrature of the bidirectional surface (DisortSolver.cpp:484-496):
+// the 100-node Gauss rule on (0, 1) of the reference's gaussianQuadrature,
+// mirrored to 200 nodes, [gmu 200 | gwt 200]; uploaded once per context.
+dsp_status get_brdf_quadrature(dsp_context ctx, const double** out) {
+  if (ctx->brdf_q) {
+    *out = ctx->brdf_q;
+    return DSP_OK;
+  }
+  const int n = 100;
+  std::vector<double> q(400, 0.0);
+  for (int i = 1; i <= n; ++i) {
+    double z = std::cos(M_PI * (i - 0.25) / (n + 0.5)), z1, pp;
+    int iter = 0;
+    do {
+      double p1 = 1.0, p2 = 0.0;
+      for (int j = 1; j <= n; ++j) {
+        const double p3 = p2;
+        p2 = p1;
+        p1 = ((2.0 * j - 1.0) * z * p2 - (j - 1.0) * p3) / j;
+      }
+      pp = n * (z * p1 - p2) / (z * z - 1.0);
+      z1 = z;
+      z = z1 - p1 / pp;
+      if (++iter > 10) return fail(ctx, DSP_ERR_EIGEN, "BRDF azimuth quadrature did not converge");
+    } while (std::fabs(z - z1) > 3.0e-14);
+    q[i - 1] = 0.5 * (1.0 + z);
+    q[200 + i - 1] = 1.0 / ((1.0 - z * z) * pp * pp);
+  }
+  for (int i = 0; i < n; ++i) {
+    q[n + i] = -q[i];
+    q[200 + n + i] = q[200 + i];
+  }
+  double* d = nullptr;
+  cudaError_t e = cudaMalloc(&d, q.size() * sizeof(double));
+  if (e != cudaSuccess) return cuda_fail(ctx, e, "cudaMalloc(BRDF quadrature)");
+  e = cudaMemcpy(d, q.data(), q.size() * sizeof(double), cudaMemcpyHostToDevice);
+  if (e != cudaSuccess) {
+    cudaFree(d);
+    return cuda_fail(ctx, e, "cudaMemcpy(BRDF quadrature)");
+  }
+  ctx->brdf_q = d;
   *out = d;
   return DSP_OK;
 }
@@ -169,6 +215,11 @@ dsp_status launch_general_chunk(dsp_context ctx, FluxParams p, long long layers,
     p.g.m = m;
     p.tables = tabs + (size_t)m * tab_size(N);
     int* head = order ? heads + m : nullptr;
+    if (p.g.brdf) {
+      // the surface's Fourier coefficients of this mode, before the boundary-value problem
+      KernelTimer kt(ctx, "gen_brdf_kernel");
+      gen_brdf_kernel<N><<<p.n, 128, 0, s>>>(p);
+    }
     if (m == 0 && jrecs) launch_general_mode<N, true, SPH>(ctx, p, layers, s, order, head);
     else launch_general_mode<N, false, SPH>(ctx, p, layers, s, order, head);
     if (m == 0 && jv) {
@@ -315,6 +366,11 @@ dsp_status general_solve(dsp_context ctx, const dsp_general_batch* bin, const ds
     return fail(ctx, DSP_ERR_INVALID_INPUT, "num_phi must be positive when comp_only_fluxes=false");
   if (b.accuracy_fourier_series < 0.0)
     return fail(ctx, DSP_ERR_INVALID_INPUT, "accuracy_fourier_series must be non-negative (0 = disabled)");
+  const bool brdf = b.brdf_type != DSP_BRDF_LAMBERTIAN;
+  if (b.brdf_type < DSP_BRDF_LAMBERTIAN || b.brdf_type > DSP_BRDF_HAPKE)
+    return fail(ctx, DSP_ERR_INVALID_INPUT, "bidirReflectivity: unknown BRDF type");
+  if (brdf && !b.brdf_params.ptr)
+    return fail(ctx, DSP_ERR_INVALID_INPUT, "a bidirectional surface needs brdf_params");
   for (int f = 0; f < 8; ++f)
     if (!out->flux[f]) return fail(ctx, DSP_ERR_INVALID_INPUT, "every flux output array is required");
   if (do_int && (!out->intensity || !out->intensity_azimuth_avg))
@@ -377,6 +433,7 @@ dsp_status general_solve(dsp_context ctx, const dsp_general_batch* bin, const ds
   const double* d_temp = nullptr;
   const double* d_zalt = nullptr;
   dsp_darray d_rbot = b.bottom_radius;
+  dsp_darray d_bpar = b.brdf_params;
   const int32_t* d_L;
   const int64_t* d_off;
   const int32_t* d_nmom;
@@ -389,6 +446,7 @@ dsp_status general_solve(dsp_context ctx, const dsp_general_batch* bin, const ds
       if (thermal) need += align256((total_layers + n) * sizeof(double));
       if (spherical)
         need += align256((total_layers + n) * sizeof(double)) + align256(darray_elems(b.bottom_radius, 1) * sizeof(double));
+      if (brdf) need += align256(darray_elems(b.brdf_params, DSP_BRDF_PARAMS) * sizeof(double));
       for (int k = 0; k < 3; ++k)
         if (lists[k]->ptr && list_n[k] > 0) need += align256(darray_elems(*lists[k], list_n[k]) * sizeof(double));
     }
@@ -426,6 +484,9 @@ dsp_status general_solve(dsp_context ctx, const dsp_general_batch* bin, const ds
         d_rbot.ptr =
             static_cast<const double*>(put(b.bottom_radius.ptr, darray_elems(b.bottom_radius, 1) * sizeof(double)));
       }
+      if (brdf)
+        d_bpar.ptr = static_cast<const double*>(
+            put(b.brdf_params.ptr, darray_elems(b.brdf_params, DSP_BRDF_PARAMS) * sizeof(double)));
       for (int k = 0; k < 3; ++k) {
         dlists[k] = *lists[k];
         if (lists[k]->ptr && list_n[k] > 0)
@@ -529,6 +590,7 @@ dsp_status general_solve(dsp_context ctx, const dsp_general_batch* bin, const ds
     std::vector<int32_t> ids;
     std::vector<int64_t> inst_off, lay_off;
     int64_t inst_doubles = 0, layers = 0;
+    int64_t surf_doubles = 0;  // bidirectional surface tables, one per slot
     int maxm = 0;
     // persistent boundary-value launches: the slots by descending layer count
     std::vector<int32_t> order;
@@ -570,13 +632,14 @@ dsp_status general_solve(dsp_context ctx, const dsp_general_batch* bin, const ds
       if (hN[i] != N) continue;
       const int L = hL[i] > 0 ? hL[i] : 0;
       const int NT = user_tau ? b.num_user_tau : L + 1;
-      const int64_t rec = GenLayout::make(L, N, NT).stride;
+      const int64_t rec = GenLayout::make(L, N, NT).stride + (brdf ? brdf_stride(N, numu_eff) : 0);
       const size_t ib = (size_t)(rec + (int64_t)L * per_layer) * sizeof(double);
       if (!c.ids.empty() && bytes + ib > budget) flush();
       c.ids.push_back(i);
       c.inst_off.push_back(c.inst_doubles);
       c.lay_off.push_back(c.layers);
-      c.inst_doubles += rec;
+      c.inst_doubles += GenLayout::make(L, N, NT).stride;
+      if (brdf) c.surf_doubles += brdf_stride(N, numu_eff);
       c.layers += L;
       bytes += ib;
       int naz = N - 1;
@@ -607,7 +670,7 @@ dsp_status general_solve(dsp_context ctx, const dsp_general_batch* bin, const ds
                    align256(c.layers * 4) + align256(c.order.size() * 4) + align256((c.maxm + 1) * 4);
       const int64_t lstride = glrec_stride(c.N, numu_eff);
       const size_t w =
-          (size_t)(c.inst_doubles +
+          (size_t)(c.inst_doubles + c.surf_doubles +
                    c.layers * (lstride + brec_stride(c.N) + c.N + sph_per_layer(c.N) + jac_per_layer(c.N))) *
           sizeof(double);
       if (w > ws_need) ws_need = w;
@@ -676,6 +739,11 @@ dsp_status general_solve(dsp_context ctx, const dsp_general_batch* bin, const ds
     for (int f = 0; f < 8; ++f) g.out_flux[f] = dflux[f];
     g.out_int = dint;
     g.out_iavg = diavg;
+    g.brdf_type = b.brdf_type;
+    g.brdf_par.p = brdf ? d_bpar.ptr : nullptr;
+    g.brdf_par.s = d_bpar.stride;
+    g.brdf_q = nullptr;
+    if (brdf && (st = get_brdf_quadrature(ctx, &g.brdf_q)) != DSP_OK) return st;
     for (size_t k = 0; k < chunks.size(); ++k) {
       const Chunk& c = chunks[k];
       const size_t nc = c.ids.size();
@@ -712,11 +780,16 @@ dsp_status general_solve(dsp_context ctx, const dsp_general_batch* bin, const ds
         jv.ndof_out = (int)jdof_o;
         for (int f = 0; f < 6; ++f) jv.out[f] = djac[f];
       }
+      // after every per-layer area: the surface tables of the chunk's slots
+      g.brdf = brdf ? static_cast<double*>(ctx->ws) + c.inst_doubles +
+                          c.layers * (g.lstride + brec_stride(c.N) + c.N + sph_per_layer(c.N) + jac_per_layer(c.N))
+                    : nullptr;
       const double* tabs = nullptr;
       if ((st = get_mode_tables(ctx, c.N, &tabs)) != DSP_OK) return st;
       if (ctx->debug & DSP_DEBUG_POISON_SCRATCH) {
-        const size_t wb = (size_t)(c.inst_doubles + c.layers * (g.lstride + brec_stride(c.N) + c.N +
-                                                                 sph_per_layer(c.N) + jac_per_layer(c.N))) *
+        const size_t wb = (size_t)(c.inst_doubles + c.surf_doubles +
+                                   c.layers * (g.lstride + brec_stride(c.N) + c.N + sph_per_layer(c.N) +
+                                               jac_per_layer(c.N))) *
                           sizeof(double);
         e = cudaMemsetAsync(ctx->ws, 0xFF, wb, s);
         if (e != cudaSuccess) return cuda_fail(ctx, e, "scratch poison");

@@ -37,6 +37,7 @@ struct dsp_context_s {
   std::map<int, double*> tables;
   std::map<int, std::vector<double>> host_tables;  // host copies of `tables`
   std::map<int, double*> mode_tables;  // general solver: one table per azimuth mode
+  double* brdf_q = nullptr;            // general solver: the BRDF azimuth quadrature [gmu 200 | gwt 200]
   void* meta = nullptr;                // general solver: chunk index arrays
   double* flux_defaults = nullptr;     // defaults of absent flux-batch scalars (device, uploaded once)
   size_t meta_bytes = 0;

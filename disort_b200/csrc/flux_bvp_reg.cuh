@@ -157,6 +157,11 @@ __device__ __forceinline__ void bvp_reg_instance(const FluxParams& p, const int 
   const bool dlbc = (p.flags & DSP_FLAG_DIFFUSION_LOWER_BC) != 0;
   const double fbeam = rec[H_FBEAM], umu0 = rec[H_UMU0];
   const double alb = m == 0 ? rec[H_ALB] : 0.0;
+  // bidirectional surface (general solver): this mode's table, row r =
+  // [beam | diffuse streams | emissivity]; it couples at every mode
+  const double* sft = nullptr;
+  if constexpr (GEN)
+    if (p.g.brdf) sft = p.g.brdf + (long long)slot * brdf_stride(N, p.g.numu);
   const double fisot = m == 0 ? rec[H_FISOT] : 0.0, ptop = m == 0 ? rec[H_PTOP] : 0.0;
   const double fisob = m == 0 ? rec[H_FISOB] : 0.0, pbot = m == 0 ? rec[H_PBOT] : 0.0;
   const double pbotd = m == 0 ? rec[H_PBOTD] : 0.0;
@@ -287,13 +292,18 @@ __device__ __forceinline__ void bvp_reg_instance(const FluxParams& p, const int 
         const int rb = rank, jq = NN + rb;
         const bool plain = lyrcut || dlbc;
         const double* Gl = lr;
+        const double* srow = sft ? sft + rb * brdf_row(N) : nullptr;
+        const double cpl = m == 0 ? 2.0 : 1.0;  // 1 + delta_m0
 #pragma unroll
         for (int iq = 0; iq < N; ++iq) {
           double base = ld_rec(Gl + jq * GS + iq);
           if (!plain) {
             double refl = 0.0;
-            for (int k = 0; k < NN; ++k) refl += wt[k] * mu[k] * alb * ld_rec(Gl + (NN - 1 - k) * GS + iq);
-            base = base - 2.0 * refl;
+            if (srow)
+              for (int k = 0; k < NN; ++k) refl += wt[k] * mu[k] * srow[1 + k] * ld_rec(Gl + (NN - 1 - k) * GS + iq);
+            else
+              for (int k = 0; k < NN; ++k) refl += wt[k] * mu[k] * alb * ld_rec(Gl + (NN - 1 - k) * GS + iq);
+            base = base - cpl * refl;
           }
           cur[iq] = (iq < NN) ? base : base * Ecur[N - 1 - iq];
           nxt[iq] = 0.0;
@@ -314,20 +324,20 @@ __device__ __forceinline__ void bvp_reg_instance(const FluxParams& p, const int 
               double ps = 0.0;
               if (beam) ps += SPH ? zsph(lr, l, NN - 1 - jj, tau) : ld_rec(lr + C::SZB + NN - 1 - jj) * T;
               if (thermal) ps += ld_rec(lr + C::SZ0 + NN - 1 - jj) + ld_rec(lr + C::SZ1 + NN - 1 - jj) * tau;
-              refl += wt[jj] * mu[jj] * alb * ps;
+              refl += wt[jj] * mu[jj] * (srow ? srow[1 + jj] : alb) * ps;
             }
-            sum += 2.0 * refl;
+            sum += cpl * refl;
           }
           if (beam) {
             sum -= SPH ? zsph(lr, l, NN + rb, tau) : ld_rec(lr + C::SZB + NN + rb) * T;
-            if (!lyrcut) sum += alb * umu0 * fbeam * T / PI;
+            if (!lyrcut) sum += (srow ? srow[0] : alb) * umu0 * fbeam * T / PI;
           }
           if (thermal) {
             sum -= ld_rec(lr + C::SZ0 + NN + rb);
             sum -= ld_rec(lr + C::SZ1 + NN + rb) * tau;
           }
           sum += fisob;
-          if (thermal) sum += (1.0 - alb) * pbot;
+          if (thermal) sum += (srow ? srow[NN + 1] : 1.0 - alb) * pbot;
         }
         rhs = sum;
       }

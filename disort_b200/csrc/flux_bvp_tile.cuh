@@ -165,6 +165,11 @@ __device__ __forceinline__ void bvp_tile_instance(const FluxParams& p, const int
   const bool dlbc = (p.flags & DSP_FLAG_DIFFUSION_LOWER_BC) != 0;
   const double fbeam = rec[H_FBEAM], umu0 = rec[H_UMU0];
   const double alb = mode_m == 0 ? rec[H_ALB] : 0.0;
+  // bidirectional surface (general solver): this mode's table, row r =
+  // [beam | diffuse streams | emissivity]; it couples at every mode
+  const double* sft = nullptr;
+  if constexpr (GEN)
+    if (p.g.brdf) sft = p.g.brdf + (long long)slot * brdf_stride(N, p.g.numu);
   const bool beam = fbeam > 0.0;
   const double* taus = rec + il.tau_s;
   const double* btr = rec + il.btr;
@@ -293,6 +298,8 @@ __device__ __forceinline__ void bvp_tile_instance(const FluxParams& p, const int
             const int rb = rk, jq = NN + rb;
             const bool plain = lyrcut || dlbc;
             const double* Gl = lr + lrec_G(N);
+            const double* srow = sft ? sft + rb * brdf_row(N) : nullptr;
+            const double cpl = mode_m == 0 ? 2.0 : 1.0;  // 1 + delta_m0
             if (!in_next) {
 #pragma unroll
               for (int j = 0; j < CPT; ++j) {
@@ -300,8 +307,12 @@ __device__ __forceinline__ void bvp_tile_instance(const FluxParams& p, const int
                 double base = __ldg(Gl + jq * N + iq);
                 if (!plain) {
                   double refl = 0.0;
-                  for (int kk = 0; kk < NN; ++kk) refl += wt[kk] * mu[kk] * alb * __ldg(Gl + (NN - 1 - kk) * N + iq);
-                  base = base - 2.0 * refl;
+                  if (srow)
+                    for (int kk = 0; kk < NN; ++kk)
+                      refl += wt[kk] * mu[kk] * srow[1 + kk] * __ldg(Gl + (NN - 1 - kk) * N + iq);
+                  else
+                    for (int kk = 0; kk < NN; ++kk) refl += wt[kk] * mu[kk] * alb * __ldg(Gl + (NN - 1 - kk) * N + iq);
+                  base = base - cpl * refl;
                 }
                 a[k][j] = (iq < NN) ? base : base * Ecur[N - 1 - iq];
               }
@@ -328,20 +339,20 @@ __device__ __forceinline__ void bvp_tile_instance(const FluxParams& p, const int
                   if (beam) ps += SPH ? zsph(l, NN - 1 - jj, tau) : __ldg(lr + lrec_zb(N) + NN - 1 - jj) * T;
                   if (thermal)
                     ps += __ldg(lr + lrec_z0(N) + NN - 1 - jj) + __ldg(lr + lrec_z1(N) + NN - 1 - jj) * tau;
-                  refl += wt[jj] * mu[jj] * alb * ps;
+                  refl += wt[jj] * mu[jj] * (srow ? srow[1 + jj] : alb) * ps;
                 }
-                sum += 2.0 * refl;
+                sum += cpl * refl;
               }
               if (beam) {
                 sum -= SPH ? zsph(l, NN + rb, tau) : __ldg(lr + lrec_zb(N) + NN + rb) * T;
-                if (!lyrcut) sum += alb * umu0 * fbeam * T / PI;
+                if (!lyrcut) sum += (srow ? srow[0] : alb) * umu0 * fbeam * T / PI;
               }
               if (thermal) {
                 sum -= __ldg(lr + lrec_z0(N) + NN + rb);
                 sum -= __ldg(lr + lrec_z1(N) + NN + rb) * tau;
               }
               sum += fisob;
-              if (thermal) sum += (1.0 - alb) * pbot;
+              if (thermal) sum += (srow ? srow[NN + 1] : 1.0 - alb) * pbot;
             }
             rh[k] = sum;
           }

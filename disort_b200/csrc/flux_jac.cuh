@@ -148,6 +148,11 @@ __global__ void __launch_bounds__(64) flux_jac_kernel(FluxParams p, JacView jv) 
   auto out_taus = [&](int lu) { return GEN ? rec[gl_.utaus + lu] : taus[lu]; };
   const bool dlbc = (p.flags & DSP_FLAG_DIFFUSION_LOWER_BC) != 0;
   const double alb = rec[H_ALB];
+  // bidirectional surface (general solver): mode 0's table, row r =
+  // [beam | diffuse streams | emissivity]
+  const double* sft = nullptr;
+  if constexpr (GEN)
+    if (p.g.brdf) sft = p.g.brdf + (long long)blockIdx.x * brdf_stride(N, p.g.numu);
   const double wlo = p.wlo(i), whi = p.whi(i);
   const double* temp_in = GEN ? p.g.temp + p.g.in_off[i] + i : p.temp.row(i);
   const double dtau_last = dtau_s[L - 1];
@@ -241,7 +246,7 @@ __global__ void __launch_bounds__(64) flux_jac_kernel(FluxParams p, JacView jv) 
               v = 1.0;
               if (dtau_last > 0.0) v += mu[rb] * (1.0 / dtau_last);
             } else {
-              v = 1.0 - alb;
+              v = sft ? sft[rb * brdf_row(N) + NN + 1] : 1.0 - alb;
             }
           } else {
             double d0, d1;
@@ -254,7 +259,7 @@ __global__ void __launch_bounds__(64) flux_jac_kernel(FluxParams p, JacView jv) 
               for (int jq = 0; jq < NN; ++jq) {
                 double e0, e1;
                 dz(l, NN - 1 - jq, b0, b1, e0, e1);
-                refl += wt[jq] * mu[jq] * alb * (e0 + e1 * tb);
+                refl += wt[jq] * mu[jq] * (sft ? sft[rb * brdf_row(N) + 1 + jq] : alb) * (e0 + e1 * tb);
               }
               v = 2.0 * refl;
               v -= d0 + d1 * tb;

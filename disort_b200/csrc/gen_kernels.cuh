@@ -74,7 +74,10 @@ static __global__ void __launch_bounds__(128) gen_setup_kernel(FluxParams p) {
       if (dlbc && !thermal) bad = true;
       if (fbeam < 0.0) bad = true;
       if ((umu0 <= 0.0 || umu0 > 1.0) && fbeam > 0.0) bad = true;
-      if (alb < 0.0 || alb > 1.0) bad = true;
+      // the albedo is checked for a Lambertian surface only; a BRDF excludes the
+      // diffusion lower boundary (DisortConfig.cpp:144-146, 160-163)
+      if (g.brdf_type == DSP_BRDF_LAMBERTIAN && (alb < 0.0 || alb > 1.0)) bad = true;
+      if (g.brdf_type != DSP_BRDF_LAMBERTIAN && dlbc) bad = true;
       if ((fl & DSP_FLAG_DELTA_M_PLUS) && nmom < N + 1) bad = true;
       // bottom_radius > 0 with the pseudo-spherical beam (DisortConfig.cpp:189-196)
       if ((fl & DSP_FLAG_SPHERICAL_BEAM) && !(p.rbot(i) > 0.0)) bad = true;
@@ -269,7 +272,34 @@ __global__ void __launch_bounds__(128) gen_intensity_kernel(FluxParams p) {
   // bottom-boundary reflection of the mode-0 downward field (DisortSolver.cpp:3180-3218):
   // S = sum_iq mu w dfuint(iq), in the reference's order iq = NN-1 .. 0
   double bsum = 0.0;
-  const bool lambert_bnd = (m == 0) && !lyrcut && !dlbc;
+  // bidirectional surface: this mode's table; its user rows receive the
+  // reflected sum of each user angle in their last slot
+  double* sft = g.brdf ? g.brdf + (long long)slot * brdf_stride(N, g.numu) : nullptr;
+  const bool lambert_bnd = (m == 0) && !lyrcut && !dlbc && !sft;
+  if (sft && !lyrcut) {
+    // sum_iq (1 + delta_m0) R_m(mu_u, mu_iq) mu_iq w_iq dfuint(iq) per user angle
+    // (DisortSolver.cpp:3180-3218), dfuint as below, summed across the warp
+    const double* lr = LR(L - 1);
+    const double* G = lr + lrec_G(N);
+    const double* x = cc0 + (long long)(L - 1) * N;
+    double dfu = 0.0;
+    const int iq = lane;
+    if (iq < NN) {
+      for (int jq = 0; jq < NN; ++jq) dfu += G[iq * N + jq] * x[jq];
+      for (int jq = NN; jq < N; ++jq) dfu += G[iq * N + jq] * x[jq] * exp(-lr[lrec_eig(N) + jq] * dts[L - 1]);
+      if (beam) dfu += lr[lrec_zb(N) + iq] * btr[L];
+      if (thermal) dfu += lr[lrec_z0(N) + iq] + lr[lrec_z1(N) + iq] * taus[L];
+    }
+    const double cpl = m == 0 ? 2.0 : 1.0;
+    for (int iu = 0; iu < numu; ++iu) {
+      double* ur = sft + (NN + iu) * brdf_row(N);
+      double v = iq < NN ? cpl * ur[NN - iq] * mu[NN - iq - 1] * wt[NN - iq - 1] * dfu : 0.0;
+#pragma unroll
+      for (int off = 16; off > 0; off >>= 1) v += __shfl_xor_sync(0xffffffffu, v, off);
+      if (lane == 0) ur[NN + 2] = v;
+    }
+    __syncwarp();
+  }
   if (lambert_bnd) {
     const double* lr = LR(L - 1);
     const double* G = lr + lrec_G(N);
@@ -396,8 +426,15 @@ __global__ void __launch_bounds__(128) gen_intensity_kernel(FluxParams p) {
         if (dlbc) {
           if (lyrcut || m > 0) bnd_skip = true;
           else bndint = (rec[H_PBOT] + umv * rec[H_PBOTD]) * exp((ut - taus[L]) / umv);
-        } else if (lyrcut || m > 0) {
+        } else if (lyrcut || (m > 0 && !sft)) {
           bnd_skip = true;
+        } else if (sft) {
+          // bidirectional surface at user angles (DisortSolver.cpp:3213-3220); the
+          // isotropic bottom flux enters at every mode, as the reference adds it
+          const double* ur = sft + (NN + iu) * brdf_row(N);
+          const double bnddir = umu0 * fbeam / PI * ur[0] * btr[L];
+          const double emit = m == 0 ? ur[NN + 1] * rec[H_PBOT] : 0.0;
+          bndint = (ur[NN + 2] + bnddir + emit + rec[H_FISOB]) * exp((ut - taus[L]) / umv);
         } else {
           // Lambertian surface at user angles: set for mu > 0 only (DisortSolver.cpp:2655-2662)
           const double rho = umv > 0.0 ? alb : 0.0, em = umv > 0.0 ? 1.0 - alb : 0.0;

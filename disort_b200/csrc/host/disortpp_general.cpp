@@ -10,6 +10,7 @@
 #include <cmath>
 #include <mutex>
 #include <numeric>
+#include <stdexcept>
 #include <string>
 #include <vector>
 
@@ -193,7 +194,27 @@ void check_engine(const DisortConfig& c) {
                                 " is not supported by the B200 engine (supported: 4, 6, 8, 10, 12, 14, 16, 32, 64)");
   if (f.ibcnd == BoundaryConditionType::Special)
     throw std::invalid_argument("ibcnd=Special is not supported by the B200 engine");
-  if (!f.use_lambertian_surface) throw std::invalid_argument("BRDF surfaces are not supported by the B200 engine");
+  if (!f.use_lambertian_surface) {
+    // the model's spec must be present; the reference finds out inside its
+    // solve (bidirReflectivity, DisortSolver.cpp:2902-2936) with these errors
+    switch (f.brdf_type) {
+      case BrdfType::RPV:
+        if (!c.brdf.rpv) throw std::runtime_error("bidirReflectivity: RPV BRDF selected but rpv spec is null");
+        break;
+      case BrdfType::CoxMunk:
+        if (!c.brdf.cox_munk)
+          throw std::runtime_error("bidirReflectivity: Cox-Munk BRDF selected but cox_munk spec is null");
+        break;
+      case BrdfType::Ambrals:
+        if (!c.brdf.ambrals)
+          throw std::runtime_error("bidirReflectivity: Ross-Li/Ambrals BRDF selected but ambrals spec is null");
+        break;
+      case BrdfType::Hapke:
+        break;  // defaults apply without a spec
+      default:
+        throw std::runtime_error("bidirReflectivity: unknown BRDF type");
+    }
+  }
   if (f.intensity_corr_buras || f.intensity_corr_nakajima)
     throw std::invalid_argument("intensity corrections are not supported by the B200 engine");
   if (f.output_fourier_expansion)
@@ -275,6 +296,7 @@ struct GenPacked {
   std::vector<double> dtau, ssa, pmom, temp, zalt, utau, umu, phi;
   std::vector<double> lo, hi, alb, emis, fbeam, fisot, fisob;
   double mu0 = 0.5, phi0 = 0.0, ttop = 0.0, tbot = 0.0, rbot = 0.0;
+  double bpar[DSP_BRDF_PARAMS] = {};  // the surface model's parameters, shared by every band
 };
 
 // One batch for the whole loop.  `c` already carries the automatic fields.
@@ -385,6 +407,35 @@ dsp_general_batch pack_general(const DisortConfig& c, const std::vector<std::pai
   b.direct_beam_phi = {&pk.phi0, 0};
   b.temperature_top = {&pk.ttop, 0};
   b.temperature_bottom = {&pk.tbot, 0};
+  if (!f.use_lambertian_surface) {  // the spec in the C ABI's parameter order
+    b.brdf_type = static_cast<int32_t>(f.brdf_type);
+    double* q = pk.bpar;
+    switch (f.brdf_type) {
+      case BrdfType::RPV: {
+        const RpvBrdfSpec& r = *c.brdf.rpv;
+        const double v[7] = {r.rho0, r.k, r.theta, r.sigma, r.t1, r.t2, r.scale};
+        std::copy(v, v + 7, q);
+        break;
+      }
+      case BrdfType::CoxMunk: {
+        const CoxMunkBrdfSpec& r = *c.brdf.cox_munk;
+        const double v[5] = {r.u10, r.pcl, r.xsal, r.refractive_index, r.do_shadow ? 1.0 : 0.0};
+        std::copy(v, v + 5, q);
+        break;
+      }
+      case BrdfType::Ambrals: {
+        const AmbralsBrdfSpec& r = *c.brdf.ambrals;
+        q[0] = r.iso, q[1] = r.vol, q[2] = r.geo;
+        break;
+      }
+      default: {
+        const HapkeBrdfSpec r = c.brdf.hapke ? *c.brdf.hapke : HapkeBrdfSpec{};
+        q[0] = r.b0, q[1] = r.hh, q[2] = r.w;
+        break;
+      }
+    }
+    b.brdf_params = {q, 0};
+  }
   return b;
 }
 

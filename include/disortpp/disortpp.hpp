@@ -153,13 +153,13 @@ void solveFluxSpectralBandsInto(const DisortFluxConfig& config,
 
 // ---------------------------------------------------------------------------
 // General solver (DisortConfig.hpp:11-243, DisortResult.hpp:16-125,
-// DisortSolver.hpp:87): plane-parallel geometry, Lambertian surface, Fourier
-// azimuth modes, fluxes and intensities at user optical depths and angles.
+// DisortSolver.hpp:87): plane-parallel or pseudo-spherical beam geometry,
+// Lambertian or bidirectional (BRDF) surface, Fourier azimuth modes, fluxes,
+// intensities at user optical depths and angles, temperature Jacobians.
 // Configurations asking for what the engine does not implement (special
-// boundary conditions, BRDF surfaces, intensity corrections, pseudo-spherical
-// beam, temperature Jacobians, the Fourier-expansion output, stream counts
-// outside 4-16/32/64) pass validate() like in the reference and are rejected
-// with std::invalid_argument when solved.
+// boundary conditions, intensity corrections, the Fourier-expansion output,
+// stream counts outside 4-16/32/64) pass validate() like in the reference and
+// are rejected with std::invalid_argument when solved.
 // ---------------------------------------------------------------------------
 enum class BoundaryConditionType { General = 0, Special = 1 };
 enum class BrdfType { None = 0, RPV = 1, CoxMunk = 2, Ambrals = 3, Hapke = 4 };
@@ -194,8 +194,8 @@ struct BoundaryConditions {
   double surface_albedo = 0.0;
 };
 
-// BRDF parameter sets (DisortConfig.hpp:48-111).  Carried so that configurations
-// written for the reference compile; a non-Lambertian surface is rejected at solve.
+// BRDF parameter sets (DisortConfig.hpp:48-111), used by DisortSolver when
+// flags.use_lambertian_surface is false (the model chosen by flags.brdf_type).
 struct RpvBrdfSpec {
   double rho0 = 0.0, k = 0.0, theta = 0.0, sigma = 0.0, t1 = 0.0, t2 = 0.0, scale = 1.0;
 };

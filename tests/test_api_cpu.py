@@ -151,7 +151,6 @@ def test_general_engine_rejections_before_any_gpu_work():
     solver = disortpp.DisortSolver()
     cases = [
         (lambda c: setattr(c.flags, "ibcnd", disortpp.BoundaryConditionType.Special), "ibcnd=Special"),
-        (lambda c: setattr(c.flags, "use_lambertian_surface", False), "BRDF surfaces"),
         (lambda c: setattr(c.flags, "intensity_corr_nakajima", True), "intensity corrections"),
         (lambda c: setattr(c.flags, "output_fourier_expansion", True), "output_fourier_expansion"),
     ]
@@ -159,6 +158,17 @@ def test_general_engine_rejections_before_any_gpu_work():
         c = _general_cfg()
         mutate(c)
         with pytest.raises(ValueError, match=msg):
+            solver.solve(c)
+    # a bidirectional surface without a model, or without its spec, fails like the
+    # reference's bidirReflectivity (DisortSolver.cpp:2902-2936)
+    c = _general_cfg()
+    c.flags.use_lambertian_surface = False
+    with pytest.raises(RuntimeError, match="unknown BRDF type"):
+        solver.solve(c)
+    for kind, msg in ((disortpp.BrdfType.RPV, "rpv spec is null"), (disortpp.BrdfType.CoxMunk, "cox_munk spec"),
+                      (disortpp.BrdfType.Ambrals, "ambrals spec")):
+        c.flags.brdf_type = kind
+        with pytest.raises(RuntimeError, match=msg):
             solver.solve(c)
     c = disortpp.DisortConfig(2, 18)
     c.flags.comp_only_fluxes = True
