@@ -47,6 +47,7 @@ DEBUG_POISON_SCRATCH = 1  # dsp_context_set_debug
 GFLAG_USER_TAU = 1 << 8
 GFLAG_USER_MU = 1 << 9
 GFLAG_ONLY_FLUXES = 1 << 10
+GFLAG_INTENSITY_CORR = 1 << 11
 
 SUPPORTED_NSTR = (4, 6, 8, 10, 12, 14, 16, 32, 64)
 

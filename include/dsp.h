@@ -154,6 +154,15 @@ typedef struct dsp_flux_jac_out {
 #define DSP_GFLAG_USER_TAU         (1u << 8)  /* use_user_tau (else outputs at the layer boundaries) */
 #define DSP_GFLAG_USER_MU          (1u << 9)  /* use_user_mu */
 #define DSP_GFLAG_ONLY_FLUXES      (1u << 10) /* comp_only_fluxes */
+/*
+ * intensity_corr_buras with the Nakajima-Tanaka method (intensity_corr_nakajima,
+ * or no tabulated phase function): after the mode loop the intensities get the
+ * TMS/IMS corrections where DisortSolver applies them (delta-M scaling, a beam,
+ * scattering; DisortSolver.cpp:352-368, 3274-3530) and, over a BRDF surface,
+ * the correction of the reflected beam (delta-M+ off; :376-391, 3751-3810).
+ * Fluxes and azimuthal averages are unchanged.
+ */
+#define DSP_GFLAG_INTENSITY_CORR   (1u << 11)
 
 typedef struct dsp_general_batch {
   int32_t n_inst;

@@ -22,6 +22,7 @@ struct GeneralInstance {
   double radius = 0.0;           // bottom_radius
   const double* zalt = nullptr;  // level_altitudes [L+1] (spherical only)
   double accur = 0.0;
+  bool corr = false;             // intensity_corr_buras with the Nakajima-Tanaka method
   int brdf = 0;                  // 0: Lambertian; else the BrdfType (RPV 1, CoxMunk 2, Ambrals 3, Hapke 4)
   const double* bp = nullptr;    // its parameters (SurfaceTables, oracle_common.hpp)
   double wlo = 0, whi = 0, alb = 0, emis = 1, fbeam = 0, umu0 = 0.5, phi0 = 0, fisot = 0, fisob = 0, ttop = 0, tbot = 0;
@@ -85,6 +86,141 @@ inline int validate_general(const GeneralInstance& c) {
   // boundary of the C ABI: user optical depths must be given when requested
   if (c.user_tau && (c.ntau <= 0 || !c.utau)) return DSP_ERR_INVALID_INPUT;
   return DSP_OK;
+}
+
+// xiFunc (DisortSolver.cpp:3274-3285), eq. STWL (72)
+inline double nt_xi(double umu1, double umu2, double tau) {
+  const double x1 = (umu2 - umu1) / (umu2 * umu1);
+  const double exp1 = std::exp(-tau / umu1);
+  if (x1 != 0.0) return ((tau * x1 - 1.0) * std::exp(-tau / umu2) + exp1) / (x1 * x1 * umu1 * umu2);
+  return tau * tau * exp1 / (2.0 * umu1 * umu2);
+}
+
+// singleScat (DisortSolver.cpp:3287-3328): the single-scattered intensity of
+// the beam at scaled depth tau_user, eqs. STWL (65b,d,e).  phase, omega are
+// 1-based over layers; tau is the cumulative scaled depth at the levels.
+inline double nt_single_scat(double dither, int layru, int nl, const double* phase, const double* omega,
+                             const double* tau, double umu, double umu0, double tau_user, double fbeam) {
+  const double four_pi = 4.0 * M_PI;
+  double ans = 0.0, exp0 = std::exp(-tau_user / umu0);
+  if (std::abs(umu + umu0) <= dither) {
+    for (int lyr = 1; lyr <= layru - 1; ++lyr) ans += omega[lyr] * phase[lyr] * (tau[lyr] - tau[lyr - 1]);
+    return fbeam / (four_pi * umu0) * exp0 * (ans + omega[layru] * phase[layru] * (tau_user - tau[layru - 1]));
+  }
+  if (umu > 0.0) {
+    for (int lyr = layru; lyr <= nl; ++lyr) {
+      const double exp1 = std::exp(-((tau[lyr] - tau_user) / umu + tau[lyr] / umu0));
+      ans += omega[lyr] * phase[lyr] * (exp0 - exp1);
+      exp0 = exp1;
+    }
+  } else {
+    for (int lyr = layru; lyr >= 1; --lyr) {
+      const double exp1 = std::exp(-((tau[lyr - 1] - tau_user) / umu + tau[lyr - 1] / umu0));
+      ans += omega[lyr] * phase[lyr] * (exp0 - exp1);
+      exp0 = exp1;
+    }
+  }
+  return ans * fbeam / (four_pi * (1.0 + umu / umu0));
+}
+
+// applyIntensityCorrection (DisortSolver.cpp:3403-3530) with secondaryScat
+// (:3330-3401): Nakajima-Tanaka TMS (exact single scattering in place of the
+// delta-M one) and IMS (secondary scattering in the aureole of the beam).
+// pm: unscaled moments [L][pc] (moment 0 = 1); I3(lu, iu, j) the intensities.
+template <class Acc>
+inline void nakajima_tanaka(const GeneralInstance& c, int ncut, bool lyrcut, int numu, int nphi, int ntau,
+                            const std::vector<double>& umu, const std::vector<double>& utau,
+                            const std::vector<double>& utaus, const std::vector<int>& lyr,
+                            const std::vector<double>& tauc, const std::vector<double>& taus,
+                            const std::vector<double>& fsc, const std::vector<double>& ws,
+                            const std::vector<double>& pm, Acc&& I3) {
+  const int N = c.N, nmom = c.nmom, pc = c.pc;
+  auto PM = [&](int k, int lc) { return pm[(size_t)lc * pc + k]; };
+  const double dither = 100.0 * std::numeric_limits<double>::epsilon();
+  const double dtheta = 10.0, deg = std::acos(-1.0) / 180.0, tiny = 1.0e-4;
+  std::vector<double> phasa(ncut + 1), phasm(ncut + 1), phast(ncut + 1), ssa1(ncut + 1), opr1(ncut + 1);
+  for (int lc = 1; lc <= ncut; ++lc) {
+    ssa1[lc] = c.ssa[lc - 1];
+    opr1[lc] = ws[lc - 1];
+  }
+  // secondaryScat: the IMS term of eq. STWL (A.13) at output depth lu
+  auto secondary = [&](int iu, int lu, double ctheta, int layru) {
+    const double ut = utau[lu];
+    double dtau = ut - tauc[layru];
+    double wbar = c.ssa[layru] * dtau;
+    double fbar = fsc[layru] * wbar;
+    double stau = dtau;
+    for (int l = 0; l < layru; ++l) {
+      wbar += c.dtau[l] * c.ssa[l];
+      fbar += c.dtau[l] * c.ssa[l] * fsc[l];
+      stau += c.dtau[l];
+    }
+    if (wbar <= tiny || fbar <= tiny || stau <= tiny || c.fbeam <= tiny) return 0.0;
+    fbar /= wbar;
+    wbar /= stau;
+    double pspike = 1.0, gbar = 1.0, plm1 = 1.0, plm2 = 0.0;
+    for (int k = 1; k <= N - 1; ++k) {
+      const double pl = ((2 * k - 1) * ctheta * plm1 - (k - 1) * plm2) / k;
+      plm2 = plm1;
+      plm1 = pl;
+      pspike += gbar * (2.0 - gbar) * (double)(2 * k + 1) * pl;
+    }
+    for (int k = N; k <= nmom; ++k) {
+      const double pl = ((2 * k - 1) * ctheta * plm1 - (k - 1) * plm2) / k;
+      plm2 = plm1;
+      plm1 = pl;
+      dtau = ut - tauc[layru];
+      gbar = PM(k, layru) * c.ssa[layru] * dtau;
+      for (int l = 0; l < layru; ++l) gbar += PM(k, l) * c.ssa[l] * c.dtau[l];
+      const double tmp = fbar * wbar * stau;
+      gbar = tmp <= tiny ? 0.0 : gbar / tmp;
+      pspike += gbar * (2.0 - gbar) * (double)(2 * k + 1) * pl;
+    }
+    const double umu0p = c.umu0 / (1.0 - fbar * wbar);
+    return c.fbeam / (4.0 * M_PI) * (fbar * wbar) * (fbar * wbar) / (1.0 - fbar * wbar) * pspike *
+           nt_xi(-umu[iu], umu0p, ut);
+  };
+  for (int iu = 0; iu < numu; ++iu) {
+    double theta0 = 0.0, thetap = 0.0;
+    if (umu[iu] < 0.0) {
+      theta0 = std::acos(-c.umu0) / deg;
+      thetap = std::acos(umu[iu]) / deg;
+    }
+    for (int jp = 0; jp < nphi; ++jp) {
+      const double phirad = (c.phi[jp] - c.phi0) * deg;
+      const double ctheta =
+          -c.umu0 * umu[iu] + std::sqrt((1.0 - c.umu0 * c.umu0) * (1.0 - umu[iu] * umu[iu])) * std::cos(phirad);
+      for (int lc = 1; lc <= ncut; ++lc) phasa[lc] = phasm[lc] = 1.0;
+      double plm1 = 1.0, plm2 = 0.0;
+      for (int k = 1; k <= nmom; ++k) {
+        const double pl = ((2 * k - 1) * ctheta * plm1 - (k - 1) * plm2) / k;
+        plm2 = plm1;
+        plm1 = pl;
+        for (int lc = 1; lc <= ncut; ++lc) phasa[lc] += (double)(2 * k + 1) * pl * PM(k, lc - 1);
+        if (k <= N - 1)
+          for (int lc = 1; lc <= ncut; ++lc) {
+            const double fl = fsc[lc - 1];
+            phasm[lc] += (double)(2 * k + 1) * pl * (PM(k, lc - 1) - fl) / (1.0 - fl);
+          }
+      }
+      for (int lc = 1; lc <= ncut; ++lc) phast[lc] = phasa[lc] / (1.0 - fsc[lc - 1] * c.ssa[lc - 1]);
+      for (int lu = 0; lu < ntau; ++lu) {
+        if (lyrcut && lyr[lu] >= ncut) continue;
+        const double exact = nt_single_scat(dither, lyr[lu] + 1, ncut, phast.data(), ssa1.data(), taus.data(),
+                                            umu[iu], c.umu0, utaus[lu], c.fbeam);
+        const double scaled = nt_single_scat(dither, lyr[lu] + 1, ncut, phasm.data(), opr1.data(), taus.data(),
+                                             umu[iu], c.umu0, utaus[lu], c.fbeam);
+        I3(lu, iu, jp) += exact - scaled;
+      }
+      if (umu[iu] < 0.0 && std::abs(theta0 - thetap) <= dtheta) {
+        const int ltau = utau[0] <= dither ? 1 : 0;
+        for (int lu = ltau; lu < ntau; ++lu) {
+          if (lyrcut && lyr[lu] >= ncut) continue;
+          I3(lu, iu, jp) -= secondary(iu, lu, ctheta, lyr[lu]);
+        }
+      }
+    }
+  }
 }
 
 class GeneralOracle {
@@ -293,10 +429,15 @@ inline int GeneralOracle::solve(const GeneralInstance& cin, const GeneralOutput&
   // surface reflectance and emissivity of each mode (computeSurfaceBidir)
   SurfaceTables sfc;
   sfc.init(NN, do_int ? numu : 0);
+  std::vector<double> brdf_beam_u((size_t)numu * N, 0.0);
   const bool lamb = c.brdf == BRDF_LAMBERT;
   for (int m = 0; m <= naz; ++m) {
     const double d0 = (m == 0) ? 1.0 : 0.0;
     sfc.fill(c.brdf, c.bp, c.alb, m, mu.data(), umu.data(), do_int, c.fbeam, c.umu0);
+    // the beam's surface coefficient of each mode at the user angles, for the
+    // BRDF intensity correction (DisortSolver.cpp:306-313)
+    if (!lamb && do_int && c.fbeam > 0.0)
+      for (int iu = 0; iu < numu; ++iu) brdf_beam_u[(size_t)iu * N + m] = sfc.RU(iu, 0);
     legendre_flat(N, m, N, N - 1, mu.data(), ylq.data());
     auto Yq = [&](int l, int i) { return ylq[(size_t)l * N + i]; };
     if (do_int) legendre_flat(numu, m, numu, N - 1, umu.data(), ylu.data());
@@ -1020,6 +1161,36 @@ inline int GeneralOracle::solve(const GeneralInstance& cin, const GeneralOutput&
         if (c.accur > 0.0) {
           if (maxc <= c.accur) ++kconv;
           if (kconv >= 2) break;
+        }
+      }
+    }
+  }
+  // ---- intensity corrections, after the mode loop (DisortSolver.cpp:352-392) ----
+  if (do_int && c.corr && c.fbeam > 0.0) {
+    bool scat_yes = false;
+    for (int lc = 0; lc < L; ++lc)
+      if (c.ssa[lc] > 0.0) scat_yes = true;
+    if (deltam && scat_yes) nakajima_tanaka(c, ncut, lyrcut, numu, nphi, ntau, umu, utau, utaus, lyr, tauc, taus,
+                                            fsc, ws, pm, I3);
+    if (!dmplus && !lamb) {
+      // applyBrdfIntensityCorrection (DisortSolver.cpp:3751-3810): the exact
+      // reflectance of the beam against its Fourier sum over the modes run
+      for (int iu = 0; iu < numu; ++iu) {
+        const double u = umu[iu];
+        if (u <= 0.0) continue;
+        for (int j = 0; j < nphi; ++j) {
+          const double dphi = (c.phi[j] - c.phi0) * (M_PI / 180.0);
+          const double exact = brdf_value(c.brdf, c.bp, u, c.umu0, dphi);
+          if (exact < 0.0) continue;
+          double approx = 0.0;
+          for (int m = 0; m < N; ++m) approx += brdf_beam_u[(size_t)iu * N + m] * std::cos(static_cast<double>(m) * dphi);
+          const double drho = exact - approx;
+          if (std::abs(drho) < 1e-15) continue;
+          const double to_bottom = std::exp(-taus[ncut] / c.umu0);
+          for (int lu = 0; lu < ntau; ++lu) {
+            if (lyrcut && lyr[lu] >= ncut) continue;
+            I3(lu, iu, j) += c.umu0 * c.fbeam * drho * to_bottom * std::exp((utaus[lu] - taus[ncut]) / u);
+          }
         }
       }
     }

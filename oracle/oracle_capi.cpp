@@ -143,6 +143,7 @@ int oracle_general_bands_solve_jac(const dsp_general_batch* b, const dsp_general
         c.user_tau = (fl & DSP_GFLAG_USER_TAU) != 0;
         c.user_mu = (fl & DSP_GFLAG_USER_MU) != 0;
         c.only_fluxes = (fl & DSP_GFLAG_ONLY_FLUXES) != 0;
+        c.corr = (fl & DSP_GFLAG_INTENSITY_CORR) != 0;
         c.accur = b->accuracy_fourier_series;
         c.wlo = scalar(b->wavenumber_low, i, 0.0);
         c.whi = scalar(b->wavenumber_high, i, 0.0);

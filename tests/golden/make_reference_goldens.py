@@ -124,6 +124,31 @@ CASES = [
          fbeam=200.0, umu0=0.5, brdf=(4, [1.0, 0.06, 0.6]), corr=True, utau=[0.0, 1.0, 10.0],
          umu=[-1.0, -0.1, 0.1, 1.0], phi=[90.0], thermal=True, temperature=[250.0, 300.0], wn=(0.0, 50000.0),
          btemp=300.0, ttemp=250.0, fisot=100.0 / PI),
+    # Nakajima-Tanaka intensity correction (makeICTestConfig1Layer, test_solver.cpp:3779-3825:
+    # 16 streams, 16 moments, intensity_corr_buras and intensity_corr_nakajima on,
+    # mu_user kUmu6, phi 0, black surface)
+    dict(test="IntensityCorrectionIso1a", N=16, L=1, nmom=16, dtau=[0.03125], ssa=[0.2], phase=[("iso",)],
+         fbeam=PI / 0.1, umu0=0.1, corr=True, utau=[0.0, 0.03125],
+         umu=[-1.0, -0.5, -0.1, 0.1, 0.5, 1.0], phi=[0.0]),
+    dict(test="IntensityCorrectionIso1b", N=16, L=1, nmom=16, dtau=[0.03125], ssa=[1.0], phase=[("iso",)],
+         fbeam=PI / 0.1, umu0=0.1, corr=True, utau=[0.0, 0.03125],
+         umu=[-1.0, -0.5, -0.1, 0.1, 0.5, 1.0], phi=[0.0]),
+    dict(test="IntensityCorrectionIso1d", N=16, L=1, nmom=16, dtau=[32.0], ssa=[0.2], phase=[("iso",)],
+         fbeam=PI / 0.1, umu0=0.1, corr=True, utau=[0.0, 32.0],
+         umu=[-1.0, -0.5, -0.1, 0.1, 0.5, 1.0], phi=[0.0]),
+    dict(test="IntensityCorrectionIso1e", N=16, L=1, nmom=16, dtau=[32.0], ssa=[1.0], phase=[("iso",)],
+         fbeam=PI / 0.1, umu0=0.1, corr=True, utau=[0.0, 32.0],
+         umu=[-1.0, -0.5, -0.1, 0.1, 0.5, 1.0], phi=[0.0]),
+    dict(test="IntensityCorrectionHG3a", N=16, L=1, nmom=16, dtau=[1.0], ssa=[1.0], phase=[("hg", 0.75)],
+         fbeam=PI, umu0=1.0, corr=True, utau=[0.0, 1.0],
+         umu=[-1.0, -0.5, -0.1, 0.1, 0.5, 1.0], phi=[0.0]),
+    dict(test="IntensityCorrectionHG3b", N=16, L=1, nmom=16, dtau=[8.0], ssa=[1.0], phase=[("hg", 0.75)],
+         fbeam=PI, umu0=1.0, corr=True, utau=[0.0, 8.0],
+         umu=[-1.0, -0.5, -0.1, 0.1, 0.5, 1.0], phi=[0.0]),
+    # disotest 12a (test_solver.cpp:3637-3700): 20 streams (oracle only; the engine takes 4-16, 32, 64)
+    dict(test="ValidationDisotest12a", N=20, L=1, nmom=20, dtau=[20.1], ssa=[0.5], phase=[("hg", 0.9)],
+         fbeam=1.0, umu0=1.0, albedo=1.0, corr=True, utau=[0.0, 10.0, 19.9, 20.1],
+         umu=[-1.0, -0.1, 0.1, 1.0], phi=[0.0]),
     # pseudo-spherical beam (test_solver.cpp:4459-4533): altitudes 60/30/0 km, radius 6371 km
     dict(test="SphericalGeometry", N=16, L=2, nmom=0, dtau=[0.5, 1.0], ssa=[0.9, 0.8], phase=[("hg", 0.8)],
          fbeam=1.0, umu0=0.5, albedo=0.1, spherical=True, zalt=[60.0, 30.0, 0.0], radius=6371.0,

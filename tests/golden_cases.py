@@ -14,7 +14,16 @@ GOLDEN = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden", "ref
 def load_cases() -> list:
     """The plane-parallel cases over a Lambertian surface (every solver path supports them)."""
     with open(GOLDEN) as f:
-        return [c for c in json.load(f)["cases"] if not c.get("use_spherical_beam") and not c.get("brdf_type")]
+        return [c for c in json.load(f)["cases"]
+                if not c.get("use_spherical_beam") and not c.get("brdf_type") and not c.get("intensity_corrected")]
+
+
+def load_corrected_cases(engine_only: bool = False) -> list:
+    """Lambertian cases run with the Nakajima-Tanaka intensity correction (general
+    solver only); engine_only drops stream counts the engine does not take."""
+    with open(GOLDEN) as f:
+        cases = [c for c in json.load(f)["cases"] if c.get("intensity_corrected") and not c.get("brdf_type")]
+    return [c for c in cases if not engine_only or c["num_streams"] in (4, 6, 8, 10, 12, 14, 16, 32, 64)]
 
 
 def load_brdf_cases() -> list:
@@ -89,6 +98,8 @@ def general_instance(c: dict) -> tuple[dict, int]:
         isotropic_flux_top=c["isotropic_flux_top"],
         temperature_top=c["temperature_top"], temperature_bottom=c["temperature_bottom"],
     )
+    if c.get("intensity_corrected"):
+        flags |= capi.GFLAG_INTENSITY_CORR
     if c.get("brdf_type"):
         inst["brdf_type"] = c["brdf_type"]
         inst["brdf_params"] = c["brdf_params"]

@@ -196,9 +196,8 @@ BRDF_CASES = gc.load_brdf_cases()
 
 @pytest.mark.parametrize("case", BRDF_CASES, ids=[c["name"] for c in BRDF_CASES])
 def test_general_oracle_brdf_goldens(case):
-    """Bidirectional surfaces (Hapke, RPV) against the reference's C-DISORT goldens.
-    Cases run with the intensity corrections on compare their fluxes only (the
-    corrections change intensities, not fluxes)."""
+    """Bidirectional surfaces (Hapke, RPV) against the reference's C-DISORT goldens;
+    disotest 6d-6h with the BRDF correction of the reflected beam."""
     inst, flags = gc.general_instance(case)
     o = oracle_lib.general_solve(capi.pack_general([inst], flags))
     assert o["status"][0] == 0
@@ -206,11 +205,30 @@ def test_general_oracle_brdf_goldens(case):
     for e in case["expect_flux"]:
         v = o[e["field"]][0, e["index"]]
         assert abs(v - e["value"]) <= e["tol"], (e, v)
-    if case["intensity_corrected"]:
-        return
     for e in case["expect_intensity"]:
         v = o["intensity"][0, e["lu"], e["iu"], e["j"]]
         assert abs(v - e["value"]) <= e["tol"], (e, v)
+
+
+CORR_CASES = gc.load_corrected_cases()
+
+
+@pytest.mark.parametrize("case", CORR_CASES, ids=[c["name"] for c in CORR_CASES])
+def test_general_oracle_intensity_correction_goldens(case):
+    """The Nakajima-Tanaka correction against the reference's C-DISORT goldens
+    (IntensityCorrection*, disotest 12a); without it the intensities miss them."""
+    inst, flags = gc.general_instance(case)
+    o = oracle_lib.general_solve(capi.pack_general([inst], flags))
+    assert o["status"][0] == 0
+    for e in case["expect_flux"]:
+        v = o[e["field"]][0, e["index"]]
+        assert abs(v - e["value"]) <= e["tol"], (e, v)
+    for e in case["expect_intensity"]:
+        v = o["intensity"][0, e["lu"], e["iu"], e["j"]]
+        assert abs(v - e["value"]) <= e["tol"], (e, v)
+    plain = oracle_lib.general_solve(capi.pack_general([inst], flags & ~capi.GFLAG_INTENSITY_CORR))
+    np.testing.assert_array_equal(plain["flux_up"], o["flux_up"])
+    np.testing.assert_array_equal(plain["intensity_azimuth_avg"], o["intensity_azimuth_avg"])
 
 
 @pytest.mark.parametrize("model", [capi.BRDF_RPV, capi.BRDF_COX_MUNK, capi.BRDF_AMBRALS, capi.BRDF_HAPKE])
