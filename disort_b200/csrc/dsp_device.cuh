@@ -173,8 +173,14 @@ struct GenView {
 // quadrature angles, r = NN + iu the user polar angles; each row holds
 // [beam reflectance | diffuse reflectance of incoming stream 0..NN-1 |
 //  directional emissivity (mode 0) | the intensity kernel's reflected-field sum].
+// After the rows, kept across the modes: the beam reflectance at each user angle
+// for every mode run, [numu][N] (zero for modes not run), which the BRDF
+// intensity correction sums (DisortSolver.cpp:306-313, 3783-3787).
 __host__ __device__ constexpr int brdf_row(int N) { return N / 2 + 3; }
-__host__ __device__ constexpr int brdf_stride(int N, int numu) { return round4((N / 2 + numu) * brdf_row(N)); }
+__host__ __device__ constexpr int brdf_beam_modes(int N, int numu) { return (N / 2 + numu) * brdf_row(N); }
+__host__ __device__ constexpr int brdf_stride(int N, int numu) {
+  return round4(brdf_beam_modes(N, numu) + numu * N);
+}
 
 struct FluxParams {
   int n;          // instances in this launch

@@ -16,6 +16,7 @@
 #include "flux_layer.cuh"
 #include "flux_sph.cuh"
 #include "gen_brdf.cuh"
+#include "gen_intcor.cuh"
 #include "gen_kernels.cuh"
 
 using namespace dsp;
@@ -238,6 +239,11 @@ dsp_status launch_general_chunk(dsp_context ctx, FluxParams p, long long layers,
       KernelTimer kt(ctx, "gen_intensity_kernel");
       gen_intensity_kernel<N><<<(p.n + 3) / 4, 128, 0, s>>>(p);
     }
+  }
+  if ((p.flags & DSP_GFLAG_INTENSITY_CORR) && p.g.numu > 0) {
+    // after the whole Fourier sum: the intensity corrections
+    KernelTimer kt(ctx, "gen_intcor_kernel");
+    gen_intcor_kernel<N><<<p.n, 128, 0, s>>>(p);
   }
   cudaError_t e = cudaGetLastError();
   if (e != cudaSuccess) return cuda_fail(ctx, e, "general kernel launch");

@@ -181,6 +181,13 @@ __global__ void __launch_bounds__(128) gen_brdf_kernel(FluxParams p) {
       v = fac * s;
     }
     tab[r * RW + c] = v;
+    // the beam column of the user rows, per mode, for the intensity correction
+    if (c == 0 && r >= NN) {
+      double* modes = tab + brdf_beam_modes(N, g.numu) + (r - NN) * N;
+      if (m == 0)
+        for (int mm = 1; mm < N; ++mm) modes[mm] = 0.0;
+      modes[m] = v;
+    }
   }
   // directional emissivity (mode 0); the azimuth nodes x_j run over both halves
   for (int r = 0; r < rows; ++r) {

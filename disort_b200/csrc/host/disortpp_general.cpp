@@ -215,8 +215,12 @@ void check_engine(const DisortConfig& c) {
         throw std::runtime_error("bidirReflectivity: unknown BRDF type");
     }
   }
-  if (f.intensity_corr_buras || f.intensity_corr_nakajima)
-    throw std::invalid_argument("intensity corrections are not supported by the B200 engine");
+  // the Nakajima-Tanaka correction runs on the engine; the Buras-Emde one
+  // (DisortSolver.cpp:362-367: a tabulated phase function and no
+  // intensity_corr_nakajima) does not
+  if (f.intensity_corr_buras && !f.intensity_corr_nakajima && c.num_phase_func_angles > 0)
+    throw std::invalid_argument(
+        "the Buras-Emde intensity correction (tabulated phase function) is not supported by the B200 engine");
   if (f.output_fourier_expansion)
     throw std::invalid_argument("output_fourier_expansion is not supported by the B200 engine");
   // validate() does not look at the user optical depths; the reference reads
@@ -314,7 +318,8 @@ dsp_general_batch pack_general(const DisortConfig& c, const std::vector<std::pai
             (f.index_from_bottom ? DSP_FLAG_INDEX_FROM_BOTTOM : 0u) | (f.use_user_tau ? DSP_GFLAG_USER_TAU : 0u) |
             (f.use_user_mu && !f.comp_only_fluxes ? DSP_GFLAG_USER_MU : 0u) |
             (f.comp_only_fluxes ? DSP_GFLAG_ONLY_FLUXES : 0u) |
-            (f.use_spherical_beam ? DSP_FLAG_SPHERICAL_BEAM : 0u);
+            (f.use_spherical_beam ? DSP_FLAG_SPHERICAL_BEAM : 0u) |
+            (f.intensity_corr_buras ? DSP_GFLAG_INTENSITY_CORR : 0u);
   pk.nstr.assign(n, c.num_streams);
   pk.nlyr.assign(n, L);
   pk.nmom.assign(n, c.num_phase_func_moments);

@@ -254,10 +254,17 @@ inline int GeneralOracle::solve(const GeneralInstance& cin, const GeneralOutput&
       c.zalt = rza.data();
     }
     if (c.user_tau && c.utau && c.ntau > 0) {
-      double total = 0.0;
-      for (int lc = 0; lc < L; ++lc) total += c.dtau[lc];
+      // the column total and the converted depths rounded to double at every
+      // step, as the reference computes them: the extended-precision build
+      // would otherwise turn a user depth equal to the total into a tiny
+      // negative depth above the top of the column
+      volatile double total = 0.0;
+      for (int lc = 0; lc < L; ++lc) total = total + c.dtau[lc];
       rut.assign(c.utau, c.utau + c.ntau);
-      for (auto& t : rut) t = total - t;
+      for (auto& t : rut) {
+        volatile double v = total - t;
+        t = v;
+      }
       std::reverse(rut.begin(), rut.end());
       c.utau = rut.data();
     }

@@ -151,7 +151,8 @@ def test_general_engine_rejections_before_any_gpu_work():
     solver = disortpp.DisortSolver()
     cases = [
         (lambda c: setattr(c.flags, "ibcnd", disortpp.BoundaryConditionType.Special), "ibcnd=Special"),
-        (lambda c: setattr(c.flags, "intensity_corr_nakajima", True), "intensity corrections"),
+        (lambda c: (setattr(c.flags, "intensity_corr_buras", True), setattr(c, "num_phase_func_angles", 8)),
+         "Buras-Emde intensity correction"),
         (lambda c: setattr(c.flags, "output_fourier_expansion", True), "output_fourier_expansion"),
     ]
     for mutate, msg in cases:

@@ -48,9 +48,8 @@ def test_brdf_reference_goldens(case):
         assert_parity_general(got, ref, case["name"])
     for e in case["expect_flux"]:
         assert abs(got[e["field"]][0, e["index"]] - e["value"]) <= e["tol"]
-    if not case["intensity_corrected"]:
-        for e in case["expect_intensity"]:
-            assert abs(got["intensity"][0, e["lu"], e["iu"], e["j"]] - e["value"]) <= e["tol"]
+    for e in case["expect_intensity"]:
+        assert abs(got["intensity"][0, e["lu"], e["iu"], e["j"]] - e["value"]) <= e["tol"]
 
 
 def brdf_mix(model, n, seed, nstr, layers=(3, 14), thermal=False, params=None):
