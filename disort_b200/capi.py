@@ -48,6 +48,7 @@ GFLAG_USER_TAU = 1 << 8
 GFLAG_USER_MU = 1 << 9
 GFLAG_ONLY_FLUXES = 1 << 10
 GFLAG_INTENSITY_CORR = 1 << 11
+GFLAG_INTENSITY_CORR_BE = 1 << 12
 
 SUPPORTED_NSTR = (4, 6, 8, 10, 12, 14, 16, 32, 64)
 
@@ -210,7 +211,9 @@ class GeneralBatch(ctypes.Structure):
         ("temperature", c_void_p),
         ("tau_user", DArray), ("mu_user", DArray), ("phi_user", DArray),
     ] + [(f, DArray) for f in GENERAL_SCALAR_FIELDS] + [("level_altitudes", c_void_p), ("bottom_radius", DArray),
-                                                        ("brdf_type", c_int32), ("brdf_params", DArray)]
+                                                        ("brdf_type", c_int32), ("brdf_params", DArray),
+                                                        ("num_phase_func_angles", c_int32),
+                                                        ("mu_phase_function", DArray), ("phase_function", c_void_p)]
 
 
 class GeneralOut(ctypes.Structure):
@@ -296,6 +299,16 @@ def pack_general(insts: list, flags: int, accuracy_fourier_series: float = 0.0,
             v = np.asarray(c.get("brdf_params", ()), dtype=np.float64).reshape(-1)
             bp[i, :v.size] = v
         d["brdf_params"] = bp
+    # tabulated phase function (Buras-Emde correction): angles shared or per instance,
+    # values per layer like delta_tau
+    if insts[0].get("mu_phase_function") is not None:
+        na = len(insts[0]["mu_phase_function"])
+        d["num_phase_func_angles"] = na
+        d["mu_phase_function"] = _user_list(insts, "mu_phase_function", na)
+        pf = np.zeros((tot, na))
+        for i, c in enumerate(insts):
+            pf[off[i]:off[i + 1]] = np.asarray(c["phase_function"], dtype=np.float64).reshape(-1, na)
+        d["phase_function"] = pf
     d["ntau_out"] = ntau if flags & GFLAG_USER_TAU else int(L.max()) + 1
     d["numu_out"] = numu if (flags & GFLAG_USER_MU and not flags & GFLAG_ONLY_FLUXES) else int(N.max())
     return d
@@ -332,6 +345,11 @@ def make_general_batch(d: dict) -> tuple[GeneralBatch, list]:
         a = d["bottom_radius"]
         b.bottom_radius = DArray(_ptr(a), 1 if a.shape[0] > 1 else 0)
     b.brdf_type = d.get("brdf_type", BRDF_LAMBERTIAN)
+    if "mu_phase_function" in d:
+        b.num_phase_func_angles = d["num_phase_func_angles"]
+        a, stride = d["mu_phase_function"]
+        b.mu_phase_function = DArray(_ptr(a), stride)
+        b.phase_function = _ptr(d["phase_function"])
     if "brdf_params" in d:
         a = d["brdf_params"]
         b.brdf_params = DArray(_ptr(a), BRDF_PARAMS if a.shape[0] > 1 else 0)

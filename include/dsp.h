@@ -163,6 +163,15 @@ typedef struct dsp_flux_jac_out {
  * Fluxes and azimuthal averages are unchanged.
  */
 #define DSP_GFLAG_INTENSITY_CORR   (1u << 11)
+/*
+ * With DSP_GFLAG_INTENSITY_CORR: the Buras-Emde method instead
+ * (intensity_corr_buras without intensity_corr_nakajima and with a tabulated
+ * phase function, DisortSolver.cpp:362-367, 3532-3749): the exact single
+ * scattering from the tabulated phase function, the secondary scattering from
+ * its residual after the delta-M truncation.  Needs num_phase_func_angles >= 2,
+ * mu_phase_function (increasing cosines) and phase_function.
+ */
+#define DSP_GFLAG_INTENSITY_CORR_BE (1u << 12)
 
 typedef struct dsp_general_batch {
   int32_t n_inst;
@@ -206,6 +215,11 @@ typedef struct dsp_general_batch {
    */
   int32_t brdf_type;
   dsp_darray brdf_params;               /* [DSP_BRDF_PARAMS] */
+  /* tabulated phase function (DisortConfig::mu_phase_function, ::phase_function),
+     read with DSP_GFLAG_INTENSITY_CORR_BE only */
+  int32_t num_phase_func_angles;
+  dsp_darray mu_phase_function;         /* [num_phase_func_angles] per instance or shared */
+  const double* phase_function;         /* [total layers][num_phase_func_angles], layers like delta_tau */
 } dsp_general_batch;
 
 /* brdf_type values: the BrdfType enum of DisortConfig.hpp */

@@ -22,7 +22,11 @@ struct GeneralInstance {
   double radius = 0.0;           // bottom_radius
   const double* zalt = nullptr;  // level_altitudes [L+1] (spherical only)
   double accur = 0.0;
-  bool corr = false;             // intensity_corr_buras with the Nakajima-Tanaka method
+  bool corr = false;             // intensity_corr_buras
+  bool corr_be = false;          // ... with the Buras-Emde method (tabulated phase function)
+  int nangles = 0;               // num_phase_func_angles
+  const double* mup = nullptr;   // mu_phase_function [nangles], increasing
+  const double* phasef = nullptr;  // phase_function [L][nangles]
   int brdf = 0;                  // 0: Lambertian; else the BrdfType (RPV 1, CoxMunk 2, Ambrals 3, Hapke 4)
   const double* bp = nullptr;    // its parameters (SurfaceTables, oracle_common.hpp)
   double wlo = 0, whi = 0, alb = 0, emis = 1, fbeam = 0, umu0 = 0.5, phi0 = 0, fisot = 0, fisob = 0, ttop = 0, tbot = 0;
@@ -223,6 +227,232 @@ inline void nakajima_tanaka(const GeneralInstance& c, int ncut, bool lyrcut, int
   }
 }
 
+// locate (Utils.hpp:27-64): j with xx[j] <= x < xx[j+1] by bisection, 0 at
+// xx[0] and below, n-2 at xx[n-1]
+inline int be_locate(const double* xx, int n, double x) {
+  if (n <= 0) return -1;
+  if (n == 1) return 0;
+  const bool inc = xx[1] > xx[0];
+  int jl = 0, ju = n;
+  while (ju - jl > 1) {
+    const int jm = (ju + jl) >> 1;
+    if ((x >= xx[jm] && inc) || (x <= xx[jm] && !inc)) jl = jm;
+    else ju = jm;
+  }
+  if (x == xx[0]) return 0;
+  if (x == xx[n - 1]) return n - 2;
+  return jl;
+}
+
+// calcPhaseSquared (DisortSolver.cpp:3932-4023): the azimuthal integral of
+// P''(mu_1) P''(theta_12) over the grid mu_eq equidistant in |P''|; arrays of
+// output depth lu: p2[nangles], mueq[nf], neg[nf]
+inline double be_phase_squared(int na, const double* mup, const double* p2, double ctheta, int nf,
+                               const double* mueq, const int* neg, double norm) {
+  double pspike2 = 0.0;
+  const double st = std::sqrt(1.0 - ctheta * ctheta);
+  for (int j = 0; j < nf; ++j) {
+    const double me = mueq[j];
+    double phint;
+    if (ctheta == 1.0 || me == 1.0) {
+      const int i2 = be_locate(mup, na, me * ctheta);
+      phint = M_PI * (p2[i2] + (me * ctheta - mup[i2]) / (mup[i2 + 1] - mup[i2]) * (p2[i2 + 1] - p2[i2]));
+      if (ctheta == 1.0) phint /= 2.0;
+    } else {
+      phint = 0.0;
+      const double sm = std::sqrt(1.0 - me * me);
+      double mumin = ctheta * me - st * sm, mumax = ctheta * me + st * sm;
+      bool cutting = false;
+      if (me < mumax) {
+        mumax = me;
+        cutting = true;
+      }
+      if (mumin < mumax) {
+        const int imin = be_locate(mup, na, mumin), imax = be_locate(mup, na, mumax);
+        int k = imin;
+        double D = (p2[k + 1] - p2[k]) / (mup[k + 1] - mup[k]);
+        double C = p2[k] - mup[k] * D;
+        phint += (D * ctheta * me + C) * M_PI / 2.0;
+        for (k = imin + 1; k <= imax; ++k) {
+          const double Dp = (p2[k + 1] - p2[k]) / (mup[k + 1] - mup[k]);
+          const double Cp = p2[k] - mup[k] * Dp;
+          phint += (Dp - D) * std::sqrt(1.0 - ctheta * ctheta - me * me + 2.0 * ctheta * me * mup[k] - mup[k] * mup[k]) +
+                   ((Dp - D) * ctheta * me + Cp - C) * std::asin((ctheta * me - mup[k]) / (sm * st));
+          D = Dp;
+          C = Cp;
+        }
+        if (cutting)
+          phint += -D * std::sqrt(1.0 - ctheta * ctheta + 2.0 * me * me * (ctheta - 1.0)) -
+                   (D * ctheta * me + C) * std::asin((ctheta - 1.0) * me / (sm * st));
+        else
+          phint += (D * ctheta * me + C) * M_PI / 2.0;
+      }
+    }
+    const double w = (j == 0 || j == nf - 1) ? 0.5 : 1.0;
+    pspike2 += (neg[j] ? -w : w) * phint;
+  }
+  return pspike2 * norm;
+}
+
+// applyNewIntensityCorrection (DisortSolver.cpp:3532-3749) with
+// prepDoubleScatIntegr (:3812-3876) and newSecondaryScat (:3878-3930): the
+// Buras-Emde correction, TMS from the tabulated phase function and IMS from
+// the residual phase function P'' of the truncated peak and its square.
+template <class Acc>
+inline void buras_emde(const GeneralInstance& c, int ncut, bool lyrcut, int numu, int nphi, int ntau,
+                       const std::vector<double>& umu, const std::vector<double>& utau,
+                       const std::vector<double>& utaus, const std::vector<int>& lyr,
+                       const std::vector<double>& tauc, const std::vector<double>& taus,
+                       const std::vector<double>& fsc, const std::vector<double>& ws,
+                       const std::vector<double>& pm, Acc&& I3) {
+  const int N = c.N, L = c.L, na = c.nangles, pc = c.pc, nf = 100;
+  auto PM = [&](int k, int lc) { return pm[(size_t)lc * pc + k]; };
+  auto PF = [&](int lc, int it) { return c.phasef[(size_t)lc * na + it]; };
+  const double* mup = c.mup;
+  const double dither = 100.0 * std::numeric_limits<double>::epsilon();
+  const double dtheta = 10.0, tiny = 1.0e-4, deg = M_PI / 180.0;
+  bool need2 = false;
+  for (int iu = 0; iu < numu; ++iu)
+    if (umu[iu] < 0.0 && std::fabs(std::acos(-c.umu0) / deg - std::acos(umu[iu]) / deg) <= dtheta) need2 = true;
+  std::vector<double> p2((size_t)na * ntau, 0.0), mueq, normp;
+  std::vector<int> negp;
+  auto P2 = [&](int it, int lu) -> double& { return p2[(size_t)lu * na + it]; };
+  if (need2) {
+    mueq.assign((size_t)nf * ntau, 0.0);
+    negp.assign((size_t)nf * ntau, 0);
+    normp.assign(ntau, 0.0);
+    std::vector<double> phasr(L);
+    for (int it = 0; it < na; ++it) {
+      const double ct = mup[it];
+      for (int lc = 0; lc < L; ++lc) phasr[lc] = 1.0 - fsc[lc];
+      double plm1 = 1.0, plm2 = 0.0;
+      for (int k = 1; k <= N - 1; ++k) {
+        const double pl = ((2 * k - 1) * ct * plm1 - (k - 1) * plm2) / k;
+        plm2 = plm1;
+        plm1 = pl;
+        for (int lc = 0; lc < L; ++lc) phasr[lc] += (2 * k + 1) * pl * (PM(k, lc) - fsc[lc]);
+      }
+      for (int lu = 0; lu < ntau; ++lu) {
+        double v = 0.0;
+        const int ll = lyr[lu];
+        for (int l = 0; l < ll; ++l) v += (PF(l, it) - phasr[l]) * c.ssa[l] * c.dtau[l];
+        v += (PF(ll, it) - phasr[ll]) * c.ssa[ll] * (utau[lu] - tauc[ll]);
+        P2(it, lu) = v;
+      }
+    }
+    for (int lu = 0; lu < ntau; ++lu) {
+      const int ll = lyr[lu];
+      double fbar = fsc[ll] * c.ssa[ll] * (utau[lu] - tauc[ll]);
+      for (int l = 0; l < ll; ++l) fbar += c.ssa[l] * c.dtau[l] * fsc[l];
+      if (fbar <= tiny || c.fbeam <= tiny) {
+        for (int it = 0; it < na; ++it) P2(it, lu) = 0.0;
+      } else {
+        fbar = 1.0 / fbar;
+        for (int it = 0; it < na; ++it) P2(it, lu) *= fbar;
+      }
+      double f2 = 0.0;
+      for (int it = 1; it < na; ++it) f2 += (mup[it] - mup[it - 1]) * 0.5 * (P2(it, lu) + P2(it - 1, lu));
+      if (f2 != 0.0) {
+        const double norm = 2.0 / f2;
+        for (int it = 0; it < na; ++it) P2(it, lu) *= norm;
+      }
+    }
+    // prepDoubleScatIntegr
+    std::vector<double> fabs2(na);
+    for (int lu = 0; lu < ntau; ++lu) {
+      double* me = &mueq[(size_t)lu * nf];
+      int* ng = &negp[(size_t)lu * nf];
+      fabs2[0] = 0.0;
+      for (int it = 1; it < na; ++it)
+        fabs2[it] = fabs2[it - 1] + (mup[it] - mup[it - 1]) * 0.5 * (std::fabs(P2(it, lu)) + std::fabs(P2(it - 1, lu)));
+      double f = 0.0;
+      const double df = fabs2[na - 1] / (nf - 1);
+      me[0] = -1.0;
+      ng[0] = P2(0, lu) > 0.0 ? 0 : 1;
+      int it = 0;
+      for (int q = 1; q < nf - 1; ++q) {
+        f += df;
+        while (fabs2[it + 1] < f) ++it;
+        me[q] = mup[it] + (f - fabs2[it]) / (fabs2[it + 1] - fabs2[it]) * (mup[it + 1] - mup[it]);
+        if (P2(it, lu) > 0.0 && P2(it + 1, lu) > 0.0) ng[q] = 0;
+        else if (P2(it, lu) < 0.0 && P2(it + 1, lu) < 0.0) ng[q] = 1;
+        else {
+          const double val = P2(it, lu) + (f - fabs2[it]) / (fabs2[it + 1] - fabs2[it]) * (P2(it + 1, lu) - P2(it, lu));
+          ng[q] = val > 0.0 ? 0 : 1;
+        }
+      }
+      me[nf - 1] = 1.0;
+      ng[nf - 1] = P2(na - 1, lu) > 0.0 ? 0 : 1;
+      normp[lu] = fabs2[na - 1] / ((nf - 1) * M_PI);
+    }
+  }
+  std::vector<double> phasm(ncut + 1), phast(ncut + 1), ssa1(ncut + 1), opr1(ncut + 1);
+  for (int lc = 1; lc <= ncut; ++lc) {
+    ssa1[lc] = c.ssa[lc - 1];
+    opr1[lc] = ws[lc - 1];
+  }
+  for (int iu = 0; iu < numu; ++iu) {
+    double theta0 = 0.0, thetap = 0.0;
+    if (umu[iu] < 0.0) {
+      theta0 = std::acos(-c.umu0) / deg;
+      thetap = std::acos(umu[iu]) / deg;
+    }
+    for (int jp = 0; jp < nphi; ++jp) {
+      const double phirad = (c.phi[jp] - c.phi0) * deg;
+      const double ctheta =
+          -c.umu0 * umu[iu] + std::sqrt((1.0 - c.umu0 * c.umu0) * (1.0 - umu[iu] * umu[iu])) * std::cos(phirad);
+      for (int lc = 1; lc <= ncut; ++lc) phasm[lc] = 1.0;
+      const int it = be_locate(mup, na, ctheta);
+      for (int lc = 1; lc <= ncut; ++lc) {
+        const double phasa = PF(lc - 1, it) + (ctheta - mup[it]) / (mup[it + 1] - mup[it]) * (PF(lc - 1, it + 1) - PF(lc - 1, it));
+        phast[lc] = phasa / (1.0 - fsc[lc - 1] * c.ssa[lc - 1]);
+      }
+      double plm1 = 1.0, plm2 = 0.0;
+      for (int k = 1; k <= N - 1; ++k) {
+        const double pl = ((2 * k - 1) * ctheta * plm1 - (k - 1) * plm2) / k;
+        plm2 = plm1;
+        plm1 = pl;
+        for (int lc = 1; lc <= ncut; ++lc)
+          phasm[lc] += (2.0 * k + 1) * pl * (PM(k, lc - 1) - fsc[lc - 1]) / (1.0 - fsc[lc - 1]);
+      }
+      for (int lu = 0; lu < ntau; ++lu) {
+        if (lyrcut && lyr[lu] >= ncut) continue;
+        const double exact = nt_single_scat(dither, lyr[lu] + 1, ncut, phast.data(), ssa1.data(), taus.data(),
+                                            umu[iu], c.umu0, utaus[lu], c.fbeam);
+        const double scaled = nt_single_scat(dither, lyr[lu] + 1, ncut, phasm.data(), opr1.data(), taus.data(),
+                                             umu[iu], c.umu0, utaus[lu], c.fbeam);
+        I3(lu, iu, jp) += exact - scaled;
+      }
+      if (umu[iu] < 0.0 && std::abs(theta0 - thetap) <= dtheta) {
+        const int ltau = utau[0] <= dither ? 1 : 0;
+        for (int lu = ltau; lu < ntau; ++lu) {
+          if (lyrcut && lyr[lu] >= ncut) continue;
+          // newSecondaryScat
+          const int layru = lyr[lu];
+          const double ut = utau[lu];
+          double dt = ut - tauc[layru];
+          double wbar = c.ssa[layru] * dt, fbar = fsc[layru] * wbar, stau = dt;
+          for (int l = 0; l < layru; ++l) {
+            wbar += c.dtau[l] * c.ssa[l];
+            fbar += c.dtau[l] * c.ssa[l] * fsc[l];
+            stau += c.dtau[l];
+          }
+          if (wbar <= tiny || fbar <= tiny || stau <= tiny || c.fbeam <= tiny) continue;
+          fbar /= wbar;
+          wbar /= stau;
+          const double ps1 = P2(it, lu) + (ctheta - mup[it]) / (mup[it + 1] - mup[it]) * (P2(it + 1, lu) - P2(it, lu));
+          const double ps2 = be_phase_squared(na, mup, &p2[(size_t)lu * na], ctheta, nf, &mueq[(size_t)lu * nf],
+                                              &negp[(size_t)lu * nf], normp[lu]);
+          const double pspike = 2.0 * ps1 - ps2;
+          const double umu0p = c.umu0 / (1.0 - fbar * wbar);
+          I3(lu, iu, jp) -= c.fbeam / (4.0 * M_PI) * (fbar * wbar) * (fbar * wbar) / (1.0 - fbar * wbar) * pspike *
+                            nt_xi(-umu[iu], umu0p, ut);
+        }
+      }
+    }
+  }
+}
+
 class GeneralOracle {
  public:
   int solve(const GeneralInstance& in, const GeneralOutput& out);
@@ -231,7 +461,7 @@ class GeneralOracle {
 inline int GeneralOracle::solve(const GeneralInstance& cin, const GeneralOutput& out) {
   GeneralInstance c = cin;
   const int L = c.L, N = c.N, NN = N / 2;
-  std::vector<double> rdt, rss, rpm, rtp, rut, rza;
+  std::vector<double> rdt, rss, rpm, rtp, rut, rza, rpf;
   if (c.ifb) {  // reverseInputArrays (IndexConversion.hpp:16-40)
     rdt.assign(c.dtau, c.dtau + L);
     rss.assign(c.ssa, c.ssa + L);
@@ -243,6 +473,13 @@ inline int GeneralOracle::solve(const GeneralInstance& cin, const GeneralOutput&
     c.dtau = rdt.data();
     c.ssa = rss.data();
     c.pmom = rpm.data();
+    if (c.phasef && c.nangles > 0) {
+      rpf.resize((size_t)L * c.nangles);
+      for (int lc = 0; lc < L; ++lc)
+        std::memcpy(&rpf[(size_t)lc * c.nangles], c.phasef + (size_t)(L - 1 - lc) * c.nangles,
+                    sizeof(double) * c.nangles);
+      c.phasef = rpf.data();
+    }
     if (c.temp) {
       rtp.assign(c.temp, c.temp + L + 1);
       std::reverse(rtp.begin(), rtp.end());
@@ -1177,8 +1414,12 @@ inline int GeneralOracle::solve(const GeneralInstance& cin, const GeneralOutput&
     bool scat_yes = false;
     for (int lc = 0; lc < L; ++lc)
       if (c.ssa[lc] > 0.0) scat_yes = true;
-    if (deltam && scat_yes) nakajima_tanaka(c, ncut, lyrcut, numu, nphi, ntau, umu, utau, utaus, lyr, tauc, taus,
-                                            fsc, ws, pm, I3);
+    if (deltam && scat_yes) {
+      if (c.corr_be)
+        buras_emde(c, ncut, lyrcut, numu, nphi, ntau, umu, utau, utaus, lyr, tauc, taus, fsc, ws, pm, I3);
+      else
+        nakajima_tanaka(c, ncut, lyrcut, numu, nphi, ntau, umu, utau, utaus, lyr, tauc, taus, fsc, ws, pm, I3);
+    }
     if (!dmplus && !lamb) {
       // applyBrdfIntensityCorrection (DisortSolver.cpp:3751-3810): the exact
       // reflectance of the beam against its Fourier sum over the modes run

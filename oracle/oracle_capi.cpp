@@ -144,6 +144,12 @@ int oracle_general_bands_solve_jac(const dsp_general_batch* b, const dsp_general
         c.user_mu = (fl & DSP_GFLAG_USER_MU) != 0;
         c.only_fluxes = (fl & DSP_GFLAG_ONLY_FLUXES) != 0;
         c.corr = (fl & DSP_GFLAG_INTENSITY_CORR) != 0;
+        c.corr_be = c.corr && (fl & DSP_GFLAG_INTENSITY_CORR_BE) != 0;
+        if (c.corr_be) {
+          c.nangles = b->num_phase_func_angles;
+          c.mup = at(b->mu_phase_function, i);
+          c.phasef = b->phase_function ? b->phase_function + l0 * b->num_phase_func_angles : nullptr;
+        }
         c.accur = b->accuracy_fourier_series;
         c.wlo = scalar(b->wavenumber_low, i, 0.0);
         c.whi = scalar(b->wavenumber_high, i, 0.0);
@@ -175,6 +181,7 @@ int oracle_general_bands_solve_jac(const dsp_general_batch* b, const dsp_general
         c.bp = c.brdf ? at(b->brdf_params, i) : nullptr;
         if (c.L > 0 && b->layer_offset[i + 1] - l0 != c.L) st = DSP_ERR_INVALID_INPUT;
         else if (c.brdf < 0 || c.brdf > 4 || (c.brdf && !c.bp)) st = DSP_ERR_INVALID_INPUT;
+        else if (c.corr_be && (c.nangles < 2 || !c.mup || !c.phasef)) st = DSP_ERR_INVALID_INPUT;
         else if (ntau > ntau_o || numu > numu_o || c.N > 64) st = DSP_ERR_INVALID_INPUT;
         else if (jac && jac->ndof_out < c.L + 2) st = DSP_ERR_INVALID_INPUT;
         else {

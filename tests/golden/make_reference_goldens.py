@@ -145,6 +145,14 @@ CASES = [
     dict(test="IntensityCorrectionHG3b", N=16, L=1, nmom=16, dtau=[8.0], ssa=[1.0], phase=[("hg", 0.75)],
          fbeam=PI, umu0=1.0, corr=True, utau=[0.0, 8.0],
          umu=[-1.0, -0.5, -0.1, 0.1, 0.5, 1.0], phi=[0.0]),
+    # Buras-Emde correction (makeNewICTestConfig1Layer, test_solver.cpp:3940-3987): the HG phase
+    # function tabulated on 100 uniform cosines, intensity_corr_nakajima off
+    dict(test="NewICHG3a", N=16, L=1, nmom=16, dtau=[1.0], ssa=[1.0], phase=[("hg", 0.75)],
+         fbeam=PI, umu0=1.0, corr=True, tab=(0.75, 100), utau=[0.0, 1.0],
+         umu=[-1.0, -0.5, -0.1, 0.1, 0.5, 1.0], phi=[0.0]),
+    dict(test="NewICHG3b", N=16, L=1, nmom=16, dtau=[8.0], ssa=[1.0], phase=[("hg", 0.75)],
+         fbeam=PI, umu0=1.0, corr=True, tab=(0.75, 100), utau=[0.0, 8.0],
+         umu=[-1.0, -0.5, -0.1, 0.1, 0.5, 1.0], phi=[0.0]),
     # disotest 12a (test_solver.cpp:3637-3700): 20 streams (oracle only; the engine takes 4-16, 32, 64)
     dict(test="ValidationDisotest12a", N=20, L=1, nmom=20, dtau=[20.1], ssa=[0.5], phase=[("hg", 0.9)],
          fbeam=1.0, umu0=1.0, albedo=1.0, corr=True, utau=[0.0, 10.0, 19.9, 20.1],
@@ -225,6 +233,19 @@ def moments(phase, nmom_nstr: int, cloud: list) -> list:
     return pm
 
 
+def tabulated(tab, L: int) -> dict:
+    """The HG phase function on a uniform cosine grid, as makeNewICTestConfig1Layer fills it."""
+    if tab is None:
+        return {}
+    g, n = tab
+    mu = [-1.0 + 2.0 * it / (n - 1) for it in range(n)]
+    val = []
+    for ct in mu:
+        d = 1.0 + g * g - 2.0 * g * ct
+        val.append((1.0 - g * g) / (d * math.sqrt(d)))
+    return dict(mu_phase_function=mu, phase_function=[val] * L)
+
+
 def main():
     if len(sys.argv) != 2:
         sys.exit("usage: make_reference_goldens.py /path/to/DisORT (the DisORT++ source tree)")
@@ -259,6 +280,7 @@ def main():
             brdf_type=c["brdf"][0] if "brdf" in c else 0,
             brdf_params=c["brdf"][1] if "brdf" in c else [],
             intensity_corrected=bool(c.get("corr", False)),
+            **tabulated(c.get("tab"), L),
             expect_flux=fl, expect_intensity=it,
         ))
     out = dict(generated_by="tests/golden/make_reference_goldens.py",

@@ -100,6 +100,10 @@ def general_instance(c: dict) -> tuple[dict, int]:
     )
     if c.get("intensity_corrected"):
         flags |= capi.GFLAG_INTENSITY_CORR
+        if c.get("mu_phase_function"):  # a tabulated phase function: the Buras-Emde method
+            flags |= capi.GFLAG_INTENSITY_CORR_BE
+            inst["mu_phase_function"] = c["mu_phase_function"]
+            inst["phase_function"] = c["phase_function"]
     if c.get("brdf_type"):
         inst["brdf_type"] = c["brdf_type"]
         inst["brdf_params"] = c["brdf_params"]

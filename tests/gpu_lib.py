@@ -114,10 +114,10 @@ def general_solve_device(d: dict):
     keep = []
     for k in ("num_streams", "num_layers", "layer_offset", "num_phase_func_moments", "delta_tau",
               "single_scat_albedo", "phase_function_moments", "temperature", "level_altitudes",
-              "bottom_radius", "brdf_params") + capi.GENERAL_SCALAR_FIELDS:
+              "bottom_radius", "brdf_params", "phase_function") + capi.GENERAL_SCALAR_FIELDS:
         if k in d:
             dd[k] = torch.from_numpy(np.ascontiguousarray(d[k])).cuda()
-    for k in ("tau_user", "mu_user", "phi_user"):
+    for k in ("tau_user", "mu_user", "phi_user", "mu_phase_function"):
         if k in d:
             a, stride = d[k]
             dd[k] = (torch.from_numpy(np.ascontiguousarray(a)).cuda(), stride)
