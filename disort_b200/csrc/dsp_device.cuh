@@ -166,7 +166,23 @@ struct GenView {
   DArr brdf_par;
   const double* brdf_q;
   double* brdf;
+  // Buras-Emde intensity correction: the tabulated phase function and, per
+  // chunk slot, its residual-phase tables (becor_stride doubles)
+  int nangles;
+  DArr mup;
+  const double* phasef;  // [batch layers][nangles], CSR like dtau
+  double* becor;
+  long long becor_ld;    // doubles per slot: becor_stride of the batch's largest NT
 };
+
+// Per-slot tables of the Buras-Emde correction for NT output depths
+// (applyNewIntensityCorrection / prepDoubleScatIntegr, DisortSolver.cpp:3568-3640,
+// 3812-3876): the residual phase function P''[NT][na], the integration grid
+// mu_eq[NT][nf] and its signs [NT][nf], and the normalisation [NT].
+constexpr int BE_NF = 100;
+__host__ __device__ constexpr long long becor_stride(int NT, int na) {
+  return ((long long)NT * (na + 2 * BE_NF + 1) + 3) & ~3ll;
+}
 
 // Surface table of one chunk slot for the current azimuth mode
 // (computeSurfaceBidir, DisortSolver.cpp:2582-2708): rows r = 0..NN-1 are the

@@ -377,6 +377,12 @@ dsp_status general_solve(dsp_context ctx, const dsp_general_batch* bin, const ds
     return fail(ctx, DSP_ERR_INVALID_INPUT, "bidirReflectivity: unknown BRDF type");
   if (brdf && !b.brdf_params.ptr)
     return fail(ctx, DSP_ERR_INVALID_INPUT, "a bidirectional surface needs brdf_params");
+  // the Buras-Emde correction reads the tabulated phase function
+  const bool becorr = (fl & DSP_GFLAG_INTENSITY_CORR) && (fl & DSP_GFLAG_INTENSITY_CORR_BE) && do_int;
+  const int na = becorr ? b.num_phase_func_angles : 0;
+  if (becorr && (na < 2 || !b.mu_phase_function.ptr || !b.phase_function))
+    return fail(ctx, DSP_ERR_INVALID_INPUT,
+                "the Buras-Emde correction needs num_phase_func_angles >= 2, mu_phase_function and phase_function");
   for (int f = 0; f < 8; ++f)
     if (!out->flux[f]) return fail(ctx, DSP_ERR_INVALID_INPUT, "every flux output array is required");
   if (do_int && (!out->intensity || !out->intensity_azimuth_avg))
@@ -440,6 +446,8 @@ dsp_status general_solve(dsp_context ctx, const dsp_general_batch* bin, const ds
   const double* d_zalt = nullptr;
   dsp_darray d_rbot = b.bottom_radius;
   dsp_darray d_bpar = b.brdf_params;
+  dsp_darray d_mup = b.mu_phase_function;
+  const double* d_phasef = b.phase_function;
   const int32_t* d_L;
   const int64_t* d_off;
   const int32_t* d_nmom;
@@ -453,6 +461,9 @@ dsp_status general_solve(dsp_context ctx, const dsp_general_batch* bin, const ds
       if (spherical)
         need += align256((total_layers + n) * sizeof(double)) + align256(darray_elems(b.bottom_radius, 1) * sizeof(double));
       if (brdf) need += align256(darray_elems(b.brdf_params, DSP_BRDF_PARAMS) * sizeof(double));
+      if (becorr)
+        need += align256(darray_elems(b.mu_phase_function, na) * sizeof(double)) +
+                align256((size_t)total_layers * na * sizeof(double));
       for (int k = 0; k < 3; ++k)
         if (lists[k]->ptr && list_n[k] > 0) need += align256(darray_elems(*lists[k], list_n[k]) * sizeof(double));
     }
@@ -493,6 +504,11 @@ dsp_status general_solve(dsp_context ctx, const dsp_general_batch* bin, const ds
       if (brdf)
         d_bpar.ptr = static_cast<const double*>(
             put(b.brdf_params.ptr, darray_elems(b.brdf_params, DSP_BRDF_PARAMS) * sizeof(double)));
+      if (becorr) {
+        d_mup.ptr = static_cast<const double*>(
+            put(b.mu_phase_function.ptr, darray_elems(b.mu_phase_function, na) * sizeof(double)));
+        d_phasef = static_cast<const double*>(put(b.phase_function, (size_t)total_layers * na * sizeof(double)));
+      }
       for (int k = 0; k < 3; ++k) {
         dlists[k] = *lists[k];
         if (lists[k]->ptr && list_n[k] > 0)
@@ -597,6 +613,7 @@ dsp_status general_solve(dsp_context ctx, const dsp_general_batch* bin, const ds
     std::vector<int64_t> inst_off, lay_off;
     int64_t inst_doubles = 0, layers = 0;
     int64_t surf_doubles = 0;  // bidirectional surface tables, one per slot
+    int64_t be_doubles = 0;    // Buras-Emde tables, one per slot (all of one NT)
     int maxm = 0;
     // persistent boundary-value launches: the slots by descending layer count
     std::vector<int32_t> order;
@@ -638,7 +655,8 @@ dsp_status general_solve(dsp_context ctx, const dsp_general_batch* bin, const ds
       if (hN[i] != N) continue;
       const int L = hL[i] > 0 ? hL[i] : 0;
       const int NT = user_tau ? b.num_user_tau : L + 1;
-      const int64_t rec = GenLayout::make(L, N, NT).stride + (brdf ? brdf_stride(N, numu_eff) : 0);
+      const int64_t rec = GenLayout::make(L, N, NT).stride + (brdf ? brdf_stride(N, numu_eff) : 0) +
+                          (becorr ? becor_stride(ntau_need, na) : 0);
       const size_t ib = (size_t)(rec + (int64_t)L * per_layer) * sizeof(double);
       if (!c.ids.empty() && bytes + ib > budget) flush();
       c.ids.push_back(i);
@@ -646,6 +664,7 @@ dsp_status general_solve(dsp_context ctx, const dsp_general_batch* bin, const ds
       c.lay_off.push_back(c.layers);
       c.inst_doubles += GenLayout::make(L, N, NT).stride;
       if (brdf) c.surf_doubles += brdf_stride(N, numu_eff);
+      if (becorr) c.be_doubles += becor_stride(ntau_need, na);
       c.layers += L;
       bytes += ib;
       int naz = N - 1;
@@ -676,7 +695,7 @@ dsp_status general_solve(dsp_context ctx, const dsp_general_batch* bin, const ds
                    align256(c.layers * 4) + align256(c.order.size() * 4) + align256((c.maxm + 1) * 4);
       const int64_t lstride = glrec_stride(c.N, numu_eff);
       const size_t w =
-          (size_t)(c.inst_doubles + c.surf_doubles +
+          (size_t)(c.inst_doubles + c.surf_doubles + c.be_doubles +
                    c.layers * (lstride + brec_stride(c.N) + c.N + sph_per_layer(c.N) + jac_per_layer(c.N))) *
           sizeof(double);
       if (w > ws_need) ws_need = w;
@@ -750,6 +769,11 @@ dsp_status general_solve(dsp_context ctx, const dsp_general_batch* bin, const ds
     g.brdf_par.s = d_bpar.stride;
     g.brdf_q = nullptr;
     if (brdf && (st = get_brdf_quadrature(ctx, &g.brdf_q)) != DSP_OK) return st;
+    g.nangles = na;
+    g.mup.p = becorr ? d_mup.ptr : nullptr;
+    g.mup.s = d_mup.stride;
+    g.phasef = becorr ? d_phasef : nullptr;
+    g.becor_ld = becor_stride(ntau_need, na);
     for (size_t k = 0; k < chunks.size(); ++k) {
       const Chunk& c = chunks[k];
       const size_t nc = c.ids.size();
@@ -787,13 +811,14 @@ dsp_status general_solve(dsp_context ctx, const dsp_general_batch* bin, const ds
         for (int f = 0; f < 6; ++f) jv.out[f] = djac[f];
       }
       // after every per-layer area: the surface tables of the chunk's slots
-      g.brdf = brdf ? static_cast<double*>(ctx->ws) + c.inst_doubles +
-                          c.layers * (g.lstride + brec_stride(c.N) + c.N + sph_per_layer(c.N) + jac_per_layer(c.N))
-                    : nullptr;
+      double* const wend = static_cast<double*>(ctx->ws) + c.inst_doubles +
+                           c.layers * (g.lstride + brec_stride(c.N) + c.N + sph_per_layer(c.N) + jac_per_layer(c.N));
+      g.brdf = brdf ? wend : nullptr;
+      g.becor = becorr ? wend + c.surf_doubles : nullptr;
       const double* tabs = nullptr;
       if ((st = get_mode_tables(ctx, c.N, &tabs)) != DSP_OK) return st;
       if (ctx->debug & DSP_DEBUG_POISON_SCRATCH) {
-        const size_t wb = (size_t)(c.inst_doubles + c.surf_doubles +
+        const size_t wb = (size_t)(c.inst_doubles + c.surf_doubles + c.be_doubles +
                                    c.layers * (g.lstride + brec_stride(c.N) + c.N + sph_per_layer(c.N) +
                                                jac_per_layer(c.N))) *
                           sizeof(double);

@@ -215,12 +215,18 @@ void check_engine(const DisortConfig& c) {
         throw std::runtime_error("bidirReflectivity: unknown BRDF type");
     }
   }
-  // the Nakajima-Tanaka correction runs on the engine; the Buras-Emde one
-  // (DisortSolver.cpp:362-367: a tabulated phase function and no
-  // intensity_corr_nakajima) does not
-  if (f.intensity_corr_buras && !f.intensity_corr_nakajima && c.num_phase_func_angles > 0)
-    throw std::invalid_argument(
-        "the Buras-Emde intensity correction (tabulated phase function) is not supported by the B200 engine");
+  // the Buras-Emde correction (DisortSolver.cpp:362-367) interpolates the tabulated
+  // phase function between angles: it needs two and every layer's values
+  if (f.intensity_corr_buras && !f.intensity_corr_nakajima && c.num_phase_func_angles > 0) {
+    const size_t na = static_cast<size_t>(c.num_phase_func_angles);
+    bool ok = na >= 2 && c.mu_phase_function.size() >= na &&
+              c.phase_function.size() >= static_cast<size_t>(c.num_layers);
+    for (int lc = 0; ok && lc < c.num_layers; ++lc) ok = c.phase_function[lc].size() >= na;
+    if (!ok)
+      throw std::invalid_argument(
+          "intensity_corr_buras with a tabulated phase function needs num_phase_func_angles >= 2, "
+          "mu_phase_function and phase_function of every layer");
+  }
   if (f.output_fourier_expansion)
     throw std::invalid_argument("output_fourier_expansion is not supported by the B200 engine");
   // validate() does not look at the user optical depths; the reference reads
@@ -301,6 +307,7 @@ struct GenPacked {
   std::vector<double> lo, hi, alb, emis, fbeam, fisot, fisob;
   double mu0 = 0.5, phi0 = 0.0, ttop = 0.0, tbot = 0.0, rbot = 0.0;
   double bpar[DSP_BRDF_PARAMS] = {};  // the surface model's parameters, shared by every band
+  std::vector<double> mup, phasef;   // tabulated phase function (Buras-Emde correction)
 };
 
 // One batch for the whole loop.  `c` already carries the automatic fields.
@@ -412,6 +419,20 @@ dsp_general_batch pack_general(const DisortConfig& c, const std::vector<std::pai
   b.direct_beam_phi = {&pk.phi0, 0};
   b.temperature_top = {&pk.ttop, 0};
   b.temperature_bottom = {&pk.tbot, 0};
+  if (f.intensity_corr_buras && !f.intensity_corr_nakajima && c.num_phase_func_angles > 0) {
+    // the Buras-Emde method: the table, layer rows per band in the batch's layer order
+    const int na = c.num_phase_func_angles;
+    b.flags |= DSP_GFLAG_INTENSITY_CORR_BE;
+    b.num_phase_func_angles = na;
+    pk.mup.assign(c.mu_phase_function.begin(), c.mu_phase_function.begin() + na);
+    b.mu_phase_function = {pk.mup.data(), 0};
+    pk.phasef.resize(static_cast<size_t>(n) * L * na);
+    for (int i = 0; i < n; ++i)
+      for (int lc = 0; lc < L; ++lc)
+        std::copy(c.phase_function[lc].begin(), c.phase_function[lc].begin() + na,
+                  pk.phasef.begin() + (static_cast<size_t>(i) * L + lc) * na);
+    b.phase_function = pk.phasef.data();
+  }
   if (!f.use_lambertian_surface) {  // the spec in the C ABI's parameter order
     b.brdf_type = static_cast<int32_t>(f.brdf_type);
     double* q = pk.bpar;

@@ -157,7 +157,7 @@ void solveFluxSpectralBandsInto(const DisortFluxConfig& config,
 // Lambertian or bidirectional (BRDF) surface, Fourier azimuth modes, fluxes,
 // intensities at user optical depths and angles, temperature Jacobians.
 // Configurations asking for what the engine does not implement (special
-// boundary conditions, the Buras-Emde intensity correction, the Fourier-expansion output,
+// boundary conditions, the Fourier-expansion output,
 // stream counts outside 4-16/32/64) pass validate() like in the reference and
 // are rejected with std::invalid_argument when solved.
 // ---------------------------------------------------------------------------

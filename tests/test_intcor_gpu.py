@@ -131,5 +131,81 @@ def test_intcor_through_solver_object():
     np.testing.assert_allclose(np.asarray(r.intensity), got["intensity"][0], rtol=1e-12, atol=1e-15)
     f.intensity_corr_nakajima = False
     cfg.num_phase_func_angles = 8
-    with pytest.raises(ValueError, match="Buras-Emde"):
+    with pytest.raises(ValueError, match="needs num_phase_func_angles >= 2"):
         db.DisortSolver().solve(cfg)
+
+
+def tabulate(insts, na=121):
+    """Each layer's HG phase function tabulated on na uniform cosines (the
+    Buras-Emde method's input)."""
+    mu = np.linspace(-1.0, 1.0, na)
+    for c in insts:
+        g = np.asarray(c["phase_function_moments"])[:, 1]
+        d = 1.0 + g[:, None] ** 2 - 2.0 * g[:, None] * mu[None, :]
+        c["mu_phase_function"] = mu
+        c["phase_function"] = (1.0 - g[:, None] ** 2) / (d * np.sqrt(d))
+    return insts
+
+
+@pytest.mark.parametrize("nstr", [(4, 8), (16,), (32,), (64,)])
+def test_buras_emde_mix(nstr):
+    n = 3 if nstr == (64,) else 8
+    insts, flags = corr_mix(n, seed=80 + nstr[0], nstr=nstr, layers=(3, 6) if nstr == (64,) else (3, 12))
+    insts = tabulate(insts)
+    flags |= capi.GFLAG_INTENSITY_CORR_BE
+    got, ref, _ = both(insts, flags)
+    assert (got["status"] == 0).all() and (ref["status"] == 0).all()
+    assert_parity_general(got, ref, f"Buras-Emde N {nstr}")
+    nt, _, _ = both(insts, flags & ~capi.GFLAG_INTENSITY_CORR_BE)
+    assert np.abs(nt["intensity"] - got["intensity"]).max() > 0.0  # a different method
+
+
+def test_buras_emde_levels_bottom_up_and_device_pointers():
+    """Output at the layer boundaries (a different number of depths per
+    instance), bottom-up indexing and device pointers."""
+    insts, flags = corr_mix(6, seed=88, nstr=(8, 16))
+    insts = tabulate(insts, na=64)
+    flags |= capi.GFLAG_INTENSITY_CORR_BE
+    lv = [dict(c) for c in insts]
+    for c in lv:
+        c.pop("tau_user")
+    got, ref, _ = both(lv, flags & ~capi.GFLAG_USER_TAU)
+    assert_parity_general(got, ref, "Buras-Emde at the levels")
+    got, ref, _ = both(insts, flags | capi.FLAG_INDEX_FROM_BOTTOM)
+    assert_parity_general(got, ref, "Buras-Emde bottom-up")
+    d = capi.pack_general(insts, flags)
+    ref = oracle_lib.general_solve(d)
+    got, rc = gpu_lib.general_solve_device(d)
+    assert rc == 0
+    assert_parity_general(got, ref, "Buras-Emde device pointers")
+
+
+def test_buras_emde_through_solver_object():
+    import disort_b200 as db
+    cfg = db.DisortConfig(2, 8, 12)
+    f = cfg.flags
+    f.use_user_tau, f.use_user_mu = True, True
+    f.intensity_corr_buras, f.intensity_corr_nakajima = True, False
+    cfg.num_user_tau, cfg.num_user_mu, cfg.num_phi = 2, 3, 2
+    cfg.num_phase_func_angles = 41
+    cfg.allocate()
+    cfg.delta_tau = [0.4, 1.1]
+    cfg.single_scat_albedo = [0.9, 0.7]
+    cfg.set_henyey_greenstein(0.8)
+    mu = np.linspace(-1.0, 1.0, 41)
+    d = 1.0 + 0.64 - 1.6 * mu
+    tab = (1.0 - 0.64) / (d * np.sqrt(d))
+    cfg.mu_phase_function = list(mu)
+    cfg.phase_function = [list(tab), list(tab)]
+    cfg.tau_user = [0.0, 1.5]
+    cfg.mu_user = [-0.5, -0.2, 0.6]
+    cfg.phi_user = [0.0, 30.0]
+    cfg.bc.direct_beam_flux, cfg.bc.direct_beam_mu = 1.0, 0.5
+    r = db.DisortSolver().solve(cfg)
+    inst = dict(num_streams=8, num_layers=2, num_phase_func_moments=12, delta_tau=[0.4, 1.1],
+                single_scat_albedo=[0.9, 0.7], phase_function_moments=workloads.hg_moments(np.array([0.8, 0.8]), 13),
+                direct_beam_flux=1.0, direct_beam_mu=0.5, tau_user=[0.0, 1.5], mu_user=[-0.5, -0.2, 0.6],
+                phi_user=[0.0, 30.0], mu_phase_function=mu, phase_function=np.stack([tab, tab]))
+    fl = capi.GFLAG_USER_TAU | capi.GFLAG_USER_MU | capi.GFLAG_INTENSITY_CORR | capi.GFLAG_INTENSITY_CORR_BE
+    got, ref, _ = both([inst], fl)
+    np.testing.assert_allclose(np.asarray(r.intensity), got["intensity"][0], rtol=1e-12, atol=1e-15)
