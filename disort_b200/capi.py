@@ -373,6 +373,28 @@ def alloc_general_out_numpy(d: dict) -> tuple[dict, GeneralOut, list]:
     return outs, o, [outs]
 
 
+class AlbTransOut(ctypes.Structure):
+    """dsp_albtrans_out (ibcnd = Special)."""
+    _fields_ = [("albedo_medium", POINTER(c_double)), ("transmissivity_medium", POINTER(c_double)),
+                ("spherical_albedo", POINTER(c_double)), ("spherical_transmissivity", POINTER(c_double)),
+                ("status", POINTER(c_int32)), ("numu_out", c_int32)]
+
+
+def alloc_albtrans_numpy(d: dict) -> tuple[dict, AlbTransOut, list]:
+    """NaN-filled host outputs of dsp_general_bands_albtrans for a pack_general batch."""
+    n = d["n_inst"]
+    nu = d["num_user_mu"] if d["flags"] & GFLAG_USER_MU else int(d["num_streams"].max()) // 2
+    outs = {"albedo_medium": np.full((n, nu), np.nan), "transmissivity_medium": np.full((n, nu), np.nan),
+            "spherical_albedo": np.full(n, np.nan), "spherical_transmissivity": np.full(n, np.nan),
+            "status": np.full(n, -1, dtype=np.int32)}
+    o = AlbTransOut()
+    for f in ("albedo_medium", "transmissivity_medium", "spherical_albedo", "spherical_transmissivity"):
+        setattr(o, f, ctypes.cast(c_void_p(_ptr(outs[f])), POINTER(c_double)))
+    o.status = ctypes.cast(c_void_p(_ptr(outs["status"])), POINTER(c_int32))
+    o.numu_out = nu
+    return outs, o, [outs]
+
+
 class GeneralJacOut(ctypes.Structure):
     _fields_ = [(f, POINTER(c_double)) for f in JAC_FIELDS] + [("ndof_out", c_int32)]
 

@@ -362,6 +362,31 @@ dsp_status dsp_general_bands_solve_jac(dsp_context ctx, const dsp_general_batch*
                                        const dsp_general_out* out, const dsp_general_jac_out* jac);
 
 /*
+ * Albedo and transmissivity of the medium (ibcnd = Special; DisortSolver::solve
+ * with computeAlbTrans, src/DisortSolver.cpp:52-58, 169-176, 4025-4358):
+ * isotropic illumination of unit intensity from the top, and for more than
+ * one layer from the bottom, of each instance with a black surface.  Reads
+ * num_streams, num_layers, layer_offset, num_phase_func_moments, delta_tau,
+ * single_scat_albedo, phase_function_moments, surface_albedo (the spherical
+ * albedo correction), DSP_FLAG_DELTA_M_PLUS, DSP_FLAG_INDEX_FROM_BOTTOM and,
+ * with DSP_GFLAG_USER_MU, the num_user_mu positive cosines of mu_user (else
+ * the N/2 quadrature cosines); sources, optical depths and azimuths are not
+ * read.  Host pointers only.  Outputs per instance: albedo_medium and
+ * transmissivity_medium at the cosines [n_inst][numu_out], the spherical
+ * albedo and transmissivity [n_inst] (zero unless surface_albedo > 0).
+ */
+typedef struct dsp_albtrans_out {
+  double* albedo_medium;
+  double* transmissivity_medium;
+  double* spherical_albedo;
+  double* spherical_transmissivity;
+  int32_t* status;                  /* [n_inst] or NULL */
+  int32_t numu_out;                 /* >= num_user_mu (or max N/2 without user angles) */
+} dsp_albtrans_out;
+dsp_status dsp_general_bands_albtrans(dsp_context ctx, const dsp_general_batch* batch,
+                                      const dsp_albtrans_out* out);
+
+/*
  * Flux solve without any allocation (no counterpart in the reference: DisORT++
  * solves on the CPU and allocates freely).  For callers that must not let a
  * library allocate device memory -- applications that hand the GPU to their own

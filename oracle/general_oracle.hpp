@@ -22,6 +22,7 @@ struct GeneralInstance {
   double radius = 0.0;           // bottom_radius
   const double* zalt = nullptr;  // level_altitudes [L+1] (spherical only)
   double accur = 0.0;
+  bool special = false;          // ibcnd = Special: albedo and transmissivity of the medium
   bool corr = false;             // intensity_corr_buras
   bool corr_be = false;          // ... with the Buras-Emde method (tabulated phase function)
   int nangles = 0;               // num_phase_func_angles
@@ -44,6 +45,9 @@ struct GeneralOutput {
   // or null: flux_up, flux_down, mean_intensity, _down, _up, flux_divergence
   double* jac[6] = {nullptr, nullptr, nullptr, nullptr, nullptr, nullptr};
   int jac_stride = 0;
+  // ibcnd = Special: albedo_medium, transmissivity_medium [numu_half] and the
+  // spherical albedo and transmissivity [1] each
+  double* albtrans[4] = {nullptr, nullptr, nullptr, nullptr};
 };
 
 // DisortConfig::validate (DisortConfig.cpp:72-249) for the fields carried here,
@@ -74,7 +78,7 @@ inline int validate_general(const GeneralInstance& c) {
       if (iu > 0 && c.umu[iu] <= c.umu[iu - 1]) return DSP_ERR_INVALID_INPUT;
     }
   }
-  if (!c.only_fluxes) {
+  if (!c.only_fluxes && !c.special) {  // DisortConfig.cpp:200
     if (c.nphi <= 0 || !c.phi) return DSP_ERR_INVALID_INPUT;
     for (int j = 0; j < c.nphi; ++j)
       if (c.phi[j] < 0.0 || c.phi[j] > 360.0) return DSP_ERR_INVALID_INPUT;
@@ -507,8 +511,36 @@ inline int GeneralOracle::solve(const GeneralInstance& cin, const GeneralOutput&
     }
   }
   if (int st = validate_general(c)) return st;
+  // ibcnd = Special (computeAlbTrans, DisortSolver.cpp:4025-4163): isotropic
+  // illumination of unit intensity from the top (and the bottom), no other
+  // source, a black surface in the boundary-value problem; the user angles
+  // become [-mu reversed | +mu] (DisortSolver.cpp:52-58, 852-865)
+  const double special_alb = c.alb;
+  std::vector<double> sp_umu;
+  if (c.special) {
+    c.fbeam = 0.0;
+    c.thermal = false;
+    c.spherical = false;
+    c.fisot = 1.0;
+    c.fisob = 0.0;
+    c.alb = 0.0;
+    c.brdf = BRDF_LAMBERT;
+    c.corr = false;
+    c.user_tau = false;
+    c.only_fluxes = false;
+    c.temperature_jac = false;
+    if (c.user_mu) {
+      sp_umu.resize(2 * c.numu);
+      for (int iu = 0; iu < c.numu; ++iu) {
+        sp_umu[c.numu + iu] = c.umu[iu];
+        sp_umu[iu] = -c.umu[c.numu - 1 - iu];
+      }
+      c.umu = sp_umu.data();
+      c.numu *= 2;
+    }
+  }
   const int ntau = c.user_tau ? c.ntau : L + 1;
-  const bool do_int = !c.only_fluxes && c.user_mu;
+  const bool do_int = (!c.only_fluxes && c.user_mu) || c.special;
   const int numu = (c.user_mu && !c.only_fluxes) ? c.numu : N;
   const int nphi = c.nphi;
   const int pc = c.pc;
@@ -591,7 +623,7 @@ inline int GeneralOracle::solve(const GeneralInstance& cin, const GeneralOutput&
       }
     }
   }
-  const bool lyrcut = (abstau >= 10.0 && !c.thermal && L > 1);
+  const bool lyrcut = !c.special && (abstau >= 10.0 && !c.thermal && L > 1);  // computeAlbTrans: no cut
   if (!lyrcut) ncut = L;
   std::vector<double> utaus(ntau);
   std::vector<int> lyr(ntau);
@@ -1103,6 +1135,84 @@ inline int GeneralOracle::solve(const GeneralInstance& cin, const GeneralOutput&
     }
     std::vector<int> ipvt(nc);
     if (!band_factor(band.data(), lda, nc, ncd, ncd, ipvt.data())) status = DSP_ERR_SINGULAR;
+    if (c.special) {
+      // solve1 (DisortSolver.cpp:4165-4220) for the top and the bottom
+      // illumination, albTransIntensity (:4222-4293) at the top and the bottom
+      // for the half of the angles leaving the medium there, albTransSpherical
+      // (:4295-4358)
+      const int half = numu / 2;
+      auto solve1 = [&](bool top, std::vector<double>& x) {
+        x.assign(nc, 0.0);
+        for (int q = 0; q < NN; ++q) x[top ? q : nc - NN + q] = c.fisot;
+        band_solve(band.data(), lda, nc, ncd, ncd, ipvt.data(), x.data());
+      };
+      auto intensity = [&](const std::vector<double>& x, int iu, bool top) {
+        const double ut = top ? 0.0 : taus[L], sgn = top ? 1.0 : -1.0, um = umu[iu];
+        double pal = 0.0;
+        std::vector<double> wk(NN);
+        for (int lc = 0; lc < L; ++lc) {
+          const double dtau = taus[lc + 1] - taus[lc];
+          const double e1 = std::exp((ut - taus[lc]) / um), e2 = std::exp((ut - taus[lc + 1]) / um);
+          for (int iq = 0; iq < NN; ++iq) {
+            const double k = kk[(size_t)lc * N + iq];
+            wk[iq] = std::exp(k * dtau);
+            const double den = 1.0 + um * k;
+            const double expn = std::abs(den) < 0.0001 ? dtau / um * e2 : (e1 * wk[iq] - e2) * sgn / den;
+            pal += GU[((size_t)lc * numu + iu) * N + iq] * x[(size_t)lc * N + iq] * expn;
+          }
+          for (int iq = NN; iq < N; ++iq) {
+            const double den = 1.0 + um * kk[(size_t)lc * N + iq];
+            const double expn = std::abs(den) < 0.0001 ? -dtau / um * e1 : (e1 - e2 * wk[N - 1 - iq]) * sgn / den;
+            pal += GU[((size_t)lc * numu + iu) * N + iq] * x[(size_t)lc * N + iq] * expn;
+          }
+        }
+        return pal;
+      };
+      std::vector<double> xt, xb;
+      solve1(true, xt);
+      double* alb_out = out.albtrans[0];
+      double* trn_out = out.albtrans[1];
+      for (int iu = 0; iu < half; ++iu) alb_out[iu] = intensity(xt, iu + half, true);
+      if (L == 1) {
+        for (int iu = 0; iu < half; ++iu)
+          trn_out[iu] = intensity(xt, half - 1 - iu, false) + std::exp(-taus[L] / umu[iu + half]);
+      } else {
+        solve1(false, xb);
+        for (int iu = 0; iu < half; ++iu)
+          trn_out[iu] = intensity(xb, iu + half, true) + std::exp(-taus[L] / umu[iu + half]);
+      }
+      out.albtrans[2][0] = 0.0;
+      out.albtrans[3][0] = 0.0;
+      if (special_alb > 0.0) {
+        const std::vector<double>& x = L == 1 ? xt : xb;
+        double up = 0.0, dn = 0.0;
+        for (int iq = NN; iq < N; ++iq) {
+          double z = 0.0;
+          for (int jq = 0; jq < NN; ++jq) z += Gv(0, iq, jq) * x[jq] * std::exp(kk[jq] * (taus[1] - taus[0]));
+          for (int jq = NN; jq < N; ++jq) z += Gv(0, iq, jq) * x[jq];
+          up += wt[iq - NN] * mu[iq - NN] * z;
+        }
+        const int ll = L - 1;
+        for (int iq = 0; iq < NN; ++iq) {
+          double z = 0.0;
+          for (int jq = 0; jq < NN; ++jq) z += Gv(ll, iq, jq) * x[(size_t)ll * N + jq];
+          for (int jq = NN; jq < N; ++jq)
+            z += Gv(ll, iq, jq) * x[(size_t)ll * N + jq] * std::exp(-kk[(size_t)ll * N + jq] * (taus[L] - taus[L - 1]));
+          dn += wt[NN - 1 - iq] * mu[NN - 1 - iq] * z;
+        }
+        up *= 2.0;
+        dn *= 2.0;
+        const double sphalb = L == 1 ? up : dn, sphtrn = L == 1 ? dn : up;
+        const double corr = special_alb / (1.0 - special_alb * sphalb);
+        for (int iu = 0; iu < half; ++iu) {
+          alb_out[iu] += corr * sphtrn * trn_out[iu];
+          trn_out[iu] += corr * sphalb * trn_out[iu];
+        }
+        out.albtrans[2][0] = sphalb;
+        out.albtrans[3][0] = sphtrn;
+      }
+      return status;
+    }
     band_solve(band.data(), lda, nc, ncd, ncd, ipvt.data(), b.data());
     std::fill(cc.begin(), cc.end(), 0.0);
     for (int k = 0; k < nc; ++k) cc[k] = b[k];  // the reference's reorder is the identity

@@ -212,6 +212,66 @@ int oracle_general_bands_solve_jac(const dsp_general_batch* b, const dsp_general
   return worst;
 }
 
+// ibcnd = Special per instance (computeAlbTrans restated in general_oracle.hpp)
+int oracle_general_bands_albtrans(const dsp_general_batch* b, const dsp_albtrans_out* o, int nthreads) {
+  if (!b || !o || b->n_inst < 0) return DSP_ERR_INVALID_INPUT;
+  const int n = b->n_inst;
+  const uint32_t fl = b->flags;
+  int worst = DSP_OK;
+  if (nthreads <= 0) nthreads = omp_get_max_threads();
+#pragma omp parallel num_threads(nthreads)
+  {
+    oracle::GeneralOracle solver;
+    int local_worst = DSP_OK;
+#pragma omp for schedule(static)
+    for (int i = 0; i < n; ++i) {
+      oracle::GeneralInstance c;
+      int st = DSP_OK;
+      if (!b->num_streams || !b->num_layers || !b->layer_offset || !b->num_phase_func_moments ||
+          !b->delta_tau || !b->single_scat_albedo || !b->phase_function_moments) {
+        st = DSP_ERR_INVALID_INPUT;
+      } else {
+        const int64_t l0 = b->layer_offset[i];
+        c.special = true;
+        c.L = b->num_layers[i];
+        c.N = b->num_streams[i];
+        c.nmom = b->num_phase_func_moments[i];
+        c.pc = b->pmom_count;
+        c.dmplus = (fl & DSP_FLAG_DELTA_M_PLUS) != 0;
+        c.ifb = (fl & DSP_FLAG_INDEX_FROM_BOTTOM) != 0;
+        c.user_mu = (fl & DSP_GFLAG_USER_MU) != 0;
+        c.alb = scalar(b->surface_albedo, i, 0.0);
+        c.dtau = b->delta_tau + l0;
+        c.ssa = b->single_scat_albedo + l0;
+        c.pmom = b->phase_function_moments + l0 * b->pmom_count;
+        c.numu = b->num_user_mu;
+        c.umu = at(b->mu_user, i);
+        const int half = c.user_mu ? c.numu : c.N / 2;
+        if (c.L > 0 && b->layer_offset[i + 1] - l0 != c.L) st = DSP_ERR_INVALID_INPUT;
+        else if (half > o->numu_out || c.N > 64) st = DSP_ERR_INVALID_INPUT;
+        else {
+          oracle::GeneralOutput go;
+          std::vector<double> f8((size_t)8 * (c.L + 1));
+          for (int f = 0; f < 8; ++f) go.flux[f] = f8.data() + (size_t)f * (c.L + 1);
+          go.intensity = go.iavg = nullptr;
+          go.ntau_out = c.L + 1;
+          go.numu_out = 2 * half;
+          go.albtrans[0] = o->albedo_medium + (size_t)o->numu_out * i;
+          go.albtrans[1] = o->transmissivity_medium + (size_t)o->numu_out * i;
+          go.albtrans[2] = o->spherical_albedo + i;
+          go.albtrans[3] = o->spherical_transmissivity + i;
+          st = solver.solve(c, go);
+        }
+      }
+      if (o->status) o->status[i] = st;
+      if (st > local_worst) local_worst = st;
+    }
+#pragma omp critical
+    if (local_worst > worst) worst = local_worst;
+  }
+  return worst;
+}
+
 // Gauss-Legendre nodes/weights and Legendre table as the reference builds them
 // (FluxSolver.cpp:257-290 and :126); used by tests to cross-check the engine's
 // per-stream constant tables.

@@ -153,6 +153,12 @@ CASES = [
     dict(test="NewICHG3b", N=16, L=1, nmom=16, dtau=[8.0], ssa=[1.0], phase=[("hg", 0.75)],
          fbeam=PI, umu0=1.0, corr=True, tab=(0.75, 100), utau=[0.0, 8.0],
          umu=[-1.0, -0.5, -0.1, 0.1, 0.5, 1.0], phi=[0.0]),
+    # ibcnd = Special (test_solver.cpp:4206-4318): albedo and transmissivity of the medium at
+    # mu 0.5 with the spherical-albedo correction of a 0.5 surface albedo
+    dict(test="SpecialBC13a", N=16, L=1, nmom=0, dtau=[1.0], ssa=[0.99], phase=[("hg", 0.8)],
+         albedo=0.5, special=True, umu=[0.5]),
+    dict(test="SpecialBC13c", N=16, L=2, nmom=0, dtau=[0.5, 0.5], ssa=[0.99, 0.5], phase=[("hg", 0.8)],
+         albedo=0.5, special=True, umu=[0.5]),
     # disotest 12a (test_solver.cpp:3637-3700): 20 streams (oracle only; the engine takes 4-16, 32, 64)
     dict(test="ValidationDisotest12a", N=20, L=1, nmom=20, dtau=[20.1], ssa=[0.5], phase=[("hg", 0.9)],
          fbeam=1.0, umu0=1.0, albedo=1.0, corr=True, utau=[0.0, 10.0, 19.9, 20.1],
@@ -233,6 +239,14 @@ def moments(phase, nmom_nstr: int, cloud: list) -> list:
     return pm
 
 
+def albtrans_expectations(body: str) -> list:
+    """EXPECT_NEAR lines on albedo_medium / transmissivity_medium (ibcnd = Special)."""
+    pat = re.compile(r"EXPECT_NEAR\(\s*\w+\.(albedo_medium|transmissivity_medium)\[(\d+)\]\s*,\s*([-+0-9.eE]+)\s*,"
+                     r"\s*([^;]+)\);")
+    return [dict(field=m.group(1), index=int(m.group(2)), value=float(m.group(3)),
+                 tol=float(eval(m.group(4), {}, {}))) for m in pat.finditer(body)]
+
+
 def tabulated(tab, L: int) -> dict:
     """The HG phase function on a uniform cosine grid, as makeNewICTestConfig1Layer fills it."""
     if tab is None:
@@ -280,6 +294,7 @@ def main():
             brdf_type=c["brdf"][0] if "brdf" in c else 0,
             brdf_params=c["brdf"][1] if "brdf" in c else [],
             intensity_corrected=bool(c.get("corr", False)),
+            special_bc=bool(c.get("special", False)), expect_albtrans=albtrans_expectations(body),
             **tabulated(c.get("tab"), L),
             expect_flux=fl, expect_intensity=it,
         ))

@@ -15,7 +15,14 @@ def load_cases() -> list:
     """The plane-parallel cases over a Lambertian surface (every solver path supports them)."""
     with open(GOLDEN) as f:
         return [c for c in json.load(f)["cases"]
-                if not c.get("use_spherical_beam") and not c.get("brdf_type") and not c.get("intensity_corrected")]
+                if not c.get("use_spherical_beam") and not c.get("brdf_type") and not c.get("intensity_corrected")
+                and not c.get("special_bc")]
+
+
+def load_special_cases() -> list:
+    """The ibcnd = Special cases (albedo and transmissivity of the medium)."""
+    with open(GOLDEN) as f:
+        return [c for c in json.load(f)["cases"] if c.get("special_bc")]
 
 
 def load_corrected_cases(engine_only: bool = False) -> list:

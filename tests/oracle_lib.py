@@ -93,3 +93,14 @@ def general_solve_jac(d: dict, nthreads: int = 0, ext: bool = False):
     jac, jo, keep3 = capi.alloc_general_jac_numpy(d)
     lib.oracle_general_bands_solve_jac(ctypes.byref(batch), ctypes.byref(o), ctypes.byref(jo), nthreads)
     return outs, jac
+
+
+def general_albtrans(d: dict, nthreads: int = 0, ext: bool = False):
+    """ibcnd = Special through the oracle: albedo/transmissivity outputs dict."""
+    lib = load(ext=ext)
+    lib.oracle_general_bands_albtrans.restype = c_int
+    lib.oracle_general_bands_albtrans.argtypes = [POINTER(capi.GeneralBatch), POINTER(capi.AlbTransOut), c_int]
+    batch, keep = capi.make_general_batch(d)
+    outs, o, keep2 = capi.alloc_albtrans_numpy(d)
+    lib.oracle_general_bands_albtrans(ctypes.byref(batch), ctypes.byref(o), nthreads)
+    return outs

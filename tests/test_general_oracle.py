@@ -271,3 +271,40 @@ def test_general_oracle_brdf_rejections():
     assert o["status"][0] == 0
     o = oracle_lib.general_solve(capi.pack_general([dict(inst, surface_albedo=7.0)], fl))
     assert o["status"][0] == capi.DSP_ERR_INVALID_INPUT
+
+
+SPECIAL_CASES = gc.load_special_cases()
+
+
+@pytest.mark.parametrize("case", SPECIAL_CASES, ids=[c["name"] for c in SPECIAL_CASES])
+def test_general_oracle_special_bc_goldens(case):
+    """ibcnd = Special: albedo and transmissivity of the medium (computeAlbTrans)
+    against the reference's C-DISORT values, spherical-albedo correction included."""
+    inst, flags = gc.general_instance(case)
+    o = oracle_lib.general_albtrans(capi.pack_general([inst], flags))
+    assert o["status"][0] == 0
+    assert case["expect_albtrans"]
+    for e in case["expect_albtrans"]:
+        v = o[e["field"]][0, e["index"]]
+        assert abs(v - e["value"]) <= e["tol"], (e, v)
+    assert 0.0 < o["spherical_albedo"][0] < 1.0 and 0.0 < o["spherical_transmissivity"][0] < 1.0
+
+
+def test_general_oracle_special_bc_reciprocity():
+    """Without a surface the albedo of the medium at mu equals the beam albedo of a
+    general solve lit at mu (flux_up at the top / (mu F0)), and the transmissivity the
+    total downward flux at the bottom (the reference's 13b/13d verification)."""
+    rng = np.random.default_rng(13)
+    for L in (1, 3):
+        inst = random_instance(rng, 16, L, thermal=False, beam=False)
+        inst.update(surface_albedo=0.0, mu_user=[0.3, 0.5, 0.9])
+        a = oracle_lib.general_albtrans(capi.pack_general([inst], capi.GFLAG_USER_MU))
+        assert a["status"][0] == 0
+        assert a["spherical_albedo"][0] == 0.0
+        for k, mu0 in enumerate((0.3, 0.5, 0.9)):
+            beam = dict(inst, direct_beam_flux=1.0 / mu0, direct_beam_mu=mu0, isotropic_flux_top=0.0)
+            beam.pop("mu_user")
+            g = oracle_lib.general_solve(capi.pack_general([beam], capi.GFLAG_ONLY_FLUXES))
+            np.testing.assert_allclose(a["albedo_medium"][0, k], g["flux_up"][0, 0], rtol=1e-3)
+            np.testing.assert_allclose(a["transmissivity_medium"][0, k],
+                                       g["flux_down"][0, L] + g["flux_direct_beam"][0, L], rtol=1e-3)
