@@ -524,9 +524,13 @@ def general_parity(gpu: dict, idx, ref: dict, rtol=1e-9, atol=1e-12, floor_ref: 
     largest |intensity|) (a Fourier sum whose terms cancel); <= 1 passes.
 
     With `floor_ref` (the double build's outputs when `ref` is the extended-
-    precision build) an element's allowance is also at least the distance
-    between the two oracle builds there: the FP64 rounding floor of the
-    formulation itself, which no FP64 solver is held below."""
+    precision build) an element's allowance is also at least twice the
+    instance's FP64 rounding floor: the largest relative distance between the
+    two oracle builds over the instance's values of the field (values above
+    1e-6 of its largest), times the element's magnitude.  That floor belongs to
+    the formulation, which no FP64 solver (the reference included) is held
+    below; two independent FP64 evaluations sit within about twice it of each
+    other."""
     worst, where = 0.0, None
     for f in capi.FLUX_OUT_FIELDS + ("intensity", "intensity_azimuth_avg"):
         a = np.asarray(gpu[f])[idx]
@@ -538,7 +542,13 @@ def general_parity(gpu: dict, idx, ref: dict, rtol=1e-9, atol=1e-12, floor_ref: 
         else:
             denom = rtol * np.abs(b) + atol
         if floor_ref is not None:
-            denom = np.maximum(denom, np.abs(np.asarray(floor_ref[f]) - b))
+            dbl = np.asarray(floor_ref[f])
+            flat_b = np.abs(np.nan_to_num(b)).reshape(b.shape[0], -1)
+            flat_d = np.abs(np.nan_to_num(dbl - b)).reshape(b.shape[0], -1)
+            big = flat_b >= 1e-6 * flat_b.max(axis=1, keepdims=True)
+            floor = np.where(big, flat_d / np.maximum(flat_b, 1e-300), 0.0).max(axis=1)
+            floor = floor.reshape((-1,) + (1,) * (b.ndim - 1))
+            denom = np.maximum(denom, 2.0 * floor * np.abs(b))
         r = np.abs(a - b) / denom
         r = np.where(np.isnan(a) & np.isnan(b), 0.0, np.where(np.isnan(r), np.inf, r))
         k = float(r.max()) if r.size else 0.0

@@ -1,6 +1,7 @@
 """Build the native libraries of disort_b200 in-tree.
 
     python -m disort_b200.build          # libdsp.so (sm_100a) + the Python host module
+    python -m disort_b200.build --phase-clock   # tracing build of the flux path (lib/phase/)
 
 libdsp.so is compiled with nvcc for sm_100a only (-gencode arch=compute_100a,
 code=sm_100a); the host-side Python module (_disortpp) is compiled with g++
@@ -115,6 +116,24 @@ def build_host(force: bool = False) -> str:
     return mod
 
 
+def build_phase_clock(force: bool = False) -> str:
+    """lib/phase/libdsp.so: libdsp.so with the flux path's phase markers counting
+    cycles (csrc/instrument/phase_clock.cuh force-included into dsp_capi.cu);
+    the other objects are the product build's.  Read by disort_b200.phase_profile."""
+    target_dir = os.path.join(LIB, "phase")
+    os.makedirs(target_dir, exist_ok=True)
+    target = os.path.join(target_dir, "libdsp.so")
+    build_libdsp()
+    hdr = os.path.join(CSRC, "instrument", "phase_clock.cuh")
+    if force or _stale(target, _deps(".cu", ".cuh", ".h", ".hpp") + [hdr]):
+        obj = os.path.join(target_dir, "dsp_capi.o")
+        _run([NVCC, *ARCH, "-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC", "-diag-suppress", "177",
+              "-include", hdr, "-c", "-o", obj, os.path.join(CSRC, "dsp_capi.cu")])
+        _run([NVCC, *ARCH, "-shared", "-o", target, obj, os.path.join(LIB, "obj", "dsp_general.o"),
+              os.path.join(LIB, "obj", "dsp_noalloc.o")])
+    return target
+
+
 def build_all(force: bool = False) -> None:
     build_libdsp(force)
     build_emu(force)
@@ -123,4 +142,7 @@ def build_all(force: bool = False) -> None:
 
 
 if __name__ == "__main__":
-    build_all(force="--force" in sys.argv)
+    if "--phase-clock" in sys.argv:
+        build_phase_clock(force="--force" in sys.argv)
+    else:
+        build_all(force="--force" in sys.argv)

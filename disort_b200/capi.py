@@ -456,6 +456,8 @@ def load_library(path: str | None = None):
     lib.dsp_context_set_stream.restype = c_int32
     lib.dsp_context_set_stream.argtypes = [c_void_p, c_void_p]
     lib.dsp_context_last_error.restype = ctypes.c_char_p
+    lib.dsp_general_bands_albtrans.restype = c_int32
+    lib.dsp_general_bands_albtrans.argtypes = [c_void_p, POINTER(GeneralBatch), POINTER(AlbTransOut)]
     lib.dsp_context_last_error.argtypes = [c_void_p]
     lib.dsp_flux_workspace_bytes.restype = c_int64
     lib.dsp_flux_workspace_bytes.argtypes = [POINTER(FluxBatch)]
@@ -545,6 +547,10 @@ class Context:
 
     def general_bands_solve_jac(self, batch: GeneralBatch, out: GeneralOut, jac: GeneralJacOut) -> int:
         return self.lib.dsp_general_bands_solve_jac(self.h, ctypes.byref(batch), ctypes.byref(out), ctypes.byref(jac))
+
+    def general_bands_albtrans(self, batch: GeneralBatch, out: AlbTransOut) -> int:
+        """ibcnd = Special: albedo and transmissivity of the medium (host pointers)."""
+        return self.lib.dsp_general_bands_albtrans(self.h, ctypes.byref(batch), ctypes.byref(out))
 
     def set_debug(self, flags: int) -> int:
         """DSP_DEBUG_* flags (DEBUG_POISON_SCRATCH: NaN-filled workspace before each chunk)."""

@@ -336,6 +336,139 @@ extern "C" dsp_status dsp_general_bands_solve_jac(dsp_context ctx, const dsp_gen
   return general_solve(ctx, bin, out, jac);
 }
 
+// ibcnd = Special (computeAlbTrans, DisortSolver.cpp:4025-4163) from two solves
+// of the general path on the GPU: isotropic unit illumination from the top,
+// then from the bottom, with a black surface, no other source and the user
+// cosines mirrored to [-mu reversed | +mu] (DisortSolver.cpp:52-58, 852-865).
+// The albedo of the medium is the upward intensity at the top under the top
+// illumination; the transmissivity is the downward one at the bottom (one
+// layer) or the upward one at the top under the bottom illumination; both
+// include the boundary's own term, which is the reference's exp(-tau/mu).  The
+// spherical albedo and transmissivity are the corresponding fluxes / pi
+// (albTransSpherical, :4295-4358).
+extern "C" dsp_status dsp_general_bands_albtrans(dsp_context ctx, const dsp_general_batch* bin,
+                                                 const dsp_albtrans_out* out) {
+  if (!ctx) return DSP_ERR_NOT_INITIALIZED;
+  NvtxRange r("dsp_general_bands_albtrans");
+  if (!bin || !out || !out->albedo_medium || !out->transmissivity_medium || !out->spherical_albedo ||
+      !out->spherical_transmissivity)
+    return fail(ctx, DSP_ERR_INVALID_INPUT, "null batch or albedo/transmissivity output");
+  const dsp_general_batch& b = *bin;
+  if (b.flags & DSP_FLAG_DEVICE_POINTERS)
+    return fail(ctx, DSP_ERR_UNSUPPORTED, "dsp_general_bands_albtrans takes host pointers");
+  const int n = b.n_inst;
+  if (n < 0) return fail(ctx, DSP_ERR_INVALID_INPUT, "n_inst must be >= 0");
+  if (n == 0) return DSP_OK;
+  if (!b.num_streams || !b.num_layers || !b.layer_offset)
+    return fail(ctx, DSP_ERR_INVALID_INPUT, "num_streams, num_layers and layer_offset are required");
+  const bool user_mu = (b.flags & DSP_GFLAG_USER_MU) != 0;
+  if (user_mu && (b.num_user_mu <= 0 || !b.mu_user.ptr))
+    return fail(ctx, DSP_ERR_INVALID_INPUT, "num_user_mu must be positive when use_user_mu=true");
+  int maxL = 0;
+  for (int i = 0; i < n; ++i) {
+    maxL = std::max(maxL, b.num_layers[i]);
+    if (!user_mu && b.num_streams[i] != b.num_streams[0])
+      return fail(ctx, DSP_ERR_INVALID_INPUT, "without user angles every instance needs the same num_streams");
+  }
+  const int half = user_mu ? b.num_user_mu : b.num_streams[0] / 2;
+  if (out->numu_out < half) return fail(ctx, DSP_ERR_INVALID_INPUT, "numu_out is smaller than the number of angles");
+  // the mirrored cosines, shared or per instance
+  const int nu2 = 2 * half;
+  std::vector<double> umu2;
+  const bool shared_mu = !user_mu || b.mu_user.stride == 0;
+  const int nlist = shared_mu ? 1 : n;
+  umu2.resize((size_t)nlist * nu2);
+  for (int k = 0; k < nlist; ++k) {
+    double* d = umu2.data() + (size_t)k * nu2;
+    std::vector<double> pos(half);
+    if (user_mu) {
+      for (int iu = 0; iu < half; ++iu) pos[iu] = b.mu_user.ptr[b.mu_user.stride * k + iu];
+    } else {
+      std::vector<double> tab;
+      if (!build_tables(b.num_streams[0], tab)) return fail(ctx, DSP_ERR_EIGEN, "Gauss quadrature did not converge");
+      for (int iu = 0; iu < half; ++iu) pos[iu] = tab[tab_mu(b.num_streams[0]) + iu];
+      std::sort(pos.begin(), pos.end());
+    }
+    for (int iu = 0; iu < half; ++iu) {
+      d[half + iu] = pos[iu];
+      d[iu] = -pos[half - 1 - iu];
+    }
+  }
+  static const double one = 1.0, zero = 0.0, phi0 = 0.0;
+  dsp_general_batch g = b;
+  g.flags = (b.flags & (DSP_FLAG_DELTA_M_PLUS | DSP_FLAG_INDEX_FROM_BOTTOM)) | DSP_GFLAG_USER_MU;
+  g.temperature = nullptr;
+  g.level_altitudes = nullptr;
+  g.num_user_tau = 0;
+  g.tau_user = {nullptr, 0};
+  g.num_user_mu = nu2;
+  g.mu_user = {umu2.data(), shared_mu ? 0 : (int64_t)nu2};
+  g.num_phi = 1;
+  g.phi_user = {&phi0, 0};
+  g.accuracy_fourier_series = 0.0;
+  g.surface_albedo = {&zero, 0};
+  g.direct_beam_flux = {&zero, 0};
+  g.brdf_type = DSP_BRDF_LAMBERTIAN;
+  g.num_phase_func_angles = 0;
+  const int ntau = maxL + 1;
+  const size_t nf = (size_t)n * ntau;
+  std::vector<double> fl[2][8], iavg[2], inten(nf * nu2);
+  std::vector<int32_t> st[2];
+  const bool need_bot = maxL > 1;
+  for (int pass = 0; pass < (need_bot ? 2 : 1); ++pass) {
+    g.isotropic_flux_top = {pass == 0 ? &one : &zero, 0};
+    g.isotropic_flux_bottom = {pass == 0 ? &zero : &one, 0};
+    dsp_general_out o{};
+    for (int f = 0; f < 8; ++f) {
+      fl[pass][f].assign(nf, 0.0);
+      o.flux[f] = fl[pass][f].data();
+    }
+    iavg[pass].assign(nf * nu2, 0.0);
+    st[pass].assign(n, 0);
+    o.intensity = inten.data();
+    o.intensity_azimuth_avg = iavg[pass].data();
+    o.status = st[pass].data();
+    o.ntau_out = ntau;
+    o.numu_out = nu2;
+    const dsp_status e = general_solve(ctx, &g, &o, nullptr);
+    if (e != DSP_OK) return e;
+  }
+  const bool ifb = (b.flags & DSP_FLAG_INDEX_FROM_BOTTOM) != 0;
+  for (int i = 0; i < n; ++i) {
+    const int L = b.num_layers[i];
+    int32_t s0 = st[0][i];
+    if (L > 1 && st[1][i] > s0) s0 = st[1][i];
+    if (out->status) out->status[i] = s0;
+    const size_t top = (size_t)i * ntau + (ifb ? L : 0), bot = (size_t)i * ntau + (ifb ? 0 : L);
+    double* am = out->albedo_medium + (size_t)out->numu_out * i;
+    double* tm = out->transmissivity_medium + (size_t)out->numu_out * i;
+    for (int iu = 0; iu < half; ++iu) {
+      // without user angles the reference orders the cosines as its quadrature
+      // (descending); the solve above took them ascending
+      const int up = user_mu ? half + iu : nu2 - 1 - iu, dn = user_mu ? half - 1 - iu : iu;
+      am[iu] = iavg[0][top * nu2 + up];
+      tm[iu] = L == 1 ? iavg[0][bot * nu2 + dn] : iavg[1][top * nu2 + up];
+    }
+    const double alb = b.surface_albedo.ptr ? b.surface_albedo.ptr[b.surface_albedo.stride * i] : 0.0;
+    double sa = 0.0, stt = 0.0;
+    if (alb > 0.0) {
+      // FluxResult order: flux_down is [1], flux_up [2]
+      const int pass = L == 1 ? 0 : 1;
+      const double up = fl[pass][2][top] / M_PI, dn = fl[pass][1][bot] / M_PI;
+      sa = L == 1 ? up : dn;
+      stt = L == 1 ? dn : up;
+      const double corr = alb / (1.0 - alb * sa);
+      for (int iu = 0; iu < half; ++iu) {
+        am[iu] += corr * stt * tm[iu];
+        tm[iu] += corr * sa * tm[iu];
+      }
+    }
+    out->spherical_albedo[i] = sa;
+    out->spherical_transmissivity[i] = stt;
+  }
+  return DSP_OK;
+}
+
 namespace {
 
 // The general solve behind both entry points; `jac` (may be null) adds the

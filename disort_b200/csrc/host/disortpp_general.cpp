@@ -192,9 +192,9 @@ void check_engine(const DisortConfig& c) {
   if (!engine_streams(c.num_streams))
     throw std::invalid_argument("num_streams=" + std::to_string(c.num_streams) +
                                 " is not supported by the B200 engine (supported: 4, 6, 8, 10, 12, 14, 16, 32, 64)");
-  if (f.ibcnd == BoundaryConditionType::Special)
-    throw std::invalid_argument("ibcnd=Special is not supported by the B200 engine");
-  if (!f.use_lambertian_surface) {
+  // ibcnd = Special forces a Lambertian surface (computeAlbTrans,
+  // DisortSolver.cpp:4038-4043): no BRDF is evaluated
+  if (!f.use_lambertian_surface && f.ibcnd != BoundaryConditionType::Special) {
     // the model's spec must be present; the reference finds out inside its
     // solve (bidirReflectivity, DisortSolver.cpp:2902-2936) with these errors
     switch (f.brdf_type) {
@@ -611,6 +611,75 @@ std::vector<DisortResult> run_general(const DisortConfig& c, const std::vector<s
   return res;
 }
 
+// ibcnd = Special over every band (DisortSolver.cpp:52-58, 169-176, 4025-4163):
+// dsp_general_bands_albtrans; the results carry the mirrored cosines, zero
+// fluxes and intensities, and the albedo and transmissivity of the medium in the
+// first half of arrays sized like the mirrored list, as the reference's.
+std::vector<DisortResult> run_special(const DisortConfig& c0, const std::vector<std::pair<double, double>>& bands,
+                                      const SpectralOverrides& ov) {
+  const size_t n = bands.size();
+  std::vector<DisortResult> res(n);
+  if (n == 0) return res;
+  DisortConfig c = c0;
+  const int N = c.num_streams, NN = N / 2;
+  const bool user_mu = c.flags.use_user_mu;
+  const int half = user_mu ? c.num_user_mu : NN;
+  std::vector<double> mirrored(2 * half);
+  if (user_mu) {
+    for (int iu = 0; iu < half; ++iu) {
+      mirrored[half + iu] = c.mu_user[iu];
+      mirrored[iu] = -c.mu_user[half - 1 - iu];
+    }
+  } else {  // the quadrature cosines as the reference orders them (descending)
+    const std::vector<double> mu = quadrature_angles(NN);
+    for (int iu = 0; iu < NN; ++iu) mirrored[iu] = -mu[NN - 1 - iu];
+    for (int iu = NN; iu < N; ++iu) mirrored[iu] = mu[iu - NN];
+  }
+  // the batch of the general solver's layers and moments, nothing else
+  c.flags.use_thermal_emission = false;
+  c.flags.use_spherical_beam = false;
+  c.flags.use_user_tau = false;
+  c.flags.comp_only_fluxes = true;
+  c.flags.use_lambertian_surface = true;
+  c.flags.intensity_corr_buras = false;
+  c.flags.use_user_mu = false;
+  fill_automatic(c);
+  GenPacked pk;
+  dsp_general_batch b = pack_general(c, bands, ov, pk);
+  b.flags &= (DSP_FLAG_DELTA_M_PLUS | DSP_FLAG_INDEX_FROM_BOTTOM);
+  if (user_mu) {
+    pk.umu.assign(c0.mu_user.begin(), c0.mu_user.begin() + half);
+    b.flags |= DSP_GFLAG_USER_MU;
+    b.num_user_mu = half;
+    b.mu_user = {pk.umu.data(), 0};
+  }
+  std::vector<double> am(n * half), tm(n * half), sa(n), st(n);
+  std::vector<int32_t> status(n, 0);
+  dsp_albtrans_out o{am.data(), tm.data(), sa.data(), st.data(), status.data(), half};
+  {
+    std::lock_guard<std::mutex> lk(detail::engine_mutex());
+    dsp_context ctx = detail::engine_context_locked();
+    const dsp_status e = dsp_general_bands_albtrans(ctx, &b, &o);
+    if (e != DSP_OK)
+      throw std::runtime_error(std::string("disortpp: GPU solve failed: ") + dsp_status_string(e) + ": " +
+                               dsp_context_last_error(ctx));
+  }
+  for (size_t i = 0; i < n; ++i)
+    if (status[i] == DSP_ERR_INVALID_INPUT || status[i] == DSP_ERR_UNSUPPORTED)
+      throw std::invalid_argument("band " + std::to_string(i) + ": " + dsp_status_string((dsp_status)status[i]));
+  const int ntau = c0.flags.use_user_tau ? c0.num_user_tau : c0.num_layers + 1;
+  for (size_t i = 0; i < n; ++i) {
+    DisortResult& r = res[i];
+    r.allocate(ntau, 2 * half, c0.num_phi, N, true, !c0.flags.comp_only_fluxes, false);
+    r.mu_angles = mirrored;
+    std::copy(am.begin() + i * half, am.begin() + (i + 1) * half, r.albedo_medium.begin());
+    std::copy(tm.begin() + i * half, tm.begin() + (i + 1) * half, r.transmissivity_medium.begin());
+    r.spherical_albedo = sa[i];
+    r.spherical_transmissivity = st[i];
+  }
+  return res;
+}
+
 void check_override_sizes(const SpectralOverrides& ov, size_t n) {
   auto check = [&](size_t got, const char* name) {
     if (got != 0 && got != n)
@@ -633,6 +702,20 @@ DisortResult DisortSolver::solve(DisortConfig& config) {
   if (config.delta_tau.empty()) config.allocate();
   validate_as_reference(config);
   check_engine(config);
+  if (config.flags.ibcnd == BoundaryConditionType::Special) {
+    std::vector<std::pair<double, double>> one{{config.wavenumber_low, config.wavenumber_high}};
+    DisortResult r = run_special(config, one, SpectralOverrides{})[0];
+    // the config as the reference leaves it: automatic depths and moment 0, the
+    // cosines halved back (DisortSolver.cpp:4615-4620 of computeAlbTrans)
+    const int half = config.flags.use_user_mu ? config.num_user_mu : config.num_streams / 2;
+    const std::vector<double> mirrored = r.mu_angles;
+    fill_automatic(config);
+    config.mu_user = mirrored;
+    config.mu_user.resize(std::max(mirrored.size(), static_cast<size_t>(2 * half + 1)), 0.0);
+    for (int iu = 1; iu <= half; ++iu) config.mu_user[iu] = config.mu_user[iu + half];
+    config.num_user_mu = half;
+    return r;
+  }
   fill_automatic(config);
   std::vector<std::pair<double, double>> one{{config.wavenumber_low, config.wavenumber_high}};
   return run_general(config, one, SpectralOverrides{})[0];
@@ -648,6 +731,7 @@ std::vector<DisortResult> solveSpectralBands(const DisortConfig& config,
   for (size_t i = 0; i < bands.size(); ++i) validate_band(c, ov, i, bands[i].first, bands[i].second);
   if (bands.empty()) return {};
   check_engine(c);
+  if (c.flags.ibcnd == BoundaryConditionType::Special) return run_special(c, bands, ov);
   fill_automatic(c);
   return run_general(c, bands, ov);
 }
