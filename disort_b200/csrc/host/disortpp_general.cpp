@@ -227,8 +227,8 @@ void check_engine(const DisortConfig& c) {
           "intensity_corr_buras with a tabulated phase function needs num_phase_func_angles >= 2, "
           "mu_phase_function and phase_function of every layer");
   }
-  if (f.output_fourier_expansion)
-    throw std::invalid_argument("output_fourier_expansion is not supported by the B200 engine");
+  // output_fourier_expansion: the reference allocates its results without the
+  // expansion (DisortSolver.cpp:122-126), so the array stays empty; so here
   // validate() does not look at the user optical depths; the reference reads
   // tau_user[0 .. num_user_tau-1] whatever its size
   if (f.use_user_tau && (c.num_user_tau <= 0 || c.tau_user.size() < static_cast<size_t>(c.num_user_tau)))

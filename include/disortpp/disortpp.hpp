@@ -156,10 +156,11 @@ void solveFluxSpectralBandsInto(const DisortFluxConfig& config,
 // DisortSolver.hpp:87): plane-parallel or pseudo-spherical beam geometry,
 // Lambertian or bidirectional (BRDF) surface, Fourier azimuth modes, fluxes,
 // intensities at user optical depths and angles, temperature Jacobians.
-// Configurations asking for what the engine does not implement (special
-// boundary conditions, the Fourier-expansion output,
-// stream counts outside 4-16/32/64) pass validate() like in the reference and
-// are rejected with std::invalid_argument when solved.
+// Special boundary conditions (ibcnd = Special) fill albedo_medium and
+// transmissivity_medium; output_fourier_expansion leaves
+// intensity_fourier_expansion empty, as the reference does.  Stream counts
+// outside 4-16/32/64 pass validate() like in the reference and are rejected
+// with std::invalid_argument when solved.
 // ---------------------------------------------------------------------------
 enum class BoundaryConditionType { General = 0, Special = 1 };
 enum class BrdfType { None = 0, RPV = 1, CoxMunk = 2, Ambrals = 3, Hapke = 4 };

@@ -152,7 +152,6 @@ def test_general_engine_rejections_before_any_gpu_work():
     cases = [
         (lambda c: (setattr(c.flags, "intensity_corr_buras", True), setattr(c, "num_phase_func_angles", 8)),
          "needs num_phase_func_angles >= 2, mu_phase_function and phase_function"),
-        (lambda c: setattr(c.flags, "output_fourier_expansion", True), "output_fourier_expansion"),
     ]
     for mutate, msg in cases:
         c = _general_cfg()
