@@ -242,6 +242,15 @@ def committed_traffic(workload_name: str, kernel: str):
         return None
 
 
+def general_traffic(kernel: str, n: int, launches: int):
+    """Average DRAM bytes per launch of the general path's boundary-value kernel
+    on n instances, from the committed per-instance ncu figure."""
+    if kernel != "gen_bvp_kernel" or launches <= 0:
+        return None
+    per = committed_traffic("general_mix", "gen_bvp_kernel_bytes_per_instance")
+    return None if per is None else per * n / launches
+
+
 def run_e2e(args, ctx, w, douts, stream, dev, world):
     """Same solve through the C ABI with pinned host buffers: inputs up, results
     down, inside the timed region.  Returns (solves/s, h2d bytes, d2h bytes,
@@ -709,7 +718,10 @@ def measure_general(ctx, stream, dev, n, seed, steps, warmup, world=1, rank=0, e
                 "frac": (achieved / peak) if peak else None,
                 "peak_source": "measured on this GPU by disort_b200/csrc/fp64_peak.cu (FP64 FMA chains, burst)",
                 "flops_per_step": fl[dom], "flops_total_per_step": fl["total"],
-                "avg_launch_ms": dom_ms / max(1, dom_launches), "traffic": None,
+                "avg_launch_ms": dom_ms / max(1, dom_launches),
+                "traffic": general_traffic(dom, n, dom_launches),
+                "traffic_source": "profiles/traffic.json (ncu DRAM bytes per instance-solve of the boundary-value "
+                                  "kernels on a 512-instance mix, x instances / launches)",
                 "kernel_ms_per_step": {k: v[0] / args.steps for k, v in ktimes.items()},
                 "all_kernels_tflops": fl["total"] * args.steps / (ms_max / 1000.0) / 1e12}
     cpu, parity = None, None
