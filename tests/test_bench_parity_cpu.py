@@ -1,0 +1,58 @@
+"""The bench's parity measure of the general leg (bench.general_parity) on CPU.
+
+Fluxes are compared element-wise at 1e-9 relative + 1e-12 absolute;
+intensities against the instance's largest intensity; with the double oracle
+build given as `floor_ref`, an element may also differ from the extended build
+by twice the instance's FP64 rounding floor (the double build's largest
+relative distance from it over that field)."""
+import numpy as np
+
+import bench
+from disort_b200 import capi
+
+
+def outputs(n=3, nt=4, nu=2, nphi=2, seed=0):
+    rng = np.random.default_rng(seed)
+    o = {f: rng.uniform(0.1, 1.0, (n, nt)) for f in capi.FLUX_OUT_FIELDS}
+    o["intensity"] = rng.uniform(0.1, 1.0, (n, nt, nu, nphi))
+    o["intensity_azimuth_avg"] = rng.uniform(0.1, 1.0, (n, nt, nu))
+    return o
+
+
+def perturbed(o, rel, field="flux_up", at=(1, 2)):
+    p = {k: v.copy() for k, v in o.items()}
+    p[field][at] *= 1.0 + rel
+    return p
+
+
+def test_plain_parity_threshold():
+    ref = outputs()
+    idx = np.arange(3)
+    assert bench.general_parity(perturbed(ref, 5e-10), idx, ref)["passes"]
+    r = bench.general_parity(perturbed(ref, 5e-9), idx, ref)
+    assert not r["passes"] and r["at"].startswith("flux_up(1, 2)")
+
+
+def test_intensity_scaled_by_instance_maximum():
+    """A small intensity in an instance whose largest intensity is big passes
+    at the same absolute error that a relative test would fail."""
+    ref = outputs()
+    ref["intensity"][0] *= 1e-6
+    ref["intensity"][0, 0, 0, 0] = 1.0  # the instance's largest
+    got = {k: v.copy() for k, v in ref.items()}
+    got["intensity"][0, 1, 1, 1] += 5e-10  # 5e-10 of the instance maximum
+    assert bench.general_parity(got, np.arange(3), ref)["passes"]
+
+
+def test_rounding_floor_allowance():
+    ext = outputs()
+    dbl = perturbed(ext, 3e-9, at=(1, 0))  # the double build: 3e-9 off in instance 1
+    idx = np.arange(3)
+    # the GPU 5e-9 off elsewhere in instance 1: within twice the instance's floor
+    gpu = perturbed(ext, 5e-9, at=(1, 3))
+    assert not bench.general_parity(gpu, idx, ext)["passes"]
+    assert bench.general_parity(gpu, idx, ext, floor_ref=dbl)["passes"]
+    # 7e-9 is more than twice the floor; and the floor of instance 1 does not
+    # cover instance 2
+    assert not bench.general_parity(perturbed(ext, 7e-9, at=(1, 3)), idx, ext, floor_ref=dbl)["passes"]
+    assert not bench.general_parity(perturbed(ext, 5e-9, at=(2, 3)), idx, ext, floor_ref=dbl)["passes"]
