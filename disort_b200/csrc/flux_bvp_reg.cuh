@@ -566,39 +566,61 @@ __device__ __forceinline__ void bvp_reg_instance(const FluxParams& p, const int 
     // (computeFluxes, FluxSolver.cpp:1184-1188, 1216-1219)
     const double ch = SPH && beam ? SR(l)[sph_ch(N)] : 0.0;
     const double fact = beam ? (SPH ? exp(-utaupr / ch) : exp(-utaupr * rumu0)) : 0.0;
+    double s = 0.0;
     if (t < N) {
-      double s = 0.0;
 #pragma unroll
       for (int j = 0; j < N; ++j) s += ld_rec(Gl + t * GS + j) * ec[j];
       if (beam) s += SPH ? zsph(lr, l, t, utaupr) : ld_rec(lr + C::SZB + t) * fact;
       if (thermal) s += ld_rec(lr + C::SZ0 + t) + ld_rec(lr + C::SZ1 + t) * utaupr;
-      Iv[t] = s;
     }
-    __syncwarp(msk);
+    // the quadrature sums over the streams' intensities: at 16 streams as
+    // reductions over lanes 0-7 (downward streams) and 8-15 (upward), else by
+    // lane 0 from shared memory
+    double ua = 0.0, uad = 0.0, uau = 0.0, fldn = 0.0, fup = 0.0;
+    if constexpr (TEAM == 32 && NN == 8) {
+      const int cw = t < NN ? NN - t - 1 : t - NN;
+      double a = t < N ? wt[cw < NN ? cw : 0] * s : 0.0;
+      double b = t < N ? a * mu[cw < NN ? cw : 0] : 0.0;
+#pragma unroll
+      for (int off = 4; off > 0; off >>= 1) {
+        a += __shfl_xor_sync(msk, a, off);
+        b += __shfl_xor_sync(msk, b, off);
+      }
+      const double a8 = __shfl_sync(msk, a, 8), b8 = __shfl_sync(msk, b, 8);
+      uad = a;
+      fldn = b;
+      uau = a8;
+      fup = b8;
+      ua = uad + uau;
+    } else {
+      if (t < N) Iv[t] = s;
+      __syncwarp(msk);
+      if (t == 0) {
+        double iv[N];
+#pragma unroll
+        for (int k = 0; k < N; ++k) iv[k] = Iv[k];
+#pragma unroll
+        for (int iq = 0; iq < NN; ++iq) {
+          const int cw = NN - iq - 1;
+          ua += wt[cw] * iv[iq];
+          uad += wt[cw] * iv[iq];
+          fldn += wt[cw] * iv[iq] * mu[cw];
+        }
+#pragma unroll
+        for (int iq = NN; iq < N; ++iq) {
+          const int cw = iq - NN;
+          ua += wt[cw] * iv[iq];
+          uau += wt[cw] * iv[iq];
+          fup += wt[cw] * iv[iq] * mu[cw];
+        }
+      }
+    }
     if (t == 0) {
       double dirint = 0.0, fldir = 0.0, fdir = 0.0;
       if (beam) {
         dirint = fbeam * fact;
         fldir = umu0 * fbeam * fact;
         fdir = SPH ? fabs(umu0) * fbeam * exp(-utau / ch) : umu0 * fbeam * exp(-utau * rumu0);
-      }
-      double iv[N];
-#pragma unroll
-      for (int k = 0; k < N; ++k) iv[k] = Iv[k];
-      double ua = 0.0, uad = 0.0, uau = 0.0, fldn = 0.0, fup = 0.0;
-#pragma unroll
-      for (int iq = 0; iq < NN; ++iq) {
-        const int cw = NN - iq - 1;
-        ua += wt[cw] * iv[iq];
-        uad += wt[cw] * iv[iq];
-        fldn += wt[cw] * iv[iq] * mu[cw];
-      }
-#pragma unroll
-      for (int iq = NN; iq < N; ++iq) {
-        const int cw = iq - NN;
-        ua += wt[cw] * iv[iq];
-        uau += wt[cw] * iv[iq];
-        fup += wt[cw] * iv[iq] * mu[cw];
       }
       fup *= 2.0 * PI;
       fldn *= 2.0 * PI;
