@@ -209,3 +209,22 @@ def test_buras_emde_through_solver_object():
     fl = capi.GFLAG_USER_TAU | capi.GFLAG_USER_MU | capi.GFLAG_INTENSITY_CORR | capi.GFLAG_INTENSITY_CORR_BE
     got, ref, _ = both([inst], fl)
     np.testing.assert_allclose(np.asarray(r.intensity), got["intensity"][0], rtol=1e-12, atol=1e-15)
+
+
+def test_deep_columns_brdf_and_correction_against_extended_oracle():
+    """32 and 64 streams, 60-100 layers, an RPV surface and the Nakajima-Tanaka
+    correction over every azimuth mode: against the extended-precision oracle,
+    each element allowed 1e-9 (intensities: of the instance's largest) or twice
+    the instance's FP64 rounding floor (the double oracle's own distance from
+    the extended one), the bench's parity of record."""
+    import bench
+    insts, flags = corr_mix(2, seed=77, nstr=(32, 64), layers=(60, 100))
+    for c in insts:
+        c.update(brdf_type=capi.BRDF_RPV, brdf_params=[0.12, 0.85, -0.15, 0.0, 0.0, 0.0, 1.0])
+    d = capi.pack_general(insts, flags)
+    got, rc = gpu_lib.general_solve(d)
+    assert rc == 0 and (got["status"] == 0).all()
+    ext = oracle_lib.general_solve(d, ext=True)
+    dbl = oracle_lib.general_solve(d)
+    r = bench.general_parity(got, np.arange(len(insts)), ext, floor_ref=dbl)
+    assert r["passes"], r
