@@ -518,6 +518,9 @@ def general_oracle_lib(ext: bool = False):
     return lib
 
 
+ULP_COPIES = 2  # one-ulp-perturbed copies of the sample behind the FP64 floor
+
+
 def general_cpu_time(lib, insts, flags, threads, keep_outputs=False):
     d = capi.pack_general(insts, flags, pmom_count=66)
     b, keep = capi.make_general_batch(d)
@@ -528,19 +531,45 @@ def general_cpu_time(lib, insts, flags, threads, keep_outputs=False):
     return (t, outs) if keep_outputs else t
 
 
-def general_parity(gpu: dict, idx, ref: dict, rtol=1e-9, atol=1e-12, floor_ref: dict | None = None) -> dict:
+def ulp_perturbed(inst: dict, rng) -> dict:
+    """A copy of a general instance whose layer optical depths, single-
+    scattering albedos and phase-function moments past the zeroth each move one
+    ulp up or down at random (zeros stay, albedos stay <= 1); user depths at the
+    half and the full column follow its new total.  The double oracle's spread
+    over such copies is how closely the FP64-representable inputs determine an
+    instance's outputs."""
+    p = dict(inst)
+    for k in ("delta_tau", "single_scat_albedo", "phase_function_moments"):
+        a = np.asarray(inst[k], dtype=np.float64)
+        up = rng.integers(0, 2, a.shape).astype(bool)
+        b = np.where(up, np.nextafter(a, np.inf), np.nextafter(a, -np.inf))
+        b = np.where(a == 0.0, a, b)
+        if k == "single_scat_albedo":
+            b = np.where(a <= 1.0, np.minimum(b, 1.0), b)
+        if k == "phase_function_moments":
+            b[..., 0] = a[..., 0]
+        p[k] = b
+    if inst.get("tau_user") is not None:
+        t0 = workloads.column_total(np.asarray(inst["delta_tau"], dtype=np.float64))
+        t1 = workloads.column_total(p["delta_tau"])
+        p["tau_user"] = [t1 if t == t0 else t1 / 2.0 if t == t0 / 2.0 else t for t in inst["tau_user"]]
+    return p
+
+
+def general_parity(gpu: dict, idx, ref: dict, rtol=1e-9, atol=1e-12, floor_ref=None) -> dict:
     """Fluxes element-wise; intensities against max(|value|, the instance's
     largest |intensity|) (a Fourier sum whose terms cancel); <= 1 passes.
 
-    With `floor_ref` (the double build's outputs when `ref` is the extended-
-    precision build) an element's allowance is also at least twice the
-    instance's FP64 rounding floor: the largest relative distance between the
-    two oracle builds over the instance's values of the field (values above
-    1e-6 of its largest), times the element's magnitude.  That floor belongs to
-    the formulation, which no FP64 solver (the reference included) is held
-    below; two independent FP64 evaluations sit within about twice it of each
-    other."""
-    worst, where = 0.0, None
+    With `floor_ref` (FP64 evaluations when `ref` is the extended-precision
+    build: one output dict or a list of them, the double build on the given
+    inputs and on one-ulp-perturbed copies) an element's allowance is also at
+    least twice the instance's FP64 floor: the largest relative distance from
+    `ref` of any of those evaluations over the instance's values of the field
+    (values above 1e-6 of its largest and above `atol`; instances an evaluation
+    did not solve left out), times the element's magnitude.  That floor belongs to the
+    formulation, which no FP64 solver (the reference included) is held below."""
+    floor_refs = [] if floor_ref is None else [floor_ref] if isinstance(floor_ref, dict) else list(floor_ref)
+    worst, where, floor_max = 0.0, None, 0.0
     for f in capi.FLUX_OUT_FIELDS + ("intensity", "intensity_azimuth_avg"):
         a = np.asarray(gpu[f])[idx]
         b = np.asarray(ref[f])
@@ -550,12 +579,17 @@ def general_parity(gpu: dict, idx, ref: dict, rtol=1e-9, atol=1e-12, floor_ref: 
             denom = rtol * np.maximum(np.abs(b), scale) + atol
         else:
             denom = rtol * np.abs(b) + atol
-        if floor_ref is not None:
-            dbl = np.asarray(floor_ref[f])
+        if floor_refs:
             flat_b = np.abs(np.nan_to_num(b)).reshape(b.shape[0], -1)
-            flat_d = np.abs(np.nan_to_num(dbl - b)).reshape(b.shape[0], -1)
-            big = flat_b >= 1e-6 * flat_b.max(axis=1, keepdims=True)
-            floor = np.where(big, flat_d / np.maximum(flat_b, 1e-300), 0.0).max(axis=1)
+            big = flat_b >= np.maximum(1e-6 * flat_b.max(axis=1, keepdims=True), atol)
+            floor = np.zeros(b.shape[0])
+            for fr in floor_refs:
+                flat_d = np.abs(np.nan_to_num(np.asarray(fr[f]) - b)).reshape(b.shape[0], -1)
+                fl = np.where(big, flat_d / np.maximum(flat_b, 1e-300), 0.0).max(axis=1)
+                if "status" in fr:
+                    fl = np.where(np.asarray(fr["status"]).reshape(-1) == 0, fl, 0.0)
+                floor = np.maximum(floor, fl)
+            floor_max = max(floor_max, float(floor.max()) if floor.size else 0.0)
             floor = floor.reshape((-1,) + (1,) * (b.ndim - 1))
             denom = np.maximum(denom, 2.0 * floor * np.abs(b))
         r = np.abs(a - b) / denom
@@ -563,8 +597,11 @@ def general_parity(gpu: dict, idx, ref: dict, rtol=1e-9, atol=1e-12, floor_ref: 
         k = float(r.max()) if r.size else 0.0
         if k > worst:
             worst, where = k, f + str(tuple(int(x) for x in np.unravel_index(int(np.argmax(r)), r.shape)))
-    return {"max_ratio": worst, "at": where, "rtol": rtol, "atol": atol, "instances_compared": int(len(idx)),
-            "passes": worst <= 1.0}
+    out = {"max_ratio": worst, "at": where, "rtol": rtol, "atol": atol, "instances_compared": int(len(idx)),
+           "passes": worst <= 1.0}
+    if floor_refs:
+        out["fp64_floor_max"] = floor_max
+    return out
 
 
 def general_cpu_sample(insts, target_s: float):
@@ -739,12 +776,20 @@ def measure_general(ctx, stream, dev, n, seed, steps, warmup, world=1, rank=0, e
             if ext_parity:
                 # the checker of record: the extended-precision build, each
                 # element allowed max(1e-9 rel + 1e-12, twice the instance's FP64
-                # rounding floor, the double build's own distance from it); the
-                # plain comparisons with both builds beside it
+                # floor: the farthest of the double build on the given inputs
+                # and on one-ulp-perturbed copies); the plain comparisons with
+                # both builds beside it
                 _, ref_ext = general_cpu_time(general_oracle_lib(ext=True), sample, flags, threads, keep_outputs=True)
-                parity = general_parity(got, idx, ref_ext, floor_ref=ref)
+                floor_refs = [ref]
+                for copy_no in range(ULP_COPIES):
+                    rng = np.random.default_rng(1000 + copy_no)
+                    floor_refs.append(general_cpu_time(lib, [ulp_perturbed(c, rng) for c in sample], flags,
+                                                       threads, keep_outputs=True)[1])
+                parity = general_parity(got, idx, ref_ext, floor_ref=floor_refs)
                 parity["checker"] = ("oracle (extended precision), allowance max(1e-9 rel + 1e-12 abs, twice the "
-                                     "instance's FP64 rounding floor)")
+                                     "instance's FP64 floor: the largest distance from it of the double build on "
+                                     f"the given inputs and on {ULP_COPIES} copies with every layer input moved "
+                                     "one ulp)")
                 parity["vs_extended_precision_oracle"] = general_parity(got, idx, ref_ext)
                 parity["vs_double_oracle"] = vs_double
     return {

@@ -1,10 +1,11 @@
 """The bench's parity measure of the general leg (bench.general_parity) on CPU.
 
 Fluxes are compared element-wise at 1e-9 relative + 1e-12 absolute;
-intensities against the instance's largest intensity; with the double oracle
-build given as `floor_ref`, an element may also differ from the extended build
-by twice the instance's FP64 rounding floor (the double build's largest
-relative distance from it over that field)."""
+intensities against the instance's largest intensity; with FP64 evaluations
+given as `floor_ref` (the double oracle build on the given inputs and on
+one-ulp-perturbed copies of them), an element may also differ from the
+extended build by twice the instance's FP64 floor (the farthest of those
+evaluations' relative distances from it over that field)."""
 import numpy as np
 
 import bench
@@ -56,3 +57,43 @@ def test_rounding_floor_allowance():
     # cover instance 2
     assert not bench.general_parity(perturbed(ext, 7e-9, at=(1, 3)), idx, ext, floor_ref=dbl)["passes"]
     assert not bench.general_parity(perturbed(ext, 5e-9, at=(2, 3)), idx, ext, floor_ref=dbl)["passes"]
+
+
+def test_floor_over_several_evaluations():
+    """The floor is the farthest of several FP64 evaluations; one that did not
+    solve the instance, and values below the absolute tolerance, add nothing."""
+    ext = outputs()
+    idx = np.arange(3)
+    near = perturbed(ext, 1e-10, at=(1, 0))
+    far = perturbed(ext, 3e-9, at=(1, 0))
+    gpu = perturbed(ext, 5e-9, at=(1, 3))
+    assert not bench.general_parity(gpu, idx, ext, floor_ref=[near])["passes"]
+    r = bench.general_parity(gpu, idx, ext, floor_ref=[near, far])
+    assert r["passes"] and abs(r["fp64_floor_max"] - 3e-9) < 1e-12
+    far["status"] = np.array([0, 5, 0])
+    assert not bench.general_parity(gpu, idx, ext, floor_ref=[near, far])["passes"]
+    tiny = {k: v.copy() for k, v in ext.items()}
+    tiny["flux_down"][1] = 1e-18
+    wild = perturbed(tiny, 10.0, field="flux_down", at=(1, 0))
+    r = bench.general_parity(tiny, idx, tiny, floor_ref=wild)
+    assert r["passes"] and r["fp64_floor_max"] == 0.0
+
+
+def test_ulp_perturbed_copy():
+    """Every layer input moves by exactly one ulp; the zeroth moment, zero
+    entries and the albedo bound stay; the user depths follow the new total."""
+    from disort_b200 import workloads
+    insts, _ = workloads.general_mix(4, seed=1)
+    c = dict(insts[0])
+    c["single_scat_albedo"] = np.asarray(c["single_scat_albedo"], dtype=np.float64).copy()
+    c["single_scat_albedo"][:2] = (1.0, 0.0)
+    p = bench.ulp_perturbed(c, np.random.default_rng(0))
+    for k in ("delta_tau", "single_scat_albedo", "phase_function_moments"):
+        a, b = np.asarray(c[k], dtype=np.float64), np.asarray(p[k])
+        moved = a != b
+        assert np.all(np.abs(b[moved] - a[moved]) <= np.spacing(np.abs(a[moved])) * 1.0000001)
+    a = np.asarray(c["phase_function_moments"])
+    assert np.array_equal(np.asarray(p["phase_function_moments"])[..., 0], a[..., 0])
+    assert p["single_scat_albedo"][0] <= 1.0 and p["single_scat_albedo"][1] == 0.0
+    tot = workloads.column_total(p["delta_tau"])
+    assert p["tau_user"][-1] == tot and p["tau_user"][1] == tot / 2.0
