@@ -518,7 +518,7 @@ def general_oracle_lib(ext: bool = False):
     return lib
 
 
-ULP_COPIES = 2  # one-ulp-perturbed copies of the sample behind the FP64 floor
+ULP_COPIES = 2  # one-ulp-perturbed copies of the sample behind the FP64 spread
 
 
 def general_cpu_time(lib, insts, flags, threads, keep_outputs=False):
@@ -562,14 +562,14 @@ def general_parity(gpu: dict, idx, ref: dict, rtol=1e-9, atol=1e-12, floor_ref=N
 
     With `floor_ref` (FP64 evaluations when `ref` is the extended-precision
     build: one output dict or a list of them, the double build on the given
-    inputs and on one-ulp-perturbed copies) an element's allowance is also at
-    least twice the instance's FP64 floor: the largest relative distance from
-    `ref` of any of those evaluations over the instance's values of the field
-    (values above 1e-6 of its largest and above `atol`; instances an evaluation
-    did not solve left out), times the element's magnitude.  That floor belongs to the
-    formulation, which no FP64 solver (the reference included) is held below."""
+    inputs and on one-ulp-perturbed copies) an element's allowance widens to
+    twice the instance's FP64 spread when that is larger: the largest distance
+    from `ref` of any of those evaluations over the instance's values of the
+    field, in units of the same plain allowance (instances an evaluation did not
+    solve left out).  That spread belongs to the formulation, which no FP64
+    solver (the reference included) is held below."""
     floor_refs = [] if floor_ref is None else [floor_ref] if isinstance(floor_ref, dict) else list(floor_ref)
-    worst, where, floor_max = 0.0, None, 0.0
+    worst, where, spread_max = 0.0, None, 0.0
     for f in capi.FLUX_OUT_FIELDS + ("intensity", "intensity_azimuth_avg"):
         a = np.asarray(gpu[f])[idx]
         b = np.asarray(ref[f])
@@ -580,18 +580,15 @@ def general_parity(gpu: dict, idx, ref: dict, rtol=1e-9, atol=1e-12, floor_ref=N
         else:
             denom = rtol * np.abs(b) + atol
         if floor_refs:
-            flat_b = np.abs(np.nan_to_num(b)).reshape(b.shape[0], -1)
-            big = flat_b >= np.maximum(1e-6 * flat_b.max(axis=1, keepdims=True), atol)
-            floor = np.zeros(b.shape[0])
+            spread = np.zeros(b.shape[0])
             for fr in floor_refs:
-                flat_d = np.abs(np.nan_to_num(np.asarray(fr[f]) - b)).reshape(b.shape[0], -1)
-                fl = np.where(big, flat_d / np.maximum(flat_b, 1e-300), 0.0).max(axis=1)
+                rf = (np.abs(np.nan_to_num(np.asarray(fr[f]) - b)) / denom).reshape(b.shape[0], -1)
+                sp = rf.max(axis=1) if rf.size else np.zeros(b.shape[0])
                 if "status" in fr:
-                    fl = np.where(np.asarray(fr["status"]).reshape(-1) == 0, fl, 0.0)
-                floor = np.maximum(floor, fl)
-            floor_max = max(floor_max, float(floor.max()) if floor.size else 0.0)
-            floor = floor.reshape((-1,) + (1,) * (b.ndim - 1))
-            denom = np.maximum(denom, 2.0 * floor * np.abs(b))
+                    sp = np.where(np.asarray(fr["status"]).reshape(-1) == 0, sp, 0.0)
+                spread = np.maximum(spread, sp)
+            spread_max = max(spread_max, float(spread.max()) if spread.size else 0.0)
+            denom = denom * np.maximum(1.0, 2.0 * spread).reshape((-1,) + (1,) * (b.ndim - 1))
         r = np.abs(a - b) / denom
         r = np.where(np.isnan(a) & np.isnan(b), 0.0, np.where(np.isnan(r), np.inf, r))
         k = float(r.max()) if r.size else 0.0
@@ -600,7 +597,7 @@ def general_parity(gpu: dict, idx, ref: dict, rtol=1e-9, atol=1e-12, floor_ref=N
     out = {"max_ratio": worst, "at": where, "rtol": rtol, "atol": atol, "instances_compared": int(len(idx)),
            "passes": worst <= 1.0}
     if floor_refs:
-        out["fp64_floor_max"] = floor_max
+        out["fp64_spread_max"] = spread_max
     return out
 
 
@@ -775,10 +772,10 @@ def measure_general(ctx, stream, dev, n, seed, steps, warmup, world=1, rank=0, e
             parity = vs_double
             if ext_parity:
                 # the checker of record: the extended-precision build, each
-                # element allowed max(1e-9 rel + 1e-12, twice the instance's FP64
-                # floor: the farthest of the double build on the given inputs
-                # and on one-ulp-perturbed copies); the plain comparisons with
-                # both builds beside it
+                # element allowed 1e-9 rel + 1e-12 times max(1, twice the
+                # instance's FP64 spread: the farthest of the double build on
+                # the given inputs and on one-ulp-perturbed copies, in units of
+                # that allowance); the plain comparisons with both builds beside it
                 _, ref_ext = general_cpu_time(general_oracle_lib(ext=True), sample, flags, threads, keep_outputs=True)
                 floor_refs = [ref]
                 for copy_no in range(ULP_COPIES):
@@ -786,10 +783,10 @@ def measure_general(ctx, stream, dev, n, seed, steps, warmup, world=1, rank=0, e
                     floor_refs.append(general_cpu_time(lib, [ulp_perturbed(c, rng) for c in sample], flags,
                                                        threads, keep_outputs=True)[1])
                 parity = general_parity(got, idx, ref_ext, floor_ref=floor_refs)
-                parity["checker"] = ("oracle (extended precision), allowance max(1e-9 rel + 1e-12 abs, twice the "
-                                     "instance's FP64 floor: the largest distance from it of the double build on "
-                                     f"the given inputs and on {ULP_COPIES} copies with every layer input moved "
-                                     "one ulp)")
+                parity["checker"] = ("oracle (extended precision), allowance (1e-9 rel + 1e-12 abs) x max(1, twice "
+                                     "the instance's FP64 spread: the largest distance from it, in those units, of "
+                                     f"the double build on the given inputs and on {ULP_COPIES} copies with every "
+                                     "layer input moved one ulp)")
                 parity["vs_extended_precision_oracle"] = general_parity(got, idx, ref_ext)
                 parity["vs_double_oracle"] = vs_double
     return {
